@@ -1,0 +1,394 @@
+/*
+ * physxcoopa_b200.h -- C-ABI of the B200 (sm_100a) XPBD cloth and hair-strand solver.
+ *
+ * This library replaces the CPU soft-body substep of physxcoopa (a header-only C++20 physics
+ * library) behind its own boundary: `cloth::solve_cloth` (physxcoopa/cloth/cloth_solver.h:158-467)
+ * and `hair::solve_strands` (physxcoopa/hair/strand_solver.h:121-327), batched at the granularity
+ * of their per-frame callers `PhysicsWorld::step_cloths_` / `step_strands_`
+ * (physxcoopa/world.h:1749-1847, 1861-1957).
+ *
+ * Conventions
+ *  - Every entry point returns a pxb_status and never throws or aborts. On failure the context
+ *    keeps a message retrievable with pxb_last_error().
+ *  - One host thread per context. A context owns one CUDA stream on one device; all device work
+ *    is ordered on it.
+ *  - No CPU fallback: an input the device path does not implement (mesh / convex-hull colliders,
+ *    self-collision) is refused with PXB_ERR_UNSUPPORTED instead of being solved on the host.
+ *  - The plain-old-data structs below reproduce the reference's in-memory layouts byte for byte
+ *    (glm::vec3 = 3 floats, glm::quat = x,y,z,w floats, no SIMD alignment), so a C++ caller can
+ *    hand `std::vector<ClothParticle>::data()` and friends straight to this API.
+ */
+#ifndef PHYSXCOOPA_B200_H
+#define PHYSXCOOPA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------ */
+/* Status                                                                                      */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef enum pxb_status {
+    PXB_OK = 0,
+    PXB_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad index, inconsistent sizes */
+    PXB_ERR_UNSUPPORTED = 2,      /* valid reference input the device path does not implement */
+    PXB_ERR_CUDA = 3,             /* a CUDA runtime call failed (message has the CUDA error) */
+    PXB_ERR_OUT_OF_MEMORY = 4,
+    PXB_ERR_INVALID_HANDLE = 5,   /* stale or unknown cloth / strand-set id */
+    PXB_ERR_DEVICE_STATUS = 6,    /* a kernel reported an error word (bounded wait expired, bad index) */
+    PXB_ERR_TOO_LARGE = 7         /* input exceeds a documented capacity limit */
+} pxb_status;
+
+/* ------------------------------------------------------------------------------------------ */
+/* Reference-layout data types                                                                  */
+/* ------------------------------------------------------------------------------------------ */
+
+/* cloth::ClothParticle (physxcoopa/cloth/cloth.h:83-88). 40 bytes. inv_mass == 0 means pinned. */
+typedef struct pxb_particle {
+    float position[3];
+    float prev_position[3];
+    float velocity[3];
+    float inv_mass;
+} pxb_particle;
+
+/* cloth::ClothConstraint (physxcoopa/cloth/cloth.h:103-108). 16 bytes. */
+typedef struct pxb_constraint {
+    uint32_t a;
+    uint32_t b;
+    float rest_length;
+    float lambda;
+} pxb_constraint;
+
+/* cloth::ConstraintBatch (physxcoopa/cloth/cloth.h:270-273): particle-disjoint [begin, end). */
+typedef struct pxb_batch {
+    uint32_t begin;
+    uint32_t end;
+} pxb_batch;
+
+/* cloth::ClothTether (physxcoopa/cloth/cloth.h:122-126). 12 bytes. */
+typedef struct pxb_tether {
+    uint32_t particle;
+    uint32_t anchor;
+    float max_length;
+} pxb_tether;
+
+/* cloth::ClothAnchor (physxcoopa/cloth/cloth.h:140-160), BodyId flattened. 48 bytes.
+ * world_position is this frame's target (resolved by the caller from the body pose, as
+ * PhysicsWorld::step_cloths_ does at world.h:1766-1773); prev_world_position is last frame's. */
+typedef struct pxb_anchor {
+    uint32_t particle;
+    uint32_t body_index;
+    uint32_t body_generation;
+    float local_position[3];
+    float world_position[3];
+    float prev_world_position[3];
+} pxb_anchor;
+
+/* cloth::ClothParams (physxcoopa/cloth/cloth.h:167-256), field for field, plus one extension:
+ * `has_shear_compliance` / `shear_compliance` are NOT in the reference; the reference solves
+ * structural and shear edges with one `stretch_compliance`. Leave has_shear_compliance = 0 for
+ * reference behaviour. pxb_cloth_params_default() returns the reference defaults. */
+typedef struct pxb_cloth_params {
+    float stretch_compliance;
+    float bend_compliance;
+    float damping;
+    float thickness;
+    float friction;
+    float gravity_scale;
+    float max_velocity;
+    float external_acceleration[3];
+    float wind[3];
+    float wind_turbulence;
+    float air_drag;
+    float air_lift;
+    int32_t self_collision;
+    float self_distance;
+    float tether_scale;
+    uint32_t substeps;
+    uint32_t iterations;
+    float sleep_threshold;
+    float sleep_time;
+    uint32_t layer;
+    int32_t has_shear_compliance;
+    float shear_compliance;
+} pxb_cloth_params;
+
+/* collision::ShapeType (physxcoopa/collision/shape.h:33-39). */
+typedef enum pxb_shape_type {
+    PXB_SHAPE_SPHERE = 0,
+    PXB_SHAPE_BOX = 1,
+    PXB_SHAPE_CAPSULE = 2,
+    PXB_SHAPE_TRIANGLE_MESH = 3, /* refused with PXB_ERR_UNSUPPORTED */
+    PXB_SHAPE_CONVEX_HULL = 4    /* refused with PXB_ERR_UNSUPPORTED */
+} pxb_shape_type;
+
+/* cloth::ClothCollider (physxcoopa/cloth/cloth_collision.h:53-78) with the fields of the
+ * collision::Shape it points at (physxcoopa/collision/shape.h:54-102) copied in: the snapshot a
+ * collider is for one step. Quaternions are (x, y, z, w). 144 bytes. */
+typedef struct pxb_collider {
+    int32_t type;               /* pxb_shape_type */
+    int32_t enabled;            /* Shape::enabled; a disabled shape never collides */
+    float position[3];          /* owning body's world position */
+    float orientation[4];       /* owning body's world orientation */
+    float local_center[3];      /* Shape::local_center */
+    float local_rotation[4];    /* Shape::local_rotation */
+    float radius;               /* Sphere */
+    float half_extents[3];      /* Box */
+    float capsule_radius;       /* Capsule */
+    float capsule_half_height;  /* Capsule, cylindrical half-length */
+    int32_t capsule_axis;       /* Capsule long axis: 0=X, 1=Y, 2=Z */
+    float sweep[3];             /* ClothCollider::sweep (PhysicsWorld leaves it zero) */
+    float end_orientation[4];   /* ClothCollider::end_orientation */
+    float bounds_min[3];        /* ClothCollider::bounds (world AABB over both poses) */
+    float bounds_max[3];
+} pxb_collider;
+
+/* PhysicsWorld::GravitySource (physxcoopa/world.h:1154-1159). */
+typedef struct pxb_gravity_source {
+    float centre[3];
+    float strength;
+    float radius;
+    float range; /* 0 = unlimited */
+} pxb_gravity_source;
+
+/* A cloth as the reference stores it (physxcoopa/cloth/cloth.h:284-315): plain pointers into
+ * caller memory, reference layouts. The optional per-batch compliance arrays (NULL = every batch
+ * uses params.stretch_compliance / params.bend_compliance, the reference behaviour) let a caller
+ * give shear edges their own compliance; make_grid_cloth fills them when has_shear_compliance. */
+typedef struct pxb_cloth_desc {
+    const pxb_particle* particles;
+    uint32_t n_particles;
+    const pxb_constraint* stretch;
+    uint32_t n_stretch;
+    const pxb_batch* stretch_batches;
+    uint32_t n_stretch_batches;
+    const pxb_constraint* bend;
+    uint32_t n_bend;
+    const pxb_batch* bend_batches;
+    uint32_t n_bend_batches;
+    const pxb_tether* tethers;
+    uint32_t n_tethers;
+    const pxb_anchor* anchors;
+    uint32_t n_anchors;
+    const uint32_t* triangles; /* 3 indices per triangle */
+    uint32_t n_triangle_indices;
+    uint32_t columns; /* grid dimensions when built by make_grid_cloth, else 0 */
+    uint32_t rows;
+    pxb_cloth_params params;
+    float time;       /* Cloth::time, drives the deterministic wind gust */
+    const float* stretch_batch_compliance; /* optional, n_stretch_batches entries */
+    const float* bend_batch_compliance;    /* optional, n_bend_batches entries */
+} pxb_cloth_desc;
+
+
+/* hair::Strand (physxcoopa/hair/strand.h:79-87). 64 bytes. `first` is the root particle. */
+typedef struct pxb_strand {
+    uint32_t first;
+    uint32_t count;
+    float root_position[3];
+    float root_orientation[4];      /* (x, y, z, w) */
+    float prev_root_position[3];
+    float prev_root_orientation[4]; /* (x, y, z, w) */
+} pxb_strand;
+
+/* hair::StrandParams (physxcoopa/hair/strand.h:93-148), field for field. */
+typedef struct pxb_strand_params {
+    float stretch_compliance;
+    float global_shape;
+    float global_shape_falloff;
+    float local_shape;
+    float damping;
+    float thickness;
+    float friction;
+    float gravity_scale;
+    float max_velocity;
+    float external_acceleration[3];
+    float wind[3];
+    float wind_turbulence;
+    float air_drag;
+    uint32_t substeps;
+    uint32_t iterations;
+    float sleep_threshold;
+    float sleep_time;
+    uint32_t layer;
+} pxb_strand_params;
+
+/* hair::StrandSet (physxcoopa/hair/strand.h:157-191) as plain pointers, reference layouts.
+ * rest_local / rest_offset are 3 floats per particle, parallel to `particles`. */
+typedef struct pxb_strand_set_desc {
+    const pxb_particle* particles;
+    uint32_t n_particles;
+    const pxb_constraint* stretch;
+    uint32_t n_stretch;
+    const pxb_batch* stretch_batches;
+    uint32_t n_stretch_batches;
+    const float* rest_local;
+    const float* rest_offset;
+    const pxb_strand* strands;
+    uint32_t n_strands;
+    pxb_strand_params params;
+    float time;
+} pxb_strand_set_desc;
+
+/* ------------------------------------------------------------------------------------------ */
+/* Context                                                                                      */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct pxb_context pxb_context;
+
+/* Creates a context on CUDA device `device` with its own non-blocking stream. */
+pxb_status pxb_context_create(int device, pxb_context** out);
+pxb_status pxb_context_destroy(pxb_context* ctx);
+/* Message of the last failure on this context ("" if none). Valid until the next call. */
+const char* pxb_last_error(const pxb_context* ctx);
+/* The context's cudaStream_t, for callers that want to time or order work around it. */
+pxb_status pxb_context_stream(pxb_context* ctx, void** stream_out);
+pxb_status pxb_context_synchronize(pxb_context* ctx);
+/* Number of solver kernel launches issued on this context so far. */
+uint64_t pxb_context_launch_count(const pxb_context* ctx);
+
+/* Fills `out` with the reference's ClothParams defaults (physxcoopa/cloth/cloth.h:167-256). */
+void pxb_cloth_params_default(pxb_cloth_params* out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Cloth registry: mirrors PhysicsWorld::add_cloth / remove_cloth / get_cloth                   */
+/* (physxcoopa/world.h:552-596).                                                                */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Uploads a cloth. Refuses an empty cloth (n_particles == 0) like add_cloth does, and a cloth
+ * the device path does not implement (self_collision on) with PXB_ERR_UNSUPPORTED. The returned
+ * id is generational: it goes stale after pxb_cloth_remove. */
+pxb_status pxb_cloth_add(pxb_context* ctx, const pxb_cloth_desc* desc, uint64_t* id_out);
+pxb_status pxb_cloth_remove(pxb_context* ctx, uint64_t id);
+/* Replaces a live cloth's tunables (ClothComponent::cloth_mut()->params is edited live). */
+pxb_status pxb_cloth_set_params(pxb_context* ctx, uint64_t id, const pxb_cloth_params* params);
+/* Host edit of particle state between steps (all four fields of every particle). */
+pxb_status pxb_cloth_write_particles(pxb_context* ctx, uint64_t id, const pxb_particle* particles,
+                                     uint32_t n);
+/* Reads particle state back (positions, prev positions, velocities, inv_mass). */
+pxb_status pxb_cloth_read_particles(pxb_context* ctx, uint64_t id, pxb_particle* out, uint32_t n);
+/* Reads the constraint lambdas left by the last substep, in the reference's list order. */
+pxb_status pxb_cloth_read_lambdas(pxb_context* ctx, uint64_t id, float* stretch_out,
+                                  uint32_t n_stretch, float* bend_out, uint32_t n_bend);
+/* Sets this frame's anchor targets (3 floats per anchor, anchor-list order). The previous
+ * targets become prev_world_position, as the reference's per-step epilogue leaves them
+ * (cloth_solver.h:457). */
+pxb_status pxb_cloth_set_anchor_targets(pxb_context* ctx, uint64_t id, const float* world_xyz,
+                                        uint32_t n_anchors);
+/* Reads the anchors' current (prev, world) targets back, reference layout. */
+pxb_status pxb_cloth_read_anchors(pxb_context* ctx, uint64_t id, pxb_anchor* out, uint32_t n);
+/* Cloth::time after the last step. */
+pxb_status pxb_cloth_read_time(pxb_context* ctx, uint64_t id, float* time_out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Batched step: one solve_cloth per listed cloth, all in one device launch sequence.           */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct pxb_cloth_step_desc {
+    const uint64_t* cloths;       /* ids to advance */
+    uint32_t n_cloths;
+    const pxb_collider* colliders;          /* flat collider list */
+    const uint32_t* collider_offsets;       /* n_cloths + 1 offsets; NULL = no colliders */
+    float gravity[3];                       /* world gravity (PhysicsWorld::gravity_) */
+    const pxb_gravity_source* sources;      /* flat gravity-source list, may be NULL */
+    const uint32_t* source_offsets;         /* n_cloths + 1 offsets; NULL = no sources */
+    uint32_t substeps;    /* solve_cloth's `substeps` (a cloth's params.substeps wins) */
+    uint32_t iterations;  /* solve_cloth's `iterations` (a cloth's params.iterations wins) */
+    float h;              /* step length, seconds */
+} pxb_cloth_step_desc;
+
+/* Per-cloth results of a step: the world AABB (Cloth::bounds) and max particle speed that the
+ * caller's broadphase query and sleep gate read (world.h:1777-1779, 1837). */
+typedef struct pxb_cloth_frame_result {
+    float bounds_min[3];
+    float bounds_max[3];
+    float max_speed;
+    float time;
+} pxb_cloth_frame_result;
+
+/* Advances every listed cloth by one call of solve_cloth, with gravity evaluated per cloth at
+ * its mean particle position when it has gravity sources (PhysicsWorld::gravity_at(cloth_centre_),
+ * world.h:1833, 2048-2076). Enqueued on the context stream; returns before completion. */
+pxb_status pxb_cloths_step(pxb_context* ctx, const pxb_cloth_step_desc* step);
+/* Copies the last step's per-cloth results to host memory (synchronizes the stream). */
+pxb_status pxb_cloths_read_results(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
+                                   pxb_cloth_frame_result* out);
+/* Copies positions of the listed cloths (3 floats per particle, cloths in list order) into
+ * host memory `out` of `capacity` floats (synchronizes the stream). This is what a renderer or
+ * a determinism hash reads back each frame. */
+pxb_status pxb_cloths_read_positions(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
+                                     float* out, size_t capacity);
+
+/* Drop-in single-cloth solve on HOST memory, the exact contract of cloth::solve_cloth: the cloth
+ * described by `desc` is uploaded, advanced, and its particles / lambdas / anchors / time /
+ * bounds written back to the caller's arrays. `particles`, `stretch`, `bend`, `anchors` are
+ * updated in place through the non-const pointers; `time_inout` and `bounds_out` (6 floats) may
+ * be NULL. Uses a per-context cache so repeated calls on the same arrays do not re-upload the
+ * topology. */
+pxb_status pxb_solve_cloth_host(pxb_context* ctx, const pxb_cloth_desc* desc,
+                                pxb_particle* particles, pxb_constraint* stretch,
+                                pxb_constraint* bend, pxb_anchor* anchors,
+                                const pxb_collider* colliders, uint32_t n_colliders,
+                                const float gravity[3], uint32_t substeps, uint32_t iterations,
+                                float h, float* time_inout, float* bounds_out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Collision primitive: cloth::project_particle (physxcoopa/cloth/cloth_collision.h:386-420)    */
+/* evaluated on the device for a batch of points (the collision stage of both solvers).         */
+/* ------------------------------------------------------------------------------------------ */
+
+/* For each of n points: projects it out of `collider` with standoff `thickness`. Writes the
+ * corrected point, the normal and depth, and hit (1/0). Host arrays; synchronous. */
+pxb_status pxb_project_particles(pxb_context* ctx, const pxb_collider* collider, float thickness,
+                                 const float* points_xyz, const float* motion_start_xyz,
+                                 uint32_t n, float* points_out, float* normals_out,
+                                 float* depths_out, int32_t* hit_out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Grid builders (host, setup time): cloth::make_grid_cloth / pin_static / build_tethers        */
+/* (physxcoopa/cloth/cloth_builder.h:81-358). A built cloth lives in library host memory; view  */
+/* it as a pxb_cloth_desc, edit it through the view's arrays, upload it with pxb_cloth_add.      */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct pxb_host_cloth pxb_host_cloth;
+
+/* cloth::GridClothDesc (physxcoopa/cloth/cloth_builder.h:52-64) plus a seeded jitter: when
+ * jitter > 0 every particle is displaced by an independent uniform draw in [-jitter, jitter] per
+ * axis (splitmix64 stream from jitter_seed) BEFORE rest lengths are captured, so the jittered
+ * sheet starts unstrained. jitter = 0 reproduces make_grid_cloth exactly. */
+typedef struct pxb_grid_cloth_desc {
+    uint32_t columns;
+    uint32_t rows;
+    float width;
+    float height;
+    float center[3];
+    float orientation[4]; /* (x, y, z, w) */
+    float total_mass;
+    int32_t shear;
+    pxb_cloth_params params;
+    float jitter;
+    uint64_t jitter_seed;
+} pxb_grid_cloth_desc;
+
+pxb_status pxb_host_cloth_make_grid(const pxb_grid_cloth_desc* desc, pxb_host_cloth** out);
+pxb_status pxb_host_cloth_destroy(pxb_host_cloth* cloth);
+/* cloth::pin_static (cloth_builder.h:271-292). Writes the number newly pinned to pinned_out. */
+pxb_status pxb_host_cloth_pin_static(pxb_host_cloth* cloth, const float world_point[3],
+                                     float radius, uint32_t* pinned_out);
+/* cloth::build_tethers (cloth_builder.h:308-358): geodesic Dijkstra over the stretch graph. */
+pxb_status pxb_host_cloth_build_tethers(pxb_host_cloth* cloth);
+/* A view of the cloth's arrays; pointers stay valid until the next builder call on it. */
+pxb_status pxb_host_cloth_view(pxb_host_cloth* cloth, pxb_cloth_desc* view_out);
+/* Mutable pointers into the same arrays, for host edits before upload. */
+pxb_status pxb_host_cloth_mutable(pxb_host_cloth* cloth, pxb_particle** particles,
+                                  pxb_anchor** anchors, pxb_cloth_params** params);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* PHYSXCOOPA_B200_H */

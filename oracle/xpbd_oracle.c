@@ -1,0 +1,873 @@
+/*
+ * xpbd_oracle.c -- CPU restatement of physxcoopa's XPBD cloth substep (see xpbd_oracle.h).
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the GPU path, never part of the shipped library.
+ * Build: oracle/Makefile (gcc -O2 -ffp-contract=off). All arithmetic is IEEE single precision
+ * in the order the reference writes it; glm's vector helpers are spelled out with the GLSL
+ * definitions (dot left to right, length = sqrt(dot), mix = x*(1-a) + y*a).
+ */
+#include "xpbd_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* util::k_epsilon (physxcoopa/util/math.h:19). */
+#define K_EPSILON 1e-6f
+/* util::k_max_cloth_substeps (physxcoopa/util/math.h:37). */
+#define K_MAX_CLOTH_SUBSTEPS 16u
+
+typedef struct { float x, y, z; } v3;
+typedef struct { float x, y, z, w; } q4;
+
+static inline v3 mk(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static inline v3 ld(const float* p) { return mk(p[0], p[1], p[2]); }
+static inline void st(float* p, v3 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; }
+static inline q4 ldq(const float* p) { q4 q = {p[0], p[1], p[2], p[3]}; return q; }
+static inline v3 add(v3 a, v3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub(v3 a, v3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 mul(v3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+static inline v3 smul(float s, v3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+static inline v3 divs(v3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+static inline v3 neg(v3 a) { return mk(-a.x, -a.y, -a.z); }
+static inline float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline float len(v3 a) { return sqrtf(dot(a, a)); }
+static inline v3 cross(v3 a, v3 b) {
+    return mk(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+static inline float fminr(float a, float b) { return b < a ? b : a; } /* glm::min / std::min */
+static inline float fmaxr(float a, float b) { return a < b ? b : a; } /* glm::max / std::max */
+static inline v3 mixv(v3 x, v3 y, float a) { return add(mul(x, 1.0f - a), mul(y, a)); }
+static inline float clampf(float x, float lo, float hi) { /* std::clamp */
+    return x < lo ? lo : (hi < x ? hi : x);
+}
+
+/* Unit-quaternion rotation v + 2*(w*(u x v) + u x (u x v)), u = (x,y,z). */
+static inline v3 qrot(q4 q, v3 v) {
+    const v3 u = mk(q.x, q.y, q.z);
+    const v3 uv = cross(u, v);
+    const v3 uuv = cross(u, uv);
+    return add(v, mul(add(mul(uv, q.w), uuv), 2.0f));
+}
+/* Hamilton product p*q. */
+static inline q4 qmul(q4 p, q4 q) {
+    q4 r;
+    r.w = p.w * q.w - p.x * q.x - p.y * q.y - p.z * q.z;
+    r.x = p.w * q.x + p.x * q.w + p.y * q.z - p.z * q.y;
+    r.y = p.w * q.y + p.y * q.w + p.z * q.x - p.x * q.z;
+    r.z = p.w * q.z + p.z * q.w + p.x * q.y - p.y * q.x;
+    return r;
+}
+/* Columns of the rotation matrix of unit q (glm::mat3_cast), i.e. the rotated basis. */
+static inline void qaxes(q4 q, v3* ax, v3* ay, v3* az) {
+    const float xx = q.x * q.x, yy = q.y * q.y, zz = q.z * q.z;
+    const float xz = q.x * q.z, xy = q.x * q.y, yz = q.y * q.z;
+    const float wx = q.w * q.x, wy = q.w * q.y, wz = q.w * q.z;
+    *ax = mk(1.0f - 2.0f * (yy + zz), 2.0f * (xy + wz), 2.0f * (xz - wy));
+    *ay = mk(2.0f * (xy - wz), 1.0f - 2.0f * (xx + zz), 2.0f * (yz + wx));
+    *az = mk(2.0f * (xz + wy), 2.0f * (yz - wx), 1.0f - 2.0f * (xx + yy));
+}
+static inline float comp(v3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+static inline void setcomp(v3* v, int i, float s) {
+    if (i == 0) v->x = s; else if (i == 1) v->y = s; else v->z = s;
+}
+
+/* util::safe_normalize (math.h:46-50). */
+static v3 safe_normalize(v3 v) {
+    const float l2 = dot(v, v);
+    if (l2 < K_EPSILON * K_EPSILON) return mk(0.0f, 0.0f, 0.0f);
+    return mul(v, 1.0f / sqrtf(l2));
+}
+/* util::orthonormal_basis (math.h:62-68), first tangent only. */
+static v3 orthonormal_t1(v3 n) {
+    const float sign = n.z >= 0.0f ? 1.0f : -1.0f;
+    const float a = -1.0f / (sign + n.z);
+    const float b = n.x * n.y * a;
+    return mk(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x);
+}
+/* geometry::closest_point_on_segment (capsule.h:39-49). */
+static v3 closest_point_on_segment(v3 point, v3 a, v3 b) {
+    const v3 ab = sub(b, a);
+    const float len2 = dot(ab, ab);
+    if (len2 < K_EPSILON) return a;
+    float t = dot(sub(point, a), ab) / len2;
+    t = clampf(t, 0.0f, 1.0f);
+    return add(a, mul(ab, t));
+}
+
+/* cloth::detail::project_at_pose_ (cloth_collision.h:109-203), Sphere / Capsule / Box. */
+static int project_at_pose(const pxb_collider* s, v3 pose_pos, q4 pose_rot, v3 sweep,
+                           float thickness, v3* p, v3* normal_out, float* depth_out) {
+    const int swept = dot(sweep, sweep) > K_EPSILON * K_EPSILON;
+    const v3 local_center = ld(s->local_center);
+    switch (s->type) {
+        case PXB_SHAPE_SPHERE: {
+            /* collision::world_sphere (shape.h:160-165) */
+            const v3 center = add(pose_pos, qrot(pose_rot, local_center));
+            const v3 axis_a = center;
+            const v3 axis_b = add(center, sweep);
+            const v3 on_axis = swept ? closest_point_on_segment(*p, axis_a, axis_b) : axis_a;
+            const v3 d = sub(*p, on_axis);
+            const float l = len(d);
+            const float target = s->radius + thickness;
+            if (l >= target) return 0;
+            const v3 n = (l > K_EPSILON) ? divs(d, l) : mk(0.0f, 0.0f, 1.0f);
+            *depth_out = target - l;
+            *p = add(on_axis, mul(n, target));
+            *normal_out = n;
+            return 1;
+        }
+        case PXB_SHAPE_CAPSULE: {
+            /* collision::world_capsule (shape.h:177-188) */
+            v3 axis_local = mk(0.0f, 0.0f, 0.0f);
+            setcomp(&axis_local, s->capsule_axis, 1.0f);
+            const v3 axis_world = qrot(qmul(pose_rot, ldq(s->local_rotation)), axis_local);
+            const v3 center = add(pose_pos, qrot(pose_rot, local_center));
+            const v3 ca = sub(center, mul(axis_world, s->capsule_half_height));
+            const v3 cb = add(center, mul(axis_world, s->capsule_half_height));
+            const v3 on_axis = closest_point_on_segment(*p, ca, cb);
+            const v3 d = sub(*p, on_axis);
+            const float l = len(d);
+            const float target = s->capsule_radius + thickness;
+            if (l >= target) return 0;
+            v3 n = d;
+            if (l > K_EPSILON) {
+                n = divs(d, l);
+            } else {
+                const v3 axis = safe_normalize(sub(cb, ca));
+                n = orthonormal_t1(axis);
+            }
+            *depth_out = target - l;
+            *p = add(on_axis, mul(n, target));
+            *normal_out = n;
+            return 1;
+        }
+        case PXB_SHAPE_BOX: {
+            /* collision::world_obb (shape.h:168-174), OBB::axes (obb.h:31-36) */
+            const v3 center = add(pose_pos, qrot(pose_rot, local_center));
+            const q4 orient = qmul(pose_rot, ldq(s->local_rotation));
+            v3 ax, ay, az;
+            qaxes(orient, &ax, &ay, &az);
+            const v3 d = sub(*p, center);
+            const v3 local = mk(dot(d, ax), dot(d, ay), dot(d, az));
+            const v3 he = ld(s->half_extents);
+            const int inside = fabsf(local.x) <= he.x && fabsf(local.y) <= he.y &&
+                               fabsf(local.z) <= he.z;
+            v3 local_target, local_normal;
+            if (inside) {
+                const v3 slack = mk(he.x - fabsf(local.x), he.y - fabsf(local.y),
+                                    he.z - fabsf(local.z));
+                const int axis = (slack.x <= slack.y && slack.x <= slack.z)
+                                     ? 0 : (slack.y <= slack.z ? 1 : 2);
+                const float sign = (comp(local, axis) >= 0.0f) ? 1.0f : -1.0f;
+                local_target = local;
+                setcomp(&local_target, axis, sign * (comp(he, axis) + thickness));
+                local_normal = mk(0.0f, 0.0f, 0.0f);
+                setcomp(&local_normal, axis, sign);
+                *depth_out = comp(slack, axis) + thickness;
+            } else {
+                /* glm::clamp(local, -he, he) = min(max(local, -he), he) */
+                local_target = mk(fminr(fmaxr(local.x, -he.x), he.x),
+                                  fminr(fmaxr(local.y, -he.y), he.y),
+                                  fminr(fmaxr(local.z, -he.z), he.z));
+                const v3 delta = sub(local, local_target);
+                const float l = len(delta);
+                if (l >= thickness) return 0;
+                local_normal = (l > K_EPSILON) ? divs(delta, l) : mk(0.0f, 0.0f, 1.0f);
+                *depth_out = thickness - l;
+                local_target = add(local_target, mul(local_normal, thickness));
+            }
+            *p = add(add(add(center, mul(ax, local_target.x)), mul(ay, local_target.y)),
+                     mul(az, local_target.z));
+            {
+                const v3 nw = add(add(mul(ax, local_normal.x), mul(ay, local_normal.y)),
+                                  mul(az, local_normal.z));
+                *normal_out = mul(nw, 1.0f / sqrtf(dot(nw, nw))); /* glm::normalize */
+            }
+            return 1;
+        }
+        default:
+            return -1;
+    }
+}
+
+/* cloth::project_particle (cloth_collision.h:386-420). */
+static int project_particle(const pxb_collider* col, float thickness, v3* p, v3* normal_out,
+                            float* depth_out) {
+    if (!col->enabled) return 0;
+    if (col->type != PXB_SHAPE_SPHERE && col->type != PXB_SHAPE_BOX &&
+        col->type != PXB_SHAPE_CAPSULE) {
+        return -1;
+    }
+    const v3 sweep = ld(col->sweep);
+    const int is_swept = dot(sweep, sweep) > K_EPSILON * K_EPSILON;
+    const int two_pose = is_swept && (col->type == PXB_SHAPE_BOX || col->type == PXB_SHAPE_CAPSULE);
+    const v3 pos = ld(col->position);
+    const q4 rot = ldq(col->orientation);
+    if (!two_pose) {
+        return project_at_pose(col, pos, rot, sweep, thickness, p, normal_out, depth_out);
+    }
+    v3 p_start = *p, n_start = mk(0, 0, 0);
+    float d_start = 0.0f;
+    const v3 zero = mk(0.0f, 0.0f, 0.0f);
+    const int hit_start = project_at_pose(col, pos, rot, zero, thickness, &p_start, &n_start,
+                                          &d_start);
+    v3 p_end = *p, n_end = mk(0, 0, 0);
+    float d_end = 0.0f;
+    const int hit_end = project_at_pose(col, add(pos, sweep), ldq(col->end_orientation), zero,
+                                        thickness, &p_end, &n_end, &d_end);
+    if (!hit_start && !hit_end) return 0;
+    if (hit_end && (!hit_start || d_end > d_start)) {
+        *p = p_end; *normal_out = n_end; *depth_out = d_end;
+    } else {
+        *p = p_start; *normal_out = n_start; *depth_out = d_start;
+    }
+    return 1;
+}
+
+int orc_project_particle(const pxb_collider* collider, float thickness, float p[3],
+                         float normal_out[3], float* depth_out, const float* motion_start) {
+    (void)motion_start; /* consumed only by the TriangleMesh branch, which is not restated */
+    v3 pp = ld(p), n = mk(0, 0, 0);
+    float d = 0.0f;
+    const int r = project_particle(collider, thickness, &pp, &n, &d);
+    if (r == 1) {
+        st(p, pp);
+        st(normal_out, n);
+        *depth_out = d;
+    }
+    return r;
+}
+
+/* cloth::detail::project_distance (cloth_solver.h:119-138). */
+static inline void project_distance(pxb_particle* particles, pxb_constraint* k, float alpha) {
+    pxb_particle* pa = &particles[k->a];
+    pxb_particle* pb = &particles[k->b];
+    const float w = pa->inv_mass + pb->inv_mass;
+    if (w <= 0.0f) return;
+    const v3 d = sub(ld(pa->position), ld(pb->position));
+    const float l = len(d);
+    if (l < K_EPSILON) return;
+    const v3 n = divs(d, l);
+    const float c = l - k->rest_length;
+    const float dlambda = (-c - alpha * k->lambda) / (w + alpha);
+    k->lambda += dlambda;
+    const v3 correction = smul(dlambda, n);
+    st(pa->position, add(ld(pa->position), smul(pa->inv_mass, correction)));
+    st(pb->position, sub(ld(pb->position), smul(pb->inv_mass, correction)));
+}
+
+/* cloth::detail::hash_cell / hash_bucket_count (cloth_solver.h:101-115). */
+static inline uint32_t hash_cell(int32_t x, int32_t y, int32_t z, uint32_t buckets) {
+    const uint32_t h = ((uint32_t)x * 73856093u) ^ ((uint32_t)y * 19349663u) ^
+                       ((uint32_t)z * 83492791u);
+    return h & (buckets - 1u);
+}
+static uint32_t hash_bucket_count(size_t n) {
+    uint32_t b = 16;
+    while (b < n * 2u && b < (1u << 22)) b <<= 1;
+    return b;
+}
+
+/* Stage 6, self-collision (cloth_solver.h:295-366). */
+static void self_collide(orc_cloth* c, uint32_t buckets, uint32_t* cell_of, uint32_t* counts,
+                         uint32_t* sorted) {
+    const uint32_t n = c->n_particles;
+    const float d_min = c->params.self_distance;
+    const float inv_cell = 1.0f / d_min;
+    memset(counts, 0, sizeof(uint32_t) * (buckets + 1));
+    for (uint32_t i = 0; i < n; ++i) {
+        const v3 p = ld(c->particles[i].position);
+        const uint32_t cell = hash_cell((int32_t)floorf(p.x * inv_cell),
+                                        (int32_t)floorf(p.y * inv_cell),
+                                        (int32_t)floorf(p.z * inv_cell), buckets);
+        cell_of[i] = cell;
+        ++counts[cell];
+    }
+    uint32_t running = 0;
+    for (uint32_t b = 0; b < buckets; ++b) {
+        const uint32_t cnt = counts[b];
+        counts[b] = running;
+        running += cnt;
+    }
+    counts[buckets] = running;
+    for (uint32_t i = 0; i < n; ++i) sorted[counts[cell_of[i]]++] = i;
+
+    for (uint32_t i = 0; i < n; ++i) {
+        pxb_particle* pi = &c->particles[i];
+        if (pi->inv_mass == 0.0f) continue;
+        const v3 base = mul(ld(pi->position), inv_cell);
+        const int32_t cx = (int32_t)floorf(base.x);
+        const int32_t cy = (int32_t)floorf(base.y);
+        const int32_t cz = (int32_t)floorf(base.z);
+        for (int32_t dz = -1; dz <= 1; ++dz)
+        for (int32_t dy = -1; dy <= 1; ++dy)
+        for (int32_t dx = -1; dx <= 1; ++dx) {
+            const uint32_t b = hash_cell(cx + dx, cy + dy, cz + dz, buckets);
+            const uint32_t first = (b == 0) ? 0u : counts[b - 1];
+            const uint32_t last = counts[b];
+            for (uint32_t s = first; s < last; ++s) {
+                const uint32_t j = sorted[s];
+                if (j <= i) continue;
+                if (c->columns > 0) {
+                    const int32_t xi = (int32_t)(i % c->columns), yi = (int32_t)(i / c->columns);
+                    const int32_t xj = (int32_t)(j % c->columns), yj = (int32_t)(j / c->columns);
+                    if (abs(xi - xj) <= 1 && abs(yi - yj) <= 1) continue;
+                }
+                pxb_particle* pj = &c->particles[j];
+                const float w = pi->inv_mass + pj->inv_mass;
+                if (w <= 0.0f) continue;
+                const v3 d = sub(ld(pi->position), ld(pj->position));
+                const float len2 = dot(d, d);
+                if (len2 >= d_min * d_min || len2 < K_EPSILON) continue;
+                const float l = sqrtf(len2);
+                const v3 push = mul(divs(d, l), (d_min - l) / w);
+                st(pi->position, add(ld(pi->position), mul(push, pi->inv_mass)));
+                st(pj->position, sub(ld(pj->position), mul(push, pj->inv_mass)));
+            }
+        }
+    }
+}
+
+/* geometry::AABB over the particles, cloth::compute_bounds (cloth.h:319-326). */
+static void compute_bounds(const pxb_particle* particles, uint32_t n, float mn[3], float mx[3]) {
+    v3 lo = mk(3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f);
+    v3 hi = mk(-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f);
+    for (uint32_t i = 0; i < n; ++i) {
+        const v3 p = ld(particles[i].position);
+        lo = mk(fminr(lo.x, p.x), fminr(lo.y, p.y), fminr(lo.z, p.z));
+        hi = mk(fmaxr(hi.x, p.x), fmaxr(hi.y, p.y), fmaxr(hi.z, p.z));
+    }
+    st(mn, lo);
+    st(mx, hi);
+}
+
+int orc_solve_cloth(orc_cloth* c, const pxb_collider* colliders, uint32_t n_colliders,
+                    const float gravity_in[3], uint32_t substeps, uint32_t iterations, float h) {
+    /* cloth_solver.h:162-194: prologue */
+    const uint32_t n = c->n_particles;
+    if (n == 0 || h <= 0.0f) return 0;
+    for (uint32_t k = 0; k < n_colliders; ++k) {
+        if (colliders[k].enabled && colliders[k].type != PXB_SHAPE_SPHERE &&
+            colliders[k].type != PXB_SHAPE_BOX && colliders[k].type != PXB_SHAPE_CAPSULE) {
+            return -1;
+        }
+    }
+    const pxb_cloth_params* P = &c->params;
+    uint32_t steps = P->substeps ? P->substeps : substeps;
+    if (steps < 1) steps = 1;
+    uint32_t iters = P->iterations ? P->iterations : iterations;
+    if (iters < 1) iters = 1;
+    const float hs = h / (float)steps;
+    const float inv_hs = 1.0f / hs;
+
+    const int self_collision = P->self_collision && P->self_distance > K_EPSILON;
+    const uint32_t buckets = self_collision ? hash_bucket_count(n) : 16u;
+
+    v3* accel = (v3*)calloc(n, sizeof(v3));
+    v3* contact_normal = (v3*)calloc(n, sizeof(v3));
+    float* contact_depth = (float*)calloc(n, sizeof(float));
+    uint32_t* cell_of = self_collision ? (uint32_t*)calloc(n, sizeof(uint32_t)) : NULL;
+    uint32_t* counts = self_collision ? (uint32_t*)calloc(buckets + 1, sizeof(uint32_t)) : NULL;
+    uint32_t* sorted = self_collision ? (uint32_t*)calloc(n, sizeof(uint32_t)) : NULL;
+
+    const float stretch_alpha = P->stretch_compliance / (hs * hs);
+    const float bend_alpha = P->bend_compliance / (hs * hs);
+
+    v3 wind = ld(P->wind);
+    if (P->wind_turbulence > 0.0f) {
+        const float t = c->time;
+        const v3 gust = mk(sinf(t * 1.7f) * cosf(t * 0.9f), sinf(t * 1.1f + 1.3f) * cosf(t * 1.9f),
+                           sinf(t * 0.7f + 2.7f) * cosf(t * 1.3f));
+        wind = add(wind, smul(P->wind_turbulence, gust));
+    }
+    const v3 gravity = ld(gravity_in);
+    const v3 base_accel = add(mul(gravity, P->gravity_scale), ld(P->external_acceleration));
+    const int aero = (P->air_drag > 0.0f || P->air_lift > 0.0f) && c->n_triangle_indices > 0;
+    const float max_velocity2 = P->max_velocity * P->max_velocity;
+
+    for (uint32_t step = 0; step < steps; ++step) {
+        /* 1. aerodynamics (cloth_solver.h:202-227) */
+        memset(accel, 0, sizeof(v3) * n);
+        if (aero) {
+            for (uint32_t t = 0; t + 2 < c->n_triangle_indices; t += 3) {
+                const uint32_t i0 = c->triangles[t], i1 = c->triangles[t + 1],
+                               i2 = c->triangles[t + 2];
+                const v3 p0 = ld(c->particles[i0].position);
+                const v3 e1 = sub(ld(c->particles[i1].position), p0);
+                const v3 e2 = sub(ld(c->particles[i2].position), p0);
+                const v3 cr = cross(e1, e2);
+                const float twice_area = len(cr);
+                if (twice_area < K_EPSILON) continue;
+                const v3 face_n = divs(cr, twice_area);
+                const v3 vsum = add(add(ld(c->particles[i0].velocity), ld(c->particles[i1].velocity)),
+                                    ld(c->particles[i2].velocity));
+                const v3 v = sub(mul(vsum, 1.0f / 3.0f), wind);
+                const float vn = dot(v, face_n);
+                const v3 vt = sub(v, smul(vn, face_n));
+                const float scale = -0.5f * twice_area * fabsf(vn);
+                const v3 inner = add(smul(P->air_drag * vn, face_n), smul(P->air_lift, vt));
+                const v3 force = smul(scale, inner);
+                const v3 share = mul(force, 1.0f / 3.0f);
+                accel[i0] = add(accel[i0], share);
+                accel[i1] = add(accel[i1], share);
+                accel[i2] = add(accel[i2], share);
+            }
+        }
+
+        /* 2. integrate (cloth_solver.h:230-240) */
+        const float damping_factor = 1.0f / (1.0f + P->damping * hs);
+        for (uint32_t i = 0; i < n; ++i) {
+            pxb_particle* p = &c->particles[i];
+            memcpy(p->prev_position, p->position, sizeof(float) * 3);
+            if (p->inv_mass == 0.0f) continue;
+            v3 v = ld(p->velocity);
+            v = add(v, mul(add(base_accel, mul(accel[i], p->inv_mass)), hs));
+            v = mul(v, damping_factor);
+            st(p->velocity, v);
+            st(p->position, add(ld(p->position), mul(v, hs)));
+        }
+
+        /* 3. anchors (cloth_solver.h:245-250) */
+        const float alpha_t = (float)(step + 1) / (float)steps;
+        for (uint32_t a = 0; a < c->n_anchors; ++a) {
+            const pxb_anchor* an = &c->anchors[a];
+            if (an->particle >= n) continue;
+            st(c->particles[an->particle].position,
+               mixv(ld(an->prev_world_position), ld(an->world_position), alpha_t));
+        }
+
+        /* 4. constraints (cloth_solver.h:253-271) */
+        for (uint32_t k = 0; k < c->n_stretch; ++k) c->stretch[k].lambda = 0.0f;
+        for (uint32_t k = 0; k < c->n_bend; ++k) c->bend[k].lambda = 0.0f;
+        for (uint32_t it = 0; it < iters; ++it) {
+            for (uint32_t b = 0; b < c->n_stretch_batches; ++b) {
+                const pxb_batch bt = c->stretch_batches[b];
+                const float alpha = c->stretch_batch_compliance
+                                        ? c->stretch_batch_compliance[b] / (hs * hs)
+                                        : stretch_alpha;
+                for (uint32_t i = bt.begin; i < bt.end; ++i)
+                    project_distance(c->particles, &c->stretch[i], alpha);
+            }
+            for (uint32_t b = 0; b < c->n_bend_batches; ++b) {
+                const pxb_batch bt = c->bend_batches[b];
+                const float alpha = c->bend_batch_compliance
+                                        ? c->bend_batch_compliance[b] / (hs * hs)
+                                        : bend_alpha;
+                for (uint32_t i = bt.begin; i < bt.end; ++i)
+                    project_distance(c->particles, &c->bend[i], alpha);
+            }
+        }
+
+        /* 5. tethers (cloth_solver.h:276-289) */
+        for (uint32_t k = 0; k < c->n_tethers; ++k) {
+            const pxb_tether* t = &c->tethers[k];
+            pxb_particle* p = &c->particles[t->particle];
+            if (p->inv_mass == 0.0f) continue;
+            const v3 anchor = ld(c->particles[t->anchor].position);
+            const v3 d = sub(ld(p->position), anchor);
+            const float l = len(d);
+            if (l <= t->max_length || l < K_EPSILON) continue;
+            st(p->position, add(anchor, mul(d, t->max_length / l)));
+        }
+
+        /* 6. self-collision (cloth_solver.h:295-366) */
+        if (self_collision) self_collide(c, buckets, cell_of, counts, sorted);
+
+        /* 7. collisions (cloth_solver.h:376-411) */
+        memset(contact_normal, 0, sizeof(v3) * n);
+        memset(contact_depth, 0, sizeof(float) * n);
+        if (n_colliders > 0) {
+            const float m = P->thickness;
+            for (uint32_t i = 0; i < n; ++i) {
+                pxb_particle* p = &c->particles[i];
+                if (p->inv_mass == 0.0f) continue;
+                for (uint32_t k = 0; k < n_colliders; ++k) {
+                    const pxb_collider* col = &colliders[k];
+                    const float* lo = col->bounds_min;
+                    const float* hi = col->bounds_max;
+                    const float* x = p->position;
+                    if (x[0] < lo[0] - m || x[0] > hi[0] + m || x[1] < lo[1] - m ||
+                        x[1] > hi[1] + m || x[2] < lo[2] - m || x[2] > hi[2] + m) {
+                        continue;
+                    }
+                    v3 pp = ld(p->position), normal = mk(0, 0, 0);
+                    float depth = 0.0f;
+                    if (project_particle(col, P->thickness, &pp, &normal, &depth) != 1) continue;
+                    st(p->position, pp);
+                    contact_normal[i] = add(contact_normal[i], normal);
+                    contact_depth[i] += depth;
+                }
+            }
+        }
+
+        /* 8. finalize velocities + friction (cloth_solver.h:414-451) */
+        for (uint32_t i = 0; i < n; ++i) {
+            pxb_particle* p = &c->particles[i];
+            v3 v = mul(sub(ld(p->position), ld(p->prev_position)), inv_hs);
+            const float depth = contact_depth[i];
+            if (depth > 0.0f) {
+                const v3 nsum = contact_normal[i];
+                const float nlen = len(nsum);
+                if (nlen > K_EPSILON) {
+                    const v3 nrm = divs(nsum, nlen);
+                    const float vn = dot(v, nrm);
+                    const v3 vt = sub(v, smul(vn, nrm));
+                    if (vn < 0.0f) v = sub(v, smul(vn, nrm));
+                    const float budget = P->friction * depth * inv_hs;
+                    const float vt_len = len(vt);
+                    if (vt_len > K_EPSILON) v = sub(v, mul(vt, fminr(1.0f, budget / vt_len)));
+                }
+            }
+            const float v2 = dot(v, v);
+            if (v2 > max_velocity2) v = mul(v, P->max_velocity / sqrtf(v2));
+            st(p->velocity, v);
+        }
+
+        c->time += hs;
+    }
+
+    /* epilogue (cloth_solver.h:457-459) */
+    for (uint32_t a = 0; a < c->n_anchors; ++a)
+        memcpy(c->anchors[a].prev_world_position, c->anchors[a].world_position, sizeof(float) * 3);
+    compute_bounds(c->particles, n, c->bounds_min, c->bounds_max);
+
+    free(accel);
+    free(contact_normal);
+    free(contact_depth);
+    free(cell_of);
+    free(counts);
+    free(sorted);
+    return 0;
+}
+
+void orc_gravity_at(const float gravity[3], const pxb_gravity_source* sources,
+                    uint32_t n_sources, const float p_in[3], float out[3]) {
+    /* world.h:1186-1190 -> field_at_ world.h:2048-2068 */
+    if (n_sources == 0) {
+        memcpy(out, gravity, sizeof(float) * 3);
+        return;
+    }
+    const v3 p = ld(p_in);
+    float best = 0.0f;
+    v3 pull = ld(gravity);
+    int found = 0;
+    for (uint32_t k = 0; k < n_sources; ++k) {
+        const pxb_gravity_source* g = &sources[k];
+        const v3 d = sub(ld(g->centre), p);
+        const float r = len(d);
+        if (g->range > 0.0f && r > g->range) continue;
+        if (r < 1e-6f) continue;
+        const float a = r <= g->radius ? g->strength
+                                       : g->strength * (g->radius / r) * (g->radius / r);
+        if (!found || a > best) {
+            best = a;
+            pull = mul(divs(d, r), a);
+            found = 1;
+        }
+    }
+    st(out, found ? pull : ld(gravity));
+}
+
+void orc_cloth_centre(const pxb_particle* particles, uint32_t n, float out[3]) {
+    v3 sum = mk(0.0f, 0.0f, 0.0f);
+    for (uint32_t i = 0; i < n; ++i) sum = add(sum, ld(particles[i].position));
+    st(out, n == 0 ? sum : divs(sum, (float)n));
+}
+
+int orc_step_cloth(orc_cloth* c, const pxb_collider* colliders, uint32_t n_colliders,
+                   const float gravity[3], const pxb_gravity_source* sources,
+                   uint32_t n_sources, uint32_t substeps, uint32_t iterations, float h) {
+    float g[3];
+    if (n_sources == 0) {
+        memcpy(g, gravity, sizeof(g));
+    } else {
+        float centre[3];
+        orc_cloth_centre(c->particles, c->n_particles, centre);
+        orc_gravity_at(gravity, sources, n_sources, centre, g);
+    }
+    return orc_solve_cloth(c, colliders, n_colliders, g, substeps, iterations, h);
+}
+
+float orc_max_particle_speed(const pxb_particle* particles, uint32_t n) {
+    float max2 = 0.0f;
+    for (uint32_t i = 0; i < n; ++i) max2 = fmaxr(max2, dot(ld(particles[i].velocity), ld(particles[i].velocity)));
+    return sqrtf(max2);
+}
+
+uint32_t orc_frame_substeps(float dt, float fixed_dt, uint32_t cloth_substeps) {
+    /* world.h:1753-1757 */
+    float internal_h = fixed_dt / (float)(cloth_substeps > 1u ? cloth_substeps : 1u);
+    if (internal_h < K_EPSILON) internal_h = K_EPSILON;
+    long r = lroundf(dt / internal_h);
+    uint32_t s = (uint32_t)r;
+    if (s < 1u) s = 1u;
+    if (s > K_MAX_CLOTH_SUBSTEPS) s = K_MAX_CLOTH_SUBSTEPS;
+    return s;
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* Hair                                                                                      */
+/* ---------------------------------------------------------------------------------------- */
+
+/* hair::k_reference_step (strand_solver.h:63). */
+#define K_REFERENCE_STEP (1.0f / 60.0f)
+
+static inline q4 mkq(float w, float x, float y, float z) { q4 q = {x, y, z, w}; return q; }
+static inline q4 qscale(q4 q, float s) { return mkq(q.w * s, q.x * s, q.y * s, q.z * s); }
+static inline q4 qadd(q4 a, q4 b) { return mkq(a.w + b.w, a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline float qdot(q4 a, q4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+static inline float mixf(float x, float y, float a) { return x * (1.0f - a) + y * a; }
+
+/* Quaternion for a rotation of `angle` about unit `axis` (glm::angleAxis). */
+static q4 angle_axis(float angle, v3 axis) {
+    const float s = sinf(angle * 0.5f);
+    return mkq(cosf(angle * 0.5f), axis.x * s, axis.y * s, axis.z * s);
+}
+/* Shortest-arc spherical interpolation with a component-wise lerp when the two rotations are
+ * within FLT_EPSILON (glm::slerp, used at strand_solver.h:219-220). */
+static q4 slerp(q4 a, q4 b, float t) {
+    float cos_theta = qdot(a, b);
+    if (cos_theta < 0.0f) {
+        b = mkq(-b.w, -b.x, -b.y, -b.z);
+        cos_theta = -cos_theta;
+    }
+    if (cos_theta > 1.0f - 1.19209290e-07f) {
+        return mkq(mixf(a.w, b.w, t), mixf(a.x, b.x, t), mixf(a.y, b.y, t), mixf(a.z, b.z, t));
+    }
+    const float theta = acosf(cos_theta);
+    const q4 r = qadd(qscale(a, sinf((1.0f - t) * theta)), qscale(b, sinf(t * theta)));
+    const float sn = sinf(theta);
+    return mkq(r.w / sn, r.x / sn, r.y / sn, r.z / sn);
+}
+
+/* hair::detail::rotation_between (strand_solver.h:91-105). */
+static q4 rotation_between(v3 from, v3 to) {
+    const float d = fminr(fmaxr(dot(from, to), -1.0f), 1.0f);
+    if (d > 0.999999f) return mkq(1.0f, 0.0f, 0.0f, 0.0f);
+    if (d < -0.999999f) {
+        v3 axis = cross(mk(0.0f, 0.0f, 1.0f), from);
+        if (dot(axis, axis) < 1e-8f) axis = cross(mk(1.0f, 0.0f, 0.0f), from);
+        const v3 nrm = mul(axis, 1.0f / sqrtf(dot(axis, axis)));
+        return angle_axis(3.14159265358979323846f, nrm);
+    }
+    const v3 axis = cross(from, to);
+    const float l = len(axis);
+    if (l < 1e-8f) return mkq(1.0f, 0.0f, 0.0f, 0.0f);
+    return angle_axis(acosf(d), divs(axis, l));
+}
+
+int orc_solve_strands(orc_strand_set* s, const pxb_collider* colliders, uint32_t n_colliders,
+                      const float gravity_in[3], uint32_t substeps, uint32_t iterations, float h) {
+    /* strand_solver.h:124-155: prologue */
+    const uint32_t n = s->n_particles;
+    if (n == 0 || s->n_strands == 0 || h <= 0.0f) return 0;
+    for (uint32_t k = 0; k < n_colliders; ++k) {
+        if (colliders[k].enabled && colliders[k].type != PXB_SHAPE_SPHERE &&
+            colliders[k].type != PXB_SHAPE_BOX && colliders[k].type != PXB_SHAPE_CAPSULE) {
+            return -1;
+        }
+    }
+    const pxb_strand_params* P = &s->params;
+    uint32_t steps = P->substeps ? P->substeps : substeps;
+    if (steps < 1) steps = 1;
+    uint32_t iters = P->iterations ? P->iterations : iterations;
+    if (iters < 1) iters = 1;
+    const float hs = h / (float)steps;
+    const float inv_hs = 1.0f / hs;
+
+    v3* contact_normal = (v3*)calloc(n, sizeof(v3));
+    float* contact_depth = (float*)calloc(n, sizeof(float));
+    uint8_t* contacted = (uint8_t*)calloc(n, 1);
+
+    const float alpha = P->stretch_compliance * inv_hs * inv_hs;
+    const v3 accel = add(mul(ld(gravity_in), P->gravity_scale), ld(P->external_acceleration));
+    const float max_speed2 = P->max_velocity * P->max_velocity;
+    const float substep_fraction = hs / K_REFERENCE_STEP;
+    const float global_per_substep =
+        1.0f - powf(1.0f - clampf(P->global_shape, 0.0f, 1.0f) , substep_fraction);
+    const float local_per_substep =
+        1.0f - powf(1.0f - clampf(P->local_shape, 0.0f, 1.0f), substep_fraction);
+
+    for (uint32_t sub_i = 0; sub_i < steps; ++sub_i) {
+        const float t = (float)(sub_i + 1) / (float)steps;
+
+        /* 1 + 2: aerodynamics and integration (strand_solver.h:162-189) */
+        for (uint32_t i = 0; i < n; ++i) {
+            pxb_particle* p = &s->particles[i];
+            if (p->inv_mass <= 0.0f) continue;
+            v3 a = accel;
+            v3 vel = ld(p->velocity);
+            if (P->air_drag > 0.0f) {
+                v3 wind = ld(P->wind);
+                if (P->wind_turbulence > 0.0f) {
+                    const float phase = s->time * 2.3f + p->position[0] * 1.7f +
+                                        p->position[1] * 2.1f + p->position[2] * 1.3f;
+                    const float amp = P->wind_turbulence * len(ld(P->wind));
+                    wind = add(wind, smul(amp, mk(sinf(phase), sinf(phase * 1.37f + 2.1f),
+                                                  sinf(phase * 0.81f + 4.2f))));
+                }
+                a = add(a, mul(sub(wind, vel), P->air_drag));
+            }
+            vel = add(vel, mul(a, hs));
+            vel = mul(vel, 1.0f / (1.0f + P->damping * hs));
+            const float v2 = dot(vel, vel);
+            if (v2 > max_speed2) vel = mul(vel, P->max_velocity / sqrtf(v2));
+            st(p->velocity, vel);
+            memcpy(p->prev_position, p->position, sizeof(float) * 3);
+            st(p->position, add(ld(p->position), mul(vel, hs)));
+        }
+
+        /* 3: roots (strand_solver.h:194-201) */
+        for (uint32_t k = 0; k < s->n_strands; ++k) {
+            const pxb_strand* sd = &s->strands[k];
+            if (sd->count == 0) continue;
+            const v3 root = mixv(ld(sd->prev_root_position), ld(sd->root_position), t);
+            pxb_particle* p = &s->particles[sd->first];
+            memcpy(p->prev_position, p->position, sizeof(float) * 3);
+            st(p->position, root);
+            st(p->velocity, mk(0.0f, 0.0f, 0.0f));
+        }
+
+        /* 4: stretch (strand_solver.h:204-211) */
+        for (uint32_t k = 0; k < s->n_stretch; ++k) s->stretch[k].lambda = 0.0f;
+        for (uint32_t it = 0; it < iters; ++it) {
+            for (uint32_t b = 0; b < s->n_stretch_batches; ++b) {
+                const pxb_batch bt = s->stretch_batches[b];
+                for (uint32_t ci = bt.begin; ci < bt.end; ++ci)
+                    project_distance(s->particles, &s->stretch[ci], alpha);
+            }
+        }
+
+        /* 5: global shape (strand_solver.h:216-235) */
+        if (P->global_shape > 0.0f) {
+            for (uint32_t k = 0; k < s->n_strands; ++k) {
+                const pxb_strand* sd = &s->strands[k];
+                if (sd->count < 2) continue;
+                const q4 orientation = slerp(ldq(sd->prev_root_orientation),
+                                             ldq(sd->root_orientation), t);
+                const v3 root = mixv(ld(sd->prev_root_position), ld(sd->root_position), t);
+                const float inv_last = 1.0f / (float)(sd->count - 1);
+                for (uint32_t j = 1; j < sd->count; ++j) {
+                    const uint32_t i = sd->first + j;
+                    pxb_particle* p = &s->particles[i];
+                    if (p->inv_mass <= 0.0f) continue;
+                    const float along = (float)j * inv_last;
+                    const float weight = global_per_substep *
+                                         powf(1.0f - along, P->global_shape_falloff);
+                    if (weight <= 0.0f) continue;
+                    const v3 target = add(root, qrot(orientation, ld(&s->rest_local[3 * i])));
+                    st(p->position, mixv(ld(p->position), target, fminr(weight, 1.0f)));
+                }
+            }
+        }
+
+        /* 6: local shape (strand_solver.h:241-272) */
+        if (P->local_shape > 0.0f) {
+            const float k_local = local_per_substep;
+            for (uint32_t k = 0; k < s->n_strands; ++k) {
+                const pxb_strand* sd = &s->strands[k];
+                if (sd->count < 3) continue;
+                for (uint32_t j = 1; j + 1 < sd->count; ++j) {
+                    const uint32_t prv = sd->first + j - 1;
+                    const uint32_t cur = sd->first + j;
+                    const uint32_t nxt = sd->first + j + 1;
+                    const v3 rest_prev = ld(&s->rest_offset[3 * cur]);
+                    const v3 live_prev = sub(ld(s->particles[cur].position),
+                                             ld(s->particles[prv].position));
+                    const float rest_len = len(rest_prev);
+                    const float live_len = len(live_prev);
+                    if (rest_len <= 1e-8f || live_len <= 1e-8f) continue;
+                    const q4 turn = rotation_between(divs(rest_prev, rest_len),
+                                                     divs(live_prev, live_len));
+                    const v3 target = add(ld(s->particles[cur].position),
+                                          qrot(turn, ld(&s->rest_offset[3 * nxt])));
+                    const v3 delta = mul(sub(target, ld(s->particles[nxt].position)), k_local);
+                    pxb_particle* pa = &s->particles[cur];
+                    pxb_particle* pb = &s->particles[nxt];
+                    const float w = pa->inv_mass + pb->inv_mass;
+                    if (w <= 0.0f) continue;
+                    st(pb->position, add(ld(pb->position), mul(delta, pb->inv_mass / w)));
+                    st(pa->position, sub(ld(pa->position), mul(delta, pa->inv_mass / w)));
+                }
+            }
+        }
+
+        /* 7: collisions, deepest contact kept (strand_solver.h:275-298) */
+        memset(contacted, 0, n);
+        if (n_colliders > 0) {
+            for (uint32_t i = 0; i < n; ++i) {
+                pxb_particle* p = &s->particles[i];
+                if (p->inv_mass <= 0.0f) continue;
+                for (uint32_t k = 0; k < n_colliders; ++k) {
+                    v3 pp = ld(p->position), normal = mk(0, 0, 0);
+                    float depth = 0.0f;
+                    if (project_particle(&colliders[k], P->thickness, &pp, &normal, &depth) != 1)
+                        continue;
+                    st(p->position, pp);
+                    if (contacted[i] == 0 || depth > contact_depth[i]) {
+                        contact_normal[i] = normal;
+                        contact_depth[i] = depth;
+                    }
+                    contacted[i] = 1;
+                }
+            }
+        }
+
+        /* 8: finalize + positional friction (strand_solver.h:301-321) */
+        for (uint32_t i = 0; i < n; ++i) {
+            pxb_particle* p = &s->particles[i];
+            if (p->inv_mass <= 0.0f) continue;
+            const v3 prev = ld(p->prev_position);
+            st(p->velocity, mul(sub(ld(p->position), prev), inv_hs));
+            if (contacted[i] != 0 && P->friction > 0.0f) {
+                const v3 normal = contact_normal[i];
+                const v3 motion = sub(ld(p->position), prev);
+                const v3 tangential = sub(motion, mul(normal, dot(motion, normal)));
+                const float t_len = len(tangential);
+                if (t_len > K_EPSILON) {
+                    const float limit = P->friction * contact_depth[i];
+                    const float scale = fmaxr(0.0f, 1.0f - fminr(limit, t_len) / t_len);
+                    st(p->position, sub(ld(p->position), mul(tangential, 1.0f - scale)));
+                    st(p->velocity, mul(sub(ld(p->position), prev), inv_hs));
+                }
+            }
+        }
+
+        s->time += hs;
+    }
+
+    compute_bounds(s->particles, n, s->bounds_min, s->bounds_max);
+    free(contact_normal);
+    free(contact_depth);
+    free(contacted);
+    return 0;
+}
+
+int orc_step_strands(orc_strand_set* s, const pxb_collider* colliders, uint32_t n_colliders,
+                     const float gravity[3], const pxb_gravity_source* sources,
+                     uint32_t n_sources, uint32_t substeps, uint32_t iterations, float h) {
+    float g[3];
+    if (n_sources == 0) {
+        memcpy(g, gravity, sizeof(g));
+    } else {
+        /* world.h:1941: centre = 0.5 * (bounds.min + bounds.max) */
+        const v3 centre = smul(0.5f, add(ld(s->bounds_min), ld(s->bounds_max)));
+        float c[3];
+        st(c, centre);
+        orc_gravity_at(gravity, sources, n_sources, c, g);
+    }
+    return orc_solve_strands(s, colliders, n_colliders, g, substeps, iterations, h);
+}
+
+void orc_set_strand_roots(orc_strand_set* s, const float* positions, uint32_t n_positions,
+                          const float* orientations, uint32_t n_orientations) {
+    const uint32_t n = s->n_strands < n_positions ? s->n_strands : n_positions;
+    for (uint32_t i = 0; i < n; ++i) {
+        pxb_strand* sd = &s->strands[i];
+        memcpy(sd->prev_root_position, sd->root_position, sizeof(float) * 3);
+        memcpy(sd->prev_root_orientation, sd->root_orientation, sizeof(float) * 4);
+        memcpy(sd->root_position, &positions[3 * i], sizeof(float) * 3);
+        if (i < n_orientations) memcpy(sd->root_orientation, &orientations[4 * i], sizeof(float) * 4);
+    }
+}

@@ -1,0 +1,118 @@
+/*
+ * xpbd_oracle.h -- CPU restatement of physxcoopa's XPBD cloth and hair substeps.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the checker the GPU path is compared against; nothing in
+ * the shipped library links, loads or calls it. Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg use it.
+ *
+ * Each function restates the reference algorithm stage by stage, in the reference's operation
+ * order, in plain C99 single-precision arithmetic (compiled with -ffp-contract=off so no fused
+ * multiply-add changes the rounding). Citations are to files of the physxcoopa tree.
+ * The restatement is pinned against the reference's own headers compiled into oracle/_ref
+ * (oracle/ref_driver.cpp) and against the known answers of the reference's tests.
+ */
+#ifndef PXB_XPBD_ORACLE_H
+#define PXB_XPBD_ORACLE_H
+
+#include <stdint.h>
+
+#include "../include/physxcoopa_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A cloth in reference layout, mutable (the oracle advances it in place). */
+typedef struct orc_cloth {
+    pxb_particle* particles;
+    uint32_t n_particles;
+    pxb_constraint* stretch;
+    uint32_t n_stretch;
+    const pxb_batch* stretch_batches;
+    uint32_t n_stretch_batches;
+    pxb_constraint* bend;
+    uint32_t n_bend;
+    const pxb_batch* bend_batches;
+    uint32_t n_bend_batches;
+    const pxb_tether* tethers;
+    uint32_t n_tethers;
+    pxb_anchor* anchors;
+    uint32_t n_anchors;
+    const uint32_t* triangles;
+    uint32_t n_triangle_indices;
+    uint32_t columns;
+    uint32_t rows;
+    pxb_cloth_params params;
+    float time;
+    const float* stretch_batch_compliance; /* optional */
+    const float* bend_batch_compliance;    /* optional */
+    float bounds_min[3];
+    float bounds_max[3];
+} orc_cloth;
+
+/* cloth::solve_cloth (cloth_solver.h:158-460), serial dispatch. Returns 0, or -1 when a
+ * collider is a mesh / hull (not restated here). */
+int orc_solve_cloth(orc_cloth* c, const pxb_collider* colliders, uint32_t n_colliders,
+                    const float gravity[3], uint32_t substeps, uint32_t iterations, float h);
+
+/* cloth::project_particle (cloth_collision.h:386-420). Returns 1 on hit, 0 on miss, -1 for an
+ * unsupported shape type. motion_start may be NULL. */
+int orc_project_particle(const pxb_collider* collider, float thickness, float p[3],
+                         float normal_out[3], float* depth_out, const float* motion_start);
+
+/* PhysicsWorld::gravity_at (world.h:1186-1190 over field_at_ world.h:2048-2068). */
+void orc_gravity_at(const float gravity[3], const pxb_gravity_source* sources,
+                    uint32_t n_sources, const float p[3], float out[3]);
+
+/* PhysicsWorld::cloth_centre_ (world.h:2072-2076): sequential mean particle position. */
+void orc_cloth_centre(const pxb_particle* particles, uint32_t n, float out[3]);
+
+/* The per-cloth body of PhysicsWorld::step_cloths_ that concerns the solver (world.h:1832-1834):
+ * gravity = sources ? gravity_at(cloth_centre_) : gravity, then solve_cloth. */
+int orc_step_cloth(orc_cloth* c, const pxb_collider* colliders, uint32_t n_colliders,
+                   const float gravity[3], const pxb_gravity_source* sources,
+                   uint32_t n_sources, uint32_t substeps, uint32_t iterations, float h);
+
+/* A strand set in reference layout, mutable. rest_local / rest_offset: 3 floats per particle. */
+typedef struct orc_strand_set {
+    pxb_particle* particles;
+    uint32_t n_particles;
+    pxb_constraint* stretch;
+    uint32_t n_stretch;
+    const pxb_batch* stretch_batches;
+    uint32_t n_stretch_batches;
+    const float* rest_local;
+    const float* rest_offset;
+    pxb_strand* strands;
+    uint32_t n_strands;
+    pxb_strand_params params;
+    float time;
+    float bounds_min[3];
+    float bounds_max[3];
+} orc_strand_set;
+
+/* hair::solve_strands (strand_solver.h:121-327). Returns 0, or -1 for a mesh / hull collider. */
+int orc_solve_strands(orc_strand_set* s, const pxb_collider* colliders, uint32_t n_colliders,
+                      const float gravity[3], uint32_t substeps, uint32_t iterations, float h);
+
+/* The per-set body of PhysicsWorld::step_strands_ that concerns the solver (world.h:1941-1945):
+ * gravity = sources ? gravity_at(bounds centre) : gravity, then solve_strands. */
+int orc_step_strands(orc_strand_set* s, const pxb_collider* colliders, uint32_t n_colliders,
+                     const float gravity[3], const pxb_gravity_source* sources,
+                     uint32_t n_sources, uint32_t substeps, uint32_t iterations, float h);
+
+/* hair::set_strand_roots (strand_builder.h:139-149); orientations may be NULL. */
+void orc_set_strand_roots(orc_strand_set* s, const float* positions, uint32_t n_positions,
+                          const float* orientations, uint32_t n_orientations);
+
+/* cloth::max_particle_speed (cloth.h:330-336). */
+float orc_max_particle_speed(const pxb_particle* particles, uint32_t n);
+
+/* The substep count PhysicsWorld::step_cloths_ derives from a frame dt (world.h:1753-1757). */
+uint32_t orc_frame_substeps(float dt, float fixed_dt, uint32_t cloth_substeps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PXB_XPBD_ORACLE_H */

@@ -1,0 +1,167 @@
+"""ctypes / numpy mirrors of the plain-old-data types in include/physxcoopa_b200.h.
+
+The numpy dtypes reproduce the reference's in-memory layouts (physxcoopa/cloth/cloth.h:83-160,
+physxcoopa/hair/strand.h:79-87) byte for byte, so arrays built here can be handed to the C-ABI
+(and to the reference's own code) without conversion.
+"""
+import ctypes as C
+
+import numpy as np
+
+f32 = C.c_float
+u32 = C.c_uint32
+i32 = C.c_int32
+
+PARTICLE = np.dtype([("position", "<f4", 3), ("prev_position", "<f4", 3),
+                     ("velocity", "<f4", 3), ("inv_mass", "<f4")])
+CONSTRAINT = np.dtype([("a", "<u4"), ("b", "<u4"), ("rest_length", "<f4"), ("lambda", "<f4")])
+BATCH = np.dtype([("begin", "<u4"), ("end", "<u4")])
+TETHER = np.dtype([("particle", "<u4"), ("anchor", "<u4"), ("max_length", "<f4")])
+ANCHOR = np.dtype([("particle", "<u4"), ("body_index", "<u4"), ("body_generation", "<u4"),
+                   ("local_position", "<f4", 3), ("world_position", "<f4", 3),
+                   ("prev_world_position", "<f4", 3)])
+STRAND = np.dtype([("first", "<u4"), ("count", "<u4"), ("root_position", "<f4", 3),
+                   ("root_orientation", "<f4", 4), ("prev_root_position", "<f4", 3),
+                   ("prev_root_orientation", "<f4", 4)])
+COLLIDER = np.dtype([("type", "<i4"), ("enabled", "<i4"), ("position", "<f4", 3),
+                     ("orientation", "<f4", 4), ("local_center", "<f4", 3),
+                     ("local_rotation", "<f4", 4), ("radius", "<f4"), ("half_extents", "<f4", 3),
+                     ("capsule_radius", "<f4"), ("capsule_half_height", "<f4"),
+                     ("capsule_axis", "<i4"), ("sweep", "<f4", 3), ("end_orientation", "<f4", 4),
+                     ("bounds_min", "<f4", 3), ("bounds_max", "<f4", 3)])
+GRAVITY_SOURCE = np.dtype([("centre", "<f4", 3), ("strength", "<f4"), ("radius", "<f4"),
+                           ("range", "<f4")])
+FRAME_RESULT = np.dtype([("bounds_min", "<f4", 3), ("bounds_max", "<f4", 3),
+                         ("max_speed", "<f4"), ("time", "<f4")])
+
+assert PARTICLE.itemsize == 40 and CONSTRAINT.itemsize == 16 and ANCHOR.itemsize == 48
+assert STRAND.itemsize == 64 and COLLIDER.itemsize == 144 and TETHER.itemsize == 12
+
+SHAPE_SPHERE, SHAPE_BOX, SHAPE_CAPSULE, SHAPE_TRIANGLE_MESH, SHAPE_CONVEX_HULL = range(5)
+
+STATUS_NAMES = {0: "PXB_OK", 1: "PXB_ERR_INVALID_ARGUMENT", 2: "PXB_ERR_UNSUPPORTED",
+                3: "PXB_ERR_CUDA", 4: "PXB_ERR_OUT_OF_MEMORY", 5: "PXB_ERR_INVALID_HANDLE",
+                6: "PXB_ERR_DEVICE_STATUS", 7: "PXB_ERR_TOO_LARGE"}
+
+
+class ClothParams(C.Structure):
+    """pxb_cloth_params == cloth::ClothParams (cloth.h:167-256) + the shear-compliance extension."""
+    _fields_ = [("stretch_compliance", f32), ("bend_compliance", f32), ("damping", f32),
+                ("thickness", f32), ("friction", f32), ("gravity_scale", f32),
+                ("max_velocity", f32), ("external_acceleration", f32 * 3), ("wind", f32 * 3),
+                ("wind_turbulence", f32), ("air_drag", f32), ("air_lift", f32),
+                ("self_collision", i32), ("self_distance", f32), ("tether_scale", f32),
+                ("substeps", u32), ("iterations", u32), ("sleep_threshold", f32),
+                ("sleep_time", f32), ("layer", u32), ("has_shear_compliance", i32),
+                ("shear_compliance", f32)]
+
+    @classmethod
+    def defaults(cls):
+        """The reference's ClothParams defaults (cloth.h:171-255)."""
+        p = cls()
+        p.stretch_compliance = 0.0
+        p.bend_compliance = 5e-5
+        p.damping = 0.05
+        p.thickness = 0.03
+        p.friction = 0.5
+        p.gravity_scale = 1.0
+        p.max_velocity = 100.0
+        p.wind_turbulence = 0.0
+        p.air_drag = 0.02
+        p.air_lift = 0.02
+        p.self_collision = 0
+        p.self_distance = 0.0
+        p.tether_scale = 1.02
+        p.substeps = 0
+        p.iterations = 0
+        p.sleep_threshold = 0.05
+        p.sleep_time = 0.5
+        p.layer = 0
+        p.has_shear_compliance = 0
+        p.shear_compliance = 0.0
+        return p
+
+
+class StrandParams(C.Structure):
+    """pxb_strand_params == hair::StrandParams (strand.h:93-148)."""
+    _fields_ = [("stretch_compliance", f32), ("global_shape", f32),
+                ("global_shape_falloff", f32), ("local_shape", f32), ("damping", f32),
+                ("thickness", f32), ("friction", f32), ("gravity_scale", f32),
+                ("max_velocity", f32), ("external_acceleration", f32 * 3), ("wind", f32 * 3),
+                ("wind_turbulence", f32), ("air_drag", f32), ("substeps", u32),
+                ("iterations", u32), ("sleep_threshold", f32), ("sleep_time", f32),
+                ("layer", u32)]
+
+    @classmethod
+    def defaults(cls):
+        """The reference's StrandParams defaults (strand.h:96-147)."""
+        p = cls()
+        p.stretch_compliance = 0.0
+        p.global_shape = 0.22
+        p.global_shape_falloff = 1.6
+        p.local_shape = 0.35
+        p.damping = 0.08
+        p.thickness = 0.01
+        p.friction = 0.4
+        p.gravity_scale = 1.0
+        p.max_velocity = 50.0
+        p.wind_turbulence = 0.1
+        p.air_drag = 0.6
+        p.substeps = 0
+        p.iterations = 0
+        p.sleep_threshold = 0.02
+        p.sleep_time = 0.6
+        p.layer = 0
+        return p
+
+
+P = C.c_void_p
+
+
+class ClothDesc(C.Structure):
+    """pxb_cloth_desc: a cloth as plain pointers into caller memory."""
+    _fields_ = [("particles", P), ("n_particles", u32), ("stretch", P), ("n_stretch", u32),
+                ("stretch_batches", P), ("n_stretch_batches", u32), ("bend", P),
+                ("n_bend", u32), ("bend_batches", P), ("n_bend_batches", u32), ("tethers", P),
+                ("n_tethers", u32), ("anchors", P), ("n_anchors", u32), ("triangles", P),
+                ("n_triangle_indices", u32), ("columns", u32), ("rows", u32),
+                ("params", ClothParams), ("time", f32), ("stretch_batch_compliance", P),
+                ("bend_batch_compliance", P)]
+
+
+class StrandSetDesc(C.Structure):
+    """pxb_strand_set_desc."""
+    _fields_ = [("particles", P), ("n_particles", u32), ("stretch", P), ("n_stretch", u32),
+                ("stretch_batches", P), ("n_stretch_batches", u32), ("rest_local", P),
+                ("rest_offset", P), ("strands", P), ("n_strands", u32),
+                ("params", StrandParams), ("time", f32)]
+
+
+class GridClothDesc(C.Structure):
+    """pxb_grid_cloth_desc == cloth::GridClothDesc (cloth_builder.h:52-64) + seeded jitter."""
+    _fields_ = [("columns", u32), ("rows", u32), ("width", f32), ("height", f32),
+                ("center", f32 * 3), ("orientation", f32 * 4), ("total_mass", f32),
+                ("shear", i32), ("params", ClothParams), ("jitter", f32),
+                ("jitter_seed", C.c_uint64)]
+
+
+class ClothStepDesc(C.Structure):
+    """pxb_cloth_step_desc."""
+    _fields_ = [("cloths", P), ("n_cloths", u32), ("colliders", P), ("collider_offsets", P),
+                ("gravity", f32 * 3), ("sources", P), ("source_offsets", P),
+                ("substeps", u32), ("iterations", u32), ("h", f32)]
+
+
+class StrandStepDesc(C.Structure):
+    """pxb_strand_step_desc."""
+    _fields_ = [("sets", P), ("n_sets", u32), ("colliders", P), ("collider_offsets", P),
+                ("gravity", f32 * 3), ("sources", P), ("source_offsets", P),
+                ("substeps", u32), ("iterations", u32), ("h", f32)]
+
+
+def ptr(a):
+    """Data pointer of a numpy array (None for an empty/None array)."""
+    if a is None or a.size == 0:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data

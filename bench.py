@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Cloth XPBD benchmark: cloth vertex-substeps/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+                    [--workload uniform_batch|single_drape|uneven_batch] [--cloths C]
+
+One step = one PhysicsWorld cloth frame for every cloth of the workload: a single batched
+launch of the device solver (pxb_cloths_step) advancing each cloth by solve_cloth(h = 1/60,
+4 substeps, 10 iterations). Default workload: the uniform batch, 1024 sheets of 64x64, seeded
+synthetic scenes (physxcoopa_b200/scenes.py). Vertex-substeps = sum of particles x substeps x
+steps.
+
+  value    device-resident throughput: inputs in HBM, K steps timed with CUDA events on the
+           library's own stream, max over ranks (weak scaling: each rank runs the full batch).
+  e2e      the same steps through the public C-ABI as an engine frame uses it: per step the
+           step inputs (per-cloth step records, colliders) go host->device from pinned memory
+           and every cloth's particle positions plus per-cloth bounds/speed come back to
+           pinned host memory.
+  roofline shared-memory bound (the cloth lives in shared memory during a step): algorithmic
+           bytes per launch = sum over cloths of (iterations x constraints x 68 B + particles x
+           150 B) x substeps, over the measured per-launch duration, against the device's
+           shared-memory bandwidth measured on the spot by pxb_measure_smem_bandwidth.
+  cpu_baseline  the reference's own solve_cloth (oracle/_ref, compiled from the reference's
+           headers) on a bounded sample of the workload on the host's cores, whole cloths per
+           thread as the reference's serial dispatch solves them.
+
+--impl reference runs only that CPU implementation (rank 0; other ranks exit 0).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SPEC = "cloth vertex-substeps/s on 1 B200: plain XPBD vs NN warm-start at equal residual"
+METRIC = "cloth vertex-substeps/s (plain XPBD)"
+UNIT = "vertex-substeps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    ap.add_argument("--workload", default="uniform_batch",
+                    choices=["uniform_batch", "single_drape", "uneven_batch"])
+    ap.add_argument("--cloths", type=int, default=None)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def build_scene(args, rank):
+    from physxcoopa_b200 import scenes
+    if args.workload == "single_drape":
+        return scenes.single_drape(seed=rank)
+    if args.workload == "uniform_batch":
+        return scenes.uniform_batch(n=args.cloths or 1024, side=64, seed=1 + rank)
+    return scenes.uneven_batch(n=args.cloths or 4096, seed=2 + rank)
+
+
+def workload_config(args, sc):
+    return {"workload": sc.name, "cloths": len(sc.cloths), "vertices": sc.vertices,
+            "substeps": sc.substeps, "iterations": sc.iterations, "h": sc.h,
+            "compliance": "structural 0 / shear 1e-6 / bend 1e-4",
+            "l2": "inputs larger than L2 (device state of the batch exceeds 126 MB)"
+            if sc.vertices * 64 > 126e6 else "inputs fit in L2"}
+
+
+# ------------------------------------------------------------------------------------------
+# clocks
+# ------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------------------------------
+# reference CPU implementation (oracle/_ref) on the host cores
+# ------------------------------------------------------------------------------------------
+
+def reference_cpu(sc, seconds_target=12.0, threads=None):
+    """Times the reference's solve_cloth on a bounded sample of the workload. Returns a dict."""
+    import ctypes as C
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _checkers as K
+    from physxcoopa_b200 import _abi as A
+    threads = threads or os.cpu_count() or 1
+    kind = "reference" if K.ref_available() else "port"
+    n_total = len(sc.cloths)
+
+    def timed(sample, steps, nthreads):
+        if kind == "reference":
+            refs = [K.RefCloth.from_arrays(sc.cloths[i]) for i in sample]
+            cols = [sc.colliders[i] for i in sample]
+            flat = np.ascontiguousarray(np.concatenate(cols)) if cols else np.zeros(0, A.COLLIDER)
+            offs = np.zeros(len(sample) + 1, np.uint32)
+            offs[1:] = np.cumsum([len(c) for c in cols])
+            handles = (C.c_void_p * len(refs))(*[r.h for r in refs])
+            return K.ref().pxbref_bench_cloths(handles, len(refs), A.ptr(flat), A.ptr(offs),
+                                               K.vec(sc.gravity), sc.substeps, sc.iterations,
+                                               sc.h, steps, nthreads)
+        # the C restatement, single-threaded
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for i in sample:
+                c = sc.cloths[i].copy()
+                K.oracle_step_cloth(c, sc.colliders[i], substeps=sc.substeps,
+                                    iterations=sc.iterations, h=sc.h)
+        return time.perf_counter() - t0
+
+    # calibrate on one cloth, one step, one thread
+    probe = timed([0], 1, 1)
+    per_cloth = max(probe, 1e-4)
+    nthreads = threads if kind == "reference" else 1
+    n_sample = int(min(n_total, max(nthreads, seconds_target * nthreads / per_cloth)))
+    n_sample = max(1, (n_sample // nthreads) * nthreads) if n_sample >= nthreads else n_sample
+    sample = list(range(n_sample))
+    wall = timed(sample, 1, nthreads)
+    steps = 1
+    if wall < 0.5 * seconds_target and n_sample == n_total:
+        steps = max(1, int(seconds_target / max(wall, 1e-3)))
+        wall = timed(sample, steps, nthreads)
+    verts = sum(len(sc.cloths[i].particles) for i in sample) * sc.substeps * steps
+    return {"value": verts / wall, "unit": UNIT, "cores": nthreads, "kind": kind,
+            "sample": f"{n_sample} of {n_total} cloths of the workload, {steps} step(s) each, "
+                      f"{nthreads} host threads, {wall:.1f} s (reference solve_cloth -O2; the "
+                      f"reference has one stretch compliance, so shear runs at the structural one)"
+            if kind == "reference" else f"{n_sample} cloths, oracle port, 1 thread, {wall:.1f} s"}
+
+
+# ------------------------------------------------------------------------------------------
+# main
+# ------------------------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        sc = build_scene(args, 0)
+        res = []
+        for _ in range(max(args.warmup, 0)):
+            pass  # the reference has no warm-up state; each sample builds fresh cloths
+        for _ in range(args.steps):
+            res.append(reference_cpu(sc, seconds_target=8.0))
+        value = statistics.median(r["value"] for r in res)
+        cb = dict(res[0])
+        cb["value"] = value
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes)",
+                "config": workload_config(args, sc), "impl": "reference", "cpu_baseline": cb,
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    from physxcoopa_b200 import runtime as R
+
+    sc = build_scene(args, rank)
+    ctx = R.Context(local_rank)
+    ids = [ctx.add_cloth(c) for c in sc.cloths]
+    d, keep = ctx.make_step(ids, sc.colliders, sc.gravity, sc.sources, sc.substeps,
+                            sc.iterations, sc.h)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local_rank))
+
+    for _ in range(max(args.warmup, 3)):
+        ctx.step_desc(d)
+    ctx.synchronize()
+    smem_bw = ctx.measure_smem_bandwidth()
+    if dist:
+        dist.barrier()
+
+    # --- device-resident timed region ----------------------------------------------------
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = ctx.launch_count
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    with torch.cuda.stream(stream):
+        t_start.record(stream)
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            ctx.step_desc(d)
+            ev[k][1].record(stream)
+        t_end.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = ctx.launch_count - launches0
+    elapsed_ms = t_start.elapsed_time(t_end)
+    per_launch_ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    if dist:
+        t = torch.tensor([elapsed_ms, per_launch_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms, per_launch_ms = float(t[0]), float(t[1])
+
+    verts_per_step = sc.vertices * sc.substeps
+    value = world * verts_per_step * args.steps / (elapsed_ms * 1e-3)
+
+    # --- roofline of the dominant kernel (shared memory) ----------------------------------
+    cons = sum(len(c.stretch) + len(c.bend) for c in sc.cloths)
+    algo_bytes = sc.substeps * (sc.iterations * cons * 68 + sc.vertices * 150)
+    achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
+    peak = smem_bw / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"cloth_step_{args.workload}.json")
+    if os.path.exists(prof):
+        try:
+            pj = json.load(open(prof))
+            traffic = pj.get("dram_bytes_per_launch_full_workload")
+        except (OSError, ValueError):
+            traffic = None
+
+    # --- end to end through the public API with host buffers -----------------------------
+    import ctypes as C
+    e2e_steps = args.e2e_steps or max(3, args.steps // 2)
+    out = torch.empty(3 * sc.vertices, dtype=torch.float32, pin_memory=True)
+    out_np = out.numpy()
+    ids_np = np.ascontiguousarray(ids, np.uint64)
+    from physxcoopa_b200 import _abi as A
+    res_out = np.zeros(len(ids), A.FRAME_RESULT)
+    # pxb_cloths_step uploads one staging block per step: per-cloth step records (184 B),
+    # collider snapshots (236 B), gravity sources (24 B) and the launch order (4 B), each
+    # section padded to 256 B.
+    al = lambda x: (x + 255) & ~255
+    n_col = sum(len(c) for c in sc.colliders)
+    n_src = sum(0 if s is None else len(s) for s in (sc.sources or []))
+    h2d = al(184 * len(ids)) + al(236 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * len(ids))
+    d2h = 12 * sc.vertices + 32 * len(ids) + 4
+    ctx.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            ctx.step_desc(d)
+            ctx.read_positions(ids_np, out_np)
+            ctx.lib.pxb_cloths_read_results(ctx.h, A.ptr(ids_np), len(ids_np), A.ptr(res_out))
+        e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t[0])
+    e2e_value = world * verts_per_step * e2e_steps / (e2e_ms * 1e-3)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = reference_cpu(sc)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scenes)",
+            "config": dict(workload_config(args, sc), parallelism=f"independent cloth batches x{world}"),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+            "roofline": {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "measured on this GPU by pxb_measure_smem_bandwidth",
+                         "kernel": "cloth_step_kernel", "per_launch_ms": per_launch_ms,
+                         "algorithmic_bytes_per_launch": algo_bytes},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "spec_metric": SPEC,
+        }
+        print(json.dumps(line))
+    del keep
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -387,6 +387,15 @@ pxb_status pxb_host_cloth_view(pxb_host_cloth* cloth, pxb_cloth_desc* view_out);
 pxb_status pxb_host_cloth_mutable(pxb_host_cloth* cloth, pxb_particle** particles,
                                   pxb_anchor** anchors, pxb_cloth_params** params);
 
+/* ------------------------------------------------------------------------------------------ */
+/* Diagnostics                                                                                  */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Measures the achievable shared-memory bandwidth of the whole device (bytes read + written
+ * per second, one 1024-thread CTA per SM copying float4s between two shared buffers). The
+ * cloth kernel is bound by this figure; benchmarks use it as the roofline denominator. */
+pxb_status pxb_measure_smem_bandwidth(pxb_context* ctx, double* bytes_per_second);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

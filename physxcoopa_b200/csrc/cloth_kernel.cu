@@ -1,0 +1,742 @@
+// cloth_kernel.cu -- the XPBD cloth substep on sm_100a: one CTA per cloth, the cloth resident
+// in shared memory for the whole step.
+//
+// Replaces cloth::solve_cloth (physxcoopa/cloth/cloth_solver.h:158-460) for grid cloths. One
+// launch advances a batch of cloths by one call each (the loop of PhysicsWorld::step_cloths_,
+// world.h:1759-1847). Per CTA:
+//
+//   prologue   cp.async.bulk (TMA, no multicast) stages positions and rest lengths from HBM into
+//              shared memory behind an mbarrier. A thread owns layout slots tid, tid + T, ...;
+//              their velocities and substep-start positions stay in the cloth's own HBM arrays
+//              (L2-resident while the CTA runs; only the owner touches a slot), which leaves the
+//              whole register budget to the projection loop.
+//   substeps   1 aero (per-particle gather of its incident triangles, ascending triangle order)
+//              2+3 integrate + anchor lerp (owner thread)
+//              4 iterations x colours of project_distance over affine colour segments,
+//                one __syncthreads per colour (colours are particle-disjoint)
+//              5+7+8 tethers, collider projection, velocity + friction + clamp (owner thread)
+//   epilogue   positions back to HBM with cp.async.bulk, lambdas stored, bounds and max speed
+//              reduced with warp shuffles.
+//
+// Arithmetic is IEEE single precision with no contraction (built with -fmad=false) and the
+// reference's operation order, so a step reproduces the CPU oracle to the bit (up to the sign of
+// an exactly-zero coordinate; see the lambda note in the colour loop).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/physxcoopa_b200.h"
+#include "pxb_internal.h"
+#include "pxb_kernels.h"
+
+namespace pxb {
+namespace {
+
+constexpr int kMaxThreads = 1024;
+constexpr uint32_t kWaitLimit = 1u << 26;  // bounded mbarrier polls before giving up
+
+// ------------------------------------------------------------------------------------------
+// TMA bulk copies and mbarriers (inline PTX)
+// ------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t saddr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(saddr(dst)),
+        "l"(src), "r"(bytes), "r"(saddr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(saddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on phase `parity`; returns false (and the caller raises an error word) if the
+// transaction never completes.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(saddr(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit_and_wait() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// ------------------------------------------------------------------------------------------
+// Vector helpers, single precision, reference operation order
+// ------------------------------------------------------------------------------------------
+
+struct f3 {
+    float x, y, z;
+};
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return f3{x, y, z}; }
+__device__ __forceinline__ f3 add(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ f3 sub(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ f3 mul(f3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ f3 smul(float s, f3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ f3 divs(f3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float len(f3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+    return mk(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+__device__ __forceinline__ f3 xyz(float4 v) { return mk(v.x, v.y, v.z); }
+__device__ __forceinline__ f3 ld3(const float* p) { return mk(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }
+__device__ __forceinline__ float minr(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float maxr(float a, float b) { return a < b ? b : a; }
+__device__ __forceinline__ float clamp01(float t) { return t < 0.0f ? 0.0f : (1.0f < t ? 1.0f : t); }
+
+// ------------------------------------------------------------------------------------------
+// Collision: cloth::project_particle (cloth_collision.h:386-420) over a precomputed snapshot
+// ------------------------------------------------------------------------------------------
+
+// geometry::closest_point_on_segment (capsule.h:39-49).
+__device__ __forceinline__ f3 closest_on_segment(f3 point, f3 a, f3 b) {
+    const f3 ab = sub(b, a);
+    const float len2 = dot(ab, ab);
+    if (len2 < PXB_EPSILON) return a;
+    const float t = clamp01(dot(sub(point, a), ab) / len2);
+    return add(a, mul(ab, t));
+}
+
+// cloth::detail::project_at_pose_ (cloth_collision.h:109-203) for one pose of the snapshot.
+__device__ bool project_pose(const PxbDevCollider* __restrict__ c, int pose, bool allow_sweep,
+                             float thickness, f3& p, f3& normal_out, float& depth_out) {
+    const PxbPose* ps = &c->pose[pose];
+    const int type = __ldg(&c->type);
+    if (type == PXB_SHAPE_SPHERE) {
+        const f3 center = ld3(ps->center);
+        f3 on_axis = center;
+        if (allow_sweep && __ldg(&c->swept_sphere)) on_axis = closest_on_segment(p, center, ld3(ps->cb));
+        const f3 d = sub(p, on_axis);
+        const float l = len(d);
+        const float target = __ldg(&c->radius) + thickness;
+        if (l >= target) return false;
+        const f3 n = (l > PXB_EPSILON) ? divs(d, l) : mk(0.0f, 0.0f, 1.0f);
+        depth_out = target - l;
+        p = add(on_axis, mul(n, target));
+        normal_out = n;
+        return true;
+    }
+    if (type == PXB_SHAPE_CAPSULE) {
+        const f3 on_axis = closest_on_segment(p, ld3(ps->ca), ld3(ps->cb));
+        const f3 d = sub(p, on_axis);
+        const float l = len(d);
+        const float target = __ldg(&c->radius) + thickness;
+        if (l >= target) return false;
+        const f3 n = (l > PXB_EPSILON) ? divs(d, l) : ld3(ps->t1);
+        depth_out = target - l;
+        p = add(on_axis, mul(n, target));
+        normal_out = n;
+        return true;
+    }
+    // Box
+    const f3 center = ld3(ps->center);
+    const f3 ax = ld3(ps->ax), ay = ld3(ps->ay), az = ld3(ps->az);
+    const f3 d = sub(p, center);
+    const f3 local = mk(dot(d, ax), dot(d, ay), dot(d, az));
+    const f3 he = ld3(c->he);
+    const bool inside = fabsf(local.x) <= he.x && fabsf(local.y) <= he.y && fabsf(local.z) <= he.z;
+    f3 lt, ln;
+    if (inside) {
+        const f3 slack = mk(he.x - fabsf(local.x), he.y - fabsf(local.y), he.z - fabsf(local.z));
+        const int axis = (slack.x <= slack.y && slack.x <= slack.z) ? 0 : (slack.y <= slack.z ? 1 : 2);
+        const float lc = axis == 0 ? local.x : (axis == 1 ? local.y : local.z);
+        const float hc = axis == 0 ? he.x : (axis == 1 ? he.y : he.z);
+        const float sc = axis == 0 ? slack.x : (axis == 1 ? slack.y : slack.z);
+        const float sign = (lc >= 0.0f) ? 1.0f : -1.0f;
+        lt = local;
+        ln = mk(0.0f, 0.0f, 0.0f);
+        const float tv = sign * (hc + thickness);
+        if (axis == 0) { lt.x = tv; ln.x = sign; }
+        else if (axis == 1) { lt.y = tv; ln.y = sign; }
+        else { lt.z = tv; ln.z = sign; }
+        depth_out = sc + thickness;
+    } else {
+        lt = mk(minr(maxr(local.x, -he.x), he.x), minr(maxr(local.y, -he.y), he.y),
+                minr(maxr(local.z, -he.z), he.z));
+        const f3 delta = sub(local, lt);
+        const float l = len(delta);
+        if (l >= thickness) return false;
+        ln = (l > PXB_EPSILON) ? divs(delta, l) : mk(0.0f, 0.0f, 1.0f);
+        depth_out = thickness - l;
+        lt = add(lt, mul(ln, thickness));
+    }
+    p = add(add(add(center, mul(ax, lt.x)), mul(ay, lt.y)), mul(az, lt.z));
+    const f3 nw = add(add(mul(ax, ln.x), mul(ay, ln.y)), mul(az, ln.z));
+    normal_out = mul(nw, 1.0f / sqrtf(dot(nw, nw)));
+    return true;
+}
+
+__device__ __forceinline__ bool project_particle(const PxbDevCollider* __restrict__ c,
+                                                 float thickness, f3& p, f3& n, float& depth) {
+    if (!__ldg(&c->enabled)) return false;
+    if (!__ldg(&c->two_pose)) return project_pose(c, 0, true, thickness, p, n, depth);
+    f3 p0 = p, n0 = mk(0, 0, 0), p1 = p, n1 = mk(0, 0, 0);
+    float d0 = 0.0f, d1 = 0.0f;
+    const bool h0 = project_pose(c, 0, false, thickness, p0, n0, d0);
+    const bool h1 = project_pose(c, 1, false, thickness, p1, n1, d1);
+    if (!h0 && !h1) return false;
+    if (h1 && (!h0 || d1 > d0)) {
+        p = p1; n = n1; depth = d1;
+    } else {
+        p = p0; n = n0; depth = d0;
+    }
+    return true;
+}
+
+// ------------------------------------------------------------------------------------------
+// Aerodynamics: one triangle's per-corner share (cloth_solver.h:204-225)
+// ------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ void tri_share(f3 p0, f3 p1, f3 p2, f3 v0, f3 v1, f3 v2, f3 wind,
+                                          float drag, float lift, f3& acc) {
+    const f3 e1 = sub(p1, p0);
+    const f3 e2 = sub(p2, p0);
+    const f3 cr = cross(e1, e2);
+    const float twice_area = len(cr);
+    if (twice_area < PXB_EPSILON) return;
+    const f3 face_n = divs(cr, twice_area);
+    const f3 v = sub(mul(add(add(v0, v1), v2), 1.0f / 3.0f), wind);
+    const float vn = dot(v, face_n);
+    const f3 vt = sub(v, smul(vn, face_n));
+    const float scale = -0.5f * twice_area * fabsf(vn);
+    const f3 inner = add(smul(drag * vn, face_n), smul(lift, vt));
+    const f3 force = smul(scale, inner);
+    acc = add(acc, mul(force, 1.0f / 3.0f));
+}
+
+__device__ __forceinline__ int lay(int x, int y, int Q, int S) { return y * S + (x & 3) * Q + (x >> 2); }
+
+// ------------------------------------------------------------------------------------------
+// One XPBD distance projection, two at a time for ILP (cloth_solver.h:119-138)
+// ------------------------------------------------------------------------------------------
+
+// Computes the new endpoint positions of one constraint. Returns false when the reference
+// returns early (both pinned, or coincident endpoints) -- nothing is written then.
+__device__ __forceinline__ bool solve_pair(float4& pa, float4& pb, float rest, float lam,
+                                           float alpha, float& dlambda) {
+    const float w = pa.w + pb.w;
+    if (w <= 0.0f) return false;
+    const float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
+    const float l = sqrtf(dx * dx + dy * dy + dz * dz);
+    if (l < PXB_EPSILON) return false;
+    const float nx = dx / l, ny = dy / l, nz = dz / l;
+    const float c = l - rest;
+    dlambda = (-c - alpha * lam) / (w + alpha);
+    const float cx = dlambda * nx, cy = dlambda * ny, cz = dlambda * nz;
+    pa.x = pa.x + pa.w * cx;
+    pa.y = pa.y + pa.w * cy;
+    pa.z = pa.z + pa.w * cz;
+    pb.x = pb.x - pb.w * cx;
+    pb.y = pb.y - pb.w * cy;
+    pb.z = pb.z - pb.w * cz;
+    return true;
+}
+
+struct SegReg {
+    int count, per_row, a_base, row_stride, d, rest_base, lam_base;
+    uint32_t magic;
+};
+
+__device__ __forceinline__ void seg_slots(const SegReg& s, int i, int& la, int& lb) {
+    // magic == 0 marks per_row == 1 (floor(2^32 / 1) + 1 does not fit in 32 bits).
+    const int r = s.magic ? static_cast<int>(__umulhi(static_cast<uint32_t>(i), s.magic)) : i;
+    const int k = i - r * s.per_row;
+    la = s.a_base + r * s.row_stride + k;
+    lb = la + s.d;
+}
+
+// ------------------------------------------------------------------------------------------
+// Block reductions (warp shuffles, fixed order -> deterministic)
+// ------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ float warp_sum(float v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_min(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// The kernel
+// ------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kMaxThreads, 1)
+cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
+                  const PxbDevCollider* __restrict__ colliders,
+                  const pxb_gravity_source* __restrict__ sources,
+                  const int32_t* __restrict__ order, PxbFrameResult* __restrict__ results,
+                  uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ PxbSeg s_seg[PXB_MAX_SEGS];
+    // Per-cloth scalars live in shared memory and are read at their point of use: held in
+    // registers for the whole kernel they would crowd out the particle state (64 registers at
+    // 1024 threads).
+    __shared__ PxbClothDev sC;
+    __shared__ PxbClothStep sP;
+    __shared__ float s_red[32][7];
+    __shared__ float s_base[3];
+
+    const int tid = threadIdx.x;
+    const int T = blockDim.x;
+    const int slot = blockIdx.x;
+    {
+        const int ci = __ldg(&order[slot]);
+        const int* srcC = reinterpret_cast<const int*>(&cloths[ci]);
+        int* dstC = reinterpret_cast<int*>(&sC);
+        for (int i = tid; i < static_cast<int>(sizeof(PxbClothDev) / 4); i += T) dstC[i] = srcC[i];
+        const int* srcP = reinterpret_cast<const int*>(&stepp[slot]);
+        int* dstP = reinterpret_cast<int*>(&sP);
+        for (int i = tid; i < static_cast<int>(sizeof(PxbClothStep) / 4); i += T) dstP[i] = srcP[i];
+    }
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_proxy_async();
+    }
+    __syncthreads();
+
+    const int n_layout = sC.n_layout;
+    float4* pos = reinterpret_cast<float4*>(smem);
+    float* rest = reinterpret_cast<float*>(smem + 16 * static_cast<size_t>(n_layout));
+    float* U = rest + sC.n_rest_pad;  // lambdas of compliant colours / velocity scratch (SoA)
+
+    // --- prologue: stage positions and rest lengths with TMA bulk copies -------------------
+    if (tid == 0) {
+        const uint32_t pos_bytes = 16u * static_cast<uint32_t>(n_layout);
+        const uint32_t rest_bytes = 4u * static_cast<uint32_t>(sC.n_rest_pad);
+        mbar_arrive_expect_tx(&bar, pos_bytes + rest_bytes);
+        bulk_g2s(pos, sC.pos, pos_bytes, &bar);
+        if (rest_bytes) bulk_g2s(rest, sC.rest, rest_bytes, &bar);
+    }
+    for (int i = tid; i < sC.n_segs; i += T) s_seg[i] = sC.segs[i];
+
+    const bool staged = mbar_wait_bounded(&bar, 0);
+    if (!staged && tid == 0) atomicOr(err, PXB_DEVERR_TMA_TIMEOUT);
+    __syncthreads();
+    if (!staged) return;
+
+    // --- gravity: uniform, or the source field at the cloth's mean position (world.h:1833) --
+    if (sP.src_count > 0) {
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+        for (int l = tid; l < n_layout; l += T) {
+            if (sC.vel[l].w != 0.0f) {
+                const float4 p = pos[l];
+                sx += p.x; sy += p.y; sz += p.z;
+            }
+        }
+        sx = warp_sum(sx); sy = warp_sum(sy); sz = warp_sum(sz);
+        if ((tid & 31) == 0) {
+            s_red[tid >> 5][0] = sx; s_red[tid >> 5][1] = sy; s_red[tid >> 5][2] = sz;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+            const int nw = (T + 31) >> 5;
+            for (int w = 0; w < nw; ++w) { cx += s_red[w][0]; cy += s_red[w][1]; cz += s_red[w][2]; }
+            const float fn = static_cast<float>(sC.n_real);
+            const f3 centre = mk(cx / fn, cy / fn, cz / fn);
+            // PhysicsWorld::field_at_ (world.h:2048-2068)
+            float best = 0.0f;
+            f3 pull = mk(sP.gravity[0], sP.gravity[1], sP.gravity[2]);
+            bool found = false;
+            for (int k = 0; k < sP.src_count; ++k) {
+                const pxb_gravity_source* g = &sources[sP.src_begin + k];
+                const f3 d = sub(ld3(g->centre), centre);
+                const float r = len(d);
+                const float range = __ldg(&g->range), radius = __ldg(&g->radius),
+                            strength = __ldg(&g->strength);
+                if (range > 0.0f && r > range) continue;
+                if (r < 1e-6f) continue;
+                const float a = r <= radius ? strength : strength * (radius / r) * (radius / r);
+                if (!found || a > best) {
+                    best = a;
+                    pull = mul(divs(d, r), a);
+                    found = true;
+                }
+            }
+            const f3 base = add(mul(pull, sP.gravity_scale),
+                                mk(sP.external_acceleration[0], sP.external_acceleration[1],
+                                   sP.external_acceleration[2]));
+            s_base[0] = base.x; s_base[1] = base.y; s_base[2] = base.z;
+        }
+    } else if (tid == 0) {
+        s_base[0] = sP.base_accel[0]; s_base[1] = sP.base_accel[1]; s_base[2] = sP.base_accel[2];
+    }
+    __syncthreads();
+
+    const int steps = sP.steps;
+    float4* __restrict__ gvel = sC.vel;
+    float4* __restrict__ gprv = sC.prv;
+    for (int step = 0; step < steps; ++step) {
+        const bool aero = sP.aero != 0 && sC.aero_grid != 0;
+        // --- 1. aerodynamics: gather the shares of the incident triangles -----------------
+        // Velocities are parked in U (SoA) for the neighbour reads; each particle's summed
+        // share is parked in its own prv slot until integrate consumes it.
+        if (aero) {
+            for (int l = tid; l < n_layout; l += T) {
+                const float4 vv = gvel[l];
+                U[l] = vv.x;
+                U[n_layout + l] = vv.y;
+                U[2 * n_layout + l] = vv.z;
+            }
+            __syncthreads();
+            const int Q = sC.Q, S = sC.S, cols = sC.columns, rows = sC.rows;
+            const f3 wind = mk(sP.wind[0], sP.wind[1], sP.wind[2]);
+            const float drag = sP.air_drag, lift = sP.air_lift;
+            for (int l = tid; l < n_layout; l += T) {
+                const int y = l / S;
+                const int j = l - y * S;
+                const int cls = j / Q;
+                const int x = 4 * (j - cls * Q) + cls;
+                if (x >= cols) continue;  // ghost slot
+                const bool xm = x >= 1, xp = x + 1 < cols, ym = y >= 1, yp = y + 1 < rows;
+                auto P3 = [&](int li) { return xyz(pos[li]); };
+                auto V3 = [&](int li) { return mk(U[li], U[n_layout + li], U[2 * n_layout + li]); };
+                const f3 p00 = P3(l), v00 = V3(l);
+                f3 a = mk(0.0f, 0.0f, 0.0f);
+                if (xm && ym) {  // cell (x-1, y-1): T0 then T1
+                    const int lmm = lay(x - 1, y - 1, Q, S), l0m = lay(x, y - 1, Q, S),
+                              lm0 = lay(x - 1, y, Q, S);
+                    tri_share(P3(lmm), P3(l0m), p00, V3(lmm), V3(l0m), v00, wind, drag, lift, a);
+                    tri_share(P3(lmm), p00, P3(lm0), V3(lmm), v00, V3(lm0), wind, drag, lift, a);
+                }
+                if (xp && ym) {  // cell (x, y-1): T1
+                    const int l0m = lay(x, y - 1, Q, S), lp0 = lay(x + 1, y, Q, S);
+                    tri_share(P3(l0m), P3(lp0), p00, V3(l0m), V3(lp0), v00, wind, drag, lift, a);
+                }
+                if (xm && yp) {  // cell (x-1, y): T0
+                    const int lm0 = lay(x - 1, y, Q, S), l0p = lay(x, y + 1, Q, S);
+                    tri_share(P3(lm0), p00, P3(l0p), V3(lm0), v00, V3(l0p), wind, drag, lift, a);
+                }
+                if (xp && yp) {  // cell (x, y): T0 then T1
+                    const int lp0 = lay(x + 1, y, Q, S), lpp = lay(x + 1, y + 1, Q, S),
+                              l0p = lay(x, y + 1, Q, S);
+                    tri_share(p00, P3(lp0), P3(lpp), v00, V3(lp0), V3(lpp), wind, drag, lift, a);
+                    tri_share(p00, P3(lpp), P3(l0p), v00, V3(lpp), V3(l0p), wind, drag, lift, a);
+                }
+                gprv[l] = make_float4(a.x, a.y, a.z, 0.0f);
+            }
+            __syncthreads();
+        }
+
+        // --- 4a. lambda reset (cloth_solver.h:253-254) ----------------------------------
+        for (int i = tid; i < sC.n_lam; i += T) U[i] = 0.0f;
+
+        // --- 2 + 3. integrate, then the anchor lerp (cloth_solver.h:230-250) --------------
+        {
+            const float alpha_t = static_cast<float>(step + 1) / static_cast<float>(steps);
+            const float hs = sP.hs, damping_factor = sP.damping_factor;
+            const f3 base_accel = mk(s_base[0], s_base[1], s_base[2]);
+            const PxbAnchorRec* anchors = reinterpret_cast<const PxbAnchorRec*>(sC.anchors);
+            for (int l = tid; l < n_layout; l += T) {
+                float4 p = pos[l];
+                const f3 acc = aero ? xyz(gprv[l]) : mk(0.0f, 0.0f, 0.0f);
+                gprv[l] = make_float4(p.x, p.y, p.z, 0.0f);
+                if (p.w != 0.0f) {
+                    f3 vv = xyz(gvel[l]);
+                    vv = add(vv, mul(add(base_accel, mul(acc, p.w)), hs));
+                    vv = mul(vv, damping_factor);
+                    p.x = p.x + vv.x * hs;
+                    p.y = p.y + vv.y * hs;
+                    p.z = p.z + vv.z * hs;
+                }
+                const int anc = __ldg(&sC.anchor_of[l]);
+                if (anc >= 0) {
+                    const PxbAnchorRec& a = anchors[anc];
+                    const float om = 1.0f - alpha_t;
+                    p.x = a.prev[0] * om + a.world[0] * alpha_t;
+                    p.y = a.prev[1] * om + a.world[1] * alpha_t;
+                    p.z = a.prev[2] * om + a.world[2] * alpha_t;
+                }
+                pos[l] = p;
+            }
+        }
+        __syncthreads();
+
+        // --- 4b. constraint iterations: colour by colour (cloth_solver.h:256-271) ----------
+        // A zero-compliance colour keeps no lambda: with alpha == 0 the multiplier never
+        // reaches a position (dlambda = (-c - 0*lambda)/w); only the sign of an exactly-zero
+        // correction could differ, which moves no coordinate that is not itself +-0.
+        {
+            const int iters = sP.iters, n_colours = sC.n_colours;
+            for (int it = 0; it < iters; ++it) {
+                for (int c = 0; c < n_colours; ++c) {
+                    const float alpha = sP.alpha[c];
+                    const int sb = sC.colour_seg[c], se = sC.colour_seg[c + 1];
+                    for (int sg = sb; sg < se; ++sg) {
+                        const PxbSeg& g = s_seg[sg];
+                        const SegReg sr{g.count, g.per_row, g.a_base, g.row_stride, g.d,
+                                        g.rest_base, g.lam_base, g.magic};
+                        const bool has_lam = sr.lam_base >= 0;
+                        int i = tid;
+                        for (; i + T < sr.count; i += 2 * T) {
+                            int la0, lb0, la1, lb1;
+                            seg_slots(sr, i, la0, lb0);
+                            seg_slots(sr, i + T, la1, lb1);
+                            float4 pa0 = pos[la0], pb0 = pos[lb0];
+                            float4 pa1 = pos[la1], pb1 = pos[lb1];
+                            const float r0 = rest[sr.rest_base + i];
+                            const float r1 = rest[sr.rest_base + i + T];
+                            const float lam0 = has_lam ? U[sr.lam_base + i] : 0.0f;
+                            const float lam1 = has_lam ? U[sr.lam_base + i + T] : 0.0f;
+                            float d0 = 0.0f, d1 = 0.0f;
+                            const bool w0 = solve_pair(pa0, pb0, r0, lam0, alpha, d0);
+                            const bool w1 = solve_pair(pa1, pb1, r1, lam1, alpha, d1);
+                            if (w0) {
+                                pos[la0] = pa0;
+                                pos[lb0] = pb0;
+                                if (has_lam) U[sr.lam_base + i] = lam0 + d0;
+                            }
+                            if (w1) {
+                                pos[la1] = pa1;
+                                pos[lb1] = pb1;
+                                if (has_lam) U[sr.lam_base + i + T] = lam1 + d1;
+                            }
+                        }
+                        if (i < sr.count) {
+                            int la0, lb0;
+                            seg_slots(sr, i, la0, lb0);
+                            float4 pa0 = pos[la0], pb0 = pos[lb0];
+                            const float lam0 = has_lam ? U[sr.lam_base + i] : 0.0f;
+                            float d0 = 0.0f;
+                            if (solve_pair(pa0, pb0, rest[sr.rest_base + i], lam0, alpha, d0)) {
+                                pos[la0] = pa0;
+                                pos[lb0] = pb0;
+                                if (has_lam) U[sr.lam_base + i] = lam0 + d0;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+
+        // --- 5 + 7 + 8. tethers, collisions, velocities (owner thread) ---------------------
+        {
+            const int col_begin = sP.col_begin, col_count = sP.col_count;
+            const float thickness = sP.thickness, inv_hs = sP.inv_hs;
+            for (int l = tid; l < n_layout; l += T) {
+                float4 p4 = pos[l];
+                f3 p = xyz(p4);
+                bool moved = false;
+                f3 nsum = mk(0.0f, 0.0f, 0.0f);
+                float dsum = 0.0f;
+                if (p4.w != 0.0f) {
+                    // 5. tether (cloth_solver.h:276-289); its anchor is a pinned particle
+                    const int2 teth = __ldg(&sC.tether[l]);
+                    if (teth.x >= 0) {
+                        const f3 anchor = xyz(pos[teth.x]);
+                        const f3 d = sub(p, anchor);
+                        const float l2 = len(d);
+                        const float max_len = __int_as_float(teth.y);
+                        if (!(l2 <= max_len || l2 < PXB_EPSILON)) {
+                            p = add(anchor, mul(d, max_len / l2));
+                            moved = true;
+                        }
+                    }
+                    // 7. colliders in list order (cloth_solver.h:379-410)
+                    for (int k = 0; k < col_count; ++k) {
+                        const PxbDevCollider* c = &colliders[col_begin + k];
+                        if (p.x < __ldg(&c->bmin[0]) - thickness || p.x > __ldg(&c->bmax[0]) + thickness ||
+                            p.y < __ldg(&c->bmin[1]) - thickness || p.y > __ldg(&c->bmax[1]) + thickness ||
+                            p.z < __ldg(&c->bmin[2]) - thickness || p.z > __ldg(&c->bmax[2]) + thickness) {
+                            continue;
+                        }
+                        f3 n = mk(0.0f, 0.0f, 0.0f);
+                        float depth = 0.0f;
+                        if (!project_particle(c, thickness, p, n, depth)) continue;
+                        moved = true;
+                        nsum = add(nsum, n);
+                        dsum += depth;
+                    }
+                }
+                if (moved) {
+                    p4.x = p.x; p4.y = p.y; p4.z = p.z;
+                    pos[l] = p4;
+                }
+                // 8. finalize (cloth_solver.h:414-451), every particle
+                const float4 pv = gprv[l];
+                f3 vv = mul(sub(p, xyz(pv)), inv_hs);
+                if (dsum > 0.0f) {
+                    const float nlen = len(nsum);
+                    if (nlen > PXB_EPSILON) {
+                        const f3 nrm = divs(nsum, nlen);
+                        const float vn = dot(vv, nrm);
+                        const f3 vt = sub(vv, smul(vn, nrm));
+                        if (vn < 0.0f) vv = sub(vv, smul(vn, nrm));
+                        const float budget = sP.friction * dsum * inv_hs;
+                        const float vt_len = len(vt);
+                        if (vt_len > PXB_EPSILON) vv = sub(vv, mul(vt, minr(1.0f, budget / vt_len)));
+                    }
+                }
+                const float v2 = dot(vv, vv);
+                if (v2 > sP.max_velocity2) vv = mul(vv, sP.max_velocity / sqrtf(v2));
+                const float real = gvel[l].w;
+                gvel[l] = make_float4(vv.x, vv.y, vv.z, real);
+            }
+        }
+        __syncthreads();
+    }
+
+    // --- epilogue --------------------------------------------------------------------------
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+        bulk_s2g(sC.pos, pos, 16u * static_cast<uint32_t>(n_layout));
+        bulk_commit_and_wait();
+    }
+    float bmin[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float bmax[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+    float vmax2 = 0.0f;
+    for (int l = tid; l < n_layout; l += T) {
+        const float4 vv = gvel[l];
+        if (vv.w == 0.0f) continue;  // ghost slot
+        const float4 p = pos[l];
+        bmin[0] = minr(bmin[0], p.x); bmin[1] = minr(bmin[1], p.y); bmin[2] = minr(bmin[2], p.z);
+        bmax[0] = maxr(bmax[0], p.x); bmax[1] = maxr(bmax[1], p.y); bmax[2] = maxr(bmax[2], p.z);
+        vmax2 = maxr(vmax2, dot(xyz(vv), xyz(vv)));
+    }
+    if (sP.write_lambdas) {
+        for (int i = tid; i < sC.n_lam; i += T) sC.lam_out[i] = U[i];
+    }
+    for (int a = tid; a < sC.n_anchors; a += T) {
+        PxbAnchorRec* rec = reinterpret_cast<PxbAnchorRec*>(sC.anchors) + a;
+        rec->prev[0] = rec->world[0];
+        rec->prev[1] = rec->world[1];
+        rec->prev[2] = rec->world[2];
+    }
+    float r[7] = {bmin[0], bmin[1], bmin[2], bmax[0], bmax[1], bmax[2], vmax2};
+    r[0] = warp_min(r[0]); r[1] = warp_min(r[1]); r[2] = warp_min(r[2]);
+    r[3] = warp_max(r[3]); r[4] = warp_max(r[4]); r[5] = warp_max(r[5]);
+    r[6] = warp_max(r[6]);
+    if ((tid & 31) == 0) {
+        for (int k = 0; k < 7; ++k) s_red[tid >> 5][k] = r[k];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const int nw = (T + 31) >> 5;
+        for (int w = 1; w < nw; ++w) {
+            for (int k = 0; k < 3; ++k) r[k] = fminf(r[k], s_red[w][k]);
+            for (int k = 3; k < 7; ++k) r[k] = fmaxf(r[k], s_red[w][k]);
+        }
+        PxbFrameResult* out = &results[slot];
+        for (int k = 0; k < 3; ++k) { out->bounds_min[k] = r[k]; out->bounds_max[k] = r[k + 3]; }
+        out->max_speed = sqrtf(r[6]);
+        out->time = 0.0f;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// project_particle over a batch of points (the collision primitive on its own)
+// ------------------------------------------------------------------------------------------
+
+__global__ void project_points_kernel(const PxbDevCollider* __restrict__ c, float thickness,
+                                      const float* __restrict__ pts, int n, float* __restrict__ out,
+                                      float* __restrict__ normals, float* __restrict__ depths,
+                                      int32_t* __restrict__ hits) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f3 p = mk(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+    f3 nn = mk(0, 0, 0);
+    float d = 0.0f;
+    const bool hit = project_particle(c, thickness, p, nn, d);
+    out[3 * i] = p.x; out[3 * i + 1] = p.y; out[3 * i + 2] = p.z;
+    normals[3 * i] = nn.x; normals[3 * i + 1] = nn.y; normals[3 * i + 2] = nn.z;
+    depths[i] = d;
+    hits[i] = hit ? 1 : 0;
+}
+
+// Positions from layout order to particle order (what a renderer or a state hash reads).
+__global__ void gather_positions_kernel(const PxbClothDev* __restrict__ cloths,
+                                        const int32_t* __restrict__ order,
+                                        const int64_t* __restrict__ out_offsets,
+                                        float* __restrict__ out) {
+    const PxbClothDev* C = &cloths[__ldg(&order[blockIdx.y])];
+    const int cols = C->columns, n = C->n_real, Q = C->Q, S = C->S;
+    float* dst = out + __ldg(&out_offsets[blockIdx.y]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int y = i / cols, x = i - y * cols;
+        const float4 p = C->pos[lay(x, y, Q, S)];
+        dst[3 * i] = p.x;
+        dst[3 * i + 1] = p.y;
+        dst[3 * i + 2] = p.z;
+    }
+}
+
+cudaError_t launch_gather_positions(const PxbClothDev* cloths, const int32_t* order,
+                                    const int64_t* out_offsets, int n_cloths, float* out,
+                                    cudaStream_t stream) {
+    if (n_cloths <= 0) return cudaSuccess;
+    dim3 grid(8, n_cloths);
+    gather_positions_kernel<<<grid, 256, 0, stream>>>(cloths, order, out_offsets, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cloth_step(const PxbClothDev* cloths, const PxbClothStep* steps,
+                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
+                              int n_blocks, int threads, int smem_bytes, cudaStream_t stream) {
+    static uint64_t configured = 0;  // one bit per device the attribute has been set on
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && !(configured >> dev & 1ull)) {
+        e = cudaFuncSetAttribute(cloth_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kMaxDynamicSmem);
+        if (e != cudaSuccess) return e;
+        configured |= 1ull << dev;
+    }
+    cloth_step_kernel<<<n_blocks, threads, smem_bytes, stream>>>(cloths, steps, colliders, sources,
+                                                                  order, results, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness, const float* pts,
+                                  int n, float* out, float* normals, float* depths, int32_t* hits,
+                                  cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const int tb = 256;
+    project_points_kernel<<<(n + tb - 1) / tb, tb, 0, stream>>>(collider, thickness, pts, n, out,
+                                                                 normals, depths, hits);
+    return cudaGetLastError();
+}
+
+}  // namespace pxb

@@ -1,0 +1,126 @@
+// pxb_internal.h -- host/device shared definitions of the B200 cloth / strand solver.
+//
+// Device data layout of one grid cloth (all in HBM, staged into shared memory per step):
+//
+//   layout index   l = y * S + (x % 4) * Q + x / 4,   Q = ceil(columns / 4), S = 4 * Q
+//
+// i.e. every row is split into the four "x mod 4" classes, each padded to Q slots. Slots with
+// x >= columns are ghosts: pinned (inv_mass 0), never touched by a constraint, excluded from
+// every reduction. In this order each of the 16 constraint colours of a make_grid_cloth sheet
+// (cloth_builder.h:128-194) reads and writes CONTIGUOUS float4 runs, so a warp's shared-memory
+// accesses are bank-conflict free for every colour.
+//
+// A colour is a list of affine segments. Constraint i of a segment joins layout slots
+//   la = a_base + r * row_stride + k,  lb = la + d,   r = i / per_row, k = i % per_row
+// and reads its rest length from slot (rest_base + i) and, when the colour is compliant, its
+// lambda from slot (lam_base + i). The host derives the segments from the reference's own
+// constraint lists and refuses the fast path unless they reproduce those lists exactly.
+#ifndef PXB_INTERNAL_H
+#define PXB_INTERNAL_H
+
+#include <stdint.h>
+
+#define PXB_MAX_COLOURS 16
+#define PXB_MAX_SEGS 64
+#define PXB_MAX_COLLIDERS_PER_CLOTH 64
+#define PXB_EPSILON 1e-6f  // util::k_epsilon (physxcoopa/util/math.h:19)
+
+// Error word bits a kernel may raise (never traps; the host reads them after the step).
+#define PXB_DEVERR_BAD_INDEX 0x1u
+#define PXB_DEVERR_TMA_TIMEOUT 0x2u
+#define PXB_DEVERR_QUEUE_TIMEOUT 0x4u
+
+struct PxbSeg {
+    int32_t count;      // constraints in this segment
+    int32_t per_row;    // run length
+    uint32_t magic;     // floor(2^32 / per_row) + 1: i / per_row == umulhi(i, magic) for i < 2^16
+    int32_t a_base;     // layout slot of constraint 0's `a`
+    int32_t row_stride; // layout distance between runs
+    int32_t d;          // lb - la
+    int32_t rest_base;  // rest-length slot of constraint 0
+    int32_t lam_base;   // lambda slot of constraint 0, or -1 when the colour has zero compliance
+};
+
+// Static per-cloth description, device resident, written at registration.
+struct PxbClothDev {
+    float4* pos;            // [n_layout] xyz + inv_mass
+    float4* vel;            // [n_layout] xyz + (1 real particle, 0 ghost)
+    float4* prv;            // [n_layout] prev_position (start of the last substep)
+    const float* rest;      // [n_rest_pad]
+    float* lam_out;         // [n_lam] lambdas left by the last substep (written when requested)
+    const int32_t* anchor_of;   // [n_layout] anchor record index or -1
+    const int2* tether;         // [n_layout] (anchor layout slot or -1, max_length bits)
+    float* anchors;             // [n_anchors * 8] prev xyz, pad, world xyz, pad
+    const PxbSeg* segs;         // [n_segs]
+    int32_t n_segs;
+    int32_t n_colours;
+    int32_t colour_seg[PXB_MAX_COLOURS + 1]; // colour c = segs [colour_seg[c], colour_seg[c+1])
+    int32_t colour_is_bend[PXB_MAX_COLOURS];
+    int32_t n_layout;
+    int32_t n_real;
+    int32_t columns, rows, Q, S;
+    int32_t n_rest_pad;     // multiple of 4
+    int32_t n_lam;          // lambda slots (compliant colours only)
+    int32_t u_floats;       // floats of the union region (lambdas / velocity scratch)
+    int32_t n_anchors;
+    int32_t smem_bytes;     // dynamic shared memory this cloth needs
+    int32_t threads;        // block size this cloth runs with
+    int32_t aero_grid;      // triangles are exactly make_grid_cloth's (cloth_builder.h:200-207)
+    int32_t pad_;
+};
+
+// One anchor target pair as the device keeps it (ClothAnchor::prev_world_position /
+// world_position, cloth.h:152-159), 32 bytes.
+struct PxbAnchorRec {
+    float prev[3];
+    float pad0;
+    float world[3];
+    float pad1;
+};
+
+// Collider snapshot with its world-space derived quantities precomputed on the host by the
+// same formulas the reference evaluates per call (shape.h:160-188, obb.h:31-36).
+struct PxbPose {
+    float center[3];
+    float ax[3], ay[3], az[3];  // box axes
+    float ca[3], cb[3];         // capsule segment
+    float t1[3];                // capsule on-axis fallback normal (orthonormal_basis)
+};
+struct PxbDevCollider {
+    int32_t type;
+    int32_t enabled;
+    int32_t two_pose;       // swept Box / Capsule: probe both poses, keep the deeper
+    int32_t swept_sphere;
+    float radius;           // sphere radius or capsule radius
+    float he[3];
+    float sweep[3];
+    float bmin[3], bmax[3];
+    PxbPose pose[2];
+};
+
+// Per cloth, per step, computed on the host (the prologue of solve_cloth, cloth_solver.h:162-194).
+struct PxbClothStep {
+    float hs, inv_hs, damping_factor, max_velocity, max_velocity2;
+    float thickness, friction, air_drag, air_lift;
+    float base_accel[3];     // used when n_sources == 0
+    float gravity[3];        // world gravity (for the source field)
+    float gravity_scale;
+    float external_acceleration[3];
+    float wind[3];
+    float alpha[PXB_MAX_COLOURS];
+    int32_t steps, iters, aero;
+    int32_t col_begin, col_count, src_begin, src_count;
+    int32_t write_lambdas;
+};
+
+struct PxbFrameResult {
+    float bounds_min[3];
+    float bounds_max[3];
+    float max_speed;
+    float time;
+};
+
+static_assert(sizeof(PxbClothStep) == 184, "per-step record size is part of the staging contract");
+static_assert(sizeof(PxbDevCollider) == 236, "collider snapshot size is part of the staging contract");
+
+#endif  // PXB_INTERNAL_H

@@ -1,0 +1,36 @@
+// pxb_kernels.h -- launch entry points of the device kernels (host side).
+#ifndef PXB_KERNELS_H
+#define PXB_KERNELS_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/physxcoopa_b200.h"
+#include "pxb_internal.h"
+
+namespace pxb {
+
+// Dynamic shared memory a cloth CTA may use: the sm_100 per-block limit (227 KB) minus the
+// kernel's static shared memory and a margin.
+constexpr int kMaxDynamicSmem = 232448 - 4096;
+constexpr int kClothOwned = 4;      // particles per thread in the cloth kernel
+constexpr int kClothMaxThreads = 1024;
+
+cudaError_t launch_cloth_step(const PxbClothDev* cloths, const PxbClothStep* steps,
+                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
+                              int n_blocks, int threads, int smem_bytes, cudaStream_t stream);
+
+cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness,
+                                  const float* pts, int n, float* out, float* normals,
+                                  float* depths, int32_t* hits, cudaStream_t stream);
+
+// Gathers positions of the listed cloths from layout order into particle order, 3 floats per
+// particle, cloth after cloth starting at out_offsets[k] (floats).
+cudaError_t launch_gather_positions(const PxbClothDev* cloths, const int32_t* order,
+                                    const int64_t* out_offsets, int n_cloths, float* out,
+                                    cudaStream_t stream);
+
+}  // namespace pxb
+
+#endif  // PXB_KERNELS_H

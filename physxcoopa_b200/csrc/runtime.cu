@@ -1,0 +1,1134 @@
+// runtime.cu -- host runtime of the C-ABI (include/physxcoopa_b200.h): contexts, the cloth
+// registry, the per-step host prologue, launches and read-backs.
+//
+// The registry mirrors PhysicsWorld's cloth slots (add_cloth / remove_cloth, world.h:552-596):
+// generational ids, state resident on the device between steps. A cloth is accepted on the
+// device path when its constraint lists are exactly make_grid_cloth's (cloth_builder.h:81-219);
+// its colours are then expressed as affine segments over the class-permuted layout described in
+// pxb_internal.h, and every segment pair is checked against the reference lists before upload.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/physxcoopa_b200.h"
+#include "host_math.h"
+#include "pxb_internal.h"
+#include "pxb_kernels.h"
+#include "runtime_internal.h"
+
+using namespace pxb;
+
+// ------------------------------------------------------------------------------------------
+// Context helpers
+// ------------------------------------------------------------------------------------------
+
+pxb_status pxb_context::fail(pxb_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    error = buf;
+    return s;
+}
+
+pxb_status pxb_context::cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return PXB_OK;
+    return fail(e == cudaErrorMemoryAllocation ? PXB_ERR_OUT_OF_MEMORY : PXB_ERR_CUDA,
+                "%s: %s", what, cudaGetErrorString(e));
+}
+
+pxb_status pxb_context::grow(DevBuf& b, size_t bytes, const char* what) {
+    if (b.bytes >= bytes) return PXB_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    want = want + want / 2;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) return cuda(e, what);
+    b.bytes = want;
+    return PXB_OK;
+}
+
+pxb_status pxb_context::grow_pinned(size_t bytes) {
+    if (pinned_bytes >= bytes) return PXB_OK;
+    if (pinned) {
+        cudaEventSynchronize(staged);
+        cudaFreeHost(pinned);
+    }
+    pinned = nullptr;
+    pinned_bytes = 0;
+    size_t want = bytes + bytes / 2 + 4096;
+    cudaError_t e = cudaHostAlloc(&pinned, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda(e, "cudaHostAlloc(staging)");
+    pinned_bytes = want;
+    return PXB_OK;
+}
+
+ClothEntry* pxb_context::lookup(uint64_t id) {
+    const uint32_t index = static_cast<uint32_t>(id & 0xffffffffu);
+    const uint32_t gen = static_cast<uint32_t>(id >> 32);
+    if (index >= cloths.size()) return nullptr;
+    ClothEntry& e = cloths[index];
+    if (!e.alive || e.generation != gen) return nullptr;
+    return &e;
+}
+
+namespace {
+
+// ------------------------------------------------------------------------------------------
+// Grid recognition and colour segments
+// ------------------------------------------------------------------------------------------
+
+// Number of k >= 0 with 4k + c + need < cols.
+int count_k(int cols, int c, int need) {
+    const int top = cols - 1 - c - need;
+    return top < 0 ? 0 : top / 4 + 1;
+}
+
+struct ColourSpec {
+    bool bend;
+    std::vector<PxbSeg> segs;  // rest_base / lam_base filled later
+    int total() const {
+        int t = 0;
+        for (const PxbSeg& s : segs) t += s.count;
+        return t;
+    }
+};
+
+PxbSeg seg(int rows_n, int per_row, int a_base, int row_stride, int d) {
+    PxbSeg s{};
+    s.count = rows_n * per_row;
+    s.per_row = per_row;
+    s.a_base = a_base;
+    s.row_stride = row_stride;
+    s.d = d;
+    s.rest_base = 0;
+    s.lam_base = -1;
+    s.magic = per_row == 1 ? 0u
+                           : static_cast<uint32_t>((0x100000000ull / static_cast<uint64_t>(per_row)) + 1ull);
+    return s;
+}
+
+// Runs of contiguous layout slots covering the real x of a row: classes 0..3 in order, a run
+// continuing into the next class while the current class is full (count == Q).
+void class_runs(int cols, int Q, std::vector<std::pair<int, int>>& runs) {
+    runs.clear();
+    int c = 0;
+    while (c < 4) {
+        const int cnt = count_k(cols, c, 0);
+        if (cnt == 0) break;
+        int start = c, len = cnt;
+        while (c < 3 && count_k(cols, c, 0) == Q && count_k(cols, c + 1, 0) > 0) {
+            ++c;
+            len += count_k(cols, c, 0);
+        }
+        runs.push_back({start * Q, len});
+        ++c;
+    }
+}
+
+// The 16 colours of make_grid_cloth in its batch order (cloth_builder.h:128-194), as segments.
+void grid_colours(int cols, int rows, bool shear, int Q, int S, std::vector<ColourSpec>& out) {
+    out.clear();
+    std::vector<std::pair<int, int>> runs;
+    class_runs(cols, Q, runs);
+    auto H = [&](int p) {
+        ColourSpec cs{false, {}};
+        for (int c = p; c < 4; c += 2) {
+            const int cnt = count_k(cols, c, 1);
+            if (cnt > 0) cs.segs.push_back(seg(rows, cnt, c * Q, S, c < 3 ? Q : 1 - 3 * Q));
+        }
+        return cs;
+    };
+    auto V = [&](int p, int step, int need, int d, bool bend) {
+        ColourSpec cs{bend, {}};
+        const int top = rows - 1 - p - need;
+        const int nr = top < 0 ? 0 : top / step + 1;
+        if (nr > 0)
+            for (auto& r : runs) cs.segs.push_back(seg(nr, r.second, p * S + r.first, step * S, d));
+        return cs;
+    };
+    auto D1 = [&](int p) {  // "\" (x,y)-(x+1,y+1)
+        ColourSpec cs{false, {}};
+        for (int c = p; c < 4; c += 2) {
+            const int cnt = count_k(cols, c, 1);
+            if (cnt > 0) cs.segs.push_back(seg(rows - 1, cnt, c * Q, S, c < 3 ? S + Q : S + 1 - 3 * Q));
+        }
+        return cs;
+    };
+    auto D2 = [&](int p) {  // "/" (x+1,y)-(x,y+1)
+        ColourSpec cs{false, {}};
+        for (int c = p; c < 4; c += 2) {
+            const int cnt = count_k(cols, c, 1);
+            if (cnt == 0) continue;
+            if (c < 3) cs.segs.push_back(seg(rows - 1, cnt, (c + 1) * Q, S, S - Q));
+            else cs.segs.push_back(seg(rows - 1, cnt, 1, S, S + 3 * Q - 1));
+        }
+        return cs;
+    };
+    auto BH = [&](int ph) {
+        ColourSpec cs{true, {}};
+        const int cnt = count_k(cols, ph, 2);
+        if (cnt > 0) cs.segs.push_back(seg(rows, cnt, ph * Q, S, ph < 2 ? 2 * Q : 1 - 2 * Q));
+        return cs;
+    };
+    std::vector<ColourSpec> all;
+    all.push_back(H(0));
+    all.push_back(H(1));
+    all.push_back(V(0, 2, 1, S, false));
+    all.push_back(V(1, 2, 1, S, false));
+    if (shear) {
+        all.push_back(D1(0));
+        all.push_back(D1(1));
+        all.push_back(D2(0));
+        all.push_back(D2(1));
+    }
+    for (int ph = 0; ph < 4; ++ph) all.push_back(BH(ph));
+    for (int ph = 0; ph < 4; ++ph) all.push_back(V(ph, 4, 2, 2 * S, true));
+    for (auto& cs : all)
+        if (cs.total() > 0) out.push_back(std::move(cs));
+}
+
+int particle_of_slot(int l, int cols, int rows, int Q, int S) {
+    if (l < 0 || l >= rows * S) return -1;
+    const int y = l / S;
+    const int j = l - y * S;
+    const int cls = j / Q;
+    const int x = 4 * (j - cls * Q) + cls;
+    if (cls > 3 || x >= cols) return -1;
+    return y * cols + x;
+}
+
+int slot_of_particle(int i, int cols, int Q, int S) {
+    const int y = i / cols, x = i - y * cols;
+    return y * S + (x & 3) * Q + (x >> 2);
+}
+
+// Tries to express the cloth's lists as the grid colours; fills `out` and the slot -> reference
+// constraint map (stretch index, or n_stretch + bend index).
+bool recognise_grid(const pxb_cloth_desc* d, int Q, int S, std::vector<ColourSpec>& out,
+                    std::vector<int32_t>& rest_ref, std::vector<int32_t>& colour_batch) {
+    const int cols = static_cast<int>(d->columns), rows = static_cast<int>(d->rows);
+    for (int shear = 1; shear >= 0; --shear) {
+        std::vector<ColourSpec> cs;
+        grid_colours(cols, rows, shear != 0, Q, S, cs);
+        int n_str = 0, n_bend = 0;
+        for (auto& c : cs) (c.bend ? n_bend : n_str)++;
+        if (n_str != static_cast<int>(d->n_stretch_batches) || n_bend != static_cast<int>(d->n_bend_batches))
+            continue;
+        bool ok = true;
+        std::vector<int32_t> by_a(d->n_particles, -1);
+        std::vector<int32_t> refs;
+        std::vector<int32_t> cb;
+        int si = 0, bi = 0;
+        for (auto& c : cs) {
+            const pxb_batch bt = c.bend ? d->bend_batches[bi] : d->stretch_batches[si];
+            const pxb_constraint* list = c.bend ? d->bend : d->stretch;
+            const uint32_t n_list = c.bend ? d->n_bend : d->n_stretch;
+            cb.push_back(c.bend ? bi : si);
+            if (c.bend) ++bi; else ++si;
+            if (bt.begin > bt.end || bt.end > n_list ||
+                static_cast<int>(bt.end - bt.begin) != c.total()) { ok = false; break; }
+            for (uint32_t k = bt.begin; k < bt.end; ++k) by_a[list[k].a] = static_cast<int32_t>(k);
+            for (const PxbSeg& s : c.segs) {
+                for (int i = 0; i < s.count && ok; ++i) {
+                    const int r = i / s.per_row, k = i - r * s.per_row;
+                    const int la = s.a_base + r * s.row_stride + k, lb = la + s.d;
+                    const int pa = particle_of_slot(la, cols, rows, Q, S), pb = particle_of_slot(lb, cols, rows, Q, S);
+                    if (pa < 0 || pb < 0) { ok = false; break; }
+                    const int32_t ref = by_a[pa];
+                    if (ref < static_cast<int32_t>(bt.begin) || ref >= static_cast<int32_t>(bt.end) ||
+                        list[ref].b != static_cast<uint32_t>(pb)) { ok = false; break; }
+                    refs.push_back(c.bend ? static_cast<int32_t>(d->n_stretch) + ref : ref);
+                }
+            }
+            for (uint32_t k = bt.begin; k < bt.end; ++k) by_a[list[k].a] = -1;
+            if (!ok) break;
+        }
+        if (!ok) continue;
+        out = std::move(cs);
+        rest_ref = std::move(refs);
+        colour_batch = std::move(cb);
+        return true;
+    }
+    return false;
+}
+
+bool grid_triangles(const pxb_cloth_desc* d) {
+    const uint32_t cols = d->columns, rows = d->rows;
+    if (d->n_triangle_indices != (cols - 1) * (rows - 1) * 6) return false;
+    size_t t = 0;
+    for (uint32_t y = 0; y + 1 < rows; ++y) {
+        for (uint32_t x = 0; x + 1 < cols; ++x) {
+            const uint32_t i00 = y * cols + x, i10 = i00 + 1, i01 = i00 + cols, i11 = i01 + 1;
+            const uint32_t want[6] = {i00, i10, i11, i00, i11, i01};
+            for (int k = 0; k < 6; ++k)
+                if (d->triangles[t++] != want[k]) return false;
+        }
+    }
+    return true;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+// Compliance of colour `c` of entry `e` (per-batch override, else the params value).
+float colour_compliance(const ClothEntry& e, int c) {
+    const bool bend = e.colour_is_bend[c] != 0;
+    const int b = e.colour_batch[c];
+    if (bend) return e.bend_batch_comp.empty() ? e.params.bend_compliance : e.bend_batch_comp[b];
+    return e.stretch_batch_comp.empty() ? e.params.stretch_compliance : e.stretch_batch_comp[b];
+}
+
+}  // namespace
+
+// Re-derives everything that depends on params: lambda slots, union region, shared memory.
+void pxb_context::refresh_layout(ClothEntry& e) {
+    int lam = 0;
+    for (int c = 0; c < e.n_colours; ++c) {
+        const bool has_lam = colour_compliance(e, c) != 0.0f;
+        for (int s = e.colour_seg[c]; s < e.colour_seg[c + 1]; ++s) {
+            e.segs[s].lam_base = has_lam ? lam : -1;
+            if (has_lam) lam += e.segs[s].count;
+        }
+    }
+    e.n_lam = lam;
+    const bool aero = (e.params.air_drag > 0.0f || e.params.air_lift > 0.0f) && e.n_triangle_indices > 0;
+    const int u_floats = std::max(lam, (aero && e.aero_grid) ? 3 * e.n_layout : 0);
+    e.dev.n_lam = lam;
+    e.dev.u_floats = u_floats;
+    e.dev.smem_bytes = 16 * e.n_layout + 4 * e.n_rest_pad + 4 * ((u_floats + 3) & ~3);
+    registry_dirty = true;
+}
+
+pxb_status pxb_context::upload_segments(ClothEntry& e) {
+    return cuda(cudaMemcpyAsync(const_cast<PxbSeg*>(e.dev.segs), e.segs.data(),
+                                sizeof(PxbSeg) * e.segs.size(), cudaMemcpyHostToDevice, stream),
+                "upload segments");
+}
+
+pxb_status pxb_context::upload_particles(ClothEntry& e, const pxb_particle* particles) {
+    const int n = static_cast<int>(e.n_particles);
+    std::vector<float4> pos(e.n_layout, make_float4(0, 0, 0, 0)), vel(e.n_layout, make_float4(0, 0, 0, 0)),
+        prv(e.n_layout, make_float4(0, 0, 0, 0));
+    for (int i = 0; i < n; ++i) {
+        const int l = slot_of_particle(i, e.cols, e.Q, e.S);
+        const pxb_particle& p = particles[i];
+        pos[l] = make_float4(p.position[0], p.position[1], p.position[2], p.inv_mass);
+        vel[l] = make_float4(p.velocity[0], p.velocity[1], p.velocity[2], 1.0f);
+        prv[l] = make_float4(p.prev_position[0], p.prev_position[1], p.prev_position[2], 0.0f);
+    }
+    // Tether anchors must be pinned for the per-particle tether stage to equal the reference's
+    // list-order pass (cloth_solver.h:274-275 relies on the same fact).
+    for (const pxb_tether& t : e.tethers) {
+        if (particles[t.anchor].inv_mass != 0.0f && particles[t.particle].inv_mass != 0.0f)
+            return fail(PXB_ERR_UNSUPPORTED, "tether %u anchors to an unpinned particle %u", t.particle,
+                        t.anchor);
+    }
+    const size_t bytes = 16 * static_cast<size_t>(e.n_layout);
+    pxb_status s = cuda(cudaMemcpyAsync(e.dev.pos, pos.data(), bytes, cudaMemcpyHostToDevice, stream), "upload pos");
+    if (s) return s;
+    s = cuda(cudaMemcpyAsync(e.dev.vel, vel.data(), bytes, cudaMemcpyHostToDevice, stream), "upload vel");
+    if (s) return s;
+    s = cuda(cudaMemcpyAsync(e.dev.prv, prv.data(), bytes, cudaMemcpyHostToDevice, stream), "upload prv");
+    if (s) return s;
+    return cuda(cudaStreamSynchronize(stream), "upload particles");
+}
+
+pxb_status pxb_context::upload_anchor_records(ClothEntry& e) {
+    if (e.anchor_recs.empty()) return PXB_OK;
+    pxb_status s = cuda(cudaMemcpyAsync(e.dev.anchors, e.anchor_recs.data(),
+                                        sizeof(PxbAnchorRec) * e.anchor_recs.size(),
+                                        cudaMemcpyHostToDevice, stream),
+                        "upload anchors");
+    if (s) return s;
+    return cuda(cudaStreamSynchronize(stream), "upload anchors");
+}
+
+pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
+    if (!d || !id_out) return fail(PXB_ERR_INVALID_ARGUMENT, "null argument");
+    if (d->n_particles == 0 || !d->particles)
+        return fail(PXB_ERR_INVALID_ARGUMENT, "an empty cloth is refused (PhysicsWorld::add_cloth does the same)");
+    if (d->params.self_collision && d->params.self_distance > PXB_EPSILON)
+        return fail(PXB_ERR_UNSUPPORTED, "self-collision is not implemented on the device path");
+    const uint32_t n = d->n_particles;
+    auto chk_list = [&](const pxb_constraint* l, uint32_t cnt, const char* name) -> bool {
+        if (cnt && !l) return false;
+        for (uint32_t k = 0; k < cnt; ++k)
+            if (l[k].a >= n || l[k].b >= n) {
+                fail(PXB_ERR_INVALID_ARGUMENT, "%s[%u] indexes past the particles", name, k);
+                return false;
+            }
+        return true;
+    };
+    if (!chk_list(d->stretch, d->n_stretch, "stretch") || !chk_list(d->bend, d->n_bend, "bend"))
+        return PXB_ERR_INVALID_ARGUMENT;
+    if ((d->n_stretch_batches && !d->stretch_batches) || (d->n_bend_batches && !d->bend_batches) ||
+        (d->n_tethers && !d->tethers) || (d->n_anchors && !d->anchors) ||
+        (d->n_triangle_indices && !d->triangles))
+        return fail(PXB_ERR_INVALID_ARGUMENT, "null array with a nonzero count");
+    for (uint32_t k = 0; k < d->n_tethers; ++k)
+        if (d->tethers[k].particle >= n || d->tethers[k].anchor >= n)
+            return fail(PXB_ERR_INVALID_ARGUMENT, "tether %u indexes past the particles", k);
+    for (uint32_t k = 0; k < d->n_triangle_indices; ++k)
+        if (d->triangles[k] >= n) return fail(PXB_ERR_INVALID_ARGUMENT, "triangle index past the particles");
+    if (d->n_stretch_batches > PXB_MAX_COLOURS || d->n_bend_batches > PXB_MAX_COLOURS)
+        return fail(PXB_ERR_UNSUPPORTED, "more batches than the grid colouring has");
+
+    // --- grid recognition ---
+    if (d->columns < 2 || d->rows < 2 || d->columns * d->rows != n)
+        return fail(PXB_ERR_UNSUPPORTED, "only make_grid_cloth sheets run on the device path");
+    ClothEntry e;
+    e.cols = static_cast<int>(d->columns);
+    e.rows = static_cast<int>(d->rows);
+    e.Q = (e.cols + 3) / 4;
+    e.S = 4 * e.Q;
+    e.n_layout = e.rows * e.S;
+    e.n_particles = n;
+    std::vector<ColourSpec> cs;
+    std::vector<int32_t> rest_ref, colour_batch;
+    if (!recognise_grid(d, e.Q, e.S, cs, rest_ref, colour_batch))
+        return fail(PXB_ERR_UNSUPPORTED,
+                    "constraint lists are not make_grid_cloth's for a %ux%u grid; only those run on the device path",
+                    d->columns, d->rows);
+    if (d->n_triangle_indices > 0 && !grid_triangles(d))
+        return fail(PXB_ERR_UNSUPPORTED, "triangle list is not make_grid_cloth's");
+    e.aero_grid = d->n_triangle_indices > 0 ? 1 : 0;
+    e.n_triangle_indices = d->n_triangle_indices;
+
+    // --- colours -> segments, rest slots ---
+    e.n_colours = static_cast<int>(cs.size());
+    e.colour_seg.assign(e.n_colours + 1, 0);
+    e.colour_is_bend.assign(e.n_colours, 0);
+    e.colour_batch = colour_batch;
+    int rest = 0;
+    for (int c = 0; c < e.n_colours; ++c) {
+        e.colour_seg[c] = static_cast<int>(e.segs.size());
+        e.colour_is_bend[c] = cs[c].bend ? 1 : 0;
+        for (PxbSeg s : cs[c].segs) {
+            if (s.count >= 65536) return fail(PXB_ERR_TOO_LARGE, "a colour segment exceeds 65535 constraints");
+            s.rest_base = rest;
+            rest += s.count;
+            e.segs.push_back(s);
+        }
+    }
+    e.colour_seg[e.n_colours] = static_cast<int>(e.segs.size());
+    if (e.segs.size() > PXB_MAX_SEGS) return fail(PXB_ERR_TOO_LARGE, "too many colour segments");
+    e.n_rest_pad = (rest + 3) & ~3;
+    e.rest_ref = rest_ref;
+    e.n_stretch = d->n_stretch;
+    e.n_bend = d->n_bend;
+    e.n_stretch_batches = d->n_stretch_batches;
+    e.n_bend_batches = d->n_bend_batches;
+    if (d->stretch_batch_compliance)
+        e.stretch_batch_comp.assign(d->stretch_batch_compliance, d->stretch_batch_compliance + d->n_stretch_batches);
+    if (d->bend_batch_compliance)
+        e.bend_batch_comp.assign(d->bend_batch_compliance, d->bend_batch_compliance + d->n_bend_batches);
+    e.params = d->params;
+    e.time = d->time;
+    int max_colour = 0;
+    for (auto& c : cs) max_colour = std::max(max_colour, c.total());
+    e.threads = std::min(kClothMaxThreads, std::max(64, ((max_colour + 1) / 2 + 31) & ~31));
+    e.tethers.assign(d->tethers, d->tethers + d->n_tethers);
+    {
+        std::vector<int> per(n, 0);
+        for (const pxb_tether& t : e.tethers)
+            if (++per[t.particle] > 1)
+                return fail(PXB_ERR_UNSUPPORTED, "particle %u has more than one tether", t.particle);
+    }
+
+    // --- anchors: one device record per anchor; a particle follows its LAST anchor ---
+    e.anchors.assign(d->anchors, d->anchors + d->n_anchors);
+    e.anchor_recs.resize(e.anchors.size());
+    for (size_t a = 0; a < e.anchors.size(); ++a) {
+        PxbAnchorRec r{};
+        std::memcpy(r.prev, e.anchors[a].prev_world_position, 12);
+        std::memcpy(r.world, e.anchors[a].world_position, 12);
+        e.anchor_recs[a] = r;
+    }
+    std::vector<int32_t> anchor_of(e.n_layout, -1);
+    for (size_t a = 0; a < e.anchors.size(); ++a)
+        if (e.anchors[a].particle < n)
+            anchor_of[slot_of_particle(static_cast<int>(e.anchors[a].particle), e.cols, e.Q, e.S)] =
+                static_cast<int32_t>(a);
+    std::vector<int2> tether(e.n_layout, make_int2(-1, 0));
+    for (const pxb_tether& t : e.tethers) {
+        int ml;
+        std::memcpy(&ml, &t.max_length, 4);
+        tether[slot_of_particle(static_cast<int>(t.particle), e.cols, e.Q, e.S)] =
+            make_int2(slot_of_particle(static_cast<int>(t.anchor), e.cols, e.Q, e.S), ml);
+    }
+    std::vector<float> rest_h(e.n_rest_pad, 0.0f);
+    for (int s = 0; s < rest; ++s) {
+        const int32_t r = e.rest_ref[s];
+        rest_h[s] = r < static_cast<int32_t>(e.n_stretch) ? d->stretch[r].rest_length
+                                                          : d->bend[r - e.n_stretch].rest_length;
+    }
+    e.topology.resize(d->n_stretch + d->n_bend);
+    for (uint32_t k = 0; k < d->n_stretch; ++k) e.topology[k] = {d->stretch[k].a, d->stretch[k].b, d->stretch[k].rest_length};
+    for (uint32_t k = 0; k < d->n_bend; ++k) e.topology[d->n_stretch + k] = {d->bend[k].a, d->bend[k].b, d->bend[k].rest_length};
+
+    // --- device memory: one allocation, 256-byte aligned sub-buffers ---
+    const size_t L = static_cast<size_t>(e.n_layout);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256(std::max<size_t>(bytes, 16));
+        return o;
+    };
+    const size_t o_pos = take(16 * L), o_vel = take(16 * L), o_prv = take(16 * L);
+    const size_t o_rest = take(4 * static_cast<size_t>(e.n_rest_pad));
+    const size_t o_lam = take(4 * static_cast<size_t>(rest));
+    const size_t o_anc = take(4 * L), o_teth = take(8 * L);
+    const size_t o_recs = take(sizeof(PxbAnchorRec) * e.anchor_recs.size());
+    const size_t o_segs = take(sizeof(PxbSeg) * PXB_MAX_SEGS);
+    cudaError_t ce = cudaMalloc(&e.dmem, off);
+    if (ce != cudaSuccess) return cuda(ce, "cudaMalloc(cloth)");
+    e.dbytes = off;
+    char* base = static_cast<char*>(e.dmem);
+    std::memset(&e.dev, 0, sizeof(e.dev));
+    e.dev.pos = reinterpret_cast<float4*>(base + o_pos);
+    e.dev.vel = reinterpret_cast<float4*>(base + o_vel);
+    e.dev.prv = reinterpret_cast<float4*>(base + o_prv);
+    e.dev.rest = reinterpret_cast<const float*>(base + o_rest);
+    e.dev.lam_out = reinterpret_cast<float*>(base + o_lam);
+    e.dev.anchor_of = reinterpret_cast<const int32_t*>(base + o_anc);
+    e.dev.tether = reinterpret_cast<const int2*>(base + o_teth);
+    e.dev.anchors = reinterpret_cast<float*>(base + o_recs);
+    e.dev.segs = reinterpret_cast<const PxbSeg*>(base + o_segs);
+    e.dev.n_segs = static_cast<int32_t>(e.segs.size());
+    e.dev.n_colours = e.n_colours;
+    for (int c = 0; c <= e.n_colours; ++c) e.dev.colour_seg[c] = e.colour_seg[c];
+    for (int c = 0; c < e.n_colours; ++c) e.dev.colour_is_bend[c] = e.colour_is_bend[c];
+    e.dev.n_layout = e.n_layout;
+    e.dev.n_real = static_cast<int32_t>(n);
+    e.dev.columns = e.cols;
+    e.dev.rows = e.rows;
+    e.dev.Q = e.Q;
+    e.dev.S = e.S;
+    e.dev.n_rest_pad = e.n_rest_pad;
+    e.dev.n_anchors = static_cast<int32_t>(e.anchor_recs.size());
+    e.dev.threads = e.threads;
+    e.dev.aero_grid = e.aero_grid;
+    refresh_layout(e);
+    if (e.dev.smem_bytes > kMaxDynamicSmem) {
+        cudaFree(e.dmem);
+        return fail(PXB_ERR_TOO_LARGE, "cloth needs %d bytes of shared memory; the single-CTA path holds %d",
+                    e.dev.smem_bytes, kMaxDynamicSmem);
+    }
+    pxb_status st = PXB_OK;
+    auto up = [&](void* dst, const void* src, size_t bytes, const char* what) {
+        if (st || bytes == 0) return;
+        st = cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), what);
+    };
+    up(base + o_rest, rest_h.data(), 4 * rest_h.size(), "upload rest");
+    up(base + o_anc, anchor_of.data(), 4 * L, "upload anchor_of");
+    up(base + o_teth, tether.data(), 8 * L, "upload tethers");
+    if (!st) st = upload_segments(e);
+    if (!st) st = cuda(cudaMemsetAsync(base + o_lam, 0, 4 * static_cast<size_t>(rest), stream), "zero lambdas");
+    if (!st) st = upload_anchor_records(e);
+    if (!st) st = upload_particles(e, d->particles);
+    if (st) {
+        cudaFree(e.dmem);
+        return st;
+    }
+
+    // --- slot ---
+    uint32_t index = 0;
+    while (index < cloths.size() && cloths[index].alive) ++index;
+    if (index == cloths.size()) cloths.emplace_back();
+    e.generation = cloths[index].generation + 1;
+    e.alive = true;
+    cloths[index] = std::move(e);
+    registry_dirty = true;
+    *id_out = (static_cast<uint64_t>(cloths[index].generation) << 32) | index;
+    return PXB_OK;
+}
+
+pxb_status pxb_context::sync_registry() {
+    if (!registry_dirty) return PXB_OK;
+    std::vector<PxbClothDev> h(std::max<size_t>(cloths.size(), 1));
+    std::memset(h.data(), 0, sizeof(PxbClothDev) * h.size());
+    for (size_t i = 0; i < cloths.size(); ++i)
+        if (cloths[i].alive) h[i] = cloths[i].dev;
+    pxb_status s = grow(d_registry, sizeof(PxbClothDev) * h.size(), "registry");
+    if (s) return s;
+    // The registry may be read by an in-flight launch; order the update on the stream.
+    s = cuda(cudaMemcpyAsync(d_registry.p, h.data(), sizeof(PxbClothDev) * h.size(),
+                             cudaMemcpyHostToDevice, stream),
+             "upload registry");
+    if (s) return s;
+    s = cuda(cudaStreamSynchronize(stream), "upload registry");
+    if (s) return s;
+    registry_dirty = false;
+    return PXB_OK;
+}
+
+// Collider snapshot -> device record with the world-space quantities the reference derives
+// per call (collision::world_sphere / world_obb / world_capsule, shape.h:160-188).
+static void make_dev_collider(const pxb_collider& c, PxbDevCollider& o) {
+    using namespace pxb::hm;
+    std::memset(&o, 0, sizeof(o));
+    o.type = c.type;
+    o.enabled = c.enabled;
+    const V3 sweep = ld(c.sweep);
+    const bool swept = dot(sweep, sweep) > 1e-6f * 1e-6f;
+    o.two_pose = swept && (c.type == PXB_SHAPE_BOX || c.type == PXB_SHAPE_CAPSULE) ? 1 : 0;
+    o.swept_sphere = swept && c.type == PXB_SHAPE_SPHERE ? 1 : 0;
+    o.radius = c.type == PXB_SHAPE_SPHERE ? c.radius : c.capsule_radius;
+    std::memcpy(o.he, c.half_extents, 12);
+    std::memcpy(o.sweep, c.sweep, 12);
+    std::memcpy(o.bmin, c.bounds_min, 12);
+    std::memcpy(o.bmax, c.bounds_max, 12);
+    const V3 lc = ld(c.local_center);
+    const Q4 lr = ldq(c.local_rotation);
+    for (int pose = 0; pose < (o.two_pose ? 2 : 1); ++pose) {
+        const V3 pp = pose == 0 ? ld(c.position) : add(ld(c.position), sweep);
+        const Q4 rot = pose == 0 ? ldq(c.orientation) : ldq(c.end_orientation);
+        PxbPose& ps = o.pose[pose];
+        const V3 center = add(pp, qrot(rot, lc));
+        st(ps.center, center);
+        const Q4 orient = qmul(rot, lr);
+        V3 ax, ay, az;
+        axes(orient, ax, ay, az);
+        st(ps.ax, ax);
+        st(ps.ay, ay);
+        st(ps.az, az);
+        if (c.type == PXB_SHAPE_CAPSULE) {
+            V3 axis_local{0.0f, 0.0f, 0.0f};
+            if (c.capsule_axis == 0) axis_local.x = 1.0f;
+            else if (c.capsule_axis == 1) axis_local.y = 1.0f;
+            else axis_local.z = 1.0f;
+            const V3 axis_world = qrot(orient, axis_local);
+            const V3 ca = sub(center, mul(axis_world, c.capsule_half_height));
+            const V3 cb = add(center, mul(axis_world, c.capsule_half_height));
+            st(ps.ca, ca);
+            st(ps.cb, cb);
+            st(ps.t1, orthonormal_t1(safe_normalize(sub(cb, ca))));
+        } else if (c.type == PXB_SHAPE_SPHERE) {
+            st(ps.cb, add(center, sweep));
+        }
+    }
+}
+
+static pxb_status check_colliders(pxb_context* ctx, const pxb_collider* c, uint32_t n) {
+    for (uint32_t k = 0; k < n; ++k) {
+        if (!c[k].enabled) continue;
+        if (c[k].type == PXB_SHAPE_TRIANGLE_MESH || c[k].type == PXB_SHAPE_CONVEX_HULL)
+            return ctx->fail(PXB_ERR_UNSUPPORTED, "mesh and convex-hull colliders are not implemented on the device path");
+        if (c[k].type < 0 || c[k].type > PXB_SHAPE_CONVEX_HULL)
+            return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "collider %u has an unknown shape type", k);
+        if (c[k].type == PXB_SHAPE_CAPSULE && (c[k].capsule_axis < 0 || c[k].capsule_axis > 2))
+            return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "collider %u has capsule_axis outside 0..2", k);
+    }
+    return PXB_OK;
+}
+
+pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
+    if (!sd || (sd->n_cloths && !sd->cloths)) return fail(PXB_ERR_INVALID_ARGUMENT, "null step");
+    const uint32_t n = sd->n_cloths;
+    if (n == 0) return PXB_OK;
+    if (!(sd->h > 0.0f)) return PXB_OK;  // solve_cloth is a no-op for h <= 0 (cloth_solver.h:163)
+    std::vector<ClothEntry*> ents(n);
+    uint32_t n_col = 0, n_src = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        ents[k] = lookup(sd->cloths[k]);
+        if (!ents[k]) return fail(PXB_ERR_INVALID_HANDLE, "cloth id %llu is not live", (unsigned long long)sd->cloths[k]);
+        if (ents[k]->params.self_collision && ents[k]->params.self_distance > PXB_EPSILON)
+            return fail(PXB_ERR_UNSUPPORTED, "self-collision is not implemented on the device path");
+        if (sd->collider_offsets) {
+            if (sd->collider_offsets[k + 1] < sd->collider_offsets[k])
+                return fail(PXB_ERR_INVALID_ARGUMENT, "collider offsets decrease");
+        }
+        if (sd->source_offsets && sd->source_offsets[k + 1] < sd->source_offsets[k])
+            return fail(PXB_ERR_INVALID_ARGUMENT, "source offsets decrease");
+    }
+    if (sd->collider_offsets) n_col = sd->collider_offsets[n];
+    if (sd->source_offsets) n_src = sd->source_offsets[n];
+    if (n_col && !sd->colliders) return fail(PXB_ERR_INVALID_ARGUMENT, "null colliders");
+    if (n_src && !sd->sources) return fail(PXB_ERR_INVALID_ARGUMENT, "null sources");
+    if (pxb_status s = check_colliders(this, sd->colliders, n_col)) return s;
+    if (pxb_status s = sync_registry()) return s;
+
+    // --- staging layout: steps | colliders | sources | order ---
+    const size_t b_steps = sizeof(PxbClothStep) * n;
+    const size_t b_cols = sizeof(PxbDevCollider) * std::max<uint32_t>(n_col, 1);
+    const size_t b_src = sizeof(pxb_gravity_source) * std::max<uint32_t>(n_src, 1);
+    const size_t b_order = sizeof(int32_t) * n;
+    const size_t o_cols = align256(b_steps), o_src = o_cols + align256(b_cols),
+                 o_order = o_src + align256(b_src), total = o_order + align256(b_order);
+    if (pxb_status s = grow_pinned(total)) return s;
+    if (pxb_status s = grow(d_stage, total, "step staging")) return s;
+    if (pxb_status s = grow(d_results, sizeof(PxbFrameResult) * n, "results")) return s;
+    cudaEventSynchronize(staged);  // the previous step's upload has left the pinned buffer
+    char* hb = static_cast<char*>(pinned);
+    auto* hs_steps = reinterpret_cast<PxbClothStep*>(hb);
+    auto* hs_cols = reinterpret_cast<PxbDevCollider*>(hb + o_cols);
+    auto* hs_src = reinterpret_cast<pxb_gravity_source*>(hb + o_src);
+    auto* hs_order = reinterpret_cast<int32_t*>(hb + o_order);
+    for (uint32_t k = 0; k < n_col; ++k) make_dev_collider(sd->colliders[k], hs_cols[k]);
+    if (n_src) std::memcpy(hs_src, sd->sources, sizeof(pxb_gravity_source) * n_src);
+    int threads = 64, smem = 0;
+    const pxb::hm::V3 g = pxb::hm::ld(sd->gravity);
+    for (uint32_t k = 0; k < n; ++k) {
+        ClothEntry& e = *ents[k];
+        const pxb_cloth_params& P = e.params;
+        PxbClothStep& s = hs_steps[k];
+        std::memset(&s, 0, sizeof(s));
+        // solve_cloth prologue (cloth_solver.h:165-194), evaluated exactly as the reference does
+        const uint32_t steps = std::max<uint32_t>(1, P.substeps ? P.substeps : sd->substeps);
+        const uint32_t iters = std::max<uint32_t>(1, P.iterations ? P.iterations : sd->iterations);
+        const float hs = sd->h / static_cast<float>(steps);
+        s.hs = hs;
+        s.inv_hs = 1.0f / hs;
+        s.steps = static_cast<int32_t>(steps);
+        s.iters = static_cast<int32_t>(iters);
+        for (int c = 0; c < e.n_colours; ++c) s.alpha[c] = colour_compliance(e, c) / (hs * hs);
+        pxb::hm::V3 wind = pxb::hm::ld(P.wind);
+        if (P.wind_turbulence > 0.0f) {
+            const float t = e.time;
+            const pxb::hm::V3 gust{std::sin(t * 1.7f) * std::cos(t * 0.9f),
+                                   std::sin(t * 1.1f + 1.3f) * std::cos(t * 1.9f),
+                                   std::sin(t * 0.7f + 2.7f) * std::cos(t * 1.3f)};
+            wind = pxb::hm::add(wind, pxb::hm::V3{P.wind_turbulence * gust.x, P.wind_turbulence * gust.y,
+                                                  P.wind_turbulence * gust.z});
+        }
+        pxb::hm::st(s.wind, wind);
+        const pxb::hm::V3 base = pxb::hm::add(pxb::hm::mul(g, P.gravity_scale), pxb::hm::ld(P.external_acceleration));
+        pxb::hm::st(s.base_accel, base);
+        pxb::hm::st(s.gravity, g);
+        s.gravity_scale = P.gravity_scale;
+        std::memcpy(s.external_acceleration, P.external_acceleration, 12);
+        s.aero = ((P.air_drag > 0.0f || P.air_lift > 0.0f) && e.n_triangle_indices > 0) ? 1 : 0;
+        s.air_drag = P.air_drag;
+        s.air_lift = P.air_lift;
+        s.max_velocity = P.max_velocity;
+        s.max_velocity2 = P.max_velocity * P.max_velocity;
+        s.damping_factor = 1.0f / (1.0f + P.damping * hs);
+        s.thickness = P.thickness;
+        s.friction = P.friction;
+        s.col_begin = sd->collider_offsets ? static_cast<int32_t>(sd->collider_offsets[k]) : 0;
+        s.col_count = sd->collider_offsets ? static_cast<int32_t>(sd->collider_offsets[k + 1] - sd->collider_offsets[k]) : 0;
+        s.src_begin = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k]) : 0;
+        s.src_count = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k + 1] - sd->source_offsets[k]) : 0;
+        s.write_lambdas = 1;
+        hs_order[k] = static_cast<int32_t>(ents[k] - cloths.data());
+        threads = std::max(threads, e.threads);
+        smem = std::max(smem, e.dev.smem_bytes);
+        // Cloth::time advances by hs per substep (cloth_solver.h:453), mirrored on the host.
+        for (uint32_t q = 0; q < steps; ++q) e.time += hs;
+        // Anchors reach their targets: next step lerps from here (cloth_solver.h:457).
+        for (PxbAnchorRec& r : e.anchor_recs) std::memcpy(r.prev, r.world, 12);
+        for (pxb_anchor& a : e.anchors) std::memcpy(a.prev_world_position, a.world_position, 12);
+    }
+    char* db = static_cast<char*>(d_stage.p);
+    if (pxb_status s = cuda(cudaMemcpyAsync(db, hb, total, cudaMemcpyHostToDevice, stream), "upload step")) return s;
+    cudaEventRecord(staged, stream);
+    cudaError_t le = launch_cloth_step(static_cast<const PxbClothDev*>(d_registry.p),
+                                       reinterpret_cast<const PxbClothStep*>(db),
+                                       reinterpret_cast<const PxbDevCollider*>(db + o_cols),
+                                       reinterpret_cast<const pxb_gravity_source*>(db + o_src),
+                                       reinterpret_cast<const int32_t*>(db + o_order),
+                                       static_cast<PxbFrameResult*>(d_results.p), d_err,
+                                       static_cast<int>(n), threads, smem, stream);
+    if (le != cudaSuccess) return cuda(le, "launch cloth_step");
+    ++launches;
+    last_step.assign(sd->cloths, sd->cloths + n);
+    results_fresh = false;
+    return PXB_OK;
+}
+
+pxb_status pxb_context::check_device_error() {
+    uint32_t h = 0;
+    pxb_status s = cuda(cudaMemcpyAsync(&h, d_err, 4, cudaMemcpyDeviceToHost, stream), "read error word");
+    if (s) return s;
+    s = cuda(cudaStreamSynchronize(stream), "synchronize");
+    if (s) return s;
+    if (h) {
+        cudaMemsetAsync(d_err, 0, 4, stream);
+        return fail(PXB_ERR_DEVICE_STATUS, "device error word 0x%x (1 bad index, 2 staging wait expired, 4 queue wait expired)", h);
+    }
+    return PXB_OK;
+}
+
+pxb_status pxb_context::fetch_results() {
+    if (results_fresh) return PXB_OK;
+    const size_t n = last_step.size();
+    std::vector<PxbFrameResult> h(n);
+    if (n) {
+        pxb_status s = cuda(cudaMemcpyAsync(h.data(), d_results.p, sizeof(PxbFrameResult) * n,
+                                            cudaMemcpyDeviceToHost, stream),
+                            "read results");
+        if (s) return s;
+    }
+    if (pxb_status s = check_device_error()) return s;
+    for (size_t k = 0; k < n; ++k) {
+        ClothEntry* e = lookup(last_step[k]);
+        if (!e) continue;
+        e->result = h[k];
+        e->result.time = e->time;
+        e->has_result = true;
+    }
+    results_fresh = true;
+    return PXB_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// C-ABI
+// ------------------------------------------------------------------------------------------
+
+extern "C" {
+
+pxb_status pxb_context_create(int device, pxb_context** out) {
+    if (!out) return PXB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    auto* ctx = new (std::nothrow) pxb_context();
+    if (!ctx) return PXB_ERR_OUT_OF_MEMORY;
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->staged, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_err, 4);
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, 4);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return e == cudaErrorMemoryAllocation ? PXB_ERR_OUT_OF_MEMORY : PXB_ERR_CUDA;
+    }
+    *out = ctx;
+    return PXB_OK;
+}
+
+pxb_status pxb_context_destroy(pxb_context* ctx) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+    return PXB_OK;
+}
+
+const char* pxb_last_error(const pxb_context* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+pxb_status pxb_context_stream(pxb_context* ctx, void** stream_out) {
+    if (!ctx || !stream_out) return PXB_ERR_INVALID_ARGUMENT;
+    *stream_out = ctx->stream;
+    return PXB_OK;
+}
+
+pxb_status pxb_context_synchronize(pxb_context* ctx) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    return ctx->check_device_error();
+}
+
+uint64_t pxb_context_launch_count(const pxb_context* ctx) { return ctx ? ctx->launches : 0; }
+
+pxb_status pxb_cloth_add(pxb_context* ctx, const pxb_cloth_desc* desc, uint64_t* id_out) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    return ctx->add_cloth(desc, id_out);
+}
+
+pxb_status pxb_cloth_remove(pxb_context* ctx, uint64_t id) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry* e = ctx->lookup(id);
+    if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(e->dmem);
+    const uint32_t gen = e->generation;
+    *e = ClothEntry();
+    e->generation = gen;
+    e->alive = false;
+    ctx->registry_dirty = true;
+    ctx->results_fresh = false;
+    ctx->last_step.clear();
+    return PXB_OK;
+}
+
+pxb_status pxb_cloth_set_params(pxb_context* ctx, uint64_t id, const pxb_cloth_params* params) {
+    if (!ctx || !params) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry* e = ctx->lookup(id);
+    if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+    if (params->self_collision && params->self_distance > PXB_EPSILON)
+        return ctx->fail(PXB_ERR_UNSUPPORTED, "self-collision is not implemented on the device path");
+    const pxb_cloth_params old = e->params;
+    e->params = *params;
+    ctx->refresh_layout(*e);
+    if (e->dev.smem_bytes > kMaxDynamicSmem) {
+        e->params = old;
+        ctx->refresh_layout(*e);
+        return ctx->fail(PXB_ERR_TOO_LARGE, "these params need more shared memory than the path holds");
+    }
+    if (pxb_status s = ctx->upload_segments(*e)) return s;
+    return ctx->cuda(cudaStreamSynchronize(ctx->stream), "set params");
+}
+
+pxb_status pxb_cloth_write_particles(pxb_context* ctx, uint64_t id, const pxb_particle* particles, uint32_t n) {
+    if (!ctx || !particles) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry* e = ctx->lookup(id);
+    if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+    if (n != e->n_particles) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "particle count mismatch");
+    return ctx->upload_particles(*e, particles);
+}
+
+pxb_status pxb_cloth_read_particles(pxb_context* ctx, uint64_t id, pxb_particle* out, uint32_t n) {
+    if (!ctx || !out) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry* e = ctx->lookup(id);
+    if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+    if (n != e->n_particles) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "particle count mismatch");
+    const size_t L = static_cast<size_t>(e->n_layout);
+    std::vector<float4> pos(L), vel(L), prv(L);
+    pxb_status s = ctx->cuda(cudaMemcpyAsync(pos.data(), e->dev.pos, 16 * L, cudaMemcpyDeviceToHost, ctx->stream), "read pos");
+    if (!s) s = ctx->cuda(cudaMemcpyAsync(vel.data(), e->dev.vel, 16 * L, cudaMemcpyDeviceToHost, ctx->stream), "read vel");
+    if (!s) s = ctx->cuda(cudaMemcpyAsync(prv.data(), e->dev.prv, 16 * L, cudaMemcpyDeviceToHost, ctx->stream), "read prv");
+    if (!s) s = ctx->check_device_error();
+    if (s) return s;
+    for (uint32_t i = 0; i < n; ++i) {
+        const int l = slot_of_particle(static_cast<int>(i), e->cols, e->Q, e->S);
+        pxb_particle& p = out[i];
+        p.position[0] = pos[l].x; p.position[1] = pos[l].y; p.position[2] = pos[l].z;
+        p.inv_mass = pos[l].w;
+        p.velocity[0] = vel[l].x; p.velocity[1] = vel[l].y; p.velocity[2] = vel[l].z;
+        p.prev_position[0] = prv[l].x; p.prev_position[1] = prv[l].y; p.prev_position[2] = prv[l].z;
+    }
+    return PXB_OK;
+}
+
+pxb_status pxb_cloth_read_lambdas(pxb_context* ctx, uint64_t id, float* stretch_out, uint32_t n_stretch,
+                                  float* bend_out, uint32_t n_bend) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry* e = ctx->lookup(id);
+    if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+    if ((stretch_out && n_stretch != e->n_stretch) || (bend_out && n_bend != e->n_bend))
+        return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "lambda count mismatch");
+    std::vector<float> lam(std::max(e->n_lam, 1));
+    pxb_status s = PXB_OK;
+    if (e->n_lam)
+        s = ctx->cuda(cudaMemcpyAsync(lam.data(), e->dev.lam_out, 4 * static_cast<size_t>(e->n_lam),
+                                      cudaMemcpyDeviceToHost, ctx->stream), "read lambdas");
+    if (!s) s = ctx->check_device_error();
+    if (s) return s;
+    if (stretch_out) std::fill(stretch_out, stretch_out + n_stretch, 0.0f);
+    if (bend_out) std::fill(bend_out, bend_out + n_bend, 0.0f);
+    for (int c = 0; c < e->n_colours; ++c) {
+        for (int sg = e->colour_seg[c]; sg < e->colour_seg[c + 1]; ++sg) {
+            const PxbSeg& g = e->segs[sg];
+            if (g.lam_base < 0) continue;
+            for (int i = 0; i < g.count; ++i) {
+                const int32_t r = e->rest_ref[g.rest_base + i];
+                const float v = lam[g.lam_base + i];
+                if (r < static_cast<int32_t>(e->n_stretch)) { if (stretch_out) stretch_out[r] = v; }
+                else if (bend_out) bend_out[r - e->n_stretch] = v;
+            }
+        }
+    }
+    return PXB_OK;
+}
+
+pxb_status pxb_cloth_set_anchor_targets(pxb_context* ctx, uint64_t id, const float* world_xyz, uint32_t n) {
+    if (!ctx || (n && !world_xyz)) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry* e = ctx->lookup(id);
+    if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+    if (n != e->anchors.size()) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "anchor count mismatch");
+    for (uint32_t a = 0; a < n; ++a) {
+        std::memcpy(e->anchor_recs[a].world, world_xyz + 3 * a, 12);
+        std::memcpy(e->anchors[a].world_position, world_xyz + 3 * a, 12);
+    }
+    return ctx->upload_anchor_records(*e);
+}
+
+pxb_status pxb_cloth_read_anchors(pxb_context* ctx, uint64_t id, pxb_anchor* out, uint32_t n) {
+    if (!ctx || (n && !out)) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry* e = ctx->lookup(id);
+    if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+    if (n != e->anchors.size()) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "anchor count mismatch");
+    if (n) std::memcpy(out, e->anchors.data(), sizeof(pxb_anchor) * n);
+    return PXB_OK;
+}
+
+pxb_status pxb_cloth_read_time(pxb_context* ctx, uint64_t id, float* time_out) {
+    if (!ctx || !time_out) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry* e = ctx->lookup(id);
+    if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+    *time_out = e->time;
+    return PXB_OK;
+}
+
+pxb_status pxb_cloths_step(pxb_context* ctx, const pxb_cloth_step_desc* step) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    return ctx->step_cloths(step);
+}
+
+pxb_status pxb_cloths_read_results(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
+                                   pxb_cloth_frame_result* out) {
+    if (!ctx || (n && (!cloths || !out))) return PXB_ERR_INVALID_ARGUMENT;
+    if (pxb_status s = ctx->fetch_results()) return s;
+    for (uint32_t k = 0; k < n; ++k) {
+        ClothEntry* e = ctx->lookup(cloths[k]);
+        if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+        if (!e->has_result) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "cloth has not been stepped");
+        static_assert(sizeof(pxb_cloth_frame_result) == sizeof(PxbFrameResult), "result layout");
+        std::memcpy(&out[k], &e->result, sizeof(PxbFrameResult));
+    }
+    return PXB_OK;
+}
+
+pxb_status pxb_cloths_read_positions(pxb_context* ctx, const uint64_t* cloths, uint32_t n, float* out,
+                                     size_t capacity) {
+    if (!ctx || (n && (!cloths || !out))) return PXB_ERR_INVALID_ARGUMENT;
+    std::vector<int32_t> order(n);
+    std::vector<int64_t> offs(n);
+    int64_t total = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        ClothEntry* e = ctx->lookup(cloths[k]);
+        if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+        order[k] = static_cast<int32_t>(e - ctx->cloths.data());
+        offs[k] = total;
+        total += 3 * static_cast<int64_t>(e->n_particles);
+    }
+    if (static_cast<size_t>(total) > capacity) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "output too small");
+    if (n == 0) return PXB_OK;
+    if (pxb_status s = ctx->sync_registry()) return s;
+    if (pxb_status s = ctx->grow(ctx->d_gather_meta, 16 * static_cast<size_t>(n), "gather meta")) return s;
+    if (pxb_status s = ctx->grow(ctx->d_gather, 4 * static_cast<size_t>(total), "gather")) return s;
+    char* meta = static_cast<char*>(ctx->d_gather_meta.p);
+    pxb_status s = ctx->cuda(cudaMemcpyAsync(meta, order.data(), 4 * n, cudaMemcpyHostToDevice, ctx->stream), "gather order");
+    if (!s) s = ctx->cuda(cudaMemcpyAsync(meta + align256(4 * n), offs.data(), 8 * n, cudaMemcpyHostToDevice, ctx->stream), "gather offsets");
+    if (s) return s;
+    if (ctx->d_gather_meta.bytes < align256(4 * n) + 8 * n) {
+        if ((s = ctx->grow(ctx->d_gather_meta, align256(4 * n) + 8 * n, "gather meta"))) return s;
+        return pxb_cloths_read_positions(ctx, cloths, n, out, capacity);
+    }
+    cudaError_t le = launch_gather_positions(static_cast<const PxbClothDev*>(ctx->d_registry.p),
+                                             reinterpret_cast<const int32_t*>(meta),
+                                             reinterpret_cast<const int64_t*>(meta + align256(4 * n)),
+                                             static_cast<int>(n), static_cast<float*>(ctx->d_gather.p),
+                                             ctx->stream);
+    if (le != cudaSuccess) return ctx->cuda(le, "launch gather");
+    s = ctx->cuda(cudaMemcpyAsync(out, ctx->d_gather.p, 4 * static_cast<size_t>(total), cudaMemcpyDeviceToHost,
+                                  ctx->stream), "read positions");
+    if (s) return s;
+    return ctx->check_device_error();
+}
+
+pxb_status pxb_project_particles(pxb_context* ctx, const pxb_collider* collider, float thickness,
+                                 const float* points_xyz, const float* motion_start_xyz, uint32_t n,
+                                 float* points_out, float* normals_out, float* depths_out, int32_t* hit_out) {
+    (void)motion_start_xyz;  // consumed only by the TriangleMesh branch, which is refused
+    if (!ctx || !collider || (n && (!points_xyz || !points_out || !normals_out || !depths_out || !hit_out)))
+        return PXB_ERR_INVALID_ARGUMENT;
+    if (pxb_status s = check_colliders(ctx, collider, 1)) return s;
+    PxbDevCollider dc;
+    make_dev_collider(*collider, dc);
+    const size_t o_pts = align256(sizeof(dc)), o_out = o_pts + align256(12 * static_cast<size_t>(n)),
+                 o_nrm = o_out + align256(12 * static_cast<size_t>(n)),
+                 o_dep = o_nrm + align256(12 * static_cast<size_t>(n)),
+                 o_hit = o_dep + align256(4 * static_cast<size_t>(n)), total = o_hit + align256(4 * static_cast<size_t>(n));
+    if (pxb_status s = ctx->grow(ctx->d_scratch, total, "projection scratch")) return s;
+    char* b = static_cast<char*>(ctx->d_scratch.p);
+    pxb_status s = ctx->cuda(cudaMemcpyAsync(b, &dc, sizeof(dc), cudaMemcpyHostToDevice, ctx->stream), "upload collider");
+    if (!s && n) s = ctx->cuda(cudaMemcpyAsync(b + o_pts, points_xyz, 12 * static_cast<size_t>(n), cudaMemcpyHostToDevice, ctx->stream), "upload points");
+    if (s) return s;
+    cudaError_t le = launch_project_points(reinterpret_cast<const PxbDevCollider*>(b), thickness,
+                                           reinterpret_cast<const float*>(b + o_pts), static_cast<int>(n),
+                                           reinterpret_cast<float*>(b + o_out), reinterpret_cast<float*>(b + o_nrm),
+                                           reinterpret_cast<float*>(b + o_dep), reinterpret_cast<int32_t*>(b + o_hit),
+                                           ctx->stream);
+    if (le != cudaSuccess) return ctx->cuda(le, "launch projection");
+    ++ctx->launches;
+    if (n) {
+        s = ctx->cuda(cudaMemcpyAsync(points_out, b + o_out, 12 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, ctx->stream), "read points");
+        if (!s) s = ctx->cuda(cudaMemcpyAsync(normals_out, b + o_nrm, 12 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, ctx->stream), "read normals");
+        if (!s) s = ctx->cuda(cudaMemcpyAsync(depths_out, b + o_dep, 4 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, ctx->stream), "read depths");
+        if (!s) s = ctx->cuda(cudaMemcpyAsync(hit_out, b + o_hit, 4 * static_cast<size_t>(n), cudaMemcpyDeviceToHost, ctx->stream), "read hits");
+        if (s) return s;
+    }
+    return ctx->check_device_error();
+}
+
+pxb_status pxb_solve_cloth_host(pxb_context* ctx, const pxb_cloth_desc* desc, pxb_particle* particles,
+                                pxb_constraint* stretch, pxb_constraint* bend, pxb_anchor* anchors,
+                                const pxb_collider* colliders, uint32_t n_colliders, const float gravity[3],
+                                uint32_t substeps, uint32_t iterations, float h, float* time_inout,
+                                float* bounds_out) {
+    if (!ctx || !desc || !gravity) return PXB_ERR_INVALID_ARGUMENT;
+    if (desc->n_particles == 0 || !(h > 0.0f)) return PXB_OK;  // solve_cloth no-ops (cloth_solver.h:163)
+    // Reuse the registration made for these arrays when the topology is unchanged.
+    HostSolveCache* hit = nullptr;
+    for (HostSolveCache& c : ctx->host_cache) {
+        if (c.particles != desc->particles || !ctx->lookup(c.id)) continue;
+        ClothEntry* e = ctx->lookup(c.id);
+        bool same = e->n_particles == desc->n_particles && e->n_stretch == desc->n_stretch &&
+                    e->n_bend == desc->n_bend && e->anchors.size() == desc->n_anchors &&
+                    e->tethers.size() == desc->n_tethers;
+        for (uint32_t k = 0; same && k < desc->n_stretch; ++k)
+            same = e->topology[k].a == desc->stretch[k].a && e->topology[k].b == desc->stretch[k].b &&
+                   e->topology[k].rest == desc->stretch[k].rest_length;
+        for (uint32_t k = 0; same && k < desc->n_bend; ++k)
+            same = e->topology[desc->n_stretch + k].a == desc->bend[k].a &&
+                   e->topology[desc->n_stretch + k].b == desc->bend[k].b &&
+                   e->topology[desc->n_stretch + k].rest == desc->bend[k].rest_length;
+        for (uint32_t k = 0; same && k < desc->n_tethers; ++k)
+            same = std::memcmp(&e->tethers[k], &desc->tethers[k], sizeof(pxb_tether)) == 0;
+        if (same) { hit = &c; break; }
+        pxb_cloth_remove(ctx, c.id);
+        c.particles = nullptr;
+    }
+    uint64_t id = 0;
+    pxb_status s = PXB_OK;
+    if (!hit) {
+        if ((s = ctx->add_cloth(desc, &id))) return s;
+        ctx->host_cache.push_back(HostSolveCache{desc->particles, id});
+    } else {
+        id = hit->id;
+        ClothEntry* e = ctx->lookup(id);
+        e->params = desc->params;
+        ctx->refresh_layout(*e);
+        if (e->dev.smem_bytes > kMaxDynamicSmem) return ctx->fail(PXB_ERR_TOO_LARGE, "params need too much shared memory");
+        if ((s = ctx->upload_segments(*e))) return s;
+        if ((s = ctx->upload_particles(*e, desc->particles))) return s;
+        for (uint32_t a = 0; a < desc->n_anchors; ++a) {
+            e->anchors[a] = desc->anchors[a];
+            std::memcpy(e->anchor_recs[a].prev, desc->anchors[a].prev_world_position, 12);
+            std::memcpy(e->anchor_recs[a].world, desc->anchors[a].world_position, 12);
+        }
+        if ((s = ctx->upload_anchor_records(*e))) return s;
+        e->time = desc->time;
+    }
+    ClothEntry* e = ctx->lookup(id);
+    if (time_inout) e->time = *time_inout;
+    std::vector<uint32_t> offs = {0, n_colliders};
+    pxb_cloth_step_desc sd{};
+    sd.cloths = &id;
+    sd.n_cloths = 1;
+    sd.colliders = colliders;
+    sd.collider_offsets = offs.data();
+    std::memcpy(sd.gravity, gravity, 12);
+    sd.substeps = substeps;
+    sd.iterations = iterations;
+    sd.h = h;
+    if ((s = ctx->step_cloths(&sd))) return s;
+    if ((s = pxb_cloth_read_particles(ctx, id, particles, desc->n_particles))) return s;
+    if (stretch || bend) {
+        std::vector<float> ls(desc->n_stretch), lb(desc->n_bend);
+        if ((s = pxb_cloth_read_lambdas(ctx, id, ls.data(), desc->n_stretch, lb.data(), desc->n_bend))) return s;
+        if (stretch) for (uint32_t k = 0; k < desc->n_stretch; ++k) stretch[k].lambda = ls[k];
+        if (bend) for (uint32_t k = 0; k < desc->n_bend; ++k) bend[k].lambda = lb[k];
+    }
+    if (anchors) for (uint32_t a = 0; a < desc->n_anchors; ++a) std::memcpy(anchors[a].prev_world_position, anchors[a].world_position, 12);
+    if (time_inout) *time_inout = e->time;
+    if (bounds_out) {
+        pxb_cloth_frame_result r;
+        if ((s = pxb_cloths_read_results(ctx, &id, 1, &r))) return s;
+        std::memcpy(bounds_out, r.bounds_min, 12);
+        std::memcpy(bounds_out + 3, r.bounds_max, 12);
+    }
+    return PXB_OK;
+}
+
+}  // extern "C"

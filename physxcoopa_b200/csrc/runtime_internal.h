@@ -1,0 +1,105 @@
+// runtime_internal.h -- host-side state behind the C-ABI handles.
+#ifndef PXB_RUNTIME_INTERNAL_H
+#define PXB_RUNTIME_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/physxcoopa_b200.h"
+#include "pxb_internal.h"
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct TopologyEdge {
+    uint32_t a, b;
+    float rest;
+};
+
+// One registered cloth: host mirrors of what the reference keeps on the Cloth (params, time,
+// anchors, tethers) plus the device-side description and its allocation.
+struct ClothEntry {
+    bool alive = false;
+    uint32_t generation = 0;
+    uint32_t n_particles = 0;
+    int cols = 0, rows = 0, Q = 0, S = 0, n_layout = 0;
+    int n_colours = 0;
+    std::vector<PxbSeg> segs;
+    std::vector<int> colour_seg;
+    std::vector<int> colour_is_bend;
+    std::vector<int32_t> colour_batch;     // colour -> reference batch index in its list
+    std::vector<int32_t> rest_ref;         // rest slot -> stretch index, or n_stretch + bend index
+    int n_rest_pad = 0;
+    int n_lam = 0;
+    int threads = 64;
+    int aero_grid = 0;
+    uint32_t n_triangle_indices = 0;
+    uint32_t n_stretch = 0, n_bend = 0, n_stretch_batches = 0, n_bend_batches = 0;
+    std::vector<float> stretch_batch_comp, bend_batch_comp;
+    std::vector<TopologyEdge> topology;
+    std::vector<pxb_tether> tethers;
+    std::vector<pxb_anchor> anchors;
+    std::vector<PxbAnchorRec> anchor_recs;
+    pxb_cloth_params params{};
+    float time = 0.0f;
+    PxbClothDev dev{};
+    void* dmem = nullptr;
+    size_t dbytes = 0;
+    PxbFrameResult result{};
+    bool has_result = false;
+};
+
+// pxb_solve_cloth_host keeps the registration it made for a caller's arrays.
+struct HostSolveCache {
+    const pxb_particle* particles;
+    uint64_t id;
+};
+
+struct pxb_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t staged = nullptr;
+    uint32_t* d_err = nullptr;
+    std::string error;
+    uint64_t launches = 0;
+    std::vector<ClothEntry> cloths;
+    bool registry_dirty = true;
+    DevBuf d_registry, d_stage, d_results, d_gather, d_gather_meta, d_scratch;
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    std::vector<uint64_t> last_step;  // ids of the last step, in launch-slot order
+    bool results_fresh = false;
+    std::vector<HostSolveCache> host_cache;
+
+    ~pxb_context() {
+        for (ClothEntry& e : cloths)
+            if (e.alive && e.dmem) cudaFree(e.dmem);
+        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch})
+            if (b->p) cudaFree(b->p);
+        if (pinned) cudaFreeHost(pinned);
+        if (d_err) cudaFree(d_err);
+        if (staged) cudaEventDestroy(staged);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    pxb_status fail(pxb_status s, const char* fmt, ...);
+    pxb_status cuda(cudaError_t e, const char* what);
+    pxb_status grow(DevBuf& b, size_t bytes, const char* what);
+    pxb_status grow_pinned(size_t bytes);
+    ClothEntry* lookup(uint64_t id);
+    void refresh_layout(ClothEntry& e);
+    pxb_status upload_segments(ClothEntry& e);
+    pxb_status upload_particles(ClothEntry& e, const pxb_particle* particles);
+    pxb_status upload_anchor_records(ClothEntry& e);
+    pxb_status add_cloth(const pxb_cloth_desc* d, uint64_t* id_out);
+    pxb_status sync_registry();
+    pxb_status step_cloths(const pxb_cloth_step_desc* sd);
+    pxb_status check_device_error();
+    pxb_status fetch_results();
+};
+
+#endif  // PXB_RUNTIME_INTERNAL_H

@@ -1,0 +1,316 @@
+"""ctypes host over the C-ABI library (include/physxcoopa_b200.h).
+
+`Context` mirrors the reference's cloth entry points at PhysicsWorld granularity
+(add_cloth / remove_cloth / step, physxcoopa/world.h:552-596, 1749-1847) and the drop-in
+`solve_cloth` contract (physxcoopa/cloth/cloth_solver.h:158-467) on host arrays.
+`HostCloth` wraps the library's setup-time builders (make_grid_cloth / pin_static /
+build_tethers, physxcoopa/cloth/cloth_builder.h).
+
+There is no fallback: if the shared library is missing, loading raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi as A
+from .arrays import ClothArrays
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libphysxcoopa_b200.so")
+
+P = C.c_void_p
+u32 = C.c_uint32
+u64 = C.c_uint64
+f32 = C.c_float
+f32p = C.POINTER(C.c_float)
+
+# Every symbol the header declares, with its argument types.
+SIGNATURES = {
+    "pxb_context_create": ([C.c_int, C.POINTER(P)], C.c_int),
+    "pxb_context_destroy": ([P], C.c_int),
+    "pxb_last_error": ([P], C.c_char_p),
+    "pxb_context_stream": ([P, C.POINTER(P)], C.c_int),
+    "pxb_context_synchronize": ([P], C.c_int),
+    "pxb_context_launch_count": ([P], u64),
+    "pxb_cloth_params_default": ([C.POINTER(A.ClothParams)], None),
+    "pxb_cloth_add": ([P, C.POINTER(A.ClothDesc), C.POINTER(u64)], C.c_int),
+    "pxb_cloth_remove": ([P, u64], C.c_int),
+    "pxb_cloth_set_params": ([P, u64, C.POINTER(A.ClothParams)], C.c_int),
+    "pxb_cloth_write_particles": ([P, u64, P, u32], C.c_int),
+    "pxb_cloth_read_particles": ([P, u64, P, u32], C.c_int),
+    "pxb_cloth_read_lambdas": ([P, u64, P, u32, P, u32], C.c_int),
+    "pxb_cloth_set_anchor_targets": ([P, u64, P, u32], C.c_int),
+    "pxb_cloth_read_anchors": ([P, u64, P, u32], C.c_int),
+    "pxb_cloth_read_time": ([P, u64, f32p], C.c_int),
+    "pxb_cloths_step": ([P, C.POINTER(A.ClothStepDesc)], C.c_int),
+    "pxb_cloths_read_results": ([P, P, u32, P], C.c_int),
+    "pxb_cloths_read_positions": ([P, P, u32, P, C.c_size_t], C.c_int),
+    "pxb_solve_cloth_host": ([P, C.POINTER(A.ClothDesc), P, P, P, P, P, u32, f32p, u32, u32, f32,
+                              f32p, f32p], C.c_int),
+    "pxb_project_particles": ([P, P, f32, P, P, u32, P, P, P, P], C.c_int),
+    "pxb_host_cloth_make_grid": ([C.POINTER(A.GridClothDesc), C.POINTER(P)], C.c_int),
+    "pxb_host_cloth_destroy": ([P], C.c_int),
+    "pxb_host_cloth_pin_static": ([P, f32p, f32, C.POINTER(u32)], C.c_int),
+    "pxb_host_cloth_build_tethers": ([P], C.c_int),
+    "pxb_host_cloth_view": ([P, C.POINTER(A.ClothDesc)], C.c_int),
+    "pxb_host_cloth_mutable": ([P, C.POINTER(P), C.POINTER(P), C.POINTER(P)], C.c_int),
+    "pxb_measure_smem_bandwidth": ([P, C.POINTER(C.c_double)], C.c_int),
+}
+
+_lib = None
+
+
+class PxbError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{A.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def library():
+    """Loads libphysxcoopa_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m physxcoopa_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib
+
+
+def _vec(x, n=3):
+    return (C.c_float * n)(*[float(v) for v in x])
+
+
+class HostCloth:
+    """A cloth built by the library's host builders (cloth_builder.h), in library memory."""
+
+    def __init__(self, columns, rows, width, height, center=(0, 0, 0), orientation=(0, 0, 0, 1),
+                 total_mass=1.0, shear=True, params=None, jitter=0.0, seed=0):
+        d = A.GridClothDesc()
+        d.columns, d.rows, d.width, d.height = columns, rows, width, height
+        d.center = _vec(center)
+        d.orientation = _vec(orientation, 4)
+        d.total_mass = total_mass
+        d.shear = 1 if shear else 0
+        d.params = params if params is not None else A.ClothParams.defaults()
+        d.jitter = jitter
+        d.jitter_seed = seed
+        self._h = P()
+        st = library().pxb_host_cloth_make_grid(C.byref(d), C.byref(self._h))
+        if st:
+            raise PxbError(st, "make_grid failed")
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pxb_host_cloth_destroy(self._h)
+            self._h = None
+
+    def pin_static(self, point, radius):
+        n = u32()
+        st = library().pxb_host_cloth_pin_static(self._h, _vec(point), radius, C.byref(n))
+        if st:
+            raise PxbError(st, "pin_static failed")
+        return n.value
+
+    def build_tethers(self):
+        st = library().pxb_host_cloth_build_tethers(self._h)
+        if st:
+            raise PxbError(st, "build_tethers failed")
+
+    def arrays(self) -> ClothArrays:
+        v = A.ClothDesc()
+        library().pxb_host_cloth_view(self._h, C.byref(v))
+        return ClothArrays.from_desc(v)
+
+
+def make_grid_cloth(columns, rows, width, height, **kw) -> ClothArrays:
+    pins = kw.pop("pins", ())
+    tethers = kw.pop("tethers", False)
+    h = HostCloth(columns, rows, width, height, **kw)
+    for point, radius in pins:
+        h.pin_static(point, radius)
+    if tethers:
+        h.build_tethers()
+    return h.arrays()
+
+
+def _flatten(per_cloth, dtype, n):
+    """A list of per-cloth record arrays -> (flat array, offsets) or (None, None)."""
+    if per_cloth is None:
+        return None, None
+    if isinstance(per_cloth, np.ndarray) and per_cloth.dtype == dtype:
+        per_cloth = [per_cloth] * n
+    lens = [0 if a is None else len(a) for a in per_cloth]
+    offs = np.zeros(n + 1, np.uint32)
+    offs[1:] = np.cumsum(lens)
+    if offs[-1] == 0:
+        return None, None
+    flat = np.ascontiguousarray(np.concatenate([a for a in per_cloth if a is not None and len(a)]))
+    return flat, offs
+
+
+class Context:
+    """One device, one stream (pxb_context)."""
+
+    def __init__(self, device=0):
+        self.lib = library()
+        self.h = P()
+        st = self.lib.pxb_context_create(device, C.byref(self.h))
+        if st:
+            raise PxbError(st, "pxb_context_create failed (is a CUDA device visible?)")
+        self._keep = []
+
+    def close(self):
+        if self.h:
+            self.lib.pxb_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st:
+            raise PxbError(st, f"{what}: {self.lib.pxb_last_error(self.h).decode()}")
+
+    @property
+    def stream(self):
+        s = P()
+        self._check(self.lib.pxb_context_stream(self.h, C.byref(s)), "stream")
+        return s.value
+
+    def synchronize(self):
+        self._check(self.lib.pxb_context_synchronize(self.h), "synchronize")
+
+    def measure_smem_bandwidth(self):
+        """Achievable device-wide shared-memory bandwidth, bytes/s (roofline denominator)."""
+        v = C.c_double()
+        self._check(self.lib.pxb_measure_smem_bandwidth(self.h, C.byref(v)), "measure_smem_bandwidth")
+        return v.value
+
+    @property
+    def launch_count(self):
+        return int(self.lib.pxb_context_launch_count(self.h))
+
+    # --- registry ------------------------------------------------------------------------
+    def add_cloth(self, c: ClothArrays) -> int:
+        d = c.desc()
+        out = u64()
+        self._check(self.lib.pxb_cloth_add(self.h, C.byref(d), C.byref(out)), "add_cloth")
+        return out.value
+
+    def remove_cloth(self, cid):
+        self._check(self.lib.pxb_cloth_remove(self.h, cid), "remove_cloth")
+
+    def set_params(self, cid, params):
+        self._check(self.lib.pxb_cloth_set_params(self.h, cid, C.byref(params)), "set_params")
+
+    def write_particles(self, cid, particles):
+        p = np.ascontiguousarray(particles, A.PARTICLE)
+        self._check(self.lib.pxb_cloth_write_particles(self.h, cid, A.ptr(p), len(p)), "write_particles")
+
+    def read_particles(self, cid, n):
+        out = np.zeros(n, A.PARTICLE)
+        self._check(self.lib.pxb_cloth_read_particles(self.h, cid, A.ptr(out), n), "read_particles")
+        return out
+
+    def read_lambdas(self, cid, n_stretch, n_bend):
+        s = np.zeros(n_stretch, np.float32)
+        b = np.zeros(n_bend, np.float32)
+        self._check(self.lib.pxb_cloth_read_lambdas(self.h, cid, A.ptr(s) if n_stretch else None,
+                                                    n_stretch, A.ptr(b) if n_bend else None, n_bend),
+                    "read_lambdas")
+        return s, b
+
+    def set_anchor_targets(self, cid, world):
+        w = np.ascontiguousarray(world, np.float32).reshape(-1, 3)
+        self._check(self.lib.pxb_cloth_set_anchor_targets(self.h, cid, A.ptr(w), len(w)),
+                    "set_anchor_targets")
+
+    def read_anchors(self, cid, n):
+        out = np.zeros(n, A.ANCHOR)
+        self._check(self.lib.pxb_cloth_read_anchors(self.h, cid, A.ptr(out), n), "read_anchors")
+        return out
+
+    def read_time(self, cid):
+        t = f32()
+        self._check(self.lib.pxb_cloth_read_time(self.h, cid, C.byref(t)), "read_time")
+        return t.value
+
+    # --- stepping ------------------------------------------------------------------------
+    def make_step(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
+                  iterations=10, h=1.0 / 60.0):
+        """Builds (and keeps alive) a pxb_cloth_step_desc; reuse it to step repeatedly."""
+        ids = np.ascontiguousarray(ids, np.uint64)
+        n = len(ids)
+        cols, coff = _flatten(colliders, A.COLLIDER, n)
+        src, soff = _flatten(sources, A.GRAVITY_SOURCE, n)
+        d = A.ClothStepDesc()
+        d.cloths = A.ptr(ids)
+        d.n_cloths = n
+        d.colliders = A.ptr(cols)
+        d.collider_offsets = A.ptr(coff)
+        d.gravity = _vec(gravity)
+        d.sources = A.ptr(src)
+        d.source_offsets = A.ptr(soff)
+        d.substeps, d.iterations, d.h = substeps, iterations, h
+        keep = (ids, cols, coff, src, soff)
+        return d, keep
+
+    def step_desc(self, d):
+        self._check(self.lib.pxb_cloths_step(self.h, C.byref(d)), "cloths_step")
+
+    def step(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
+             iterations=10, h=1.0 / 60.0):
+        d, keep = self.make_step(ids, colliders, gravity, sources, substeps, iterations, h)
+        self.step_desc(d)
+        del keep
+
+    def read_results(self, ids):
+        ids = np.ascontiguousarray(ids, np.uint64)
+        out = np.zeros(len(ids), A.FRAME_RESULT)
+        self._check(self.lib.pxb_cloths_read_results(self.h, A.ptr(ids), len(ids), A.ptr(out)),
+                    "read_results")
+        return out
+
+    def read_positions(self, ids, out=None):
+        ids = np.ascontiguousarray(ids, np.uint64)
+        if out is None:
+            raise ValueError("pass an output float32 array (3 floats per particle)")
+        self._check(self.lib.pxb_cloths_read_positions(self.h, A.ptr(ids), len(ids), out.ctypes.data,
+                                                       out.size), "read_positions")
+        return out
+
+    def project_particles(self, collider, thickness, points):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        n = len(pts)
+        col = np.ascontiguousarray(np.asarray(collider, A.COLLIDER).reshape(1))
+        out = np.zeros_like(pts)
+        nrm = np.zeros_like(pts)
+        dep = np.zeros(n, np.float32)
+        hit = np.zeros(n, np.int32)
+        self._check(self.lib.pxb_project_particles(self.h, A.ptr(col), thickness, A.ptr(pts), None, n,
+                                                   A.ptr(out), A.ptr(nrm), A.ptr(dep), A.ptr(hit)),
+                    "project_particles")
+        return hit, out, nrm, dep
+
+    def solve_cloth_host(self, c: ClothArrays, colliders=None, gravity=(0, 0, -9.81), substeps=4,
+                         iterations=10, h=1.0 / 60.0):
+        """The drop-in solve_cloth on host arrays: advances `c` in place."""
+        d = c.desc()
+        cols = colliders if colliders is not None else np.zeros(0, A.COLLIDER)
+        t = f32(c.time)
+        b = (C.c_float * 6)()
+        self._check(self.lib.pxb_solve_cloth_host(
+            self.h, C.byref(d), A.ptr(c.particles), A.ptr(c.stretch), A.ptr(c.bend),
+            A.ptr(c.anchors), A.ptr(cols), len(cols), _vec(gravity), substeps, iterations, h,
+            C.byref(t), b), "solve_cloth_host")
+        c.time = t.value
+        c.bounds = np.array(b[:], np.float32)
+        return c

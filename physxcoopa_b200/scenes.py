@@ -1,0 +1,145 @@
+"""Seeded synthetic workloads for the cloth benchmark configurations.
+
+No public dataset exists for this path; every scene is generated from a seed with the sizes and
+value distributions of the benchmark configurations:
+
+  single_drape   one 32x32 sheet, 0.05 m spacing, +-1 mm jitter, two top corners pinned (with
+                 geodesic tethers), sphere r = 0.3 m 0.5 m below the centre; compliance 0
+                 (structural) / 1e-6 (shear) / 1e-4 (bending); 4 substeps x 10 iterations.
+  uniform_batch  N sheets of side 64 (default 1024), same constraint types and compliances;
+                 per sheet from the seed: pin pattern (2 corners, 4 corners or the full top
+                 edge) and one sphere, radius U(0.2, 0.5) m, centre 0.5 m below the sheet
+                 centre offset by U(-0.3, 0.3) m per axis.
+  uneven_batch   N sheets (default 4096), side U{16..128}, 1-3 colliders each drawn from sphere
+                 / capsule (r U(0.1, 0.3), half-length U(0.2, 0.6)) / oriented box (half-extents
+                 U(0.1, 0.5)); half the sheets get one point gravity source (9.81, radius 1 m,
+                 range 10 m).
+
+Parameters the configurations leave open keep the reference's ClothParams defaults
+(physxcoopa/cloth/cloth.h:171-255): damping 0.05, aero drag / lift 0.02, thickness 0.03,
+friction 0.5, tether_scale 1.02, max_velocity 100. Sleep plays no part (the solver is stepped
+unconditionally). Sheets are horizontal (identity orientation), 1 kg each, rest lengths captured
+after the jitter so a sheet starts unstrained.
+"""
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import _abi as A
+from .arrays import ClothArrays, box, capsule, collider_array, gravity_sources, sphere
+from .runtime import HostCloth
+
+SPACING = 0.05
+STRUCTURAL, SHEAR, BEND = 0.0, 1e-6, 1e-4
+
+
+@dataclass
+class ClothScene:
+    name: str
+    cloths: List[ClothArrays]
+    colliders: List[np.ndarray]
+    sources: Optional[List[np.ndarray]] = None
+    gravity: tuple = (0.0, 0.0, -9.81)
+    substeps: int = 4
+    iterations: int = 10
+    h: float = 1.0 / 60.0
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def vertices(self):
+        return sum(len(c.particles) for c in self.cloths)
+
+
+def cloth_params(**kw):
+    p = A.ClothParams.defaults()
+    p.stretch_compliance = STRUCTURAL
+    p.bend_compliance = BEND
+    p.has_shear_compliance = 1
+    p.shear_compliance = SHEAR
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _sheet(side, center, seed, pins, params=None, tethers=True):
+    width = (side - 1) * SPACING
+    h = HostCloth(side, side, width, width, center=center, params=params or cloth_params(),
+                  jitter=1e-3, seed=seed)
+    for point, radius in pins:
+        h.pin_static(point, radius)
+    if tethers and pins:
+        h.build_tethers()
+    return h.arrays()
+
+
+def _corner_pins(side, center, pattern):
+    half = (side - 1) * SPACING * 0.5
+    cx, cy, cz = center
+    r = 0.3 * SPACING  # smaller than the spacing: exactly the chosen particle despite the jitter
+    top = [((cx - half, cy + half, cz), r), ((cx + half, cy + half, cz), r)]
+    if pattern == 0:
+        return top
+    if pattern == 1:
+        return top + [((cx - half, cy - half, cz), r), ((cx + half, cy - half, cz), r)]
+    return [((cx - half + k * SPACING, cy + half, cz), r) for k in range(side)]
+
+
+def single_drape(seed=0):
+    center = (0.0, 0.0, 1.0)
+    c = _sheet(32, center, seed, _corner_pins(32, center, 0))
+    col = collider_array([sphere(0.3, (0.0, 0.0, 0.5))])
+    return ClothScene("single_drape 32x32", [c], [col], meta={"side": 32})
+
+
+def uniform_batch(n=1024, side=64, seed=1):
+    rng = np.random.default_rng(seed)
+    center = (0.0, 0.0, 1.0)
+    cloths, cols = [], []
+    for k in range(n):
+        pattern = int(rng.integers(0, 3))
+        cloths.append(_sheet(side, center, seed * 100003 + k, _corner_pins(side, center, pattern)))
+        r = float(rng.uniform(0.2, 0.5))
+        off = rng.uniform(-0.3, 0.3, 3)
+        cols.append(collider_array([sphere(r, (center[0] + off[0], center[1] + off[1],
+                                               center[2] - 0.5 + off[2]))]))
+    return ClothScene(f"uniform_batch {n}x{side}^2", cloths, cols, meta={"side": side, "n": n})
+
+
+def _random_quat(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    return tuple(float(v) for v in q.astype(np.float32))
+
+
+def uneven_batch(n=4096, lo=16, hi=128, seed=2, max_side=None):
+    rng = np.random.default_rng(seed)
+    cloths, cols, srcs = [], [], []
+    for k in range(n):
+        side = int(rng.integers(lo, hi + 1))
+        if max_side is not None:
+            side = min(side, max_side)
+        center = (0.0, 0.0, 1.0)
+        pattern = int(rng.integers(0, 3))
+        cloths.append(_sheet(side, center, seed * 100003 + k, _corner_pins(side, center, pattern)))
+        recs = []
+        for _ in range(int(rng.integers(1, 4))):
+            kind = int(rng.integers(0, 3))
+            off = rng.uniform(-0.3, 0.3, 3)
+            pos = (float(off[0]), float(off[1]), 0.5 + float(off[2]))
+            if kind == 0:
+                recs.append(sphere(float(rng.uniform(0.2, 0.5)), pos))
+            elif kind == 1:
+                recs.append(capsule(float(rng.uniform(0.1, 0.3)), float(rng.uniform(0.2, 0.6)), pos,
+                                    _random_quat(rng)))
+            else:
+                recs.append(box(tuple(float(v) for v in rng.uniform(0.1, 0.5, 3)), pos,
+                                _random_quat(rng)))
+        cols.append(collider_array(recs))
+        if k % 2 == 0:
+            srcs.append(gravity_sources([((float(rng.uniform(-2, 2)), float(rng.uniform(-2, 2)),
+                                           -3.0), 9.81, 1.0, 10.0)]))
+        else:
+            srcs.append(None)
+    return ClothScene(f"uneven_batch {n} sides U{{{lo}..{hi}}}", cloths, cols, sources=srcs,
+                      meta={"n": n, "lo": lo, "hi": hi})

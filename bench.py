@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--cloths", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="fix the kernel variant (0/1/2) instead of autotuning")
     return ap.parse_args()
 
 
@@ -230,6 +232,14 @@ def main():
                             sc.iterations, sc.h)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local_rank))
 
+    tune = None
+    if args.variant is None:
+        best, ms = ctx.autotune(d, trials=2)
+        tune = {"chosen_variant": best, "ms_per_step_by_variant": ms,
+                "variants": "block-size cap 512 / 768 / 1024 threads"}
+    else:
+        ctx.set_cloth_variant(args.variant)
+        tune = {"chosen_variant": args.variant, "fixed": True}
     for _ in range(max(args.warmup, 3)):
         ctx.step_desc(d)
     ctx.synchronize()
@@ -331,7 +341,8 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scenes)",
-            "config": dict(workload_config(args, sc), parallelism=f"independent cloth batches x{world}"),
+            "config": dict(workload_config(args, sc), parallelism=f"independent cloth batches x{world}",
+                           autotune=tune),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
             "roofline": {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -336,6 +336,17 @@ pxb_status pxb_solve_cloth_host(pxb_context* ctx, const pxb_cloth_desc* desc,
                                 const float gravity[3], uint32_t substeps, uint32_t iterations,
                                 float h, float* time_inout, float* bounds_out);
 
+/* Kernel variant used by pxb_cloths_step: the block-size cap of the cloth kernel (0 = 512
+ * threads, 1 = 768, 2 = 1024; a larger block has more warps to hide latency but fewer
+ * registers per thread). Results are identical across variants; only speed differs. */
+pxb_status pxb_context_set_cloth_variant(pxb_context* ctx, int32_t variant);
+/* Autotuner: times every kernel variant on `step` (the caller's real batch, `trials` launches
+ * each after one warm-up) and keeps the fastest on the context. The listed cloths' device state
+ * and host mirrors are saved first and restored after, so tuning does not advance them.
+ * variant_out and ms_out (one entry per variant, milliseconds per step) may be NULL. */
+pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step, uint32_t trials,
+                               int32_t* variant_out, float* ms_out);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Collision primitive: cloth::project_particle (physxcoopa/cloth/cloth_collision.h:386-420)    */
 /* evaluated on the device for a batch of points (the collision stage of both solvers).         */

@@ -31,7 +31,6 @@
 namespace pxb {
 namespace {
 
-constexpr int kMaxThreads = 1024;
 constexpr uint32_t kWaitLimit = 1u << 26;  // bounded mbarrier polls before giving up
 
 // ------------------------------------------------------------------------------------------
@@ -262,17 +261,21 @@ __device__ __forceinline__ bool solve_pair(float4& pa, float4& pb, float rest, f
     return true;
 }
 
-struct SegReg {
-    int count, per_row, a_base, row_stride, d, rest_base, lam_base;
-    uint32_t magic;
-};
-
-__device__ __forceinline__ void seg_slots(const SegReg& s, int i, int& la, int& lb) {
+// Slots of item g of the colour whose segments are segs[sb, se): endpoints la / lb, rest slot
+// rs, lambda slot ls (-1 when the colour keeps none).
+__device__ __forceinline__ void item_slots(const PxbSeg* __restrict__ segs, int sb, int se, int g,
+                                           int& la, int& lb, int& rs, int& ls) {
+    int s = sb;
+    while (s + 1 < se && g >= segs[s + 1].start) ++s;
+    const PxbSeg& q = segs[s];
+    const int i = g - q.start;
     // magic == 0 marks per_row == 1 (floor(2^32 / 1) + 1 does not fit in 32 bits).
-    const int r = s.magic ? static_cast<int>(__umulhi(static_cast<uint32_t>(i), s.magic)) : i;
-    const int k = i - r * s.per_row;
-    la = s.a_base + r * s.row_stride + k;
-    lb = la + s.d;
+    const int r = q.magic ? static_cast<int>(__umulhi(static_cast<uint32_t>(i), q.magic)) : i;
+    const int k = i - r * q.per_row;
+    la = q.a_base + r * q.row_stride + k;
+    lb = la + q.d;
+    rs = q.rest_base + i;
+    ls = q.lam_base >= 0 ? q.lam_base + i : -1;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -298,6 +301,7 @@ __device__ __forceinline__ float warp_max(float v) {
 // The kernel
 // ------------------------------------------------------------------------------------------
 
+template <int kMaxThreads>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders,
@@ -355,23 +359,19 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
 
     // --- gravity: uniform, or the source field at the cloth's mean position (world.h:1833) --
     if (sP.src_count > 0) {
-        float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-        for (int l = tid; l < n_layout; l += T) {
-            if (sC.vel[l].w != 0.0f) {
-                const float4 p = pos[l];
-                sx += p.x; sy += p.y; sz += p.z;
-            }
-        }
-        sx = warp_sum(sx); sy = warp_sum(sy); sz = warp_sum(sz);
-        if ((tid & 31) == 0) {
-            s_red[tid >> 5][0] = sx; s_red[tid >> 5][1] = sy; s_red[tid >> 5][2] = sz;
-        }
-        __syncthreads();
         if (tid == 0) {
+            // PhysicsWorld::cloth_centre_ (world.h:2072-2076): the mean in particle order, summed
+            // sequentially exactly as the reference does, so the gravity it selects is the
+            // reference's to the bit (a reordered sum drifts the drape chaotically).
+            const int Q = sC.Q, S = sC.S, cols = sC.columns, n = sC.n_real;
             float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-            const int nw = (T + 31) >> 5;
-            for (int w = 0; w < nw; ++w) { cx += s_red[w][0]; cy += s_red[w][1]; cz += s_red[w][2]; }
-            const float fn = static_cast<float>(sC.n_real);
+            int x = 0, y = 0;
+            for (int i = 0; i < n; ++i) {
+                const float4 p = pos[lay(x, y, Q, S)];
+                cx += p.x; cy += p.y; cz += p.z;
+                if (++x == cols) { x = 0; ++y; }
+            }
+            const float fn = static_cast<float>(n);
             const f3 centre = mk(cx / fn, cy / fn, cz / fn);
             // PhysicsWorld::field_at_ (world.h:2048-2068)
             float best = 0.0f;
@@ -492,6 +492,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         __syncthreads();
 
         // --- 4b. constraint iterations: colour by colour (cloth_solver.h:256-271) ----------
+        // The segments of a colour form one index space; a thread takes items g and g + T
+        // together so two independent projections are in flight (colours are disjoint).
         // A zero-compliance colour keeps no lambda: with alpha == 0 the multiplier never
         // reaches a position (dlambda = (-c - 0*lambda)/w); only the sign of an exactly-zero
         // correction could differ, which moves no coordinate that is not itself +-0.
@@ -501,47 +503,36 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 for (int c = 0; c < n_colours; ++c) {
                     const float alpha = sP.alpha[c];
                     const int sb = sC.colour_seg[c], se = sC.colour_seg[c + 1];
-                    for (int sg = sb; sg < se; ++sg) {
-                        const PxbSeg& g = s_seg[sg];
-                        const SegReg sr{g.count, g.per_row, g.a_base, g.row_stride, g.d,
-                                        g.rest_base, g.lam_base, g.magic};
-                        const bool has_lam = sr.lam_base >= 0;
-                        int i = tid;
-                        for (; i + T < sr.count; i += 2 * T) {
-                            int la0, lb0, la1, lb1;
-                            seg_slots(sr, i, la0, lb0);
-                            seg_slots(sr, i + T, la1, lb1);
-                            float4 pa0 = pos[la0], pb0 = pos[lb0];
-                            float4 pa1 = pos[la1], pb1 = pos[lb1];
-                            const float r0 = rest[sr.rest_base + i];
-                            const float r1 = rest[sr.rest_base + i + T];
-                            const float lam0 = has_lam ? U[sr.lam_base + i] : 0.0f;
-                            const float lam1 = has_lam ? U[sr.lam_base + i + T] : 0.0f;
-                            float d0 = 0.0f, d1 = 0.0f;
-                            const bool w0 = solve_pair(pa0, pb0, r0, lam0, alpha, d0);
-                            const bool w1 = solve_pair(pa1, pb1, r1, lam1, alpha, d1);
-                            if (w0) {
-                                pos[la0] = pa0;
-                                pos[lb0] = pb0;
-                                if (has_lam) U[sr.lam_base + i] = lam0 + d0;
-                            }
-                            if (w1) {
-                                pos[la1] = pa1;
-                                pos[lb1] = pb1;
-                                if (has_lam) U[sr.lam_base + i + T] = lam1 + d1;
-                            }
+                    const int total = sC.colour_total[c];
+                    for (int g = tid; g < total; g += 2 * T) {
+                        int la0, lb0, rs0, ls0, la1 = 0, lb1 = 0, rs1 = 0, ls1 = -1;
+                        item_slots(s_seg, sb, se, g, la0, lb0, rs0, ls0);
+                        const int g1 = g + T;
+                        const bool two = g1 < total;
+                        if (two) item_slots(s_seg, sb, se, g1, la1, lb1, rs1, ls1);
+                        float4 pa0 = pos[la0], pb0 = pos[lb0];
+                        const float r0 = rest[rs0];
+                        const float lam0 = ls0 >= 0 ? U[ls0] : 0.0f;
+                        float4 pa1, pb1;
+                        float r1 = 0.0f, lam1 = 0.0f;
+                        if (two) {
+                            pa1 = pos[la1];
+                            pb1 = pos[lb1];
+                            r1 = rest[rs1];
+                            lam1 = ls1 >= 0 ? U[ls1] : 0.0f;
                         }
-                        if (i < sr.count) {
-                            int la0, lb0;
-                            seg_slots(sr, i, la0, lb0);
-                            float4 pa0 = pos[la0], pb0 = pos[lb0];
-                            const float lam0 = has_lam ? U[sr.lam_base + i] : 0.0f;
-                            float d0 = 0.0f;
-                            if (solve_pair(pa0, pb0, rest[sr.rest_base + i], lam0, alpha, d0)) {
-                                pos[la0] = pa0;
-                                pos[lb0] = pb0;
-                                if (has_lam) U[sr.lam_base + i] = lam0 + d0;
-                            }
+                        float d0 = 0.0f, d1 = 0.0f;
+                        const bool w0 = solve_pair(pa0, pb0, r0, lam0, alpha, d0);
+                        const bool w1 = two && solve_pair(pa1, pb1, r1, lam1, alpha, d1);
+                        if (w0) {
+                            pos[la0] = pa0;
+                            pos[lb0] = pb0;
+                            if (ls0 >= 0) U[ls0] = lam0 + d0;
+                        }
+                        if (w1) {
+                            pos[la1] = pa1;
+                            pos[lb1] = pb1;
+                            if (ls1 >= 0) U[ls1] = lam1 + d1;
                         }
                     }
                     __syncthreads();
@@ -710,23 +701,46 @@ cudaError_t launch_gather_positions(const PxbClothDev* cloths, const int32_t* or
     return cudaGetLastError();
 }
 
-cudaError_t launch_cloth_step(const PxbClothDev* cloths, const PxbClothStep* steps,
-                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
-                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
-                              int n_blocks, int threads, int smem_bytes, cudaStream_t stream) {
+template <int kMaxThreads>
+static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
+                                  const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                                  const int32_t* order, PxbFrameResult* results, uint32_t* err,
+                                  int n_blocks, int threads, int smem_bytes, cudaStream_t stream) {
     static uint64_t configured = 0;  // one bit per device the attribute has been set on
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && !(configured >> dev & 1ull)) {
-        e = cudaFuncSetAttribute(cloth_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kMaxDynamicSmem);
+        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
         if (e != cudaSuccess) return e;
         configured |= 1ull << dev;
     }
-    cloth_step_kernel<<<n_blocks, threads, smem_bytes, stream>>>(cloths, steps, colliders, sources,
-                                                                  order, results, err);
+    cloth_step_kernel<kMaxThreads><<<n_blocks, threads, smem_bytes, stream>>>(
+        cloths, steps, colliders, sources, order, results, err);
     return cudaGetLastError();
+}
+
+int cloth_variant_threads(int variant) {
+    return variant == 0 ? 512 : (variant == 1 ? 768 : 1024);
+}
+
+cudaError_t launch_cloth_step(int variant, const PxbClothDev* cloths, const PxbClothStep* steps,
+                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
+                              int n_blocks, int threads, int smem_bytes, cudaStream_t stream) {
+    if (threads > cloth_variant_threads(variant)) threads = cloth_variant_threads(variant);
+    switch (variant) {
+        case 0:
+            return launch_variant<512>(cloths, steps, colliders, sources, order, results, err,
+                                       n_blocks, threads, smem_bytes, stream);
+        case 1:
+            return launch_variant<768>(cloths, steps, colliders, sources, order, results, err,
+                                       n_blocks, threads, smem_bytes, stream);
+        default:
+            return launch_variant<1024>(cloths, steps, colliders, sources, order, results, err,
+                                        n_blocks, threads, smem_bytes, stream);
+    }
 }
 
 cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness, const float* pts,

@@ -39,6 +39,7 @@ struct PxbSeg {
     int32_t d;          // lb - la
     int32_t rest_base;  // rest-length slot of constraint 0
     int32_t lam_base;   // lambda slot of constraint 0, or -1 when the colour has zero compliance
+    int32_t start;      // index of constraint 0 among all constraints of its colour
 };
 
 // Static per-cloth description, device resident, written at registration.
@@ -56,6 +57,7 @@ struct PxbClothDev {
     int32_t n_colours;
     int32_t colour_seg[PXB_MAX_COLOURS + 1]; // colour c = segs [colour_seg[c], colour_seg[c+1])
     int32_t colour_is_bend[PXB_MAX_COLOURS];
+    int32_t colour_total[PXB_MAX_COLOURS];  // constraints per colour
     int32_t n_layout;
     int32_t n_real;
     int32_t columns, rows, Q, S;

@@ -16,7 +16,11 @@ constexpr int kMaxDynamicSmem = 232448 - 4096;
 constexpr int kClothOwned = 4;      // particles per thread in the cloth kernel
 constexpr int kClothMaxThreads = 1024;
 
-cudaError_t launch_cloth_step(const PxbClothDev* cloths, const PxbClothStep* steps,
+// Kernel variants differ in their block-size cap (and so their register budget): 0 = 512
+// threads (no spills), 1 = 768, 2 = 1024.
+constexpr int kClothVariants = 3;
+int cloth_variant_threads(int variant);
+cudaError_t launch_cloth_step(int variant, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,
                               int n_blocks, int threads, int smem_bytes, cudaStream_t stream);

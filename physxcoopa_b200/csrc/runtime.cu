@@ -113,6 +113,7 @@ PxbSeg seg(int rows_n, int per_row, int a_base, int row_stride, int d) {
     s.d = d;
     s.rest_base = 0;
     s.lam_base = -1;
+    s.start = 0;
     s.magic = per_row == 1 ? 0u
                            : static_cast<uint32_t>((0x100000000ull / static_cast<uint64_t>(per_row)) + 1ull);
     return s;
@@ -413,12 +414,16 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     for (int c = 0; c < e.n_colours; ++c) {
         e.colour_seg[c] = static_cast<int>(e.segs.size());
         e.colour_is_bend[c] = cs[c].bend ? 1 : 0;
+        int start = 0;
         for (PxbSeg s : cs[c].segs) {
             if (s.count >= 65536) return fail(PXB_ERR_TOO_LARGE, "a colour segment exceeds 65535 constraints");
             s.rest_base = rest;
+            s.start = start;
             rest += s.count;
+            start += s.count;
             e.segs.push_back(s);
         }
+        e.colour_total.push_back(start);
     }
     e.colour_seg[e.n_colours] = static_cast<int>(e.segs.size());
     if (e.segs.size() > PXB_MAX_SEGS) return fail(PXB_ERR_TOO_LARGE, "too many colour segments");
@@ -508,6 +513,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.n_colours = e.n_colours;
     for (int c = 0; c <= e.n_colours; ++c) e.dev.colour_seg[c] = e.colour_seg[c];
     for (int c = 0; c < e.n_colours; ++c) e.dev.colour_is_bend[c] = e.colour_is_bend[c];
+    for (int c = 0; c < e.n_colours; ++c) e.dev.colour_total[c] = e.colour_total[c];
     e.dev.n_layout = e.n_layout;
     e.dev.n_real = static_cast<int32_t>(n);
     e.dev.columns = e.cols;
@@ -732,7 +738,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     char* db = static_cast<char*>(d_stage.p);
     if (pxb_status s = cuda(cudaMemcpyAsync(db, hb, total, cudaMemcpyHostToDevice, stream), "upload step")) return s;
     cudaEventRecord(staged, stream);
-    cudaError_t le = launch_cloth_step(static_cast<const PxbClothDev*>(d_registry.p),
+    cudaError_t le = launch_cloth_step(cloth_variant, static_cast<const PxbClothDev*>(d_registry.p),
                                        reinterpret_cast<const PxbClothStep*>(db),
                                        reinterpret_cast<const PxbDevCollider*>(db + o_cols),
                                        reinterpret_cast<const pxb_gravity_source*>(db + o_src),
@@ -1128,6 +1134,98 @@ pxb_status pxb_solve_cloth_host(pxb_context* ctx, const pxb_cloth_desc* desc, px
         std::memcpy(bounds_out, r.bounds_min, 12);
         std::memcpy(bounds_out + 3, r.bounds_max, 12);
     }
+    return PXB_OK;
+}
+
+
+pxb_status pxb_context_set_cloth_variant(pxb_context* ctx, int32_t variant) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    if (variant < 0 || variant >= kClothVariants)
+        return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "variant must be in [0, %d)", kClothVariants);
+    ctx->cloth_variant = variant;
+    return PXB_OK;
+}
+
+pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step, uint32_t trials,
+                               int32_t* variant_out, float* ms_out) {
+    if (!ctx || !step) return PXB_ERR_INVALID_ARGUMENT;
+    if (trials == 0) trials = 1;
+    const uint32_t n = step->n_cloths;
+    std::vector<ClothEntry*> ents(n);
+    size_t bytes = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        ents[k] = ctx->lookup(step->cloths[k]);
+        if (!ents[k]) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+        bytes += 48 * static_cast<size_t>(ents[k]->n_layout) + 4 * static_cast<size_t>(ents[k]->n_lam) +
+                 sizeof(PxbAnchorRec) * ents[k]->anchor_recs.size() + 3 * 256;
+    }
+    if (pxb_status s = ctx->grow(ctx->d_tune, bytes, "autotune state")) return s;
+    // Save the device state and the host mirrors a step touches.
+    struct Saved { float time; std::vector<PxbAnchorRec> recs; std::vector<pxb_anchor> anchors; PxbFrameResult result; bool has; };
+    std::vector<Saved> saved(n);
+    auto copy_state = [&](bool save) -> pxb_status {
+        char* t = static_cast<char*>(ctx->d_tune.p);
+        for (uint32_t k = 0; k < n; ++k) {
+            ClothEntry& e = *ents[k];
+            const size_t L = 16 * static_cast<size_t>(e.n_layout);
+            void* parts[4] = {e.dev.pos, e.dev.vel, e.dev.prv, e.dev.lam_out};
+            const size_t sz[4] = {L, L, L, 4 * static_cast<size_t>(e.n_lam)};
+            for (int q = 0; q < 4; ++q) {
+                if (sz[q]) {
+                    cudaError_t ce = cudaMemcpyAsync(save ? static_cast<void*>(t) : parts[q],
+                                                     save ? parts[q] : static_cast<void*>(t), sz[q],
+                                                     cudaMemcpyDeviceToDevice, ctx->stream);
+                    if (ce != cudaSuccess) return ctx->cuda(ce, "autotune save/restore");
+                }
+                t += align256(sz[q]);
+            }
+            if (save) saved[k] = Saved{e.time, e.anchor_recs, e.anchors, e.result, e.has_result};
+            else {
+                e.time = saved[k].time;
+                e.anchor_recs = saved[k].recs;
+                e.anchors = saved[k].anchors;
+                e.result = saved[k].result;
+                e.has_result = saved[k].has;
+                if (pxb_status s = ctx->upload_anchor_records(e)) return s;
+            }
+        }
+        return PXB_OK;
+    };
+    if (pxb_status s = copy_state(true)) return s;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    const int before = ctx->cloth_variant;
+    int best = before;
+    float best_ms = 0.0f;
+    pxb_status st = PXB_OK;
+    for (int v = 0; v < kClothVariants && !st; ++v) {
+        ctx->cloth_variant = v;
+        st = ctx->step_cloths(step);  // warm-up (and attribute set-up) of this variant
+        if (st) break;
+        cudaEventRecord(t0, ctx->stream);
+        for (uint32_t r = 0; r < trials && !st; ++r) st = ctx->step_cloths(step);
+        cudaEventRecord(t1, ctx->stream);
+        if (cudaEventSynchronize(t1) != cudaSuccess) st = ctx->fail(PXB_ERR_CUDA, "autotune timing");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        ms /= static_cast<float>(trials);
+        if (ms_out) ms_out[v] = ms;
+        if (v == 0 || ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    pxb_status rs = copy_state(false);
+    if (!rs) rs = ctx->check_device_error();
+    ctx->results_fresh = false;
+    ctx->last_step.clear();
+    ctx->cloth_variant = st ? before : best;
+    if (st) return st;
+    if (rs) return rs;
+    if (variant_out) *variant_out = best;
     return PXB_OK;
 }
 

@@ -31,6 +31,7 @@ struct ClothEntry {
     std::vector<PxbSeg> segs;
     std::vector<int> colour_seg;
     std::vector<int> colour_is_bend;
+    std::vector<int> colour_total;
     std::vector<int32_t> colour_batch;     // colour -> reference batch index in its list
     std::vector<int32_t> rest_ref;         // rest slot -> stretch index, or n_stretch + bend index
     int n_rest_pad = 0;
@@ -74,11 +75,13 @@ struct pxb_context {
     std::vector<uint64_t> last_step;  // ids of the last step, in launch-slot order
     bool results_fresh = false;
     std::vector<HostSolveCache> host_cache;
+    int cloth_variant = 0;  // kernel block-size cap, see pxb_kernels.h (autotuned or set)
+    DevBuf d_tune;          // cloth state saved across an autotune
 
     ~pxb_context() {
         for (ClothEntry& e : cloths)
             if (e.alive && e.dmem) cudaFree(e.dmem);
-        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch})
+        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune})
             if (b->p) cudaFree(b->p);
         if (pinned) cudaFreeHost(pinned);
         if (d_err) cudaFree(d_err);

@@ -55,6 +55,8 @@ SIGNATURES = {
     "pxb_host_cloth_view": ([P, C.POINTER(A.ClothDesc)], C.c_int),
     "pxb_host_cloth_mutable": ([P, C.POINTER(P), C.POINTER(P), C.POINTER(P)], C.c_int),
     "pxb_measure_smem_bandwidth": ([P, C.POINTER(C.c_double)], C.c_int),
+    "pxb_context_set_cloth_variant": ([P, C.c_int32], C.c_int),
+    "pxb_cloths_autotune": ([P, C.POINTER(A.ClothStepDesc), u32, C.POINTER(C.c_int32), P], C.c_int),
 }
 
 _lib = None
@@ -271,6 +273,17 @@ class Context:
         d, keep = self.make_step(ids, colliders, gravity, sources, substeps, iterations, h)
         self.step_desc(d)
         del keep
+
+    def set_cloth_variant(self, variant):
+        self._check(self.lib.pxb_context_set_cloth_variant(self.h, variant), "set_cloth_variant")
+
+    def autotune(self, d, trials=3):
+        """Times the kernel variants on step desc `d` (state restored); returns (best, ms list)."""
+        best = C.c_int32()
+        ms = (C.c_float * 3)()
+        self._check(self.lib.pxb_cloths_autotune(self.h, C.byref(d), trials, C.byref(best), ms),
+                    "autotune")
+        return best.value, list(ms)
 
     def read_results(self, ids):
         ids = np.ascontiguousarray(ids, np.uint64)

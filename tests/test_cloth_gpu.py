@@ -2,10 +2,9 @@
 
 Bars: pinned particles equal exactly; every particle within 1e-5 m after one step and within
 1e-3 m after 300 steps. The kernel uses the reference's operation order with IEEE single
-precision and no contraction, so wherever no device-side reduction or transcendental enters
-(every scene here without a gravity source) it is asserted EQUAL to the oracle, value for value.
-With gravity sources the cloth centre is a parallel sum on the device (the reference sums
-sequentially), which is held to the tolerance bars instead.
+precision and no contraction, and the one reduction that feeds the solve (the cloth centre a
+gravity source is evaluated at) is summed in the reference's sequential order, so every scene
+here is also asserted EQUAL to the oracle, value for value.
 """
 import numpy as np
 import pytest

@@ -261,23 +261,6 @@ __device__ __forceinline__ bool solve_pair(float4& pa, float4& pb, float rest, f
     return true;
 }
 
-// Slots of item g of the colour whose segments are segs[sb, se): endpoints la / lb, rest slot
-// rs, lambda slot ls (-1 when the colour keeps none).
-__device__ __forceinline__ void item_slots(const PxbSeg* __restrict__ segs, int sb, int se, int g,
-                                           int& la, int& lb, int& rs, int& ls) {
-    int s = sb;
-    while (s + 1 < se && g >= segs[s + 1].start) ++s;
-    const PxbSeg& q = segs[s];
-    const int i = g - q.start;
-    // magic == 0 marks per_row == 1 (floor(2^32 / 1) + 1 does not fit in 32 bits).
-    const int r = q.magic ? static_cast<int>(__umulhi(static_cast<uint32_t>(i), q.magic)) : i;
-    const int k = i - r * q.per_row;
-    la = q.a_base + r * q.row_stride + k;
-    lb = la + q.d;
-    rs = q.rest_base + i;
-    ls = q.lam_base >= 0 ? q.lam_base + i : -1;
-}
-
 // ------------------------------------------------------------------------------------------
 // Block reductions (warp shuffles, fixed order -> deterministic)
 // ------------------------------------------------------------------------------------------
@@ -492,47 +475,75 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         __syncthreads();
 
         // --- 4b. constraint iterations: colour by colour (cloth_solver.h:256-271) ----------
-        // The segments of a colour form one index space; a thread takes items g and g + T
-        // together so two independent projections are in flight (colours are disjoint).
+        // Per segment the descriptor is read once; a thread takes items i and i + T together so
+        // two independent projections are in flight (a colour's constraints are disjoint).
         // A zero-compliance colour keeps no lambda: with alpha == 0 the multiplier never
         // reaches a position (dlambda = (-c - 0*lambda)/w); only the sign of an exactly-zero
         // correction could differ, which moves no coordinate that is not itself +-0.
         {
             const int iters = sP.iters, n_colours = sC.n_colours;
+            const int4* seg4 = reinterpret_cast<const int4*>(s_seg);
             for (int it = 0; it < iters; ++it) {
                 for (int c = 0; c < n_colours; ++c) {
                     const float alpha = sP.alpha[c];
-                    const int sb = sC.colour_seg[c], se = sC.colour_seg[c + 1];
-                    const int total = sC.colour_total[c];
-                    for (int g = tid; g < total; g += 2 * T) {
-                        int la0, lb0, rs0, ls0, la1 = 0, lb1 = 0, rs1 = 0, ls1 = -1;
-                        item_slots(s_seg, sb, se, g, la0, lb0, rs0, ls0);
-                        const int g1 = g + T;
-                        const bool two = g1 < total;
-                        if (two) item_slots(s_seg, sb, se, g1, la1, lb1, rs1, ls1);
-                        float4 pa0 = pos[la0], pb0 = pos[lb0];
-                        const float r0 = rest[rs0];
-                        const float lam0 = ls0 >= 0 ? U[ls0] : 0.0f;
-                        float4 pa1, pb1;
-                        float r1 = 0.0f, lam1 = 0.0f;
-                        if (two) {
-                            pa1 = pos[la1];
-                            pb1 = pos[lb1];
-                            r1 = rest[rs1];
-                            lam1 = ls1 >= 0 ? U[ls1] : 0.0f;
+                    const int se = sC.colour_seg[c + 1];
+                    for (int sg = sC.colour_seg[c]; sg < se; ++sg) {
+                        const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
+                        const int count_pad = h0.x, shift = h0.y, per_row = h0.z, a_base = h0.w;
+                        const int row_stride = h1.x, d = h1.y, rest_base = h1.z, lam_base = h1.w;
+                        const int mask = (1 << shift) - 1;
+                        if constexpr (kMaxThreads >= 1024) {
+                            // 32 warps supply the parallelism; one item at a time keeps the
+                            // loop inside the 64-register budget of a 1024-thread block.
+                            for (int i = tid; i < count_pad; i += T) {
+                                const int k0 = i & mask;
+                                if (k0 >= per_row) continue;
+                                const int la0 = a_base + (i >> shift) * row_stride + k0;
+                                float4 pa0 = pos[la0], pb0 = pos[la0 + d];
+                                const float lam0 = lam_base >= 0 ? U[lam_base + i] : 0.0f;
+                                float d0 = 0.0f;
+                                if (solve_pair(pa0, pb0, rest[rest_base + i], lam0, alpha, d0)) {
+                                    pos[la0] = pa0;
+                                    pos[la0 + d] = pb0;
+                                    if (lam_base >= 0) U[lam_base + i] = lam0 + d0;
+                                }
+                            }
+                            continue;
                         }
-                        float d0 = 0.0f, d1 = 0.0f;
-                        const bool w0 = solve_pair(pa0, pb0, r0, lam0, alpha, d0);
-                        const bool w1 = two && solve_pair(pa1, pb1, r1, lam1, alpha, d1);
-                        if (w0) {
-                            pos[la0] = pa0;
-                            pos[lb0] = pb0;
-                            if (ls0 >= 0) U[ls0] = lam0 + d0;
-                        }
-                        if (w1) {
-                            pos[la1] = pa1;
-                            pos[lb1] = pb1;
-                            if (ls1 >= 0) U[ls1] = lam1 + d1;
+                        for (int i = tid; i < count_pad; i += 2 * T) {
+                            const int i1 = i + T;
+                            const int k0 = i & mask, k1 = i1 & mask;
+                            const bool v0 = k0 < per_row;
+                            const bool v1 = i1 < count_pad && k1 < per_row;
+                            const int la0 = a_base + (i >> shift) * row_stride + k0;
+                            const int la1 = a_base + (i1 >> shift) * row_stride + k1;
+                            float4 pa0, pb0, pa1, pb1;
+                            float r0 = 0.0f, r1 = 0.0f, lam0 = 0.0f, lam1 = 0.0f;
+                            if (v0) {
+                                pa0 = pos[la0];
+                                pb0 = pos[la0 + d];
+                                r0 = rest[rest_base + i];
+                                if (lam_base >= 0) lam0 = U[lam_base + i];
+                            }
+                            if (v1) {
+                                pa1 = pos[la1];
+                                pb1 = pos[la1 + d];
+                                r1 = rest[rest_base + i1];
+                                if (lam_base >= 0) lam1 = U[lam_base + i1];
+                            }
+                            float d0 = 0.0f, d1 = 0.0f;
+                            const bool w0 = v0 && solve_pair(pa0, pb0, r0, lam0, alpha, d0);
+                            const bool w1 = v1 && solve_pair(pa1, pb1, r1, lam1, alpha, d1);
+                            if (w0) {
+                                pos[la0] = pa0;
+                                pos[la0 + d] = pb0;
+                                if (lam_base >= 0) U[lam_base + i] = lam0 + d0;
+                            }
+                            if (w1) {
+                                pos[la1] = pa1;
+                                pos[la1 + d] = pb1;
+                                if (lam_base >= 0) U[lam_base + i1] = lam1 + d1;
+                            }
                         }
                     }
                     __syncthreads();

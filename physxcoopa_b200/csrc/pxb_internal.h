@@ -10,11 +10,14 @@
 // (cloth_builder.h:128-194) reads and writes CONTIGUOUS float4 runs, so a warp's shared-memory
 // accesses are bank-conflict free for every colour.
 //
-// A colour is a list of affine segments. Constraint i of a segment joins layout slots
-//   la = a_base + r * row_stride + k,  lb = la + d,   r = i / per_row, k = i % per_row
-// and reads its rest length from slot (rest_base + i) and, when the colour is compliant, its
-// lambda from slot (lam_base + i). The host derives the segments from the reference's own
-// constraint lists and refuses the fast path unless they reproduce those lists exactly.
+// A colour is a list of affine segments. Rows of a segment are padded to a power of two,
+// row_pad = 1 << shift; item i of a segment is row r = i >> shift, column k = i & (row_pad - 1),
+// live when k < per_row, and joins layout slots
+//   la = a_base + r * row_stride + k,  lb = la + d
+// reading its rest length from slot rest_base + i and, when the colour is compliant, its lambda
+// from slot lam_base + i (padding slots are never read). The host derives the segments from the
+// reference's own constraint lists and refuses the fast path unless they reproduce those lists
+// exactly.
 #ifndef PXB_INTERNAL_H
 #define PXB_INTERNAL_H
 
@@ -31,15 +34,14 @@
 #define PXB_DEVERR_QUEUE_TIMEOUT 0x4u
 
 struct PxbSeg {
-    int32_t count;      // constraints in this segment
-    int32_t per_row;    // run length
-    uint32_t magic;     // floor(2^32 / per_row) + 1: i / per_row == umulhi(i, magic) for i < 2^16
-    int32_t a_base;     // layout slot of constraint 0's `a`
-    int32_t row_stride; // layout distance between runs
+    int32_t count_pad;  // items including row padding (rows * row_pad)
+    int32_t shift;      // log2(row_pad)
+    int32_t per_row;    // live items per row
+    int32_t a_base;     // layout slot of item 0's `a`
+    int32_t row_stride; // layout distance between rows
     int32_t d;          // lb - la
-    int32_t rest_base;  // rest-length slot of constraint 0
-    int32_t lam_base;   // lambda slot of constraint 0, or -1 when the colour has zero compliance
-    int32_t start;      // index of constraint 0 among all constraints of its colour
+    int32_t rest_base;  // rest-length slot of item 0
+    int32_t lam_base;   // lambda slot of item 0, or -1 when the colour has zero compliance
 };
 
 // Static per-cloth description, device resident, written at registration.
@@ -57,12 +59,11 @@ struct PxbClothDev {
     int32_t n_colours;
     int32_t colour_seg[PXB_MAX_COLOURS + 1]; // colour c = segs [colour_seg[c], colour_seg[c+1])
     int32_t colour_is_bend[PXB_MAX_COLOURS];
-    int32_t colour_total[PXB_MAX_COLOURS];  // constraints per colour
     int32_t n_layout;
     int32_t n_real;
     int32_t columns, rows, Q, S;
     int32_t n_rest_pad;     // multiple of 4
-    int32_t n_lam;          // lambda slots (compliant colours only)
+    int32_t n_lam;          // lambda slots (compliant colours only, padded rows)
     int32_t u_floats;       // floats of the union region (lambdas / velocity scratch)
     int32_t n_anchors;
     int32_t smem_bytes;     // dynamic shared memory this cloth needs

@@ -94,29 +94,23 @@ int count_k(int cols, int c, int need) {
     return top < 0 ? 0 : top / 4 + 1;
 }
 
+// A segment as recognised: `count` live items in rows of `per_row`.
+struct HostSeg {
+    int count, per_row, a_base, row_stride, d;
+};
+
 struct ColourSpec {
     bool bend;
-    std::vector<PxbSeg> segs;  // rest_base / lam_base filled later
+    std::vector<HostSeg> segs;
     int total() const {
         int t = 0;
-        for (const PxbSeg& s : segs) t += s.count;
+        for (const HostSeg& s : segs) t += s.count;
         return t;
     }
 };
 
-PxbSeg seg(int rows_n, int per_row, int a_base, int row_stride, int d) {
-    PxbSeg s{};
-    s.count = rows_n * per_row;
-    s.per_row = per_row;
-    s.a_base = a_base;
-    s.row_stride = row_stride;
-    s.d = d;
-    s.rest_base = 0;
-    s.lam_base = -1;
-    s.start = 0;
-    s.magic = per_row == 1 ? 0u
-                           : static_cast<uint32_t>((0x100000000ull / static_cast<uint64_t>(per_row)) + 1ull);
-    return s;
+HostSeg seg(int rows_n, int per_row, int a_base, int row_stride, int d) {
+    return HostSeg{rows_n * per_row, per_row, a_base, row_stride, d};
 }
 
 // Runs of contiguous layout slots covering the real x of a row: classes 0..3 in order, a run
@@ -240,7 +234,7 @@ bool recognise_grid(const pxb_cloth_desc* d, int Q, int S, std::vector<ColourSpe
             if (bt.begin > bt.end || bt.end > n_list ||
                 static_cast<int>(bt.end - bt.begin) != c.total()) { ok = false; break; }
             for (uint32_t k = bt.begin; k < bt.end; ++k) by_a[list[k].a] = static_cast<int32_t>(k);
-            for (const PxbSeg& s : c.segs) {
+            for (const HostSeg& s : c.segs) {
                 for (int i = 0; i < s.count && ok; ++i) {
                     const int r = i / s.per_row, k = i - r * s.per_row;
                     const int la = s.a_base + r * s.row_stride + k, lb = la + s.d;
@@ -298,7 +292,7 @@ void pxb_context::refresh_layout(ClothEntry& e) {
         const bool has_lam = colour_compliance(e, c) != 0.0f;
         for (int s = e.colour_seg[c]; s < e.colour_seg[c + 1]; ++s) {
             e.segs[s].lam_base = has_lam ? lam : -1;
-            if (has_lam) lam += e.segs[s].count;
+            if (has_lam) lam += e.segs[s].count_pad;
         }
     }
     e.n_lam = lam;
@@ -405,28 +399,48 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.aero_grid = d->n_triangle_indices > 0 ? 1 : 0;
     e.n_triangle_indices = d->n_triangle_indices;
 
-    // --- colours -> segments, rest slots ---
+    // --- colours -> device segments with power-of-two rows, rest slots ---
     e.n_colours = static_cast<int>(cs.size());
     e.colour_seg.assign(e.n_colours + 1, 0);
     e.colour_is_bend.assign(e.n_colours, 0);
     e.colour_batch = colour_batch;
     int rest = 0;
+    size_t ref_pos = 0;
+    int max_colour = 0;
+    std::vector<int32_t> padded_ref;
     for (int c = 0; c < e.n_colours; ++c) {
         e.colour_seg[c] = static_cast<int>(e.segs.size());
         e.colour_is_bend[c] = cs[c].bend ? 1 : 0;
-        int start = 0;
-        for (PxbSeg s : cs[c].segs) {
-            if (s.count >= 65536) return fail(PXB_ERR_TOO_LARGE, "a colour segment exceeds 65535 constraints");
-            s.rest_base = rest;
-            s.start = start;
-            rest += s.count;
-            start += s.count;
-            e.segs.push_back(s);
+        int colour_items = 0;
+        for (const HostSeg& h : cs[c].segs) {
+            int shift = 0;
+            while ((1 << shift) < h.per_row) ++shift;
+            const int row_pad = 1 << shift;
+            const int nrows = h.count / h.per_row;
+            PxbSeg g{};
+            g.count_pad = nrows * row_pad;
+            g.shift = shift;
+            g.per_row = h.per_row;
+            g.a_base = h.a_base;
+            g.row_stride = h.row_stride;
+            g.d = h.d;
+            g.rest_base = rest;
+            g.lam_base = -1;
+            if (g.count_pad >= (1 << 24)) return fail(PXB_ERR_TOO_LARGE, "a colour segment is too large");
+            for (int i = 0; i < g.count_pad; ++i) {
+                const int r = i >> shift, k = i & (row_pad - 1);
+                padded_ref.push_back(k < h.per_row ? rest_ref[ref_pos + static_cast<size_t>(r) * h.per_row + k] : -1);
+            }
+            ref_pos += static_cast<size_t>(h.count);
+            rest += g.count_pad;
+            colour_items += g.count_pad;
+            e.segs.push_back(g);
         }
-        e.colour_total.push_back(start);
+        max_colour = std::max(max_colour, colour_items);
     }
     e.colour_seg[e.n_colours] = static_cast<int>(e.segs.size());
     if (e.segs.size() > PXB_MAX_SEGS) return fail(PXB_ERR_TOO_LARGE, "too many colour segments");
+    rest_ref.swap(padded_ref);
     e.n_rest_pad = (rest + 3) & ~3;
     e.rest_ref = rest_ref;
     e.n_stretch = d->n_stretch;
@@ -439,8 +453,6 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
         e.bend_batch_comp.assign(d->bend_batch_compliance, d->bend_batch_compliance + d->n_bend_batches);
     e.params = d->params;
     e.time = d->time;
-    int max_colour = 0;
-    for (auto& c : cs) max_colour = std::max(max_colour, c.total());
     e.threads = std::min(kClothMaxThreads, std::max(64, ((max_colour + 1) / 2 + 31) & ~31));
     e.tethers.assign(d->tethers, d->tethers + d->n_tethers);
     {
@@ -474,6 +486,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     std::vector<float> rest_h(e.n_rest_pad, 0.0f);
     for (int s = 0; s < rest; ++s) {
         const int32_t r = e.rest_ref[s];
+        if (r < 0) continue;  // row padding
         rest_h[s] = r < static_cast<int32_t>(e.n_stretch) ? d->stretch[r].rest_length
                                                           : d->bend[r - e.n_stretch].rest_length;
     }
@@ -513,7 +526,6 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.n_colours = e.n_colours;
     for (int c = 0; c <= e.n_colours; ++c) e.dev.colour_seg[c] = e.colour_seg[c];
     for (int c = 0; c < e.n_colours; ++c) e.dev.colour_is_bend[c] = e.colour_is_bend[c];
-    for (int c = 0; c < e.n_colours; ++c) e.dev.colour_total[c] = e.colour_total[c];
     e.dev.n_layout = e.n_layout;
     e.dev.n_real = static_cast<int32_t>(n);
     e.dev.columns = e.cols;
@@ -925,8 +937,9 @@ pxb_status pxb_cloth_read_lambdas(pxb_context* ctx, uint64_t id, float* stretch_
         for (int sg = e->colour_seg[c]; sg < e->colour_seg[c + 1]; ++sg) {
             const PxbSeg& g = e->segs[sg];
             if (g.lam_base < 0) continue;
-            for (int i = 0; i < g.count; ++i) {
+            for (int i = 0; i < g.count_pad; ++i) {
                 const int32_t r = e->rest_ref[g.rest_base + i];
+                if (r < 0) continue;  // row padding
                 const float v = lam[g.lam_base + i];
                 if (r < static_cast<int32_t>(e->n_stretch)) { if (stretch_out) stretch_out[r] = v; }
                 else if (bend_out) bend_out[r - e->n_stretch] = v;

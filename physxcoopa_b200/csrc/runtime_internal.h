@@ -31,9 +31,8 @@ struct ClothEntry {
     std::vector<PxbSeg> segs;
     std::vector<int> colour_seg;
     std::vector<int> colour_is_bend;
-    std::vector<int> colour_total;
     std::vector<int32_t> colour_batch;     // colour -> reference batch index in its list
-    std::vector<int32_t> rest_ref;         // rest slot -> stretch index, or n_stretch + bend index
+    std::vector<int32_t> rest_ref;         // rest slot -> stretch index, or n_stretch + bend index (-1 padding)
     int n_rest_pad = 0;
     int n_lam = 0;
     int threads = 64;

@@ -293,7 +293,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                   uint32_t* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ PxbSeg s_seg[PXB_MAX_SEGS];
+    __shared__ __align__(16) PxbSeg s_seg[PXB_MAX_SEGS];
     // Per-cloth scalars live in shared memory and are read at their point of use: held in
     // registers for the whole kernel they would crowd out the particle state (64 registers at
     // 1024 threads).

@@ -33,7 +33,8 @@
 #define PXB_DEVERR_TMA_TIMEOUT 0x2u
 #define PXB_DEVERR_QUEUE_TIMEOUT 0x4u
 
-struct PxbSeg {
+// 16-byte aligned: the kernel reads a descriptor as two 16-byte words.
+struct alignas(16) PxbSeg {
     int32_t count_pad;  // items including row padding (rows * row_pad)
     int32_t shift;      // log2(row_pad)
     int32_t per_row;    // live items per row
@@ -123,6 +124,7 @@ struct PxbFrameResult {
     float time;
 };
 
+static_assert(sizeof(PxbSeg) == 32 && alignof(PxbSeg) == 16, "segment descriptor layout");
 static_assert(sizeof(PxbClothStep) == 184, "per-step record size is part of the staging contract");
 static_assert(sizeof(PxbDevCollider) == 236, "collider snapshot size is part of the staging contract");
 

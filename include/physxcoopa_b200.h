@@ -399,6 +399,73 @@ pxb_status pxb_host_cloth_mutable(pxb_host_cloth* cloth, pxb_particle** particle
                                   pxb_anchor** anchors, pxb_cloth_params** params);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Hair strand sets: mirrors PhysicsWorld::add_strands / step_strands_ (world.h:632-650,       */
+/* 1861-1957) and hair::solve_strands (physxcoopa/hair/strand_solver.h:121-327).                */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Uploads a strand set built by make_strands (strand_builder.h:58-127): strands contiguous,
+ * stretch constraints in the builder's even / odd batches. Refuses an empty set with
+ * PXB_ERR_INVALID_ARGUMENT (add_strands does the same), another layout with
+ * PXB_ERR_UNSUPPORTED, and a strand of more than 32 particles with PXB_ERR_TOO_LARGE. */
+pxb_status pxb_strands_add(pxb_context* ctx, const pxb_strand_set_desc* desc, uint64_t* id_out);
+pxb_status pxb_strands_remove(pxb_context* ctx, uint64_t id);
+pxb_status pxb_strands_set_params(pxb_context* ctx, uint64_t id, const pxb_strand_params* params);
+/* hair::set_strand_roots (strand_builder.h:139-149): every strand's previous root becomes its
+ * current one, then the new targets are written (3 floats per strand; orientations, 4 floats
+ * (x, y, z, w) per strand, may be NULL / shorter to keep the current ones). */
+pxb_status pxb_strands_set_roots(pxb_context* ctx, uint64_t id, const float* positions,
+                                 uint32_t n_positions, const float* orientations,
+                                 uint32_t n_orientations);
+pxb_status pxb_strands_write_particles(pxb_context* ctx, uint64_t id, const pxb_particle* particles,
+                                       uint32_t n);
+pxb_status pxb_strands_read_particles(pxb_context* ctx, uint64_t id, pxb_particle* out, uint32_t n);
+/* Lambdas of the stretch constraints left by the last substep, reference list order. */
+pxb_status pxb_strands_read_lambdas(pxb_context* ctx, uint64_t id, float* out, uint32_t n);
+/* The strand records (root targets), reference layout. */
+pxb_status pxb_strands_read_strands(pxb_context* ctx, uint64_t id, pxb_strand* out, uint32_t n);
+pxb_status pxb_strands_read_time(pxb_context* ctx, uint64_t id, float* time_out);
+
+typedef struct pxb_strand_step_desc {
+    const uint64_t* sets;
+    uint32_t n_sets;
+    const pxb_collider* colliders;
+    const uint32_t* collider_offsets;   /* n_sets + 1; NULL = no colliders */
+    float gravity[3];
+    const pxb_gravity_source* sources;
+    const uint32_t* source_offsets;     /* n_sets + 1; NULL = no sources */
+    uint32_t substeps;
+    uint32_t iterations;
+    float h;
+} pxb_strand_step_desc;
+
+/* Advances every listed set by one solve_strands, gravity evaluated at the centre of the set's
+ * last bounds when it has sources (world.h:1941-1945). */
+pxb_status pxb_strands_step(pxb_context* ctx, const pxb_strand_step_desc* step);
+/* Per-set bounds, max particle speed and time after the last step (synchronizes). */
+pxb_status pxb_strands_read_results(pxb_context* ctx, const uint64_t* sets, uint32_t n,
+                                    pxb_cloth_frame_result* out);
+
+/* Drop-in hair::solve_strands on HOST memory: the set described by `desc` is advanced and its
+ * particles, stretch lambdas and time written back (bounds_out, 6 floats, may be NULL). */
+pxb_status pxb_solve_strands_host(pxb_context* ctx, const pxb_strand_set_desc* desc,
+                                  pxb_particle* particles, pxb_constraint* stretch,
+                                  const pxb_collider* colliders, uint32_t n_colliders,
+                                  const float gravity[3], uint32_t substeps, uint32_t iterations,
+                                  float h, float* time_inout, float* bounds_out);
+
+/* Builder: hair::make_strands (strand_builder.h:58-127) from n_strands polylines of counts[i]
+ * points (3 floats each, packed), one root orientation (x, y, z, w) and particle mass per strand
+ * (either may be NULL: identity / 0.001 kg). */
+typedef struct pxb_host_strands pxb_host_strands;
+pxb_status pxb_host_strands_make(uint32_t n_strands, const uint32_t* counts, const float* points,
+                                 const float* root_orientations, const float* particle_masses,
+                                 const pxb_strand_params* params, pxb_host_strands** out);
+pxb_status pxb_host_strands_destroy(pxb_host_strands* set);
+pxb_status pxb_host_strands_view(pxb_host_strands* set, pxb_strand_set_desc* view_out);
+/* Fills `out` with the reference's StrandParams defaults (physxcoopa/hair/strand.h:96-147). */
+void pxb_strand_params_default(pxb_strand_params* out);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Diagnostics                                                                                  */
 /* ------------------------------------------------------------------------------------------ */
 

@@ -117,6 +117,37 @@ struct PxbClothStep {
     int32_t write_lambdas;
 };
 
+// One registered strand set on the device. Particles are strand-major, 32 slots per strand
+// (slot = strand * 32 + k, k < count[strand] <= 32); slot k's rest length is the one of the
+// stretch constraint (k, k + 1).
+struct PxbStrandDev {
+    float4* pos;               // xyz + inv_mass
+    float4* vel;
+    float4* prv;
+    const float4* rest_local;  // StrandSet::rest_local
+    const float4* rest_offset; // StrandSet::rest_offset
+    const float* rest;
+    const float* wshape;       // pow(1 - k / (count - 1), global_shape_falloff), host-evaluated
+    float* lam;
+    const int32_t* count;
+    const float* roots;        // 16 floats per strand: root pos, root q, pad, prev pos, prev q, pad
+    int* bounds_next;          // 7 order-preserving keys reduced by the step
+    float* bounds_prev;        // last decoded bounds: min xyz, max xyz, max speed^2
+    float* bounds_out;         // where this step's decoded bounds go (same buffer, stream-ordered)
+    int32_t n_strands;
+    int32_t pad_;
+};
+
+// Per set, per step: the prologue of solve_strands (strand_solver.h:127-155) on the host.
+struct PxbStrandStep {
+    float hs, inv_hs, alpha, damping_factor, max_velocity, max_speed2;
+    float air_drag, wind_turbulence, turbulence_amp, thickness, friction;
+    float global_per_substep, local_per_substep, time;
+    float accel[3], gravity[3], gravity_scale, external_acceleration[3], wind[3];
+    int32_t steps, iters, global_shape_on, local_shape_on;
+    int32_t col_begin, col_count, src_begin, src_count;
+};
+
 struct PxbFrameResult {
     float bounds_min[3];
     float bounds_max[3];

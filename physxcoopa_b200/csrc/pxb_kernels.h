@@ -35,6 +35,10 @@ cudaError_t launch_gather_positions(const PxbClothDev* cloths, const int32_t* or
                                     const int64_t* out_offsets, int n_cloths, float* out,
                                     cudaStream_t stream);
 
+cudaError_t launch_strand_step(const PxbStrandDev& d, const PxbStrandStep& p,
+                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                               cudaStream_t stream);
+
 }  // namespace pxb
 
 #endif  // PXB_KERNELS_H

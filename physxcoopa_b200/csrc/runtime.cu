@@ -592,7 +592,7 @@ pxb_status pxb_context::sync_registry() {
 
 // Collider snapshot -> device record with the world-space quantities the reference derives
 // per call (collision::world_sphere / world_obb / world_capsule, shape.h:160-188).
-static void make_dev_collider(const pxb_collider& c, PxbDevCollider& o) {
+void pxb_make_dev_collider(const pxb_collider& c, PxbDevCollider& o) {
     using namespace pxb::hm;
     std::memset(&o, 0, sizeof(o));
     o.type = c.type;
@@ -692,7 +692,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     auto* hs_cols = reinterpret_cast<PxbDevCollider*>(hb + o_cols);
     auto* hs_src = reinterpret_cast<pxb_gravity_source*>(hb + o_src);
     auto* hs_order = reinterpret_cast<int32_t*>(hb + o_order);
-    for (uint32_t k = 0; k < n_col; ++k) make_dev_collider(sd->colliders[k], hs_cols[k]);
+    for (uint32_t k = 0; k < n_col; ++k) pxb_make_dev_collider(sd->colliders[k], hs_cols[k]);
     if (n_src) std::memcpy(hs_src, sd->sources, sizeof(pxb_gravity_source) * n_src);
     int threads = 64, smem = 0;
     const pxb::hm::V3 g = pxb::hm::ld(sd->gravity);
@@ -1043,7 +1043,7 @@ pxb_status pxb_project_particles(pxb_context* ctx, const pxb_collider* collider,
         return PXB_ERR_INVALID_ARGUMENT;
     if (pxb_status s = check_colliders(ctx, collider, 1)) return s;
     PxbDevCollider dc;
-    make_dev_collider(*collider, dc);
+    pxb_make_dev_collider(*collider, dc);
     const size_t o_pts = align256(sizeof(dc)), o_out = o_pts + align256(12 * static_cast<size_t>(n)),
                  o_nrm = o_out + align256(12 * static_cast<size_t>(n)),
                  o_dep = o_nrm + align256(12 * static_cast<size_t>(n)),

@@ -53,6 +53,23 @@ struct ClothEntry {
     bool has_result = false;
 };
 
+// One registered strand set (hair::StrandSet mirrors + device buffers).
+struct StrandEntry {
+    bool alive = false;
+    uint32_t generation = 0;
+    uint32_t n_particles = 0, n_strands = 0, n_stretch = 0;
+    std::vector<uint32_t> first, count;
+    std::vector<pxb_strand> records;       // root targets, host mirror
+    std::vector<int32_t> stretch_slot;     // stretch list index -> device slot
+    std::vector<TopologyEdge> topology;
+    pxb_strand_params params{};
+    float time = 0.0f;
+    void* dmem = nullptr;
+    PxbStrandDev dev{};
+    float bounds[7] = {0, 0, 0, 0, 0, 0, 0};
+    bool has_result = false;
+};
+
 // pxb_solve_cloth_host keeps the registration it made for a caller's arrays.
 struct HostSolveCache {
     const pxb_particle* particles;
@@ -74,11 +91,15 @@ struct pxb_context {
     std::vector<uint64_t> last_step;  // ids of the last step, in launch-slot order
     bool results_fresh = false;
     std::vector<HostSolveCache> host_cache;
+    std::vector<StrandEntry> strand_sets;
+    std::vector<HostSolveCache> strand_cache;
     int cloth_variant = 0;  // kernel block-size cap, see pxb_kernels.h (autotuned or set)
     DevBuf d_tune;          // cloth state saved across an autotune
 
     ~pxb_context() {
         for (ClothEntry& e : cloths)
+            if (e.alive && e.dmem) cudaFree(e.dmem);
+        for (StrandEntry& e : strand_sets)
             if (e.alive && e.dmem) cudaFree(e.dmem);
         for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune})
             if (b->p) cudaFree(b->p);
@@ -102,6 +123,12 @@ struct pxb_context {
     pxb_status step_cloths(const pxb_cloth_step_desc* sd);
     pxb_status check_device_error();
     pxb_status fetch_results();
+    StrandEntry* lookup_strands(uint64_t id);
+    pxb_status upload_strand_records(StrandEntry& e);
+    pxb_status upload_strand_shape(StrandEntry& e);
 };
+
+// Collider snapshot -> device record with the reference's per-call world-space quantities.
+void pxb_make_dev_collider(const pxb_collider& c, PxbDevCollider& o);
 
 #endif  // PXB_RUNTIME_INTERNAL_H

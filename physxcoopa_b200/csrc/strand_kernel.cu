@@ -1,0 +1,333 @@
+// strand_kernel.cu -- the XPBD hair-strand substep on sm_100a: one warp per strand, one lane
+// per particle, the whole strand in registers.
+//
+// Replaces hair::solve_strands (physxcoopa/hair/strand_solver.h:121-327) for sets built by
+// make_strands (strand_builder.h:58-127). Per warp and substep:
+//   1+2 integrate with air drag and the speed clamp          (lane = particle)
+//   3   root lerp                                             (lane 0)
+//   4   stretch, even then odd constraints, `iterations` times: both lanes of a constraint fetch
+//       the other endpoint with a shuffle and evaluate the same projection, each keeping its own
+//       endpoint -- bit-identical on both sides, so nothing is written back
+//   5   global shape toward the root-frame rest pose          (lane = particle)
+//   6   local shape, the reference's serial chain k = 1..n-2, warp-uniform
+//   7   collider projection keeping the deepest contact       (lane = particle)
+//   8   velocities + positional friction                      (lane = particle)
+// Bounds and the largest speed of the whole set are reduced with warp shuffles and combined
+// across warps with integer atomics on an order-preserving float encoding (exact, order-free).
+//
+// Arithmetic follows the reference's operation order in IEEE single precision without
+// contraction. The transcendental calls (sin / acos / cos in the wind gust, slerp and the
+// local-shape rotation) use CUDA's libm, which can differ from the host's by an ulp.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/physxcoopa_b200.h"
+#include "pxb_internal.h"
+#include "pxb_kernels.h"
+#include "pxb_device_math.cuh"
+
+namespace pxb {
+namespace {
+
+constexpr int kWarpsPerBlock = 8;
+
+struct q4 {
+    float x, y, z, w;
+};
+__device__ __forceinline__ q4 mkq(float w, float x, float y, float z) { return q4{x, y, z, w}; }
+
+// Unit-quaternion rotation v + 2*(w*(u x v) + u x (u x v)).
+__device__ __forceinline__ f3 qrot(q4 q, f3 v) {
+    const f3 u = mk(q.x, q.y, q.z);
+    const f3 uv = cross(u, v);
+    const f3 uuv = cross(u, uv);
+    return add(v, mul(add(mul(uv, q.w), uuv), 2.0f));
+}
+__device__ __forceinline__ float mixf(float x, float y, float a) { return x * (1.0f - a) + y * a; }
+__device__ __forceinline__ f3 mixv(f3 x, f3 y, float a) { return add(mul(x, 1.0f - a), mul(y, a)); }
+
+// Shortest-arc slerp with the component-wise lerp when cos(theta) > 1 - FLT_EPSILON.
+__device__ q4 slerp(q4 a, q4 b, float t) {
+    float c = a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
+    if (c < 0.0f) {
+        b = mkq(-b.w, -b.x, -b.y, -b.z);
+        c = -c;
+    }
+    if (c > 1.0f - 1.19209290e-07f)
+        return mkq(mixf(a.w, b.w, t), mixf(a.x, b.x, t), mixf(a.y, b.y, t), mixf(a.z, b.z, t));
+    const float theta = acosf(c);
+    const float sa = sinf((1.0f - t) * theta), sb = sinf(t * theta), sn = sinf(theta);
+    return mkq((sa * a.w + sb * b.w) / sn, (sa * a.x + sb * b.x) / sn, (sa * a.y + sb * b.y) / sn,
+               (sa * a.z + sb * b.z) / sn);
+}
+__device__ __forceinline__ q4 angle_axis(float angle, f3 axis) {
+    const float s = sinf(angle * 0.5f);
+    return mkq(cosf(angle * 0.5f), axis.x * s, axis.y * s, axis.z * s);
+}
+// hair::detail::rotation_between (strand_solver.h:91-105).
+__device__ q4 rotation_between(f3 from, f3 to) {
+    const float d = minr(maxr(dot(from, to), -1.0f), 1.0f);
+    if (d > 0.999999f) return mkq(1.0f, 0.0f, 0.0f, 0.0f);
+    if (d < -0.999999f) {
+        f3 axis = cross(mk(0.0f, 0.0f, 1.0f), from);
+        if (dot(axis, axis) < 1e-8f) axis = cross(mk(1.0f, 0.0f, 0.0f), from);
+        return angle_axis(3.14159265358979323846f, mul(axis, 1.0f / sqrtf(dot(axis, axis))));
+    }
+    const f3 axis = cross(from, to);
+    const float l = len(axis);
+    if (l < 1e-8f) return mkq(1.0f, 0.0f, 0.0f, 0.0f);
+    return angle_axis(acosf(d), divs(axis, l));
+}
+
+__device__ __forceinline__ f3 shfl3(f3 v, int src) {
+    return mk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+              __shfl_sync(0xffffffffu, v.z, src));
+}
+
+// Order-preserving int encoding of a float for atomicMin / atomicMax.
+__device__ __forceinline__ int fkey(float f) {
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+strand_step_kernel(PxbStrandDev D, PxbStrandStep P, const PxbDevCollider* __restrict__ colliders,
+                   const pxb_gravity_source* __restrict__ sources) {
+    const int lane = threadIdx.x & 31;
+    const int strand = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    if (strand >= D.n_strands) return;  // whole warp exits together
+    const int count = __ldg(&D.count[strand]);
+    const int slot = strand * 32 + lane;
+    const bool live = lane < count;
+
+    // --- gravity: uniform, or the source field at the set's last bounds centre (world.h:1941) --
+    f3 accel = mk(P.accel[0], P.accel[1], P.accel[2]);
+    if (P.src_count > 0) {
+        const float* b = D.bounds_prev;
+        const f3 bmin = mk(b[0], b[1], b[2]), bmax = mk(b[3], b[4], b[5]);
+        const f3 centre = smul(0.5f, add(bmin, bmax));
+        float best = 0.0f;
+        f3 pull = mk(P.gravity[0], P.gravity[1], P.gravity[2]);
+        bool found = false;
+        for (int k = 0; k < P.src_count; ++k) {
+            const pxb_gravity_source* g = &sources[P.src_begin + k];
+            const f3 d = sub(ld3(g->centre), centre);
+            const float r = len(d);
+            const float range = __ldg(&g->range), radius = __ldg(&g->radius), strength = __ldg(&g->strength);
+            if (range > 0.0f && r > range) continue;
+            if (r < 1e-6f) continue;
+            const float a = r <= radius ? strength : strength * (radius / r) * (radius / r);
+            if (!found || a > best) {
+                best = a;
+                pull = mul(divs(d, r), a);
+                found = true;
+            }
+        }
+        accel = add(mul(pull, P.gravity_scale), mk(P.external_acceleration[0], P.external_acceleration[1],
+                                                   P.external_acceleration[2]));
+    }
+
+    float4 p4 = live ? D.pos[slot] : make_float4(0, 0, 0, 0);
+    f3 p = xyz(p4);
+    const float w = p4.w;
+    f3 v = live ? xyz(D.vel[slot]) : mk(0, 0, 0);
+    f3 prev = live ? xyz(D.prv[slot]) : mk(0, 0, 0);
+    const f3 rest_local = live ? xyz(D.rest_local[slot]) : mk(0, 0, 0);
+    const f3 rest_offset = live ? xyz(D.rest_offset[slot]) : mk(0, 0, 0);
+    const float rest_next = live ? __ldg(&D.rest[slot]) : 0.0f;   // constraint (lane, lane + 1)
+    const float wshape = live ? __ldg(&D.wshape[slot]) : 0.0f;     // pow(1 - along, falloff)
+    const float* rr = D.roots + 16 * static_cast<size_t>(strand);
+    const f3 root_pos = mk(__ldg(rr + 0), __ldg(rr + 1), __ldg(rr + 2));
+    const q4 root_q = q4{__ldg(rr + 3), __ldg(rr + 4), __ldg(rr + 5), __ldg(rr + 6)};
+    const f3 prev_root_pos = mk(__ldg(rr + 8), __ldg(rr + 9), __ldg(rr + 10));
+    const q4 prev_root_q = q4{__ldg(rr + 11), __ldg(rr + 12), __ldg(rr + 13), __ldg(rr + 14)};
+    float lam = 0.0f;
+    float time = P.time;
+    const f3 wind0 = mk(P.wind[0], P.wind[1], P.wind[2]);
+
+    for (int step = 0; step < P.steps; ++step) {
+        const float t = static_cast<float>(step + 1) / static_cast<float>(P.steps);
+        // --- 1 + 2: aerodynamics and integration (strand_solver.h:162-189) --------------
+        if (live && w > 0.0f) {
+            f3 a = accel;
+            if (P.air_drag > 0.0f) {
+                f3 wind = wind0;
+                if (P.wind_turbulence > 0.0f) {
+                    const float phase = time * 2.3f + p.x * 1.7f + p.y * 2.1f + p.z * 1.3f;
+                    const f3 gust = mk(sinf(phase), sinf(phase * 1.37f + 2.1f), sinf(phase * 0.81f + 4.2f));
+                    wind = add(wind, smul(P.turbulence_amp, gust));
+                }
+                a = add(a, mul(sub(wind, v), P.air_drag));
+            }
+            v = add(v, mul(a, P.hs));
+            v = mul(v, P.damping_factor);
+            const float v2 = dot(v, v);
+            if (v2 > P.max_speed2) v = mul(v, P.max_velocity / sqrtf(v2));
+            prev = p;
+            p = add(p, mul(v, P.hs));
+        }
+        // --- 3: roots (strand_solver.h:194-201) ------------------------------------------
+        if (lane == 0 && count > 0) {
+            prev = p;
+            p = mixv(prev_root_pos, root_pos, t);
+            v = mk(0.0f, 0.0f, 0.0f);
+        }
+        // --- 4: stretch, even then odd batch (strand_solver.h:204-211) ---------------------
+        lam = 0.0f;
+        for (int it = 0; it < P.iters; ++it) {
+            for (int parity = 0; parity < 2; ++parity) {
+                // Lane k is endpoint `a` of constraint k (k -> k+1) when k has this parity, and
+                // endpoint `b` of constraint k-1 when k-1 has it.
+                const bool is_a = live && lane + 1 < count && (lane & 1) == parity;
+                const bool is_b = live && lane >= 1 && ((lane - 1) & 1) == parity;
+                const f3 up = shfl3(p, min(lane + 1, 31));
+                const float w_up = __shfl_sync(0xffffffffu, w, min(lane + 1, 31));
+                const f3 dn = shfl3(p, max(lane - 1, 0));
+                const float w_dn = __shfl_sync(0xffffffffu, w, max(lane - 1, 0));
+                const float rest_dn = __shfl_sync(0xffffffffu, rest_next, max(lane - 1, 0));
+                const float lam_dn = __shfl_sync(0xffffffffu, lam, max(lane - 1, 0));
+                float4 pa, pb;
+                float rest, lam_c;
+                if (is_a) {
+                    pa = make_float4(p.x, p.y, p.z, w);
+                    pb = make_float4(up.x, up.y, up.z, w_up);
+                    rest = rest_next;
+                    lam_c = lam;
+                } else {
+                    pa = make_float4(dn.x, dn.y, dn.z, w_dn);
+                    pb = make_float4(p.x, p.y, p.z, w);
+                    rest = rest_dn;
+                    lam_c = lam_dn;
+                }
+                float dl = 0.0f;
+                if ((is_a || is_b) && solve_pair(pa, pb, rest, lam_c, P.alpha, dl)) {
+                    if (is_a) {
+                        p = xyz(pa);
+                        lam = lam_c + dl;
+                    } else {
+                        p = xyz(pb);
+                    }
+                }
+            }
+        }
+        // --- 5: global shape (strand_solver.h:216-235) -----------------------------------
+        if (P.global_shape_on && count >= 2) {
+            const q4 orientation = slerp(prev_root_q, root_q, t);
+            const f3 root = mixv(prev_root_pos, root_pos, t);
+            if (live && lane >= 1 && w > 0.0f) {
+                const float weight = P.global_per_substep * wshape;
+                if (weight > 0.0f) {
+                    const f3 target = add(root, qrot(orientation, rest_local));
+                    p = mixv(p, target, minr(weight, 1.0f));
+                }
+            }
+        }
+        // --- 6: local shape, the serial chain (strand_solver.h:241-272) -------------------
+        if (P.local_shape_on && count >= 3) {
+            for (int k = 1; k + 1 < count; ++k) {
+                const f3 pp = shfl3(p, k - 1), pc = shfl3(p, k), pn = shfl3(p, k + 1);
+                const f3 ro_c = shfl3(rest_offset, k), ro_n = shfl3(rest_offset, k + 1);
+                const float wc = __shfl_sync(0xffffffffu, w, k), wn = __shfl_sync(0xffffffffu, w, k + 1);
+                const f3 live_prev = sub(pc, pp);
+                const float rest_len = len(ro_c);
+                const float live_len = len(live_prev);
+                if (rest_len <= 1e-8f || live_len <= 1e-8f) continue;
+                const q4 turn = rotation_between(divs(ro_c, rest_len), divs(live_prev, live_len));
+                const f3 target = add(pc, qrot(turn, ro_n));
+                const f3 delta = mul(sub(target, pn), P.local_per_substep);
+                const float ws = wc + wn;
+                if (ws <= 0.0f) continue;
+                if (lane == k + 1) p = add(p, mul(delta, wn / ws));
+                if (lane == k) p = sub(p, mul(delta, wc / ws));
+            }
+        }
+        // --- 7: collisions, deepest contact kept (strand_solver.h:275-298) ---------------
+        bool contacted = false;
+        f3 cn = mk(0.0f, 0.0f, 0.0f);
+        float cd = 0.0f;
+        if (live && w > 0.0f) {
+            for (int k = 0; k < P.col_count; ++k) {
+                f3 n = mk(0.0f, 0.0f, 0.0f);
+                float depth = 0.0f;
+                if (!project_particle(&colliders[P.col_begin + k], P.thickness, p, n, depth)) continue;
+                if (!contacted || depth > cd) {
+                    cn = n;
+                    cd = depth;
+                }
+                contacted = true;
+            }
+        }
+        // --- 8: finalize + positional friction (strand_solver.h:301-321) ----------------
+        if (live && w > 0.0f) {
+            v = mul(sub(p, prev), P.inv_hs);
+            if (contacted && P.friction > 0.0f) {
+                const f3 motion = sub(p, prev);
+                const f3 tangential = sub(motion, mul(cn, dot(motion, cn)));
+                const float t_len = len(tangential);
+                if (t_len > PXB_EPSILON) {
+                    const float limit = P.friction * cd;
+                    const float scale = maxr(0.0f, 1.0f - minr(limit, t_len) / t_len);
+                    p = sub(p, mul(tangential, 1.0f - scale));
+                    v = mul(sub(p, prev), P.inv_hs);
+                }
+            }
+        }
+        time = time + P.hs;
+    }
+
+    if (live) {
+        D.pos[slot] = make_float4(p.x, p.y, p.z, w);
+        D.vel[slot] = make_float4(v.x, v.y, v.z, 0.0f);
+        D.prv[slot] = make_float4(prev.x, prev.y, prev.z, 0.0f);
+        D.lam[slot] = lam;
+    }
+    // --- set bounds and largest speed (strand.h:195-211) ---------------------------------
+    float r[7];
+    r[0] = live ? p.x : 3.402823466e+38f;
+    r[1] = live ? p.y : 3.402823466e+38f;
+    r[2] = live ? p.z : 3.402823466e+38f;
+    r[3] = live ? p.x : -3.402823466e+38f;
+    r[4] = live ? p.y : -3.402823466e+38f;
+    r[5] = live ? p.z : -3.402823466e+38f;
+    r[6] = live ? dot(v, v) : 0.0f;
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int k = 0; k < 3; ++k) r[k] = fminf(r[k], __shfl_xor_sync(0xffffffffu, r[k], o));
+        for (int k = 3; k < 7; ++k) r[k] = fmaxf(r[k], __shfl_xor_sync(0xffffffffu, r[k], o));
+    }
+    if (lane == 0) {
+        for (int k = 0; k < 3; ++k) atomicMin(&D.bounds_next[k], fkey(r[k]));
+        for (int k = 3; k < 7; ++k) atomicMax(&D.bounds_next[k], fkey(r[k]));
+    }
+}
+
+// Sets the 7 reduction keys of a bounds buffer to their identities.
+__global__ void strand_bounds_reset_kernel(int* keys) {
+    const int k = threadIdx.x;
+    if (k < 3) keys[k] = fkey(3.402823466e+38f);
+    else if (k < 6) keys[k] = fkey(-3.402823466e+38f);
+    else if (k == 6) keys[k] = fkey(0.0f);
+}
+
+// Decodes a bounds buffer's keys into floats (min xyz, max xyz, max speed^2).
+__global__ void strand_bounds_decode_kernel(const int* keys, float* out) {
+    const int k = threadIdx.x;
+    if (k < 7) {
+        const int i = keys[k];
+        out[k] = __int_as_float(i >= 0 ? i : i ^ 0x7fffffff);
+    }
+}
+
+cudaError_t launch_strand_step(const PxbStrandDev& d, const PxbStrandStep& p,
+                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                               cudaStream_t stream) {
+    strand_bounds_reset_kernel<<<1, 32, 0, stream>>>(d.bounds_next);
+    const int blocks = (d.n_strands + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (blocks > 0)
+        strand_step_kernel<<<blocks, kWarpsPerBlock * 32, 0, stream>>>(d, p, colliders, sources);
+    strand_bounds_decode_kernel<<<1, 32, 0, stream>>>(d.bounds_next, d.bounds_out);
+    return cudaGetLastError();
+}
+
+}  // namespace pxb

@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 from . import _abi as A
-from .arrays import ClothArrays
+from .arrays import ClothArrays, StrandArrays
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libphysxcoopa_b200.so")
 
@@ -56,6 +56,23 @@ SIGNATURES = {
     "pxb_host_cloth_mutable": ([P, C.POINTER(P), C.POINTER(P), C.POINTER(P)], C.c_int),
     "pxb_measure_smem_bandwidth": ([P, C.POINTER(C.c_double)], C.c_int),
     "pxb_context_set_cloth_variant": ([P, C.c_int32], C.c_int),
+    "pxb_strands_add": ([P, C.POINTER(A.StrandSetDesc), C.POINTER(u64)], C.c_int),
+    "pxb_strands_remove": ([P, u64], C.c_int),
+    "pxb_strands_set_params": ([P, u64, C.POINTER(A.StrandParams)], C.c_int),
+    "pxb_strands_set_roots": ([P, u64, P, u32, P, u32], C.c_int),
+    "pxb_strands_write_particles": ([P, u64, P, u32], C.c_int),
+    "pxb_strands_read_particles": ([P, u64, P, u32], C.c_int),
+    "pxb_strands_read_lambdas": ([P, u64, P, u32], C.c_int),
+    "pxb_strands_read_strands": ([P, u64, P, u32], C.c_int),
+    "pxb_strands_read_time": ([P, u64, f32p], C.c_int),
+    "pxb_strands_step": ([P, C.POINTER(A.StrandStepDesc)], C.c_int),
+    "pxb_strands_read_results": ([P, P, u32, P], C.c_int),
+    "pxb_solve_strands_host": ([P, C.POINTER(A.StrandSetDesc), P, P, P, u32, f32p, u32, u32, f32, f32p,
+                                f32p], C.c_int),
+    "pxb_host_strands_make": ([u32, P, P, P, P, C.POINTER(A.StrandParams), C.POINTER(P)], C.c_int),
+    "pxb_host_strands_destroy": ([P], C.c_int),
+    "pxb_host_strands_view": ([P, C.POINTER(A.StrandSetDesc)], C.c_int),
+    "pxb_strand_params_default": ([C.POINTER(A.StrandParams)], None),
     "pxb_cloths_autotune": ([P, C.POINTER(A.ClothStepDesc), u32, C.POINTER(C.c_int32), P], C.c_int),
 }
 
@@ -127,6 +144,43 @@ class HostCloth:
         v = A.ClothDesc()
         library().pxb_host_cloth_view(self._h, C.byref(v))
         return ClothArrays.from_desc(v)
+
+
+def make_strands(polylines, params=None, root_orientations=None, particle_masses=None) -> StrandArrays:
+    """hair::make_strands (strand_builder.h:58-127) through the library's host builder."""
+    counts = np.array([len(p) for p in polylines], np.uint32)
+    pts = (np.ascontiguousarray(np.concatenate([np.asarray(p, np.float32).reshape(-1, 3) for p in polylines]),
+                                np.float32) if len(polylines) else np.zeros((0, 3), np.float32))
+    rot = None if root_orientations is None else np.ascontiguousarray(root_orientations, np.float32)
+    mass = None if particle_masses is None else np.ascontiguousarray(particle_masses, np.float32)
+    params = params if params is not None else A.StrandParams.defaults()
+    h = P()
+    lib = library()
+    st = lib.pxb_host_strands_make(len(counts), A.ptr(counts), A.ptr(pts), A.ptr(rot), A.ptr(mass),
+                                   C.byref(params), C.byref(h))
+    if st:
+        raise PxbError(st, "make_strands failed")
+    try:
+        v = A.StrandSetDesc()
+        lib.pxb_host_strands_view(h, C.byref(v))
+
+        def grab(addr, n, dtype):
+            if n == 0 or not addr:
+                return np.zeros(0, dtype)
+            return np.frombuffer(bytes((C.c_char * (n * dtype.itemsize)).from_address(addr)), dtype).copy()
+        n = v.n_particles
+        f = np.dtype("<f4")
+        p = A.StrandParams()
+        C.pointer(p)[0] = v.params
+        return StrandArrays(particles=grab(v.particles, n, A.PARTICLE),
+                            stretch=grab(v.stretch, v.n_stretch, A.CONSTRAINT),
+                            stretch_batches=grab(v.stretch_batches, v.n_stretch_batches, A.BATCH),
+                            rest_local=grab(v.rest_local, 3 * n, f).reshape(-1, 3),
+                            rest_offset=grab(v.rest_offset, 3 * n, f).reshape(-1, 3),
+                            strands=grab(v.strands, v.n_strands, A.STRAND), params=p, time=0.0,
+                            bounds=None)
+    finally:
+        lib.pxb_host_strands_destroy(h)
 
 
 def make_grid_cloth(columns, rows, width, height, **kw) -> ClothArrays:
@@ -312,6 +366,92 @@ class Context:
                                                    A.ptr(out), A.ptr(nrm), A.ptr(dep), A.ptr(hit)),
                     "project_particles")
         return hit, out, nrm, dep
+
+    # --- strand sets ----------------------------------------------------------------------
+    def add_strands(self, s: StrandArrays) -> int:
+        d = s.desc()
+        out = u64()
+        self._check(self.lib.pxb_strands_add(self.h, C.byref(d), C.byref(out)), "add_strands")
+        return out.value
+
+    def remove_strands(self, sid):
+        self._check(self.lib.pxb_strands_remove(self.h, sid), "remove_strands")
+
+    def set_strand_params(self, sid, params):
+        self._check(self.lib.pxb_strands_set_params(self.h, sid, C.byref(params)), "set_strand_params")
+
+    def set_strand_roots(self, sid, positions, orientations=None):
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        rot = None if orientations is None else np.ascontiguousarray(orientations, np.float32).reshape(-1, 4)
+        self._check(self.lib.pxb_strands_set_roots(self.h, sid, A.ptr(pos), len(pos), A.ptr(rot),
+                                                   0 if rot is None else len(rot)), "set_strand_roots")
+
+    def read_strand_particles(self, sid, n):
+        out = np.zeros(n, A.PARTICLE)
+        self._check(self.lib.pxb_strands_read_particles(self.h, sid, A.ptr(out), n), "read_strand_particles")
+        return out
+
+    def write_strand_particles(self, sid, particles):
+        p = np.ascontiguousarray(particles, A.PARTICLE)
+        self._check(self.lib.pxb_strands_write_particles(self.h, sid, A.ptr(p), len(p)), "write_strand_particles")
+
+    def read_strand_lambdas(self, sid, n):
+        out = np.zeros(n, np.float32)
+        self._check(self.lib.pxb_strands_read_lambdas(self.h, sid, A.ptr(out) if n else None, n),
+                    "read_strand_lambdas")
+        return out
+
+    def read_strand_time(self, sid):
+        t = f32()
+        self._check(self.lib.pxb_strands_read_time(self.h, sid, C.byref(t)), "read_strand_time")
+        return t.value
+
+    def make_strand_step(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
+                         iterations=4, h=1.0 / 60.0):
+        ids = np.ascontiguousarray(ids, np.uint64)
+        n = len(ids)
+        cols, coff = _flatten(colliders, A.COLLIDER, n)
+        src, soff = _flatten(sources, A.GRAVITY_SOURCE, n)
+        d = A.StrandStepDesc()
+        d.sets = A.ptr(ids)
+        d.n_sets = n
+        d.colliders = A.ptr(cols)
+        d.collider_offsets = A.ptr(coff)
+        d.gravity = _vec(gravity)
+        d.sources = A.ptr(src)
+        d.source_offsets = A.ptr(soff)
+        d.substeps, d.iterations, d.h = substeps, iterations, h
+        return d, (ids, cols, coff, src, soff)
+
+    def step_strands(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
+                     iterations=4, h=1.0 / 60.0):
+        d, keep = self.make_strand_step(ids, colliders, gravity, sources, substeps, iterations, h)
+        self._check(self.lib.pxb_strands_step(self.h, C.byref(d)), "strands_step")
+        del keep
+
+    def step_strands_desc(self, d):
+        self._check(self.lib.pxb_strands_step(self.h, C.byref(d)), "strands_step")
+
+    def read_strand_results(self, ids):
+        ids = np.ascontiguousarray(ids, np.uint64)
+        out = np.zeros(len(ids), A.FRAME_RESULT)
+        self._check(self.lib.pxb_strands_read_results(self.h, A.ptr(ids), len(ids), A.ptr(out)),
+                    "read_strand_results")
+        return out
+
+    def solve_strands_host(self, s: StrandArrays, colliders=None, gravity=(0, 0, -9.81), substeps=4,
+                           iterations=4, h=1.0 / 60.0):
+        """The drop-in solve_strands on host arrays: advances `s` in place."""
+        d = s.desc()
+        cols = colliders if colliders is not None else np.zeros(0, A.COLLIDER)
+        t = f32(s.time)
+        b = (C.c_float * 6)()
+        self._check(self.lib.pxb_solve_strands_host(self.h, C.byref(d), A.ptr(s.particles), A.ptr(s.stretch),
+                                                    A.ptr(cols), len(cols), _vec(gravity), substeps,
+                                                    iterations, h, C.byref(t), b), "solve_strands_host")
+        s.time = t.value
+        s.bounds = np.array(b[:], np.float32)
+        return s
 
     def solve_cloth_host(self, c: ClothArrays, colliders=None, gravity=(0, 0, -9.81), substeps=4,
                          iterations=10, h=1.0 / 60.0):

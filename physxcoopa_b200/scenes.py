@@ -143,3 +143,54 @@ def uneven_batch(n=4096, lo=16, hi=128, seed=2, max_side=None):
             srcs.append(None)
     return ClothScene(f"uneven_batch {n} sides U{{{lo}..{hi}}}", cloths, cols, sources=srcs,
                       meta={"n": n, "lo": lo, "hi": hi})
+
+
+@dataclass
+class StrandScene:
+    name: str
+    sets: list
+    colliders: List[np.ndarray]
+    root_path: object = None  # callable(frame) -> (positions (n, 3), orientations or None)
+    gravity: tuple = (0.0, 0.0, -9.81)
+    substeps: int = 4
+    iterations: int = 20
+    h: float = 1.0 / 60.0
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def particles(self):
+        return sum(len(s.particles) for s in self.sets)
+
+
+def hair_groom(n_strands=65536, count=32, segment=0.01, seed=3, iterations=20):
+    """65,536 strands of 32 particles, 1 cm segments, rooted on a sphere of radius 0.1 m (seeded
+    directions) and growing outward; one sphere collider (the head) rides with the roots, whose
+    centre follows a seeded 0.2 m, 1 Hz sinusoid. Stretch plus the reference's global and local
+    shape constraints (its strand "bending"), reference StrandParams defaults otherwise."""
+    from .runtime import make_strands
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n_strands, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d[:, 2] = np.abs(d[:, 2])  # upper hemisphere
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    head_r = 0.1
+    roots = (d * head_r).astype(np.float32)
+    k = np.arange(count, dtype=np.float32)[None, :, None]
+    pts = (roots[:, None, :] + d[:, None, :] * (segment * k)).astype(np.float32)
+    s = make_strands(list(pts))
+    phase = float(rng.uniform(0, 2 * np.pi))
+    amp_dir = rng.normal(size=3).astype(np.float32)
+    amp_dir /= np.linalg.norm(amp_dir)
+
+    def centre(frame, h=1.0 / 60.0):
+        return (0.2 * np.sin(2 * np.pi * 1.0 * frame * h + phase) * amp_dir).astype(np.float32)
+
+    def root_path(frame):
+        return (roots + centre(frame)[None, :]).astype(np.float32), None
+
+    def colliders(frame):
+        return collider_array([sphere(head_r * 0.95, tuple(centre(frame)))])
+
+    return StrandScene(f"hair_groom {n_strands}x{count}", [s], [colliders(0)], root_path=root_path,
+                       iterations=iterations,
+                       meta={"n_strands": n_strands, "count": count, "colliders_at": colliders})

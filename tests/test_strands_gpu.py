@@ -1,0 +1,170 @@
+"""Parity of the device strand solver with the oracle (oracle/xpbd_oracle.c, solve_strands).
+
+Stages without a transcendental call run in the reference's operation order in IEEE single
+precision, and scenes that only use those (no local shape, no turning root, no wind) are asserted
+EQUAL to the oracle. The local-shape rotation (acos / sin / cos) and the slerp of a turning root
+use CUDA's libm, which may differ from the host's by an ulp; those scenes are held to the bars:
+within 1e-5 m after one step and 1e-3 m after many.
+"""
+import numpy as np
+import pytest
+
+from physxcoopa_b200 import _abi as A
+from physxcoopa_b200 import runtime as R
+from physxcoopa_b200 import scenes
+from physxcoopa_b200.arrays import box, capsule, collider_array, gravity_sources, sphere
+
+import _checkers as K
+from test_strands_oracle_ref import bent, params, straight
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = R.Context(0)
+    yield c
+    c.close()
+
+
+def maxdiff(a, b):
+    return float(np.max(np.abs(a.astype(np.float64) - b.astype(np.float64)))) if a.size else 0.0
+
+
+def run_pair(ctx, s, steps, cols=None, sources=None, iters=4, roots=None):
+    orc = s.copy()
+    sid = ctx.add_strands(s)
+    try:
+        for f in range(steps):
+            if roots is not None:
+                pos, rot = roots(f)
+                ctx.set_strand_roots(sid, pos, rot)
+                K.oracle_set_strand_roots(orc, pos, rot)
+            ctx.step_strands([sid], None if cols is None else [cols],
+                             sources=None if sources is None else [sources], iterations=iters)
+            K.oracle_step_strands(orc, cols, sources=sources, iterations=iters)
+        gpu = ctx.read_strand_particles(sid, len(s.particles))
+        lam = ctx.read_strand_lambdas(sid, len(s.stretch))
+        res = ctx.read_strand_results([sid])[0]
+        t = ctx.read_strand_time(sid)
+    finally:
+        ctx.remove_strands(sid)
+    return gpu, orc, lam, res, t
+
+
+EXACT = {
+    "hanging_no_shape": dict(lines=[straight((0, 0, 0), 10)], p=params(global_shape=0.0, local_shape=0.0)),
+    "global_shape_only": dict(lines=[straight((0, 0, 0), 9), straight((0, 0.1, 0), 32)],
+                              p=params(global_shape=0.5, global_shape_falloff=2.0, local_shape=0.0)),
+    "collider_drape": dict(lines=[straight((0, 0, 0.6), 12)], p=params(global_shape=0.0, local_shape=0.0, thickness=0.02),
+                           cols=[sphere(0.3)]),
+    "three_colliders": dict(lines=[straight((0.02 * i, 0, 0.5), 10) for i in range(5)], p=params(local_shape=0.0),
+                            cols=[sphere(0.2, (0.1, 0, 0.2)), capsule(0.1, 0.3, (0.2, 0.0, 0.3), axis=1),
+                                  box((0.2, 0.2, 0.05), (0.1, 0.0, 0.1))]),
+    "compliant": dict(lines=[straight((0, 0, 0), 16)], p=params(stretch_compliance=1e-5, local_shape=0.0), iters=7),
+    "short_and_single": dict(lines=[straight((0, 0, 0), 2), straight((0, 0.2, 0), 3)], p=params(local_shape=0.0)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(EXACT))
+def test_exact_scenes_equal_oracle(ctx, name):
+    sc = EXACT[name]
+    s = R.make_strands(sc["lines"], sc["p"])
+    cols = collider_array(sc["cols"]) if "cols" in sc else None
+    gpu, orc, lam, res, t = run_pair(ctx, s, 40, cols, iters=sc.get("iters", 4))
+    for f in ("position", "velocity", "prev_position", "inv_mass"):
+        assert np.array_equal(gpu[f], orc.particles[f]), f"{f}: {maxdiff(gpu[f], orc.particles[f])}"
+    assert np.array_equal(lam, orc.stretch["lambda"])
+    assert np.float32(t) == np.float32(orc.time)
+    assert np.array_equal(res["bounds_min"], orc.bounds[:3]) and np.array_equal(res["bounds_max"], orc.bounds[3:])
+
+
+TOLERANT = {
+    "defaults": dict(lines=[straight((0, 0, 0))], p=params()),
+    "local_shape_curl": dict(lines=[bent((0, 0, 0))], p=params(global_shape=0.0, local_shape=0.9)),
+    "wind_turbulence": dict(lines=[straight((0, 0.02 * i, 0)) for i in range(4)],
+                            p=params(wind=(1.0, 0.5, 0.0), wind_turbulence=0.7)),
+    "many_with_collider": dict(lines=[straight((0.01 * i, 0.01 * (i % 7), 0.35), 32) for i in range(64)],
+                               p=params(), cols=[sphere(0.3)]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(TOLERANT))
+def test_transcendental_scenes_within_bars(ctx, name):
+    sc = TOLERANT[name]
+    s = R.make_strands(sc["lines"], sc["p"])
+    cols = collider_array(sc["cols"]) if "cols" in sc else None
+    gpu, orc, _, _, _ = run_pair(ctx, s, 1, cols)
+    assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-5
+    roots = orc.particles["inv_mass"] == 0
+    assert np.array_equal(gpu["position"][roots], orc.particles["position"][roots])
+    gpu, orc, _, _, _ = run_pair(ctx, s, 300, cols)
+    assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-3
+    assert np.array_equal(gpu["position"][roots], orc.particles["position"][roots])
+
+
+def test_moving_and_turning_roots(ctx):
+    s = R.make_strands([straight((0, 0, 0)), straight((0, 0.3, 0), 20)], params(global_shape=0.4))
+
+    def roots(f):
+        ang = 0.01 * f
+        pos = np.array([[0.01 * f, 0, 0], [0.01 * f, 0.3, 0]], np.float32)
+        rot = np.array([[0, 0, np.sin(ang / 2), np.cos(ang / 2)]] * 2, np.float32)
+        return pos, rot
+    gpu, orc, _, _, _ = run_pair(ctx, s, 120, roots=roots, iters=1)
+    assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-3
+    assert abs(gpu["position"][0][0] - 1.19) < 1e-3
+
+
+def test_gravity_source_at_bounds_centre(ctx):
+    s = R.make_strands([straight((0.05 * i, 0, 0), 12) for i in range(6)], params(local_shape=0.0))
+    src = gravity_sources([((0.5, 0.3, -1.0), 9.81, 0.5, 10.0)])
+    gpu, orc, _, _, _ = run_pair(ctx, s, 60, sources=src)
+    assert np.array_equal(gpu["position"], orc.particles["position"])
+
+
+def test_drop_in_solve_strands_on_host_arrays(ctx):
+    mine = R.make_strands([straight((0, 0, 0.5), 12) for _ in range(3)], params(local_shape=0.0))
+    orc = mine.copy()
+    col = collider_array([sphere(0.3)])
+    for _ in range(20):
+        ctx.solve_strands_host(mine, col)
+        K.oracle_step_strands(orc, col)
+    assert np.array_equal(mine.particles["position"], orc.particles["position"])
+    assert np.array_equal(mine.stretch["lambda"], orc.stretch["lambda"])
+    assert np.float32(mine.time) == np.float32(orc.time)
+
+
+def test_refusals(ctx):
+    long = R.make_strands([straight((0, 0, 0), 40)])
+    with pytest.raises(R.PxbError) as e:
+        ctx.add_strands(long)
+    assert e.value.status == 7
+    ok = R.make_strands([straight((0, 0, 0))])
+    odd = ok.copy()
+    odd.stretch = odd.stretch[::-1].copy()
+    with pytest.raises(R.PxbError) as e:
+        ctx.add_strands(odd)
+    assert e.value.status == 2
+    sid = ctx.add_strands(ok)
+    ctx.remove_strands(sid)
+    with pytest.raises(R.PxbError) as e:
+        ctx.step_strands([sid])
+    assert e.value.status == 5
+
+
+def test_groom_sample_runs_and_keeps_roots(ctx):
+    sc = scenes.hair_groom(n_strands=2048, iterations=20)
+    s = sc.sets[0]
+    orc = s.copy()
+    sid = ctx.add_strands(s)
+    for f in range(3):
+        pos, rot = sc.root_path(f)
+        ctx.set_strand_roots(sid, pos, rot)
+        K.oracle_set_strand_roots(orc, pos, rot)
+        cols = sc.meta["colliders_at"](f)
+        ctx.step_strands([sid], [cols], iterations=sc.iterations)
+        K.oracle_step_strands(orc, cols, iterations=sc.iterations)
+    gpu = ctx.read_strand_particles(sid, len(s.particles))
+    assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-4
+    ctx.remove_strands(sid)

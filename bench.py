@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--workload", default="uniform_batch",
-                    choices=["uniform_batch", "single_drape", "uneven_batch"])
+                    choices=["uniform_batch", "single_drape", "uneven_batch", "hair_groom"])
     ap.add_argument("--cloths", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -190,6 +190,61 @@ def reference_cpu(sc, seconds_target=12.0, threads=None):
 # main
 # ------------------------------------------------------------------------------------------
 
+def bench_hair(args, ctx_factory):
+    """65,536 strands x 32 particles (hair_groom): particle-substeps/s of solve_strands."""
+    import torch
+    from physxcoopa_b200 import scenes
+    sc = scenes.hair_groom(n_strands=args.cloths or 65536)
+    ctx = ctx_factory()
+    sid = ctx.add_strands(sc.sets[0])
+    pos, rot = sc.root_path(0)
+    ctx.set_strand_roots(sid, pos, rot)
+    col = sc.meta["colliders_at"](0)
+    d, keep = ctx.make_strand_step([sid], [col], iterations=sc.iterations, substeps=sc.substeps, h=sc.h)
+    for _ in range(max(args.warmup, 3)):
+        ctx.step_strands_desc(d)
+    ctx.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    l0 = ctx.launch_count
+    with torch.cuda.stream(stream):
+        t0.record(stream)
+        for _ in range(args.steps):
+            ctx.step_strands_desc(d)
+        t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    units = sc.particles * sc.substeps
+    value = units * args.steps / (ms * 1e-3)
+    # end to end: per frame the roots go up, the step runs, positions come back
+    n = len(sc.sets[0].particles)
+    out = np.zeros(n, __import__("physxcoopa_b200._abi", fromlist=["A"]).PARTICLE)
+    e0 = time.perf_counter()
+    for f in range(max(3, args.steps // 2)):
+        pos, rot = sc.root_path(f + 1)
+        ctx.set_strand_roots(sid, pos, rot)
+        ctx.step_strands([sid], [sc.meta["colliders_at"](f + 1)], iterations=sc.iterations)
+        out = ctx.read_strand_particles(sid, n)
+    e2e_s = (time.perf_counter() - e0) / max(3, args.steps // 2)
+    line = {"metric": "hair particle-substeps/s", "value": value, "unit": "particle-substeps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded groom)",
+            "config": {"workload": sc.name, "strands": len(sc.sets[0].strands), "particles": n,
+                       "substeps": sc.substeps, "iterations": sc.iterations},
+            "e2e": {"value": units / e2e_s, "unit": "particle-substeps/s",
+                    "h2d_bytes_per_step": 64 * len(sc.sets[0].strands), "d2h_bytes_per_step": 48 * n},
+            "gpu_launches": ctx.launch_count - l0, "clocks": clk}
+    print(json.dumps(line))
+    del keep
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -215,6 +270,10 @@ def main():
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
+
+    if args.workload == "hair_groom":
+        from physxcoopa_b200 import runtime as R
+        return bench_hair(args, lambda: R.Context(local_rank))
 
     import torch
     dist = None

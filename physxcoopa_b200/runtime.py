@@ -172,13 +172,18 @@ def make_strands(polylines, params=None, root_orientations=None, particle_masses
         f = np.dtype("<f4")
         p = A.StrandParams()
         C.pointer(p)[0] = v.params
-        return StrandArrays(particles=grab(v.particles, n, A.PARTICLE),
+        parts = grab(v.particles, n, A.PARTICLE)
+        pos = parts["position"]
+        # StrandSet::bounds = compute_bounds(set) at build (strand_builder.h:125, strand.h:195-202)
+        bounds = (np.concatenate([pos.min(axis=0), pos.max(axis=0)]).astype(np.float32) if n else
+                  np.array([3.4028235e38] * 3 + [-3.4028235e38] * 3, np.float32))
+        return StrandArrays(particles=parts,
                             stretch=grab(v.stretch, v.n_stretch, A.CONSTRAINT),
                             stretch_batches=grab(v.stretch_batches, v.n_stretch_batches, A.BATCH),
                             rest_local=grab(v.rest_local, 3 * n, f).reshape(-1, 3),
                             rest_offset=grab(v.rest_offset, 3 * n, f).reshape(-1, 3),
                             strands=grab(v.strands, v.n_strands, A.STRAND), params=p, time=0.0,
-                            bounds=None)
+                            bounds=bounds)
     finally:
         lib.pxb_host_strands_destroy(h)
 

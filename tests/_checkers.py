@@ -165,7 +165,10 @@ def _orc_strands(s: StrandArrays):
     o.n_strands = len(s.strands)
     o.params = s.params
     o.time = s.time
-    b = s.bounds if s.bounds is not None else np.zeros(6, np.float32)
+    if s.bounds is None:  # compute_bounds over the particles (strand.h:195-202)
+        pos = s.particles["position"]
+        s.bounds = np.concatenate([pos.min(axis=0), pos.max(axis=0)]).astype(np.float32)
+    b = s.bounds
     o.bounds_min = (C.c_float * 3)(*b[:3])
     o.bounds_max = (C.c_float * 3)(*b[3:])
     return o

@@ -1,0 +1,214 @@
+// physxcoopa_b200.hpp -- C++ drop-in facade over the C-ABI for physxcoopa code.
+//
+// Include this AFTER the physxcoopa headers (it uses cloth::Cloth, cloth::ClothCollider,
+// hair::StrandSet, collision::Shape). It offers the reference's own solve signatures
+//
+//   cloth::solve_cloth(Cloth&, colliders, gravity, substeps, iterations, h, scratch[, dispatch])
+//        (physxcoopa/cloth/cloth_solver.h:158-161, 463-467)
+//   hair::solve_strands(StrandSet&, colliders, gravity, substeps, iterations, h, scratch)
+//        (physxcoopa/hair/strand_solver.h:121-123)
+//
+// in namespace pxb::b200, backed by the device solver. The Cloth / StrandSet is advanced in
+// place exactly as the reference advances it; the scratch and dispatcher arguments are accepted
+// for signature compatibility and not used (the device needs neither). Vectors are handed to
+// the library as they are: pxb_particle, pxb_constraint, pxb_anchor... are the reference's own
+// byte layouts (static_asserts below). Errors throw std::runtime_error with the library's
+// message -- the reference throws nothing, so a caller that cannot accept an exception should
+// call the C-ABI directly and read pxb_status.
+#ifndef PHYSXCOOPA_B200_HPP
+#define PHYSXCOOPA_B200_HPP
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "physxcoopa_b200.h"
+
+namespace pxb {
+namespace b200 {
+
+static_assert(sizeof(coopa::physx::cloth::ClothParticle) == sizeof(pxb_particle), "particle layout");
+static_assert(sizeof(coopa::physx::cloth::ClothConstraint) == sizeof(pxb_constraint), "constraint layout");
+static_assert(sizeof(coopa::physx::cloth::ConstraintBatch) == sizeof(pxb_batch), "batch layout");
+static_assert(sizeof(coopa::physx::cloth::ClothTether) == sizeof(pxb_tether), "tether layout");
+static_assert(sizeof(coopa::physx::cloth::ClothAnchor) == sizeof(pxb_anchor), "anchor layout");
+static_assert(sizeof(coopa::physx::hair::Strand) == sizeof(pxb_strand), "strand layout");
+
+// One context per thread that steps cloths (the C-ABI is single-threaded per context).
+class Device {
+public:
+    explicit Device(int device = 0) {
+        if (pxb_context_create(device, &ctx_) != PXB_OK) throw std::runtime_error("pxb_context_create failed");
+    }
+    ~Device() { pxb_context_destroy(ctx_); }
+    Device(const Device&) = delete;
+    Device& operator=(const Device&) = delete;
+    pxb_context* get() const { return ctx_; }
+    void check(pxb_status s, const char* what) const {
+        if (s != PXB_OK) throw std::runtime_error(std::string(what) + ": " + pxb_last_error(ctx_));
+    }
+
+private:
+    pxb_context* ctx_ = nullptr;
+};
+
+inline void put3(float* o, const glm::vec3& v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
+inline void put4(float* o, const glm::quat& q) { o[0] = q.x; o[1] = q.y; o[2] = q.z; o[3] = q.w; }
+
+// cloth::ClothCollider + the collision::Shape it points at -> the C-ABI snapshot.
+inline pxb_collider to_collider(const coopa::physx::cloth::ClothCollider& c) {
+    pxb_collider o;
+    std::memset(&o, 0, sizeof(o));
+    const coopa::physx::collision::Shape* s = c.shape;
+    o.enabled = (s && s->enabled) ? 1 : 0;
+    if (s) {
+        o.type = static_cast<int32_t>(s->type);
+        put3(o.local_center, s->local_center);
+        put4(o.local_rotation, s->local_rotation);
+        o.radius = s->radius;
+        put3(o.half_extents, s->half_extents);
+        o.capsule_radius = s->capsule_radius;
+        o.capsule_half_height = s->capsule_half_height;
+        o.capsule_axis = s->capsule_axis;
+    }
+    put3(o.position, c.position);
+    put4(o.orientation, c.orientation);
+    put3(o.sweep, c.sweep);
+    put4(o.end_orientation, c.end_orientation);
+    put3(o.bounds_min, c.bounds.min);
+    put3(o.bounds_max, c.bounds.max);
+    return o;
+}
+
+inline pxb_cloth_params to_params(const coopa::physx::cloth::ClothParams& p) {
+    pxb_cloth_params o;
+    pxb_cloth_params_default(&o);
+    o.stretch_compliance = p.stretch_compliance;
+    o.bend_compliance = p.bend_compliance;
+    o.damping = p.damping;
+    o.thickness = p.thickness;
+    o.friction = p.friction;
+    o.gravity_scale = p.gravity_scale;
+    o.max_velocity = p.max_velocity;
+    put3(o.external_acceleration, p.external_acceleration);
+    put3(o.wind, p.wind);
+    o.wind_turbulence = p.wind_turbulence;
+    o.air_drag = p.air_drag;
+    o.air_lift = p.air_lift;
+    o.self_collision = p.self_collision ? 1 : 0;
+    o.self_distance = p.self_distance;
+    o.tether_scale = p.tether_scale;
+    o.substeps = p.substeps;
+    o.iterations = p.iterations;
+    o.sleep_threshold = p.sleep_threshold;
+    o.sleep_time = p.sleep_time;
+    o.layer = p.layer;
+    return o;
+}
+
+inline pxb_strand_params to_params(const coopa::physx::hair::StrandParams& p) {
+    pxb_strand_params o;
+    pxb_strand_params_default(&o);
+    o.stretch_compliance = p.stretch_compliance;
+    o.global_shape = p.global_shape;
+    o.global_shape_falloff = p.global_shape_falloff;
+    o.local_shape = p.local_shape;
+    o.damping = p.damping;
+    o.thickness = p.thickness;
+    o.friction = p.friction;
+    o.gravity_scale = p.gravity_scale;
+    o.max_velocity = p.max_velocity;
+    put3(o.external_acceleration, p.external_acceleration);
+    put3(o.wind, p.wind);
+    o.wind_turbulence = p.wind_turbulence;
+    o.air_drag = p.air_drag;
+    o.substeps = p.substeps;
+    o.iterations = p.iterations;
+    o.sleep_threshold = p.sleep_threshold;
+    o.sleep_time = p.sleep_time;
+    o.layer = p.layer;
+    return o;
+}
+
+// cloth::solve_cloth on the device (cloth_solver.h:158-467 contract).
+template <typename Scratch, typename Dispatch = int>
+void solve_cloth(Device& dev, coopa::physx::cloth::Cloth& c,
+                 const std::vector<coopa::physx::cloth::ClothCollider>& colliders,
+                 const glm::vec3& gravity, uint32_t substeps, uint32_t iterations, float h,
+                 Scratch& /*scratch*/, Dispatch&& /*dispatch*/ = Dispatch{}) {
+    pxb_cloth_desc d;
+    std::memset(&d, 0, sizeof(d));
+    d.particles = reinterpret_cast<const pxb_particle*>(c.particles.data());
+    d.n_particles = static_cast<uint32_t>(c.particles.size());
+    d.stretch = reinterpret_cast<const pxb_constraint*>(c.stretch.data());
+    d.n_stretch = static_cast<uint32_t>(c.stretch.size());
+    d.stretch_batches = reinterpret_cast<const pxb_batch*>(c.stretch_batches.data());
+    d.n_stretch_batches = static_cast<uint32_t>(c.stretch_batches.size());
+    d.bend = reinterpret_cast<const pxb_constraint*>(c.bend.data());
+    d.n_bend = static_cast<uint32_t>(c.bend.size());
+    d.bend_batches = reinterpret_cast<const pxb_batch*>(c.bend_batches.data());
+    d.n_bend_batches = static_cast<uint32_t>(c.bend_batches.size());
+    d.tethers = reinterpret_cast<const pxb_tether*>(c.tethers.data());
+    d.n_tethers = static_cast<uint32_t>(c.tethers.size());
+    d.anchors = reinterpret_cast<const pxb_anchor*>(c.anchors.data());
+    d.n_anchors = static_cast<uint32_t>(c.anchors.size());
+    d.triangles = c.triangles.data();
+    d.n_triangle_indices = static_cast<uint32_t>(c.triangles.size());
+    d.columns = c.columns;
+    d.rows = c.rows;
+    d.params = to_params(c.params);
+    d.time = c.time;
+    std::vector<pxb_collider> cols;
+    cols.reserve(colliders.size());
+    for (const auto& k : colliders) cols.push_back(to_collider(k));
+    const float g[3] = {gravity.x, gravity.y, gravity.z};
+    float bounds[6];
+    dev.check(pxb_solve_cloth_host(dev.get(), &d, reinterpret_cast<pxb_particle*>(c.particles.data()),
+                                   reinterpret_cast<pxb_constraint*>(c.stretch.data()),
+                                   reinterpret_cast<pxb_constraint*>(c.bend.data()),
+                                   reinterpret_cast<pxb_anchor*>(c.anchors.data()),
+                                   cols.data(), static_cast<uint32_t>(cols.size()), g, substeps,
+                                   iterations, h, &c.time, bounds),
+              "solve_cloth");
+    c.bounds.min = glm::vec3(bounds[0], bounds[1], bounds[2]);
+    c.bounds.max = glm::vec3(bounds[3], bounds[4], bounds[5]);
+}
+
+// hair::solve_strands on the device (strand_solver.h:121-327 contract).
+template <typename Scratch>
+void solve_strands(Device& dev, coopa::physx::hair::StrandSet& set,
+                   const std::vector<coopa::physx::cloth::ClothCollider>& colliders,
+                   const glm::vec3& gravity, uint32_t substeps, uint32_t iterations, float h,
+                   Scratch& /*scratch*/) {
+    pxb_strand_set_desc d;
+    std::memset(&d, 0, sizeof(d));
+    d.particles = reinterpret_cast<const pxb_particle*>(set.particles.data());
+    d.n_particles = static_cast<uint32_t>(set.particles.size());
+    d.stretch = reinterpret_cast<const pxb_constraint*>(set.stretch.data());
+    d.n_stretch = static_cast<uint32_t>(set.stretch.size());
+    d.stretch_batches = reinterpret_cast<const pxb_batch*>(set.stretch_batches.data());
+    d.n_stretch_batches = static_cast<uint32_t>(set.stretch_batches.size());
+    d.rest_local = reinterpret_cast<const float*>(set.rest_local.data());
+    d.rest_offset = reinterpret_cast<const float*>(set.rest_offset.data());
+    d.strands = reinterpret_cast<const pxb_strand*>(set.strands.data());
+    d.n_strands = static_cast<uint32_t>(set.strands.size());
+    d.params = to_params(set.params);
+    d.time = set.time;
+    std::vector<pxb_collider> cols;
+    for (const auto& k : colliders) cols.push_back(to_collider(k));
+    const float g[3] = {gravity.x, gravity.y, gravity.z};
+    float bounds[6];
+    dev.check(pxb_solve_strands_host(dev.get(), &d, reinterpret_cast<pxb_particle*>(set.particles.data()),
+                                     reinterpret_cast<pxb_constraint*>(set.stretch.data()), cols.data(),
+                                     static_cast<uint32_t>(cols.size()), g, substeps, iterations, h,
+                                     &set.time, bounds),
+              "solve_strands");
+    set.bounds.min = glm::vec3(bounds[0], bounds[1], bounds[2]);
+    set.bounds.max = glm::vec3(bounds[3], bounds[4], bounds[5]);
+}
+
+}  // namespace b200
+}  // namespace pxb
+
+#endif  // PHYSXCOOPA_B200_HPP

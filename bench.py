@@ -153,17 +153,22 @@ def reference_cpu(sc, seconds_target=12.0, threads=None):
             flat = np.ascontiguousarray(np.concatenate(cols)) if cols else np.zeros(0, A.COLLIDER)
             offs = np.zeros(len(sample) + 1, np.uint32)
             offs[1:] = np.cumsum([len(c) for c in cols])
+            srcs = [sc.sources[i] if sc.sources and sc.sources[i] is not None
+                    else np.zeros(0, A.GRAVITY_SOURCE) for i in sample]
+            sflat = np.ascontiguousarray(np.concatenate(srcs)) if srcs else np.zeros(0, A.GRAVITY_SOURCE)
+            soffs = np.zeros(len(sample) + 1, np.uint32)
+            soffs[1:] = np.cumsum([len(x) for x in srcs])
             handles = (C.c_void_p * len(refs))(*[r.h for r in refs])
             return K.ref().pxbref_bench_cloths(handles, len(refs), A.ptr(flat), A.ptr(offs),
-                                               K.vec(sc.gravity), sc.substeps, sc.iterations,
-                                               sc.h, steps, nthreads)
+                                               A.ptr(sflat), A.ptr(soffs), K.vec(sc.gravity),
+                                               sc.substeps, sc.iterations, sc.h, steps, nthreads)
         # the C restatement, single-threaded
         t0 = time.perf_counter()
         for _ in range(steps):
             for i in sample:
                 c = sc.cloths[i].copy()
-                K.oracle_step_cloth(c, sc.colliders[i], substeps=sc.substeps,
-                                    iterations=sc.iterations, h=sc.h)
+                K.oracle_step_cloth(c, sc.colliders[i], sources=sc.sources[i] if sc.sources else None,
+                                    substeps=sc.substeps, iterations=sc.iterations, h=sc.h)
         return time.perf_counter() - t0
 
     # calibrate on one cloth, one step, one thread

@@ -264,6 +264,25 @@ void pxb_cloth_params_default(pxb_cloth_params* out);
  * id is generational: it goes stale after pxb_cloth_remove. */
 pxb_status pxb_cloth_add(pxb_context* ctx, const pxb_cloth_desc* desc, uint64_t* id_out);
 pxb_status pxb_cloth_remove(pxb_context* ctx, uint64_t id);
+
+/* How pxb_cloth_add would lay a cloth out on the device. A cloth whose state does not fit one
+ * CTA's shared memory is split by rows over a thread-block cluster of n_ranks CTAs (1, 2, 4 or
+ * 8). No counterpart in the reference, which has no device layout. */
+typedef struct pxb_cloth_plan {
+    int32_t n_ranks;          /* CTAs holding the cloth (a cluster when > 1) */
+    int32_t rows_per_rank;    /* grid rows per CTA (the last CTA may hold fewer) */
+    int32_t threads;          /* threads per CTA the cloth asks for */
+    int32_t smem_bytes;       /* largest per-CTA dynamic shared memory */
+    int32_t n_colours;        /* independent constraint sets solved one after another */
+    int32_t n_segments;       /* affine segments over all CTAs and colours */
+    int32_t layout_slots;     /* rows * 4 * ceil(columns / 4) particle slots */
+    int32_t constraint_slots; /* rest-length slots over all CTAs, row padding included */
+} pxb_cloth_plan;
+
+/* Plans a cloth without a context or a GPU: validates it exactly as pxb_cloth_add does and
+ * fills *out. On failure the message goes to err (NUL-terminated, at most err_cap bytes). */
+pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out, char* err,
+                                 uint32_t err_cap);
 /* Replaces a live cloth's tunables (ClothComponent::cloth_mut()->params is edited live). */
 pxb_status pxb_cloth_set_params(pxb_context* ctx, uint64_t id, const pxb_cloth_params* params);
 /* Host edit of particle state between steps (all four fields of every particle). */

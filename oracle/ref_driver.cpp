@@ -290,10 +290,42 @@ int pxbref_project_particle(const pxb_collider* collider, float thickness, float
 // CPU baseline: advances every listed cloth by `steps` calls of solve_cloth on `threads` host
 // threads, whole cloths handed out from a shared counter and each solved serially -- the
 // reference's own SerialDispatch per cloth. Returns wall seconds.
+// PhysicsWorld::cloth_centre_ and field_at_ (world.h:2048-2076) are private members of the world;
+// the timing driver restates them over the same sources so each cloth is stepped with the
+// gravity step_cloths_ would give it (world.h:1833).
+static glm::vec3 bench_gravity(const px::cloth::Cloth& c, const glm::vec3& uniform,
+                               const pxb_gravity_source* src, uint32_t n_src) {
+    if (n_src == 0) return uniform;
+    glm::vec3 sum(0.0f);
+    for (const px::cloth::ClothParticle& p : c.particles) sum += p.position;
+    const glm::vec3 centre = c.particles.empty() ? sum : sum / static_cast<float>(c.particles.size());
+    float best = 0.0f;
+    glm::vec3 pull = uniform;
+    bool found = false;
+    for (uint32_t k = 0; k < n_src; ++k) {
+        const glm::vec3 d = v3(src[k].centre) - centre;
+        const float r = glm::length(d);
+        if (src[k].range > 0.0f && r > src[k].range) continue;
+        if (r < 1e-6f) continue;
+        const float a = r <= src[k].radius ? src[k].strength
+                                           : src[k].strength * (src[k].radius / r) * (src[k].radius / r);
+        if (!found || a > best) {
+            best = a;
+            pull = d / r * a;
+            found = true;
+        }
+    }
+    return found ? pull : uniform;
+}
+
+// Steps n reference cloths `steps` times over `threads` host threads (an atomic work counter,
+// one solve_cloth per cloth per step, as PhysicsWorld::step_cloths_ with a thread-pool
+// dispatcher). Sources (optional, per-cloth offsets) select each cloth's gravity. Returns the
+// wall-clock seconds.
 double pxbref_bench_cloths(void** handles, uint32_t n, const pxb_collider* colliders,
-                           const uint32_t* collider_offsets, const float* gravity,
-                           uint32_t substeps, uint32_t iterations, float dt, uint32_t steps,
-                           uint32_t threads) {
+                           const uint32_t* collider_offsets, const pxb_gravity_source* sources,
+                           const uint32_t* source_offsets, const float* gravity, uint32_t substeps,
+                           uint32_t iterations, float dt, uint32_t steps, uint32_t threads) {
     if (threads < 1) threads = 1;
     std::vector<RefColliders> cols;
     cols.reserve(n);
@@ -302,6 +334,7 @@ double pxbref_bench_cloths(void** handles, uint32_t n, const pxb_collider* colli
         const uint32_t e = collider_offsets ? collider_offsets[i + 1] : 0;
         cols.emplace_back(colliders + b, e - b);
     }
+    const glm::vec3 g0 = v3(gravity);
     const auto t0 = std::chrono::steady_clock::now();
     for (uint32_t s = 0; s < steps; ++s) {
         std::atomic<uint32_t> next{0};
@@ -310,8 +343,11 @@ double pxbref_bench_cloths(void** handles, uint32_t n, const pxb_collider* colli
             for (;;) {
                 const uint32_t i = next.fetch_add(1);
                 if (i >= n) break;
-                px::cloth::solve_cloth(*static_cast<px::cloth::Cloth*>(handles[i]), cols[i].colliders,
-                                       v3(gravity), substeps, iterations, dt, scratch);
+                px::cloth::Cloth& c = *static_cast<px::cloth::Cloth*>(handles[i]);
+                const uint32_t sb = source_offsets ? source_offsets[i] : 0;
+                const uint32_t se = source_offsets ? source_offsets[i + 1] : 0;
+                const glm::vec3 g = bench_gravity(c, g0, sources ? sources + sb : nullptr, se - sb);
+                px::cloth::solve_cloth(c, cols[i].colliders, g, substeps, iterations, dt, scratch);
             }
         };
         if (threads == 1) {

@@ -118,6 +118,16 @@ class StrandParams(C.Structure):
 P = C.c_void_p
 
 
+class ClothPlan(C.Structure):
+    """pxb_cloth_plan: the device layout pxb_cloth_add would choose."""
+    _fields_ = [("n_ranks", C.c_int32), ("rows_per_rank", C.c_int32), ("threads", C.c_int32),
+                ("smem_bytes", C.c_int32), ("n_colours", C.c_int32), ("n_segments", C.c_int32),
+                ("layout_slots", C.c_int32), ("constraint_slots", C.c_int32)]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
 class ClothDesc(C.Structure):
     """pxb_cloth_desc: a cloth as plain pointers into caller memory."""
     _fields_ = [("particles", P), ("n_particles", u32), ("stretch", P), ("n_stretch", u32),

@@ -21,6 +21,7 @@
 // Arithmetic is IEEE single precision with no contraction (built with -fmad=false) and the
 // reference's operation order, so a step reproduces the CPU oracle to the bit (up to the sign of
 // an exactly-zero coordinate; see the lambda note in the colour loop).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -28,6 +29,8 @@
 #include "pxb_internal.h"
 #include "pxb_kernels.h"
 #include "pxb_device_math.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace pxb {
 namespace {
@@ -132,7 +135,37 @@ __device__ __forceinline__ float warp_max(float v) {
 // The kernel
 // ------------------------------------------------------------------------------------------
 
-template <int kMaxThreads>
+// Slot addressing of a cloth split over a cluster: a CTA (rank) holds rows [row0, row0 +
+// n_rows); its neighbours' rows are reached through distributed shared memory.
+struct RankView {
+    float4* pos;        // this rank's positions (shared memory)
+    float* U;           // this rank's union region (lambdas / velocity scratch)
+    int base;           // global layout slot of local slot 0
+    int n_local;        // slots held
+};
+
+template <int CL>
+__device__ __forceinline__ RankView rank_view(const PxbClothDev& C, unsigned char* smem, int r) {
+    const PxbRank& R = C.rank[r];
+    RankView v;
+    v.n_local = R.n_rows * C.S;
+    v.base = R.row0 * C.S;
+    unsigned char* b = smem;
+    if constexpr (CL > 1) {
+        b = static_cast<unsigned char*>(cg::this_cluster().map_shared_rank(static_cast<void*>(smem), r));
+    }
+    v.pos = reinterpret_cast<float4*>(b);
+    v.U = reinterpret_cast<float*>(b + 16 * static_cast<size_t>(v.n_local)) + R.n_rest_pad;
+    return v;
+}
+
+template <int CL>
+__device__ __forceinline__ void cluster_or_block_sync() {
+    if constexpr (CL > 1) cg::this_cluster().sync();
+    else __syncthreads();
+}
+
+template <int kMaxThreads, int CL>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders,
@@ -143,16 +176,20 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     __shared__ __align__(8) uint64_t bar;
     __shared__ __align__(16) PxbSeg s_seg[PXB_MAX_SEGS];
     // Per-cloth scalars live in shared memory and are read at their point of use: held in
-    // registers for the whole kernel they would crowd out the particle state (64 registers at
-    // 1024 threads).
-    __shared__ PxbClothDev sC;
+    // registers for the whole kernel they would crowd out the projection loop (64 registers
+    // at 1024 threads).
+    __shared__ __align__(16) PxbClothDev sC;
     __shared__ PxbClothStep sP;
     __shared__ float s_red[32][7];
+    __shared__ float s_rank_red[PXB_MAX_RANKS][7];
     __shared__ float s_base[3];
+    __shared__ float s_run[3];
 
     const int tid = threadIdx.x;
     const int T = blockDim.x;
-    const int slot = blockIdx.x;
+    int rank = 0;
+    if constexpr (CL > 1) rank = static_cast<int>(cg::this_cluster().block_rank());
+    const int slot = blockIdx.x / CL;
     {
         const int ci = __ldg(&order[slot]);
         const int* srcC = reinterpret_cast<const int*>(&cloths[ci]);
@@ -168,70 +205,96 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
     __syncthreads();
 
-    const int n_layout = sC.n_layout;
-    float4* pos = reinterpret_cast<float4*>(smem);
-    float* rest = reinterpret_cast<float*>(smem + 16 * static_cast<size_t>(n_layout));
-    float* U = rest + sC.n_rest_pad;  // lambdas of compliant colours / velocity scratch (SoA)
+    const int n_ranks = CL > 1 ? sC.n_ranks : 1;
+    const RankView me = rank_view<1>(sC, smem, rank);  // local view, plain shared addresses
+    float4* pos = me.pos;
+    float* U = me.U;
+    const int n_local = me.n_local;
+    const int base = me.base;
+    float* rest = reinterpret_cast<float*>(smem + 16 * static_cast<size_t>(n_local));
+    RankView prv_rank{}, nxt_rank{};
+    if constexpr (CL > 1) {
+        if (rank > 0) prv_rank = rank_view<CL>(sC, smem, rank - 1);
+        if (rank + 1 < n_ranks) nxt_rank = rank_view<CL>(sC, smem, rank + 1);
+    }
 
     // --- prologue: stage positions and rest lengths with TMA bulk copies -------------------
     if (tid == 0) {
-        const uint32_t pos_bytes = 16u * static_cast<uint32_t>(n_layout);
-        const uint32_t rest_bytes = 4u * static_cast<uint32_t>(sC.n_rest_pad);
+        const uint32_t pos_bytes = 16u * static_cast<uint32_t>(n_local);
+        const uint32_t rest_bytes = 4u * static_cast<uint32_t>(sC.rank[rank].n_rest_pad);
         mbar_arrive_expect_tx(&bar, pos_bytes + rest_bytes);
-        bulk_g2s(pos, sC.pos, pos_bytes, &bar);
-        if (rest_bytes) bulk_g2s(rest, sC.rest, rest_bytes, &bar);
+        bulk_g2s(pos, sC.pos + base, pos_bytes, &bar);
+        if (rest_bytes) bulk_g2s(rest, sC.rest + sC.rank[rank].rest_off, rest_bytes, &bar);
     }
-    for (int i = tid; i < sC.n_segs; i += T) s_seg[i] = sC.segs[i];
-
+    {
+        const int sb = sC.rank[rank].seg_begin;
+        const int ns = sC.rank[rank].colour_seg[sC.n_colours];
+        for (int i = tid; i < ns; i += T) s_seg[i] = sC.segs[sb + i];
+    }
+    // A staging wait that runs out records the error and carries on: leaving early would strand
+    // the other ranks of the cluster at their barriers.
     const bool staged = mbar_wait_bounded(&bar, 0);
     if (!staged && tid == 0) atomicOr(err, PXB_DEVERR_TMA_TIMEOUT);
     __syncthreads();
-    if (!staged) return;
 
     // --- gravity: uniform, or the source field at the cloth's mean position (world.h:1833) --
     if (sP.src_count > 0) {
-        if (tid == 0) {
-            // PhysicsWorld::cloth_centre_ (world.h:2072-2076): the mean in particle order, summed
-            // sequentially exactly as the reference does, so the gravity it selects is the
-            // reference's to the bit (a reordered sum drifts the drape chaotically).
-            const int Q = sC.Q, S = sC.S, cols = sC.columns, n = sC.n_real;
-            float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-            int x = 0, y = 0;
-            for (int i = 0; i < n; ++i) {
-                const float4 p = pos[lay(x, y, Q, S)];
-                cx += p.x; cy += p.y; cz += p.z;
-                if (++x == cols) { x = 0; ++y; }
-            }
-            const float fn = static_cast<float>(n);
-            const f3 centre = mk(cx / fn, cy / fn, cz / fn);
-            // PhysicsWorld::field_at_ (world.h:2048-2068)
-            float best = 0.0f;
-            f3 pull = mk(sP.gravity[0], sP.gravity[1], sP.gravity[2]);
-            bool found = false;
-            for (int k = 0; k < sP.src_count; ++k) {
-                const pxb_gravity_source* g = &sources[sP.src_begin + k];
-                const f3 d = sub(ld3(g->centre), centre);
-                const float r = len(d);
-                const float range = __ldg(&g->range), radius = __ldg(&g->radius),
-                            strength = __ldg(&g->strength);
-                if (range > 0.0f && r > range) continue;
-                if (r < 1e-6f) continue;
-                const float a = r <= radius ? strength : strength * (radius / r) * (radius / r);
-                if (!found || a > best) {
-                    best = a;
-                    pull = mul(divs(d, r), a);
-                    found = true;
+        // PhysicsWorld::cloth_centre_ (world.h:2072-2076): the mean in particle order, summed
+        // sequentially exactly as the reference does (rank after rank, handing the running sum
+        // on), so the gravity it selects is the reference's to the bit.
+        for (int r = 0; r < n_ranks; ++r) {
+            if (r == rank && tid == 0) {
+                const int Q = sC.Q, S = sC.S, cols = sC.columns;
+                float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+                if (r > 0) { cx = s_run[0]; cy = s_run[1]; cz = s_run[2]; }
+                const int y0 = sC.rank[r].row0, y1 = y0 + sC.rank[r].n_rows;
+                for (int y = y0; y < y1 && y < sC.rows; ++y)
+                    for (int x = 0; x < cols; ++x) {
+                        const float4 p = pos[lay(x, y, Q, S) - base];
+                        cx += p.x; cy += p.y; cz += p.z;
+                    }
+                if (r + 1 < n_ranks) {
+                    float* dst = s_run;
+                    if constexpr (CL > 1) dst = cg::this_cluster().map_shared_rank(s_run, r + 1);
+                    dst[0] = cx; dst[1] = cy; dst[2] = cz;
+                } else {
+                    const float fn = static_cast<float>(sC.n_real);
+                    const f3 centre = mk(cx / fn, cy / fn, cz / fn);
+                    // PhysicsWorld::field_at_ (world.h:2048-2068)
+                    float best = 0.0f;
+                    f3 pull = mk(sP.gravity[0], sP.gravity[1], sP.gravity[2]);
+                    bool found = false;
+                    for (int k = 0; k < sP.src_count; ++k) {
+                        const pxb_gravity_source* g = &sources[sP.src_begin + k];
+                        const f3 d = sub(ld3(g->centre), centre);
+                        const float rr = len(d);
+                        const float range = __ldg(&g->range), radius = __ldg(&g->radius),
+                                    strength = __ldg(&g->strength);
+                        if (range > 0.0f && rr > range) continue;
+                        if (rr < 1e-6f) continue;
+                        const float a = rr <= radius ? strength : strength * (radius / rr) * (radius / rr);
+                        if (!found || a > best) {
+                            best = a;
+                            pull = mul(divs(d, rr), a);
+                            found = true;
+                        }
+                    }
+                    const f3 bacc = add(mul(pull, sP.gravity_scale),
+                                        mk(sP.external_acceleration[0], sP.external_acceleration[1],
+                                           sP.external_acceleration[2]));
+                    for (int q = 0; q < n_ranks; ++q) {
+                        float* dst = s_base;
+                        if constexpr (CL > 1) dst = cg::this_cluster().map_shared_rank(s_base, q);
+                        dst[0] = bacc.x; dst[1] = bacc.y; dst[2] = bacc.z;
+                    }
                 }
             }
-            const f3 base = add(mul(pull, sP.gravity_scale),
-                                mk(sP.external_acceleration[0], sP.external_acceleration[1],
-                                   sP.external_acceleration[2]));
-            s_base[0] = base.x; s_base[1] = base.y; s_base[2] = base.z;
+            cluster_or_block_sync<CL>();
         }
     } else if (tid == 0) {
         s_base[0] = sP.base_accel[0]; s_base[1] = sP.base_accel[1]; s_base[2] = sP.base_accel[2];
     }
-    __syncthreads();
+    cluster_or_block_sync<CL>();
 
     const int steps = sP.steps;
     float4* __restrict__ gvel = sC.vel;
@@ -242,26 +305,42 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         // Velocities are parked in U (SoA) for the neighbour reads; each particle's summed
         // share is parked in its own prv slot until integrate consumes it.
         if (aero) {
-            for (int l = tid; l < n_layout; l += T) {
-                const float4 vv = gvel[l];
+            for (int l = tid; l < n_local; l += T) {
+                const float4 vv = gvel[base + l];
                 U[l] = vv.x;
-                U[n_layout + l] = vv.y;
-                U[2 * n_layout + l] = vv.z;
+                U[n_local + l] = vv.y;
+                U[2 * n_local + l] = vv.z;
             }
-            __syncthreads();
+            cluster_or_block_sync<CL>();
             const int Q = sC.Q, S = sC.S, cols = sC.columns, rows = sC.rows;
             const f3 wind = mk(sP.wind[0], sP.wind[1], sP.wind[2]);
             const float drag = sP.air_drag, lift = sP.air_lift;
-            for (int l = tid; l < n_layout; l += T) {
-                const int y = l / S;
-                const int j = l - y * S;
+            // neighbour rows may belong to the previous / next rank
+            auto P3 = [&](int g) -> f3 {
+                const int l = g - base;
+                if (CL == 1 || (l >= 0 && l < n_local)) return xyz(pos[l]);
+                if (l < 0) return xyz(prv_rank.pos[l + prv_rank.n_local]);
+                return xyz(nxt_rank.pos[l - n_local]);
+            };
+            auto V3 = [&](int g) -> f3 {
+                const int l = g - base;
+                if (CL == 1 || (l >= 0 && l < n_local)) return mk(U[l], U[n_local + l], U[2 * n_local + l]);
+                if (l < 0) {
+                    const int m = l + prv_rank.n_local, n = prv_rank.n_local;
+                    return mk(prv_rank.U[m], prv_rank.U[n + m], prv_rank.U[2 * n + m]);
+                }
+                const int m = l - n_local, n = nxt_rank.n_local;
+                return mk(nxt_rank.U[m], nxt_rank.U[n + m], nxt_rank.U[2 * n + m]);
+            };
+            for (int l = tid; l < n_local; l += T) {
+                const int gl = base + l;
+                const int y = gl / S;
+                const int j = gl - y * S;
                 const int cls = j / Q;
                 const int x = 4 * (j - cls * Q) + cls;
-                if (x >= cols) continue;  // ghost slot
+                if (x >= cols || y >= rows) continue;  // ghost slot
                 const bool xm = x >= 1, xp = x + 1 < cols, ym = y >= 1, yp = y + 1 < rows;
-                auto P3 = [&](int li) { return xyz(pos[li]); };
-                auto V3 = [&](int li) { return mk(U[li], U[n_layout + li], U[2 * n_layout + li]); };
-                const f3 p00 = P3(l), v00 = V3(l);
+                const f3 p00 = xyz(pos[l]), v00 = mk(U[l], U[n_local + l], U[2 * n_local + l]);
                 f3 a = mk(0.0f, 0.0f, 0.0f);
                 if (xm && ym) {  // cell (x-1, y-1): T0 then T1
                     const int lmm = lay(x - 1, y - 1, Q, S), l0m = lay(x, y - 1, Q, S),
@@ -283,13 +362,13 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     tri_share(p00, P3(lp0), P3(lpp), v00, V3(lp0), V3(lpp), wind, drag, lift, a);
                     tri_share(p00, P3(lpp), P3(l0p), v00, V3(lpp), V3(l0p), wind, drag, lift, a);
                 }
-                gprv[l] = make_float4(a.x, a.y, a.z, 0.0f);
+                gprv[gl] = make_float4(a.x, a.y, a.z, 0.0f);
             }
-            __syncthreads();
+            cluster_or_block_sync<CL>();
         }
 
         // --- 4a. lambda reset (cloth_solver.h:253-254) ----------------------------------
-        for (int i = tid; i < sC.n_lam; i += T) U[i] = 0.0f;
+        for (int i = tid; i < sC.rank[rank].n_lam; i += T) U[i] = 0.0f;
 
         // --- 2 + 3. integrate, then the anchor lerp (cloth_solver.h:230-250) --------------
         {
@@ -297,19 +376,20 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             const float hs = sP.hs, damping_factor = sP.damping_factor;
             const f3 base_accel = mk(s_base[0], s_base[1], s_base[2]);
             const PxbAnchorRec* anchors = reinterpret_cast<const PxbAnchorRec*>(sC.anchors);
-            for (int l = tid; l < n_layout; l += T) {
+            for (int l = tid; l < n_local; l += T) {
+                const int gl = base + l;
                 float4 p = pos[l];
-                const f3 acc = aero ? xyz(gprv[l]) : mk(0.0f, 0.0f, 0.0f);
-                gprv[l] = make_float4(p.x, p.y, p.z, 0.0f);
+                const f3 acc = aero ? xyz(gprv[gl]) : mk(0.0f, 0.0f, 0.0f);
+                gprv[gl] = make_float4(p.x, p.y, p.z, 0.0f);
                 if (p.w != 0.0f) {
-                    f3 vv = xyz(gvel[l]);
+                    f3 vv = xyz(gvel[gl]);
                     vv = add(vv, mul(add(base_accel, mul(acc, p.w)), hs));
                     vv = mul(vv, damping_factor);
                     p.x = p.x + vv.x * hs;
                     p.y = p.y + vv.y * hs;
                     p.z = p.z + vv.z * hs;
                 }
-                const int anc = __ldg(&sC.anchor_of[l]);
+                const int anc = __ldg(&sC.anchor_of[gl]);
                 if (anc >= 0) {
                     const PxbAnchorRec& a = anchors[anc];
                     const float om = 1.0f - alpha_t;
@@ -320,81 +400,51 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 pos[l] = p;
             }
         }
-        __syncthreads();
+        cluster_or_block_sync<CL>();
 
         // --- 4b. constraint iterations: colour by colour (cloth_solver.h:256-271) ----------
-        // Per segment the descriptor is read once; a thread takes items i and i + T together so
-        // two independent projections are in flight (a colour's constraints are disjoint).
-        // A zero-compliance colour keeps no lambda: with alpha == 0 the multiplier never
-        // reaches a position (dlambda = (-c - 0*lambda)/w); only the sign of an exactly-zero
-        // correction could differ, which moves no coordinate that is not itself +-0.
+        // Per segment the descriptor is read once. An item's `a` endpoint is local; its `b`
+        // endpoint is local or in the next rank. A zero-compliance colour keeps no lambda: with
+        // alpha == 0 the multiplier never reaches a position (dlambda = (-c - 0*lambda)/w); only
+        // the sign of an exactly-zero correction could differ, which moves no coordinate that
+        // is not itself +-0.
         {
             const int iters = sP.iters, n_colours = sC.n_colours;
             const int4* seg4 = reinterpret_cast<const int4*>(s_seg);
+            const uint32_t cross = sC.cross_mask;
+            float4* pos_next = nxt_rank.pos;
             for (int it = 0; it < iters; ++it) {
                 for (int c = 0; c < n_colours; ++c) {
                     const float alpha = sP.alpha[c];
-                    const int se = sC.colour_seg[c + 1];
-                    for (int sg = sC.colour_seg[c]; sg < se; ++sg) {
+                    const int se = sC.rank[rank].colour_seg[c + 1];
+                    for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
                         const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
                         const int count_pad = h0.x, shift = h0.y, per_row = h0.z, a_base = h0.w;
                         const int row_stride = h1.x, d = h1.y, rest_base = h1.z, lam_base = h1.w;
                         const int mask = (1 << shift) - 1;
-                        if constexpr (kMaxThreads >= 1024) {
-                            // 32 warps supply the parallelism; one item at a time keeps the
-                            // loop inside the 64-register budget of a 1024-thread block.
-                            for (int i = tid; i < count_pad; i += T) {
-                                const int k0 = i & mask;
-                                if (k0 >= per_row) continue;
-                                const int la0 = a_base + (i >> shift) * row_stride + k0;
-                                float4 pa0 = pos[la0], pb0 = pos[la0 + d];
-                                const float lam0 = lam_base >= 0 ? U[lam_base + i] : 0.0f;
-                                float d0 = 0.0f;
-                                if (solve_pair(pa0, pb0, rest[rest_base + i], lam0, alpha, d0)) {
-                                    pos[la0] = pa0;
-                                    pos[la0 + d] = pb0;
-                                    if (lam_base >= 0) U[lam_base + i] = lam0 + d0;
-                                }
+                        for (int i = tid; i < count_pad; i += T) {
+                            const int k0 = i & mask;
+                            if (k0 >= per_row) continue;
+                            const int la = a_base + (i >> shift) * row_stride + k0;
+                            const int lb = la + d;
+                            float4* pb_ptr = (CL == 1 || lb < n_local) ? &pos[lb] : &pos_next[lb - n_local];
+                            float4 pa = pos[la], pb = *pb_ptr;
+                            const float lam = lam_base >= 0 ? U[lam_base + i] : 0.0f;
+                            float dl = 0.0f;
+                            if (solve_pair(pa, pb, rest[rest_base + i], lam, alpha, dl)) {
+                                pos[la] = pa;
+                                *pb_ptr = pb;
+                                if (lam_base >= 0) U[lam_base + i] = lam + dl;
                             }
-                        } else {
-                        for (int i = tid; i < count_pad; i += 2 * T) {
-                            const int i1 = i + T;
-                            const int k0 = i & mask, k1 = i1 & mask;
-                            const bool v0 = k0 < per_row;
-                            const bool v1 = i1 < count_pad && k1 < per_row;
-                            const int la0 = a_base + (i >> shift) * row_stride + k0;
-                            const int la1 = a_base + (i1 >> shift) * row_stride + k1;
-                            float4 pa0, pb0, pa1, pb1;
-                            float r0 = 0.0f, r1 = 0.0f, lam0 = 0.0f, lam1 = 0.0f;
-                            if (v0) {
-                                pa0 = pos[la0];
-                                pb0 = pos[la0 + d];
-                                r0 = rest[rest_base + i];
-                                if (lam_base >= 0) lam0 = U[lam_base + i];
-                            }
-                            if (v1) {
-                                pa1 = pos[la1];
-                                pb1 = pos[la1 + d];
-                                r1 = rest[rest_base + i1];
-                                if (lam_base >= 0) lam1 = U[lam_base + i1];
-                            }
-                            float d0 = 0.0f, d1 = 0.0f;
-                            const bool w0 = v0 && solve_pair(pa0, pb0, r0, lam0, alpha, d0);
-                            const bool w1 = v1 && solve_pair(pa1, pb1, r1, lam1, alpha, d1);
-                            if (w0) {
-                                pos[la0] = pa0;
-                                pos[la0 + d] = pb0;
-                                if (lam_base >= 0) U[lam_base + i] = lam0 + d0;
-                            }
-                            if (w1) {
-                                pos[la1] = pa1;
-                                pos[la1 + d] = pb1;
-                                if (lam_base >= 0) U[lam_base + i1] = lam1 + d1;
-                            }
-                        }
                         }
                     }
-                    __syncthreads();
+                    // Colours that join rows need every rank to see the others' writes; a pair
+                    // of row-local colours only needs this CTA's. The last colour always syncs
+                    // the cluster: the tether stage reads anchors anywhere in the cloth.
+                    const int cn = (c + 1 < n_colours) ? c + 1 : 0;
+                    const bool last = it + 1 == iters && c + 1 == n_colours;
+                    if (CL > 1 && (((cross >> c) | (cross >> cn)) & 1u || last)) cluster_or_block_sync<CL>();
+                    else __syncthreads();
                 }
             }
         }
@@ -403,7 +453,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         {
             const int col_begin = sP.col_begin, col_count = sP.col_count;
             const float thickness = sP.thickness, inv_hs = sP.inv_hs;
-            for (int l = tid; l < n_layout; l += T) {
+            for (int l = tid; l < n_local; l += T) {
+                const int gl = base + l;
                 float4 p4 = pos[l];
                 f3 p = xyz(p4);
                 bool moved = false;
@@ -411,9 +462,17 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 float dsum = 0.0f;
                 if (p4.w != 0.0f) {
                     // 5. tether (cloth_solver.h:276-289); its anchor is a pinned particle
-                    const int2 teth = __ldg(&sC.tether[l]);
+                    const int2 teth = __ldg(&sC.tether[gl]);
                     if (teth.x >= 0) {
-                        const f3 anchor = xyz(pos[teth.x]);
+                        f3 anchor;
+                        if (CL == 1) {
+                            anchor = xyz(pos[teth.x]);
+                        } else {
+                            int o = 0;
+                            while (o + 1 < n_ranks && teth.x >= sC.rank[o + 1].row0 * sC.S) ++o;
+                            const RankView ov = o == rank ? me : rank_view<CL>(sC, smem, o);
+                            anchor = xyz(ov.pos[teth.x - ov.base]);
+                        }
                         const f3 d = sub(p, anchor);
                         const float l2 = len(d);
                         const float max_len = __int_as_float(teth.y);
@@ -443,7 +502,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     pos[l] = p4;
                 }
                 // 8. finalize (cloth_solver.h:414-451), every particle
-                const float4 pv = gprv[l];
+                const float4 pv = gprv[gl];
                 f3 vv = mul(sub(p, xyz(pv)), inv_hs);
                 if (dsum > 0.0f) {
                     const float nlen = len(nsum);
@@ -459,25 +518,32 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 }
                 const float v2 = dot(vv, vv);
                 if (v2 > sP.max_velocity2) vv = mul(vv, sP.max_velocity / sqrtf(v2));
-                const float real = gvel[l].w;
-                gvel[l] = make_float4(vv.x, vv.y, vv.z, real);
+                const float real = gvel[gl].w;
+                gvel[gl] = make_float4(vv.x, vv.y, vv.z, real);
             }
         }
-        __syncthreads();
+        cluster_or_block_sync<CL>();
     }
 
     // --- epilogue --------------------------------------------------------------------------
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-        bulk_s2g(sC.pos, pos, 16u * static_cast<uint32_t>(n_layout));
-        bulk_commit_and_wait();
+    // One CTA: a bulk copy back to HBM (its own threads wrote every slot, then fenced). A
+    // cluster rank's slots were also written by its neighbour through distributed shared
+    // memory, so it stores with plain coalesced writes instead of the async proxy.
+    if constexpr (CL == 1) {
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            bulk_s2g(sC.pos + base, pos, 16u * static_cast<uint32_t>(n_local));
+            bulk_commit_and_wait();
+        }
+    } else {
+        for (int l = tid; l < n_local; l += T) sC.pos[base + l] = pos[l];
     }
     float bmin[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
     float bmax[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
     float vmax2 = 0.0f;
-    for (int l = tid; l < n_layout; l += T) {
-        const float4 vv = gvel[l];
+    for (int l = tid; l < n_local; l += T) {
+        const float4 vv = gvel[base + l];
         if (vv.w == 0.0f) continue;  // ghost slot
         const float4 p = pos[l];
         bmin[0] = minr(bmin[0], p.x); bmin[1] = minr(bmin[1], p.y); bmin[2] = minr(bmin[2], p.z);
@@ -485,13 +551,16 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         vmax2 = maxr(vmax2, dot(xyz(vv), xyz(vv)));
     }
     if (sP.write_lambdas) {
-        for (int i = tid; i < sC.n_lam; i += T) sC.lam_out[i] = U[i];
+        float* lo = sC.lam_out + sC.rank[rank].lam_off;
+        for (int i = tid; i < sC.rank[rank].n_lam; i += T) lo[i] = U[i];
     }
-    for (int a = tid; a < sC.n_anchors; a += T) {
-        PxbAnchorRec* rec = reinterpret_cast<PxbAnchorRec*>(sC.anchors) + a;
-        rec->prev[0] = rec->world[0];
-        rec->prev[1] = rec->world[1];
-        rec->prev[2] = rec->world[2];
+    if (rank == 0) {
+        for (int a = tid; a < sC.n_anchors; a += T) {
+            PxbAnchorRec* rec = reinterpret_cast<PxbAnchorRec*>(sC.anchors) + a;
+            rec->prev[0] = rec->world[0];
+            rec->prev[1] = rec->world[1];
+            rec->prev[2] = rec->world[2];
+        }
     }
     float r[7] = {bmin[0], bmin[1], bmin[2], bmax[0], bmax[1], bmax[2], vmax2};
     r[0] = warp_min(r[0]); r[1] = warp_min(r[1]); r[2] = warp_min(r[2]);
@@ -507,11 +576,22 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             for (int k = 0; k < 3; ++k) r[k] = fminf(r[k], s_red[w][k]);
             for (int k = 3; k < 7; ++k) r[k] = fmaxf(r[k], s_red[w][k]);
         }
+        float* dst = s_rank_red[rank];
+        if constexpr (CL > 1) dst = cg::this_cluster().map_shared_rank(&s_rank_red[rank][0], 0);
+        for (int k = 0; k < 7; ++k) dst[k] = r[k];
+    }
+    cluster_or_block_sync<CL>();
+    if (rank == 0 && tid == 0) {
+        for (int q = 1; q < n_ranks; ++q) {
+            for (int k = 0; k < 3; ++k) r[k] = fminf(r[k], s_rank_red[q][k]);
+            for (int k = 3; k < 7; ++k) r[k] = fmaxf(r[k], s_rank_red[q][k]);
+        }
         PxbFrameResult* out = &results[slot];
         for (int k = 0; k < 3; ++k) { out->bounds_min[k] = r[k]; out->bounds_max[k] = r[k + 3]; }
         out->max_speed = sqrtf(r[6]);
         out->time = 0.0f;
     }
+    if constexpr (CL > 1) cg::this_cluster().sync();  // no rank leaves while its memory is read
 }
 
 // ------------------------------------------------------------------------------------------
@@ -560,45 +640,70 @@ cudaError_t launch_gather_positions(const PxbClothDev* cloths, const int32_t* or
     return cudaGetLastError();
 }
 
-template <int kMaxThreads>
+template <int kMaxThreads, int CL>
 static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
                                   const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                   const int32_t* order, PxbFrameResult* results, uint32_t* err,
-                                  int n_blocks, int threads, int smem_bytes, cudaStream_t stream) {
-    static uint64_t configured = 0;  // one bit per device the attribute has been set on
+                                  int n_cloths, int threads, int smem_bytes, cudaStream_t stream) {
+    static uint64_t configured = 0;  // one bit per device the attributes have been set on
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && !(configured >> dev & 1ull)) {
-        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads>,
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL>);
+        if (e != cudaSuccess) return e;
+        if (fa.sharedSizeBytes > static_cast<size_t>(kClothStaticSmem)) return cudaErrorInvalidConfiguration;
+        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
         if (e != cudaSuccess) return e;
         configured |= 1ull << dev;
     }
-    cloth_step_kernel<kMaxThreads><<<n_blocks, threads, smem_bytes, stream>>>(
-        cloths, steps, colliders, sources, order, results, err);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(n_cloths * CL));
+    cfg.blockDim = dim3(static_cast<unsigned>(threads));
+    cfg.dynamicSmemBytes = static_cast<size_t>(smem_bytes);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL>, cloths, steps, colliders,
+                              sources, order, results, err);
 }
 
 int cloth_variant_threads(int variant) {
     return variant == 0 ? 512 : (variant == 1 ? 768 : 1024);
 }
 
-cudaError_t launch_cloth_step(int variant, const PxbClothDev* cloths, const PxbClothStep* steps,
-                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
-                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
-                              int n_blocks, int threads, int smem_bytes, cudaStream_t stream) {
+template <int kMaxThreads>
+static cudaError_t launch_cl(int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
+                             const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                             const int32_t* order, PxbFrameResult* results, uint32_t* err,
+                             int n_cloths, int threads, int smem_bytes, cudaStream_t stream) {
+    switch (cluster) {
+        case 1: return launch_variant<kMaxThreads, 1>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
+        case 2: return launch_variant<kMaxThreads, 2>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
+        case 4: return launch_variant<kMaxThreads, 4>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
+        case 8: return launch_variant<kMaxThreads, 8>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloths,
+                              const PxbClothStep* steps, const PxbDevCollider* colliders,
+                              const pxb_gravity_source* sources, const int32_t* order,
+                              PxbFrameResult* results, uint32_t* err, int n_cloths, int threads,
+                              int smem_bytes, cudaStream_t stream) {
+    if (n_cloths <= 0) return cudaSuccess;
     if (threads > cloth_variant_threads(variant)) threads = cloth_variant_threads(variant);
     switch (variant) {
-        case 0:
-            return launch_variant<512>(cloths, steps, colliders, sources, order, results, err,
-                                       n_blocks, threads, smem_bytes, stream);
-        case 1:
-            return launch_variant<768>(cloths, steps, colliders, sources, order, results, err,
-                                       n_blocks, threads, smem_bytes, stream);
-        default:
-            return launch_variant<1024>(cloths, steps, colliders, sources, order, results, err,
-                                        n_blocks, threads, smem_bytes, stream);
+        case 0: return launch_cl<512>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
+        case 1: return launch_cl<768>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
+        default: return launch_cl<1024>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
     }
 }
 

@@ -45,32 +45,43 @@ struct alignas(16) PxbSeg {
     int32_t lam_base;   // lambda slot of item 0, or -1 when the colour has zero compliance
 };
 
+#define PXB_MAX_RANKS 8
+
+// One CTA of a cloth's thread-block cluster: it holds rows [row0, row0 + n_rows) of the layout,
+// its own colour segments (every item's `a` endpoint in its rows; `b` there or in the next
+// rank's rows), rest lengths and lambdas. A cloth that fits one CTA has one rank.
+struct PxbRank {
+    int32_t row0, n_rows;
+    int32_t seg_begin;                        // first segment of this rank in `segs`
+    int32_t colour_seg[PXB_MAX_COLOURS + 1];  // colour c = segs[seg_begin + colour_seg[c] ...)
+    int32_t rest_off, n_rest_pad;             // this rank's rest slots in `rest` (multiple of 4)
+    int32_t lam_off, n_lam;                   // this rank's lambda slots in `lam_out`
+    int32_t smem_bytes;                       // dynamic shared memory of this rank
+};
+
 // Static per-cloth description, device resident, written at registration.
 struct PxbClothDev {
     float4* pos;            // [n_layout] xyz + inv_mass
     float4* vel;            // [n_layout] xyz + (1 real particle, 0 ghost)
     float4* prv;            // [n_layout] prev_position (start of the last substep)
-    const float* rest;      // [n_rest_pad]
-    float* lam_out;         // [n_lam] lambdas left by the last substep (written when requested)
+    const float* rest;      // rest lengths, rank after rank
+    float* lam_out;         // lambdas left by the last substep, rank after rank
     const int32_t* anchor_of;   // [n_layout] anchor record index or -1
     const int2* tether;         // [n_layout] (anchor layout slot or -1, max_length bits)
     float* anchors;             // [n_anchors * 8] prev xyz, pad, world xyz, pad
-    const PxbSeg* segs;         // [n_segs]
-    int32_t n_segs;
+    const PxbSeg* segs;         // all ranks' segments
+    PxbRank rank[PXB_MAX_RANKS];
+    int32_t n_ranks;            // CTAs per cloth (cluster size)
+    int32_t rows_per_rank;      // rows of every rank but the last
     int32_t n_colours;
-    int32_t colour_seg[PXB_MAX_COLOURS + 1]; // colour c = segs [colour_seg[c], colour_seg[c+1])
-    int32_t colour_is_bend[PXB_MAX_COLOURS];
+    uint32_t cross_mask;        // bit c: colour c joins particles of different rows
     int32_t n_layout;
     int32_t n_real;
     int32_t columns, rows, Q, S;
-    int32_t n_rest_pad;     // multiple of 4
-    int32_t n_lam;          // lambda slots (compliant colours only, padded rows)
-    int32_t u_floats;       // floats of the union region (lambdas / velocity scratch)
     int32_t n_anchors;
-    int32_t smem_bytes;     // dynamic shared memory this cloth needs
-    int32_t threads;        // block size this cloth runs with
-    int32_t aero_grid;      // triangles are exactly make_grid_cloth's (cloth_builder.h:200-207)
-    int32_t pad_;
+    int32_t smem_bytes;         // max over ranks
+    int32_t threads;            // block size this cloth runs with
+    int32_t aero_grid;          // triangles are exactly make_grid_cloth's (cloth_builder.h:200-207)
 };
 
 // One anchor target pair as the device keeps it (ClothAnchor::prev_world_position /

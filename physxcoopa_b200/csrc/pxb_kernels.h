@@ -10,9 +10,11 @@
 
 namespace pxb {
 
-// Dynamic shared memory a cloth CTA may use: the sm_100 per-block limit (227 KB) minus the
-// kernel's static shared memory and a margin.
-constexpr int kMaxDynamicSmem = 232448 - 4096;
+// Static shared memory the cloth kernel may declare (checked against the compiled kernel before
+// its first launch on a device) and the dynamic shared memory left to a cloth CTA under the
+// sm_100 per-block limit of 227 KB.
+constexpr int kClothStaticSmem = 4352;
+constexpr int kMaxDynamicSmem = 232448 - kClothStaticSmem;
 constexpr int kClothOwned = 4;      // particles per thread in the cloth kernel
 constexpr int kClothMaxThreads = 1024;
 
@@ -20,10 +22,10 @@ constexpr int kClothMaxThreads = 1024;
 // threads (no spills), 1 = 768, 2 = 1024.
 constexpr int kClothVariants = 3;
 int cloth_variant_threads(int variant);
-cudaError_t launch_cloth_step(int variant, const PxbClothDev* cloths, const PxbClothStep* steps,
+cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,
-                              int n_blocks, int threads, int smem_bytes, cudaStream_t stream);
+                              int n_cloths, int threads, int smem_bytes, cudaStream_t stream);
 
 cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness,
                                   const float* pts, int n, float* out, float* normals,

@@ -283,24 +283,151 @@ float colour_compliance(const ClothEntry& e, int c) {
     return e.stretch_batch_comp.empty() ? e.params.stretch_compliance : e.stretch_batch_comp[b];
 }
 
-}  // namespace
 
-// Re-derives everything that depends on params: lambda slots, union region, shared memory.
-void pxb_context::refresh_layout(ClothEntry& e) {
-    int lam = 0;
-    for (int c = 0; c < e.n_colours; ++c) {
-        const bool has_lam = colour_compliance(e, c) != 0.0f;
-        for (int s = e.colour_seg[c]; s < e.colour_seg[c + 1]; ++s) {
-            e.segs[s].lam_base = has_lam ? lam : -1;
-            if (has_lam) lam += e.segs[s].count_pad;
+// Restricts the recognised colours to the rows of each of `n_ranks` CTAs and builds the device
+// segments (power-of-two rows). `refs` lists, in the colours' enumeration order, the reference
+// constraint of every item. Fills e.ranks / e.segs / e.n_rest_total and the padded slot map.
+bool build_ranks(ClothEntry& e, const std::vector<ColourSpec>& cs, const std::vector<int32_t>& refs,
+                 int n_ranks, std::vector<int32_t>& padded_ref, int& max_colour_items) {
+    const int S = e.S;
+    const int R = (e.rows + n_ranks - 1) / n_ranks;
+    e.ranks.assign(n_ranks, ClothEntry::Rank{});
+    e.segs.clear();
+    padded_ref.clear();
+    std::vector<std::vector<size_t>> seg_ref_off(cs.size());
+    size_t off = 0;
+    for (size_t c = 0; c < cs.size(); ++c)
+        for (const HostSeg& h : cs[c].segs) {
+            seg_ref_off[c].push_back(off);
+            off += static_cast<size_t>(h.count);
+        }
+    int rest_total = 0;
+    max_colour_items = 0;
+    for (int r = 0; r < n_ranks; ++r) {
+        ClothEntry::Rank& rk = e.ranks[r];
+        rk.row0 = r * R;
+        rk.n_rows = std::min(e.rows, (r + 1) * R) - rk.row0;
+        if (n_ranks > 1 && rk.n_rows < 2) return false;  // a bend reaches two rows ahead
+        rk.seg_begin = static_cast<int>(e.segs.size());
+        rk.colour_seg.assign(e.n_colours + 1, 0);
+        rk.rest_off = rest_total;
+        int rest = 0;
+        const int Y0 = rk.row0, Y1 = rk.row0 + rk.n_rows;
+        for (int c = 0; c < e.n_colours; ++c) {
+            rk.colour_seg[c] = static_cast<int>(e.segs.size()) - rk.seg_begin;
+            int items = 0;
+            for (size_t hi = 0; hi < cs[c].segs.size(); ++hi) {
+                const HostSeg& h = cs[c].segs[hi];
+                const int nrows = h.count / h.per_row;
+                const int y0 = h.a_base / S, step = h.row_stride / S;
+                const int r_lo = Y0 <= y0 ? 0 : (Y0 - y0 + step - 1) / step;
+                const int r_hi = Y1 <= y0 ? 0 : std::min(nrows, (Y1 - y0 + step - 1) / step);
+                if (r_hi <= r_lo) continue;
+                int shift = 0;
+                while ((1 << shift) < h.per_row) ++shift;
+                const int row_pad = 1 << shift;
+                PxbSeg g{};
+                g.count_pad = (r_hi - r_lo) * row_pad;
+                g.shift = shift;
+                g.per_row = h.per_row;
+                g.a_base = h.a_base + r_lo * h.row_stride - Y0 * S;
+                g.row_stride = h.row_stride;
+                g.d = h.d;
+                g.rest_base = rest;
+                g.lam_base = -1;
+                for (int i = 0; i < g.count_pad; ++i) {
+                    const int rr = i >> shift, k = i & (row_pad - 1);
+                    padded_ref.push_back(k < h.per_row
+                                             ? refs[seg_ref_off[c][hi] + static_cast<size_t>(r_lo + rr) * h.per_row + k]
+                                             : -1);
+                }
+                rest += g.count_pad;
+                items += g.count_pad;
+                e.segs.push_back(g);
+            }
+            max_colour_items = std::max(max_colour_items, items);
+        }
+        rk.colour_seg[e.n_colours] = static_cast<int>(e.segs.size()) - rk.seg_begin;
+        if (rk.colour_seg[e.n_colours] > PXB_MAX_SEGS) return false;
+        rk.n_rest_pad = (rest + 3) & ~3;
+        for (int i = rest; i < rk.n_rest_pad; ++i) padded_ref.push_back(-1);
+        rest_total += rk.n_rest_pad;
+    }
+    e.n_rest_total = rest_total;
+    return true;
+}
+
+// Every live item of every rank: `a` in this rank's rows, `b` in them or the next rank's, and
+// the pair is the reference constraint its rest slot says.
+bool verify_ranks(const ClothEntry& e, const pxb_cloth_desc* d) {
+    const int n_ranks = static_cast<int>(e.ranks.size());
+    for (int r = 0; r < n_ranks; ++r) {
+        const ClothEntry::Rank& rk = e.ranks[r];
+        const int n_local = rk.n_rows * e.S;
+        const int n_next = r + 1 < n_ranks ? e.ranks[r + 1].n_rows * e.S : 0;
+        const int base = rk.row0 * e.S;
+        for (int sg = rk.seg_begin; sg < rk.seg_begin + rk.colour_seg[e.n_colours]; ++sg) {
+            const PxbSeg& g = e.segs[sg];
+            const int mask = (1 << g.shift) - 1;
+            for (int i = 0; i < g.count_pad; ++i) {
+                const int k = i & mask;
+                const int32_t ref = e.rest_ref[rk.rest_off + g.rest_base + i];
+                if (k >= g.per_row) {
+                    if (ref != -1) return false;
+                    continue;
+                }
+                const int la = g.a_base + (i >> g.shift) * g.row_stride + k, lb = la + g.d;
+                if (la < 0 || la >= n_local || lb < 0 || lb >= n_local + n_next || ref < 0) return false;
+                const pxb_constraint& kc = ref < static_cast<int32_t>(d->n_stretch) ? d->stretch[ref]
+                                                                                    : d->bend[ref - d->n_stretch];
+                if (particle_of_slot(base + la, e.cols, e.rows, e.Q, e.S) != static_cast<int>(kc.a) ||
+                    particle_of_slot(base + lb, e.cols, e.rows, e.Q, e.S) != static_cast<int>(kc.b))
+                    return false;
+            }
         }
     }
-    e.n_lam = lam;
+    return true;
+}
+}  // namespace
+
+// Re-derives everything that depends on params: lambda slots, union regions, shared memory.
+static void layout_ranks(ClothEntry& e) {
     const bool aero = (e.params.air_drag > 0.0f || e.params.air_lift > 0.0f) && e.n_triangle_indices > 0;
-    const int u_floats = std::max(lam, (aero && e.aero_grid) ? 3 * e.n_layout : 0);
-    e.dev.n_lam = lam;
-    e.dev.u_floats = u_floats;
-    e.dev.smem_bytes = 16 * e.n_layout + 4 * e.n_rest_pad + 4 * ((u_floats + 3) & ~3);
+    int lam_total = 0, smem_max = 0;
+    for (size_t r = 0; r < e.ranks.size(); ++r) {
+        ClothEntry::Rank& rk = e.ranks[r];
+        int lam = 0;
+        for (int c = 0; c < e.n_colours; ++c) {
+            const bool has_lam = colour_compliance(e, c) != 0.0f;
+            for (int sg = rk.seg_begin + rk.colour_seg[c]; sg < rk.seg_begin + rk.colour_seg[c + 1]; ++sg) {
+                e.segs[sg].lam_base = has_lam ? lam : -1;
+                if (has_lam) lam += e.segs[sg].count_pad;
+            }
+        }
+        rk.n_lam = lam;
+        rk.lam_off = lam_total;
+        lam_total += lam;
+        const int n_local = rk.n_rows * e.S;
+        const int u_floats = std::max(lam, (aero && e.aero_grid) ? 3 * n_local : 0);
+        rk.smem = 16 * n_local + 4 * rk.n_rest_pad + 4 * ((u_floats + 3) & ~3);
+        smem_max = std::max(smem_max, rk.smem);
+        PxbRank& dr = e.dev.rank[r];
+        dr.row0 = rk.row0;
+        dr.n_rows = rk.n_rows;
+        dr.seg_begin = rk.seg_begin;
+        for (int c = 0; c <= e.n_colours; ++c) dr.colour_seg[c] = rk.colour_seg[c];
+        dr.rest_off = rk.rest_off;
+        dr.n_rest_pad = rk.n_rest_pad;
+        dr.lam_off = rk.lam_off;
+        dr.n_lam = rk.n_lam;
+        dr.smem_bytes = rk.smem;
+    }
+    e.n_lam = lam_total;
+    e.dev.smem_bytes = smem_max;
+}
+
+void pxb_context::refresh_layout(ClothEntry& e) {
+    layout_ranks(e);
     registry_dirty = true;
 }
 
@@ -348,8 +475,17 @@ pxb_status pxb_context::upload_anchor_records(ClothEntry& e) {
     return cuda(cudaStreamSynchronize(stream), "upload anchors");
 }
 
-pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
-    if (!d || !id_out) return fail(PXB_ERR_INVALID_ARGUMENT, "null argument");
+// Everything add_cloth decides before touching the device: validation, grid recognition, the
+// cluster size, per-rank colour segments (verified item by item against the constraint lists)
+// and the shared-memory layout. Needs no context, so the layout can be planned on any host.
+static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string& err) {
+    char buf[512];
+    auto fail = [&](pxb_status st, const char* fmt, auto... args) {
+        snprintf(buf, sizeof(buf), fmt, args...);
+        err = buf;
+        return st;
+    };
+    if (!d) return fail(PXB_ERR_INVALID_ARGUMENT, "null argument");
     if (d->n_particles == 0 || !d->particles)
         return fail(PXB_ERR_INVALID_ARGUMENT, "an empty cloth is refused (PhysicsWorld::add_cloth does the same)");
     if (d->params.self_collision && d->params.self_distance > PXB_EPSILON)
@@ -381,7 +517,6 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     // --- grid recognition ---
     if (d->columns < 2 || d->rows < 2 || d->columns * d->rows != n)
         return fail(PXB_ERR_UNSUPPORTED, "only make_grid_cloth sheets run on the device path");
-    ClothEntry e;
     e.cols = static_cast<int>(d->columns);
     e.rows = static_cast<int>(d->rows);
     e.Q = (e.cols + 3) / 4;
@@ -399,50 +534,16 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.aero_grid = d->n_triangle_indices > 0 ? 1 : 0;
     e.n_triangle_indices = d->n_triangle_indices;
 
-    // --- colours -> device segments with power-of-two rows, rest slots ---
+    // --- colours -> per-rank device segments; the smallest cluster whose ranks fit ---
     e.n_colours = static_cast<int>(cs.size());
-    e.colour_seg.assign(e.n_colours + 1, 0);
     e.colour_is_bend.assign(e.n_colours, 0);
     e.colour_batch = colour_batch;
-    int rest = 0;
-    size_t ref_pos = 0;
-    int max_colour = 0;
-    std::vector<int32_t> padded_ref;
+    e.cross_mask = 0;
     for (int c = 0; c < e.n_colours; ++c) {
-        e.colour_seg[c] = static_cast<int>(e.segs.size());
         e.colour_is_bend[c] = cs[c].bend ? 1 : 0;
-        int colour_items = 0;
-        for (const HostSeg& h : cs[c].segs) {
-            int shift = 0;
-            while ((1 << shift) < h.per_row) ++shift;
-            const int row_pad = 1 << shift;
-            const int nrows = h.count / h.per_row;
-            PxbSeg g{};
-            g.count_pad = nrows * row_pad;
-            g.shift = shift;
-            g.per_row = h.per_row;
-            g.a_base = h.a_base;
-            g.row_stride = h.row_stride;
-            g.d = h.d;
-            g.rest_base = rest;
-            g.lam_base = -1;
-            if (g.count_pad >= (1 << 24)) return fail(PXB_ERR_TOO_LARGE, "a colour segment is too large");
-            for (int i = 0; i < g.count_pad; ++i) {
-                const int r = i >> shift, k = i & (row_pad - 1);
-                padded_ref.push_back(k < h.per_row ? rest_ref[ref_pos + static_cast<size_t>(r) * h.per_row + k] : -1);
-            }
-            ref_pos += static_cast<size_t>(h.count);
-            rest += g.count_pad;
-            colour_items += g.count_pad;
-            e.segs.push_back(g);
-        }
-        max_colour = std::max(max_colour, colour_items);
+        for (const HostSeg& h : cs[c].segs)
+            if (h.a_base / e.S != (h.a_base + h.d) / e.S) e.cross_mask |= 1u << c;
     }
-    e.colour_seg[e.n_colours] = static_cast<int>(e.segs.size());
-    if (e.segs.size() > PXB_MAX_SEGS) return fail(PXB_ERR_TOO_LARGE, "too many colour segments");
-    rest_ref.swap(padded_ref);
-    e.n_rest_pad = (rest + 3) & ~3;
-    e.rest_ref = rest_ref;
     e.n_stretch = d->n_stretch;
     e.n_bend = d->n_bend;
     e.n_stretch_batches = d->n_stretch_batches;
@@ -452,6 +553,20 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     if (d->bend_batch_compliance)
         e.bend_batch_comp.assign(d->bend_batch_compliance, d->bend_batch_compliance + d->n_bend_batches);
     e.params = d->params;
+    e.n_triangle_indices = d->n_triangle_indices;
+    int max_colour = 0;
+    bool placed = false;
+    for (int cl = 1; cl <= PXB_MAX_RANKS && !placed; cl *= 2) {
+        std::vector<int32_t> padded;
+        if (!build_ranks(e, cs, rest_ref, cl, padded, max_colour)) continue;
+        e.rest_ref.swap(padded);
+        layout_ranks(e);
+        if (e.dev.smem_bytes <= kMaxDynamicSmem) placed = true;
+    }
+    if (!placed)
+        return fail(PXB_ERR_TOO_LARGE, "a %ux%u cloth does not fit a cluster of %d CTAs", d->columns, d->rows,
+                    PXB_MAX_RANKS);
+    if (!verify_ranks(e, d)) return fail(PXB_ERR_UNSUPPORTED, "colour segments do not reproduce the constraint lists");
     e.time = d->time;
     e.threads = std::min(kClothMaxThreads, std::max(64, ((max_colour + 1) / 2 + 31) & ~31));
     e.tethers.assign(d->tethers, d->tethers + d->n_tethers);
@@ -461,6 +576,16 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
             if (++per[t.particle] > 1)
                 return fail(PXB_ERR_UNSUPPORTED, "particle %u has more than one tether", t.particle);
     }
+
+    return PXB_OK;
+}
+
+pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
+    if (!d || !id_out) return fail(PXB_ERR_INVALID_ARGUMENT, "null argument");
+    ClothEntry e;
+    std::string msg;
+    if (pxb_status st = plan_cloth(d, e, msg)) return fail(st, "%s", msg.c_str());
+    const uint32_t n = d->n_particles;
 
     // --- anchors: one device record per anchor; a particle follows its LAST anchor ---
     e.anchors.assign(d->anchors, d->anchors + d->n_anchors);
@@ -483,8 +608,8 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
         tether[slot_of_particle(static_cast<int>(t.particle), e.cols, e.Q, e.S)] =
             make_int2(slot_of_particle(static_cast<int>(t.anchor), e.cols, e.Q, e.S), ml);
     }
-    std::vector<float> rest_h(e.n_rest_pad, 0.0f);
-    for (int s = 0; s < rest; ++s) {
+    std::vector<float> rest_h(e.n_rest_total, 0.0f);
+    for (int s = 0; s < e.n_rest_total; ++s) {
         const int32_t r = e.rest_ref[s];
         if (r < 0) continue;  // row padding
         rest_h[s] = r < static_cast<int32_t>(e.n_stretch) ? d->stretch[r].rest_length
@@ -503,16 +628,19 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
         return o;
     };
     const size_t o_pos = take(16 * L), o_vel = take(16 * L), o_prv = take(16 * L);
-    const size_t o_rest = take(4 * static_cast<size_t>(e.n_rest_pad));
-    const size_t o_lam = take(4 * static_cast<size_t>(rest));
+    const size_t o_rest = take(4 * static_cast<size_t>(e.n_rest_total));
+    const size_t o_lam = take(4 * static_cast<size_t>(e.n_rest_total));
     const size_t o_anc = take(4 * L), o_teth = take(8 * L);
     const size_t o_recs = take(sizeof(PxbAnchorRec) * e.anchor_recs.size());
-    const size_t o_segs = take(sizeof(PxbSeg) * PXB_MAX_SEGS);
+    const size_t o_segs = take(sizeof(PxbSeg) * e.segs.size());
     cudaError_t ce = cudaMalloc(&e.dmem, off);
     if (ce != cudaSuccess) return cuda(ce, "cudaMalloc(cloth)");
     e.dbytes = off;
     char* base = static_cast<char*>(e.dmem);
+    const PxbClothDev keep_ranks = e.dev;  // refresh_layout filled the rank fields
     std::memset(&e.dev, 0, sizeof(e.dev));
+    std::memcpy(e.dev.rank, keep_ranks.rank, sizeof(e.dev.rank));
+    e.dev.smem_bytes = keep_ranks.smem_bytes;
     e.dev.pos = reinterpret_cast<float4*>(base + o_pos);
     e.dev.vel = reinterpret_cast<float4*>(base + o_vel);
     e.dev.prv = reinterpret_cast<float4*>(base + o_prv);
@@ -522,26 +650,19 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.tether = reinterpret_cast<const int2*>(base + o_teth);
     e.dev.anchors = reinterpret_cast<float*>(base + o_recs);
     e.dev.segs = reinterpret_cast<const PxbSeg*>(base + o_segs);
-    e.dev.n_segs = static_cast<int32_t>(e.segs.size());
+    e.dev.n_ranks = static_cast<int32_t>(e.ranks.size());
+    e.dev.rows_per_rank = e.ranks[0].n_rows;
     e.dev.n_colours = e.n_colours;
-    for (int c = 0; c <= e.n_colours; ++c) e.dev.colour_seg[c] = e.colour_seg[c];
-    for (int c = 0; c < e.n_colours; ++c) e.dev.colour_is_bend[c] = e.colour_is_bend[c];
+    e.dev.cross_mask = e.cross_mask;
     e.dev.n_layout = e.n_layout;
     e.dev.n_real = static_cast<int32_t>(n);
     e.dev.columns = e.cols;
     e.dev.rows = e.rows;
     e.dev.Q = e.Q;
     e.dev.S = e.S;
-    e.dev.n_rest_pad = e.n_rest_pad;
     e.dev.n_anchors = static_cast<int32_t>(e.anchor_recs.size());
     e.dev.threads = e.threads;
     e.dev.aero_grid = e.aero_grid;
-    refresh_layout(e);
-    if (e.dev.smem_bytes > kMaxDynamicSmem) {
-        cudaFree(e.dmem);
-        return fail(PXB_ERR_TOO_LARGE, "cloth needs %d bytes of shared memory; the single-CTA path holds %d",
-                    e.dev.smem_bytes, kMaxDynamicSmem);
-    }
     pxb_status st = PXB_OK;
     auto up = [&](void* dst, const void* src, size_t bytes, const char* what) {
         if (st || bytes == 0) return;
@@ -551,7 +672,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     up(base + o_anc, anchor_of.data(), 4 * L, "upload anchor_of");
     up(base + o_teth, tether.data(), 8 * L, "upload tethers");
     if (!st) st = upload_segments(e);
-    if (!st) st = cuda(cudaMemsetAsync(base + o_lam, 0, 4 * static_cast<size_t>(rest), stream), "zero lambdas");
+    if (!st) st = cuda(cudaMemsetAsync(base + o_lam, 0, 4 * static_cast<size_t>(e.n_rest_total), stream), "zero lambdas");
     if (!st) st = upload_anchor_records(e);
     if (!st) st = upload_particles(e, d->particles);
     if (st) {
@@ -694,12 +815,21 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     auto* hs_order = reinterpret_cast<int32_t*>(hb + o_order);
     for (uint32_t k = 0; k < n_col; ++k) pxb_make_dev_collider(sd->colliders[k], hs_cols[k]);
     if (n_src) std::memcpy(hs_src, sd->sources, sizeof(pxb_gravity_source) * n_src);
-    int threads = 64, smem = 0;
+    // Launch slots grouped by cluster size (one launch per size), larger cloths first within a
+    // group so the block scheduler's tail holds the small ones.
+    std::vector<uint32_t> perm(n);
+    for (uint32_t k = 0; k < n; ++k) perm[k] = k;
+    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
+        const size_t rx = ents[x]->ranks.size(), ry = ents[y]->ranks.size();
+        if (rx != ry) return rx < ry;
+        return ents[x]->n_layout > ents[y]->n_layout;
+    });
     const pxb::hm::V3 g = pxb::hm::ld(sd->gravity);
-    for (uint32_t k = 0; k < n; ++k) {
+    for (uint32_t slot = 0; slot < n; ++slot) {
+        const uint32_t k = perm[slot];
         ClothEntry& e = *ents[k];
         const pxb_cloth_params& P = e.params;
-        PxbClothStep& s = hs_steps[k];
+        PxbClothStep& s = hs_steps[slot];
         std::memset(&s, 0, sizeof(s));
         // solve_cloth prologue (cloth_solver.h:165-194), evaluated exactly as the reference does
         const uint32_t steps = std::max<uint32_t>(1, P.substeps ? P.substeps : sd->substeps);
@@ -738,9 +868,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
         s.src_begin = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k]) : 0;
         s.src_count = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k + 1] - sd->source_offsets[k]) : 0;
         s.write_lambdas = 1;
-        hs_order[k] = static_cast<int32_t>(ents[k] - cloths.data());
-        threads = std::max(threads, e.threads);
-        smem = std::max(smem, e.dev.smem_bytes);
+        hs_order[slot] = static_cast<int32_t>(ents[k] - cloths.data());
         // Cloth::time advances by hs per substep (cloth_solver.h:453), mirrored on the host.
         for (uint32_t q = 0; q < steps; ++q) e.time += hs;
         // Anchors reach their targets: next step lerps from here (cloth_solver.h:457).
@@ -750,16 +878,28 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     char* db = static_cast<char*>(d_stage.p);
     if (pxb_status s = cuda(cudaMemcpyAsync(db, hb, total, cudaMemcpyHostToDevice, stream), "upload step")) return s;
     cudaEventRecord(staged, stream);
-    cudaError_t le = launch_cloth_step(cloth_variant, static_cast<const PxbClothDev*>(d_registry.p),
-                                       reinterpret_cast<const PxbClothStep*>(db),
-                                       reinterpret_cast<const PxbDevCollider*>(db + o_cols),
-                                       reinterpret_cast<const pxb_gravity_source*>(db + o_src),
-                                       reinterpret_cast<const int32_t*>(db + o_order),
-                                       static_cast<PxbFrameResult*>(d_results.p), d_err,
-                                       static_cast<int>(n), threads, smem, stream);
-    if (le != cudaSuccess) return cuda(le, "launch cloth_step");
-    ++launches;
-    last_step.assign(sd->cloths, sd->cloths + n);
+    for (uint32_t g0 = 0; g0 < n;) {
+        const int cluster = static_cast<int>(ents[perm[g0]]->ranks.size());
+        uint32_t g1 = g0;
+        int threads = 64, smem = 0;
+        while (g1 < n && static_cast<int>(ents[perm[g1]]->ranks.size()) == cluster) {
+            threads = std::max(threads, ents[perm[g1]]->threads);
+            smem = std::max(smem, ents[perm[g1]]->dev.smem_bytes);
+            ++g1;
+        }
+        cudaError_t le = launch_cloth_step(cloth_variant, cluster, static_cast<const PxbClothDev*>(d_registry.p),
+                                           reinterpret_cast<const PxbClothStep*>(db) + g0,
+                                           reinterpret_cast<const PxbDevCollider*>(db + o_cols),
+                                           reinterpret_cast<const pxb_gravity_source*>(db + o_src),
+                                           reinterpret_cast<const int32_t*>(db + o_order) + g0,
+                                           static_cast<PxbFrameResult*>(d_results.p) + g0, d_err,
+                                           static_cast<int>(g1 - g0), threads, smem, stream);
+        if (le != cudaSuccess) return cuda(le, "launch cloth_step");
+        ++launches;
+        g0 = g1;
+    }
+    last_step.resize(n);
+    for (uint32_t slot = 0; slot < n; ++slot) last_step[slot] = sd->cloths[perm[slot]];
     results_fresh = false;
     return PXB_OK;
 }
@@ -852,6 +992,27 @@ pxb_status pxb_cloth_add(pxb_context* ctx, const pxb_cloth_desc* desc, uint64_t*
     return ctx->add_cloth(desc, id_out);
 }
 
+pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out, char* err, uint32_t err_cap) {
+    if (err && err_cap) err[0] = 0;
+    if (!out) return PXB_ERR_INVALID_ARGUMENT;
+    ClothEntry e;
+    std::string msg;
+    const pxb_status st = plan_cloth(desc, e, msg);
+    if (st) {
+        if (err && err_cap) snprintf(err, err_cap, "%s", msg.c_str());
+        return st;
+    }
+    out->n_ranks = static_cast<int32_t>(e.ranks.size());
+    out->rows_per_rank = e.ranks[0].n_rows;
+    out->threads = e.threads;
+    out->smem_bytes = e.dev.smem_bytes;
+    out->n_colours = e.n_colours;
+    out->n_segments = static_cast<int32_t>(e.segs.size());
+    out->layout_slots = e.n_layout;
+    out->constraint_slots = e.n_rest_total;
+    return PXB_OK;
+}
+
 pxb_status pxb_cloth_remove(pxb_context* ctx, uint64_t id) {
     if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
     ClothEntry* e = ctx->lookup(id);
@@ -933,14 +1094,14 @@ pxb_status pxb_cloth_read_lambdas(pxb_context* ctx, uint64_t id, float* stretch_
     if (s) return s;
     if (stretch_out) std::fill(stretch_out, stretch_out + n_stretch, 0.0f);
     if (bend_out) std::fill(bend_out, bend_out + n_bend, 0.0f);
-    for (int c = 0; c < e->n_colours; ++c) {
-        for (int sg = e->colour_seg[c]; sg < e->colour_seg[c + 1]; ++sg) {
+    for (const ClothEntry::Rank& rk : e->ranks) {
+        for (int sg = rk.seg_begin; sg < rk.seg_begin + rk.colour_seg[e->n_colours]; ++sg) {
             const PxbSeg& g = e->segs[sg];
             if (g.lam_base < 0) continue;
             for (int i = 0; i < g.count_pad; ++i) {
-                const int32_t r = e->rest_ref[g.rest_base + i];
+                const int32_t r = e->rest_ref[rk.rest_off + g.rest_base + i];
                 if (r < 0) continue;  // row padding
-                const float v = lam[g.lam_base + i];
+                const float v = lam[rk.lam_off + g.lam_base + i];
                 if (r < static_cast<int32_t>(e->n_stretch)) { if (stretch_out) stretch_out[r] = v; }
                 else if (bend_out) bend_out[r - e->n_stretch] = v;
             }

@@ -28,13 +28,20 @@ struct ClothEntry {
     uint32_t n_particles = 0;
     int cols = 0, rows = 0, Q = 0, S = 0, n_layout = 0;
     int n_colours = 0;
-    std::vector<PxbSeg> segs;
-    std::vector<int> colour_seg;
+    std::vector<PxbSeg> segs;              // every rank's device segments, rank after rank
     std::vector<int> colour_is_bend;
+    // One CTA of the cloth's cluster (see PxbRank); the host keeps the same fields.
+    struct Rank {
+        int row0 = 0, n_rows = 0, seg_begin = 0;
+        std::vector<int> colour_seg;       // relative to seg_begin, n_colours + 1 entries
+        int rest_off = 0, n_rest_pad = 0, lam_off = 0, n_lam = 0, smem = 0;
+    };
+    std::vector<Rank> ranks;
+    uint32_t cross_mask = 0;
     std::vector<int32_t> colour_batch;     // colour -> reference batch index in its list
-    std::vector<int32_t> rest_ref;         // rest slot -> stretch index, or n_stretch + bend index (-1 padding)
-    int n_rest_pad = 0;
-    int n_lam = 0;
+    std::vector<int32_t> rest_ref;         // global rest slot -> stretch index, or n_stretch + bend index (-1 padding)
+    int n_rest_total = 0;
+    int n_lam = 0;                         // lambda slots over all ranks
     int threads = 64;
     int aero_grid = 0;
     uint32_t n_triangle_indices = 0;

@@ -35,6 +35,7 @@ SIGNATURES = {
     "pxb_cloth_params_default": ([C.POINTER(A.ClothParams)], None),
     "pxb_cloth_add": ([P, C.POINTER(A.ClothDesc), C.POINTER(u64)], C.c_int),
     "pxb_cloth_remove": ([P, u64], C.c_int),
+    "pxb_cloth_plan_layout": ([C.POINTER(A.ClothDesc), C.POINTER(A.ClothPlan), C.c_char_p, u32], C.c_int),
     "pxb_cloth_set_params": ([P, u64, C.POINTER(A.ClothParams)], C.c_int),
     "pxb_cloth_write_particles": ([P, u64, P, u32], C.c_int),
     "pxb_cloth_read_particles": ([P, u64, P, u32], C.c_int),
@@ -102,6 +103,18 @@ def library():
 
 def _vec(x, n=3):
     return (C.c_float * n)(*[float(v) for v in x])
+
+
+def plan_cloth(c: ClothArrays) -> dict:
+    """The device layout pxb_cloth_add would give this cloth (no GPU needed); raises PxbError
+    with the library's message for a cloth it would refuse."""
+    d = c.desc()
+    out = A.ClothPlan()
+    err = C.create_string_buffer(512)
+    st = library().pxb_cloth_plan_layout(C.byref(d), C.byref(out), err, 512)
+    if st:
+        raise PxbError(st, err.value.decode())
+    return out.as_dict()
 
 
 class HostCloth:

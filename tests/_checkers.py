@@ -88,8 +88,8 @@ def ref():
         lib.pxbref_solve_cloth.argtypes = [P, P, A.u32, f32p, A.u32, A.u32, A.f32]
         lib.pxbref_project_particle.argtypes = [P, A.f32, f32p, f32p, f32p, P]
         lib.pxbref_project_particle.restype = C.c_int
-        lib.pxbref_bench_cloths.argtypes = [C.POINTER(P), A.u32, P, P, f32p, A.u32, A.u32, A.f32,
-                                            A.u32, A.u32]
+        lib.pxbref_bench_cloths.argtypes = [C.POINTER(P), A.u32, P, P, P, P, f32p, A.u32, A.u32,
+                                            A.f32, A.u32, A.u32]
         lib.pxbref_bench_cloths.restype = C.c_double
         lib.pxbref_strands_make.argtypes = [A.u32, P, P, P, P, C.POINTER(A.StrandParams)]
         lib.pxbref_strands_make.restype = P

@@ -367,3 +367,91 @@ def test_reference_drape_pin_through_the_device(ctx):
     assert (np.linalg.norm(pos[st["a"]] - pos[st["b"]], axis=1) / st["rest_length"]).max() < 1.25
     assert ctx.read_results([cid])[0]["bounds_min"][2] < centre[2]
     ctx.remove_cloth(cid)
+
+
+# --- cloths split over a thread-block cluster --------------------------------------------------
+
+def clustered_sheet(cols, rows, seed, pins="corners", params=None):
+    w, hgt = 0.05 * (cols - 1), 0.05 * (rows - 1)
+    h = R.HostCloth(cols, rows, w, hgt, center=(0, 0, 1), params=params or scenes.cloth_params(),
+                    jitter=1e-3, seed=seed)
+    arr = h.arrays()
+    if pins == "edge":
+        for p in arr.particles["position"][(rows - 1) * cols:]:
+            h.pin_static(tuple(p), 0.01)
+    else:
+        h.pin_static((-w / 2, hgt / 2, 1), 0.02)
+        h.pin_static((w / 2, hgt / 2, 1), 0.02)
+    h.build_tethers()
+    return h.arrays()
+
+
+CLUSTERED = {
+    # (columns, rows); the planner gives these 2, 4, 8, 4 and 2 CTAs
+    "c2_65": dict(shape=(65, 65), cols=[sphere(0.5, (0.1, 0, 0.4))]),
+    "c4_80_sources": dict(shape=(80, 80), cols=[capsule(0.2, 0.5, (0, 0, 0.5), axis=0)],
+                          sources=[((0.5, -0.3, -2.0), 9.81, 1.0, 10.0)]),
+    "c8_128_edge": dict(shape=(128, 128), pins="edge",
+                        cols=[box((0.6, 0.5, 0.4), (0.2, 0.1, 0.3), (0.0, 0.3826834, 0.0, 0.9238795))]),
+    "c4_tall_40x180": dict(shape=(40, 180), cols=[sphere(0.6, (0, 0.5, 0.2))]),
+    "c2_wind_97x61": dict(shape=(97, 61), params=dict(wind=(0.5, 0.2, 0.0), wind_turbulence=0.5)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CLUSTERED))
+def test_clustered_cloth_equals_oracle(ctx, name):
+    """Cloths too large for one CTA's shared memory run on a cluster of CTAs (rows split, the
+    neighbour rows read through distributed shared memory); results equal the oracle's."""
+    sc = CLUSTERED[name]
+    params = scenes.cloth_params(**{k: (A.C.c_float * 3)(*v) if isinstance(v, tuple) else v
+                                    for k, v in sc.get("params", {}).items()})
+    cloth = clustered_sheet(*sc["shape"], seed=11, pins=sc.get("pins", "corners"), params=params)
+    plan = R.plan_cloth(cloth)
+    assert plan["n_ranks"] > 1, plan
+    cols = collider_array(sc["cols"]) if sc.get("cols") else None
+    src = gravity_sources(sc["sources"]) if sc.get("sources") else None
+    gpu, orc, res_, lam, t = run_pair(ctx, cloth, cols, sources=src, steps=1)
+    assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-5
+    assert_pins_exact(gpu, orc.particles)
+    gpu, orc, res_, lam, t = run_pair(ctx, cloth, cols, sources=src, steps=30)
+    assert_equal_particles(gpu, orc.particles, name)
+    assert np.float32(t) == np.float32(orc.time)
+    assert np.array_equal(res_["bounds_min"], orc.bounds[:3])
+    assert np.array_equal(res_["bounds_max"], orc.bounds[3:])
+    assert np.float32(res_["max_speed"]) == K.oracle().orc_max_particle_speed(
+        A.ptr(orc.particles), len(orc.particles))
+    assert np.array_equal(lam[1], orc.bend["lambda"])
+    sh = orc.stretch["lambda"]
+    assert np.array_equal(lam[0][sh != 0], sh[sh != 0])  # structural (compliance 0) keeps none
+
+
+def test_batch_of_every_cluster_size(ctx):
+    """One step call over cloths of every cluster size: one launch per size, all equal to the
+    oracle, positions gathered in the caller's order."""
+    shapes = [(20, 20), (128, 128), (64, 64), (65, 65), (90, 90), (16, 16), (72, 72)]
+    cloths = [clustered_sheet(c, r, seed=k) for k, (c, r) in enumerate(shapes)]
+    sizes = {R.plan_cloth(c)["n_ranks"] for c in cloths}
+    assert sizes == {1, 2, 4, 8}
+    cols = [collider_array([sphere(0.3 + 0.05 * k, (0.05 * k, 0, 0.4))]) for k in range(len(cloths))]
+    orcs = [c.copy() for c in cloths]
+    ids = [ctx.add_cloth(c) for c in cloths]
+    n0 = ctx.launch_count
+    for _ in range(5):
+        ctx.step(ids, cols)
+        for o, c in zip(orcs, cols):
+            K.oracle_step_cloth(o, c, substeps=4, iterations=10)
+    assert ctx.launch_count - n0 == 5 * len(sizes)
+    total = sum(len(c.particles) for c in cloths)
+    out = np.zeros(3 * total, np.float32)
+    ctx.read_positions(ids, out)
+    res = ctx.read_results(ids)
+    off = 0
+    for k, (cid, o) in enumerate(zip(ids, orcs)):
+        g = ctx.read_particles(cid, len(o.particles))
+        assert_equal_particles(g, o.particles, f"cloth {shapes[k]}")
+        n = len(o.particles)
+        assert np.array_equal(out[off:off + 3 * n].reshape(-1, 3), o.particles["position"])
+        assert np.array_equal(res[k]["bounds_min"], o.bounds[:3])
+        off += 3 * n
+    for cid in ids:
+        ctx.remove_cloth(cid)

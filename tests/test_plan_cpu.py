@@ -1,0 +1,91 @@
+"""Device layout planning on the host (pxb_cloth_plan_layout): no GPU needed.
+
+pxb_cloth_add recognises a make_grid_cloth sheet, chooses how many CTAs hold it (a cloth whose
+positions, rest lengths and lambdas overflow one CTA's shared memory is split by rows over a
+thread-block cluster), restricts every colour's affine segments to each CTA's rows and verifies
+every device item against the reference constraint it replaces. The same planner runs here on the
+CPU, so these tests cover the verification for every size of the uneven benchmark batch.
+"""
+import numpy as np
+import pytest
+
+from physxcoopa_b200 import _abi as A
+from physxcoopa_b200 import runtime as R
+from physxcoopa_b200 import scenes
+
+SMEM_LIMIT = 232448 - 4352  # sm_100 per-block limit minus the kernel's static shared memory
+
+
+def sheet(cols, rows, shear=True, params=None):
+    w = 0.05 * (cols - 1)
+    hgt = 0.05 * (rows - 1)
+    return R.HostCloth(cols, rows, w, hgt, shear=shear, params=params or scenes.cloth_params(),
+                       jitter=1e-3, seed=cols * 1000 + rows).arrays()
+
+
+def test_every_uneven_batch_side_plans():
+    for side in range(16, 129):
+        p = R.plan_cloth(sheet(side, side))
+        assert p["n_ranks"] in (1, 2, 4, 8)
+        assert 0 < p["smem_bytes"] <= SMEM_LIMIT
+        assert p["rows_per_rank"] * p["n_ranks"] >= side
+        assert p["rows_per_rank"] >= 2
+        assert p["threads"] % 32 == 0 and 64 <= p["threads"] <= 1024
+        assert p["layout_slots"] == side * 4 * ((side + 3) // 4)
+        assert p["n_colours"] == 16
+
+
+def test_headline_sheet_stays_in_one_cta():
+    p = R.plan_cloth(sheet(64, 64))
+    assert p["n_ranks"] == 1 and p["threads"] == 1024
+
+
+@pytest.mark.parametrize("shape", [(2, 2), (5, 5), (17, 6), (128, 16), (16, 128), (3, 200),
+                                   (200, 3), (97, 61), (64, 65), (150, 150)])
+@pytest.mark.parametrize("shear", [True, False])
+def test_rectangles_and_no_shear_plan(shape, shear):
+    p = R.plan_cloth(sheet(*shape, shear=shear))
+    assert p["smem_bytes"] <= SMEM_LIMIT
+    assert p["n_colours"] == (16 if shear else 12) or min(shape) < 8
+
+
+def test_aero_off_needs_less_memory():
+    on = R.plan_cloth(sheet(64, 64))
+    off = R.plan_cloth(sheet(64, 64, params=scenes.cloth_params(air_drag=0.0, air_lift=0.0)))
+    assert off["smem_bytes"] <= on["smem_bytes"]
+
+
+def test_too_large_and_refusals_match_add_cloth():
+    with pytest.raises(R.PxbError) as e:
+        R.plan_cloth(sheet(181, 181))
+    assert e.value.status == 7  # PXB_ERR_TOO_LARGE
+    assert "cluster" in str(e.value)
+    ok = sheet(9, 9)
+    odd = ok.copy()
+    odd.stretch = odd.stretch[::-1].copy()
+    with pytest.raises(R.PxbError) as e:
+        R.plan_cloth(odd)
+    assert e.value.status == 2
+    empty = ok.copy()
+    empty.particles = empty.particles[:0]
+    with pytest.raises(R.PxbError) as e:
+        R.plan_cloth(empty)
+    assert e.value.status == 1
+    p = A.ClothParams.defaults()
+    p.self_collision = 1
+    p.self_distance = 0.1
+    with pytest.raises(R.PxbError) as e:
+        R.plan_cloth(sheet(9, 9, params=p))
+    assert e.value.status == 2
+
+
+def test_swapped_pair_is_caught_by_item_verification():
+    """Reversing one bend constraint's endpoints keeps the lists' shape but not the device's
+    (a, b) order: the planner must refuse rather than solve a different pair order."""
+    c = sheet(20, 20)
+    k = len(c.bend) // 2
+    a, b = int(c.bend[k]["a"]), int(c.bend[k]["b"])
+    c.bend[k]["a"], c.bend[k]["b"] = b, a
+    with pytest.raises(R.PxbError) as e:
+        R.plan_cloth(c)
+    assert e.value.status == 2

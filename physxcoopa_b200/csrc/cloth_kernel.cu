@@ -679,6 +679,19 @@ int cloth_variant_threads(int variant) {
     return variant == 0 ? 512 : (variant == 1 ? 768 : 1024);
 }
 
+int cloth_variant_registers(int variant) {
+    static int regs[kClothVariants] = {0, 0, 0};
+    const int v = variant < 0 ? 0 : (variant >= kClothVariants ? kClothVariants - 1 : variant);
+    if (!regs[v]) {
+        cudaFuncAttributes fa;
+        cudaError_t e = v == 0 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<512, 1>)
+                               : (v == 1 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<768, 1>)
+                                         : cudaFuncGetAttributes(&fa, cloth_step_kernel<1024, 1>));
+        regs[v] = e == cudaSuccess ? fa.numRegs : 255;
+    }
+    return regs[v];
+}
+
 template <int kMaxThreads>
 static cudaError_t launch_cl(int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,

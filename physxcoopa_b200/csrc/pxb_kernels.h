@@ -22,6 +22,8 @@ constexpr int kClothMaxThreads = 1024;
 // threads (no spills), 1 = 768, 2 = 1024.
 constexpr int kClothVariants = 3;
 int cloth_variant_threads(int variant);
+// Registers per thread of a variant's one-CTA kernel (read from the compiled kernel once).
+int cloth_variant_registers(int variant);
 cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,

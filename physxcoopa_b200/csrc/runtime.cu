@@ -284,6 +284,16 @@ float colour_compliance(const ClothEntry& e, int c) {
 }
 
 
+// CTAs of the cloth kernel one SM holds at once: 228 KB of shared memory (1 KB of it reserved
+// per CTA), 2048 threads, 64 K registers, 32 CTAs.
+int ctas_per_sm(int smem_bytes, int threads, int regs) {
+    const int warps = (threads + 31) / 32;
+    const int by_smem = 233472 / (smem_bytes + kClothStaticSmem + 1024);
+    const int by_threads = 64 / std::max(warps, 1);
+    const int by_regs = 65536 / std::max(warps * 32 * ((regs + 7) & ~7), 1);
+    return std::max(1, std::min(std::min(by_smem, by_threads), std::min(by_regs, 32)));
+}
+
 // Restricts the recognised colours to the rows of each of `n_ranks` CTAs and builds the device
 // segments (power-of-two rows). `refs` lists, in the colours' enumeration order, the reference
 // constraint of every item. Fills e.ranks / e.segs / e.n_rest_total and the padded slot map.
@@ -361,6 +371,7 @@ bool build_ranks(ClothEntry& e, const std::vector<ColourSpec>& cs, const std::ve
 // the pair is the reference constraint its rest slot says.
 bool verify_ranks(const ClothEntry& e, const pxb_cloth_desc* d) {
     const int n_ranks = static_cast<int>(e.ranks.size());
+    std::vector<uint8_t> seen(static_cast<size_t>(d->n_stretch) + d->n_bend, 0);
     for (int r = 0; r < n_ranks; ++r) {
         const ClothEntry::Rank& rk = e.ranks[r];
         const int n_local = rk.n_rows * e.S;
@@ -383,9 +394,12 @@ bool verify_ranks(const ClothEntry& e, const pxb_cloth_desc* d) {
                 if (particle_of_slot(base + la, e.cols, e.rows, e.Q, e.S) != static_cast<int>(kc.a) ||
                     particle_of_slot(base + lb, e.cols, e.rows, e.Q, e.S) != static_cast<int>(kc.b))
                     return false;
+                if (seen[ref]++) return false;  // solved twice
             }
         }
     }
+    for (uint8_t v : seen)
+        if (!v) return false;  // never solved
     return true;
 }
 }  // namespace
@@ -815,13 +829,20 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     auto* hs_order = reinterpret_cast<int32_t*>(hb + o_order);
     for (uint32_t k = 0; k < n_col; ++k) pxb_make_dev_collider(sd->colliders[k], hs_cols[k]);
     if (n_src) std::memcpy(hs_src, sd->sources, sizeof(pxb_gravity_source) * n_src);
-    // Launch slots grouped by cluster size (one launch per size), larger cloths first within a
-    // group so the block scheduler's tail holds the small ones.
+    // Launch slots grouped by cluster size and by how many of the cloth's CTAs one SM holds
+    // (shared memory, threads, registers): one launch per group, so a small cloth is not
+    // launched with a large one's shared memory and thread count. Larger cloths first within a
+    // group, so the block scheduler's tail holds the small ones.
+    const int cap = cloth_variant_threads(cloth_variant);
+    const int regs = cloth_variant_registers(cloth_variant);
+    std::vector<int> fit(n);
+    for (uint32_t k = 0; k < n; ++k) fit[k] = ctas_per_sm(ents[k]->dev.smem_bytes, std::min(ents[k]->threads, cap), regs);
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
         const size_t rx = ents[x]->ranks.size(), ry = ents[y]->ranks.size();
         if (rx != ry) return rx < ry;
+        if (fit[x] != fit[y]) return fit[x] < fit[y];
         return ents[x]->n_layout > ents[y]->n_layout;
     });
     const pxb::hm::V3 g = pxb::hm::ld(sd->gravity);
@@ -880,9 +901,10 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     cudaEventRecord(staged, stream);
     for (uint32_t g0 = 0; g0 < n;) {
         const int cluster = static_cast<int>(ents[perm[g0]]->ranks.size());
+        const int group_fit = fit[perm[g0]];
         uint32_t g1 = g0;
         int threads = 64, smem = 0;
-        while (g1 < n && static_cast<int>(ents[perm[g1]]->ranks.size()) == cluster) {
+        while (g1 < n && static_cast<int>(ents[perm[g1]]->ranks.size()) == cluster && fit[perm[g1]] == group_fit) {
             threads = std::max(threads, ents[perm[g1]]->threads);
             smem = std::max(smem, ents[perm[g1]]->dev.smem_bytes);
             ++g1;

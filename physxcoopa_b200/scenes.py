@@ -194,3 +194,22 @@ def hair_groom(n_strands=65536, count=32, segment=0.01, seed=3, iterations=20):
     return StrandScene(f"hair_groom {n_strands}x{count}", [s], [colliders(0)], root_path=root_path,
                        iterations=iterations,
                        meta={"n_strands": n_strands, "count": count, "colliders_at": colliders})
+
+
+def hanging_strands(n_strands=256, count=32, segment=0.01, tilt=0.3, seed=7, iterations=20):
+    """Strands hanging from a square grid of roots (2 cm pitch) at z = 1 m, each tilted from
+    straight down by a seeded U(-tilt, tilt) in x and y: they swing to rest under gravity, a
+    stable equilibrium (unlike a groom growing upward, whose strands buckle). Static roots, no
+    colliders, reference StrandParams defaults."""
+    from .runtime import make_strands
+    rng = np.random.default_rng(seed)
+    g = int(np.ceil(np.sqrt(n_strands)))
+    xs, ys = np.meshgrid(np.arange(g) * 0.02, np.arange(g) * 0.02)
+    roots = np.stack([xs.ravel(), ys.ravel(), np.ones(g * g)], 1)[:n_strands].astype(np.float32)
+    d = np.concatenate([rng.uniform(-tilt, tilt, (n_strands, 2)), -np.ones((n_strands, 1))], 1)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    k = np.arange(count)[None, :, None]
+    pts = (roots[:, None, :] + d[:, None, :] * segment * k).astype(np.float32)
+    s = make_strands(list(pts))
+    return StrandScene(f"hanging_strands {n_strands}x{count}", [s], [None], iterations=iterations,
+                       meta={"n_strands": n_strands, "count": count})

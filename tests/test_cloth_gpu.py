@@ -214,7 +214,7 @@ def test_kernel_variants_agree_and_autotune_restores_state(ctx):
     ctx.set_cloth_variant(0)
 
 
-def test_batch_of_mixed_sizes_in_one_launch(ctx):
+def test_batch_of_mixed_sizes_in_one_call(ctx):
     cloths, cols = [], []
     for k, side in enumerate([5, 16, 33, 64, 2, 47]):
         h = R.HostCloth(side, side, 0.05 * (side - 1), 0.05 * (side - 1), center=(0, 0, 1),
@@ -232,7 +232,8 @@ def test_batch_of_mixed_sizes_in_one_launch(ctx):
         ctx.step(ids, cols, substeps=4, iterations=10)
         for o, c in zip(orcs, cols):
             K.oracle_step_cloth(o, c, substeps=4, iterations=10)
-    assert ctx.launch_count - n0 == 10  # one launch per step for the whole batch
+    # one launch per (cluster size, CTAs per SM) group: at most one per cloth, fewer here
+    assert 10 <= ctx.launch_count - n0 < 10 * len(cloths)
     total = sum(len(c.particles) for c in cloths)
     out = np.zeros(3 * total, np.float32)
     ctx.read_positions(ids, out)
@@ -421,13 +422,25 @@ def test_clustered_cloth_equals_oracle(ctx, name):
     assert np.float32(res_["max_speed"]) == K.oracle().orc_max_particle_speed(
         A.ptr(orc.particles), len(orc.particles))
     assert np.array_equal(lam[1], orc.bend["lambda"])
-    sh = orc.stretch["lambda"]
-    assert np.array_equal(lam[0][sh != 0], sh[sh != 0])  # structural (compliance 0) keeps none
+    # stretch list: structural batches (compliance 0, no lambda kept on the device) and shear
+    # batches (compliance 1e-6), compared where the batch is compliant
+    keep = compliant_mask(cloth.stretch_batches, cloth.stretch_batch_compliance, len(cloth.stretch))
+    assert keep.any() and not keep.all()
+    assert np.array_equal(lam[0][keep], orc.stretch["lambda"][keep])
+    assert not lam[0][~keep].any()
+
+
+def compliant_mask(batches, compliance, n):
+    m = np.zeros(n, bool)
+    for b, c in zip(batches, compliance):
+        if c != 0.0:
+            m[b["begin"]:b["end"]] = True
+    return m
 
 
 def test_batch_of_every_cluster_size(ctx):
-    """One step call over cloths of every cluster size: one launch per size, all equal to the
-    oracle, positions gathered in the caller's order."""
+    """One step call over cloths of every cluster size: at least one launch per size, all equal
+    to the oracle, positions gathered in the caller's order."""
     shapes = [(20, 20), (128, 128), (64, 64), (65, 65), (90, 90), (16, 16), (72, 72)]
     cloths = [clustered_sheet(c, r, seed=k) for k, (c, r) in enumerate(shapes)]
     sizes = {R.plan_cloth(c)["n_ranks"] for c in cloths}
@@ -440,7 +453,7 @@ def test_batch_of_every_cluster_size(ctx):
         ctx.step(ids, cols)
         for o, c in zip(orcs, cols):
             K.oracle_step_cloth(o, c, substeps=4, iterations=10)
-    assert ctx.launch_count - n0 == 5 * len(sizes)
+    assert 5 * len(sizes) <= ctx.launch_count - n0 < 5 * len(cloths)
     total = sum(len(c.particles) for c in cloths)
     out = np.zeros(3 * total, np.float32)
     ctx.read_positions(ids, out)

@@ -129,6 +129,92 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
+// ------------------------------------------------------------------------------------------
+// One colour segment: project_distance (cloth_solver.h:119-138) for every item
+// ------------------------------------------------------------------------------------------
+
+// Items of one colour share no particle, so with registers to spare (512-thread blocks) a
+// thread takes two per pass and loads both before storing either: two independent dependency
+// chains (square root, divisions) in flight per thread. The reference's early returns (both endpoints pinned; coincident endpoints) become a
+// predicate on the stores, with its comparisons kept as written (a NaN weight is not skipped).
+// Padding slots at row ends and a second item past the segment read item 0's slots and store
+// nothing. h0 = {count_pad, shift, per_row, a_base}, h1 = {row_stride, d, rest_base, lam_base}.
+struct PairItem {
+    float4* pa;
+    float4* pb;
+    float4 a, b;
+    float rest, lam;
+    bool live;
+};
+
+template <int CL, bool kLam>
+__device__ __forceinline__ void load_item(PairItem& it, float4* pos, float4* pos_next, const float* rest,
+                                          const float* lamv, int n_local, int i, int count_pad, int shift,
+                                          int per_row, int a_base, int row_stride, int d) {
+    const int mask = (1 << shift) - 1;
+    const int k = i & mask;
+    it.live = i < count_pad && k < per_row;
+    const int ii = it.live ? i : 0;
+    const int la = it.live ? a_base + (i >> shift) * row_stride + k : a_base;
+    const int lb = la + d;
+    it.pa = &pos[la];
+    it.pb = (CL == 1 || lb < n_local) ? &pos[lb] : &pos_next[lb - n_local];
+    it.a = *it.pa;
+    it.b = *it.pb;
+    it.rest = rest[ii];
+    it.lam = kLam ? lamv[ii] : 0.0f;
+}
+
+template <bool kLam>
+__device__ __forceinline__ void project_item(PairItem& it, float* lamv, int i, float alpha) {
+    const float w = it.a.w + it.b.w;
+    const float dx = it.a.x - it.b.x, dy = it.a.y - it.b.y, dz = it.a.z - it.b.z;
+    const float l = sqrtf(dx * dx + dy * dy + dz * dz);
+    const bool ok = it.live && !(w <= 0.0f) && !(l < PXB_EPSILON);
+    const float nx = dx / l, ny = dy / l, nz = dz / l;
+    const float c = l - it.rest;
+    const float dlambda = (-c - alpha * it.lam) / (w + alpha);
+    const float cx = dlambda * nx, cy = dlambda * ny, cz = dlambda * nz;
+    float4 a = it.a, b = it.b;
+    a.x = a.x + a.w * cx;
+    a.y = a.y + a.w * cy;
+    a.z = a.z + a.w * cz;
+    b.x = b.x - b.w * cx;
+    b.y = b.y - b.w * cy;
+    b.z = b.z - b.w * cz;
+    if (ok) {
+        *it.pa = a;
+        *it.pb = b;
+        if (kLam) lamv[i] = it.lam + dlambda;
+    }
+}
+
+template <int CL, bool kLam, int kItems>
+__device__ __forceinline__ void project_segment(float4* __restrict__ pos, float4* __restrict__ pos_next,
+                                                const float* __restrict__ rest, float* __restrict__ lamv,
+                                                int n_local, int4 h0, int4 h1, float alpha, int tid, int T) {
+    const int count_pad = h0.x, shift = h0.y, per_row = h0.z, a_base = h0.w;
+    const int row_stride = h1.x, d = h1.y;
+    if constexpr (kItems == 2) {
+        for (int i = tid; i < count_pad; i += 2 * T) {
+            PairItem x, y;
+            load_item<CL, kLam>(x, pos, pos_next, rest, lamv, n_local, i, count_pad, shift, per_row, a_base,
+                                row_stride, d);
+            load_item<CL, kLam>(y, pos, pos_next, rest, lamv, n_local, i + T, count_pad, shift, per_row,
+                                a_base, row_stride, d);
+            project_item<kLam>(x, lamv, i, alpha);
+            project_item<kLam>(y, lamv, i + T, alpha);
+        }
+    } else {
+        for (int i = tid; i < count_pad; i += T) {
+            PairItem x;
+            load_item<CL, kLam>(x, pos, pos_next, rest, lamv, n_local, i, count_pad, shift, per_row, a_base,
+                                row_stride, d);
+            project_item<kLam>(x, lamv, i, alpha);
+        }
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
@@ -419,24 +505,11 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     const int se = sC.rank[rank].colour_seg[c + 1];
                     for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
                         const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
-                        const int count_pad = h0.x, shift = h0.y, per_row = h0.z, a_base = h0.w;
-                        const int row_stride = h1.x, d = h1.y, rest_base = h1.z, lam_base = h1.w;
-                        const int mask = (1 << shift) - 1;
-                        for (int i = tid; i < count_pad; i += T) {
-                            const int k0 = i & mask;
-                            if (k0 >= per_row) continue;
-                            const int la = a_base + (i >> shift) * row_stride + k0;
-                            const int lb = la + d;
-                            float4* pb_ptr = (CL == 1 || lb < n_local) ? &pos[lb] : &pos_next[lb - n_local];
-                            float4 pa = pos[la], pb = *pb_ptr;
-                            const float lam = lam_base >= 0 ? U[lam_base + i] : 0.0f;
-                            float dl = 0.0f;
-                            if (solve_pair(pa, pb, rest[rest_base + i], lam, alpha, dl)) {
-                                pos[la] = pa;
-                                *pb_ptr = pb;
-                                if (lam_base >= 0) U[lam_base + i] = lam + dl;
-                            }
-                        }
+                        constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
+                        if (h1.w >= 0)
+                            project_segment<CL, true, kItems>(pos, pos_next, rest + h1.z, U + h1.w, n_local, h0, h1, alpha, tid, T);
+                        else
+                            project_segment<CL, false, kItems>(pos, pos_next, rest + h1.z, U, n_local, h0, h1, alpha, tid, T);
                     }
                     // Colours that join rows need every rank to see the others' writes; a pair
                     // of row-local colours only needs this CTA's. The last colour always syncs

@@ -899,26 +899,50 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     char* db = static_cast<char*>(d_stage.p);
     if (pxb_status s = cuda(cudaMemcpyAsync(db, hb, total, cudaMemcpyHostToDevice, stream), "upload step")) return s;
     cudaEventRecord(staged, stream);
+    // Launch groups: (cluster size, CTAs per SM). With several, each goes to a side stream so
+    // they share the SMs instead of running one after another (a group of small cloths alone
+    // leaves most of the device idle).
+    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; };
+    std::vector<Group> groups;
     for (uint32_t g0 = 0; g0 < n;) {
         const int cluster = static_cast<int>(ents[perm[g0]]->ranks.size());
         const int group_fit = fit[perm[g0]];
-        uint32_t g1 = g0;
-        int threads = 64, smem = 0;
-        while (g1 < n && static_cast<int>(ents[perm[g1]]->ranks.size()) == cluster && fit[perm[g1]] == group_fit) {
-            threads = std::max(threads, ents[perm[g1]]->threads);
-            smem = std::max(smem, ents[perm[g1]]->dev.smem_bytes);
-            ++g1;
+        Group G{g0, g0, cluster, 64, 0, 0.0};
+        while (G.g1 < n && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster && fit[perm[G.g1]] == group_fit) {
+            const ClothEntry& e = *ents[perm[G.g1]];
+            G.threads = std::max(G.threads, e.threads);
+            G.smem = std::max(G.smem, e.dev.smem_bytes);
+            G.work += static_cast<double>(e.n_layout);
+            ++G.g1;
         }
-        cudaError_t le = launch_cloth_step(cloth_variant, cluster, static_cast<const PxbClothDev*>(d_registry.p),
-                                           reinterpret_cast<const PxbClothStep*>(db) + g0,
+        groups.push_back(G);
+        g0 = G.g1;
+    }
+    std::stable_sort(groups.begin(), groups.end(), [](const Group& a, const Group& b) { return a.work > b.work; });
+    const bool fan_out = groups.size() > 1;
+    if (fan_out) {
+        if (pxb_status s = cuda(cudaEventRecord(fork, stream), "fork")) return s;
+        for (int k = 0; k < std::min<int>(kSideStreams, static_cast<int>(groups.size())); ++k)
+            if (pxb_status s = cuda(cudaStreamWaitEvent(side[k], fork, 0), "fork wait")) return s;
+    }
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& G = groups[gi];
+        cudaStream_t st = fan_out ? side[gi % kSideStreams] : stream;
+        cudaError_t le = launch_cloth_step(cloth_variant, G.cluster, static_cast<const PxbClothDev*>(d_registry.p),
+                                           reinterpret_cast<const PxbClothStep*>(db) + G.g0,
                                            reinterpret_cast<const PxbDevCollider*>(db + o_cols),
                                            reinterpret_cast<const pxb_gravity_source*>(db + o_src),
-                                           reinterpret_cast<const int32_t*>(db + o_order) + g0,
-                                           static_cast<PxbFrameResult*>(d_results.p) + g0, d_err,
-                                           static_cast<int>(g1 - g0), threads, smem, stream);
+                                           reinterpret_cast<const int32_t*>(db + o_order) + G.g0,
+                                           static_cast<PxbFrameResult*>(d_results.p) + G.g0, d_err,
+                                           static_cast<int>(G.g1 - G.g0), G.threads, G.smem, st);
         if (le != cudaSuccess) return cuda(le, "launch cloth_step");
         ++launches;
-        g0 = g1;
+    }
+    if (fan_out) {
+        for (int k = 0; k < std::min<int>(kSideStreams, static_cast<int>(groups.size())); ++k) {
+            if (pxb_status s = cuda(cudaEventRecord(join[k], side[k]), "join")) return s;
+            if (pxb_status s = cuda(cudaStreamWaitEvent(stream, join[k], 0), "join wait")) return s;
+        }
     }
     last_step.resize(n);
     for (uint32_t slot = 0; slot < n; ++slot) last_step[slot] = sd->cloths[perm[slot]];
@@ -976,6 +1000,11 @@ pxb_status pxb_context_create(int device, pxb_context** out) {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->staged, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
+    for (int k = 0; k < pxb_context::kSideStreams && e == cudaSuccess; ++k) {
+        e = cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join[k], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_err, 4);
     if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, 4);
     if (e != cudaSuccess) {

@@ -87,6 +87,12 @@ struct pxb_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t staged = nullptr;
+    // Side streams for launch groups that run side by side: forked from `stream` after the
+    // step's upload, joined back before anything else is queued on it.
+    static constexpr int kSideStreams = 8;
+    cudaStream_t side[kSideStreams] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kSideStreams] = {};
     uint32_t* d_err = nullptr;
     std::string error;
     uint64_t launches = 0;
@@ -113,6 +119,11 @@ struct pxb_context {
         if (pinned) cudaFreeHost(pinned);
         if (d_err) cudaFree(d_err);
         if (staged) cudaEventDestroy(staged);
+        if (fork) cudaEventDestroy(fork);
+        for (int k = 0; k < kSideStreams; ++k) {
+            if (join[k]) cudaEventDestroy(join[k]);
+            if (side[k]) cudaStreamDestroy(side[k]);
+        }
         if (stream) cudaStreamDestroy(stream);
     }
 

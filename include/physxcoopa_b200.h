@@ -485,6 +485,39 @@ pxb_status pxb_host_strands_view(pxb_host_strands* set, pxb_strand_set_desc* vie
 void pxb_strand_params_default(pxb_strand_params* out);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Warm-start network. No counterpart in the reference (physxcoopa has no learned component).  */
+/* Per free vertex of a cloth, after integration: 24 features (predicted displacement, velocity,*/
+/* the strain vectors of its 6 grid edges) -> 64 -> SiLU -> 64 -> SiLU -> 3, a displacement      */
+/* added to the predicted position before a few constraint iterations; the solver falls back   */
+/* to the plain iteration count when the residual stays above the cloth's threshold. BF16      */
+/* weights and activations, FP32 accumulation, on the tensor cores.                            */
+/* ------------------------------------------------------------------------------------------ */
+
+#define PXB_MLP_INPUTS 24
+#define PXB_MLP_HIDDEN 64
+#define PXB_MLP_OUTPUTS 3
+
+/* Weights row-major (out x in), as a linear layer stores them. Inputs are normalised as
+ * (x - in_mean) * in_scale; outputs are multiplied by out_scale. */
+typedef struct pxb_mlp_weights {
+    float w1[PXB_MLP_HIDDEN][PXB_MLP_INPUTS];
+    float b1[PXB_MLP_HIDDEN];
+    float w2[PXB_MLP_HIDDEN][PXB_MLP_HIDDEN];
+    float b2[PXB_MLP_HIDDEN];
+    float w3[PXB_MLP_OUTPUTS][PXB_MLP_HIDDEN];
+    float b3[PXB_MLP_OUTPUTS];
+    float in_mean[PXB_MLP_INPUTS];
+    float in_scale[PXB_MLP_INPUTS];
+    float out_scale[PXB_MLP_OUTPUTS];
+} pxb_mlp_weights;
+
+/* Installs / reads the context's network. */
+pxb_status pxb_mlp_set_weights(pxb_context* ctx, const pxb_mlp_weights* weights);
+pxb_status pxb_mlp_get_weights(pxb_context* ctx, pxb_mlp_weights* out);
+/* Runs the installed network on n host feature rows (n x 24 floats) into out (n x 3). */
+pxb_status pxb_mlp_infer(pxb_context* ctx, const float* features, uint32_t n, float* out);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Diagnostics                                                                                  */
 /* ------------------------------------------------------------------------------------------ */
 

@@ -128,6 +128,27 @@ class ClothPlan(C.Structure):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
 
+class MlpWeights(C.Structure):
+    """pxb_mlp_weights: the warm-start network (row-major weights, out x in)."""
+    _fields_ = [("w1", (f32 * 24) * 64), ("b1", f32 * 64), ("w2", (f32 * 64) * 64), ("b2", f32 * 64),
+                ("w3", (f32 * 64) * 3), ("b3", f32 * 3), ("in_mean", f32 * 24), ("in_scale", f32 * 24),
+                ("out_scale", f32 * 3)]
+
+    @classmethod
+    def from_numpy(cls, w1, b1, w2, b2, w3, b3, in_mean=None, in_scale=None, out_scale=None):
+        m = cls()
+        for name, arr in (("w1", w1), ("b1", b1), ("w2", w2), ("b2", b2), ("w3", w3), ("b3", b3),
+                          ("in_mean", np.zeros(24) if in_mean is None else in_mean),
+                          ("in_scale", np.ones(24) if in_scale is None else in_scale),
+                          ("out_scale", np.ones(3) if out_scale is None else out_scale)):
+            dst = np.ctypeslib.as_array(getattr(m, name))
+            dst[...] = np.asarray(arr, np.float32).reshape(dst.shape)
+        return m
+
+    def as_numpy(self):
+        return {name: np.ctypeslib.as_array(getattr(self, name)).copy() for name, _ in self._fields_}
+
+
 class ClothDesc(C.Structure):
     """pxb_cloth_desc: a cloth as plain pointers into caller memory."""
     _fields_ = [("particles", P), ("n_particles", u32), ("stretch", P), ("n_stretch", u32),

@@ -32,6 +32,7 @@
 #define PXB_DEVERR_BAD_INDEX 0x1u
 #define PXB_DEVERR_TMA_TIMEOUT 0x2u
 #define PXB_DEVERR_QUEUE_TIMEOUT 0x4u
+#define PXB_DEVERR_MMA_TIMEOUT 0x8u
 
 // 16-byte aligned: the kernel reads a descriptor as two 16-byte words.
 struct alignas(16) PxbSeg {

@@ -29,6 +29,12 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,
                               int n_cloths, int threads, int smem_bytes, cudaStream_t stream);
 
+// Warm-start network (mlp_kernel.cu).
+int mlp_infer_smem_bytes();
+cudaError_t launch_mlp_infer(const float* X, int n, const unsigned char* blob, float* Y, uint32_t* err,
+                             int n_sms, cudaStream_t stream);
+void mlp_pack_blob(const pxb_mlp_weights& m, unsigned char* out);
+
 cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness,
                                   const float* pts, int n, float* out, float* normals,
                                   float* depths, int32_t* hits, cudaStream_t stream);

@@ -958,7 +958,7 @@ pxb_status pxb_context::check_device_error() {
     if (s) return s;
     if (h) {
         cudaMemsetAsync(d_err, 0, 4, stream);
-        return fail(PXB_ERR_DEVICE_STATUS, "device error word 0x%x (1 bad index, 2 staging wait expired, 4 queue wait expired)", h);
+        return fail(PXB_ERR_DEVICE_STATUS, "device error word 0x%x (1 bad index, 2 staging wait expired, 4 queue wait expired, 8 tensor-core wait expired)", h);
     }
     return PXB_OK;
 }
@@ -1005,6 +1005,7 @@ pxb_status pxb_context_create(int device, pxb_context** out) {
         e = cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join[k], cudaEventDisableTiming);
     }
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->n_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_err, 4);
     if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, 4);
     if (e != cudaSuccess) {

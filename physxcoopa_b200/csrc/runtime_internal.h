@@ -102,6 +102,11 @@ struct pxb_context {
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
     std::vector<uint64_t> last_step;  // ids of the last step, in launch-slot order
+    // warm-start network: host copy of the weights and the packed device blob
+    bool has_mlp = false;
+    pxb_mlp_weights mlp{};
+    DevBuf d_mlp, d_mlp_io;
+    int n_sms = 148;
     bool results_fresh = false;
     std::vector<HostSolveCache> host_cache;
     std::vector<StrandEntry> strand_sets;
@@ -114,7 +119,7 @@ struct pxb_context {
             if (e.alive && e.dmem) cudaFree(e.dmem);
         for (StrandEntry& e : strand_sets)
             if (e.alive && e.dmem) cudaFree(e.dmem);
-        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune})
+        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune, &d_mlp, &d_mlp_io})
             if (b->p) cudaFree(b->p);
         if (pinned) cudaFreeHost(pinned);
         if (d_err) cudaFree(d_err);
@@ -133,6 +138,7 @@ struct pxb_context {
     pxb_status grow_pinned(size_t bytes);
     ClothEntry* lookup(uint64_t id);
     void refresh_layout(ClothEntry& e);
+    pxb_status upload_mlp();
     pxb_status upload_segments(ClothEntry& e);
     pxb_status upload_particles(ClothEntry& e, const pxb_particle* particles);
     pxb_status upload_anchor_records(ClothEntry& e);

@@ -35,6 +35,9 @@ SIGNATURES = {
     "pxb_cloth_params_default": ([C.POINTER(A.ClothParams)], None),
     "pxb_cloth_add": ([P, C.POINTER(A.ClothDesc), C.POINTER(u64)], C.c_int),
     "pxb_cloth_remove": ([P, u64], C.c_int),
+    "pxb_mlp_set_weights": ([P, C.POINTER(A.MlpWeights)], C.c_int),
+    "pxb_mlp_get_weights": ([P, C.POINTER(A.MlpWeights)], C.c_int),
+    "pxb_mlp_infer": ([P, P, u32, P], C.c_int),
     "pxb_cloth_plan_layout": ([C.POINTER(A.ClothDesc), C.POINTER(A.ClothPlan), C.c_char_p, u32], C.c_int),
     "pxb_cloth_set_params": ([P, u64, C.POINTER(A.ClothParams)], C.c_int),
     "pxb_cloth_write_particles": ([P, u64, P, u32], C.c_int),
@@ -271,6 +274,21 @@ class Context:
     @property
     def launch_count(self):
         return int(self.lib.pxb_context_launch_count(self.h))
+
+    # --- warm-start network ---------------------------------------------------------------
+    def set_mlp(self, weights):
+        self._check(self.lib.pxb_mlp_set_weights(self.h, C.byref(weights)), "mlp_set_weights")
+
+    def get_mlp(self):
+        w = A.MlpWeights()
+        self._check(self.lib.pxb_mlp_get_weights(self.h, C.byref(w)), "mlp_get_weights")
+        return w
+
+    def mlp_infer(self, features):
+        x = np.ascontiguousarray(features, np.float32).reshape(-1, 24)
+        out = np.zeros((len(x), 3), np.float32)
+        self._check(self.lib.pxb_mlp_infer(self.h, A.ptr(x), len(x), A.ptr(out)), "mlp_infer")
+        return out
 
     # --- registry ------------------------------------------------------------------------
     def add_cloth(self, c: ClothArrays) -> int:

@@ -486,8 +486,9 @@ void pxb_strand_params_default(pxb_strand_params* out);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Warm-start network. No counterpart in the reference (physxcoopa has no learned component).  */
-/* Per free vertex of a cloth, after integration: 24 features (predicted displacement, velocity,*/
-/* the strain vectors of its 6 grid edges) -> 64 -> SiLU -> 64 -> SiLU -> 3, a displacement      */
+/* Per free vertex of a cloth, after integration: 24 features (predicted displacement, velocity*/
+/* at the substep start, the strain vectors of its 6 triangulation edges) -> 64 -> SiLU -> 64 ->*/
+/* SiLU -> 3, a displacement                                                                  */
 /* added to the predicted position before a few constraint iterations; the solver falls back   */
 /* to the plain iteration count when the residual stays above the cloth's threshold. BF16      */
 /* weights and activations, FP32 accumulation, on the tensor cores.                            */
@@ -516,6 +517,36 @@ pxb_status pxb_mlp_set_weights(pxb_context* ctx, const pxb_mlp_weights* weights)
 pxb_status pxb_mlp_get_weights(pxb_context* ctx, pxb_mlp_weights* out);
 /* Runs the installed network on n host feature rows (n x 24 floats) into out (n x 3). */
 pxb_status pxb_mlp_infer(pxb_context* ctx, const float* features, uint32_t n, float* out);
+
+/* Warm-started step: as pxb_cloths_step, but in every substep each free particle (not pinned,
+ * not anchored) is first moved by the network's displacement, then warm_iterations run; when
+ * the residual -- the max relative strain of the stretch constraints, max |len / rest - 1| -- is
+ * still above the cloth's threshold, the substep restarts from the unmoved prediction with the
+ * plain iteration count. warm_iterations == 0 runs the plain solve and only measures the
+ * residual (no network needed), which is how a caller calibrates thresholds. */
+typedef struct pxb_warm_start_desc {
+    uint32_t warm_iterations;
+    float residual_threshold;  /* used when thresholds is NULL */
+    const float* thresholds;   /* optional, one per cloth of the step */
+} pxb_warm_start_desc;
+
+typedef struct pxb_cloth_warm_result {
+    float residual;      /* max over the step's substeps of the residual it ended with */
+    uint32_t fallbacks;  /* substeps that fell back to the plain iteration count */
+    uint32_t substeps;
+} pxb_cloth_warm_result;
+
+pxb_status pxb_cloths_step_warm(pxb_context* ctx, const pxb_cloth_step_desc* step, const pxb_warm_start_desc* warm);
+/* Results of the last pxb_cloths_step_warm, per listed cloth (synchronizes the stream). */
+pxb_status pxb_cloths_read_warm_results(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
+                                        pxb_cloth_warm_result* out);
+/* Training rows from the plain solver: advances the listed cloths by one plain step and, during
+ * substep `substep`, records for every free particle the network's 24 input features and the
+ * displacement the plain iterations moved it by (3 floats). At most `capacity` rows are written
+ * to features (capacity x 24) and targets (capacity x 3), cloths in list order, particles in
+ * device layout order; *rows_out is the number written. */
+pxb_status pxb_cloths_record(pxb_context* ctx, const pxb_cloth_step_desc* step, uint32_t substep,
+                             float* features, float* targets, uint64_t capacity, uint64_t* rows_out);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Diagnostics                                                                                  */

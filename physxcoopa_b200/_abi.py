@@ -149,6 +149,14 @@ class MlpWeights(C.Structure):
         return {name: np.ctypeslib.as_array(getattr(self, name)).copy() for name, _ in self._fields_}
 
 
+class WarmStartDesc(C.Structure):
+    """pxb_warm_start_desc."""
+    _fields_ = [("warm_iterations", u32), ("residual_threshold", f32), ("thresholds", P)]
+
+
+WARM_RESULT = np.dtype([("residual", "<f4"), ("fallbacks", "<u4"), ("substeps", "<u4")])
+
+
 class ClothDesc(C.Structure):
     """pxb_cloth_desc: a cloth as plain pointers into caller memory."""
     _fields_ = [("particles", P), ("n_particles", u32), ("stretch", P), ("n_stretch", u32),

@@ -28,6 +28,7 @@
 #include "../../include/physxcoopa_b200.h"
 #include "pxb_internal.h"
 #include "pxb_kernels.h"
+#include "pxb_mlp.cuh"
 #include "pxb_device_math.cuh"
 
 namespace cg = cooperative_groups;
@@ -251,14 +252,19 @@ __device__ __forceinline__ void cluster_or_block_sync() {
     else __syncthreads();
 }
 
-template <int kMaxThreads, int CL>
+template <int kMaxThreads, int CL, bool kWarm>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders,
                   const pxb_gravity_source* __restrict__ sources,
                   const int32_t* __restrict__ order, PxbFrameResult* __restrict__ results,
-                  uint32_t* __restrict__ err) {
+                  uint32_t* __restrict__ err, const PxbWarmStep* __restrict__ wsteps,
+                  const unsigned char* __restrict__ mlp_blob, PxbWarmResult* __restrict__ wres) {
     extern __shared__ __align__(16) unsigned char smem[];
+    // warm-start state: per-rank residuals, the network warpgroups' MMA barriers, TMEM base
+    __shared__ float s_resid[PXB_MAX_RANKS];
+    __shared__ __align__(8) uint64_t s_wbar[kWarmGroups];
+    __shared__ uint32_t s_tmem;
     __shared__ __align__(8) uint64_t bar;
     __shared__ __align__(16) PxbSeg s_seg[PXB_MAX_SEGS];
     // Per-cloth scalars live in shared memory and are read at their point of use: held in
@@ -287,6 +293,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
     if (tid == 0) {
         mbar_init(&bar, 1);
+        if constexpr (kWarm)
+            for (int g = 0; g < kWarmGroups; ++g) tc::mbar_init(&s_wbar[g], 1);
         fence_proxy_async();
     }
     __syncthreads();
@@ -382,6 +390,81 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
     cluster_or_block_sync<CL>();
 
+    const int4* seg4 = reinterpret_cast<const int4*>(s_seg);
+    float4* pos_next = nxt_rank.pos;
+    auto iterate = [&](int iters) {
+        const int n_colours = sC.n_colours;
+        const uint32_t cross = sC.cross_mask;
+        for (int it = 0; it < iters; ++it) {
+            for (int c = 0; c < n_colours; ++c) {
+                const float alpha = sP.alpha[c];
+                const int se = sC.rank[rank].colour_seg[c + 1];
+                for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
+                    const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
+                    constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
+                    if (h1.w >= 0)
+                        project_segment<CL, true, kItems>(pos, pos_next, rest + h1.z, U + h1.w, n_local, h0, h1, alpha, tid, T);
+                    else
+                        project_segment<CL, false, kItems>(pos, pos_next, rest + h1.z, U, n_local, h0, h1, alpha, tid, T);
+                }
+                // Colours that join rows need every rank to see the others' writes; a pair
+                // of row-local colours only needs this CTA's. The last colour always syncs
+                // the cluster: the tether stage reads anchors anywhere in the cloth.
+                const int cn = (c + 1 < n_colours) ? c + 1 : 0;
+                const bool last = it + 1 == iters && c + 1 == n_colours;
+                if (CL > 1 && (((cross >> c) | (cross >> cn)) & 1u || last)) cluster_or_block_sync<CL>();
+                else __syncthreads();
+            }
+        }
+    };
+    // Max relative strain of the stretch-list constraints, max |len / rest - 1|, over the whole
+    // cloth (every rank gets the same value).
+    auto stretch_residual = [&]() -> float {
+        float r = 0.0f;
+        const uint32_t smask = sC.stretch_mask;
+        for (int c = 0; c < sC.n_colours; ++c) {
+            if (!((smask >> c) & 1u)) continue;
+            const int se = sC.rank[rank].colour_seg[c + 1];
+            for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
+                const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
+                const int count_pad = h0.x, shift = h0.y, per_row = h0.z, a_base = h0.w;
+                const int row_stride = h1.x, d = h1.y;
+                const float* rr = rest + h1.z;
+                const int mask = (1 << shift) - 1;
+                for (int i = tid; i < count_pad; i += T) {
+                    const int k = i & mask;
+                    if (k >= per_row) continue;
+                    const int la = a_base + (i >> shift) * row_stride + k, lb = la + d;
+                    const float4 pa = pos[la];
+                    const float4 pb = (CL == 1 || lb < n_local) ? pos[lb] : pos_next[lb - n_local];
+                    const float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
+                    const float len = sqrtf(dx * dx + dy * dy + dz * dz);
+                    r = fmaxf(r, fabsf(len / rr[i] - 1.0f));
+                }
+            }
+        }
+        r = warp_max(r);
+        if ((tid & 31) == 0) s_red[tid >> 5][0] = r;
+        __syncthreads();
+        if (tid == 0) {
+            float m = s_red[0][0];
+            for (int w = 1; w < ((T + 31) >> 5); ++w) m = fmaxf(m, s_red[w][0]);
+            for (int q = 0; q < n_ranks; ++q) {
+                float* dst = &s_resid[rank];
+                if constexpr (CL > 1) dst = cg::this_cluster().map_shared_rank(&s_resid[rank], q);
+                *dst = m;
+            }
+        }
+        cluster_or_block_sync<CL>();
+        float m = s_resid[0];
+        for (int q = 1; q < n_ranks; ++q) m = fmaxf(m, s_resid[q]);
+        cluster_or_block_sync<CL>();  // s_red / s_resid free again
+        return m;
+    };
+    uint32_t wphase = 0;   // parity of this thread's network-warpgroup MMA barrier
+    float w_resid = 0.0f;  // max residual over the step's substeps
+    int w_fallbacks = 0;
+
     const int steps = sP.steps;
     float4* __restrict__ gvel = sC.vel;
     float4* __restrict__ gprv = sC.prv;
@@ -453,8 +536,10 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             cluster_or_block_sync<CL>();
         }
 
-        // --- 4a. lambda reset (cloth_solver.h:253-254) ----------------------------------
-        for (int i = tid; i < sC.rank[rank].n_lam; i += T) U[i] = 0.0f;
+        // --- 4a. lambda reset (cloth_solver.h:253-254); the warm-start path resets after
+        // the network, whose tiles borrow the lambda region ----------------------------------
+        if constexpr (!kWarm)
+            for (int i = tid; i < sC.rank[rank].n_lam; i += T) U[i] = 0.0f;
 
         // --- 2 + 3. integrate, then the anchor lerp (cloth_solver.h:230-250) --------------
         {
@@ -494,30 +579,139 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         // alpha == 0 the multiplier never reaches a position (dlambda = (-c - 0*lambda)/w); only
         // the sign of an exactly-zero correction could differ, which moves no coordinate that
         // is not itself +-0.
-        {
-            const int iters = sP.iters, n_colours = sC.n_colours;
-            const int4* seg4 = reinterpret_cast<const int4*>(s_seg);
-            const uint32_t cross = sC.cross_mask;
-            float4* pos_next = nxt_rank.pos;
-            for (int it = 0; it < iters; ++it) {
-                for (int c = 0; c < n_colours; ++c) {
-                    const float alpha = sP.alpha[c];
-                    const int se = sC.rank[rank].colour_seg[c + 1];
-                    for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
-                        const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
-                        constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
-                        if (h1.w >= 0)
-                            project_segment<CL, true, kItems>(pos, pos_next, rest + h1.z, U + h1.w, n_local, h0, h1, alpha, tid, T);
-                        else
-                            project_segment<CL, false, kItems>(pos, pos_next, rest + h1.z, U, n_local, h0, h1, alpha, tid, T);
+        if constexpr (!kWarm) {
+            iterate(sP.iters);
+        } else {
+            // --- warm start: network displacement, a few iterations, residual, fallback ---
+            const PxbWarmStep& W = wsteps[slot];
+            const int warm_iters = W.warm_iters;
+            const bool rec = W.record != 0 && step == W.record_substep;
+            const bool net = warm_iters > 0 && mlp_blob != nullptr;
+            float4* __restrict__ gpos = sC.pos;
+            // the prediction goes to HBM: the fallback restarts from it, targets are measured from it
+            for (int l = tid; l < n_local; l += T) gpos[base + l] = pos[l];
+            if (net || rec) {
+                unsigned char* ub = reinterpret_cast<unsigned char*>(U);
+                uint32_t dyn;
+                asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+                const int u_cap = static_cast<int>(dyn) - (16 * n_local + 4 * sC.rank[rank].n_rest_pad);
+                int n_wg = (u_cap - kWarmTileOff) / kWarmTileBytes;
+                n_wg = n_wg < T / 128 ? n_wg : T / 128;
+                n_wg = n_wg < kWarmGroups ? n_wg : kWarmGroups;
+                if (n_wg < 1) {
+                    if (tid == 0) atomicOr(err, PXB_DEVERR_BAD_INDEX);
+                } else {
+                    if (net) {
+                        for (int i = tid; i < kMlpBlobBytes / 16; i += T)
+                            reinterpret_cast<uint4*>(ub)[i] = reinterpret_cast<const uint4*>(mlp_blob)[i];
+                        if (tid < 32) tc::tmem_alloc(&s_tmem, n_wg > 1 ? 128u : 64u);
                     }
-                    // Colours that join rows need every rank to see the others' writes; a pair
-                    // of row-local colours only needs this CTA's. The last colour always syncs
-                    // the cluster: the tether stage reads anchors anywhere in the cloth.
-                    const int cn = (c + 1 < n_colours) ? c + 1 : 0;
-                    const bool last = it + 1 == iters && c + 1 == n_colours;
-                    if (CL > 1 && (((cross >> c) | (cross >> cn)) & 1u || last)) cluster_or_block_sync<CL>();
-                    else __syncthreads();
+                    tc::fence_before_sync();
+                    __syncthreads();
+                    tc::fence_after_sync();
+                    const int g = tid >> 7;
+                    if (g < n_wg) {
+                        const int wt = tid & 127;
+                        MlpSmem S;
+                        S.w = ub;
+                        S.f = reinterpret_cast<const float*>(ub + kMlpWBytes);
+                        S.a = ub + kWarmTileOff + g * kWarmTileBytes;
+                        S.h = S.a + kMlpTileA;
+                        S.bar = &s_wbar[g];
+                        S.tmem = s_tmem + 64u * static_cast<uint32_t>(g);
+                        const int Q = sC.Q, S_ = sC.S, cols = sC.columns, rows = sC.rows, nl = sC.n_layout;
+                        bool mma_ok = true;
+                        for (int t = g; t * 128 < n_local; t += n_wg) {
+                            const int l = t * 128 + wt;
+                            float x[kMlpIn];
+                            for (int k = 0; k < kMlpIn; ++k) x[k] = 0.0f;
+                            const int gl = base + l;
+                            if (l < n_local) {
+                                const int y = gl / S_;
+                                const int j = gl - y * S_;
+                                const int cls = j / Q;
+                                const int xx = 4 * (j - cls * Q) + cls;
+                                if (xx < cols && y < rows) {
+                                    const float4 p = pos[l];
+                                    const float4 q0 = gprv[gl], v = gvel[gl];
+                                    x[0] = p.x - q0.x; x[1] = p.y - q0.y; x[2] = p.z - q0.z;
+                                    x[3] = v.x; x[4] = v.y; x[5] = v.z;
+                                    const int dxs[6] = {1, -1, 0, 0, 1, -1}, dys[6] = {0, 0, 1, -1, 1, -1};
+#pragma unroll
+                                    for (int e = 0; e < 6; ++e) {
+                                        const int nx = xx + dxs[e], ny = y + dys[e];
+                                        const float r = __ldg(&sC.edge_rest[e * nl + gl]);
+                                        if (nx < 0 || ny < 0 || nx >= cols || ny >= rows || !(r > 0.0f)) continue;
+                                        const int ng = lay(nx, ny, Q, S_);
+                                        const int nloc = ng - base;
+                                        float4 q;
+                                        if (CL == 1 || (nloc >= 0 && nloc < n_local)) q = pos[nloc];
+                                        else if (nloc < 0) q = prv_rank.pos[nloc + prv_rank.n_local];
+                                        else q = nxt_rank.pos[nloc - n_local];
+                                        const float ex = q.x - p.x, ey = q.y - p.y, ez = q.z - p.z;
+                                        const float len = sqrtf(ex * ex + ey * ey + ez * ez);
+                                        if (len > PXB_EPSILON) {
+                                            const float f = 1.0f - r / len;
+                                            x[6 + 3 * e] = ex * f; x[7 + 3 * e] = ey * f; x[8 + 3 * e] = ez * f;
+                                        }
+                                    }
+                                }
+                                if (rec) {
+                                    float* row = W.rec_x + (W.rec_row0 + gl) * kMlpIn;
+                                    for (int k = 0; k < kMlpIn; ++k) row[k] = x[k];
+                                }
+                            }
+                            if (net) {
+                                mlp_put_input(S, wt, x);
+                                float d3[kMlpOut];
+                                if (mma_ok) mma_ok = mlp_tile(S, wt, (tid >> 5) & 3, 1 + g, wphase, d3);
+                                if (l < n_local)
+                                    sC.disp[gl] = make_float4(mma_ok ? d3[0] : 0.0f, mma_ok ? d3[1] : 0.0f,
+                                                              mma_ok ? d3[2] : 0.0f, 0.0f);
+                            }
+                        }
+                        if (!mma_ok && wt == 0) atomicOr(err, PXB_DEVERR_MMA_TIMEOUT);
+                    }
+                    tc::fence_before_sync();
+                    __syncthreads();
+                    tc::fence_after_sync();
+                    if (net && tid < 32) tc::tmem_dealloc(s_tmem, n_wg > 1 ? 128u : 64u);
+                }
+                // every rank's features are read before any rank moves a particle
+                cluster_or_block_sync<CL>();
+                if (net) {
+                    for (int l = tid; l < n_local; l += T) {
+                        const int gl = base + l;
+                        float4 p = pos[l];
+                        if (p.w != 0.0f && __ldg(&sC.anchor_of[gl]) < 0 && gvel[gl].w != 0.0f) {
+                            const float4 d = sC.disp[gl];
+                            p.x = p.x + d.x; p.y = p.y + d.y; p.z = p.z + d.z;
+                            pos[l] = p;
+                        }
+                    }
+                }
+            }
+            for (int i = tid; i < sC.rank[rank].n_lam; i += T) U[i] = 0.0f;
+            cluster_or_block_sync<CL>();
+            iterate(net ? warm_iters : sP.iters);
+            float r = stretch_residual();
+            if (net && r > W.tau) {
+                // fallback: restart from the unmoved prediction with the plain iteration count
+                for (int l = tid; l < n_local; l += T) pos[l] = gpos[base + l];
+                for (int i = tid; i < sC.rank[rank].n_lam; i += T) U[i] = 0.0f;
+                cluster_or_block_sync<CL>();
+                iterate(sP.iters);
+                r = stretch_residual();
+                ++w_fallbacks;
+            }
+            w_resid = fmaxf(w_resid, r);
+            if (rec) {
+                for (int l = tid; l < n_local; l += T) {
+                    const int gl = base + l;
+                    const float4 p = pos[l], q = gpos[gl];
+                    const bool free = p.w != 0.0f && __ldg(&sC.anchor_of[gl]) < 0 && gvel[gl].w != 0.0f;
+                    float* row = W.rec_y + (W.rec_row0 + gl) * 4;
+                    row[0] = p.x - q.x; row[1] = p.y - q.y; row[2] = p.z - q.z; row[3] = free ? 1.0f : 0.0f;
                 }
             }
         }
@@ -659,6 +853,12 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             for (int k = 0; k < 3; ++k) r[k] = fminf(r[k], s_rank_red[q][k]);
             for (int k = 3; k < 7; ++k) r[k] = fmaxf(r[k], s_rank_red[q][k]);
         }
+        if constexpr (kWarm) {
+            PxbWarmResult* wr = &wres[slot];
+            wr->residual = w_resid;
+            wr->fallbacks = w_fallbacks;
+            wr->substeps = sP.steps;
+        }
         PxbFrameResult* out = &results[slot];
         for (int k = 0; k < 3; ++k) { out->bounds_min[k] = r[k]; out->bounds_max[k] = r[k + 3]; }
         out->max_speed = sqrtf(r[6]);
@@ -713,21 +913,22 @@ cudaError_t launch_gather_positions(const PxbClothDev* cloths, const int32_t* or
     return cudaGetLastError();
 }
 
-template <int kMaxThreads, int CL>
+template <int kMaxThreads, int CL, bool kWarm>
 static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
                                   const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                   const int32_t* order, PxbFrameResult* results, uint32_t* err,
-                                  int n_cloths, int threads, int smem_bytes, cudaStream_t stream) {
+                                  int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
+                                  const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres) {
     static uint64_t configured = 0;  // one bit per device the attributes have been set on
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && !(configured >> dev & 1ull)) {
         cudaFuncAttributes fa;
-        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL>);
+        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm>);
         if (e != cudaSuccess) return e;
         if (fa.sharedSizeBytes > static_cast<size_t>(kClothStaticSmem)) return cudaErrorInvalidConfiguration;
-        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL>,
+        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
         if (e != cudaSuccess) return e;
         configured |= 1ull << dev;
@@ -744,8 +945,8 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL>, cloths, steps, colliders,
-                              sources, order, results, err);
+    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm>, cloths, steps, colliders,
+                              sources, order, results, err, wsteps, mlp, wres);
 }
 
 int cloth_variant_threads(int variant) {
@@ -757,24 +958,25 @@ int cloth_variant_registers(int variant) {
     const int v = variant < 0 ? 0 : (variant >= kClothVariants ? kClothVariants - 1 : variant);
     if (!regs[v]) {
         cudaFuncAttributes fa;
-        cudaError_t e = v == 0 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<512, 1>)
-                               : (v == 1 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<768, 1>)
-                                         : cudaFuncGetAttributes(&fa, cloth_step_kernel<1024, 1>));
+        cudaError_t e = v == 0 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<512, 1, false>)
+                               : (v == 1 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<768, 1, false>)
+                                         : cudaFuncGetAttributes(&fa, cloth_step_kernel<1024, 1, false>));
         regs[v] = e == cudaSuccess ? fa.numRegs : 255;
     }
     return regs[v];
 }
 
-template <int kMaxThreads>
+template <int kMaxThreads, bool kWarm>
 static cudaError_t launch_cl(int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
-                             int n_cloths, int threads, int smem_bytes, cudaStream_t stream) {
+                             int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
+                             const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres) {
     switch (cluster) {
-        case 1: return launch_variant<kMaxThreads, 1>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
-        case 2: return launch_variant<kMaxThreads, 2>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
-        case 4: return launch_variant<kMaxThreads, 4>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
-        case 8: return launch_variant<kMaxThreads, 8>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
+        case 1: return launch_variant<kMaxThreads, 1, kWarm>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 2: return launch_variant<kMaxThreads, 2, kWarm>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 4: return launch_variant<kMaxThreads, 4, kWarm>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 8: return launch_variant<kMaxThreads, 8, kWarm>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -783,13 +985,25 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
                               const PxbClothStep* steps, const PxbDevCollider* colliders,
                               const pxb_gravity_source* sources, const int32_t* order,
                               PxbFrameResult* results, uint32_t* err, int n_cloths, int threads,
-                              int smem_bytes, cudaStream_t stream) {
+                              int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
+                              const unsigned char* mlp, PxbWarmResult* wres) {
     if (n_cloths <= 0) return cudaSuccess;
+    if (wsteps) {
+        // warm-start kernels: the 512-thread variant (registers for the network epilogue) or
+        // the 1024-thread one
+        if (variant == 0) {
+            if (threads > 512) threads = 512;
+            return launch_cl<512, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        }
+        if (threads > 1024) threads = 1024;
+        if (threads < 128) threads = 128;
+        return launch_cl<1024, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+    }
     if (threads > cloth_variant_threads(variant)) threads = cloth_variant_threads(variant);
     switch (variant) {
-        case 0: return launch_cl<512>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
-        case 1: return launch_cl<768>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
-        default: return launch_cl<1024>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream);
+        case 0: return launch_cl<512, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        case 1: return launch_cl<768, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        default: return launch_cl<1024, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
     }
 }
 

@@ -83,6 +83,29 @@ struct PxbClothDev {
     int32_t smem_bytes;         // max over ranks
     int32_t threads;            // block size this cloth runs with
     int32_t aero_grid;          // triangles are exactly make_grid_cloth's (cloth_builder.h:200-207)
+    uint32_t stretch_mask;      // bit c: colour c comes from the stretch list
+    int32_t pad0;
+    const float* edge_rest;     // [6][n_layout] rest length to the grid neighbour (+x, -x, +y,
+                                // -y, +x+y, -x-y), 0 where no stretch constraint joins them
+    float4* disp;               // [n_layout] warm-start displacement scratch
+};
+
+// Warm-start controls of one cloth for one step (pxb_cloths_step_warm / pxb_cloths_record).
+struct PxbWarmStep {
+    float tau;              // fall back when the residual after warm_iters exceeds this
+    int32_t warm_iters;     // iterations after the network's displacement; 0 = plain solve
+    int32_t record;         // record training rows during substep record_substep
+    int32_t record_substep;
+    float* rec_x;           // [rows][24] features of every layout slot
+    float* rec_y;           // [rows][4] displacement made by the plain iterations, free flag
+    int64_t rec_row0;       // this cloth's first row
+};
+
+struct PxbWarmResult {
+    float residual;         // max over the step's substeps of the final residual
+    int32_t fallbacks;      // substeps that fell back to the plain iteration count
+    int32_t substeps;
+    int32_t pad;
 };
 
 // One anchor target pair as the device keeps it (ClothAnchor::prev_world_position /

@@ -13,7 +13,7 @@ namespace pxb {
 // Static shared memory the cloth kernel may declare (checked against the compiled kernel before
 // its first launch on a device) and the dynamic shared memory left to a cloth CTA under the
 // sm_100 per-block limit of 227 KB.
-constexpr int kClothStaticSmem = 4352;
+constexpr int kClothStaticSmem = 4608;
 constexpr int kMaxDynamicSmem = 232448 - kClothStaticSmem;
 constexpr int kClothOwned = 4;      // particles per thread in the cloth kernel
 constexpr int kClothMaxThreads = 1024;
@@ -24,10 +24,21 @@ constexpr int kClothVariants = 3;
 int cloth_variant_threads(int variant);
 // Registers per thread of a variant's one-CTA kernel (read from the compiled kernel once).
 int cloth_variant_registers(int variant);
+// wsteps non-null selects the warm-start kernel (mlp may then be null: plain solve with the
+// residual measured, or recording only).
 cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,
-                              int n_cloths, int threads, int smem_bytes, cudaStream_t stream);
+                              int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
+                              const PxbWarmStep* wsteps = nullptr, const unsigned char* mlp = nullptr,
+                              PxbWarmResult* wres = nullptr);
+
+// Warm-start kernel: network warpgroups per CTA and the shared memory they borrow from the
+// lambda region (weights blob, then per warpgroup an input and an activation tile).
+constexpr int kWarmGroups = 2;
+constexpr int kWarmTileOff = 15232;      // kMlpBlobBytes rounded up to 128
+constexpr int kWarmTileBytes = 24576;    // kMlpTileA + kMlpTileH
+constexpr int kWarmUMin = kWarmTileOff + kWarmTileBytes;
 
 // Warm-start network (mlp_kernel.cu).
 int mlp_infer_smem_bytes();

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <unordered_map>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -407,7 +408,7 @@ bool verify_ranks(const ClothEntry& e, const pxb_cloth_desc* d) {
 // Re-derives everything that depends on params: lambda slots, union regions, shared memory.
 static void layout_ranks(ClothEntry& e) {
     const bool aero = (e.params.air_drag > 0.0f || e.params.air_lift > 0.0f) && e.n_triangle_indices > 0;
-    int lam_total = 0, smem_max = 0;
+    int lam_total = 0, smem_max = 0, warm_max = 0;
     for (size_t r = 0; r < e.ranks.size(); ++r) {
         ClothEntry::Rank& rk = e.ranks[r];
         int lam = 0;
@@ -425,6 +426,7 @@ static void layout_ranks(ClothEntry& e) {
         const int u_floats = std::max(lam, (aero && e.aero_grid) ? 3 * n_local : 0);
         rk.smem = 16 * n_local + 4 * rk.n_rest_pad + 4 * ((u_floats + 3) & ~3);
         smem_max = std::max(smem_max, rk.smem);
+        warm_max = std::max(warm_max, 16 * n_local + 4 * rk.n_rest_pad + std::max(4 * ((u_floats + 3) & ~3), kWarmUMin));
         PxbRank& dr = e.dev.rank[r];
         dr.row0 = rk.row0;
         dr.n_rows = rk.n_rows;
@@ -438,6 +440,7 @@ static void layout_ranks(ClothEntry& e) {
     }
     e.n_lam = lam_total;
     e.dev.smem_bytes = smem_max;
+    e.warm_smem = warm_max;
 }
 
 void pxb_context::refresh_layout(ClothEntry& e) {
@@ -647,6 +650,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     const size_t o_anc = take(4 * L), o_teth = take(8 * L);
     const size_t o_recs = take(sizeof(PxbAnchorRec) * e.anchor_recs.size());
     const size_t o_segs = take(sizeof(PxbSeg) * e.segs.size());
+    const size_t o_edge = take(4 * 6 * L), o_disp = take(16 * L);
     cudaError_t ce = cudaMalloc(&e.dmem, off);
     if (ce != cudaSuccess) return cuda(ce, "cudaMalloc(cloth)");
     e.dbytes = off;
@@ -677,6 +681,32 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.n_anchors = static_cast<int32_t>(e.anchor_recs.size());
     e.dev.threads = e.threads;
     e.dev.aero_grid = e.aero_grid;
+    for (int c = 0; c < e.n_colours; ++c)
+        if (!e.colour_is_bend[c]) e.dev.stretch_mask |= 1u << c;
+    e.dev.edge_rest = reinterpret_cast<const float*>(base + o_edge);
+    e.dev.disp = reinterpret_cast<float4*>(base + o_disp);
+    // rest length from each slot to its six triangulation neighbours (+x, -x, +y, -y, +x+y,
+    // -x-y), from the stretch list; 0 where no stretch constraint joins the pair
+    std::vector<float> edge_rest(6 * L, 0.0f);
+    {
+        std::unordered_map<uint64_t, float> by_pair;
+        by_pair.reserve(2 * d->n_stretch);
+        auto key = [](uint32_t a, uint32_t b) {
+            return a < b ? (static_cast<uint64_t>(a) << 32 | b) : (static_cast<uint64_t>(b) << 32 | a);
+        };
+        for (uint32_t k = 0; k < d->n_stretch; ++k) by_pair[key(d->stretch[k].a, d->stretch[k].b)] = d->stretch[k].rest_length;
+        const int dxs[6] = {1, -1, 0, 0, 1, -1}, dys[6] = {0, 0, 1, -1, 1, -1};
+        for (int y = 0; y < e.rows; ++y)
+            for (int x = 0; x < e.cols; ++x) {
+                const int l = slot_of_particle(y * e.cols + x, e.cols, e.Q, e.S);
+                for (int k = 0; k < 6; ++k) {
+                    const int nx = x + dxs[k], ny = y + dys[k];
+                    if (nx < 0 || ny < 0 || nx >= e.cols || ny >= e.rows) continue;
+                    auto it = by_pair.find(key(static_cast<uint32_t>(y * e.cols + x), static_cast<uint32_t>(ny * e.cols + nx)));
+                    if (it != by_pair.end()) edge_rest[static_cast<size_t>(k) * L + l] = it->second;
+                }
+            }
+    }
     pxb_status st = PXB_OK;
     auto up = [&](void* dst, const void* src, size_t bytes, const char* what) {
         if (st || bytes == 0) return;
@@ -685,6 +715,8 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     up(base + o_rest, rest_h.data(), 4 * rest_h.size(), "upload rest");
     up(base + o_anc, anchor_of.data(), 4 * L, "upload anchor_of");
     up(base + o_teth, tether.data(), 8 * L, "upload tethers");
+    up(base + o_edge, edge_rest.data(), 4 * 6 * L, "upload edge rest lengths");
+    if (!st) st = cuda(cudaMemsetAsync(base + o_disp, 0, 16 * L, stream), "zero displacement scratch");
     if (!st) st = upload_segments(e);
     if (!st) st = cuda(cudaMemsetAsync(base + o_lam, 0, 4 * static_cast<size_t>(e.n_rest_total), stream), "zero lambdas");
     if (!st) st = upload_anchor_records(e);
@@ -785,7 +817,7 @@ static pxb_status check_colliders(pxb_context* ctx, const pxb_collider* c, uint3
     return PXB_OK;
 }
 
-pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
+pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg* warm) {
     if (!sd || (sd->n_cloths && !sd->cloths)) return fail(PXB_ERR_INVALID_ARGUMENT, "null step");
     const uint32_t n = sd->n_cloths;
     if (n == 0) return PXB_OK;
@@ -811,13 +843,24 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     if (pxb_status s = check_colliders(this, sd->colliders, n_col)) return s;
     if (pxb_status s = sync_registry()) return s;
 
-    // --- staging layout: steps | colliders | sources | order ---
+    if (warm) {
+        for (uint32_t k = 0; k < n; ++k)
+            if (ents[k]->warm_smem > kMaxDynamicSmem)
+                return fail(PXB_ERR_TOO_LARGE, "cloth %llu: the warm-start kernel needs %d bytes of shared memory",
+                            (unsigned long long)sd->cloths[k], ents[k]->warm_smem);
+        if (warm->warm_iters > 0 && !has_mlp) return fail(PXB_ERR_INVALID_ARGUMENT, "no network installed");
+        if (pxb_status s = grow(d_wresults, sizeof(PxbWarmResult) * n, "warm results")) return s;
+    }
+
+    // --- staging layout: steps | colliders | sources | order | warm controls ---
     const size_t b_steps = sizeof(PxbClothStep) * n;
     const size_t b_cols = sizeof(PxbDevCollider) * std::max<uint32_t>(n_col, 1);
     const size_t b_src = sizeof(pxb_gravity_source) * std::max<uint32_t>(n_src, 1);
     const size_t b_order = sizeof(int32_t) * n;
+    const size_t b_warm = warm ? sizeof(PxbWarmStep) * n : 0;
     const size_t o_cols = align256(b_steps), o_src = o_cols + align256(b_cols),
-                 o_order = o_src + align256(b_src), total = o_order + align256(b_order);
+                 o_order = o_src + align256(b_src), o_warm = o_order + align256(b_order),
+                 total = o_warm + align256(b_warm);
     if (pxb_status s = grow_pinned(total)) return s;
     if (pxb_status s = grow(d_stage, total, "step staging")) return s;
     if (pxb_status s = grow(d_results, sizeof(PxbFrameResult) * n, "results")) return s;
@@ -827,6 +870,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     auto* hs_cols = reinterpret_cast<PxbDevCollider*>(hb + o_cols);
     auto* hs_src = reinterpret_cast<pxb_gravity_source*>(hb + o_src);
     auto* hs_order = reinterpret_cast<int32_t*>(hb + o_order);
+    auto* hs_warm = reinterpret_cast<PxbWarmStep*>(hb + o_warm);
     for (uint32_t k = 0; k < n_col; ++k) pxb_make_dev_collider(sd->colliders[k], hs_cols[k]);
     if (n_src) std::memcpy(hs_src, sd->sources, sizeof(pxb_gravity_source) * n_src);
     // Launch slots grouped by cluster size and by how many of the cloth's CTAs one SM holds
@@ -836,7 +880,12 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     const int cap = cloth_variant_threads(cloth_variant);
     const int regs = cloth_variant_registers(cloth_variant);
     std::vector<int> fit(n);
-    for (uint32_t k = 0; k < n; ++k) fit[k] = ctas_per_sm(ents[k]->dev.smem_bytes, std::min(ents[k]->threads, cap), regs);
+    auto launch_smem = [&](const ClothEntry& e) { return warm ? e.warm_smem : e.dev.smem_bytes; };
+    auto launch_threads = [&](const ClothEntry& e) {
+        // the warm-start kernel runs whole warpgroups (the network's tiles are 128 rows)
+        return warm ? std::min(cap, std::max(128, (e.threads + 127) & ~127)) : std::min(e.threads, cap);
+    };
+    for (uint32_t k = 0; k < n; ++k) fit[k] = ctas_per_sm(launch_smem(*ents[k]), launch_threads(*ents[k]), regs);
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
@@ -890,6 +939,17 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
         s.src_count = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k + 1] - sd->source_offsets[k]) : 0;
         s.write_lambdas = 1;
         hs_order[slot] = static_cast<int32_t>(ents[k] - cloths.data());
+        if (warm) {
+            PxbWarmStep& w = hs_warm[slot];
+            std::memset(&w, 0, sizeof(w));
+            w.tau = warm->taus ? warm->taus[k] : warm->tau;
+            w.warm_iters = warm->warm_iters;
+            w.record = warm->record;
+            w.record_substep = warm->record_substep;
+            w.rec_x = warm->rec_x;
+            w.rec_y = warm->rec_y;
+            w.rec_row0 = warm->rec_row0 ? warm->rec_row0[k] : 0;
+        }
         // Cloth::time advances by hs per substep (cloth_solver.h:453), mirrored on the host.
         for (uint32_t q = 0; q < steps; ++q) e.time += hs;
         // Anchors reach their targets: next step lerps from here (cloth_solver.h:457).
@@ -910,8 +970,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
         Group G{g0, g0, cluster, 64, 0, 0.0};
         while (G.g1 < n && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster && fit[perm[G.g1]] == group_fit) {
             const ClothEntry& e = *ents[perm[G.g1]];
-            G.threads = std::max(G.threads, e.threads);
-            G.smem = std::max(G.smem, e.dev.smem_bytes);
+            G.threads = std::max(G.threads, launch_threads(e));
+            G.smem = std::max(G.smem, launch_smem(e));
             G.work += static_cast<double>(e.n_layout);
             ++G.g1;
         }
@@ -934,7 +994,10 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
                                            reinterpret_cast<const pxb_gravity_source*>(db + o_src),
                                            reinterpret_cast<const int32_t*>(db + o_order) + G.g0,
                                            static_cast<PxbFrameResult*>(d_results.p) + G.g0, d_err,
-                                           static_cast<int>(G.g1 - G.g0), G.threads, G.smem, st);
+                                           static_cast<int>(G.g1 - G.g0), G.threads, G.smem, st,
+                                           warm ? reinterpret_cast<const PxbWarmStep*>(db + o_warm) + G.g0 : nullptr,
+                                           warm && warm->warm_iters > 0 ? static_cast<const unsigned char*>(d_mlp.p) : nullptr,
+                                           warm ? static_cast<PxbWarmResult*>(d_wresults.p) + G.g0 : nullptr);
         if (le != cudaSuccess) return cuda(le, "launch cloth_step");
         ++launches;
     }
@@ -946,6 +1009,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd) {
     }
     last_step.resize(n);
     for (uint32_t slot = 0; slot < n; ++slot) last_step[slot] = sd->cloths[perm[slot]];
+    last_step_warm = warm != nullptr;
+    warm_fresh = false;
     results_fresh = false;
     return PXB_OK;
 }
@@ -960,6 +1025,27 @@ pxb_status pxb_context::check_device_error() {
         cudaMemsetAsync(d_err, 0, 4, stream);
         return fail(PXB_ERR_DEVICE_STATUS, "device error word 0x%x (1 bad index, 2 staging wait expired, 4 queue wait expired, 8 tensor-core wait expired)", h);
     }
+    return PXB_OK;
+}
+
+pxb_status pxb_context::fetch_warm_results() {
+    if (warm_fresh) return PXB_OK;
+    if (!last_step_warm) return PXB_OK;
+    const size_t n = last_step.size();
+    std::vector<PxbWarmResult> h(n);
+    if (n) {
+        pxb_status s = cuda(cudaMemcpyAsync(h.data(), d_wresults.p, sizeof(PxbWarmResult) * n,
+                                            cudaMemcpyDeviceToHost, stream), "read warm results");
+        if (s) return s;
+    }
+    if (pxb_status s = check_device_error()) return s;
+    for (size_t k = 0; k < n; ++k) {
+        ClothEntry* e = lookup(last_step[k]);
+        if (!e) continue;
+        e->warm_result = h[k];
+        e->has_warm_result = true;
+    }
+    warm_fresh = true;
     return PXB_OK;
 }
 

@@ -43,6 +43,7 @@ struct ClothEntry {
     int n_rest_total = 0;
     int n_lam = 0;                         // lambda slots over all ranks
     int threads = 64;
+    int warm_smem = 0;  // dynamic shared memory of the warm-start kernel (max over ranks)
     int aero_grid = 0;
     uint32_t n_triangle_indices = 0;
     uint32_t n_stretch = 0, n_bend = 0, n_stretch_batches = 0, n_bend_batches = 0;
@@ -58,6 +59,8 @@ struct ClothEntry {
     size_t dbytes = 0;
     PxbFrameResult result{};
     bool has_result = false;
+    PxbWarmResult warm_result{};
+    bool has_warm_result = false;
 };
 
 // One registered strand set (hair::StrandSet mirrors + device buffers).
@@ -119,7 +122,7 @@ struct pxb_context {
             if (e.alive && e.dmem) cudaFree(e.dmem);
         for (StrandEntry& e : strand_sets)
             if (e.alive && e.dmem) cudaFree(e.dmem);
-        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune, &d_mlp, &d_mlp_io})
+        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune, &d_mlp, &d_mlp_io, &d_wresults, &d_rec})
             if (b->p) cudaFree(b->p);
         if (pinned) cudaFreeHost(pinned);
         if (d_err) cudaFree(d_err);
@@ -144,7 +147,21 @@ struct pxb_context {
     pxb_status upload_anchor_records(ClothEntry& e);
     pxb_status add_cloth(const pxb_cloth_desc* d, uint64_t* id_out);
     pxb_status sync_registry();
-    pxb_status step_cloths(const pxb_cloth_step_desc* sd);
+    // Warm-start / recording controls of a step (null: the plain kernel).
+    struct WarmCfg {
+        int warm_iters = 0;
+        float tau = 0.0f;
+        const float* taus = nullptr;      // per cloth, overrides tau
+        int record = 0, record_substep = 0;
+        float* rec_x = nullptr;           // device rows, cloth k from rec_row0[k]
+        float* rec_y = nullptr;
+        const int64_t* rec_row0 = nullptr;
+    };
+    pxb_status step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg* warm = nullptr);
+    DevBuf d_wresults, d_rec;
+    bool warm_fresh = false;
+    bool last_step_warm = false;
+    pxb_status fetch_warm_results();
     pxb_status check_device_error();
     pxb_status fetch_results();
     StrandEntry* lookup_strands(uint64_t id);

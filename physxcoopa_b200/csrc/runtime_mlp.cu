@@ -72,4 +72,70 @@ pxb_status pxb_mlp_infer(pxb_context* ctx, const float* features, uint32_t n, fl
     return ctx->check_device_error();
 }
 
+pxb_status pxb_cloths_step_warm(pxb_context* ctx, const pxb_cloth_step_desc* step, const pxb_warm_start_desc* warm) {
+    if (!ctx || !step || !warm) return PXB_ERR_INVALID_ARGUMENT;
+    pxb_context::WarmCfg cfg;
+    cfg.warm_iters = static_cast<int>(warm->warm_iterations);
+    cfg.tau = warm->residual_threshold;
+    cfg.taus = warm->thresholds;
+    return ctx->step_cloths(step, &cfg);
+}
+
+pxb_status pxb_cloths_read_warm_results(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
+                                        pxb_cloth_warm_result* out) {
+    if (!ctx || (n && (!cloths || !out))) return PXB_ERR_INVALID_ARGUMENT;
+    if (pxb_status s = ctx->fetch_warm_results()) return s;
+    for (uint32_t k = 0; k < n; ++k) {
+        ClothEntry* e = ctx->lookup(cloths[k]);
+        if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+        if (!e->has_warm_result) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "cloth has no warm-start step");
+        out[k].residual = e->warm_result.residual;
+        out[k].fallbacks = static_cast<uint32_t>(e->warm_result.fallbacks);
+        out[k].substeps = static_cast<uint32_t>(e->warm_result.substeps);
+    }
+    return PXB_OK;
+}
+
+pxb_status pxb_cloths_record(pxb_context* ctx, const pxb_cloth_step_desc* step, uint32_t substep,
+                             float* features, float* targets, uint64_t capacity, uint64_t* rows_out) {
+    if (!ctx || !step || !rows_out || (capacity && (!features || !targets))) return PXB_ERR_INVALID_ARGUMENT;
+    *rows_out = 0;
+    if (step->n_cloths && !step->cloths) return PXB_ERR_INVALID_ARGUMENT;
+    std::vector<int64_t> row0(step->n_cloths);
+    int64_t rows = 0;
+    for (uint32_t k = 0; k < step->n_cloths; ++k) {
+        ClothEntry* e = ctx->lookup(step->cloths[k]);
+        if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+        row0[k] = rows;
+        rows += e->n_layout;
+    }
+    const size_t bytes = sizeof(float) * static_cast<size_t>(rows) * (kMlpIn + 4);
+    if (pxb_status s = ctx->grow(ctx->d_rec, std::max<size_t>(bytes, 16), "recording buffer")) return s;
+    pxb_context::WarmCfg cfg;
+    cfg.record = 1;
+    cfg.record_substep = static_cast<int>(substep);
+    cfg.rec_x = static_cast<float*>(ctx->d_rec.p);
+    cfg.rec_y = cfg.rec_x + static_cast<size_t>(rows) * kMlpIn;
+    cfg.rec_row0 = row0.data();
+    if (pxb_status s = ctx->step_cloths(step, &cfg)) return s;
+    std::vector<float> h(static_cast<size_t>(rows) * (kMlpIn + 4));
+    if (rows) {
+        if (pxb_status s = ctx->cuda(cudaMemcpyAsync(h.data(), ctx->d_rec.p, bytes, cudaMemcpyDeviceToHost, ctx->stream),
+                                     "read recording"))
+            return s;
+    }
+    if (pxb_status s = ctx->check_device_error()) return s;
+    const float* hx = h.data();
+    const float* hy = hx + static_cast<size_t>(rows) * kMlpIn;
+    uint64_t w = 0;
+    for (int64_t r = 0; r < rows && w < capacity; ++r) {
+        if (hy[4 * r + 3] == 0.0f) continue;  // pinned, anchored or ghost slot
+        std::memcpy(features + w * kMlpIn, hx + r * kMlpIn, sizeof(float) * kMlpIn);
+        std::memcpy(targets + w * 3, hy + 4 * r, sizeof(float) * 3);
+        ++w;
+    }
+    *rows_out = w;
+    return PXB_OK;
+}
+
 }  // extern "C"

@@ -38,6 +38,9 @@ SIGNATURES = {
     "pxb_mlp_set_weights": ([P, C.POINTER(A.MlpWeights)], C.c_int),
     "pxb_mlp_get_weights": ([P, C.POINTER(A.MlpWeights)], C.c_int),
     "pxb_mlp_infer": ([P, P, u32, P], C.c_int),
+    "pxb_cloths_step_warm": ([P, C.POINTER(A.ClothStepDesc), C.POINTER(A.WarmStartDesc)], C.c_int),
+    "pxb_cloths_read_warm_results": ([P, P, u32, P], C.c_int),
+    "pxb_cloths_record": ([P, C.POINTER(A.ClothStepDesc), u32, P, P, u64, C.POINTER(u64)], C.c_int),
     "pxb_cloth_plan_layout": ([C.POINTER(A.ClothDesc), C.POINTER(A.ClothPlan), C.c_char_p, u32], C.c_int),
     "pxb_cloth_set_params": ([P, u64, C.POINTER(A.ClothParams)], C.c_int),
     "pxb_cloth_write_particles": ([P, u64, P, u32], C.c_int),
@@ -240,6 +243,7 @@ class Context:
         if st:
             raise PxbError(st, "pxb_context_create failed (is a CUDA device visible?)")
         self._keep = []
+        self._slots = {}
 
     def close(self):
         if self.h:
@@ -290,11 +294,52 @@ class Context:
         self._check(self.lib.pxb_mlp_infer(self.h, A.ptr(x), len(x), A.ptr(out)), "mlp_infer")
         return out
 
+    def step_warm(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
+                  iterations=10, h=1.0 / 60.0, warm_iterations=4, threshold=1e-4, thresholds=None):
+        """One warm-started step (pxb_cloths_step_warm); warm_iterations=0 is the plain solve
+        with its residual measured."""
+        d, keep = self.make_step(ids, colliders, gravity, sources, substeps, iterations, h)
+        return self.step_warm_desc(d, warm_iterations, threshold, thresholds, keep)
+
+    def step_warm_desc(self, d, warm_iterations=4, threshold=1e-4, thresholds=None, keep=None):
+        w = A.WarmStartDesc()
+        w.warm_iterations = warm_iterations
+        w.residual_threshold = threshold
+        th = None if thresholds is None else np.ascontiguousarray(thresholds, np.float32)
+        w.thresholds = A.ptr(th)
+        self._check(self.lib.pxb_cloths_step_warm(self.h, C.byref(d), C.byref(w)), "cloths_step_warm")
+        del keep
+
+    def read_warm_results(self, ids):
+        ids = np.ascontiguousarray(ids, np.uint64)
+        out = np.zeros(len(ids), A.WARM_RESULT)
+        self._check(self.lib.pxb_cloths_read_warm_results(self.h, A.ptr(ids), len(ids), A.ptr(out)),
+                    "read_warm_results")
+        return out
+
+    def record(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
+               iterations=10, h=1.0 / 60.0, substep=0, capacity=None):
+        """Training rows from one plain step (pxb_cloths_record): (features n x 24, targets n x 3)."""
+        if capacity is None:
+            capacity = sum(self._layout_slots(i) for i in ids)
+        d, keep = self.make_step(ids, colliders, gravity, sources, substeps, iterations, h)
+        x = np.zeros((max(capacity, 1), 24), np.float32)
+        y = np.zeros((max(capacity, 1), 3), np.float32)
+        n = u64()
+        self._check(self.lib.pxb_cloths_record(self.h, C.byref(d), substep, A.ptr(x), A.ptr(y), capacity,
+                                               C.byref(n)), "cloths_record")
+        del keep
+        return x[:n.value], y[:n.value]
+
+    def _layout_slots(self, cid):
+        return self._slots.get(cid, 0)
+
     # --- registry ------------------------------------------------------------------------
     def add_cloth(self, c: ClothArrays) -> int:
         d = c.desc()
         out = u64()
         self._check(self.lib.pxb_cloth_add(self.h, C.byref(d), C.byref(out)), "add_cloth")
+        self._slots[out.value] = c.rows * 4 * ((c.columns + 3) // 4)
         return out.value
 
     def remove_cloth(self, cid):

@@ -518,6 +518,26 @@ pxb_status pxb_mlp_get_weights(pxb_context* ctx, pxb_mlp_weights* out);
 /* Runs the installed network on n host feature rows (n x 24 floats) into out (n x 3). */
 pxb_status pxb_mlp_infer(pxb_context* ctx, const float* features, uint32_t n, float* out);
 
+/* Training: fits the network to n rows (host memory: features n x 24, targets n x 3, e.g. from
+ * pxb_cloths_record) by mean squared error in normalised units with Adam (FP32, cosine
+ * learning-rate schedule over the epochs), seeded initialisation and shuffling. The
+ * normalisation comes from the data (feature mean and inverse standard deviation, target root
+ * mean square). Installs the result; *final_loss (optional) receives the last epoch's mean
+ * loss. */
+typedef struct pxb_mlp_train_desc {
+    uint32_t epochs;
+    uint32_t batch;          /* rows per optimiser step */
+    float learning_rate;     /* peak Adam step size */
+    uint64_t seed;
+} pxb_mlp_train_desc;
+pxb_status pxb_mlp_train(pxb_context* ctx, const float* features, const float* targets, uint64_t n,
+                         const pxb_mlp_train_desc* desc, float* final_loss);
+/* Loss and gradients of the installed network over n rows, as one training batch computes them
+ * (FP32): loss = mean over rows and outputs of (y - target / out_scale)^2. Gradients fill the
+ * weight and bias fields of *grads. */
+pxb_status pxb_mlp_loss_gradients(pxb_context* ctx, const float* features, const float* targets, uint64_t n,
+                                  float* loss, pxb_mlp_weights* grads);
+
 /* Warm-started step: as pxb_cloths_step, but in every substep each free particle (not pinned,
  * not anchored) is first moved by the network's displacement, then warm_iterations run; when
  * the residual -- the max relative strain of the stretch constraints, max |len / rest - 1| -- is

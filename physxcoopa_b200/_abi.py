@@ -149,6 +149,11 @@ class MlpWeights(C.Structure):
         return {name: np.ctypeslib.as_array(getattr(self, name)).copy() for name, _ in self._fields_}
 
 
+class MlpTrainDesc(C.Structure):
+    """pxb_mlp_train_desc."""
+    _fields_ = [("epochs", u32), ("batch", u32), ("learning_rate", f32), ("seed", C.c_uint64)]
+
+
 class WarmStartDesc(C.Structure):
     """pxb_warm_start_desc."""
     _fields_ = [("warm_iterations", u32), ("residual_threshold", f32), ("thresholds", P)]

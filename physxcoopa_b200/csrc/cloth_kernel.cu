@@ -462,6 +462,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         return m;
     };
     uint32_t wphase = 0;   // parity of this thread's network-warpgroup MMA barrier
+    uint32_t stage_phase = 0;  // parity of the staging barrier's last completed phase
     float w_resid = 0.0f;  // max residual over the step's substeps
     int w_fallbacks = 0;
 
@@ -591,10 +592,13 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             // the prediction goes to HBM: the fallback restarts from it, targets are measured from it
             for (int l = tid; l < n_local; l += T) gpos[base + l] = pos[l];
             if (net || rec) {
-                unsigned char* ub = reinterpret_cast<unsigned char*>(U);
+                // With the network, its scratch is the rest lengths plus the lambda region (the
+                // rest lengths are staged again below); recording alone uses the lambda region.
                 uint32_t dyn;
                 asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-                const int u_cap = static_cast<int>(dyn) - (16 * n_local + 4 * sC.rank[rank].n_rest_pad);
+                unsigned char* ub = net ? reinterpret_cast<unsigned char*>(rest) : reinterpret_cast<unsigned char*>(U);
+                const int u_cap = net ? static_cast<int>(dyn) - 16 * n_local
+                                      : static_cast<int>(dyn) - (16 * n_local + 4 * sC.rank[rank].n_rest_pad);
                 int n_wg = (u_cap - kWarmTileOff) / kWarmTileBytes;
                 n_wg = n_wg < T / 128 ? n_wg : T / 128;
                 n_wg = n_wg < kWarmGroups ? n_wg : kWarmGroups;
@@ -604,7 +608,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     if (net) {
                         for (int i = tid; i < kMlpBlobBytes / 16; i += T)
                             reinterpret_cast<uint4*>(ub)[i] = reinterpret_cast<const uint4*>(mlp_blob)[i];
-                        if (tid < 32) tc::tmem_alloc(&s_tmem, n_wg > 1 ? 128u : 64u);
+                        if (tid < 32) tc::tmem_alloc(&s_tmem, n_wg > 2 ? 256u : (n_wg > 1 ? 128u : 64u));
                     }
                     tc::fence_before_sync();
                     __syncthreads();
@@ -616,7 +620,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                         S.w = ub;
                         S.f = reinterpret_cast<const float*>(ub + kMlpWBytes);
                         S.a = ub + kWarmTileOff + g * kWarmTileBytes;
-                        S.h = S.a + kMlpTileA;
+                        S.h = S.a;
                         S.bar = &s_wbar[g];
                         S.tmem = s_tmem + 64u * static_cast<uint32_t>(g);
                         const int Q = sC.Q, S_ = sC.S, cols = sC.columns, rows = sC.rows, nl = sC.n_layout;
@@ -651,7 +655,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                                         const float ex = q.x - p.x, ey = q.y - p.y, ez = q.z - p.z;
                                         const float len = sqrtf(ex * ex + ey * ey + ez * ez);
                                         if (len > PXB_EPSILON) {
-                                            const float f = 1.0f - r / len;
+                                            const float f = 1.0f - __fdividef(r, len);
                                             x[6 + 3 * e] = ex * f; x[7 + 3 * e] = ey * f; x[8 + 3 * e] = ez * f;
                                         }
                                     }
@@ -675,7 +679,19 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     tc::fence_before_sync();
                     __syncthreads();
                     tc::fence_after_sync();
-                    if (net && tid < 32) tc::tmem_dealloc(s_tmem, n_wg > 1 ? 128u : 64u);
+                    if (net && tid < 32) tc::tmem_dealloc(s_tmem, n_wg > 2 ? 256u : (n_wg > 1 ? 128u : 64u));
+                }
+                if (net) {
+                    // the rest lengths come back: TMA bulk copy, next phase of the staging barrier
+                    fence_proxy_async();
+                    __syncthreads();
+                    if (tid == 0) {
+                        const uint32_t rest_bytes = 4u * static_cast<uint32_t>(sC.rank[rank].n_rest_pad);
+                        mbar_arrive_expect_tx(&bar, rest_bytes);
+                        if (rest_bytes) bulk_g2s(rest, sC.rest + sC.rank[rank].rest_off, rest_bytes, &bar);
+                    }
+                    stage_phase ^= 1u;
+                    if (!mbar_wait_bounded(&bar, stage_phase) && tid == 0) atomicOr(err, PXB_DEVERR_TMA_TIMEOUT);
                 }
                 // every rank's features are read before any rank moves a particle
                 cluster_or_block_sync<CL>();

@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float* __restrict_
     S.w = sm;
     S.f = reinterpret_cast<const float*>(sm + kMlpWBytes);
     S.a = sm + ((kMlpBlobBytes + 127) & ~127);
-    S.h = S.a + kMlpTileA;
+    S.h = S.a;  // the first layer consumes the inputs before the activations are written
     S.bar = &bar;
     S.tmem = tslot;
     uint32_t phase = 0;
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float* __restrict_
 
 }  // namespace
 
-int mlp_infer_smem_bytes() { return ((kMlpBlobBytes + 127) & ~127) + kMlpTileA + kMlpTileH; }
+int mlp_infer_smem_bytes() { return ((kMlpBlobBytes + 127) & ~127) + kMlpTileH; }
 
 cudaError_t launch_mlp_infer(const float* X, int n, const unsigned char* blob, float* Y, uint32_t* err,
                              int n_sms, cudaStream_t stream) {

@@ -35,9 +35,13 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
 
 // Warm-start kernel: network warpgroups per CTA and the shared memory they borrow from the
 // lambda region (weights blob, then per warpgroup an input and an activation tile).
-constexpr int kWarmGroups = 2;
+// During the network phase the rest lengths and the lambda region together are its scratch
+// (the rest lengths are staged again afterwards); a warpgroup's input tile and activation tile
+// share their bytes (the first layer's MMAs consume the inputs before the activations are
+// written). At most 4 warpgroups: 4 x 64 TMEM columns leave room for a second CTA per SM.
+constexpr int kWarmGroups = 4;
 constexpr int kWarmTileOff = 15232;      // kMlpBlobBytes rounded up to 128
-constexpr int kWarmTileBytes = 24576;    // kMlpTileA + kMlpTileH
+constexpr int kWarmTileBytes = 16384;    // max(kMlpTileA, kMlpTileH)
 constexpr int kWarmUMin = kWarmTileOff + kWarmTileBytes;
 
 // Warm-start network (mlp_kernel.cu).
@@ -45,6 +49,11 @@ int mlp_infer_smem_bytes();
 cudaError_t launch_mlp_infer(const float* X, int n, const unsigned char* blob, float* Y, uint32_t* err,
                              int n_sms, cudaStream_t stream);
 void mlp_pack_blob(const pxb_mlp_weights& m, unsigned char* out);
+// Training (mlp_train.cu): gradients of a batch given as row indices, and an Adam update.
+cudaError_t launch_mlp_grad(const float* X, const float* T, const uint32_t* idx, int rows, const pxb_mlp_weights* W,
+                            pxb_mlp_weights* G, float* loss, cudaStream_t stream);
+cudaError_t launch_mlp_adam(pxb_mlp_weights* W, const pxb_mlp_weights* G, pxb_mlp_weights* M, pxb_mlp_weights* V,
+                            float lr, float b1t, float b2t, cudaStream_t stream);
 
 cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness,
                                   const float* pts, int n, float* out, float* normals,

@@ -33,14 +33,15 @@ struct MlpSmem {
     const unsigned char* w;  // kMlpWBytes, K-major operands
     const float* f;          // kMlpFloats
     unsigned char* a;        // this warpgroup's input tile
-    unsigned char* h;        // this warpgroup's activation tile
+    unsigned char* h;        // this warpgroup's activation tile (may share the input tile's bytes)
     uint64_t* bar;           // this warpgroup's MMA-completion barrier
     uint32_t tmem;           // this warpgroup's 64 TMEM columns (lane 0)
 };
 
 __device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 
-__device__ __forceinline__ float silu(float x) { return x / (1.0f + __expf(-x)); }
+// The network needs no IEEE rounding: fast exponential and division.
+__device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
 
 // Writes row r's normalised features (24 floats) into the input tile, bf16, padded with zeros.
 __device__ __forceinline__ void mlp_put_input(const MlpSmem& S, int r, const float (&x)[kMlpIn]) {

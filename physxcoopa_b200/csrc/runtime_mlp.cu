@@ -1,6 +1,7 @@
 // runtime_mlp.cu -- C-ABI of the warm-start network: weights in and out, batch inference.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -19,6 +20,43 @@ bool finite_weights(const pxb_mlp_weights& w) {
         if (!std::isfinite(f[i])) return false;
     return true;
 }
+
+uint64_t splitmix(uint64_t& s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+double uniform01(uint64_t& s) { return static_cast<double>(splitmix(s) >> 11) * (1.0 / 9007199254740992.0); }
+double normal01(uint64_t& s) {
+    const double u1 = std::max(uniform01(s), 1e-300), u2 = uniform01(s);
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+}
+
+// Normalisation from the data: feature mean and inverse standard deviation, target root mean
+// square (floors keep constant columns finite).
+void fit_normalisation(const float* X, const float* Y, uint64_t n, pxb_mlp_weights& w) {
+    double mx[kMlpIn] = {}, sx[kMlpIn] = {}, sy[kMlpOut] = {};
+    for (uint64_t r = 0; r < n; ++r)
+        for (int k = 0; k < kMlpIn; ++k) mx[k] += X[r * kMlpIn + k];
+    for (int k = 0; k < kMlpIn; ++k) mx[k] /= static_cast<double>(n);
+    for (uint64_t r = 0; r < n; ++r) {
+        for (int k = 0; k < kMlpIn; ++k) {
+            const double d = X[r * kMlpIn + k] - mx[k];
+            sx[k] += d * d;
+        }
+        for (int j = 0; j < kMlpOut; ++j) sy[j] += static_cast<double>(Y[r * 3 + j]) * Y[r * 3 + j];
+    }
+    for (int k = 0; k < kMlpIn; ++k) {
+        const double sd = std::sqrt(sx[k] / static_cast<double>(n));
+        w.in_mean[k] = static_cast<float>(mx[k]);
+        w.in_scale[k] = static_cast<float>(1.0 / std::max(sd, 1e-12));
+    }
+    for (int j = 0; j < kMlpOut; ++j)
+        w.out_scale[j] = static_cast<float>(std::max(std::sqrt(sy[j] / static_cast<double>(n)), 1e-12));
+}
+
+size_t al256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
 
 }  // namespace
 
@@ -70,6 +108,130 @@ pxb_status pxb_mlp_infer(pxb_context* ctx, const float* features, uint32_t n, fl
                                  "read network output"))
         return s;
     return ctx->check_device_error();
+}
+
+pxb_status pxb_mlp_train(pxb_context* ctx, const float* features, const float* targets, uint64_t n,
+                         const pxb_mlp_train_desc* desc, float* final_loss) {
+    if (!ctx || !desc || !features || !targets || n == 0) return PXB_ERR_INVALID_ARGUMENT;
+    if (n > 0x7FFFFFFFull) return ctx->fail(PXB_ERR_TOO_LARGE, "more than 2^31 training rows");
+    const uint32_t batch = std::max<uint32_t>(desc->batch, 1);
+    // initial weights: N(0, 1 / fan_in), the last layer scaled down by 10
+    pxb_mlp_weights w{};
+    uint64_t seed = desc->seed;
+    for (int o = 0; o < kMlpHidden; ++o)
+        for (int i = 0; i < kMlpIn; ++i) w.w1[o][i] = static_cast<float>(normal01(seed) / std::sqrt(double(kMlpIn)));
+    for (int o = 0; o < kMlpHidden; ++o)
+        for (int i = 0; i < kMlpHidden; ++i)
+            w.w2[o][i] = static_cast<float>(normal01(seed) / std::sqrt(double(kMlpHidden)));
+    for (int o = 0; o < kMlpOut; ++o)
+        for (int i = 0; i < kMlpHidden; ++i)
+            w.w3[o][i] = static_cast<float>(0.1 * normal01(seed) / std::sqrt(double(kMlpHidden)));
+    fit_normalisation(features, targets, n, w);
+
+    // device: X | Y | row order | W | G | M | V | loss
+    const size_t bx = sizeof(float) * kMlpIn * n, by = sizeof(float) * 3 * n, bi = sizeof(uint32_t) * n;
+    const size_t bw = sizeof(pxb_mlp_weights);
+    const size_t oy = al256(bx), oi = oy + al256(by), ow = oi + al256(bi), og = ow + al256(bw), om = og + al256(bw),
+                 ov = om + al256(bw), ol = ov + al256(bw), total = ol + 256;
+    DevBuf buf;
+    if (pxb_status s = ctx->grow(buf, total, "training buffers")) return s;
+    char* b = static_cast<char*>(buf.p);
+    auto* X = reinterpret_cast<float*>(b);
+    auto* Y = reinterpret_cast<float*>(b + oy);
+    auto* I = reinterpret_cast<uint32_t*>(b + oi);
+    auto* W = reinterpret_cast<pxb_mlp_weights*>(b + ow);
+    auto* G = reinterpret_cast<pxb_mlp_weights*>(b + og);
+    auto* M = reinterpret_cast<pxb_mlp_weights*>(b + om);
+    auto* V = reinterpret_cast<pxb_mlp_weights*>(b + ov);
+    auto* L = reinterpret_cast<float*>(b + ol);
+    cudaStream_t st = ctx->stream;
+    pxb_status s = PXB_OK;
+    auto chk = [&](cudaError_t e, const char* what) {
+        if (!s && e != cudaSuccess) s = ctx->cuda(e, what);
+    };
+    chk(cudaMemcpyAsync(X, features, bx, cudaMemcpyHostToDevice, st), "upload training features");
+    chk(cudaMemcpyAsync(Y, targets, by, cudaMemcpyHostToDevice, st), "upload training targets");
+    chk(cudaMemcpyAsync(W, &w, bw, cudaMemcpyHostToDevice, st), "upload initial weights");
+    chk(cudaMemsetAsync(M, 0, ov + al256(bw) - om, st), "zero optimiser state");
+    std::vector<uint32_t> order(n);
+    for (uint64_t r = 0; r < n; ++r) order[r] = static_cast<uint32_t>(r);
+    float epoch_loss = 0.0f;
+    uint64_t t = 0;
+    const uint32_t epochs = std::max<uint32_t>(desc->epochs, 1);
+    for (uint32_t ep = 0; ep < epochs && !s; ++ep) {
+        for (uint64_t r = n - 1; r > 0; --r) std::swap(order[r], order[splitmix(seed) % (r + 1)]);
+        chk(cudaMemcpyAsync(I, order.data(), bi, cudaMemcpyHostToDevice, st), "upload batch order");
+        chk(cudaMemsetAsync(L, 0, sizeof(float), st), "zero loss");
+        // cosine learning-rate schedule over the epochs
+        const float lr = desc->learning_rate * 0.5f * (1.0f + std::cos(3.14159265f * ep / epochs));
+        for (uint64_t r0 = 0; r0 < n && !s; r0 += batch) {
+            const int rows = static_cast<int>(std::min<uint64_t>(batch, n - r0));
+            ++t;
+            chk(cudaMemsetAsync(G, 0, bw, st), "zero gradients");
+            chk(launch_mlp_grad(X, Y, I + r0, rows, W, G, L, st), "launch gradients");
+            chk(launch_mlp_adam(W, G, M, V, lr, std::pow(0.9f, float(t)), std::pow(0.999f, float(t)), st),
+                "launch adam");
+            ctx->launches += 2;
+        }
+        float lsum = 0.0f;
+        chk(cudaMemcpyAsync(&lsum, L, sizeof(float), cudaMemcpyDeviceToHost, st), "read loss");
+        chk(cudaStreamSynchronize(st), "training epoch");
+        // every batch added the squared errors of its rows: the epoch's mean over rows and outputs
+        epoch_loss = lsum / (3.0f * static_cast<float>(n));
+    }
+    pxb_mlp_weights out{};
+    chk(cudaMemcpyAsync(&out, W, bw, cudaMemcpyDeviceToHost, st), "read trained weights");
+    chk(cudaStreamSynchronize(st), "training");
+    cudaFree(buf.p);
+    if (s) return s;
+    if (pxb_status e = ctx->check_device_error()) return e;
+    if (!finite_weights(out)) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "training diverged (non-finite weights)");
+    if (final_loss) *final_loss = epoch_loss;
+    ctx->mlp = out;
+    ctx->has_mlp = true;
+    return ctx->upload_mlp();
+}
+
+pxb_status pxb_mlp_loss_gradients(pxb_context* ctx, const float* features, const float* targets, uint64_t n,
+                                  float* loss, pxb_mlp_weights* grads) {
+    if (!ctx || !features || !targets || !loss || !grads || n == 0) return PXB_ERR_INVALID_ARGUMENT;
+    if (!ctx->has_mlp) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "no network installed");
+    if (n > 0x7FFFFFFFull) return ctx->fail(PXB_ERR_TOO_LARGE, "too many rows");
+    const size_t bx = sizeof(float) * kMlpIn * n, by = sizeof(float) * 3 * n, bi = sizeof(uint32_t) * n;
+    const size_t bw = sizeof(pxb_mlp_weights);
+    const size_t oy = al256(bx), oi = oy + al256(by), ow = oi + al256(bi), og = ow + al256(bw), ol = og + al256(bw),
+                 total = ol + 256;
+    DevBuf buf;
+    if (pxb_status s = ctx->grow(buf, total, "gradient buffers")) return s;
+    char* b = static_cast<char*>(buf.p);
+    std::vector<uint32_t> order(n);
+    for (uint64_t r = 0; r < n; ++r) order[r] = static_cast<uint32_t>(r);
+    cudaStream_t st = ctx->stream;
+    pxb_status s = PXB_OK;
+    auto chk = [&](cudaError_t e, const char* what) {
+        if (!s && e != cudaSuccess) s = ctx->cuda(e, what);
+    };
+    chk(cudaMemcpyAsync(b, features, bx, cudaMemcpyHostToDevice, st), "upload features");
+    chk(cudaMemcpyAsync(b + oy, targets, by, cudaMemcpyHostToDevice, st), "upload targets");
+    chk(cudaMemcpyAsync(b + oi, order.data(), bi, cudaMemcpyHostToDevice, st), "upload rows");
+    chk(cudaMemcpyAsync(b + ow, &ctx->mlp, bw, cudaMemcpyHostToDevice, st), "upload weights");
+    chk(cudaMemsetAsync(b + og, 0, bw, st), "zero gradients");
+    chk(cudaMemsetAsync(b + ol, 0, sizeof(float), st), "zero loss");
+    chk(launch_mlp_grad(reinterpret_cast<float*>(b), reinterpret_cast<float*>(b + oy),
+                        reinterpret_cast<uint32_t*>(b + oi), static_cast<int>(n),
+                        reinterpret_cast<pxb_mlp_weights*>(b + ow), reinterpret_cast<pxb_mlp_weights*>(b + og),
+                        reinterpret_cast<float*>(b + ol), st),
+        "launch gradients");
+    ++ctx->launches;
+    float lsum = 0.0f;
+    chk(cudaMemcpyAsync(grads, b + og, bw, cudaMemcpyDeviceToHost, st), "read gradients");
+    chk(cudaMemcpyAsync(&lsum, b + ol, sizeof(float), cudaMemcpyDeviceToHost, st), "read loss");
+    chk(cudaStreamSynchronize(st), "gradients");
+    cudaFree(buf.p);
+    if (s) return s;
+    if (pxb_status e = ctx->check_device_error()) return e;
+    *loss = lsum / (3.0f * static_cast<float>(n));
+    return PXB_OK;
 }
 
 pxb_status pxb_cloths_step_warm(pxb_context* ctx, const pxb_cloth_step_desc* step, const pxb_warm_start_desc* warm) {

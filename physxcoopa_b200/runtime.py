@@ -38,6 +38,8 @@ SIGNATURES = {
     "pxb_mlp_set_weights": ([P, C.POINTER(A.MlpWeights)], C.c_int),
     "pxb_mlp_get_weights": ([P, C.POINTER(A.MlpWeights)], C.c_int),
     "pxb_mlp_infer": ([P, P, u32, P], C.c_int),
+    "pxb_mlp_train": ([P, P, P, u64, C.POINTER(A.MlpTrainDesc), C.POINTER(f32)], C.c_int),
+    "pxb_mlp_loss_gradients": ([P, P, P, u64, C.POINTER(f32), C.POINTER(A.MlpWeights)], C.c_int),
     "pxb_cloths_step_warm": ([P, C.POINTER(A.ClothStepDesc), C.POINTER(A.WarmStartDesc)], C.c_int),
     "pxb_cloths_read_warm_results": ([P, P, u32, P], C.c_int),
     "pxb_cloths_record": ([P, C.POINTER(A.ClothStepDesc), u32, P, P, u64, C.POINTER(u64)], C.c_int),
@@ -293,6 +295,25 @@ class Context:
         out = np.zeros((len(x), 3), np.float32)
         self._check(self.lib.pxb_mlp_infer(self.h, A.ptr(x), len(x), A.ptr(out)), "mlp_infer")
         return out
+
+    def mlp_train(self, features, targets, epochs=20, batch=8192, learning_rate=3e-3, seed=0):
+        """Fits and installs the network (pxb_mlp_train); returns the last epoch's mean loss."""
+        x = np.ascontiguousarray(features, np.float32).reshape(-1, 24)
+        y = np.ascontiguousarray(targets, np.float32).reshape(-1, 3)
+        d = A.MlpTrainDesc(epochs, batch, learning_rate, seed)
+        loss = f32()
+        self._check(self.lib.pxb_mlp_train(self.h, A.ptr(x), A.ptr(y), len(x), C.byref(d), C.byref(loss)),
+                    "mlp_train")
+        return loss.value
+
+    def mlp_loss_gradients(self, features, targets):
+        x = np.ascontiguousarray(features, np.float32).reshape(-1, 24)
+        y = np.ascontiguousarray(targets, np.float32).reshape(-1, 3)
+        loss = f32()
+        g = A.MlpWeights()
+        self._check(self.lib.pxb_mlp_loss_gradients(self.h, A.ptr(x), A.ptr(y), len(x), C.byref(loss), C.byref(g)),
+                    "mlp_loss_gradients")
+        return loss.value, g.as_numpy()
 
     def step_warm(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
                   iterations=10, h=1.0 / 60.0, warm_iterations=4, threshold=1e-4, thresholds=None):

@@ -341,6 +341,19 @@ pxb_status pxb_cloths_read_results(pxb_context* ctx, const uint64_t* cloths, uin
  * a determinism hash reads back each frame. */
 pxb_status pxb_cloths_read_positions(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
                                      float* out, size_t capacity);
+/* The same gather into DEVICE memory `out_device` (capacity floats), allocating nothing. No
+ * counterpart in the reference. For callers that may not allocate device memory while they run
+ * (a per-frame reader inside a fixed memory budget, or code where cudaMalloc / cudaFree would
+ * synchronise the device or is not permitted): pxb_cloths_read_positions grows internal buffers
+ * on demand, this never does. At most 4096 cloths per call (PXB_ERR_TOO_LARGE beyond); the
+ * per-call cloth list lives in a 48 KB array compiled into the library, held on every GPU that
+ * loads it until exit. The first call on a device looks up that array's address (set-up):
+ * make it before any stream capture. The registry must be current (a step since the last
+ * add / remove / parameter change), else PXB_ERR_INVALID_ARGUMENT. Enqueued on the context
+ * stream, returns before completion; calls that overlap on the GPU (other contexts or streams
+ * of the same device) share the array and race -- serialise them. */
+pxb_status pxb_cloths_gather_positions_device(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
+                                              float* out_device, size_t capacity);
 
 /* Drop-in single-cloth solve on HOST memory, the exact contract of cloth::solve_cloth: the cloth
  * described by `desc` is uploaded, advanced, and its particles / lambdas / anchors / time /

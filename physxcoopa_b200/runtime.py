@@ -35,6 +35,7 @@ SIGNATURES = {
     "pxb_cloth_params_default": ([C.POINTER(A.ClothParams)], None),
     "pxb_cloth_add": ([P, C.POINTER(A.ClothDesc), C.POINTER(u64)], C.c_int),
     "pxb_cloth_remove": ([P, u64], C.c_int),
+    "pxb_cloths_gather_positions_device": ([P, P, u32, P, C.c_size_t], C.c_int),
     "pxb_mlp_set_weights": ([P, C.POINTER(A.MlpWeights)], C.c_int),
     "pxb_mlp_get_weights": ([P, C.POINTER(A.MlpWeights)], C.c_int),
     "pxb_mlp_infer": ([P, P, u32, P], C.c_int),
@@ -455,6 +456,13 @@ class Context:
         self._check(self.lib.pxb_cloths_read_positions(self.h, A.ptr(ids), len(ids), out.ctypes.data,
                                                        out.size), "read_positions")
         return out
+
+    def gather_positions_device(self, ids, out_ptr, capacity):
+        """pxb_cloths_gather_positions_device: positions into device memory at out_ptr
+        (capacity floats), with no allocation; enqueued on the context stream."""
+        ids = np.ascontiguousarray(ids, np.uint64)
+        self._check(self.lib.pxb_cloths_gather_positions_device(self.h, A.ptr(ids), len(ids), out_ptr, capacity),
+                    "gather_positions_device")
 
     def project_particles(self, collider, thickness, points):
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)

@@ -2,7 +2,8 @@
 """Cloth XPBD benchmark: cloth vertex-substeps/s on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
-                    [--workload uniform_batch|single_drape|uneven_batch] [--cloths C]
+                    [--workload uniform_batch|single_drape|uneven_batch|warm_start|hair_groom]
+                    [--cloths C]
 
 One step = one PhysicsWorld cloth frame for every cloth of the workload: a single batched
 launch of the device solver (pxb_cloths_step) advancing each cloth by solve_cloth(h = 1/60,
@@ -24,6 +25,14 @@ steps.
            headers) on a bounded sample of the workload on the host's cores, whole cloths per
            thread as the reference's serial dispatch solves them.
 
+--workload warm_start is the learned warm start on the uneven batch: training rows recorded from
+the plain 20-iteration solver on a separately seeded batch, the network trained (Adam, lr 1e-3),
+then the same benchmark state stepped with 20 plain iterations and with the network plus 4
+iterations, falling back per substep to the 20 plain iterations where the residual (max
+|len / rest - 1| over the stretch constraints) exceeds that cloth's residual under the plain
+solver over the same steps: equal residual, cloth by cloth. `value` is the warm-start
+throughput, `plain` the plain one.
+
 --impl reference runs only that CPU implementation (rank 0; other ranks exit 0).
 """
 import argparse
@@ -41,7 +50,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SPEC = "cloth vertex-substeps/s on 1 B200: plain XPBD vs NN warm-start at equal residual"
-METRIC = "cloth vertex-substeps/s (plain XPBD)"
+METRIC = SPEC
 UNIT = "vertex-substeps/s"
 
 
@@ -52,7 +61,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--workload", default="uniform_batch",
-                    choices=["uniform_batch", "single_drape", "uneven_batch", "hair_groom"])
+                    choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom"])
     ap.add_argument("--cloths", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -250,6 +259,132 @@ def bench_hair(args, ctx_factory):
     return 0
 
 
+def bench_warm(args, local_rank):
+    """Learned warm start vs the plain 20-iteration solver at equal residual (see the module
+    docstring). Returns the JSON line."""
+    import torch
+    from physxcoopa_b200 import _abi as A
+    from physxcoopa_b200 import runtime as R
+    from physxcoopa_b200 import scenes
+    n = args.cloths or 4096
+    plain_iters, warm_iters = 20, 4
+    ctx = R.Context(local_rank)
+    ctx.set_cloth_variant(0 if args.variant is None else args.variant)
+    # --- training rows from the plain solver on a separately seeded batch -------------------
+    t0 = time.perf_counter()
+    tr = scenes.uneven_batch(n=min(512, n), seed=102)
+    ids = [ctx.add_cloth(c) for c in tr.cloths]
+    xs, ys = [], []
+    rec_steps, want = 40, 2_000_000
+    for step in range(rec_steps):
+        x, y = ctx.record(ids, tr.colliders, sources=tr.sources, iterations=plain_iters, substep=step % 4)
+        keep = np.random.default_rng(step).random(len(x)) < want / (rec_steps * max(len(x), 1))
+        xs.append(x[keep])
+        ys.append(y[keep])
+    for i in ids:
+        ctx.remove_cloth(i)
+    X, Y = np.concatenate(xs), np.concatenate(ys)
+    t_rec = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss = ctx.mlp_train(X, Y, epochs=40, batch=8192, learning_rate=1e-3, seed=0)
+    t_train = time.perf_counter() - t0
+
+    sc = scenes.uneven_batch(n=n, seed=2)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local_rank))
+    W = max(args.warmup, 3)
+
+    def run(kind, taus=None, collect=False, e2e=False):
+        """Steps a fresh copy of the benchmark batch: W plain warm-up steps, then args.steps of
+        `kind`. Timed with CUDA events unless `collect`, which reads the per-step warm results
+        (a host round trip per step) instead."""
+        ids = [ctx.add_cloth(c) for c in sc.cloths]
+        d, keep = ctx.make_step(ids, sc.colliders, sc.gravity, sc.sources, sc.substeps, plain_iters, sc.h)
+        for _ in range(W):
+            ctx.step_desc(d)
+        ctx.synchronize()
+        res = []
+        t_a, t_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launch_count
+        ids_np = np.ascontiguousarray(ids, np.uint64)
+        out = torch.empty(3 * sc.vertices, dtype=torch.float32, pin_memory=True).numpy() if e2e else None
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            t_a.record(stream)
+            for _ in range(args.steps):
+                if kind == "plain":
+                    ctx.step_desc(d)
+                elif kind == "plain_residual":
+                    ctx.step_warm_desc(d, warm_iterations=0)
+                else:
+                    ctx.step_warm_desc(d, warm_iterations=warm_iters, thresholds=taus)
+                if e2e:
+                    ctx.read_positions(ids_np, out)
+                if collect:
+                    res.append(ctx.read_warm_results(ids))
+            t_b.record(stream)
+        torch.cuda.synchronize()
+        ms = t_a.elapsed_time(t_b) / args.steps
+        launches = ctx.launch_count - l0
+        for i in ids:
+            ctx.remove_cloth(i)
+        del keep
+        return ms, res, launches
+
+    ms_plain, _, _ = run("plain")
+    _, res_p, _ = run("plain_residual", collect=True)
+    rp = np.stack([r["residual"] for r in res_p])
+    taus = rp.max(0).astype(np.float32)
+    _, res_w, _ = run("warm", taus, collect=True)
+    rw = np.stack([r["residual"] for r in res_w])
+    fb = float(sum(r["fallbacks"].sum() for r in res_w) / sum(r["substeps"].sum() for r in res_w))
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ms_w_total, _, launches = run("warm", taus)
+    clk = clocks.stop()
+    ms_e2e, _, _ = run("warm", taus, e2e=True)
+    verts = sc.vertices * sc.substeps
+    value = verts / (ms_w_total * 1e-3)
+    plain_value = verts / (ms_plain * 1e-3)
+    al = lambda x: (x + 255) & ~255
+    n_col = sum(len(c) for c in sc.colliders)
+    n_src = sum(0 if s is None else len(s) for s in (sc.sources or []))
+    h2d = al(184 * n) + al(236 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * n) + al(48 * n)
+    d2h = 12 * sc.vertices + 16 * n
+    cons = sum(len(c.stretch) + len(c.bend) for c in sc.cloths)
+    iters_done = warm_iters + fb * plain_iters
+    algo_bytes = sc.substeps * (iters_done * cons * 68 + sc.vertices * 150)
+    smem_bw = ctx.measure_smem_bandwidth()
+    achieved = algo_bytes / (ms_w_total * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": W,
+        "ms_per_step": ms_w_total, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 solve, bf16 network (fp32 accumulation)", "data": "synthetic (seeded scenes)",
+        "config": dict(workload_config(args, sc), workload=f"warm_start on {sc.name}", iterations=plain_iters,
+                       warm_iterations=warm_iters, residual="max |len/rest - 1| over stretch constraints",
+                       equal_residual="per cloth: fall back where the residual exceeds the plain solver's "
+                                      "max residual for that cloth over the same steps"),
+        "plain": {"value": plain_value, "ms_per_step": ms_plain, "residual_median": float(np.median(rp)),
+                  "residual_max": float(rp.max())},
+        "warm_start": {"speedup_vs_plain": value / plain_value, "fallback_rate": fb,
+                       "residual_median": float(np.median(rw)), "residual_max": float(rw.max()),
+                       "training": {"rows": int(len(X)), "final_loss": loss, "record_s": t_rec, "train_s": t_train,
+                                    "scenes": "uneven batch seed 102 (512 cloths), plain 20 iterations, "
+                                              f"{rec_steps} steps"}},
+        "e2e": {"value": verts / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_bw / 1e9, "unit": "GB/s",
+                     "frac": achieved * 1e9 / smem_bw, "traffic": None,
+                     "peak_source": "measured on this GPU by pxb_measure_smem_bandwidth",
+                     "kernel": "cloth_step_kernel (warm start)", "algorithmic_bytes_per_launch": algo_bytes},
+        "cpu_baseline": None,
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    ctx.close()
+    return line
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -279,6 +414,10 @@ def main():
     if args.workload == "hair_groom":
         from physxcoopa_b200 import runtime as R
         return bench_hair(args, lambda: R.Context(local_rank))
+    if args.workload == "warm_start":
+        if rank == 0:
+            print(json.dumps(bench_warm(args, local_rank)))
+        return 0
 
     import torch
     dist = None

@@ -267,9 +267,10 @@ pxb_status pxb_cloth_remove(pxb_context* ctx, uint64_t id);
 
 /* How pxb_cloth_add would lay a cloth out on the device. A cloth whose state does not fit one
  * CTA's shared memory is split by rows over a thread-block cluster of n_ranks CTAs (1, 2, 4 or
- * 8). No counterpart in the reference, which has no device layout. */
+ * 8); beyond that (e.g. 512 x 512) every SM works on it with its state in global memory
+ * (n_ranks 0). No counterpart in the reference, which has no device layout. */
 typedef struct pxb_cloth_plan {
-    int32_t n_ranks;          /* CTAs holding the cloth (a cluster when > 1) */
+    int32_t n_ranks;          /* CTAs holding the cloth (a cluster when > 1; 0: the whole GPU) */
     int32_t rows_per_rank;    /* grid rows per CTA (the last CTA may hold fewer) */
     int32_t threads;          /* threads per CTA the cloth asks for */
     int32_t smem_bytes;       /* largest per-CTA dynamic shared memory */

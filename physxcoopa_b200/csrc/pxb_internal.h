@@ -183,6 +183,15 @@ struct PxbStrandStep {
     int32_t col_begin, col_count, src_begin, src_count;
 };
 
+// Inter-CTA state of one whole-GPU cloth launch (zeroed before the launch).
+struct PxbGridSync {
+    unsigned int count;      // barrier arrivals so far
+    unsigned int gen;        // barriers completed
+    float base_accel[3];     // gravity (+ external) selected for this step
+    unsigned int keys[7];    // order-preserving keys: bounds min xyz, max xyz, max speed^2
+    unsigned int pad[4];
+};
+
 struct PxbFrameResult {
     float bounds_min[3];
     float bounds_max[3];

@@ -44,6 +44,11 @@ constexpr int kWarmTileOff = 15232;      // kMlpBlobBytes rounded up to 128
 constexpr int kWarmTileBytes = 16384;    // max(kMlpTileA, kMlpTileH)
 constexpr int kWarmUMin = kWarmTileOff + kWarmTileBytes;
 
+// Whole-GPU path for one cloth beyond an 8-CTA cluster: a cooperative launch of one CTA per SM.
+cudaError_t launch_cloth_grid(const PxbClothDev* cloths, const PxbClothStep* steps, const PxbDevCollider* colliders,
+                              const pxb_gravity_source* sources, const int32_t* order, PxbFrameResult* results,
+                              uint32_t* err, PxbGridSync* gs, int slot, int n_sms, cudaStream_t stream);
+
 // Warm-start network (mlp_kernel.cu).
 int mlp_infer_smem_bytes();
 cudaError_t launch_mlp_infer(const float* X, int n, const unsigned char* blob, float* Y, uint32_t* err,

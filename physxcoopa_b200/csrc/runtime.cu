@@ -580,9 +580,16 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
         layout_ranks(e);
         if (e.dev.smem_bytes <= kMaxDynamicSmem) placed = true;
     }
-    if (!placed)
-        return fail(PXB_ERR_TOO_LARGE, "a %ux%u cloth does not fit a cluster of %d CTAs", d->columns, d->rows,
-                    PXB_MAX_RANKS);
+    if (!placed) {
+        // Beyond a cluster: the whole-GPU path (every SM on this cloth, state in global memory).
+        std::vector<int32_t> padded;
+        if (!build_ranks(e, cs, rest_ref, 1, padded, max_colour))
+            return fail(PXB_ERR_TOO_LARGE, "a %ux%u cloth has more colour segments than supported", d->columns,
+                        d->rows);
+        e.rest_ref.swap(padded);
+        layout_ranks(e);
+        e.grid = true;
+    }
     if (!verify_ranks(e, d)) return fail(PXB_ERR_UNSUPPORTED, "colour segments do not reproduce the constraint lists");
     e.time = d->time;
     e.threads = std::min(kClothMaxThreads, std::max(64, ((max_colour + 1) / 2 + 31) & ~31));
@@ -845,6 +852,10 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
 
     if (warm) {
         for (uint32_t k = 0; k < n; ++k)
+            if (ents[k]->grid)
+                return fail(PXB_ERR_UNSUPPORTED, "cloth %llu runs on the whole-GPU path, which has no warm start",
+                            (unsigned long long)sd->cloths[k]);
+        for (uint32_t k = 0; k < n; ++k)
             if (ents[k]->warm_smem > kMaxDynamicSmem)
                 return fail(PXB_ERR_TOO_LARGE, "cloth %llu: the warm-start kernel needs %d bytes of shared memory",
                             (unsigned long long)sd->cloths[k], ents[k]->warm_smem);
@@ -889,6 +900,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
+        if (ents[x]->grid != ents[y]->grid) return ents[y]->grid;  // whole-GPU cloths last
         const size_t rx = ents[x]->ranks.size(), ry = ents[y]->ranks.size();
         if (rx != ry) return rx < ry;
         if (fit[x] != fit[y]) return fit[x] < fit[y];
@@ -962,13 +974,34 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     // Launch groups: (cluster size, CTAs per SM). With several, each goes to a side stream so
     // they share the SMs instead of running one after another (a group of small cloths alone
     // leaves most of the device idle).
+    // Whole-GPU cloths first, one cooperative launch each on the context stream: the side
+    // streams below fork after them, so nothing else holds SMs while they run.
+    uint32_t n_plain = n;
+    while (n_plain > 0 && ents[perm[n_plain - 1]]->grid) --n_plain;
+    if (n_plain < n) {
+        const size_t gbytes = sizeof(PxbGridSync) * (n - n_plain);
+        if (pxb_status s = grow(d_grid, gbytes, "grid barriers")) return s;
+        if (pxb_status s = cuda(cudaMemsetAsync(d_grid.p, 0, gbytes, stream), "zero grid barriers")) return s;
+        for (uint32_t slot = n_plain; slot < n; ++slot) {
+            cudaError_t le = launch_cloth_grid(static_cast<const PxbClothDev*>(d_registry.p),
+                                               reinterpret_cast<const PxbClothStep*>(db),
+                                               reinterpret_cast<const PxbDevCollider*>(db + o_cols),
+                                               reinterpret_cast<const pxb_gravity_source*>(db + o_src),
+                                               reinterpret_cast<const int32_t*>(db + o_order),
+                                               static_cast<PxbFrameResult*>(d_results.p), d_err,
+                                               static_cast<PxbGridSync*>(d_grid.p) + (slot - n_plain),
+                                               static_cast<int>(slot), n_sms, stream);
+            if (le != cudaSuccess) return cuda(le, "launch whole-GPU cloth");
+            ++launches;
+        }
+    }
     struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; };
     std::vector<Group> groups;
-    for (uint32_t g0 = 0; g0 < n;) {
+    for (uint32_t g0 = 0; g0 < n_plain;) {
         const int cluster = static_cast<int>(ents[perm[g0]]->ranks.size());
         const int group_fit = fit[perm[g0]];
         Group G{g0, g0, cluster, 64, 0, 0.0};
-        while (G.g1 < n && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster && fit[perm[G.g1]] == group_fit) {
+        while (G.g1 < n_plain && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster && fit[perm[G.g1]] == group_fit) {
             const ClothEntry& e = *ents[perm[G.g1]];
             G.threads = std::max(G.threads, launch_threads(e));
             G.smem = std::max(G.smem, launch_smem(e));
@@ -1140,10 +1173,10 @@ pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out
         if (err && err_cap) snprintf(err, err_cap, "%s", msg.c_str());
         return st;
     }
-    out->n_ranks = static_cast<int32_t>(e.ranks.size());
+    out->n_ranks = e.grid ? 0 : static_cast<int32_t>(e.ranks.size());
     out->rows_per_rank = e.ranks[0].n_rows;
     out->threads = e.threads;
-    out->smem_bytes = e.dev.smem_bytes;
+    out->smem_bytes = e.grid ? 0 : e.dev.smem_bytes;
     out->n_colours = e.n_colours;
     out->n_segments = static_cast<int32_t>(e.segs.size());
     out->layout_slots = e.n_layout;
@@ -1176,7 +1209,7 @@ pxb_status pxb_cloth_set_params(pxb_context* ctx, uint64_t id, const pxb_cloth_p
     const pxb_cloth_params old = e->params;
     e->params = *params;
     ctx->refresh_layout(*e);
-    if (e->dev.smem_bytes > kMaxDynamicSmem) {
+    if (!e->grid && e->dev.smem_bytes > kMaxDynamicSmem) {
         e->params = old;
         ctx->refresh_layout(*e);
         return ctx->fail(PXB_ERR_TOO_LARGE, "these params need more shared memory than the path holds");
@@ -1407,7 +1440,7 @@ pxb_status pxb_solve_cloth_host(pxb_context* ctx, const pxb_cloth_desc* desc, px
         ClothEntry* e = ctx->lookup(id);
         e->params = desc->params;
         ctx->refresh_layout(*e);
-        if (e->dev.smem_bytes > kMaxDynamicSmem) return ctx->fail(PXB_ERR_TOO_LARGE, "params need too much shared memory");
+        if (!e->grid && e->dev.smem_bytes > kMaxDynamicSmem) return ctx->fail(PXB_ERR_TOO_LARGE, "params need too much shared memory");
         if ((s = ctx->upload_segments(*e))) return s;
         if ((s = ctx->upload_particles(*e, desc->particles))) return s;
         for (uint32_t a = 0; a < desc->n_anchors; ++a) {

@@ -24,6 +24,7 @@ struct TopologyEdge {
 // anchors, tethers) plus the device-side description and its allocation.
 struct ClothEntry {
     bool alive = false;
+    bool grid = false;  // beyond a cluster: solved by every SM from global memory
     uint32_t generation = 0;
     uint32_t n_particles = 0;
     int cols = 0, rows = 0, Q = 0, S = 0, n_layout = 0;
@@ -122,7 +123,7 @@ struct pxb_context {
             if (e.alive && e.dmem) cudaFree(e.dmem);
         for (StrandEntry& e : strand_sets)
             if (e.alive && e.dmem) cudaFree(e.dmem);
-        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune, &d_mlp, &d_mlp_io, &d_wresults, &d_rec})
+        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune, &d_mlp, &d_mlp_io, &d_wresults, &d_rec, &d_grid})
             if (b->p) cudaFree(b->p);
         if (pinned) cudaFreeHost(pinned);
         if (d_err) cudaFree(d_err);
@@ -158,7 +159,7 @@ struct pxb_context {
         const int64_t* rec_row0 = nullptr;
     };
     pxb_status step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg* warm = nullptr);
-    DevBuf d_wresults, d_rec;
+    DevBuf d_wresults, d_rec, d_grid;
     bool warm_fresh = false;
     bool last_step_warm = false;
     pxb_status fetch_warm_results();

@@ -468,3 +468,52 @@ def test_batch_of_every_cluster_size(ctx):
         off += 3 * n
     for cid in ids:
         ctx.remove_cloth(cid)
+
+
+
+# --- cloths beyond a cluster: every SM on one cloth, state in global memory ---------------------
+
+def test_whole_gpu_cloth_equals_oracle(ctx):
+    """A 200 x 200 sheet (beyond an 8-CTA cluster) with a gravity source and a box: the
+    cooperative whole-GPU kernel equals the oracle, value for value, with lambdas and results."""
+    cloth = clustered_sheet(200, 200, seed=21, pins="edge")
+    assert R.plan_cloth(cloth)["n_ranks"] == 0
+    cols = collider_array([box((0.8, 0.6, 0.5), (0.3, 0.1, -0.2), (0.0, 0.3826834, 0.0, 0.9238795))])
+    src = gravity_sources([((0.5, -0.3, -3.0), 9.81, 1.0, 10.0)])
+    gpu, orc, res_, lam, t = run_pair(ctx, cloth, cols, sources=src, steps=3)
+    assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-5
+    assert_pins_exact(gpu, orc.particles)
+    assert_equal_particles(gpu, orc.particles, "200x200")
+    assert np.array_equal(res_["bounds_min"], orc.bounds[:3])
+    assert np.array_equal(res_["bounds_max"], orc.bounds[3:])
+    assert np.float32(res_["max_speed"]) == K.oracle().orc_max_particle_speed(
+        A.ptr(orc.particles), len(orc.particles))
+    assert np.array_equal(lam[1], orc.bend["lambda"])
+
+
+def test_large_cloth_512_one_step_equals_oracle(ctx):
+    """The large-cloth configuration's sheet: 512 x 512, 20 iterations, draped on a capsule."""
+    cloth = clustered_sheet(512, 512, seed=3)
+    cols = collider_array([capsule(0.4, 3.0, (0.0, 0.0, 0.4), axis=0)])
+    gpu, orc, res_, lam, t = run_pair(ctx, cloth, cols, steps=1, iterations=20)
+    assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-5
+    assert_pins_exact(gpu, orc.particles)
+    assert_equal_particles(gpu, orc.particles, "512x512")
+
+
+def test_batch_with_a_whole_gpu_cloth(ctx):
+    """Whole-GPU and shared-memory cloths in one step call."""
+    cloths = [clustered_sheet(c, c, seed=k) for k, c in enumerate((30, 190, 70))]
+    cols = [collider_array([sphere(0.4, (0.0, 0.0, 0.4))]) for _ in cloths]
+    orcs = [c.copy() for c in cloths]
+    ids = [ctx.add_cloth(c) for c in cloths]
+    for _ in range(2):
+        ctx.step(ids, cols)
+        for o, c in zip(orcs, cols):
+            K.oracle_step_cloth(o, c, substeps=4, iterations=10)
+    res = ctx.read_results(ids)
+    for k, (cid, o) in enumerate(zip(ids, orcs)):
+        assert_equal_particles(ctx.read_particles(cid, len(o.particles)), o.particles, f"cloth {k}")
+        assert np.array_equal(res[k]["bounds_max"], o.bounds[3:])
+    for cid in ids:
+        ctx.remove_cloth(cid)

@@ -55,11 +55,13 @@ def test_aero_off_needs_less_memory():
     assert off["smem_bytes"] <= on["smem_bytes"]
 
 
-def test_too_large_and_refusals_match_add_cloth():
-    with pytest.raises(R.PxbError) as e:
-        R.plan_cloth(sheet(181, 181))
-    assert e.value.status == 7  # PXB_ERR_TOO_LARGE
-    assert "cluster" in str(e.value)
+def test_beyond_a_cluster_plans_the_whole_gpu_path():
+    for side in (181, 256, 512):
+        p = R.plan_cloth(sheet(side, side))
+        assert p["n_ranks"] == 0 and p["smem_bytes"] == 0 and p["rows_per_rank"] == side
+
+
+def test_refusals_match_add_cloth():
     ok = sheet(9, 9)
     odd = ok.copy()
     odd.stretch = odd.stretch[::-1].copy()

@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--workload", default="uniform_batch",
-                    choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom"])
+                    choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom",
+                             "large_cloth_hair"])
     ap.add_argument("--cloths", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -259,6 +260,89 @@ def bench_hair(args, ctx_factory):
     return 0
 
 
+def bench_large(args, local_rank):
+    """The large-cloth configuration: one 512 x 512 sheet (20 iterations, draped on a capsule,
+    whole-GPU path) stepped together with the 65,536 x 32 groom (20 iterations, roots on a moving
+    sphere). One step = one frame of both. Units: (cloth vertices + hair particles) x substeps."""
+    import torch
+    from physxcoopa_b200 import _abi as A
+    from physxcoopa_b200 import runtime as R
+    from physxcoopa_b200 import scenes
+    from physxcoopa_b200.arrays import capsule, collider_array
+    ctx = R.Context(local_rank)
+    side = 512
+    w = scenes.SPACING * (side - 1)
+    h = R.HostCloth(side, side, w, w, center=(0.0, 0.0, 1.0), params=scenes.cloth_params(), jitter=1e-3, seed=5)
+    h.pin_static((-w / 2, w / 2, 1.0), 0.3 * scenes.SPACING)
+    h.pin_static((w / 2, w / 2, 1.0), 0.3 * scenes.SPACING)
+    h.build_tethers()
+    cloth = h.arrays()
+    cap = collider_array([capsule(0.5, 0.45 * w, (0.0, 0.0, 0.3), axis=0)])
+    cid = ctx.add_cloth(cloth)
+    dc, keep_c = ctx.make_step([cid], [cap], iterations=20)
+    hair = scenes.hair_groom(n_strands=args.cloths or 65536)
+    sid = ctx.add_strands(hair.sets[0])
+    pos, rot = hair.root_path(0)
+    ctx.set_strand_roots(sid, pos, rot)
+    ds, keep_s = ctx.make_strand_step([sid], [hair.meta["colliders_at"](0)], iterations=hair.iterations,
+                                      substeps=hair.substeps, h=hair.h)
+    W = max(args.warmup, 3)
+    for _ in range(W):
+        ctx.step_desc(dc)
+        ctx.step_strands_desc(ds)
+    ctx.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    l0 = ctx.launch_count
+    cloth_ms = 0.0
+    with torch.cuda.stream(stream):
+        t0.record(stream)
+        for _ in range(args.steps):
+            c0.record(stream)
+            ctx.step_desc(dc)
+            c1.record(stream)
+            ctx.step_strands_desc(ds)
+        t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = ctx.launch_count - l0
+    ms = t0.elapsed_time(t1) / args.steps
+    cloth_last_ms = c0.elapsed_time(c1)
+    n_cloth, n_hair = len(cloth.particles), len(hair.sets[0].particles)
+    units = (n_cloth + n_hair) * 4
+    # end to end: roots and colliders up, cloth positions and hair particles back, every frame
+    out = np.zeros(3 * n_cloth, np.float32)
+    e_steps = max(3, args.steps // 2)
+    e0 = time.perf_counter()
+    for f in range(e_steps):
+        ctx.step_desc(dc)
+        pos, rot = hair.root_path(f + 1)
+        ctx.set_strand_roots(sid, pos, rot)
+        ctx.step_strands([sid], [hair.meta["colliders_at"](f + 1)], iterations=hair.iterations)
+        ctx.read_positions(np.array([cid], np.uint64), out)
+        ctx.read_strand_particles(sid, n_hair)
+    e2e_s = (time.perf_counter() - e0) / e_steps
+    line = {"metric": METRIC, "value": units / (ms * 1e-3), "unit": "vertex-substeps/s (cloth vertices + hair particles)",
+            "n_gpus": 1, "steps": args.steps, "warmup": W, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes)",
+            "config": {"workload": f"large cloth {side}x{side} (20 iterations, capsule, whole-GPU path) + {hair.name}",
+                       "cloth_vertices": n_cloth, "hair_particles": n_hair, "substeps": 4,
+                       "cloth_iterations": 20, "hair_iterations": hair.iterations,
+                       "cloth_ms_last_step": cloth_last_ms,
+                       "l2": "cloth state (~18 MB) fits in L2; hair state 2.1 M particles x 48 B exceeds it"},
+            "e2e": {"value": units / e2e_s, "unit": "vertex-substeps/s",
+                    "h2d_bytes_per_step": 184 + 236 + 64 * len(hair.sets[0].strands) + 236,
+                    "d2h_bytes_per_step": 12 * n_cloth + 40 * n_hair},
+            "roofline": None, "cpu_baseline": None, "gpu_launches": launches, "clocks": clk}
+    del keep_c, keep_s
+    ctx.close()
+    return line
+
+
 def bench_warm(args, local_rank):
     """Learned warm start vs the plain 20-iteration solver at equal residual (see the module
     docstring). Returns the JSON line."""
@@ -414,6 +498,10 @@ def main():
     if args.workload == "hair_groom":
         from physxcoopa_b200 import runtime as R
         return bench_hair(args, lambda: R.Context(local_rank))
+    if args.workload == "large_cloth_hair":
+        if rank == 0:
+            print(json.dumps(bench_large(args, local_rank)))
+        return 0
     if args.workload == "warm_start":
         if rank == 0:
             print(json.dumps(bench_warm(args, local_rank)))

@@ -562,12 +562,18 @@ typedef struct pxb_warm_start_desc {
     uint32_t warm_iterations;
     float residual_threshold;  /* used when thresholds is NULL */
     const float* thresholds;   /* optional, one per cloth of the step */
+    /* Fallback: 0 restarts the substep from the unmoved prediction with the plain iteration
+     * count (the plain solver's result exactly); 1 keeps iterating from the warm state,
+     * warm_iterations at a time, until the residual is within the threshold or the plain count
+     * is reached. */
+    uint32_t continue_iterations;
 } pxb_warm_start_desc;
 
 typedef struct pxb_cloth_warm_result {
     float residual;      /* max over the step's substeps of the residual it ended with */
-    uint32_t fallbacks;  /* substeps that fell back to the plain iteration count */
+    uint32_t fallbacks;  /* substeps whose residual after the warm iterations was too high */
     uint32_t substeps;
+    uint32_t extra_iterations; /* iterations run after the warm ones, over the step */
 } pxb_cloth_warm_result;
 
 pxb_status pxb_cloths_step_warm(pxb_context* ctx, const pxb_cloth_step_desc* step, const pxb_warm_start_desc* warm);

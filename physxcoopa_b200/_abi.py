@@ -156,10 +156,12 @@ class MlpTrainDesc(C.Structure):
 
 class WarmStartDesc(C.Structure):
     """pxb_warm_start_desc."""
-    _fields_ = [("warm_iterations", u32), ("residual_threshold", f32), ("thresholds", P)]
+    _fields_ = [("warm_iterations", u32), ("residual_threshold", f32), ("thresholds", P),
+                ("continue_iterations", u32)]
 
 
-WARM_RESULT = np.dtype([("residual", "<f4"), ("fallbacks", "<u4"), ("substeps", "<u4")])
+WARM_RESULT = np.dtype([("residual", "<f4"), ("fallbacks", "<u4"), ("substeps", "<u4"),
+                        ("extra_iterations", "<u4")])
 
 
 class ClothDesc(C.Structure):

@@ -465,6 +465,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     uint32_t stage_phase = 0;  // parity of the staging barrier's last completed phase
     float w_resid = 0.0f;  // max residual over the step's substeps
     int w_fallbacks = 0;
+    int w_extra = 0;       // iterations run after the warm ones
 
     const int steps = sP.steps;
     float4* __restrict__ gvel = sC.vel;
@@ -712,13 +713,28 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             iterate(net ? warm_iters : sP.iters);
             float r = stretch_residual();
             if (net && r > W.tau) {
-                // fallback: restart from the unmoved prediction with the plain iteration count
-                for (int l = tid; l < n_local; l += T) pos[l] = gpos[base + l];
-                for (int i = tid; i < sC.rank[rank].n_lam; i += T) U[i] = 0.0f;
-                cluster_or_block_sync<CL>();
-                iterate(sP.iters);
-                r = stretch_residual();
                 ++w_fallbacks;
+                if (W.continue_iters) {
+                    // keep iterating from the warm state, warm_iters at a time, until the
+                    // residual is within the threshold or the plain count is reached (the
+                    // residual is the same on every rank, so every rank loops alike)
+                    int done = warm_iters;
+                    while (r > W.tau && done < sP.iters) {
+                        const int k = warm_iters < sP.iters - done ? warm_iters : sP.iters - done;
+                        iterate(k);
+                        done += k;
+                        w_extra += k;
+                        r = stretch_residual();
+                    }
+                } else {
+                    // restart from the unmoved prediction with the plain iteration count
+                    for (int l = tid; l < n_local; l += T) pos[l] = gpos[base + l];
+                    for (int i = tid; i < sC.rank[rank].n_lam; i += T) U[i] = 0.0f;
+                    cluster_or_block_sync<CL>();
+                    iterate(sP.iters);
+                    w_extra += sP.iters;
+                    r = stretch_residual();
+                }
             }
             w_resid = fmaxf(w_resid, r);
             if (rec) {
@@ -874,6 +890,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             wr->residual = w_resid;
             wr->fallbacks = w_fallbacks;
             wr->substeps = sP.steps;
+            wr->extra_iterations = w_extra;
         }
         PxbFrameResult* out = &results[slot];
         for (int k = 0; k < 3; ++k) { out->bounds_min[k] = r[k]; out->bounds_max[k] = r[k + 3]; }

@@ -99,13 +99,15 @@ struct PxbWarmStep {
     float* rec_x;           // [rows][24] features of every layout slot
     float* rec_y;           // [rows][4] displacement made by the plain iterations, free flag
     int64_t rec_row0;       // this cloth's first row
+    int32_t continue_iters; // fallback: 0 restarts with the plain count, 1 keeps iterating
+    int32_t pad0;
 };
 
 struct PxbWarmResult {
     float residual;         // max over the step's substeps of the final residual
     int32_t fallbacks;      // substeps that fell back to the plain iteration count
     int32_t substeps;
-    int32_t pad;
+    int32_t extra_iterations;  // iterations beyond warm_iters, summed over the substeps
 };
 
 // One anchor target pair as the device keeps it (ClothAnchor::prev_world_position /

@@ -961,6 +961,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
             w.rec_x = warm->rec_x;
             w.rec_y = warm->rec_y;
             w.rec_row0 = warm->rec_row0 ? warm->rec_row0[k] : 0;
+            w.continue_iters = warm->continue_iters;
         }
         // Cloth::time advances by hs per substep (cloth_solver.h:453), mirrored on the host.
         for (uint32_t q = 0; q < steps; ++q) e.time += hs;

@@ -157,6 +157,7 @@ struct pxb_context {
         float* rec_x = nullptr;           // device rows, cloth k from rec_row0[k]
         float* rec_y = nullptr;
         const int64_t* rec_row0 = nullptr;
+        int continue_iters = 0;
     };
     pxb_status step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg* warm = nullptr);
     DevBuf d_wresults, d_rec, d_grid;

@@ -240,6 +240,7 @@ pxb_status pxb_cloths_step_warm(pxb_context* ctx, const pxb_cloth_step_desc* ste
     cfg.warm_iters = static_cast<int>(warm->warm_iterations);
     cfg.tau = warm->residual_threshold;
     cfg.taus = warm->thresholds;
+    cfg.continue_iters = warm->continue_iterations ? 1 : 0;
     return ctx->step_cloths(step, &cfg);
 }
 
@@ -254,6 +255,7 @@ pxb_status pxb_cloths_read_warm_results(pxb_context* ctx, const uint64_t* cloths
         out[k].residual = e->warm_result.residual;
         out[k].fallbacks = static_cast<uint32_t>(e->warm_result.fallbacks);
         out[k].substeps = static_cast<uint32_t>(e->warm_result.substeps);
+        out[k].extra_iterations = static_cast<uint32_t>(e->warm_result.extra_iterations);
     }
     return PXB_OK;
 }

@@ -317,15 +317,18 @@ class Context:
         return loss.value, g.as_numpy()
 
     def step_warm(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
-                  iterations=10, h=1.0 / 60.0, warm_iterations=4, threshold=1e-4, thresholds=None):
+                  iterations=10, h=1.0 / 60.0, warm_iterations=4, threshold=1e-4, thresholds=None,
+                  continue_iterations=False):
         """One warm-started step (pxb_cloths_step_warm); warm_iterations=0 is the plain solve
         with its residual measured."""
         d, keep = self.make_step(ids, colliders, gravity, sources, substeps, iterations, h)
-        return self.step_warm_desc(d, warm_iterations, threshold, thresholds, keep)
+        return self.step_warm_desc(d, warm_iterations, threshold, thresholds, keep, continue_iterations)
 
-    def step_warm_desc(self, d, warm_iterations=4, threshold=1e-4, thresholds=None, keep=None):
+    def step_warm_desc(self, d, warm_iterations=4, threshold=1e-4, thresholds=None, keep=None,
+                       continue_iterations=False):
         w = A.WarmStartDesc()
         w.warm_iterations = warm_iterations
+        w.continue_iterations = 1 if continue_iterations else 0
         w.residual_threshold = threshold
         th = None if thresholds is None else np.ascontiguousarray(thresholds, np.float32)
         w.thresholds = A.ptr(th)

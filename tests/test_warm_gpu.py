@@ -5,6 +5,8 @@ the training-row recorder, held to exact properties against the plain solver:
   the reported residual is the max relative strain of the stretch constraints;
 * a network that outputs zero followed by N warm iterations equals N plain iterations;
 * a threshold below any residual falls back in every substep and equals the plain solve;
+* continuing after a zero network until the plain count equals the plain solve too (the
+  iterations resume where the warm ones stopped, lambdas included);
 * recorded features are the quantities the solver sees (velocity at the start of the substep,
   predicted displacement), recorded rows are the free particles.
 """
@@ -150,3 +152,13 @@ def test_recorded_rows_are_what_the_solver_sees(ctx):
             ctx.remove_cloth(i)
     plain, _ = run(ctx, cloths, cols, 1, lambda ids: ctx.step(ids, cols))
     assert same(after, plain)
+
+
+def test_continued_iterations_after_a_zero_network_equal_the_plain_solve(ctx):
+    cloths, cols = batch(seed=13)
+    ctx.set_mlp(random_net(np.random.default_rng(4), zero_out=True))
+    plain, _ = run(ctx, cloths, cols, 3, lambda ids: ctx.step(ids, cols, iterations=12))
+    warm, res = run(ctx, cloths, cols, 3, lambda ids: ctx.step_warm(ids, cols, iterations=12, warm_iterations=4,
+                                                                      threshold=-1.0, continue_iterations=True))
+    assert same(plain, warm)
+    assert np.all(res["fallbacks"] == res["substeps"]) and np.all(res["extra_iterations"] == 8 * res["substeps"])

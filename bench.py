@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--cloths", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--graph", action="store_true",
+                    help="step through the captured CUDA graph (pxb_cloths_step_graph) instead of pxb_cloths_step")
     ap.add_argument("--variant", type=int, default=None,
                     help="fix the kernel variant (0/1/2) instead of autotuning")
     return ap.parse_args()
@@ -541,8 +543,9 @@ def main():
     else:
         ctx.set_cloth_variant(args.variant)
         tune = {"chosen_variant": args.variant, "fixed": True}
+    step = ctx.step_graph_desc if args.graph else ctx.step_desc
     for _ in range(max(args.warmup, 3)):
-        ctx.step_desc(d)
+        step(d)
     ctx.synchronize()
     smem_bw = ctx.measure_smem_bandwidth()
     if dist:
@@ -565,7 +568,7 @@ def main():
         t_start.record(stream)
         for k in range(args.steps):
             ev[k][0].record(stream)
-            ctx.step_desc(d)
+            step(d)
             ev[k][1].record(stream)
         t_end.record(stream)
     ctx.synchronize()
@@ -620,7 +623,7 @@ def main():
     with torch.cuda.stream(stream):
         e0.record(stream)
         for _ in range(e2e_steps):
-            ctx.step_desc(d)
+            step(d)
             ctx.read_positions(ids_np, out_np)
             ctx.lib.pxb_cloths_read_results(ctx.h, A.ptr(ids_np), len(ids_np), A.ptr(res_out))
         e1.record(stream)
@@ -643,7 +646,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scenes)",
             "config": dict(workload_config(args, sc), parallelism=f"independent cloth batches x{world}",
-                           autotune=tune),
+                           autotune=tune, launch="pxb_cloths_step_graph (captured CUDA graph)" if args.graph
+                           else "pxb_cloths_step"),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
             "roofline": {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -334,6 +334,14 @@ typedef struct pxb_cloth_frame_result {
  * its mean particle position when it has gravity sources (PhysicsWorld::gravity_at(cloth_centre_),
  * world.h:1833, 2048-2076). Enqueued on the context stream; returns before completion. */
 pxb_status pxb_cloths_step(pxb_context* ctx, const pxb_cloth_step_desc* step);
+/* The same step replayed from a CUDA graph. The host prepares the step's inputs as
+ * pxb_cloths_step does; the upload and every launch of the step (side-stream groups included)
+ * are captured once and replayed while the step's shape stays the same (same cloths in the same
+ * order, same collider and gravity-source counts, same kernel variant, no cloth added, removed
+ * or re-parameterised, no internal buffer regrown). A new shape runs eagerly on its first call
+ * and is captured on its second. Results are identical to pxb_cloths_step's. Must not be called
+ * while the context stream is being captured by the caller. No counterpart in the reference. */
+pxb_status pxb_cloths_step_graph(pxb_context* ctx, const pxb_cloth_step_desc* step);
 /* Copies the last step's per-cloth results to host memory (synchronizes the stream). */
 pxb_status pxb_cloths_read_results(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
                                    pxb_cloth_frame_result* out);

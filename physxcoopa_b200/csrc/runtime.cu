@@ -446,6 +446,7 @@ static void layout_ranks(ClothEntry& e) {
 void pxb_context::refresh_layout(ClothEntry& e) {
     layout_ranks(e);
     registry_dirty = true;
+    ++registry_epoch;
 }
 
 pxb_status pxb_context::upload_segments(ClothEntry& e) {
@@ -741,6 +742,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.alive = true;
     cloths[index] = std::move(e);
     registry_dirty = true;
+    ++registry_epoch;
     *id_out = (static_cast<uint64_t>(cloths[index].generation) << 32) | index;
     return PXB_OK;
 }
@@ -824,7 +826,16 @@ static pxb_status check_colliders(pxb_context* ctx, const pxb_collider* c, uint3
     return PXB_OK;
 }
 
-pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg* warm) {
+void pxb_context::drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+    graph_key.clear();
+    graph_kernels = 0;
+}
+
+pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg* warm, bool use_graph) {
     if (!sd || (sd->n_cloths && !sd->cloths)) return fail(PXB_ERR_INVALID_ARGUMENT, "null step");
     const uint32_t n = sd->n_cloths;
     if (n == 0) return PXB_OK;
@@ -875,7 +886,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     if (pxb_status s = grow_pinned(total)) return s;
     if (pxb_status s = grow(d_stage, total, "step staging")) return s;
     if (pxb_status s = grow(d_results, sizeof(PxbFrameResult) * n, "results")) return s;
-    cudaEventSynchronize(staged);  // the previous step's upload has left the pinned buffer
+    if (pxb_status s = cuda(cudaEventSynchronize(staged), "wait for the previous upload")) return s;
     char* hb = static_cast<char*>(pinned);
     auto* hs_steps = reinterpret_cast<PxbClothStep*>(hb);
     auto* hs_cols = reinterpret_cast<PxbDevCollider*>(hb + o_cols);
@@ -970,18 +981,28 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         for (pxb_anchor& a : e.anchors) std::memcpy(a.prev_world_position, a.world_position, 12);
     }
     char* db = static_cast<char*>(d_stage.p);
+    uint32_t n_plain = n;
+    while (n_plain > 0 && ents[perm[n_plain - 1]]->grid) --n_plain;
+    if (n_plain < n)
+        if (pxb_status s = grow(d_grid, sizeof(PxbGridSync) * (n - n_plain), "grid barriers")) return s;
+    // Everything from the upload to the join is one enqueue, which a graph step captures once and
+    // replays (the upload node copies the pinned staging filled above at each replay).
+    int enqueued = 0;
+    bool capturing = false;
+    auto enqueue = [&]() -> pxb_status {
     if (pxb_status s = cuda(cudaMemcpyAsync(db, hb, total, cudaMemcpyHostToDevice, stream), "upload step")) return s;
-    cudaEventRecord(staged, stream);
+    // The pinned staging is free again once this upload ran. A captured graph cannot carry that
+    // event (an event recorded inside a capture cannot be waited on from the host); the graph
+    // path records it after the whole replay instead.
+    if (!capturing)
+        if (pxb_status s = cuda(cudaEventRecord(staged, stream), "record upload")) return s;
     // Launch groups: (cluster size, CTAs per SM). With several, each goes to a side stream so
     // they share the SMs instead of running one after another (a group of small cloths alone
     // leaves most of the device idle).
     // Whole-GPU cloths first, one cooperative launch each on the context stream: the side
     // streams below fork after them, so nothing else holds SMs while they run.
-    uint32_t n_plain = n;
-    while (n_plain > 0 && ents[perm[n_plain - 1]]->grid) --n_plain;
     if (n_plain < n) {
         const size_t gbytes = sizeof(PxbGridSync) * (n - n_plain);
-        if (pxb_status s = grow(d_grid, gbytes, "grid barriers")) return s;
         if (pxb_status s = cuda(cudaMemsetAsync(d_grid.p, 0, gbytes, stream), "zero grid barriers")) return s;
         for (uint32_t slot = n_plain; slot < n; ++slot) {
             cudaError_t le = launch_cloth_grid(static_cast<const PxbClothDev*>(d_registry.p),
@@ -993,7 +1014,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                                                static_cast<PxbGridSync*>(d_grid.p) + (slot - n_plain),
                                                static_cast<int>(slot), n_sms, stream);
             if (le != cudaSuccess) return cuda(le, "launch whole-GPU cloth");
-            ++launches;
+            ++enqueued;
         }
     }
     struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; };
@@ -1033,12 +1054,58 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                                            warm && warm->warm_iters > 0 ? static_cast<const unsigned char*>(d_mlp.p) : nullptr,
                                            warm ? static_cast<PxbWarmResult*>(d_wresults.p) + G.g0 : nullptr);
         if (le != cudaSuccess) return cuda(le, "launch cloth_step");
-        ++launches;
+        ++enqueued;
     }
     if (fan_out) {
         for (int k = 0; k < std::min<int>(kSideStreams, static_cast<int>(groups.size())); ++k) {
             if (pxb_status s = cuda(cudaEventRecord(join[k], side[k]), "join")) return s;
             if (pxb_status s = cuda(cudaStreamWaitEvent(stream, join[k], 0), "join wait")) return s;
+        }
+    }
+    return PXB_OK;
+    };
+    if (!use_graph || warm) {
+        if (pxb_status s = enqueue()) return s;
+        launches += static_cast<uint64_t>(enqueued);
+    } else {
+        // The replayed graph is valid while the launch sequence and every buffer it names are the
+        // same: same cloths in the same order, same collider / source counts and variant, no
+        // buffer regrown. A new key runs eagerly once, then is captured on its second use.
+        std::vector<uint64_t> key(sd->cloths, sd->cloths + n);
+        for (uint64_t v : {uint64_t(n_col), uint64_t(n_src), uint64_t(cloth_variant), uint64_t(total),
+                           uint64_t(reinterpret_cast<uintptr_t>(d_stage.p)), uint64_t(reinterpret_cast<uintptr_t>(d_results.p)),
+                           uint64_t(reinterpret_cast<uintptr_t>(d_registry.p)), uint64_t(reinterpret_cast<uintptr_t>(pinned)),
+                           uint64_t(reinterpret_cast<uintptr_t>(d_grid.p)), registry_epoch})
+            key.push_back(v);
+        if (graph_exec && key == graph_key) {
+            if (pxb_status s = cuda(cudaGraphLaunch(graph_exec, stream), "launch step graph")) return s;
+            if (pxb_status s = cuda(cudaEventRecord(staged, stream), "record step graph")) return s;
+            launches += static_cast<uint64_t>(graph_kernels);
+        } else if (key == graph_pending) {
+            drop_graph();
+            if (pxb_status s = cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture"))
+                return s;
+            capturing = true;
+            const pxb_status es = enqueue();
+            capturing = false;
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(stream, &g);
+            if (es) {
+                if (g) cudaGraphDestroy(g);
+                return es;
+            }
+            if (ce != cudaSuccess) return cuda(ce, "end capture");
+            graph = g;
+            if (pxb_status s = cuda(cudaGraphInstantiate(&graph_exec, graph, 0), "instantiate step graph")) return s;
+            graph_key = key;
+            graph_kernels = enqueued;
+            if (pxb_status s = cuda(cudaGraphLaunch(graph_exec, stream), "launch step graph")) return s;
+            if (pxb_status s = cuda(cudaEventRecord(staged, stream), "record step graph")) return s;
+            launches += static_cast<uint64_t>(enqueued);
+        } else {
+            if (pxb_status s = enqueue()) return s;
+            launches += static_cast<uint64_t>(enqueued);
+            graph_pending = key;
         }
     }
     last_step.resize(n);
@@ -1196,6 +1263,7 @@ pxb_status pxb_cloth_remove(pxb_context* ctx, uint64_t id) {
     e->generation = gen;
     e->alive = false;
     ctx->registry_dirty = true;
+    ++ctx->registry_epoch;
     ctx->results_fresh = false;
     ctx->last_step.clear();
     return PXB_OK;
@@ -1314,6 +1382,11 @@ pxb_status pxb_cloth_read_time(pxb_context* ctx, uint64_t id, float* time_out) {
 pxb_status pxb_cloths_step(pxb_context* ctx, const pxb_cloth_step_desc* step) {
     if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
     return ctx->step_cloths(step);
+}
+
+pxb_status pxb_cloths_step_graph(pxb_context* ctx, const pxb_cloth_step_desc* step) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    return ctx->step_cloths(step, nullptr, true);
 }
 
 pxb_status pxb_cloths_read_results(pxb_context* ctx, const uint64_t* cloths, uint32_t n,

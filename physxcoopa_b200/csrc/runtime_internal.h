@@ -102,6 +102,7 @@ struct pxb_context {
     uint64_t launches = 0;
     std::vector<ClothEntry> cloths;
     bool registry_dirty = true;
+    uint64_t registry_epoch = 0;  // advances with every change to the registry or a cloth's layout
     DevBuf d_registry, d_stage, d_results, d_gather, d_gather_meta, d_scratch;
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
@@ -119,6 +120,8 @@ struct pxb_context {
     DevBuf d_tune;          // cloth state saved across an autotune
 
     ~pxb_context() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
         for (ClothEntry& e : cloths)
             if (e.alive && e.dmem) cudaFree(e.dmem);
         for (StrandEntry& e : strand_sets)
@@ -159,7 +162,13 @@ struct pxb_context {
         const int64_t* rec_row0 = nullptr;
         int continue_iters = 0;
     };
-    pxb_status step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg* warm = nullptr);
+    pxb_status step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg* warm = nullptr, bool use_graph = false);
+    // the captured step (pxb_cloths_step_graph)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<uint64_t> graph_key, graph_pending;
+    int graph_kernels = 0;
+    void drop_graph();
     DevBuf d_wresults, d_rec, d_grid;
     bool warm_fresh = false;
     bool last_step_warm = false;

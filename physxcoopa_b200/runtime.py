@@ -53,6 +53,7 @@ SIGNATURES = {
     "pxb_cloth_read_anchors": ([P, u64, P, u32], C.c_int),
     "pxb_cloth_read_time": ([P, u64, f32p], C.c_int),
     "pxb_cloths_step": ([P, C.POINTER(A.ClothStepDesc)], C.c_int),
+    "pxb_cloths_step_graph": ([P, C.POINTER(A.ClothStepDesc)], C.c_int),
     "pxb_cloths_read_results": ([P, P, u32, P], C.c_int),
     "pxb_cloths_read_positions": ([P, P, u32, P, C.c_size_t], C.c_int),
     "pxb_solve_cloth_host": ([P, C.POINTER(A.ClothDesc), P, P, P, P, P, u32, f32p, u32, u32, f32,
@@ -427,6 +428,10 @@ class Context:
 
     def step_desc(self, d):
         self._check(self.lib.pxb_cloths_step(self.h, C.byref(d)), "cloths_step")
+
+    def step_graph_desc(self, d):
+        """pxb_cloths_step_graph: the step replayed from a captured CUDA graph."""
+        self._check(self.lib.pxb_cloths_step_graph(self.h, C.byref(d)), "cloths_step_graph")
 
     def step(self, ids, colliders=None, gravity=(0, 0, -9.81), sources=None, substeps=4,
              iterations=10, h=1.0 / 60.0):

@@ -517,3 +517,36 @@ def test_batch_with_a_whole_gpu_cloth(ctx):
         assert np.array_equal(res[k]["bounds_max"], o.bounds[3:])
     for cid in ids:
         ctx.remove_cloth(cid)
+
+
+def test_graph_steps_equal_eager_steps(ctx):
+    """pxb_cloths_step_graph: captured on the second call of a shape, replayed after; results
+    identical to pxb_cloths_step across cluster sizes and the whole-GPU path, recaptured when the
+    shape changes (a cloth removed, another list)."""
+    cloths = [clustered_sheet(c, c, seed=30 + k) for k, c in enumerate((12, 40, 64, 90, 130, 185))]
+    cols = [collider_array([sphere(0.3, (0.02 * k, 0, 0.4))]) for k in range(len(cloths))]
+    srcs = [gravity_sources([((0.5, 0.2, -2.0), 9.81, 1.0, 10.0)]) if k % 2 else None for k in range(len(cloths))]
+
+    def trajectory(use_graph, steps=5):
+        ids = [ctx.add_cloth(c) for c in cloths]
+        d, keep = ctx.make_step(ids, cols, sources=srcs)
+        out = []
+        for _ in range(steps):
+            (ctx.step_graph_desc if use_graph else ctx.step_desc)(d)
+            out.append([ctx.read_particles(i, len(c.particles)).tobytes() for i, c in zip(ids, cloths)])
+        ctx.remove_cloth(ids[0])
+        d2, keep2 = ctx.make_step(ids[1:], cols[1:], sources=srcs[1:])
+        for _ in range(3):
+            (ctx.step_graph_desc if use_graph else ctx.step_desc)(d2)
+        out.append([ctx.read_particles(i, len(c.particles)).tobytes() for i, c in zip(ids[1:], cloths[1:])])
+        res = ctx.read_results(ids[1:]).tobytes()
+        flat = np.zeros(3 * sum(len(c.particles) for c in cloths[1:]), np.float32)
+        ctx.read_positions(ids[1:], flat)  # a launch after replays: no error left behind by them
+        for i in ids[1:]:
+            ctx.remove_cloth(i)
+        del keep, keep2
+        return out, res, flat.tobytes()
+
+    eager = trajectory(False)
+    graph = trajectory(True)
+    assert graph == eager

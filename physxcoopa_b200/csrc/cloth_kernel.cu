@@ -136,10 +136,12 @@ __device__ __forceinline__ float warp_max(float v) {
 
 // Items of one colour share no particle, so with registers to spare (512-thread blocks) a
 // thread takes two per pass and loads both before storing either: two independent dependency
-// chains (square root, divisions) in flight per thread. The reference's early returns (both endpoints pinned; coincident endpoints) become a
-// predicate on the stores, with its comparisons kept as written (a NaN weight is not skipped).
-// Padding slots at row ends and a second item past the segment read item 0's slots and store
-// nothing. h0 = {count_pad, shift, per_row, a_base}, h1 = {row_stride, d, rest_base, lam_base}.
+// chains (square root, divisions) in flight per thread. The reference's early returns (both
+// endpoints pinned; coincident endpoints) become a predicate on the stores, with its comparisons
+// kept as written (a NaN weight is not skipped). An item's row is a multiply-high by the
+// segment's magic reciprocal (exact for every item index used), so segments carry no padding;
+// a second item past the segment reads item 0's slots and stores nothing.
+// h0 = {count, magic, per_row, a_base}, h1 = {row_stride, d, rest_base, lam_base}.
 struct PairItem {
     float4* pa;
     float4* pb;
@@ -148,15 +150,18 @@ struct PairItem {
     bool live;
 };
 
+__device__ __forceinline__ int seg_row(int i, uint32_t magic) {
+    return magic ? static_cast<int>(__umulhi(static_cast<uint32_t>(i), magic)) : i;
+}
+
 template <int CL, bool kLam>
 __device__ __forceinline__ void load_item(PairItem& it, float4* pos, float4* pos_next, const float* rest,
-                                          const float* lamv, int n_local, int i, int count_pad, int shift,
+                                          const float* lamv, int n_local, int i, int count, uint32_t magic,
                                           int per_row, int a_base, int row_stride, int d) {
-    const int mask = (1 << shift) - 1;
-    const int k = i & mask;
-    it.live = i < count_pad && k < per_row;
+    it.live = i < count;
     const int ii = it.live ? i : 0;
-    const int la = it.live ? a_base + (i >> shift) * row_stride + k : a_base;
+    const int row = seg_row(ii, magic);
+    const int la = a_base + row * row_stride + (ii - row * per_row);
     const int lb = la + d;
     it.pa = &pos[la];
     it.pb = (CL == 1 || lb < n_local) ? &pos[lb] : &pos_next[lb - n_local];
@@ -194,22 +199,23 @@ template <int CL, bool kLam, int kItems>
 __device__ __forceinline__ void project_segment(float4* __restrict__ pos, float4* __restrict__ pos_next,
                                                 const float* __restrict__ rest, float* __restrict__ lamv,
                                                 int n_local, int4 h0, int4 h1, float alpha, int tid, int T) {
-    const int count_pad = h0.x, shift = h0.y, per_row = h0.z, a_base = h0.w;
+    const int count = h0.x, per_row = h0.z, a_base = h0.w;
+    const uint32_t magic = static_cast<uint32_t>(h0.y);
     const int row_stride = h1.x, d = h1.y;
     if constexpr (kItems == 2) {
-        for (int i = tid; i < count_pad; i += 2 * T) {
+        for (int i = tid; i < count; i += 2 * T) {
             PairItem x, y;
-            load_item<CL, kLam>(x, pos, pos_next, rest, lamv, n_local, i, count_pad, shift, per_row, a_base,
+            load_item<CL, kLam>(x, pos, pos_next, rest, lamv, n_local, i, count, magic, per_row, a_base,
                                 row_stride, d);
-            load_item<CL, kLam>(y, pos, pos_next, rest, lamv, n_local, i + T, count_pad, shift, per_row,
+            load_item<CL, kLam>(y, pos, pos_next, rest, lamv, n_local, i + T, count, magic, per_row,
                                 a_base, row_stride, d);
             project_item<kLam>(x, lamv, i, alpha);
             project_item<kLam>(y, lamv, i + T, alpha);
         }
     } else {
-        for (int i = tid; i < count_pad; i += T) {
+        for (int i = tid; i < count; i += T) {
             PairItem x;
-            load_item<CL, kLam>(x, pos, pos_next, rest, lamv, n_local, i, count_pad, shift, per_row, a_base,
+            load_item<CL, kLam>(x, pos, pos_next, rest, lamv, n_local, i, count, magic, per_row, a_base,
                                 row_stride, d);
             project_item<kLam>(x, lamv, i, alpha);
         }
@@ -427,14 +433,13 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             const int se = sC.rank[rank].colour_seg[c + 1];
             for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
                 const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
-                const int count_pad = h0.x, shift = h0.y, per_row = h0.z, a_base = h0.w;
+                const int count = h0.x, per_row = h0.z, a_base = h0.w;
+                const uint32_t magic = static_cast<uint32_t>(h0.y);
                 const int row_stride = h1.x, d = h1.y;
                 const float* rr = rest + h1.z;
-                const int mask = (1 << shift) - 1;
-                for (int i = tid; i < count_pad; i += T) {
-                    const int k = i & mask;
-                    if (k >= per_row) continue;
-                    const int la = a_base + (i >> shift) * row_stride + k, lb = la + d;
+                for (int i = tid; i < count; i += T) {
+                    const int row = seg_row(i, magic);
+                    const int la = a_base + row * row_stride + (i - row * per_row), lb = la + d;
                     const float4 pa = pos[la];
                     const float4 pb = (CL == 1 || lb < n_local) ? pos[lb] : pos_next[lb - n_local];
                     const float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;

@@ -10,14 +10,13 @@
 // (cloth_builder.h:128-194) reads and writes CONTIGUOUS float4 runs, so a warp's shared-memory
 // accesses are bank-conflict free for every colour.
 //
-// A colour is a list of affine segments. Rows of a segment are padded to a power of two,
-// row_pad = 1 << shift; item i of a segment is row r = i >> shift, column k = i & (row_pad - 1),
-// live when k < per_row, and joins layout slots
+// A colour is a list of affine segments. Item i of a segment is row r = i / per_row (computed
+// as umulhi(i, magic) with magic = ceil(2^32 / per_row), checked exact on the host for every
+// item), column k = i - r * per_row, and joins layout slots
 //   la = a_base + r * row_stride + k,  lb = la + d
 // reading its rest length from slot rest_base + i and, when the colour is compliant, its lambda
-// from slot lam_base + i (padding slots are never read). The host derives the segments from the
-// reference's own constraint lists and refuses the fast path unless they reproduce those lists
-// exactly.
+// from slot lam_base + i. The host derives the segments from the reference's own constraint
+// lists and refuses the fast path unless they reproduce those lists exactly.
 #ifndef PXB_INTERNAL_H
 #define PXB_INTERNAL_H
 
@@ -36,9 +35,9 @@
 
 // 16-byte aligned: the kernel reads a descriptor as two 16-byte words.
 struct alignas(16) PxbSeg {
-    int32_t count_pad;  // items including row padding (rows * row_pad)
-    int32_t shift;      // log2(row_pad)
-    int32_t per_row;    // live items per row
+    int32_t count;      // items (rows * per_row)
+    uint32_t magic;     // ceil(2^32 / per_row): row of item i = umulhi(i, magic); 0 when per_row is 1
+    int32_t per_row;    // items per row
     int32_t a_base;     // layout slot of item 0's `a`
     int32_t row_stride; // layout distance between rows
     int32_t d;          // lb - la

@@ -334,26 +334,24 @@ bool build_ranks(ClothEntry& e, const std::vector<ColourSpec>& cs, const std::ve
                 const int r_lo = Y0 <= y0 ? 0 : (Y0 - y0 + step - 1) / step;
                 const int r_hi = Y1 <= y0 ? 0 : std::min(nrows, (Y1 - y0 + step - 1) / step);
                 if (r_hi <= r_lo) continue;
-                int shift = 0;
-                while ((1 << shift) < h.per_row) ++shift;
-                const int row_pad = 1 << shift;
                 PxbSeg g{};
-                g.count_pad = (r_hi - r_lo) * row_pad;
-                g.shift = shift;
+                g.count = (r_hi - r_lo) * h.per_row;
+                g.magic = h.per_row > 1 ? static_cast<uint32_t>(((1ull << 32) + h.per_row - 1) / h.per_row) : 0u;
                 g.per_row = h.per_row;
+                // the device's row of item i is umulhi(i, magic): check it for every item
+                for (int i = 0; i < g.count; ++i) {
+                    const int row = g.magic ? static_cast<int>((static_cast<uint64_t>(i) * g.magic) >> 32) : i;
+                    if (row != i / h.per_row) return false;
+                }
                 g.a_base = h.a_base + r_lo * h.row_stride - Y0 * S;
                 g.row_stride = h.row_stride;
                 g.d = h.d;
                 g.rest_base = rest;
                 g.lam_base = -1;
-                for (int i = 0; i < g.count_pad; ++i) {
-                    const int rr = i >> shift, k = i & (row_pad - 1);
-                    padded_ref.push_back(k < h.per_row
-                                             ? refs[seg_ref_off[c][hi] + static_cast<size_t>(r_lo + rr) * h.per_row + k]
-                                             : -1);
-                }
-                rest += g.count_pad;
-                items += g.count_pad;
+                for (int i = 0; i < g.count; ++i)
+                    padded_ref.push_back(refs[seg_ref_off[c][hi] + static_cast<size_t>(r_lo) * h.per_row + i]);
+                rest += g.count;
+                items += g.count;
                 e.segs.push_back(g);
             }
             max_colour_items = std::max(max_colour_items, items);
@@ -380,15 +378,10 @@ bool verify_ranks(const ClothEntry& e, const pxb_cloth_desc* d) {
         const int base = rk.row0 * e.S;
         for (int sg = rk.seg_begin; sg < rk.seg_begin + rk.colour_seg[e.n_colours]; ++sg) {
             const PxbSeg& g = e.segs[sg];
-            const int mask = (1 << g.shift) - 1;
-            for (int i = 0; i < g.count_pad; ++i) {
-                const int k = i & mask;
+            for (int i = 0; i < g.count; ++i) {
                 const int32_t ref = e.rest_ref[rk.rest_off + g.rest_base + i];
-                if (k >= g.per_row) {
-                    if (ref != -1) return false;
-                    continue;
-                }
-                const int la = g.a_base + (i >> g.shift) * g.row_stride + k, lb = la + g.d;
+                const int row = i / g.per_row, k = i - row * g.per_row;
+                const int la = g.a_base + row * g.row_stride + k, lb = la + g.d;
                 if (la < 0 || la >= n_local || lb < 0 || lb >= n_local + n_next || ref < 0) return false;
                 const pxb_constraint& kc = ref < static_cast<int32_t>(d->n_stretch) ? d->stretch[ref]
                                                                                     : d->bend[ref - d->n_stretch];
@@ -416,7 +409,7 @@ static void layout_ranks(ClothEntry& e) {
             const bool has_lam = colour_compliance(e, c) != 0.0f;
             for (int sg = rk.seg_begin + rk.colour_seg[c]; sg < rk.seg_begin + rk.colour_seg[c + 1]; ++sg) {
                 e.segs[sg].lam_base = has_lam ? lam : -1;
-                if (has_lam) lam += e.segs[sg].count_pad;
+                if (has_lam) lam += e.segs[sg].count;
             }
         }
         rk.n_lam = lam;
@@ -1338,9 +1331,9 @@ pxb_status pxb_cloth_read_lambdas(pxb_context* ctx, uint64_t id, float* stretch_
         for (int sg = rk.seg_begin; sg < rk.seg_begin + rk.colour_seg[e->n_colours]; ++sg) {
             const PxbSeg& g = e->segs[sg];
             if (g.lam_base < 0) continue;
-            for (int i = 0; i < g.count_pad; ++i) {
+            for (int i = 0; i < g.count; ++i) {
                 const int32_t r = e->rest_ref[rk.rest_off + g.rest_base + i];
-                if (r < 0) continue;  // row padding
+                if (r < 0) continue;
                 const float v = lam[rk.lam_off + g.lam_base + i];
                 if (r < static_cast<int32_t>(e->n_stretch)) { if (stretch_out) stretch_out[r] = v; }
                 else if (bend_out) bend_out[r - e->n_stretch] = v;

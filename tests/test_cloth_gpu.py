@@ -388,13 +388,13 @@ def clustered_sheet(cols, rows, seed, pins="corners", params=None):
 
 
 CLUSTERED = {
-    # (columns, rows); the planner gives these 2, 4, 8, 4 and 2 CTAs
+    # (columns, rows); the planner gives these 2, 4, 8, 2 and 2 CTAs
     "c2_65": dict(shape=(65, 65), cols=[sphere(0.5, (0.1, 0, 0.4))]),
-    "c4_80_sources": dict(shape=(80, 80), cols=[capsule(0.2, 0.5, (0, 0, 0.5), axis=0)],
+    "c4_100_sources": dict(shape=(100, 100), cols=[capsule(0.2, 0.5, (0, 0, 0.5), axis=0)],
                           sources=[((0.5, -0.3, -2.0), 9.81, 1.0, 10.0)]),
     "c8_128_edge": dict(shape=(128, 128), pins="edge",
                         cols=[box((0.6, 0.5, 0.4), (0.2, 0.1, 0.3), (0.0, 0.3826834, 0.0, 0.9238795))]),
-    "c4_tall_40x180": dict(shape=(40, 180), cols=[sphere(0.6, (0, 0.5, 0.2))]),
+    "c2_tall_40x180": dict(shape=(40, 180), cols=[sphere(0.6, (0, 0.5, 0.2))]),
     "c2_wind_97x61": dict(shape=(97, 61), params=dict(wind=(0.5, 0.2, 0.0), wind_turbulence=0.5)),
 }
 
@@ -441,7 +441,7 @@ def compliant_mask(batches, compliance, n):
 def test_batch_of_every_cluster_size(ctx):
     """One step call over cloths of every cluster size: at least one launch per size, all equal
     to the oracle, positions gathered in the caller's order."""
-    shapes = [(20, 20), (128, 128), (64, 64), (65, 65), (90, 90), (16, 16), (72, 72)]
+    shapes = [(20, 20), (128, 128), (64, 64), (65, 65), (100, 100), (16, 16), (72, 72)]
     cloths = [clustered_sheet(c, r, seed=k) for k, (c, r) in enumerate(shapes)]
     sizes = {R.plan_cloth(c)["n_ranks"] for c in cloths}
     assert sizes == {1, 2, 4, 8}

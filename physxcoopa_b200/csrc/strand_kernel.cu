@@ -9,7 +9,8 @@
 //       the other endpoint with a shuffle and evaluate the same projection, each keeping its own
 //       endpoint -- bit-identical on both sides, so nothing is written back
 //   5   global shape toward the root-frame rest pose          (lane = particle)
-//   6   local shape, the reference's serial chain k = 1..n-2, warp-uniform
+//   6   local shape, the reference's serial chain k = 1..n-2: one thread walks each strand of
+//       the block over positions gathered in shared memory
 //   7   collider projection keeping the deepest contact       (lane = particle)
 //   8   velocities + positional friction                      (lane = particle)
 // Bounds and the largest speed of the whole set are reduced with warp shuffles and combined
@@ -95,10 +96,15 @@ __device__ __forceinline__ int fkey(float f) {
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 strand_step_kernel(PxbStrandDev D, PxbStrandStep P, const PxbDevCollider* __restrict__ colliders,
                    const pxb_gravity_source* __restrict__ sources) {
+    // local-shape chains run one thread per strand over this block's strands (shared memory)
+    __shared__ float4 s_chain[kWarpsPerBlock][32];
     const int lane = threadIdx.x & 31;
-    const int strand = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    if (strand >= D.n_strands) return;  // whole warp exits together
-    const int count = __ldg(&D.count[strand]);
+    const int warp = threadIdx.x >> 5;
+    const int strand_raw = blockIdx.x * kWarpsPerBlock + warp;
+    // warps past the last strand stay (with no particles) for the block-wide barriers
+    const bool valid = strand_raw < D.n_strands;
+    const int strand = valid ? strand_raw : 0;
+    const int count = valid ? __ldg(&D.count[strand]) : 0;
     const int slot = strand * 32 + lane;
     const bool live = lane < count;
 
@@ -135,7 +141,6 @@ strand_step_kernel(PxbStrandDev D, PxbStrandStep P, const PxbDevCollider* __rest
     f3 v = live ? xyz(D.vel[slot]) : mk(0, 0, 0);
     f3 prev = live ? xyz(D.prv[slot]) : mk(0, 0, 0);
     const f3 rest_local = live ? xyz(D.rest_local[slot]) : mk(0, 0, 0);
-    const f3 rest_offset = live ? xyz(D.rest_offset[slot]) : mk(0, 0, 0);
     const float rest_next = live ? __ldg(&D.rest[slot]) : 0.0f;   // constraint (lane, lane + 1)
     const float wshape = live ? __ldg(&D.wshape[slot]) : 0.0f;     // pow(1 - along, falloff)
     const float* rr = D.roots + 16 * static_cast<size_t>(strand);
@@ -225,23 +230,39 @@ strand_step_kernel(PxbStrandDev D, PxbStrandStep P, const PxbDevCollider* __rest
             }
         }
         // --- 6: local shape, the serial chain (strand_solver.h:241-272) -------------------
-        if (P.local_shape_on && count >= 3) {
-            for (int k = 1; k + 1 < count; ++k) {
-                const f3 pp = shfl3(p, k - 1), pc = shfl3(p, k), pn = shfl3(p, k + 1);
-                const f3 ro_c = shfl3(rest_offset, k), ro_n = shfl3(rest_offset, k + 1);
-                const float wc = __shfl_sync(0xffffffffu, w, k), wn = __shfl_sync(0xffffffffu, w, k + 1);
-                const f3 live_prev = sub(pc, pp);
-                const float rest_len = len(ro_c);
-                const float live_len = len(live_prev);
-                if (rest_len <= 1e-8f || live_len <= 1e-8f) continue;
-                const q4 turn = rotation_between(divs(ro_c, rest_len), divs(live_prev, live_len));
-                const f3 target = add(pc, qrot(turn, ro_n));
-                const f3 delta = mul(sub(target, pn), P.local_per_substep);
-                const float ws = wc + wn;
-                if (ws <= 0.0f) continue;
-                if (lane == k + 1) p = add(p, mul(delta, wn / ws));
-                if (lane == k) p = sub(p, mul(delta, wc / ws));
+        // Serial along a strand: one thread walks each strand of the block (instead of a whole
+        // warp computing the same chain redundantly), on the block's positions in shared memory.
+        if (P.local_shape_on) {
+            s_chain[warp][lane] = make_float4(p.x, p.y, p.z, w);
+            __syncthreads();
+            if (threadIdx.x < kWarpsPerBlock) {
+                const int ws_ = threadIdx.x;
+                const int sg = blockIdx.x * kWarpsPerBlock + ws_;
+                const int cnt = sg < D.n_strands ? __ldg(&D.count[sg]) : 0;
+                float4* sp = s_chain[ws_];
+                const float4* ro = D.rest_offset + static_cast<size_t>(sg) * 32;
+                for (int k = 1; k + 1 < cnt; ++k) {
+                    const float4 qp = sp[k - 1], qc = sp[k], qn = sp[k + 1];
+                    const f3 pp = xyz(qp), pc = xyz(qc), pn = xyz(qn);
+                    const f3 ro_c = xyz(__ldg(&ro[k])), ro_n = xyz(__ldg(&ro[k + 1]));
+                    const float wc = qc.w, wn = qn.w;
+                    const f3 live_prev = sub(pc, pp);
+                    const float rest_len = len(ro_c);
+                    const float live_len = len(live_prev);
+                    if (rest_len <= 1e-8f || live_len <= 1e-8f) continue;
+                    const q4 turn = rotation_between(divs(ro_c, rest_len), divs(live_prev, live_len));
+                    const f3 target = add(pc, qrot(turn, ro_n));
+                    const f3 delta = mul(sub(target, pn), P.local_per_substep);
+                    const float wsum = wc + wn;
+                    if (wsum <= 0.0f) continue;
+                    const f3 nn = add(pn, mul(delta, wn / wsum));
+                    const f3 nc = sub(pc, mul(delta, wc / wsum));
+                    sp[k + 1] = make_float4(nn.x, nn.y, nn.z, wn);
+                    sp[k] = make_float4(nc.x, nc.y, nc.z, wc);
+                }
             }
+            __syncthreads();
+            p = xyz(s_chain[warp][lane]);
         }
         // --- 7: collisions, deepest contact kept (strand_solver.h:275-298) ---------------
         bool contacted = false;

@@ -30,7 +30,7 @@
 namespace pxb {
 namespace {
 
-constexpr int kWarpsPerBlock = 8;
+constexpr int kWarpsPerBlock = 32;
 
 struct q4 {
     float x, y, z, w;

@@ -264,6 +264,20 @@ def bench_hair(args, ctx_factory):
     return 0
 
 
+def hbm_roofline(traffic, per_launch_ms):
+    """The same launch against HBM: DRAM bytes per launch (ncu, profiles/) over its duration,
+    against MEASURED_PEAKS.json's copy bandwidth. Shows the step is not HBM-bound."""
+    if not traffic:
+        return None
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        src = "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, ValueError, KeyError):
+        peak, src = 6650.0, "fallback 6.65 TB/s"
+    achieved = traffic / (per_launch_ms * 1e-3) / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": src}
+
+
 def bench_large(args, local_rank):
     """The large-cloth configuration: one 512 x 512 sheet (20 iterations, draped on a capsule,
     whole-GPU path) stepped together with the 65,536 x 32 groom (20 iterations, roots on a moving
@@ -654,7 +668,8 @@ def main():
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "measured on this GPU by pxb_measure_smem_bandwidth",
                          "kernel": "cloth_step_kernel", "per_launch_ms": per_launch_ms,
-                         "algorithmic_bytes_per_launch": algo_bytes},
+                         "algorithmic_bytes_per_launch": algo_bytes,
+                         "hbm": hbm_roofline(traffic, per_launch_ms)},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk,

@@ -66,6 +66,7 @@ def parse():
                     choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom",
                              "large_cloth_hair"])
     ap.add_argument("--cloths", type=int, default=None)
+    ap.add_argument("--side", type=int, default=64, help="sheet side of the uniform batch")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--graph", action="store_true",
@@ -80,7 +81,7 @@ def build_scene(args, rank):
     if args.workload == "single_drape":
         return scenes.single_drape(seed=rank)
     if args.workload == "uniform_batch":
-        return scenes.uniform_batch(n=args.cloths or 1024, side=64, seed=1 + rank)
+        return scenes.uniform_batch(n=args.cloths or 1024, side=args.side, seed=1 + rank)
     return scenes.uneven_batch(n=args.cloths or 4096, seed=2 + rank)
 
 

@@ -12,8 +12,9 @@
  *    keeps a message retrievable with pxb_last_error().
  *  - One host thread per context. A context owns one CUDA stream on one device; all device work
  *    is ordered on it.
- *  - No CPU fallback: an input the device path does not implement (mesh / convex-hull colliders,
- *    self-collision) is refused with PXB_ERR_UNSUPPORTED instead of being solved on the host.
+ *  - No CPU fallback: an input the device path does not implement (self-collision, cloths not
+ *    built by make_grid_cloth) is refused with PXB_ERR_UNSUPPORTED instead of being solved on
+ *    the host.
  *  - The plain-old-data structs below reproduce the reference's in-memory layouts byte for byte
  *    (glm::vec3 = 3 floats, glm::quat = x,y,z,w floats, no SIMD alignment), so a C++ caller can
  *    hand `std::vector<ClothParticle>::data()` and friends straight to this API.
@@ -122,13 +123,17 @@ typedef enum pxb_shape_type {
     PXB_SHAPE_SPHERE = 0,
     PXB_SHAPE_BOX = 1,
     PXB_SHAPE_CAPSULE = 2,
-    PXB_SHAPE_TRIANGLE_MESH = 3, /* refused with PXB_ERR_UNSUPPORTED */
-    PXB_SHAPE_CONVEX_HULL = 4    /* refused with PXB_ERR_UNSUPPORTED */
+    PXB_SHAPE_TRIANGLE_MESH = 3, /* geometry from pxb_geometry_create_mesh */
+    PXB_SHAPE_CONVEX_HULL = 4    /* geometry from pxb_geometry_create_hull */
 } pxb_shape_type;
 
 /* cloth::ClothCollider (physxcoopa/cloth/cloth_collision.h:53-78) with the fields of the
  * collision::Shape it points at (physxcoopa/collision/shape.h:54-102) copied in: the snapshot a
- * collider is for one step. Quaternions are (x, y, z, w). 144 bytes. */
+ * collider is for one step. Quaternions are (x, y, z, w). 152 bytes.
+ * A TriangleMesh or ConvexHull collider names its geometry by the id pxb_geometry_create_mesh /
+ * pxb_geometry_create_hull returned (Shape::mesh / Shape::hull, shape.h:85-98; 0 = none, which
+ * like a null pointer there never collides) and carries Shape::mesh_scale / Shape::hull_scale in
+ * geometry_scale. */
 typedef struct pxb_collider {
     int32_t type;               /* pxb_shape_type */
     int32_t enabled;            /* Shape::enabled; a disabled shape never collides */
@@ -145,6 +150,8 @@ typedef struct pxb_collider {
     float end_orientation[4];   /* ClothCollider::end_orientation */
     float bounds_min[3];        /* ClothCollider::bounds (world AABB over both poses) */
     float bounds_max[3];
+    uint32_t geometry;          /* TriangleMesh / ConvexHull: registered geometry id, 0 = none */
+    float geometry_scale;       /* Shape::mesh_scale or Shape::hull_scale */
 } pxb_collider;
 
 /* PhysicsWorld::GravitySource (physxcoopa/world.h:1154-1159). */
@@ -394,11 +401,61 @@ pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step
 /* ------------------------------------------------------------------------------------------ */
 
 /* For each of n points: projects it out of `collider` with standoff `thickness`. Writes the
- * corrected point, the normal and depth, and hit (1/0). Host arrays; synchronous. */
+ * corrected point, the normal and depth, and hit (1/0). motion_start_xyz (may be NULL) is each
+ * point's position at the start of the substep, which enables the TriangleMesh swept crossing
+ * test (cloth_collision.h:217-272). Host arrays; synchronous. */
 pxb_status pxb_project_particles(pxb_context* ctx, const pxb_collider* collider, float thickness,
                                  const float* points_xyz, const float* motion_start_xyz,
                                  uint32_t n, float* points_out, float* normals_out,
                                  float* depths_out, int32_t* hit_out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Collider geometry: geometry::ConvexHull and geometry::TriangleMesh, registered once          */
+/* ------------------------------------------------------------------------------------------ */
+
+/* geometry::ConvexHull (physxcoopa/geometry/convex_hull.h:41-57), the arrays hull_vs_sphere
+ * reads: vertices (xyz), face_planes (xyz = outward unit normal, w = offset), and face f's
+ * vertex indices face_vertices[face_starts[f] .. face_starts[f + 1]), CCW about its normal. */
+typedef struct pxb_hull_desc {
+    const float* vertices;         /* 3 floats per vertex */
+    uint32_t n_vertices;
+    const float* face_planes;      /* 4 floats per face */
+    uint32_t n_faces;
+    const uint32_t* face_starts;   /* n_faces + 1 entries, starting at 0 */
+    const uint32_t* face_vertices; /* face_starts[n_faces] entries */
+} pxb_hull_desc;
+
+/* geometry::TriangleMesh (physxcoopa/geometry/triangle_mesh.h:70-96) as its four-argument
+ * constructor takes it: vertices, three indices per triangle and one face normal per triangle
+ * (TriangleMesh::normals()). normals may be NULL: they are then computed the way
+ * TriangleMesh::from_triangles does, normalize(cross(b - a, c - a)). Adjacency is not read by
+ * cloth or strand collision. */
+typedef struct pxb_mesh_desc {
+    const float* vertices;   /* 3 floats per vertex */
+    uint32_t n_vertices;
+    const uint32_t* indices; /* 3 per triangle */
+    uint32_t n_indices;
+    const float* normals;    /* 3 floats per triangle, or NULL */
+} pxb_mesh_desc;
+
+/* Copies a hull to the device and returns its id (never 0) for pxb_collider::geometry. Each
+ * step then poses it on the host (world vertices, face planes and edge normals, as
+ * collision::world_posed_hull and hull_vs_sphere derive them) and every particle tests the
+ * posed faces on the device. Refused: no faces, a face with no vertex or more than 160
+ * (k_hull_clip_cap, sat_hull.h:157), an index out of range; PXB_ERR_TOO_LARGE beyond 4096 faces
+ * or 65536 face-vertex entries. */
+pxb_status pxb_geometry_create_hull(pxb_context* ctx, const pxb_hull_desc* desc, uint32_t* id_out);
+
+/* Copies a triangle mesh to the device with its bounding-volume hierarchy, built on the host by
+ * MeshBVH::build's rule (mesh_bvh.h: leaves of at most 4 triangles, median split on the widest
+ * centroid axis), so the device visits candidate triangles in the reference's order and breaks
+ * ties between equally near triangles the same way. An empty mesh (no triangles) is accepted and
+ * never collides, like TriangleMesh::empty(). PXB_ERR_TOO_LARGE beyond 2^24 triangles. */
+pxb_status pxb_geometry_create_mesh(pxb_context* ctx, const pxb_mesh_desc* desc, uint32_t* id_out);
+
+/* Waits for the context's stream, then frees the geometry. A later step naming its id is refused
+ * with PXB_ERR_INVALID_HANDLE. */
+pxb_status pxb_geometry_destroy(pxb_context* ctx, uint32_t id);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Grid builders (host, setup time): cloth::make_grid_cloth / pin_static / build_tethers        */

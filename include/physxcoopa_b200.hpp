@@ -21,6 +21,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "physxcoopa_b200.h"
@@ -49,15 +50,63 @@ public:
         if (s != PXB_OK) throw std::runtime_error(std::string(what) + ": " + pxb_last_error(ctx_));
     }
 
+    // The device copy of a Shape's hull (Shape::hull, shape.h:97), registered the first time a
+    // collider names it. Like the reference's non-owning pointer, the object is assumed not to
+    // change afterwards: after editing or freeing one, call forget_geometry.
+    uint32_t geometry_id(const coopa::physx::geometry::ConvexHull* h) {
+        if (!h) return 0;
+        auto it = geometry_.find(h);
+        if (it != geometry_.end()) return it->second;
+        pxb_hull_desc d;
+        std::memset(&d, 0, sizeof(d));
+        d.vertices = reinterpret_cast<const float*>(h->vertices.data());
+        d.n_vertices = static_cast<uint32_t>(h->vertices.size());
+        d.face_planes = reinterpret_cast<const float*>(h->face_planes.data());
+        d.n_faces = static_cast<uint32_t>(h->face_planes.size());
+        d.face_starts = h->face_starts.data();
+        d.face_vertices = h->face_vertices.data();
+        uint32_t id = 0;
+        check(pxb_geometry_create_hull(ctx_, &d, &id), "register convex hull");
+        geometry_[h] = id;
+        return id;
+    }
+    // The device copy of a Shape's triangle mesh (Shape::mesh, shape.h:85). Height-grid meshes
+    // (TriangleMesh::from_height_grid) have no vertex arrays and are refused.
+    uint32_t geometry_id(const coopa::physx::geometry::TriangleMesh* m) {
+        if (!m) return 0;
+        auto it = geometry_.find(m);
+        if (it != geometry_.end()) return it->second;
+        if (m->height_grid()) throw std::runtime_error("height-grid meshes are not supported by the device path");
+        pxb_mesh_desc d;
+        std::memset(&d, 0, sizeof(d));
+        d.vertices = reinterpret_cast<const float*>(m->vertices().data());
+        d.n_vertices = static_cast<uint32_t>(m->vertices().size());
+        d.indices = m->indices().data();
+        d.n_indices = static_cast<uint32_t>(m->indices().size());
+        d.normals = reinterpret_cast<const float*>(m->normals().data());
+        uint32_t id = 0;
+        check(pxb_geometry_create_mesh(ctx_, &d, &id), "register triangle mesh");
+        geometry_[m] = id;
+        return id;
+    }
+    void forget_geometry(const void* object) {
+        auto it = geometry_.find(object);
+        if (it == geometry_.end()) return;
+        check(pxb_geometry_destroy(ctx_, it->second), "forget geometry");
+        geometry_.erase(it);
+    }
+
 private:
     pxb_context* ctx_ = nullptr;
+    std::unordered_map<const void*, uint32_t> geometry_;
 };
 
 inline void put3(float* o, const glm::vec3& v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
 inline void put4(float* o, const glm::quat& q) { o[0] = q.x; o[1] = q.y; o[2] = q.z; o[3] = q.w; }
 
-// cloth::ClothCollider + the collision::Shape it points at -> the C-ABI snapshot.
-inline pxb_collider to_collider(const coopa::physx::cloth::ClothCollider& c) {
+// cloth::ClothCollider + the collision::Shape it points at -> the C-ABI snapshot (a mesh or
+// hull names the device copy of its geometry).
+inline pxb_collider to_collider(Device& dev, const coopa::physx::cloth::ClothCollider& c) {
     pxb_collider o;
     std::memset(&o, 0, sizeof(o));
     const coopa::physx::collision::Shape* s = c.shape;
@@ -71,6 +120,13 @@ inline pxb_collider to_collider(const coopa::physx::cloth::ClothCollider& c) {
         o.capsule_radius = s->capsule_radius;
         o.capsule_half_height = s->capsule_half_height;
         o.capsule_axis = s->capsule_axis;
+        if (s->type == coopa::physx::collision::ShapeType::ConvexHull) {
+            o.geometry = dev.geometry_id(s->hull);
+            o.geometry_scale = s->hull_scale;
+        } else if (s->type == coopa::physx::collision::ShapeType::TriangleMesh) {
+            o.geometry = dev.geometry_id(s->mesh);
+            o.geometry_scale = s->mesh_scale;
+        }
     }
     put3(o.position, c.position);
     put4(o.orientation, c.orientation);
@@ -161,7 +217,7 @@ void solve_cloth(Device& dev, coopa::physx::cloth::Cloth& c,
     d.time = c.time;
     std::vector<pxb_collider> cols;
     cols.reserve(colliders.size());
-    for (const auto& k : colliders) cols.push_back(to_collider(k));
+    for (const auto& k : colliders) cols.push_back(to_collider(dev, k));
     const float g[3] = {gravity.x, gravity.y, gravity.z};
     float bounds[6];
     dev.check(pxb_solve_cloth_host(dev.get(), &d, reinterpret_cast<pxb_particle*>(c.particles.data()),
@@ -196,7 +252,7 @@ void solve_strands(Device& dev, coopa::physx::hair::StrandSet& set,
     d.params = to_params(set.params);
     d.time = set.time;
     std::vector<pxb_collider> cols;
-    for (const auto& k : colliders) cols.push_back(to_collider(k));
+    for (const auto& k : colliders) cols.push_back(to_collider(dev, k));
     const float g[3] = {gravity.x, gravity.y, gravity.z};
     float bounds[6];
     dev.check(pxb_solve_strands_host(dev.get(), &d, reinterpret_cast<pxb_particle*>(set.particles.data()),

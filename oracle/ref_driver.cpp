@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <thread>
 #include <vector>
@@ -112,6 +113,17 @@ px::hair::StrandParams to_params(const pxb_strand_params& p) {
     return r;
 }
 
+// Collider geometry by pxb_collider::geometry id: the reference's own ConvexHull and
+// TriangleMesh objects (the mesh's constructor builds its MeshBVH).
+std::map<uint32_t, std::unique_ptr<px::geometry::ConvexHull>> g_hulls;
+std::map<uint32_t, std::unique_ptr<px::geometry::TriangleMesh>> g_meshes;
+
+template <class M>
+auto* find_geometry(M& m, uint32_t id) {
+    auto it = m.find(id);
+    return it == m.end() ? nullptr : it->second.get();
+}
+
 // A collider snapshot owns the collision::Shape its ClothCollider points at.
 struct RefColliders {
     std::vector<px::collision::Shape> shapes;
@@ -130,6 +142,13 @@ struct RefColliders {
             s.capsule_radius = c[i].capsule_radius;
             s.capsule_half_height = c[i].capsule_half_height;
             s.capsule_axis = c[i].capsule_axis;
+            if (c[i].type == PXB_SHAPE_CONVEX_HULL) {
+                s.hull = find_geometry(g_hulls, c[i].geometry);
+                s.hull_scale = c[i].geometry_scale;
+            } else if (c[i].type == PXB_SHAPE_TRIANGLE_MESH) {
+                s.mesh = find_geometry(g_meshes, c[i].geometry);
+                s.mesh_scale = c[i].geometry_scale;
+            }
             px::cloth::ClothCollider& k = colliders[i];
             k.shape = &shapes[i];
             k.position = v3(c[i].position);
@@ -268,6 +287,70 @@ void pxbref_solve_cloth(void* h, const pxb_collider* colliders, uint32_t n_colli
     RefColliders rc(colliders, n_colliders);
     px::cloth::ClothSolverScratch scratch;
     px::cloth::solve_cloth(*c, rc.colliders, v3(gravity), substeps, iterations, dt, scratch);
+}
+
+// Registers the reference's ConvexHull (its fields as given) under `id`.
+int pxbref_geometry_set_hull(uint32_t id, const pxb_hull_desc* d) {
+    auto h = std::make_unique<px::geometry::ConvexHull>();
+    for (uint32_t i = 0; i < d->n_vertices; ++i) h->vertices.push_back(v3(&d->vertices[3 * i]));
+    for (uint32_t f = 0; f < d->n_faces; ++f) {
+        const float* q = &d->face_planes[4 * f];
+        h->face_planes.push_back(glm::vec4(q[0], q[1], q[2], q[3]));
+    }
+    h->face_starts.assign(d->face_starts, d->face_starts + d->n_faces + 1);
+    h->face_vertices.assign(d->face_vertices, d->face_vertices + d->face_starts[d->n_faces]);
+    g_hulls[id] = std::move(h);
+    return 0;
+}
+
+// Registers a TriangleMesh made by its four-argument constructor (normals NULL: from_triangles).
+int pxbref_geometry_set_mesh(uint32_t id, const pxb_mesh_desc* d) {
+    std::vector<glm::vec3> verts;
+    for (uint32_t i = 0; i < d->n_vertices; ++i) verts.push_back(v3(&d->vertices[3 * i]));
+    std::vector<uint32_t> idx(d->indices, d->indices + d->n_indices);
+    if (!d->normals) {
+        g_meshes[id] = std::make_unique<px::geometry::TriangleMesh>(
+            px::geometry::TriangleMesh::from_triangles(verts, idx));
+        return 0;
+    }
+    const uint32_t T = d->n_indices / 3;
+    std::vector<glm::vec3> normals;
+    for (uint32_t t = 0; t < T; ++t) normals.push_back(v3(&d->normals[3 * t]));
+    std::vector<px::geometry::TriangleAdjacency> adjacency(T);
+    g_meshes[id] = std::make_unique<px::geometry::TriangleMesh>(std::move(verts), std::move(idx), std::move(normals),
+                                                                std::move(adjacency));
+    return 0;
+}
+
+void pxbref_geometry_clear() {
+    g_hulls.clear();
+    g_meshes.clear();
+}
+
+// geometry::build_convex_hull (convex_hull.h:211) over `count` points: the reference's own hull
+// builder, so tests can use hulls exactly as the reference makes them. Writes up to the given
+// capacities and returns the face count (0 for a degenerate cloud, -1 when a capacity is short).
+int pxbref_build_convex_hull(const float* points, uint32_t count, float* vertices, uint32_t cap_vertices,
+                             uint32_t* n_vertices, float* planes, uint32_t cap_faces, uint32_t* starts,
+                             uint32_t* face_vertices, uint32_t cap_face_vertices) {
+    std::vector<glm::vec3> pts;
+    for (uint32_t i = 0; i < count; ++i) pts.push_back(v3(&points[3 * i]));
+    px::geometry::ConvexHull h;
+    if (!px::geometry::build_convex_hull(pts.data(), pts.size(), h)) return 0;
+    if (h.vertices.size() > cap_vertices || h.face_planes.size() > cap_faces ||
+        h.face_vertices.size() > cap_face_vertices)
+        return -1;
+    for (size_t i = 0; i < h.vertices.size(); ++i) put(&vertices[3 * i], h.vertices[i]);
+    for (size_t f = 0; f < h.face_planes.size(); ++f) {
+        planes[4 * f] = h.face_planes[f].x;
+        planes[4 * f + 1] = h.face_planes[f].y;
+        planes[4 * f + 2] = h.face_planes[f].z;
+        planes[4 * f + 3] = h.face_planes[f].w;
+    }
+    for (size_t f = 0; f < h.face_starts.size(); ++f) starts[f] = h.face_starts[f];
+    for (size_t i = 0; i < h.face_vertices.size(); ++i) face_vertices[i] = h.face_vertices[i];
+    *n_vertices = static_cast<uint32_t>(h.vertices.size());
+    return static_cast<int>(h.face_planes.size());
 }
 
 // cloth::project_particle (cloth_collision.h:386-420) on one point.

@@ -95,9 +95,406 @@ static v3 closest_point_on_segment(v3 point, v3 a, v3 b) {
     return add(a, mul(ab, t));
 }
 
-/* cloth::detail::project_at_pose_ (cloth_collision.h:109-203), Sphere / Capsule / Box. */
+/* ---- collider geometry, by pxb_collider::geometry id ---------------------------------- */
+
+typedef struct {
+    int type; /* 0: free slot */
+    /* geometry::ConvexHull (convex_hull.h:41-57) */
+    float* verts;
+    uint32_t n_verts;
+    float* planes;
+    uint32_t n_faces;
+    uint32_t* starts;
+    uint32_t* fverts;
+    /* geometry::TriangleMesh (triangle_mesh.h:70-96) and its MeshBVH */
+    float* mverts;
+    uint32_t* idx;
+    float* normals;
+    uint32_t n_tris;
+    orc_bvh_node* nodes;
+    uint32_t n_nodes;
+    uint32_t* order;
+} orc_geometry;
+
+#define ORC_MAX_GEOMETRY 1024
+static orc_geometry g_geo[ORC_MAX_GEOMETRY];
+
+static void free_geometry(orc_geometry* g) {
+    free(g->verts); free(g->planes); free(g->starts); free(g->fverts);
+    free(g->mverts); free(g->idx); free(g->normals); free(g->nodes); free(g->order);
+    memset(g, 0, sizeof(*g));
+}
+
+void orc_geometry_clear(void) {
+    for (int i = 0; i < ORC_MAX_GEOMETRY; ++i) free_geometry(&g_geo[i]);
+}
+
+static void* dup(const void* src, size_t bytes) {
+    void* d = malloc(bytes ? bytes : 1);
+    if (bytes) memcpy(d, src, bytes);
+    return d;
+}
+
+int orc_geometry_set_hull(uint32_t id, const pxb_hull_desc* d) {
+    if (id == 0 || id >= ORC_MAX_GEOMETRY || d->n_faces == 0) return -1;
+    orc_geometry* g = &g_geo[id];
+    free_geometry(g);
+    const uint32_t nfv = d->face_starts[d->n_faces];
+    g->type = PXB_SHAPE_CONVEX_HULL;
+    g->n_verts = d->n_vertices;
+    g->n_faces = d->n_faces;
+    g->verts = (float*)dup(d->vertices, sizeof(float) * 3 * d->n_vertices);
+    g->planes = (float*)dup(d->face_planes, sizeof(float) * 4 * d->n_faces);
+    g->starts = (uint32_t*)dup(d->face_starts, sizeof(uint32_t) * (d->n_faces + 1));
+    g->fverts = (uint32_t*)dup(d->face_vertices, sizeof(uint32_t) * nfv);
+    return 0;
+}
+
+int orc_geometry_set_mesh(uint32_t id, const pxb_mesh_desc* d) {
+    if (id == 0 || id >= ORC_MAX_GEOMETRY) return -1;
+    orc_geometry* g = &g_geo[id];
+    free_geometry(g);
+    const uint32_t T = d->n_indices / 3;
+    g->type = PXB_SHAPE_TRIANGLE_MESH;
+    g->n_tris = T;
+    g->mverts = (float*)dup(d->vertices, sizeof(float) * 3 * d->n_vertices);
+    g->idx = (uint32_t*)dup(d->indices, sizeof(uint32_t) * 3 * T);
+    g->normals = (float*)malloc(sizeof(float) * 3 * (T ? T : 1));
+    for (uint32_t t = 0; t < T; ++t) {
+        if (d->normals) {
+            memcpy(&g->normals[3 * t], &d->normals[3 * t], 12);
+        } else { /* TriangleMesh::from_triangles: normalize(cross(b - a, c - a)) */
+            const v3 a = ld(&d->vertices[3 * g->idx[3 * t]]), b = ld(&d->vertices[3 * g->idx[3 * t + 1]]),
+                     c = ld(&d->vertices[3 * g->idx[3 * t + 2]]);
+            const v3 cr = cross(sub(b, a), sub(c, a));
+            st(&g->normals[3 * t], mul(cr, 1.0f / sqrtf(dot(cr, cr))));
+        }
+    }
+    g->nodes = (orc_bvh_node*)malloc(sizeof(orc_bvh_node) * (2 * T + 1));
+    g->order = (uint32_t*)malloc(sizeof(uint32_t) * (T ? T : 1));
+    g->n_nodes = T ? orc_bvh_build(g->mverts, g->idx, T, g->nodes, g->order) : 0;
+    return 0;
+}
+
+static const orc_geometry* geometry_of(const pxb_collider* s, int type) {
+    if (s->geometry == 0 || s->geometry >= ORC_MAX_GEOMETRY) return NULL;
+    const orc_geometry* g = &g_geo[s->geometry];
+    return g->type == type ? g : NULL;
+}
+
+/* conjugate(q) / dot(q, q) (glm::inverse of a quaternion) */
+static inline q4 qinverse(q4 q) {
+    const float qq = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+    q4 r = {-q.x / qq, -q.y / qq, -q.z / qq, q.w / qq};
+    return r;
+}
+
+/* ---- ConvexHull: collision::hull_vs_sphere (sat_hull.h:649-688) ----------------------- */
+
+typedef struct {
+    const orc_geometry* g;
+    v3 position;
+    q4 rotation;
+    float scale;
+} posed_hull;
+
+static v3 hull_world_vertex(const posed_hull* h, uint32_t i) { /* PosedHull::world_vertex */
+    return add(h->position, qrot(h->rotation, mul(ld(&h->g->verts[3 * i]), h->scale)));
+}
+static v3 hull_world_normal(const posed_hull* h, uint32_t f) { /* PosedHull::world_face_normal */
+    return qrot(h->rotation, ld(&h->g->planes[4 * f]));
+}
+/* outward_edge_normal_ (sat_hull.h:162-166) */
+static v3 outward_edge_normal(v3 edge_dir, v3 face_normal) {
+    const v3 n = cross(edge_dir, face_normal);
+    const float l = len(n);
+    return l > 1e-12f ? divs(n, l) : face_normal;
+}
+/* closest_point_on_convex_polygon_ (sat_hull.h:601-627) */
+static v3 closest_on_convex_polygon(const v3* poly, int n, v3 normal, v3 point) {
+    const float plane_d = dot(normal, poly[0]);
+    const v3 proj = sub(point, mul(normal, dot(normal, point) - plane_d));
+    int inside = 1;
+    for (int i = 0; i < n && inside; ++i) {
+        const v3 a = poly[i], b = poly[(i + 1) % n];
+        const v3 outward = outward_edge_normal(sub(b, a), normal);
+        if (dot(outward, sub(proj, a)) > 1e-6f) inside = 0;
+    }
+    if (inside) return proj;
+    v3 best = poly[0];
+    float best_dist2 = 3.402823466e+38f;
+    for (int i = 0; i < n; ++i) {
+        const v3 a = poly[i], b = poly[(i + 1) % n];
+        const v3 ab = sub(b, a);
+        const float len2 = dot(ab, ab);
+        const float t = len2 > 1e-12f ? clampf(dot(sub(proj, a), ab) / len2, 0.0f, 1.0f) : 0.0f;
+        const v3 q = add(a, mul(ab, t));
+        const float d2 = dot(sub(proj, q), sub(proj, q));
+        if (d2 < best_dist2) {
+            best_dist2 = d2;
+            best = q;
+        }
+    }
+    return best;
+}
+static int hull_vs_sphere(const posed_hull* h, v3 center, float radius, v3* normal, float* pen, v3* point) {
+    uint32_t best_face = 0;
+    float best_dist = -3.402823466e+38f;
+    int any_positive = 0;
+    for (uint32_t f = 0; f < h->g->n_faces; ++f) {
+        const v3 n = hull_world_normal(h, f);
+        const float d = dot(n, hull_world_vertex(h, h->g->fverts[h->g->starts[f]]));
+        const float dist = dot(n, center) - d;
+        if (dist > 0.0f) any_positive = 1;
+        if (dist > best_dist) {
+            best_dist = dist;
+            best_face = f;
+        }
+    }
+    const v3 n = hull_world_normal(h, best_face);
+    v3 poly[160]; /* k_hull_clip_cap (sat_hull.h:157) */
+    const uint32_t s0 = h->g->starts[best_face], e0 = h->g->starts[best_face + 1];
+    const int count = (int)(e0 - s0) < 160 ? (int)(e0 - s0) : 160;
+    for (int i = 0; i < count; ++i) poly[i] = hull_world_vertex(h, h->g->fverts[s0 + i]);
+    *point = closest_on_convex_polygon(poly, count, n, center);
+    if (!any_positive) {
+        const v3 diff = sub(*point, center);
+        const float dist = len(diff);
+        *normal = dist > K_EPSILON ? divs(diff, dist) : n;
+        *pen = radius + (-best_dist);
+        return 1;
+    }
+    const v3 diff = sub(center, *point);
+    const float dist = len(diff);
+    if (dist > radius) return 0;
+    *normal = dist > K_EPSILON ? divs(diff, dist) : n;
+    *pen = radius - dist;
+    return 1;
+}
+
+/* ---- TriangleMesh: MeshBVH queries (mesh_bvh.h) and the mesh branch ------------------- */
+
+/* collision::closest_point_on_triangle (mesh_contact.h:63-99) */
+static v3 closest_on_triangle(v3 p, v3 a, v3 b, v3 c) {
+    const v3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f) return a;
+    const v3 bp = sub(p, b);
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) return b;
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+        const float v = d1 / (d1 - d3);
+        return add(a, smul(v, ab));
+    }
+    const v3 cp = sub(p, c);
+    const float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6) return c;
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+        const float w = d2 / (d2 - d6);
+        return add(a, smul(w, ac));
+    }
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+        const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        return add(b, smul(w, sub(c, b)));
+    }
+    const float denom = 1.0f / (va + vb + vc);
+    const float v = vb * denom;
+    const float w = vc * denom;
+    return add(add(a, mul(ab, v)), mul(ac, w));
+}
+
+typedef struct {
+    v3 origin, direction;
+    float max_distance;
+} ray3;
+
+/* Ray::intersect (ray.h:47-60) */
+static int ray_box(const ray3* r, const float* mn, const float* mx) {
+    const v3 inv = mk(1.0f / (r->direction.x + 1e-9f), 1.0f / (r->direction.y + 1e-9f),
+                      1.0f / (r->direction.z + 1e-9f));
+    const v3 t0 = mk((mn[0] - r->origin.x) * inv.x, (mn[1] - r->origin.y) * inv.y, (mn[2] - r->origin.z) * inv.z);
+    const v3 t1 = mk((mx[0] - r->origin.x) * inv.x, (mx[1] - r->origin.y) * inv.y, (mx[2] - r->origin.z) * inv.z);
+    const v3 tmin = mk(fminr(t0.x, t1.x), fminr(t0.y, t1.y), fminr(t0.z, t1.z));
+    const v3 tmax = mk(fmaxr(t0.x, t1.x), fmaxr(t0.y, t1.y), fmaxr(t0.z, t1.z));
+    /* std::max / std::min over an initializer list keep the first extreme */
+    float t_near = tmin.x;
+    if (t_near < tmin.y) t_near = tmin.y;
+    if (t_near < tmin.z) t_near = tmin.z;
+    if (t_near < 0.0f) t_near = 0.0f;
+    float t_far = tmax.x;
+    if (tmax.y < t_far) t_far = tmax.y;
+    if (tmax.z < t_far) t_far = tmax.z;
+    if (r->max_distance < t_far) t_far = r->max_distance;
+    return !(t_far < t_near);
+}
+
+/* geometry::ray_vs_triangle (ray.h:205-228) */
+static int ray_triangle(const ray3* r, v3 a, v3 b, v3 c, float* t) {
+    const v3 edge1 = sub(b, a), edge2 = sub(c, a);
+    const v3 pvec = cross(r->direction, edge2);
+    const float det = dot(edge1, pvec);
+    if (det > -K_EPSILON && det < K_EPSILON) return 0;
+    const float inv_det = 1.0f / det;
+    const v3 tvec = sub(r->origin, a);
+    const float u = dot(tvec, pvec) * inv_det;
+    if (u < 0.0f || u > 1.0f) return 0;
+    const v3 qvec = cross(tvec, edge1);
+    const float v = dot(r->direction, qvec) * inv_det;
+    if (v < 0.0f || u + v > 1.0f) return 0;
+    const float candidate = dot(edge2, qvec) * inv_det;
+    if (candidate < 0.0f || candidate > r->max_distance) return 0;
+    *t = candidate;
+    return 1;
+}
+
+static void mesh_tri(const orc_geometry* g, uint32_t t, v3* v0, v3* v1, v3* v2) {
+    *v0 = ld(&g->mverts[3 * g->idx[3 * t]]);
+    *v1 = ld(&g->mverts[3 * g->idx[3 * t + 1]]);
+    *v2 = ld(&g->mverts[3 * g->idx[3 * t + 2]]);
+}
+
+typedef struct {
+    const orc_geometry* g;
+    ray3 ray;
+    float best_t;
+    uint32_t crossed_tri;
+    int crossed;
+} raycast_state;
+
+/* MeshBVH::raycast_recursive_ with the swept crossing callback (cloth_collision.h:243-257) */
+static void raycast_node(raycast_state* s, int32_t idx) {
+    const orc_bvh_node* node = &s->g->nodes[idx];
+    if (!ray_box(&s->ray, node->mn, node->mx)) return;
+    if (node->left < 0) {
+        for (uint32_t i = 0; i < node->tri_count; ++i) {
+            const uint32_t tri = s->g->order[node->tri_start + i];
+            v3 v0, v1, v2;
+            mesh_tri(s->g, tri, &v0, &v1, &v2);
+            float t = 0.0f;
+            if ((ray_triangle(&s->ray, v0, v1, v2, &t) || ray_triangle(&s->ray, v0, v2, v1, &t)) && t < s->best_t) {
+                s->best_t = t;
+                s->crossed_tri = tri;
+                s->crossed = 1;
+            }
+        }
+    } else {
+        raycast_node(s, node->left);
+        raycast_node(s, node->right);
+    }
+}
+
+typedef struct {
+    const orc_geometry* g;
+    v3 local_p, qmin, qmax;
+    float lt2;
+    float best_d2;
+    v3 best_point, best_delta;
+    uint32_t best_tri;
+    int hit, any_front;
+} query_state;
+
+/* MeshBVH::query_recursive_ with the proximity callback (cloth_collision.h:291-310) */
+static void query_node(query_state* s, int32_t idx) {
+    const orc_bvh_node* node = &s->g->nodes[idx];
+    /* AABB::overlaps (aabb.h:35-39) */
+    if (!(node->mn[0] <= s->qmax.x && node->mx[0] >= s->qmin.x && node->mn[1] <= s->qmax.y &&
+          node->mx[1] >= s->qmin.y && node->mn[2] <= s->qmax.z && node->mx[2] >= s->qmin.z))
+        return;
+    if (node->left < 0) {
+        for (uint32_t i = 0; i < node->tri_count; ++i) {
+            const uint32_t tri = s->g->order[node->tri_start + i];
+            v3 v0, v1, v2;
+            mesh_tri(s->g, tri, &v0, &v1, &v2);
+            const v3 closest = closest_on_triangle(s->local_p, v0, v1, v2);
+            const v3 delta = sub(s->local_p, closest);
+            const float d2 = dot(delta, delta);
+            if (d2 > s->lt2) continue;
+            if (dot(delta, ld(&s->g->normals[3 * tri])) >= 0.0f) s->any_front = 1;
+            if (d2 > s->best_d2) continue;
+            s->best_d2 = d2;
+            s->best_point = closest;
+            s->best_delta = delta;
+            s->best_tri = tri;
+            s->hit = 1;
+        }
+    } else {
+        query_node(s, node->left);
+        query_node(s, node->right);
+    }
+}
+
+/* project_at_pose_'s TriangleMesh branch (cloth_collision.h:205-340) */
+static int project_mesh(const pxb_collider* s, v3 pose_pos, q4 pose_rot, float thickness, v3* p,
+                        v3* normal_out, float* depth_out, const v3* motion_start) {
+    const orc_geometry* g = geometry_of(s, PXB_SHAPE_TRIANGLE_MESH);
+    if (!g || g->n_nodes == 0) return 0;
+    const q4 rot = qmul(pose_rot, ldq(s->local_rotation));
+    const q4 inv_rot = qinverse(rot);
+    const v3 mesh_origin = add(pose_pos, qrot(pose_rot, ld(s->local_center)));
+    const float scale = (s->geometry_scale > K_EPSILON) ? s->geometry_scale : 1.0f;
+    const v3 local_p = divs(qrot(inv_rot, sub(*p, mesh_origin)), scale);
+    const float local_thickness = thickness / scale;
+
+    if (motion_start) {
+        const v3 local_start = divs(qrot(inv_rot, sub(*motion_start, mesh_origin)), scale);
+        const v3 seg = sub(local_p, local_start);
+        const float seg_len = len(seg);
+        if (seg_len > local_thickness) {
+            raycast_state rs;
+            rs.g = g;
+            rs.ray.origin = local_start;
+            rs.ray.direction = divs(seg, seg_len);
+            rs.ray.max_distance = seg_len;
+            rs.best_t = seg_len;
+            rs.crossed_tri = 0;
+            rs.crossed = 0;
+            raycast_node(&rs, 0);
+            if (rs.crossed) {
+                const v3 local_hit = add(rs.ray.origin, mul(rs.ray.direction, rs.best_t));
+                v3 face = safe_normalize(ld(&g->normals[3 * rs.crossed_tri]));
+                if (dot(sub(local_start, local_hit), face) < 0.0f) face = neg(face);
+                const v3 local_fixed = add(local_hit, mul(face, local_thickness));
+                *depth_out = len(sub(local_p, local_fixed)) * scale;
+                *p = add(mesh_origin, qrot(rot, mul(local_fixed, scale)));
+                *normal_out = qrot(rot, face);
+                return 1;
+            }
+        }
+    }
+
+    query_state qs;
+    memset(&qs, 0, sizeof(qs));
+    qs.g = g;
+    qs.local_p = local_p;
+    qs.qmin = sub(local_p, mk(local_thickness, local_thickness, local_thickness));
+    qs.qmax = add(local_p, mk(local_thickness, local_thickness, local_thickness));
+    qs.lt2 = local_thickness * local_thickness;
+    qs.best_d2 = local_thickness * local_thickness;
+    query_node(&qs, 0);
+    if (!qs.hit) return 0;
+    v3 best_normal;
+    if (!qs.any_front) {
+        best_normal = safe_normalize(ld(&g->normals[3 * qs.best_tri]));
+    } else if (qs.best_d2 > K_EPSILON * K_EPSILON) {
+        best_normal = divs(qs.best_delta, sqrtf(qs.best_d2));
+    } else {
+        const v3 face = safe_normalize(ld(&g->normals[3 * qs.best_tri]));
+        best_normal = (dot(qs.best_delta, face) < 0.0f) ? neg(face) : face;
+    }
+    const v3 local_fixed = add(qs.best_point, mul(best_normal, local_thickness));
+    *depth_out = len(sub(local_p, local_fixed)) * scale;
+    *p = add(mesh_origin, qrot(rot, mul(local_fixed, scale)));
+    *normal_out = qrot(rot, best_normal);
+    return 1;
+}
+
+/* cloth::detail::project_at_pose_ (cloth_collision.h:109-356). */
 static int project_at_pose(const pxb_collider* s, v3 pose_pos, q4 pose_rot, v3 sweep,
-                           float thickness, v3* p, v3* normal_out, float* depth_out) {
+                           float thickness, v3* p, v3* normal_out, float* depth_out,
+                           const v3* motion_start) {
     const int swept = dot(sweep, sweep) > K_EPSILON * K_EPSILON;
     const v3 local_center = ld(s->local_center);
     switch (s->type) {
@@ -186,6 +583,24 @@ static int project_at_pose(const pxb_collider* s, v3 pose_pos, q4 pose_rot, v3 s
             }
             return 1;
         }
+        case PXB_SHAPE_TRIANGLE_MESH:
+            return project_mesh(s, pose_pos, pose_rot, thickness, p, normal_out, depth_out, motion_start);
+        case PXB_SHAPE_CONVEX_HULL: {
+            /* collision::world_posed_hull (sat_hull.h:66-73), probe sphere of radius thickness */
+            posed_hull h;
+            h.g = geometry_of(s, PXB_SHAPE_CONVEX_HULL);
+            if (!h.g) return 0;
+            h.position = add(pose_pos, qrot(pose_rot, local_center));
+            h.rotation = qmul(pose_rot, ldq(s->local_rotation));
+            h.scale = s->geometry_scale;
+            v3 point, normal;
+            float pen = 0.0f;
+            if (!hull_vs_sphere(&h, *p, thickness, &normal, &pen, &point)) return 0;
+            *normal_out = normal;
+            *p = add(point, mul(normal, thickness));
+            *depth_out = pen;
+            return 1;
+        }
         default:
             return -1;
     }
@@ -193,29 +608,26 @@ static int project_at_pose(const pxb_collider* s, v3 pose_pos, q4 pose_rot, v3 s
 
 /* cloth::project_particle (cloth_collision.h:386-420). */
 static int project_particle(const pxb_collider* col, float thickness, v3* p, v3* normal_out,
-                            float* depth_out) {
+                            float* depth_out, const v3* motion_start) {
     if (!col->enabled) return 0;
-    if (col->type != PXB_SHAPE_SPHERE && col->type != PXB_SHAPE_BOX &&
-        col->type != PXB_SHAPE_CAPSULE) {
-        return -1;
-    }
+    if (col->type < PXB_SHAPE_SPHERE || col->type > PXB_SHAPE_CONVEX_HULL) return -1;
     const v3 sweep = ld(col->sweep);
     const int is_swept = dot(sweep, sweep) > K_EPSILON * K_EPSILON;
     const int two_pose = is_swept && (col->type == PXB_SHAPE_BOX || col->type == PXB_SHAPE_CAPSULE);
     const v3 pos = ld(col->position);
     const q4 rot = ldq(col->orientation);
     if (!two_pose) {
-        return project_at_pose(col, pos, rot, sweep, thickness, p, normal_out, depth_out);
+        return project_at_pose(col, pos, rot, sweep, thickness, p, normal_out, depth_out, motion_start);
     }
     v3 p_start = *p, n_start = mk(0, 0, 0);
     float d_start = 0.0f;
     const v3 zero = mk(0.0f, 0.0f, 0.0f);
     const int hit_start = project_at_pose(col, pos, rot, zero, thickness, &p_start, &n_start,
-                                          &d_start);
+                                          &d_start, motion_start);
     v3 p_end = *p, n_end = mk(0, 0, 0);
     float d_end = 0.0f;
     const int hit_end = project_at_pose(col, add(pos, sweep), ldq(col->end_orientation), zero,
-                                        thickness, &p_end, &n_end, &d_end);
+                                        thickness, &p_end, &n_end, &d_end, motion_start);
     if (!hit_start && !hit_end) return 0;
     if (hit_end && (!hit_start || d_end > d_start)) {
         *p = p_end; *normal_out = n_end; *depth_out = d_end;
@@ -227,10 +639,11 @@ static int project_particle(const pxb_collider* col, float thickness, v3* p, v3*
 
 int orc_project_particle(const pxb_collider* collider, float thickness, float p[3],
                          float normal_out[3], float* depth_out, const float* motion_start) {
-    (void)motion_start; /* consumed only by the TriangleMesh branch, which is not restated */
     v3 pp = ld(p), n = mk(0, 0, 0);
     float d = 0.0f;
-    const int r = project_particle(collider, thickness, &pp, &n, &d);
+    v3 start = mk(0, 0, 0);
+    if (motion_start) start = ld(motion_start);
+    const int r = project_particle(collider, thickness, &pp, &n, &d, motion_start ? &start : NULL);
     if (r == 1) {
         st(p, pp);
         st(normal_out, n);
@@ -347,12 +760,9 @@ int orc_solve_cloth(orc_cloth* c, const pxb_collider* colliders, uint32_t n_coll
     /* cloth_solver.h:162-194: prologue */
     const uint32_t n = c->n_particles;
     if (n == 0 || h <= 0.0f) return 0;
-    for (uint32_t k = 0; k < n_colliders; ++k) {
-        if (colliders[k].enabled && colliders[k].type != PXB_SHAPE_SPHERE &&
-            colliders[k].type != PXB_SHAPE_BOX && colliders[k].type != PXB_SHAPE_CAPSULE) {
+    for (uint32_t k = 0; k < n_colliders; ++k)
+        if (colliders[k].enabled && (colliders[k].type < PXB_SHAPE_SPHERE || colliders[k].type > PXB_SHAPE_CONVEX_HULL))
             return -1;
-        }
-    }
     const pxb_cloth_params* P = &c->params;
     uint32_t steps = P->substeps ? P->substeps : substeps;
     if (steps < 1) steps = 1;
@@ -493,7 +903,9 @@ int orc_solve_cloth(orc_cloth* c, const pxb_collider* colliders, uint32_t n_coll
                     }
                     v3 pp = ld(p->position), normal = mk(0, 0, 0);
                     float depth = 0.0f;
-                    if (project_particle(col, P->thickness, &pp, &normal, &depth) != 1) continue;
+                    /* prev_position is this substep's start (cloth_solver.h:398-403) */
+                    const v3 start = ld(p->prev_position);
+                    if (project_particle(col, P->thickness, &pp, &normal, &depth, &start) != 1) continue;
                     st(p->position, pp);
                     contact_normal[i] = add(contact_normal[i], normal);
                     contact_depth[i] += depth;
@@ -662,12 +1074,9 @@ int orc_solve_strands(orc_strand_set* s, const pxb_collider* colliders, uint32_t
     /* strand_solver.h:124-155: prologue */
     const uint32_t n = s->n_particles;
     if (n == 0 || s->n_strands == 0 || h <= 0.0f) return 0;
-    for (uint32_t k = 0; k < n_colliders; ++k) {
-        if (colliders[k].enabled && colliders[k].type != PXB_SHAPE_SPHERE &&
-            colliders[k].type != PXB_SHAPE_BOX && colliders[k].type != PXB_SHAPE_CAPSULE) {
+    for (uint32_t k = 0; k < n_colliders; ++k)
+        if (colliders[k].enabled && (colliders[k].type < PXB_SHAPE_SPHERE || colliders[k].type > PXB_SHAPE_CONVEX_HULL))
             return -1;
-        }
-    }
     const pxb_strand_params* P = &s->params;
     uint32_t steps = P->substeps ? P->substeps : substeps;
     if (steps < 1) steps = 1;
@@ -802,7 +1211,8 @@ int orc_solve_strands(orc_strand_set* s, const pxb_collider* colliders, uint32_t
                 for (uint32_t k = 0; k < n_colliders; ++k) {
                     v3 pp = ld(p->position), normal = mk(0, 0, 0);
                     float depth = 0.0f;
-                    if (project_particle(&colliders[k], P->thickness, &pp, &normal, &depth) != 1)
+                    const v3 start = ld(p->prev_position); /* strand_solver.h:283-284 */
+                    if (project_particle(&colliders[k], P->thickness, &pp, &normal, &depth, &start) != 1)
                         continue;
                     st(p->position, pp);
                     if (contacted[i] == 0 || depth > contact_depth[i]) {

@@ -50,13 +50,34 @@ typedef struct orc_cloth {
     float bounds_max[3];
 } orc_cloth;
 
-/* cloth::solve_cloth (cloth_solver.h:158-460), serial dispatch. Returns 0, or -1 when a
- * collider is a mesh / hull (not restated here). */
+/* cloth::solve_cloth (cloth_solver.h:158-460), serial dispatch. Returns 0, or -1 for a
+ * collider of unknown shape type. */
 int orc_solve_cloth(orc_cloth* c, const pxb_collider* colliders, uint32_t n_colliders,
                     const float gravity[3], uint32_t substeps, uint32_t iterations, float h);
 
+/* Collider geometry, registered under the ids pxb_collider::geometry names (1..1023). The hull
+ * is kept as given and posed per call, as collision::world_posed_hull does; the mesh gets a
+ * MeshBVH built by orc_bvh_build. */
+int orc_geometry_set_hull(uint32_t id, const pxb_hull_desc* desc);
+int orc_geometry_set_mesh(uint32_t id, const pxb_mesh_desc* desc);
+void orc_geometry_clear(void);
+
+/* One MeshBVH node (mesh_bvh.h): bounds, children (left < 0 for a leaf) and the leaf's range of
+ * the triangle order. */
+typedef struct orc_bvh_node {
+    float mn[3], mx[3];
+    int32_t left, right;
+    uint32_t tri_start, tri_count;
+} orc_bvh_node;
+
+/* MeshBVH::build (mesh_bvh.h) over n_tris triangles: writes the nodes (at most 2 * n_tris, root
+ * first, in creation order) and the triangle order, returns the node count. In
+ * oracle/xpbd_oracle_bvh.cpp: the split is std::nth_element, as in the reference. */
+uint32_t orc_bvh_build(const float* vertices, const uint32_t* indices, uint32_t n_tris,
+                       orc_bvh_node* nodes, uint32_t* order);
+
 /* cloth::project_particle (cloth_collision.h:386-420). Returns 1 on hit, 0 on miss, -1 for an
- * unsupported shape type. motion_start may be NULL. */
+ * unknown shape type. motion_start may be NULL. */
 int orc_project_particle(const pxb_collider* collider, float thickness, float p[3],
                          float normal_out[3], float* depth_out, const float* motion_start);
 
@@ -91,7 +112,8 @@ typedef struct orc_strand_set {
     float bounds_max[3];
 } orc_strand_set;
 
-/* hair::solve_strands (strand_solver.h:121-327). Returns 0, or -1 for a mesh / hull collider. */
+/* hair::solve_strands (strand_solver.h:121-327). Returns 0, or -1 for a collider of unknown
+ * shape type. */
 int orc_solve_strands(orc_strand_set* s, const pxb_collider* colliders, uint32_t n_colliders,
                       const float gravity[3], uint32_t substeps, uint32_t iterations, float h);
 

@@ -28,17 +28,20 @@ COLLIDER = np.dtype([("type", "<i4"), ("enabled", "<i4"), ("position", "<f4", 3)
                      ("local_rotation", "<f4", 4), ("radius", "<f4"), ("half_extents", "<f4", 3),
                      ("capsule_radius", "<f4"), ("capsule_half_height", "<f4"),
                      ("capsule_axis", "<i4"), ("sweep", "<f4", 3), ("end_orientation", "<f4", 4),
-                     ("bounds_min", "<f4", 3), ("bounds_max", "<f4", 3)])
+                     ("bounds_min", "<f4", 3), ("bounds_max", "<f4", 3),
+                     ("geometry", "<u4"), ("geometry_scale", "<f4")])
 GRAVITY_SOURCE = np.dtype([("centre", "<f4", 3), ("strength", "<f4"), ("radius", "<f4"),
                            ("range", "<f4")])
 FRAME_RESULT = np.dtype([("bounds_min", "<f4", 3), ("bounds_max", "<f4", 3),
                          ("max_speed", "<f4"), ("time", "<f4")])
 
 assert PARTICLE.itemsize == 40 and CONSTRAINT.itemsize == 16 and ANCHOR.itemsize == 48
-assert STRAND.itemsize == 64 and COLLIDER.itemsize == 144 and TETHER.itemsize == 12
+assert STRAND.itemsize == 64 and COLLIDER.itemsize == 152 and TETHER.itemsize == 12
 
 SHAPE_SPHERE, SHAPE_BOX, SHAPE_CAPSULE, SHAPE_TRIANGLE_MESH, SHAPE_CONVEX_HULL = range(5)
 
+(PXB_OK, PXB_ERR_INVALID_ARGUMENT, PXB_ERR_UNSUPPORTED, PXB_ERR_CUDA, PXB_ERR_OUT_OF_MEMORY,
+ PXB_ERR_INVALID_HANDLE, PXB_ERR_DEVICE_STATUS, PXB_ERR_TOO_LARGE) = range(8)
 STATUS_NAMES = {0: "PXB_OK", 1: "PXB_ERR_INVALID_ARGUMENT", 2: "PXB_ERR_UNSUPPORTED",
                 3: "PXB_ERR_CUDA", 4: "PXB_ERR_OUT_OF_MEMORY", 5: "PXB_ERR_INVALID_HANDLE",
                 6: "PXB_ERR_DEVICE_STATUS", 7: "PXB_ERR_TOO_LARGE"}
@@ -162,6 +165,18 @@ class WarmStartDesc(C.Structure):
 
 WARM_RESULT = np.dtype([("residual", "<f4"), ("fallbacks", "<u4"), ("substeps", "<u4"),
                         ("extra_iterations", "<u4")])
+
+
+class HullDesc(C.Structure):
+    """pxb_hull_desc (geometry::ConvexHull's arrays)."""
+    _fields_ = [("vertices", P), ("n_vertices", u32), ("face_planes", P), ("n_faces", u32),
+                ("face_starts", P), ("face_vertices", P)]
+
+
+class MeshDesc(C.Structure):
+    """pxb_mesh_desc (geometry::TriangleMesh's vertices, indices and face normals)."""
+    _fields_ = [("vertices", P), ("n_vertices", u32), ("indices", P), ("n_indices", u32),
+                ("normals", P)]
 
 
 class ClothDesc(C.Structure):

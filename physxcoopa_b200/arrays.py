@@ -219,7 +219,72 @@ def _world_bounds(c):
             lo = np.minimum(lo, w)
             hi = np.maximum(hi, w)
         return lo, hi
+    if c["type"] in (A.SHAPE_TRIANGLE_MESH, A.SHAPE_CONVEX_HULL):
+        raise ValueError("mesh and hull bounds need the geometry: use hull_collider / mesh_collider")
     raise ValueError("unsupported collider type")
+
+
+def _posed_bounds(lo_local, hi_local, center, orient, scale):
+    """world_bounds of a TriangleMesh / ConvexHull (shape.h:216-225): the 8 corners of the local
+    bounds through rotation * scale, plus the posed centre, re-fitted (AABB::transform)."""
+    ax, ay, az = _axes(orient)
+    s = np.float32(scale)
+    lo = np.full(3, np.finfo(np.float32).max, np.float32)
+    hi = -lo
+    for i in range(8):
+        corner = np.array([hi_local[0] if i & 1 else lo_local[0], hi_local[1] if i & 2 else lo_local[1],
+                           hi_local[2] if i & 4 else lo_local[2]], np.float32)
+        w = ((ax * s) * corner[0] + (ay * s) * corner[1]) + ((az * s) * corner[2] + center)
+        lo = np.minimum(lo, w)
+        hi = np.maximum(hi, w)
+    return lo.astype(np.float32), hi.astype(np.float32)
+
+
+class Hull:
+    """geometry::ConvexHull's arrays (physxcoopa/geometry/convex_hull.h:41-57): vertices, face
+    planes (outward unit normal, offset), and each face's vertex indices CCW about its normal."""
+
+    def __init__(self, vertices, face_planes, face_starts, face_vertices):
+        self.vertices = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        self.face_planes = np.ascontiguousarray(face_planes, np.float32).reshape(-1, 4)
+        self.face_starts = np.ascontiguousarray(face_starts, np.uint32).reshape(-1)
+        self.face_vertices = np.ascontiguousarray(face_vertices, np.uint32).reshape(-1)
+
+    def desc(self):
+        d = A.HullDesc()
+        d.vertices = A.ptr(self.vertices)
+        d.n_vertices = len(self.vertices)
+        d.face_planes = A.ptr(self.face_planes)
+        d.n_faces = len(self.face_planes)
+        d.face_starts = A.ptr(self.face_starts)
+        d.face_vertices = A.ptr(self.face_vertices)
+        return d
+
+    def local_bounds(self):
+        return self.vertices.min(axis=0), self.vertices.max(axis=0)
+
+
+class Mesh:
+    """geometry::TriangleMesh's vertices, triangle indices and face normals
+    (physxcoopa/geometry/triangle_mesh.h:70-96). normals None: computed on registration as
+    TriangleMesh::from_triangles does."""
+
+    def __init__(self, vertices, indices, normals=None):
+        self.vertices = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        self.indices = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        self.normals = None if normals is None else np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+
+    def desc(self):
+        d = A.MeshDesc()
+        d.vertices = A.ptr(self.vertices)
+        d.n_vertices = len(self.vertices)
+        d.indices = A.ptr(self.indices)
+        d.n_indices = len(self.indices)
+        d.normals = A.ptr(self.normals)
+        return d
+
+    def local_bounds(self):
+        return self.vertices.min(axis=0), self.vertices.max(axis=0)
 
 
 def make_collider(shape_type, position=(0, 0, 0), orientation=IDENTITY, *, radius=0.5,
@@ -264,6 +329,40 @@ def box(half_extents, position=(0, 0, 0), orientation=IDENTITY, **kw):
 def capsule(radius, half_height, position=(0, 0, 0), orientation=IDENTITY, axis=2, **kw):
     return make_collider(A.SHAPE_CAPSULE, position, orientation, capsule_radius=radius,
                          capsule_half_height=half_height, capsule_axis=axis, **kw)
+
+
+def _geometry_collider(shape_type, geometry_id, geometry, position, orientation, scale, local_center,
+                       local_rotation, enabled):
+    c = np.zeros((), A.COLLIDER)
+    c["type"] = shape_type
+    c["enabled"] = 1 if enabled else 0
+    c["position"] = position
+    c["orientation"] = orientation
+    c["local_center"] = local_center
+    c["local_rotation"] = local_rotation
+    c["end_orientation"] = orientation
+    c["geometry"] = geometry_id
+    c["geometry_scale"] = scale
+    center = (np.asarray(position, np.float32) + _qrot(orientation, local_center)).astype(np.float32)
+    lo, hi = geometry.local_bounds()
+    c["bounds_min"], c["bounds_max"] = _posed_bounds(lo, hi, center, _qmul(orientation, local_rotation), scale)
+    return c
+
+
+def hull_collider(geometry_id, hull, position=(0, 0, 0), orientation=IDENTITY, *, scale=1.0,
+                  local_center=(0, 0, 0), local_rotation=IDENTITY, enabled=True):
+    """A ConvexHull collider (Shape::make_hull, shape.h:147-155) naming the geometry id a context
+    returned for `hull`, with ClothCollider::bounds as world_bounds computes it."""
+    return _geometry_collider(A.SHAPE_CONVEX_HULL, geometry_id, hull, position, orientation, scale,
+                              local_center, local_rotation, enabled)
+
+
+def mesh_collider(geometry_id, mesh, position=(0, 0, 0), orientation=IDENTITY, *, scale=1.0,
+                  local_center=(0, 0, 0), local_rotation=IDENTITY, enabled=True):
+    """A TriangleMesh collider (Shape::make_mesh, shape.h:138-145; meshes are static, so it is
+    never swept) naming the geometry id a context returned for `mesh`."""
+    return _geometry_collider(A.SHAPE_TRIANGLE_MESH, geometry_id, mesh, position, orientation, scale,
+                              local_center, local_rotation, enabled)
 
 
 def collider_array(records):

@@ -258,7 +258,7 @@ __device__ __forceinline__ void cluster_or_block_sync() {
     else __syncthreads();
 }
 
-template <int kMaxThreads, int CL, bool kWarm>
+template <int kMaxThreads, int CL, bool kWarm, bool kGeo>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders,
@@ -795,7 +795,10 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                         }
                         f3 n = mk(0.0f, 0.0f, 0.0f);
                         float depth = 0.0f;
-                        if (!project_particle(c, thickness, p, n, depth)) continue;
+                        // a mesh's swept test starts from the substep's start (cloth_solver.h:398-403)
+                        const bool mesh = kGeo && __ldg(&c->type) == PXB_SHAPE_TRIANGLE_MESH;
+                        const f3 start = mesh ? xyz(gprv[gl]) : p;
+                        if (!project_particle<kGeo>(c, thickness, p, n, depth, start, mesh)) continue;
                         moved = true;
                         nsum = add(nsum, n);
                         dsum += depth;
@@ -910,7 +913,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
 // ------------------------------------------------------------------------------------------
 
 __global__ void project_points_kernel(const PxbDevCollider* __restrict__ c, float thickness,
-                                      const float* __restrict__ pts, int n, float* __restrict__ out,
+                                      const float* __restrict__ pts, const float* __restrict__ starts,
+                                      int n, float* __restrict__ out,
                                       float* __restrict__ normals, float* __restrict__ depths,
                                       int32_t* __restrict__ hits) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -918,7 +922,8 @@ __global__ void project_points_kernel(const PxbDevCollider* __restrict__ c, floa
     f3 p = mk(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
     f3 nn = mk(0, 0, 0);
     float d = 0.0f;
-    const bool hit = project_particle(c, thickness, p, nn, d);
+    const f3 start = starts ? mk(starts[3 * i], starts[3 * i + 1], starts[3 * i + 2]) : p;
+    const bool hit = project_particle<true>(c, thickness, p, nn, d, start, starts != nullptr);
     out[3 * i] = p.x; out[3 * i + 1] = p.y; out[3 * i + 2] = p.z;
     normals[3 * i] = nn.x; normals[3 * i + 1] = nn.y; normals[3 * i + 2] = nn.z;
     depths[i] = d;
@@ -994,7 +999,7 @@ __device__ __forceinline__ void grid_sync(PxbGridSync* gs, unsigned int& epoch, 
     __syncthreads();
 }
 
-template <int kThreads>
+template <int kThreads, bool kGeo>
 __global__ void __launch_bounds__(kThreads, 1)
 cloth_grid_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders, const pxb_gravity_source* __restrict__ sources,
@@ -1192,7 +1197,9 @@ cloth_grid_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                         }
                         f3 nn = mk(0.0f, 0.0f, 0.0f);
                         float depth = 0.0f;
-                        if (!project_particle(c, thickness, p, nn, depth)) continue;
+                        const bool mesh = kGeo && __ldg(&c->type) == PXB_SHAPE_TRIANGLE_MESH;
+                        const f3 start = mesh ? xyz(gprv[gl]) : p;
+                        if (!project_particle<kGeo>(c, thickness, p, nn, depth, start, mesh)) continue;
                         moved = true;
                         nsum = add(nsum, nn);
                         dsum += depth;
@@ -1268,22 +1275,31 @@ cloth_grid_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
 }
 
-cudaError_t launch_cloth_grid(const PxbClothDev* cloths, const PxbClothStep* steps, const PxbDevCollider* colliders,
-                              const pxb_gravity_source* sources, const int32_t* order, PxbFrameResult* results,
-                              uint32_t* err, PxbGridSync* gs, int slot, int n_sms, cudaStream_t stream) {
+template <bool kGeo>
+static cudaError_t launch_grid_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
+                                       const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                                       const int32_t* order, PxbFrameResult* results, uint32_t* err,
+                                       PxbGridSync* gs, int slot, int n_sms, cudaStream_t stream) {
     constexpr int kThreads = 1024;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cloth_grid_kernel<kThreads>, kThreads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cloth_grid_kernel<kThreads, kGeo>, kThreads, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     unsigned int blocks = static_cast<unsigned int>(n_sms);  // one CTA per SM: every one co-resident
     void* args[] = {(void*)&cloths, (void*)&steps, (void*)&colliders, (void*)&sources, (void*)&order,
                     (void*)&results, (void*)&err, (void*)&gs, (void*)&slot};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(cloth_grid_kernel<kThreads>), dim3(blocks),
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(cloth_grid_kernel<kThreads, kGeo>), dim3(blocks),
                                        dim3(kThreads), args, 0, stream);
 }
 
-template <int kMaxThreads, int CL, bool kWarm>
+cudaError_t launch_cloth_grid(const PxbClothDev* cloths, const PxbClothStep* steps, const PxbDevCollider* colliders,
+                              const pxb_gravity_source* sources, const int32_t* order, PxbFrameResult* results,
+                              uint32_t* err, PxbGridSync* gs, int slot, int n_sms, cudaStream_t stream, bool geo) {
+    return geo ? launch_grid_variant<true>(cloths, steps, colliders, sources, order, results, err, gs, slot, n_sms, stream)
+               : launch_grid_variant<false>(cloths, steps, colliders, sources, order, results, err, gs, slot, n_sms, stream);
+}
+
+template <int kMaxThreads, int CL, bool kWarm, bool kGeo>
 static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
                                   const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                   const int32_t* order, PxbFrameResult* results, uint32_t* err,
@@ -1295,10 +1311,10 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     if (e != cudaSuccess) return e;
     if (dev < 64 && !(configured >> dev & 1ull)) {
         cudaFuncAttributes fa;
-        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm>);
+        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm, kGeo>);
         if (e != cudaSuccess) return e;
         if (fa.sharedSizeBytes > static_cast<size_t>(kClothStaticSmem)) return cudaErrorInvalidConfiguration;
-        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm>,
+        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm, kGeo>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
         if (e != cudaSuccess) return e;
         configured |= 1ull << dev;
@@ -1315,7 +1331,7 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm>, cloths, steps, colliders,
+    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm, kGeo>, cloths, steps, colliders,
                               sources, order, results, err, wsteps, mlp, wres);
 }
 
@@ -1328,26 +1344,49 @@ int cloth_variant_registers(int variant) {
     const int v = variant < 0 ? 0 : (variant >= kClothVariants ? kClothVariants - 1 : variant);
     if (!regs[v]) {
         cudaFuncAttributes fa;
-        cudaError_t e = v == 0 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<512, 1, false>)
-                               : (v == 1 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<768, 1, false>)
-                                         : cudaFuncGetAttributes(&fa, cloth_step_kernel<1024, 1, false>));
+        cudaError_t e = v == 0 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<512, 1, false, false>)
+                               : (v == 1 ? cudaFuncGetAttributes(&fa, cloth_step_kernel<768, 1, false, false>)
+                                         : cudaFuncGetAttributes(&fa, cloth_step_kernel<1024, 1, false, false>));
         regs[v] = e == cudaSuccess ? fa.numRegs : 255;
     }
     return regs[v];
 }
 
-template <int kMaxThreads, bool kWarm>
+template <int kMaxThreads, bool kWarm, bool kGeo>
 static cudaError_t launch_cl(int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
                              int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
                              const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres) {
     switch (cluster) {
-        case 1: return launch_variant<kMaxThreads, 1, kWarm>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 2: return launch_variant<kMaxThreads, 2, kWarm>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 4: return launch_variant<kMaxThreads, 4, kWarm>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 8: return launch_variant<kMaxThreads, 8, kWarm>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 1: return launch_variant<kMaxThreads, 1, kWarm, kGeo>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 2: return launch_variant<kMaxThreads, 2, kWarm, kGeo>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 4: return launch_variant<kMaxThreads, 4, kWarm, kGeo>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 8: return launch_variant<kMaxThreads, 8, kWarm, kGeo>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
         default: return cudaErrorInvalidValue;
+    }
+}
+
+// Launches carrying a mesh or hull collider: the same dispatch over the kGeo instantiations.
+static cudaError_t launch_geo(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
+                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                              const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
+                              int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
+                              const unsigned char* mlp, PxbWarmResult* wres) {
+    if (wsteps) {
+        if (variant == 0) {
+            if (threads > 512) threads = 512;
+            return launch_cl<512, true, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        }
+        if (threads > 1024) threads = 1024;
+        if (threads < 128) threads = 128;
+        return launch_cl<1024, true, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+    }
+    if (threads > cloth_variant_threads(variant)) threads = cloth_variant_threads(variant);
+    switch (variant) {
+        case 0: return launch_cl<512, false, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        case 1: return launch_cl<768, false, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        default: return launch_cl<1024, false, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
     }
 }
 
@@ -1356,33 +1395,35 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
                               const pxb_gravity_source* sources, const int32_t* order,
                               PxbFrameResult* results, uint32_t* err, int n_cloths, int threads,
                               int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres) {
+                              const unsigned char* mlp, PxbWarmResult* wres, bool geo) {
     if (n_cloths <= 0) return cudaSuccess;
+    if (geo) return launch_geo(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths,
+                               threads, smem_bytes, stream, wsteps, mlp, wres);
     if (wsteps) {
         // warm-start kernels: the 512-thread variant (registers for the network epilogue) or
         // the 1024-thread one
         if (variant == 0) {
             if (threads > 512) threads = 512;
-            return launch_cl<512, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+            return launch_cl<512, true, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
         }
         if (threads > 1024) threads = 1024;
         if (threads < 128) threads = 128;
-        return launch_cl<1024, true>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        return launch_cl<1024, true, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
     }
     if (threads > cloth_variant_threads(variant)) threads = cloth_variant_threads(variant);
     switch (variant) {
-        case 0: return launch_cl<512, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
-        case 1: return launch_cl<768, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
-        default: return launch_cl<1024, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        case 0: return launch_cl<512, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        case 1: return launch_cl<768, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        default: return launch_cl<1024, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
     }
 }
 
 cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness, const float* pts,
-                                  int n, float* out, float* normals, float* depths, int32_t* hits,
-                                  cudaStream_t stream) {
+                                  const float* starts, int n, float* out, float* normals, float* depths,
+                                  int32_t* hits, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     const int tb = 256;
-    project_points_kernel<<<(n + tb - 1) / tb, tb, 0, stream>>>(collider, thickness, pts, n, out,
+    project_points_kernel<<<(n + tb - 1) / tb, tb, 0, stream>>>(collider, thickness, pts, starts, n, out,
                                                                  normals, depths, hits);
     return cudaGetLastError();
 }

@@ -121,9 +121,290 @@ __device__ __noinline__ bool project_pose(const PxbDevCollider* __restrict__ c, 
     return true;
 }
 
+// util::safe_normalize (math.h:46-50).
+__device__ __forceinline__ f3 safe_normalize(f3 v) {
+    const float l2 = dot(v, v);
+    if (l2 < PXB_EPSILON * PXB_EPSILON) return mk(0.0f, 0.0f, 0.0f);
+    return mul(v, 1.0f / sqrtf(l2));
+}
+__device__ __forceinline__ f3 neg(f3 a) { return mk(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ f3 ldx(const float4* p) {
+    const float4 v = __ldg(p);
+    return mk(v.x, v.y, v.z);
+}
+// Rotation of v by the unit quaternion q (x, y, z, w): v + 2*(w*(u x v) + u x (u x v)).
+__device__ __forceinline__ f3 qrot4(const float* q, f3 v) {
+    const f3 u = mk(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+    const float w = __ldg(q + 3);
+    const f3 uv = cross(u, v);
+    const f3 uuv = cross(u, uv);
+    return add(v, mul(add(mul(uv, w), uuv), 2.0f));
+}
+
+// ConvexHull branch of project_at_pose_ (cloth_collision.h:342-354): collision::hull_vs_sphere
+// (sat_hull.h:649-688) with the particle as a probe sphere of radius `thickness`, over the hull
+// posed for this step on the host (PxbDevCollider::geo), then point + normal * thickness.
+__device__ __noinline__ bool project_hull(const PxbDevCollider* __restrict__ c, float thickness, f3& p,
+                                          f3& normal_out, float& depth_out) {
+    const float4* __restrict__ g = c->geo;
+    const int F = __ldg(&c->geo_count), V = __ldg(&c->geo_aux);
+    int best_face = 0;
+    float best_dist = -3.40282347e38f;  // -numeric_limits<float>::max()
+    bool any_positive = false;
+    for (int f = 0; f < F; ++f) {
+        const float4 pl = __ldg(&g[f]);
+        const float dist = dot(mk(pl.x, pl.y, pl.z), p) - pl.w;
+        if (dist > 0.0f) any_positive = true;
+        if (dist > best_dist) {
+            best_dist = dist;
+            best_face = f;
+        }
+    }
+    const float4 npl = __ldg(&g[best_face]);
+    const f3 n = mk(npl.x, npl.y, npl.z);
+    const float4 span = __ldg(&g[F + best_face]);
+    const int first = __float_as_int(span.x), count = __float_as_int(span.y);
+    const float4* __restrict__ poly = g + 2 * F + first;
+    const float4* __restrict__ edge_out = g + 2 * F + V + first;
+    // closest_point_on_convex_polygon_ (sat_hull.h:601-627)
+    const f3 p0 = ldx(&poly[0]);
+    const float plane_d = dot(n, p0);
+    const f3 proj = sub(p, mul(n, dot(n, p) - plane_d));
+    bool inside = true;
+    for (int i = 0; i < count && inside; ++i)
+        if (dot(ldx(&edge_out[i]), sub(proj, ldx(&poly[i]))) > 1e-6f) inside = false;
+    f3 point = proj;
+    if (!inside) {
+        point = p0;
+        float best_d2 = 3.40282347e38f;
+        f3 a = p0;
+        for (int i = 0; i < count; ++i) {
+            const f3 b = ldx(&poly[i + 1 == count ? 0 : i + 1]);
+            const f3 ab = sub(b, a);
+            const float len2 = dot(ab, ab);
+            const float t = len2 > 1e-12f ? clamp01(dot(sub(proj, a), ab) / len2) : 0.0f;
+            const f3 q = add(a, mul(ab, t));
+            const f3 dq = sub(proj, q);
+            const float d2 = dot(dq, dq);
+            if (d2 < best_d2) {
+                best_d2 = d2;
+                point = q;
+            }
+            a = b;
+        }
+    }
+    f3 nrm;
+    float pen;
+    if (!any_positive) {
+        const f3 diff = sub(point, p);
+        const float dist = len(diff);
+        nrm = dist > PXB_EPSILON ? divs(diff, dist) : n;
+        pen = thickness + (-best_dist);
+    } else {
+        const f3 diff = sub(p, point);
+        const float dist = len(diff);
+        if (dist > thickness) return false;
+        nrm = dist > PXB_EPSILON ? divs(diff, dist) : n;
+        pen = thickness - dist;
+    }
+    p = add(point, mul(nrm, thickness));
+    normal_out = nrm;
+    depth_out = pen;
+    return true;
+}
+
+// collision::closest_point_on_triangle (mesh_contact.h:63-99), Ericson's region analysis.
+__device__ __forceinline__ f3 closest_on_triangle(f3 p, f3 a, f3 b, f3 c) {
+    const f3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f) return a;
+    const f3 bp = sub(p, b);
+    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) return b;
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) return add(a, smul(d1 / (d1 - d3), ab));
+    const f3 cp = sub(p, c);
+    const float d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6) return c;
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) return add(a, smul(d2 / (d2 - d6), ac));
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f)
+        return add(b, smul((d4 - d3) / ((d4 - d3) + (d5 - d6)), sub(c, b)));
+    const float denom = 1.0f / (va + vb + vc);
+    const float v = vb * denom, w = vc * denom;
+    return add(add(a, mul(ab, v)), mul(ac, w));
+}
+
+// geometry::ray_vs_triangle (ray.h:205-228), Moller-Trumbore.
+__device__ __forceinline__ bool ray_triangle(f3 o, f3 dir, float max_d, f3 a, f3 b, f3 c, float& t) {
+    const f3 e1 = sub(b, a), e2 = sub(c, a);
+    const f3 pvec = cross(dir, e2);
+    const float det = dot(e1, pvec);
+    if (det > -PXB_EPSILON && det < PXB_EPSILON) return false;
+    const float inv_det = 1.0f / det;
+    const f3 tvec = sub(o, a);
+    const float u = dot(tvec, pvec) * inv_det;
+    if (u < 0.0f || u > 1.0f) return false;
+    const f3 qvec = cross(tvec, e1);
+    const float v = dot(dir, qvec) * inv_det;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    const float cand = dot(e2, qvec) * inv_det;
+    if (cand < 0.0f || cand > max_d) return false;
+    t = cand;
+    return true;
+}
+
+// Ray::intersect (ray.h:47-60), the slab test MeshBVH::raycast prunes with; inv = 1 / (dir + 1e-9).
+__device__ __forceinline__ bool ray_box(f3 o, f3 inv, float max_d, float4 na, float4 nb) {
+    const float t0x = (na.x - o.x) * inv.x, t0y = (na.y - o.y) * inv.y, t0z = (na.z - o.z) * inv.z;
+    const float t1x = (nb.x - o.x) * inv.x, t1y = (nb.y - o.y) * inv.y, t1z = (nb.z - o.z) * inv.z;
+    // glm::min / glm::max, then std::max / std::min over {x, y, z, bound} (first extreme kept)
+    float t_near = minr(t0x, t1x);
+    float m = minr(t0y, t1y);
+    if (t_near < m) t_near = m;
+    m = minr(t0z, t1z);
+    if (t_near < m) t_near = m;
+    if (t_near < 0.0f) t_near = 0.0f;
+    float t_far = maxr(t0x, t1x);
+    m = maxr(t0y, t1y);
+    if (m < t_far) t_far = m;
+    m = maxr(t0z, t1z);
+    if (m < t_far) t_far = m;
+    if (max_d < t_far) t_far = max_d;
+    return !(t_far < t_near);
+}
+
+// TriangleMesh branch of project_at_pose_ (cloth_collision.h:205-340), in the mesh's own frame:
+// the swept crossing test (a MeshBVH::raycast from the substep's start, gated by the motion's
+// length), then the proximity query (MeshBVH::query over the thickness box). Both walk the
+// hierarchy depth first, left child before right, which is MeshBVH's recursion order, so every
+// tie between equally near triangles resolves as in the reference.
+__device__ __noinline__ bool project_mesh(const PxbDevCollider* __restrict__ c, float thickness, f3& p,
+                                          f3& normal_out, float& depth_out, f3 start, bool has_start) {
+    const int n_nodes = __ldg(&c->geo_count);
+    if (n_nodes == 0) return false;  // TriangleMesh::empty()
+    const float4* __restrict__ nodes = c->nodes;
+    const float4* __restrict__ tris = c->geo;
+    const f3 origin = ld3(c->origin);
+    const float scale = __ldg(&c->scale);
+    const f3 local_p = divs(qrot4(c->qi, sub(p, origin)), scale);
+    const float lt = thickness / scale;
+    int stack[PXB_MESH_MAX_DEPTH + 4];
+
+    if (has_start) {
+        const f3 local_start = divs(qrot4(c->qi, sub(start, origin)), scale);
+        const f3 seg = sub(local_p, local_start);
+        const float seg_len = len(seg);
+        if (seg_len > lt) {
+            const f3 dir = divs(seg, seg_len);
+            const f3 inv = mk(1.0f / (dir.x + 1e-9f), 1.0f / (dir.y + 1e-9f), 1.0f / (dir.z + 1e-9f));
+            float best_t = seg_len;
+            int crossed = -1;
+            int sp = 0;
+            stack[sp++] = 0;
+            while (sp > 0) {
+                const int idx = stack[--sp];
+                const float4 na = __ldg(&nodes[2 * idx]), nb = __ldg(&nodes[2 * idx + 1]);
+                if (!ray_box(local_start, inv, seg_len, na, nb)) continue;
+                const int left = __float_as_int(na.w), right = __float_as_int(nb.w);
+                if (left >= 0) {
+                    stack[sp++] = right;
+                    stack[sp++] = left;
+                    continue;
+                }
+                const int t0 = -1 - left;
+                for (int j = t0; j < t0 + right; ++j) {
+                    const f3 v0 = ldx(&tris[4 * j]), v1 = ldx(&tris[4 * j + 1]), v2 = ldx(&tris[4 * j + 2]);
+                    float t = 0.0f;
+                    if ((ray_triangle(local_start, dir, seg_len, v0, v1, v2, t) ||
+                         ray_triangle(local_start, dir, seg_len, v0, v2, v1, t)) && t < best_t) {
+                        best_t = t;
+                        crossed = j;
+                    }
+                }
+            }
+            if (crossed >= 0) {
+                const f3 local_hit = add(local_start, mul(dir, best_t));
+                f3 face = safe_normalize(ldx(&tris[4 * crossed + 3]));
+                if (dot(sub(local_start, local_hit), face) < 0.0f) face = neg(face);
+                const f3 local_fixed = add(local_hit, mul(face, lt));
+                depth_out = len(sub(local_p, local_fixed)) * scale;
+                p = add(origin, qrot4(c->q, mul(local_fixed, scale)));
+                normal_out = qrot4(c->q, face);
+                return true;
+            }
+        }
+    }
+
+    const f3 qmn = mk(local_p.x - lt, local_p.y - lt, local_p.z - lt);
+    const f3 qmx = mk(local_p.x + lt, local_p.y + lt, local_p.z + lt);
+    const float lt2 = lt * lt;
+    float best_d2 = lt2;
+    f3 best_point = mk(0.0f, 0.0f, 0.0f), best_delta = mk(0.0f, 0.0f, 0.0f);
+    int best_tri = -1;
+    bool any_front = false;
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int idx = stack[--sp];
+        const float4 na = __ldg(&nodes[2 * idx]), nb = __ldg(&nodes[2 * idx + 1]);
+        // AABB::overlaps (aabb.h:35-39)
+        if (!(na.x <= qmx.x && nb.x >= qmn.x && na.y <= qmx.y && nb.y >= qmn.y && na.z <= qmx.z &&
+              nb.z >= qmn.z))
+            continue;
+        const int left = __float_as_int(na.w), right = __float_as_int(nb.w);
+        if (left >= 0) {
+            stack[sp++] = right;
+            stack[sp++] = left;
+            continue;
+        }
+        const int t0 = -1 - left;
+        for (int j = t0; j < t0 + right; ++j) {
+            const f3 v0 = ldx(&tris[4 * j]), v1 = ldx(&tris[4 * j + 1]), v2 = ldx(&tris[4 * j + 2]);
+            const f3 closest = closest_on_triangle(local_p, v0, v1, v2);
+            const f3 delta = sub(local_p, closest);
+            const float d2 = dot(delta, delta);
+            if (d2 > lt2) continue;
+            if (dot(delta, ldx(&tris[4 * j + 3])) >= 0.0f) any_front = true;
+            if (d2 > best_d2) continue;
+            best_d2 = d2;
+            best_point = closest;
+            best_delta = delta;
+            best_tri = j;
+        }
+    }
+    if (best_tri < 0) return false;
+    f3 bn;
+    if (!any_front) {
+        bn = safe_normalize(ldx(&tris[4 * best_tri + 3]));
+    } else if (best_d2 > PXB_EPSILON * PXB_EPSILON) {
+        bn = divs(best_delta, sqrtf(best_d2));
+    } else {
+        const f3 face = safe_normalize(ldx(&tris[4 * best_tri + 3]));
+        bn = dot(best_delta, face) < 0.0f ? neg(face) : face;
+    }
+    const f3 local_fixed = add(best_point, mul(bn, lt));
+    depth_out = len(sub(local_p, local_fixed)) * scale;
+    p = add(origin, qrot4(c->q, mul(local_fixed, scale)));
+    normal_out = qrot4(c->q, bn);
+    return true;
+}
+
+// cloth::project_particle (cloth_collision.h:386-420). `start` is the particle's position at
+// the start of the substep (the motion_start the solvers pass), read by the mesh branch only.
+// kGeo compiles the mesh and hull branches in: kernels whose launches carry no such collider
+// are instantiated without them, since a called function's registers count against its caller.
+template <bool kGeo>
 __device__ __forceinline__ bool project_particle(const PxbDevCollider* __restrict__ c,
-                                                 float thickness, f3& p, f3& n, float& depth) {
+                                                 float thickness, f3& p, f3& n, float& depth,
+                                                 f3 start = f3{0.0f, 0.0f, 0.0f}, bool has_start = false) {
     if (!__ldg(&c->enabled)) return false;
+    if constexpr (kGeo) {
+        const int type = __ldg(&c->type);
+        if (type == PXB_SHAPE_CONVEX_HULL) return project_hull(c, thickness, p, n, depth);
+        if (type == PXB_SHAPE_TRIANGLE_MESH) return project_mesh(c, thickness, p, n, depth, start, has_start);
+    }
     if (!__ldg(&c->two_pose)) return project_pose(c, 0, true, thickness, p, n, depth);
     f3 p0 = p, n0 = mk(0, 0, 0), p1 = p, n1 = mk(0, 0, 0);
     float d0 = 0.0f, d1 = 0.0f;

@@ -136,7 +136,45 @@ struct PxbDevCollider {
     float sweep[3];
     float bmin[3], bmax[3];
     PxbPose pose[2];
+    // ConvexHull: geo = this step's posed hull (see PxbHullStage), geo_count = faces,
+    //   geo_aux = face-vertex entries.
+    // TriangleMesh: geo = triangles in hierarchy order (PxbMeshTri), nodes = the hierarchy
+    //   (PxbMeshNode, root first), geo_count = nodes (0: empty mesh), geo_aux = its depth;
+    //   q / qi / origin / scale are project_at_pose_'s rot, inverse(rot), mesh_origin and scale
+    //   (cloth_collision.h:209-213), evaluated on the host.
+    int32_t geo_count;
+    int32_t geo_aux;
+    float q[4], qi[4];
+    float origin[3];
+    float scale;
+    const float4* geo;
+    const float4* nodes;
 };
+
+// Posed hull of one step, float4 records from PxbDevCollider::geo (F faces, V face-vertex entries):
+//   [0, F)            world face normal xyz, w = its plane offset dot(n, first vertex)
+//   [F, 2F)           x = first entry of the face (as int bits), y = its vertex count
+//   [2F, 2F + V)      world position of each face-vertex entry
+//   [2F + V, 2F + 2V) outward in-plane normal of the edge from that entry to the next
+#define PXB_HULL_MAX_FACE_VERTICES 160  // k_hull_clip_cap (sat_hull.h:157)
+#define PXB_HULL_MAX_FACES 4096
+#define PXB_HULL_MAX_ENTRIES 65536
+
+// Mesh hierarchy node: a = (min xyz, left child or -1 - first triangle for a leaf), b = (max xyz,
+// right child or the leaf's triangle count), int fields as bits.
+struct alignas(16) PxbMeshNode {
+    float mn[3];
+    int32_t left;
+    float mx[3];
+    int32_t right;
+};
+// Triangle in hierarchy order: the three vertices and TriangleMesh::triangle_normal, w unused.
+struct alignas(16) PxbMeshTri {
+    float v[3][4];
+    float n[4];
+};
+#define PXB_MESH_MAX_DEPTH 60
+#define PXB_MESH_MAX_TRIANGLES (1u << 24)
 
 // Per cloth, per step, computed on the host (the prologue of solve_cloth, cloth_solver.h:162-194).
 struct PxbClothStep {
@@ -202,6 +240,7 @@ struct PxbFrameResult {
 
 static_assert(sizeof(PxbSeg) == 32 && alignof(PxbSeg) == 16, "segment descriptor layout");
 static_assert(sizeof(PxbClothStep) == 184, "per-step record size is part of the staging contract");
-static_assert(sizeof(PxbDevCollider) == 236, "collider snapshot size is part of the staging contract");
+static_assert(sizeof(PxbDevCollider) == 312, "collider snapshot size is part of the staging contract");
+static_assert(sizeof(PxbMeshNode) == 32 && sizeof(PxbMeshTri) == 64, "mesh record layout");
 
 #endif  // PXB_INTERNAL_H

@@ -31,7 +31,7 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,
                               int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
                               const PxbWarmStep* wsteps = nullptr, const unsigned char* mlp = nullptr,
-                              PxbWarmResult* wres = nullptr);
+                              PxbWarmResult* wres = nullptr, bool geo = false);
 
 // Warm-start kernel: network warpgroups per CTA and the shared memory they borrow from the
 // lambda region (weights blob, then per warpgroup an input and an activation tile).
@@ -47,7 +47,8 @@ constexpr int kWarmUMin = kWarmTileOff + kWarmTileBytes;
 // Whole-GPU path for one cloth beyond an 8-CTA cluster: a cooperative launch of one CTA per SM.
 cudaError_t launch_cloth_grid(const PxbClothDev* cloths, const PxbClothStep* steps, const PxbDevCollider* colliders,
                               const pxb_gravity_source* sources, const int32_t* order, PxbFrameResult* results,
-                              uint32_t* err, PxbGridSync* gs, int slot, int n_sms, cudaStream_t stream);
+                              uint32_t* err, PxbGridSync* gs, int slot, int n_sms, cudaStream_t stream,
+                              bool geo = false);
 
 // Warm-start network (mlp_kernel.cu).
 int mlp_infer_smem_bytes();
@@ -61,8 +62,8 @@ cudaError_t launch_mlp_adam(pxb_mlp_weights* W, const pxb_mlp_weights* G, pxb_ml
                             float lr, float b1t, float b2t, cudaStream_t stream);
 
 cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness,
-                                  const float* pts, int n, float* out, float* normals,
-                                  float* depths, int32_t* hits, cudaStream_t stream);
+                                  const float* pts, const float* starts, int n, float* out,
+                                  float* normals, float* depths, int32_t* hits, cudaStream_t stream);
 
 // Gathers positions of the listed cloths from layout order into particle order, 3 floats per
 // particle, cloth after cloth starting at out_offsets[k] (floats).
@@ -70,9 +71,11 @@ cudaError_t launch_gather_positions(const PxbClothDev* cloths, const int32_t* or
                                     const int64_t* out_offsets, int n_cloths, float* out,
                                     cudaStream_t stream);
 
+// geo: the step's colliders include a mesh or hull (selects the kernel with those branches; a
+// launch of the cloth kernels takes the same flag).
 cudaError_t launch_strand_step(const PxbStrandDev& d, const PxbStrandStep& p,
                                const PxbDevCollider* colliders, const pxb_gravity_source* sources,
-                               cudaStream_t stream);
+                               cudaStream_t stream, bool geo = false);
 
 }  // namespace pxb
 

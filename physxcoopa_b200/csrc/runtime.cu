@@ -809,8 +809,6 @@ void pxb_make_dev_collider(const pxb_collider& c, PxbDevCollider& o) {
 static pxb_status check_colliders(pxb_context* ctx, const pxb_collider* c, uint32_t n) {
     for (uint32_t k = 0; k < n; ++k) {
         if (!c[k].enabled) continue;
-        if (c[k].type == PXB_SHAPE_TRIANGLE_MESH || c[k].type == PXB_SHAPE_CONVEX_HULL)
-            return ctx->fail(PXB_ERR_UNSUPPORTED, "mesh and convex-hull colliders are not implemented on the device path");
         if (c[k].type < 0 || c[k].type > PXB_SHAPE_CONVEX_HULL)
             return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "collider %u has an unknown shape type", k);
         if (c[k].type == PXB_SHAPE_CAPSULE && (c[k].capsule_axis < 0 || c[k].capsule_axis > 2))
@@ -852,6 +850,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     if (n_col && !sd->colliders) return fail(PXB_ERR_INVALID_ARGUMENT, "null colliders");
     if (n_src && !sd->sources) return fail(PXB_ERR_INVALID_ARGUMENT, "null sources");
     if (pxb_status s = check_colliders(this, sd->colliders, n_col)) return s;
+    ColliderStage cstage;
+    if (pxb_status s = cstage.plan(this, sd->colliders, n_col)) return s;
     if (pxb_status s = sync_registry()) return s;
 
     if (warm) {
@@ -867,7 +867,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         if (pxb_status s = grow(d_wresults, sizeof(PxbWarmResult) * n, "warm results")) return s;
     }
 
-    // --- staging layout: steps | colliders | sources | order | warm controls ---
+    // --- staging layout: steps | colliders | sources | order | warm controls | posed hulls ---
     const size_t b_steps = sizeof(PxbClothStep) * n;
     const size_t b_cols = sizeof(PxbDevCollider) * std::max<uint32_t>(n_col, 1);
     const size_t b_src = sizeof(pxb_gravity_source) * std::max<uint32_t>(n_src, 1);
@@ -875,7 +875,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     const size_t b_warm = warm ? sizeof(PxbWarmStep) * n : 0;
     const size_t o_cols = align256(b_steps), o_src = o_cols + align256(b_cols),
                  o_order = o_src + align256(b_src), o_warm = o_order + align256(b_order),
-                 total = o_warm + align256(b_warm);
+                 o_geo = o_warm + align256(b_warm), total = o_geo + align256(cstage.bytes());
     if (pxb_status s = grow_pinned(total)) return s;
     if (pxb_status s = grow(d_stage, total, "step staging")) return s;
     if (pxb_status s = grow(d_results, sizeof(PxbFrameResult) * n, "results")) return s;
@@ -886,7 +886,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     auto* hs_src = reinterpret_cast<pxb_gravity_source*>(hb + o_src);
     auto* hs_order = reinterpret_cast<int32_t*>(hb + o_order);
     auto* hs_warm = reinterpret_cast<PxbWarmStep*>(hb + o_warm);
-    for (uint32_t k = 0; k < n_col; ++k) pxb_make_dev_collider(sd->colliders[k], hs_cols[k]);
+    cstage.fill(this, sd->colliders, n_col, hs_cols, reinterpret_cast<float4*>(hb + o_geo),
+                reinterpret_cast<const float4*>(static_cast<char*>(d_stage.p) + o_geo));
     if (n_src) std::memcpy(hs_src, sd->sources, sizeof(pxb_gravity_source) * n_src);
     // Launch slots grouped by cluster size and by how many of the cloth's CTAs one SM holds
     // (shared memory, threads, registers): one launch per group, so a small cloth is not
@@ -901,6 +902,11 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         return warm ? std::min(cap, std::max(128, (e.threads + 127) & ~127)) : std::min(e.threads, cap);
     };
     for (uint32_t k = 0; k < n; ++k) fit[k] = ctas_per_sm(launch_smem(*ents[k]), launch_threads(*ents[k]), regs);
+    // cloths with a mesh or hull collider launch the kernel with those branches compiled in
+    std::vector<uint8_t> has_geo(n, 0);
+    if (sd->collider_offsets)
+        for (uint32_t k = 0; k < n; ++k)
+            has_geo[k] = cstage.any_geometry(sd->collider_offsets[k], sd->collider_offsets[k + 1] - sd->collider_offsets[k]);
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
@@ -908,6 +914,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         const size_t rx = ents[x]->ranks.size(), ry = ents[y]->ranks.size();
         if (rx != ry) return rx < ry;
         if (fit[x] != fit[y]) return fit[x] < fit[y];
+        if (has_geo[x] != has_geo[y]) return has_geo[x] < has_geo[y];
         return ents[x]->n_layout > ents[y]->n_layout;
     });
     const pxb::hm::V3 g = pxb::hm::ld(sd->gravity);
@@ -1005,18 +1012,20 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                                                reinterpret_cast<const int32_t*>(db + o_order),
                                                static_cast<PxbFrameResult*>(d_results.p), d_err,
                                                static_cast<PxbGridSync*>(d_grid.p) + (slot - n_plain),
-                                               static_cast<int>(slot), n_sms, stream);
+                                               static_cast<int>(slot), n_sms, stream, has_geo[perm[slot]] != 0);
             if (le != cudaSuccess) return cuda(le, "launch whole-GPU cloth");
             ++enqueued;
         }
     }
-    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; };
+    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; bool geo; };
     std::vector<Group> groups;
     for (uint32_t g0 = 0; g0 < n_plain;) {
         const int cluster = static_cast<int>(ents[perm[g0]]->ranks.size());
         const int group_fit = fit[perm[g0]];
-        Group G{g0, g0, cluster, 64, 0, 0.0};
-        while (G.g1 < n_plain && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster && fit[perm[G.g1]] == group_fit) {
+        const bool geo = has_geo[perm[g0]] != 0;
+        Group G{g0, g0, cluster, 64, 0, 0.0, geo};
+        while (G.g1 < n_plain && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster &&
+               fit[perm[G.g1]] == group_fit && (has_geo[perm[G.g1]] != 0) == geo) {
             const ClothEntry& e = *ents[perm[G.g1]];
             G.threads = std::max(G.threads, launch_threads(e));
             G.smem = std::max(G.smem, launch_smem(e));
@@ -1045,7 +1054,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                                            static_cast<int>(G.g1 - G.g0), G.threads, G.smem, st,
                                            warm ? reinterpret_cast<const PxbWarmStep*>(db + o_warm) + G.g0 : nullptr,
                                            warm && warm->warm_iters > 0 ? static_cast<const unsigned char*>(d_mlp.p) : nullptr,
-                                           warm ? static_cast<PxbWarmResult*>(d_wresults.p) + G.g0 : nullptr);
+                                           warm ? static_cast<PxbWarmResult*>(d_wresults.p) + G.g0 : nullptr, G.geo);
         if (le != cudaSuccess) return cuda(le, "launch cloth_step");
         ++enqueued;
     }
@@ -1070,6 +1079,11 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                            uint64_t(reinterpret_cast<uintptr_t>(d_registry.p)), uint64_t(reinterpret_cast<uintptr_t>(pinned)),
                            uint64_t(reinterpret_cast<uintptr_t>(d_grid.p)), registry_epoch})
             key.push_back(v);
+        for (uint32_t k = 0; k < n; k += 64) {  // which cloths launch the mesh / hull kernels
+            uint64_t bits = 0;
+            for (uint32_t j = k; j < std::min(n, k + 64); ++j) bits |= uint64_t(has_geo[j]) << (j - k);
+            key.push_back(bits);
+        }
         if (graph_exec && key == graph_key) {
             if (pxb_status s = cuda(cudaGraphLaunch(graph_exec, stream), "launch step graph")) return s;
             if (pxb_status s = cuda(cudaEventRecord(staged, stream), "record step graph")) return s;
@@ -1437,23 +1451,32 @@ pxb_status pxb_cloths_read_positions(pxb_context* ctx, const uint64_t* cloths, u
 pxb_status pxb_project_particles(pxb_context* ctx, const pxb_collider* collider, float thickness,
                                  const float* points_xyz, const float* motion_start_xyz, uint32_t n,
                                  float* points_out, float* normals_out, float* depths_out, int32_t* hit_out) {
-    (void)motion_start_xyz;  // consumed only by the TriangleMesh branch, which is refused
     if (!ctx || !collider || (n && (!points_xyz || !points_out || !normals_out || !depths_out || !hit_out)))
         return PXB_ERR_INVALID_ARGUMENT;
     if (pxb_status s = check_colliders(ctx, collider, 1)) return s;
-    PxbDevCollider dc;
-    pxb_make_dev_collider(*collider, dc);
-    const size_t o_pts = align256(sizeof(dc)), o_out = o_pts + align256(12 * static_cast<size_t>(n)),
-                 o_nrm = o_out + align256(12 * static_cast<size_t>(n)),
-                 o_dep = o_nrm + align256(12 * static_cast<size_t>(n)),
-                 o_hit = o_dep + align256(4 * static_cast<size_t>(n)), total = o_hit + align256(4 * static_cast<size_t>(n));
+    ColliderStage cstage;
+    if (pxb_status s = cstage.plan(ctx, collider, 1)) return s;
+    const size_t nb = static_cast<size_t>(n);
+    const size_t o_geo = align256(sizeof(PxbDevCollider)), o_pts = o_geo + align256(cstage.bytes()),
+                 o_st = o_pts + align256(12 * nb), o_out = o_st + align256(motion_start_xyz ? 12 * nb : 0),
+                 o_nrm = o_out + align256(12 * nb), o_dep = o_nrm + align256(12 * nb),
+                 o_hit = o_dep + align256(4 * nb), total = o_hit + align256(4 * nb);
     if (pxb_status s = ctx->grow(ctx->d_scratch, total, "projection scratch")) return s;
     char* b = static_cast<char*>(ctx->d_scratch.p);
-    pxb_status s = ctx->cuda(cudaMemcpyAsync(b, &dc, sizeof(dc), cudaMemcpyHostToDevice, ctx->stream), "upload collider");
-    if (!s && n) s = ctx->cuda(cudaMemcpyAsync(b + o_pts, points_xyz, 12 * static_cast<size_t>(n), cudaMemcpyHostToDevice, ctx->stream), "upload points");
+    std::vector<char> host(o_pts);
+    cstage.fill(ctx, collider, 1, reinterpret_cast<PxbDevCollider*>(host.data()),
+                reinterpret_cast<float4*>(host.data() + o_geo), reinterpret_cast<const float4*>(b + o_geo));
+    pxb_status s = ctx->cuda(cudaMemcpyAsync(b, host.data(), o_pts, cudaMemcpyHostToDevice, ctx->stream), "upload collider");
+    if (!s && n) s = ctx->cuda(cudaMemcpyAsync(b + o_pts, points_xyz, 12 * nb, cudaMemcpyHostToDevice, ctx->stream), "upload points");
+    if (!s && n && motion_start_xyz)
+        s = ctx->cuda(cudaMemcpyAsync(b + o_st, motion_start_xyz, 12 * nb, cudaMemcpyHostToDevice, ctx->stream), "upload starts");
     if (s) return s;
+    // the host staging above must outlive the copies
+    if (pxb_status s2 = ctx->cuda(cudaStreamSynchronize(ctx->stream), "upload collider")) return s2;
     cudaError_t le = launch_project_points(reinterpret_cast<const PxbDevCollider*>(b), thickness,
-                                           reinterpret_cast<const float*>(b + o_pts), static_cast<int>(n),
+                                           reinterpret_cast<const float*>(b + o_pts),
+                                           motion_start_xyz ? reinterpret_cast<const float*>(b + o_st) : nullptr,
+                                           static_cast<int>(n),
                                            reinterpret_cast<float*>(b + o_out), reinterpret_cast<float*>(b + o_nrm),
                                            reinterpret_cast<float*>(b + o_dep), reinterpret_cast<int32_t*>(b + o_hit),
                                            ctx->stream);

@@ -81,6 +81,44 @@ struct StrandEntry {
     bool has_result = false;
 };
 
+// One registered collider geometry (pxb_geometry_create_hull / _mesh); id = index + 1.
+struct GeometryEntry {
+    bool alive = false;
+    int type = 0;  // PXB_SHAPE_CONVEX_HULL or PXB_SHAPE_TRIANGLE_MESH
+    // hull: host copy, posed on the host at every step
+    std::vector<float> vertices;        // xyz
+    std::vector<float> planes;          // xyzw
+    std::vector<uint32_t> starts;       // faces + 1
+    std::vector<uint32_t> face_vertices;
+    // mesh: device copy of the hierarchy (PxbMeshNode) and triangles in its order (PxbMeshTri)
+    void* dmem = nullptr;
+    const float4* d_nodes = nullptr;
+    const float4* d_tris = nullptr;
+    int n_nodes = 0, depth = 0;
+};
+
+// The colliders of one step as the device reads them: the records plus the hulls posed for this
+// step (one block per distinct geometry and pose, shared by every record naming it).
+struct ColliderStage {
+    std::vector<size_t> hull_block;   // per record: offset of its posed hull in float4s, or SIZE_MAX
+    std::vector<size_t> block_start;  // distinct posed hulls
+    std::vector<uint32_t> block_record;
+    std::vector<uint8_t> geo;         // per record: an enabled mesh or hull naming a geometry
+    size_t n_float4 = 0;
+    // Whether records [begin, begin + count) include a mesh or hull: such a launch needs the
+    // kernel instantiated with those branches.
+    bool any_geometry(uint32_t begin, uint32_t count) const {
+        for (uint32_t k = begin; k < begin + count && k < geo.size(); ++k)
+            if (geo[k]) return true;
+        return false;
+    }
+    pxb_status plan(pxb_context* ctx, const pxb_collider* c, uint32_t n);
+    size_t bytes() const { return n_float4 * 16; }
+    // Writes the device records (out) and the posed hulls (host_geo, to be copied to dev_geo).
+    void fill(const pxb_context* ctx, const pxb_collider* c, uint32_t n, PxbDevCollider* out, float4* host_geo,
+              const float4* dev_geo) const;
+};
+
 // pxb_solve_cloth_host keeps the registration it made for a caller's arrays.
 struct HostSolveCache {
     const pxb_particle* particles;
@@ -116,6 +154,10 @@ struct pxb_context {
     std::vector<HostSolveCache> host_cache;
     std::vector<StrandEntry> strand_sets;
     std::vector<HostSolveCache> strand_cache;
+    std::vector<GeometryEntry> geometries;
+    const GeometryEntry* lookup_geometry(uint32_t id) const {
+        return id >= 1 && id <= geometries.size() && geometries[id - 1].alive ? &geometries[id - 1] : nullptr;
+    }
     int cloth_variant = 0;  // kernel block-size cap, see pxb_kernels.h (autotuned or set)
     DevBuf d_tune;          // cloth state saved across an autotune
 
@@ -126,6 +168,8 @@ struct pxb_context {
             if (e.alive && e.dmem) cudaFree(e.dmem);
         for (StrandEntry& e : strand_sets)
             if (e.alive && e.dmem) cudaFree(e.dmem);
+        for (GeometryEntry& g : geometries)
+            if (g.alive && g.dmem) cudaFree(g.dmem);
         for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune, &d_mlp, &d_mlp_io, &d_wresults, &d_rec, &d_grid})
             if (b->p) cudaFree(b->p);
         if (pinned) cudaFreeHost(pinned);

@@ -211,12 +211,6 @@ static pxb_status strands_add(pxb_context* ctx, const pxb_strand_set_desc* d, ui
     return PXB_OK;
 }
 
-namespace {
-
-void make_dev_collider_s(const pxb_collider& c, PxbDevCollider& o);
-
-}  // namespace
-
 extern "C" {
 
 void pxb_strand_params_default(pxb_strand_params* out) {
@@ -355,8 +349,6 @@ pxb_status pxb_strands_step(pxb_context* ctx, const pxb_strand_step_desc* sd) {
     for (uint32_t k = 0; k < n_col; ++k) {
         const pxb_collider& c = sd->colliders[k];
         if (!c.enabled) continue;
-        if (c.type == PXB_SHAPE_TRIANGLE_MESH || c.type == PXB_SHAPE_CONVEX_HULL)
-            return ctx->fail(PXB_ERR_UNSUPPORTED, "mesh and convex-hull colliders are not implemented on the device path");
         if (c.type < 0 || c.type > PXB_SHAPE_CONVEX_HULL || (c.type == PXB_SHAPE_CAPSULE && (c.capsule_axis < 0 || c.capsule_axis > 2)))
             return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "collider %u is malformed", k);
     }
@@ -365,14 +357,18 @@ pxb_status pxb_strands_step(pxb_context* ctx, const pxb_strand_step_desc* sd) {
         ents[k] = ctx->lookup_strands(sd->sets[k]);
         if (!ents[k]) return ctx->fail(PXB_ERR_INVALID_HANDLE, "strand set id is not live");
     }
-    // colliders and sources go up once for all sets
+    ColliderStage cstage;
+    if (pxb_status s = cstage.plan(ctx, sd->colliders, n_col)) return s;
+    // colliders, sources and posed hulls go up once for all sets
     const size_t b_cols = sizeof(PxbDevCollider) * std::max<uint32_t>(n_col, 1);
-    const size_t total = al256(b_cols) + al256(sizeof(pxb_gravity_source) * std::max<uint32_t>(n_src, 1));
+    const size_t o_geo = al256(b_cols) + al256(sizeof(pxb_gravity_source) * std::max<uint32_t>(n_src, 1));
+    const size_t total = o_geo + al256(cstage.bytes());
     if (pxb_status s = ctx->grow(ctx->d_scratch, total, "strand step staging")) return s;
     std::vector<unsigned char> host(total, 0);
-    for (uint32_t k = 0; k < n_col; ++k) make_dev_collider_s(sd->colliders[k], reinterpret_cast<PxbDevCollider*>(host.data())[k]);
-    if (n_src) std::memcpy(host.data() + al256(b_cols), sd->sources, sizeof(pxb_gravity_source) * n_src);
     char* db = static_cast<char*>(ctx->d_scratch.p);
+    cstage.fill(ctx, sd->colliders, n_col, reinterpret_cast<PxbDevCollider*>(host.data()),
+                reinterpret_cast<float4*>(host.data() + o_geo), reinterpret_cast<const float4*>(db + o_geo));
+    if (n_src) std::memcpy(host.data() + al256(b_cols), sd->sources, sizeof(pxb_gravity_source) * n_src);
     if (pxb_status s = ctx->cuda(cudaMemcpyAsync(db, host.data(), total, cudaMemcpyHostToDevice, ctx->stream), "upload strand step")) return s;
     if (pxb_status s = ctx->cuda(cudaStreamSynchronize(ctx->stream), "upload strand step")) return s;
     const pxb::hm::V3 g = pxb::hm::ld(sd->gravity);
@@ -418,7 +414,9 @@ pxb_status pxb_strands_step(pxb_context* ctx, const pxb_strand_step_desc* sd) {
         p.src_count = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k + 1] - sd->source_offsets[k]) : 0;
         cudaError_t le = launch_strand_step(e.dev, p, reinterpret_cast<const PxbDevCollider*>(db),
                                             reinterpret_cast<const pxb_gravity_source*>(db + al256(b_cols)),
-                                            ctx->stream);
+                                            ctx->stream,
+                                            cstage.any_geometry(static_cast<uint32_t>(p.col_begin),
+                                                                static_cast<uint32_t>(p.col_count)));
         if (le != cudaSuccess) return ctx->cuda(le, "launch strand_step");
         ctx->launches += 3;
         for (uint32_t q = 0; q < steps; ++q) e.time += hs;  // StrandSet::time (strand_solver.h:323)
@@ -609,6 +607,3 @@ extern "C" pxb_status pxb_host_strands_view(pxb_host_strands* set, pxb_strand_se
     return PXB_OK;
 }
 
-namespace {
-void make_dev_collider_s(const pxb_collider& c, PxbDevCollider& o) { pxb_make_dev_collider(c, o); }
-}  // namespace

@@ -93,6 +93,7 @@ __device__ __forceinline__ int fkey(float f) {
 
 }  // namespace
 
+template <bool kGeo>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 strand_step_kernel(PxbStrandDev D, PxbStrandStep P, const PxbDevCollider* __restrict__ colliders,
                    const pxb_gravity_source* __restrict__ sources) {
@@ -272,7 +273,10 @@ strand_step_kernel(PxbStrandDev D, PxbStrandStep P, const PxbDevCollider* __rest
             for (int k = 0; k < P.col_count; ++k) {
                 f3 n = mk(0.0f, 0.0f, 0.0f);
                 float depth = 0.0f;
-                if (!project_particle(&colliders[P.col_begin + k], P.thickness, p, n, depth)) continue;
+                // a mesh's swept test starts from the substep's start (strand_solver.h:283-284)
+                const PxbDevCollider* c = &colliders[P.col_begin + k];
+                const bool mesh = kGeo && __ldg(&c->type) == PXB_SHAPE_TRIANGLE_MESH;
+                if (!project_particle<kGeo>(c, P.thickness, p, n, depth, prev, mesh)) continue;
                 if (!contacted || depth > cd) {
                     cn = n;
                     cd = depth;
@@ -342,11 +346,15 @@ __global__ void strand_bounds_decode_kernel(const int* keys, float* out) {
 
 cudaError_t launch_strand_step(const PxbStrandDev& d, const PxbStrandStep& p,
                                const PxbDevCollider* colliders, const pxb_gravity_source* sources,
-                               cudaStream_t stream) {
+                               cudaStream_t stream, bool geo) {
     strand_bounds_reset_kernel<<<1, 32, 0, stream>>>(d.bounds_next);
     const int blocks = (d.n_strands + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    if (blocks > 0)
-        strand_step_kernel<<<blocks, kWarpsPerBlock * 32, 0, stream>>>(d, p, colliders, sources);
+    if (blocks > 0) {
+        if (geo)
+            strand_step_kernel<true><<<blocks, kWarpsPerBlock * 32, 0, stream>>>(d, p, colliders, sources);
+        else
+            strand_step_kernel<false><<<blocks, kWarpsPerBlock * 32, 0, stream>>>(d, p, colliders, sources);
+    }
     strand_bounds_decode_kernel<<<1, 32, 0, stream>>>(d.bounds_next, d.bounds_out);
     return cudaGetLastError();
 }

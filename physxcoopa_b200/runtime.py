@@ -59,6 +59,9 @@ SIGNATURES = {
     "pxb_solve_cloth_host": ([P, C.POINTER(A.ClothDesc), P, P, P, P, P, u32, f32p, u32, u32, f32,
                               f32p, f32p], C.c_int),
     "pxb_project_particles": ([P, P, f32, P, P, u32, P, P, P, P], C.c_int),
+    "pxb_geometry_create_hull": ([P, C.POINTER(A.HullDesc), C.POINTER(u32)], C.c_int),
+    "pxb_geometry_create_mesh": ([P, C.POINTER(A.MeshDesc), C.POINTER(u32)], C.c_int),
+    "pxb_geometry_destroy": ([P, u32], C.c_int),
     "pxb_host_cloth_make_grid": ([C.POINTER(A.GridClothDesc), C.POINTER(P)], C.c_int),
     "pxb_host_cloth_destroy": ([P], C.c_int),
     "pxb_host_cloth_pin_static": ([P, f32p, f32, C.POINTER(u32)], C.c_int),
@@ -472,18 +475,38 @@ class Context:
         self._check(self.lib.pxb_cloths_gather_positions_device(self.h, A.ptr(ids), len(ids), out_ptr, capacity),
                     "gather_positions_device")
 
-    def project_particles(self, collider, thickness, points):
+    def project_particles(self, collider, thickness, points, motion_start=None):
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
         n = len(pts)
+        st = None if motion_start is None else np.ascontiguousarray(motion_start, np.float32).reshape(-1, 3)
+        assert st is None or len(st) == n
         col = np.ascontiguousarray(np.asarray(collider, A.COLLIDER).reshape(1))
         out = np.zeros_like(pts)
         nrm = np.zeros_like(pts)
         dep = np.zeros(n, np.float32)
         hit = np.zeros(n, np.int32)
-        self._check(self.lib.pxb_project_particles(self.h, A.ptr(col), thickness, A.ptr(pts), None, n,
+        self._check(self.lib.pxb_project_particles(self.h, A.ptr(col), thickness, A.ptr(pts), A.ptr(st), n,
                                                    A.ptr(out), A.ptr(nrm), A.ptr(dep), A.ptr(hit)),
                     "project_particles")
         return hit, out, nrm, dep
+
+    # --- collider geometry ----------------------------------------------------------------
+    def create_hull(self, hull) -> int:
+        """pxb_geometry_create_hull: returns the id a ConvexHull collider names."""
+        d = hull.desc()
+        out = u32()
+        self._check(self.lib.pxb_geometry_create_hull(self.h, C.byref(d), C.byref(out)), "create_hull")
+        return int(out.value)
+
+    def create_mesh(self, mesh) -> int:
+        """pxb_geometry_create_mesh: returns the id a TriangleMesh collider names."""
+        d = mesh.desc()
+        out = u32()
+        self._check(self.lib.pxb_geometry_create_mesh(self.h, C.byref(d), C.byref(out)), "create_mesh")
+        return int(out.value)
+
+    def destroy_geometry(self, gid):
+        self._check(self.lib.pxb_geometry_destroy(self.h, gid), "destroy_geometry")
 
     # --- strand sets ----------------------------------------------------------------------
     def add_strands(self, s: StrandArrays) -> int:

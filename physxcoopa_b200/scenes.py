@@ -27,7 +27,8 @@ from typing import List, Optional
 import numpy as np
 
 from . import _abi as A
-from .arrays import ClothArrays, box, capsule, collider_array, gravity_sources, sphere
+from .arrays import (ClothArrays, Hull, Mesh, box, capsule, collider_array, gravity_sources, hull_collider,
+                     mesh_collider, sphere)
 from .runtime import HostCloth
 
 SPACING = 0.05
@@ -45,6 +46,9 @@ class ClothScene:
     iterations: int = 10
     h: float = 1.0 / 60.0
     meta: dict = field(default_factory=dict)
+    # Collider geometry (arrays.Hull / arrays.Mesh); colliders name geometry k by id k + 1, the
+    # ids a fresh context hands out when they are registered in this order.
+    geometries: list = field(default_factory=list)
 
     @property
     def vertices(self):
@@ -156,6 +160,9 @@ class StrandScene:
     iterations: int = 20
     h: float = 1.0 / 60.0
     meta: dict = field(default_factory=dict)
+    # Collider geometry (arrays.Hull / arrays.Mesh); colliders name geometry k by id k + 1, the
+    # ids a fresh context hands out when they are registered in this order.
+    geometries: list = field(default_factory=list)
 
     @property
     def particles(self):
@@ -213,3 +220,121 @@ def hanging_strands(n_strands=256, count=32, segment=0.01, tilt=0.3, seed=7, ite
     s = make_strands(list(pts))
     return StrandScene(f"hanging_strands {n_strands}x{count}", [s], [None], iterations=iterations,
                        meta={"n_strands": n_strands, "count": count})
+
+
+# ------------------------------------------------------------------------------------------
+# Collider geometry: convex hulls and triangle meshes
+# ------------------------------------------------------------------------------------------
+
+def _hull_from_faces(vertices, faces):
+    """Hull from vertex positions and faces given as vertex-index lists CCW about their outward
+    normals; the plane is (unit normal of the first three vertices, dot(normal, first vertex))."""
+    v = np.asarray(vertices, np.float32)
+    planes, starts, fv = [], [0], []
+    for f in faces:
+        a, b, c = v[f[0]], v[f[1]], v[f[2]]
+        n = np.cross(b - a, c - a).astype(np.float32)
+        n = (n / np.float32(np.sqrt(np.dot(n, n)))).astype(np.float32)
+        planes.append([n[0], n[1], n[2], np.dot(n, a)])
+        fv.extend(f)
+        starts.append(len(fv))
+    return Hull(v, np.array(planes, np.float32), starts, fv)
+
+
+def prism_hull(sides=6, radius=0.3, half_height=0.2):
+    """A right prism over a regular polygon: two polygon faces and `sides` quads."""
+    ang = 2.0 * np.pi * np.arange(sides) / sides
+    ring = np.stack([radius * np.cos(ang), radius * np.sin(ang)], 1)
+    verts = [(x, y, -half_height) for x, y in ring] + [(x, y, half_height) for x, y in ring]
+    faces = [list(range(sides, 2 * sides)), list(range(sides - 1, -1, -1))]
+    for i in range(sides):
+        j = (i + 1) % sides
+        faces.append([i, j, sides + j, sides + i])
+    return _hull_from_faces(verts, faces)
+
+
+def random_hull(n_points=24, radius=0.3, seed=0):
+    """Convex hull of points drawn on a jittered sphere: triangular faces (scipy's facets)."""
+    from scipy.spatial import ConvexHull
+    rng = np.random.default_rng(seed)
+    pts = rng.normal(size=(n_points, 3))
+    pts = (radius * pts / np.linalg.norm(pts, axis=1, keepdims=True) * rng.uniform(0.8, 1.0, (n_points, 1)))
+    pts = pts.astype(np.float32)
+    ch = ConvexHull(pts)
+    faces = []
+    for simplex, eq in zip(ch.simplices, ch.equations):
+        a, b, c = pts[simplex]
+        if np.dot(np.cross(b - a, c - a), eq[:3]) < 0:
+            simplex = simplex[[0, 2, 1]]
+        faces.append([int(k) for k in simplex])
+    return _hull_from_faces(pts, faces)
+
+
+def floor_mesh(half=2.0):
+    """Two coplanar triangles forming a square floor in the z = 0 plane, normals +Z (the
+    reference tests' two-triangle floor)."""
+    v = [(-half, -half, 0.0), (half, -half, 0.0), (half, half, 0.0), (-half, half, 0.0)]
+    return Mesh(v, [0, 1, 2, 0, 2, 3], [(0, 0, 1), (0, 0, 1)])
+
+
+def corner_mesh():
+    """A right-angled inside corner: floor z = 0 (normal +Z) and wall x = 0 (normal +X)."""
+    v = [(0, -1, 0), (1, -1, 0), (1, 1, 0), (0, 1, 0), (0, -1, 1), (0, 1, 1)]
+    return Mesh(v, [0, 1, 2, 0, 2, 3, 0, 3, 5, 0, 5, 4], [(0, 0, 1), (0, 0, 1), (1, 0, 0), (1, 0, 0)])
+
+
+def terrain_mesh(n=32, size=3.0, amp=0.15, seed=0):
+    """A height-field terrain: (n + 1)^2 vertices over a size x size square, 2 n^2 triangles
+    wound to face +Z, heights a sum of three seeded sine waves of amplitude amp. Normals are left
+    to the registration (TriangleMesh::from_triangles' formula)."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(-size / 2, size / 2, n + 1)
+    X, Y = np.meshgrid(xs, xs, indexing="xy")
+    Z = np.zeros_like(X)
+    for _ in range(3):
+        k = rng.uniform(1.0, 4.0, 2)
+        ph = rng.uniform(0, 2 * np.pi, 2)
+        Z += amp / 3 * np.sin(k[0] * X + ph[0]) * np.cos(k[1] * Y + ph[1])
+    verts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1).astype(np.float32)
+    idx = []
+    for j in range(n):
+        for i in range(n):
+            a = j * (n + 1) + i
+            b, c, d = a + 1, a + n + 2, a + n + 1
+            idx += [a, b, c, a, c, d]
+    return Mesh(verts, np.array(idx, np.uint32))
+
+
+def terrain_drape(side=32, seed=11, params=None):
+    """One sheet dropped onto a seeded terrain mesh with a rotated convex-hull rock on it and a
+    sphere: the mesh, hull and analytic branches in one collider list. Geometry ids 1 (terrain)
+    and 2 (rock)."""
+    rng = np.random.default_rng(seed)
+    terrain = terrain_mesh(24, 3.0, 0.15, seed)
+    rock = prism_hull(7, 0.25, 0.15)
+    center = (0.0, 0.0, 0.45)
+    c = _sheet(side, center, seed, [], params=params, tethers=False)
+    cols = collider_array([
+        mesh_collider(1, terrain),
+        hull_collider(2, rock, (float(rng.uniform(-0.2, 0.2)), float(rng.uniform(-0.2, 0.2)), 0.12),
+                      _random_quat(rng), scale=1.1),
+        sphere(0.15, (0.4, -0.3, 0.2)),
+    ])
+    return ClothScene(f"terrain_drape {side}x{side}", [c], [cols], meta={"side": side},
+                      geometries=[terrain, rock])
+
+
+def register_geometries(ctx, scene):
+    """Registers scene.geometries with a runtime.Context and rewrites the colliders' geometry ids
+    from the scene's numbering (geometry k is id k + 1) to the ids the context returned. Returns
+    those ids."""
+    ids = [ctx.create_hull(g) if isinstance(g, Hull) else ctx.create_mesh(g) for g in scene.geometries]
+    remap = {k + 1: gid for k, gid in enumerate(ids)}
+    for cols in scene.colliders:
+        if cols is None:
+            continue
+        for c in cols:
+            if c["type"] in (A.SHAPE_TRIANGLE_MESH, A.SHAPE_CONVEX_HULL) and int(c["geometry"]) in remap:
+                c["geometry"] = remap[int(c["geometry"])]
+    scene.geometries_ids = ids
+    return ids

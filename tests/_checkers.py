@@ -63,6 +63,10 @@ def oracle():
         lib.orc_step_strands.argtypes = [C.POINTER(OrcStrandSet), P, A.u32, f32p, P, A.u32,
                                          A.u32, A.u32, A.f32]
         lib.orc_set_strand_roots.argtypes = [C.POINTER(OrcStrandSet), P, A.u32, P, A.u32]
+        lib.orc_geometry_set_hull.argtypes = [A.u32, C.POINTER(A.HullDesc)]
+        lib.orc_geometry_set_mesh.argtypes = [A.u32, C.POINTER(A.MeshDesc)]
+        lib.orc_geometry_clear.argtypes = []
+        lib.orc_geometry_clear.restype = None
         _oracle = lib
     return _oracle
 
@@ -87,6 +91,11 @@ def ref():
         lib.pxbref_cloth_bounds.argtypes = [P, f32p]
         lib.pxbref_solve_cloth.argtypes = [P, P, A.u32, f32p, A.u32, A.u32, A.f32]
         lib.pxbref_project_particle.argtypes = [P, A.f32, f32p, f32p, f32p, P]
+        lib.pxbref_geometry_set_hull.argtypes = [A.u32, C.POINTER(A.HullDesc)]
+        lib.pxbref_geometry_set_mesh.argtypes = [A.u32, C.POINTER(A.MeshDesc)]
+        lib.pxbref_geometry_clear.argtypes = []
+        lib.pxbref_geometry_clear.restype = None
+        lib.pxbref_build_convex_hull.argtypes = [P, A.u32, P, A.u32, C.POINTER(A.u32), P, A.u32, P, P, A.u32]
         lib.pxbref_project_particle.restype = C.c_int
         lib.pxbref_bench_cloths.argtypes = [C.POINTER(P), A.u32, P, P, P, P, f32p, A.u32, A.u32,
                                             A.f32, A.u32, A.u32]
@@ -195,12 +204,16 @@ def oracle_set_strand_roots(s: StrandArrays, positions, orientations=None):
                                   0 if rot is None else len(rot))
 
 
+def _start(motion_start):
+    return None if motion_start is None else (C.c_float * 3)(*[float(x) for x in motion_start])
+
+
 def oracle_project(collider, thickness, p, motion_start=None):
     pp = (C.c_float * 3)(*[float(x) for x in p])
     n = (C.c_float * 3)()
     d = C.c_float(0.0)
     col = np.ascontiguousarray(np.asarray(collider, A.COLLIDER).reshape(1))
-    r = oracle().orc_project_particle(A.ptr(col), thickness, pp, n, C.byref(d), None)
+    r = oracle().orc_project_particle(A.ptr(col), thickness, pp, n, C.byref(d), _start(motion_start))
     return r, np.array(pp[:], np.float32), np.array(n[:], np.float32), np.float32(d.value)
 
 
@@ -324,5 +337,40 @@ def ref_project(collider, thickness, p, motion_start=None):
     n = (C.c_float * 3)()
     d = C.c_float(0.0)
     col = np.ascontiguousarray(np.asarray(collider, A.COLLIDER).reshape(1))
-    r = ref().pxbref_project_particle(A.ptr(col), thickness, pp, n, C.byref(d), None)
+    r = ref().pxbref_project_particle(A.ptr(col), thickness, pp, n, C.byref(d), _start(motion_start))
     return r, np.array(pp[:], np.float32), np.array(n[:], np.float32), np.float32(d.value)
+
+
+# ------------------------------------------------------------------------------------------
+# Collider geometry, registered under the same id in the oracle and the reference
+# ------------------------------------------------------------------------------------------
+
+def register_geometry(gid, geometry):
+    """Registers a Hull or Mesh (physxcoopa_b200.arrays) under `gid` with the oracle and, when
+    it is built, the reference driver, so colliders naming `gid` mean the same shape to both."""
+    from physxcoopa_b200.arrays import Hull
+    d = geometry.desc()
+    if isinstance(geometry, Hull):
+        assert oracle().orc_geometry_set_hull(gid, C.byref(d)) == 0
+        if ref_available():
+            assert ref().pxbref_geometry_set_hull(gid, C.byref(d)) == 0
+    else:
+        assert oracle().orc_geometry_set_mesh(gid, C.byref(d)) == 0
+        if ref_available():
+            assert ref().pxbref_geometry_set_mesh(gid, C.byref(d)) == 0
+
+
+def ref_build_convex_hull(points):
+    """geometry::build_convex_hull (the reference's own builder) over `points`, as a Hull."""
+    from physxcoopa_b200.arrays import Hull
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    cap_v, cap_f, cap_fv = 256, 512, 4096
+    verts = np.zeros((cap_v, 3), np.float32)
+    planes = np.zeros((cap_f, 4), np.float32)
+    starts = np.zeros(cap_f + 1, np.uint32)
+    fverts = np.zeros(cap_fv, np.uint32)
+    nv = A.u32(0)
+    nf = ref().pxbref_build_convex_hull(A.ptr(pts), len(pts), A.ptr(verts), cap_v, C.byref(nv), A.ptr(planes),
+                                        cap_f, A.ptr(starts), A.ptr(fverts), cap_fv)
+    assert nf > 0, "degenerate point cloud or capacity too small"
+    return Hull(verts[:nv.value], planes[:nf], starts[:nf + 1], fverts[:starts[nf]])

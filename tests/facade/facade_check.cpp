@@ -76,6 +76,44 @@ int main() {
         pxb::b200::solve_strands(dev, hmine, cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 4, 1.0f / 60.0f, h2);
     }
     bad += compare("strands 16x12, 90 frames", href.particles, hmine.particles);
+
+    // --- cloth onto a triangle-mesh floor with a convex-hull rock, both the reference's own
+    //     objects (TriangleMesh::from_triangles, build_convex_hull) ---
+    std::vector<glm::vec3> fv = {glm::vec3(-2.0f, -2.0f, 0.0f), glm::vec3(2.0f, -2.0f, 0.0f),
+                                 glm::vec3(2.0f, 2.0f, 0.0f), glm::vec3(-2.0f, 2.0f, 0.0f),
+                                 glm::vec3(0.0f, 0.0f, 0.15f)};
+    std::vector<uint32_t> fi = {0, 1, 4, 1, 2, 4, 2, 3, 4, 3, 0, 4};  // a low pyramid
+    const px::geometry::TriangleMesh floor = px::geometry::TriangleMesh::from_triangles(fv, fi);
+    std::vector<glm::vec3> rock_pts;
+    for (int k = 0; k < 8; ++k)
+        rock_pts.push_back(glm::vec3(k & 1 ? 0.2f : -0.2f, k & 2 ? 0.12f : -0.12f, k & 4 ? 0.1f : -0.1f));
+    rock_pts.push_back(glm::vec3(0.0f, 0.0f, 0.22f));
+    px::geometry::ConvexHull rock;
+    if (!px::geometry::build_convex_hull(rock_pts.data(), rock_pts.size(), rock)) return 2;
+    px::collision::Shape floor_shape = px::collision::Shape::make_mesh(&floor);
+    px::collision::Shape rock_shape = px::collision::Shape::make_hull(&rock, 1.2f);
+    floor_shape.enabled = rock_shape.enabled = true;
+    px::cloth::ClothCollider fc, rc;
+    fc.shape = &floor_shape;
+    fc.bounds = px::collision::world_bounds(floor_shape, fc.position, fc.orientation);
+    rc.shape = &rock_shape;
+    rc.position = glm::vec3(0.1f, -0.05f, 0.25f);
+    rc.orientation = glm::quat(0.9659258f, 0.0f, 0.0f, 0.2588190f);
+    rc.bounds = px::collision::world_bounds(rock_shape, rc.position, rc.orientation);
+    const std::vector<px::cloth::ClothCollider> geo_cols = {fc, rc};
+    px::cloth::GridClothDesc g2;
+    g2.columns = 16;
+    g2.rows = 16;
+    g2.width = 1.2f;
+    g2.height = 1.2f;
+    g2.center = glm::vec3(0.0f, 0.0f, 0.8f);
+    px::cloth::Cloth gref = px::cloth::make_grid_cloth(g2);
+    px::cloth::Cloth gmine = gref;
+    for (int i = 0; i < 150; ++i) {
+        px::cloth::solve_cloth(gref, geo_cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 10, 1.0f / 60.0f, s1);
+        pxb::b200::solve_cloth(dev, gmine, geo_cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 10, 1.0f / 60.0f, s2);
+    }
+    bad += compare("cloth 16x16 on a mesh floor and a hull, 150 frames", gref.particles, gmine.particles);
     std::printf(bad ? "facade MISMATCH\n" : "facade ok\n");
     return bad ? 1 : 0;
 }

@@ -317,9 +317,10 @@ def test_refusals_and_handles(ctx):
     mesh = np.zeros(1, A.COLLIDER)
     mesh["type"] = A.SHAPE_TRIANGLE_MESH
     mesh["enabled"] = 1
+    mesh["geometry"] = 999  # no such registered geometry
     with pytest.raises(R.PxbError) as e:
         ctx.step([cid], [mesh])
-    assert e.value.status == 2
+    assert e.value.status == 5
     ctx.remove_cloth(cid)
     with pytest.raises(R.PxbError) as e:
         ctx.step([cid])

@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--workload", default="uniform_batch",
                     choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom",
-                             "large_cloth_hair"])
+                             "large_cloth_hair", "mesh_floor"])
     ap.add_argument("--cloths", type=int, default=None)
     ap.add_argument("--side", type=int, default=64, help="sheet side of the uniform batch")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -82,6 +82,8 @@ def build_scene(args, rank):
         return scenes.single_drape(seed=rank)
     if args.workload == "uniform_batch":
         return scenes.uniform_batch(n=args.cloths or 1024, side=args.side, seed=1 + rank)
+    if args.workload == "mesh_floor":
+        return scenes.mesh_floor_batch(n=args.cloths or 4096, side=25, seed=12 + rank)
     return scenes.uneven_batch(n=args.cloths or 4096, seed=2 + rank)
 
 
@@ -160,6 +162,11 @@ def reference_cpu(sc, seconds_target=12.0, threads=None):
     threads = threads or os.cpu_count() or 1
     kind = "reference" if K.ref_available() else "port"
     n_total = len(sc.cloths)
+
+    # collider geometry under the ids the scene's colliders name
+    gids = getattr(sc, "geometries_ids", None) or [k + 1 for k in range(len(sc.geometries))]
+    for gid, g in zip(gids, sc.geometries):
+        K.register_geometry(gid, g)
 
     def timed(sample, steps, nthreads):
         if kind == "reference":
@@ -545,6 +552,9 @@ def main():
 
     sc = build_scene(args, rank)
     ctx = R.Context(local_rank)
+    if sc.geometries:
+        from physxcoopa_b200 import scenes
+        scenes.register_geometries(ctx, sc)
     ids = [ctx.add_cloth(c) for c in sc.cloths]
     d, keep = ctx.make_step(ids, sc.colliders, sc.gravity, sc.sources, sc.substeps,
                             sc.iterations, sc.h)
@@ -623,12 +633,26 @@ def main():
     from physxcoopa_b200 import _abi as A
     res_out = np.zeros(len(ids), A.FRAME_RESULT)
     # pxb_cloths_step uploads one staging block per step: per-cloth step records (184 B),
-    # collider snapshots (236 B), gravity sources (24 B) and the launch order (4 B), each
+    # collider snapshots (312 B), gravity sources (24 B), the launch order (4 B) and the posed
+    # convex hulls (16 B x (2 faces + 2 face-vertex entries) per distinct hull and pose), each
     # section padded to 256 B.
     al = lambda x: (x + 255) & ~255
     n_col = sum(len(c) for c in sc.colliders)
     n_src = sum(0 if s is None else len(s) for s in (sc.sources or []))
-    h2d = al(184 * len(ids)) + al(236 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * len(ids))
+    hull_bytes = 0
+    seen = set()
+    gids = getattr(sc, "geometries_ids", None) or []
+    for cols in sc.colliders:
+        for c in cols:
+            if int(c["type"]) == A.SHAPE_CONVEX_HULL and c["enabled"] and int(c["geometry"]):
+                key = tuple(np.asarray(c[f]).tobytes() for f in ("geometry", "position", "orientation",
+                                                                  "local_center", "local_rotation", "geometry_scale"))
+                if key not in seen:  # one posed block per distinct hull and pose
+                    seen.add(key)
+                    g = sc.geometries[gids.index(int(c["geometry"]))]
+                    hull_bytes += 16 * (2 * len(g.face_planes) + 2 * len(g.face_vertices))
+    h2d = (al(184 * len(ids)) + al(312 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * len(ids))
+           + al(hull_bytes))
     d2h = 12 * sc.vertices + 32 * len(ids) + 4
     ctx.synchronize()
     if dist:

@@ -324,6 +324,25 @@ def terrain_drape(side=32, seed=11, params=None):
                       geometries=[terrain, rock])
 
 
+def mesh_floor_batch(n=4096, side=25, seed=12):
+    """N sheets of side x side (default 4096 x 25^2) resting on one 2048-triangle mesh floor: the
+    reference's own costing case for mesh colliders (a 25x25 sheet on a 2048-triangle floor,
+    cloth/README.md:98-102), batched. The floor is a 4 x 4 m height field of 32 x 32 cells with
+    3 cm seeded bumps; each sheet is placed 6 cm above it at a seeded position, unpinned, with the
+    floor as its one collider (geometry id 1)."""
+    rng = np.random.default_rng(seed)
+    floor = terrain_mesh(32, 4.0, 0.03, seed)
+    col = collider_array([mesh_collider(1, floor)])
+    half = (side - 1) * SPACING * 0.5
+    cloths, cols = [], []
+    for k in range(n):
+        cx, cy = (float(v) for v in rng.uniform(-2.0 + half, 2.0 - half, 2))
+        cloths.append(_sheet(side, (cx, cy, 0.06), seed * 100003 + k, [], tethers=False))
+        cols.append(col.copy())
+    return ClothScene(f"mesh_floor_batch {n}x{side}^2", cloths, cols, meta={"side": side, "n": n},
+                      geometries=[floor])
+
+
 def register_geometries(ctx, scene):
     """Registers scene.geometries with a runtime.Context and rewrites the colliders' geometry ids
     from the scene's numbering (geometry k is id k + 1) to the ids the context returned. Returns

@@ -2,8 +2,8 @@
 """Cloth XPBD benchmark: cloth vertex-substeps/s on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
-                    [--workload uniform_batch|single_drape|uneven_batch|warm_start|hair_groom]
-                    [--cloths C]
+                    [--workload uniform_batch|single_drape|uneven_batch|warm_start|hair_groom|
+                                large_cloth_hair|mesh_floor] [--cloths C] [--floor mesh|box|none]
 
 One step = one PhysicsWorld cloth frame for every cloth of the workload: a single batched
 launch of the device solver (pxb_cloths_step) advancing each cloth by solve_cloth(h = 1/60,
@@ -66,6 +66,8 @@ def parse():
                     choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom",
                              "large_cloth_hair", "mesh_floor"])
     ap.add_argument("--cloths", type=int, default=None)
+    ap.add_argument("--floor", choices=["mesh", "box", "none"], default="mesh",
+                    help="mesh_floor workload: the floor collider (box / none measure the mesh query's share)")
     ap.add_argument("--side", type=int, default=64, help="sheet side of the uniform batch")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -83,7 +85,15 @@ def build_scene(args, rank):
     if args.workload == "uniform_batch":
         return scenes.uniform_batch(n=args.cloths or 1024, side=args.side, seed=1 + rank)
     if args.workload == "mesh_floor":
-        return scenes.mesh_floor_batch(n=args.cloths or 4096, side=25, seed=12 + rank)
+        sc = scenes.mesh_floor_batch(n=args.cloths or 4096, side=25, seed=12 + rank)
+        if args.floor != "mesh":  # the same sheets on an analytic box floor, or on nothing
+            from physxcoopa_b200.arrays import box, collider_array
+            floor = collider_array([box((2.0, 2.0, 0.02), (0.0, 0.0, -0.02))]) if args.floor == "box" \
+                else collider_array([])
+            sc.colliders = [floor.copy() for _ in sc.cloths]
+            sc.geometries = []
+            sc.name += f" ({args.floor} floor)"
+        return sc
     return scenes.uneven_batch(n=args.cloths or 4096, seed=2 + rank)
 
 

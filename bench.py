@@ -371,7 +371,7 @@ def bench_large(args, local_rank):
                        "cloth_ms_last_step": cloth_last_ms,
                        "l2": "cloth state (~18 MB) fits in L2; hair state 2.1 M particles x 48 B exceeds it"},
             "e2e": {"value": units / e2e_s, "unit": "vertex-substeps/s",
-                    "h2d_bytes_per_step": 184 + 236 + 64 * len(hair.sets[0].strands) + 236,
+                    "h2d_bytes_per_step": 192 + 312 + 64 * len(hair.sets[0].strands) + 312,
                     "d2h_bytes_per_step": 12 * n_cloth + 40 * n_hair},
             "roofline": None, "cpu_baseline": None, "gpu_launches": launches, "clocks": clk}
     del keep_c, keep_s
@@ -473,7 +473,7 @@ def bench_warm(args, local_rank):
     al = lambda x: (x + 255) & ~255
     n_col = sum(len(c) for c in sc.colliders)
     n_src = sum(0 if s is None else len(s) for s in (sc.sources or []))
-    h2d = al(184 * n) + al(236 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * n) + al(48 * n)
+    h2d = al(192 * n) + al(312 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * n) + al(48 * n)
     d2h = 12 * sc.vertices + 16 * n
     cons = sum(len(c.stretch) + len(c.bend) for c in sc.cloths)
     iters_done = warm_iters + extra
@@ -642,7 +642,7 @@ def main():
     ids_np = np.ascontiguousarray(ids, np.uint64)
     from physxcoopa_b200 import _abi as A
     res_out = np.zeros(len(ids), A.FRAME_RESULT)
-    # pxb_cloths_step uploads one staging block per step: per-cloth step records (184 B),
+    # pxb_cloths_step uploads one staging block per step: per-cloth step records (192 B),
     # collider snapshots (312 B), gravity sources (24 B), the launch order (4 B) and the posed
     # convex hulls (16 B x (2 faces + 2 face-vertex entries) per distinct hull and pose), each
     # section padded to 256 B.
@@ -661,7 +661,7 @@ def main():
                     seen.add(key)
                     g = sc.geometries[gids.index(int(c["geometry"]))]
                     hull_bytes += 16 * (2 * len(g.face_planes) + 2 * len(g.face_vertices))
-    h2d = (al(184 * len(ids)) + al(312 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * len(ids))
+    h2d = (al(192 * len(ids)) + al(312 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * len(ids))
            + al(hull_bytes))
     d2h = 12 * sc.vertices + 32 * len(ids) + 4
     ctx.synchronize()

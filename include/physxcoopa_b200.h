@@ -12,9 +12,9 @@
  *    keeps a message retrievable with pxb_last_error().
  *  - One host thread per context. A context owns one CUDA stream on one device; all device work
  *    is ordered on it.
- *  - No CPU fallback: an input the device path does not implement (self-collision, cloths not
- *    built by make_grid_cloth) is refused with PXB_ERR_UNSUPPORTED instead of being solved on
- *    the host.
+ *  - No CPU fallback: an input the device path does not implement (self-collision on a cloth
+ *    larger than one CTA holds, cloths not built by make_grid_cloth) is refused with
+ *    PXB_ERR_UNSUPPORTED instead of being solved on the host.
  *  - The plain-old-data structs below reproduce the reference's in-memory layouts byte for byte
  *    (glm::vec3 = 3 floats, glm::quat = x,y,z,w floats, no SIMD alignment), so a C++ caller can
  *    hand `std::vector<ClothParticle>::data()` and friends straight to this API.
@@ -285,6 +285,10 @@ typedef struct pxb_cloth_plan {
     int32_t n_segments;       /* affine segments over all CTAs and colours */
     int32_t layout_slots;     /* rows * 4 * ceil(columns / 4) particle slots */
     int32_t constraint_slots; /* rest-length slots over all CTAs, row padding included */
+    int32_t self_collision;   /* 1: self-collision (ClothParams::self_collision) can run on this
+                                 layout (one CTA, hash tables in shared memory); 0: a step with
+                                 it enabled is refused with PXB_ERR_UNSUPPORTED */
+    int32_t self_smem_bytes;  /* dynamic shared memory per CTA with self-collision on */
 } pxb_cloth_plan;
 
 /* Plans a cloth without a context or a GPU: validates it exactly as pxb_cloth_add does and

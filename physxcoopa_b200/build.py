@@ -29,7 +29,7 @@ def sources():
 
 
 def _inputs():
-    files = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    files = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     files.append(os.path.join(INCLUDE, "physxcoopa_b200.h"))
     files.append(os.path.abspath(__file__))
     return files

@@ -30,6 +30,7 @@
 #include "pxb_kernels.h"
 #include "pxb_mlp.cuh"
 #include "pxb_device_math.cuh"
+#include "pxb_self_collision.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -258,7 +259,7 @@ __device__ __forceinline__ void cluster_or_block_sync() {
     else __syncthreads();
 }
 
-template <int kMaxThreads, int CL, bool kWarm, bool kGeo>
+template <int kMaxThreads, int CL, bool kWarm, bool kExt>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders,
@@ -757,6 +758,64 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         {
             const int col_begin = sP.col_begin, col_count = sP.col_count;
             const float thickness = sP.thickness, inv_hs = sP.inv_hs;
+            bool self = false;
+            if constexpr (kExt && CL == 1) {
+                self = sP.self_collision != 0;
+                if (self) {
+                    // 5. tethers on their own: 6. self-collision reads every particle after them
+                    for (int l = tid; l < n_local; l += T) {
+                        const float4 p4 = pos[l];
+                        if (p4.w == 0.0f) continue;
+                        const int2 teth = __ldg(&sC.tether[base + l]);
+                        if (teth.x < 0) continue;
+                        const f3 anchor = xyz(pos[teth.x]);
+                        const f3 d = sub(xyz(p4), anchor);
+                        const float l2 = len(d);
+                        const float max_len = __int_as_float(teth.y);
+                        if (!(l2 <= max_len || l2 < PXB_EPSILON)) {
+                            const f3 q = add(anchor, mul(d, max_len / l2));
+                            pos[l] = make_float4(q.x, q.y, q.z, p4.w);
+                        }
+                    }
+                    __syncthreads();
+                    // 6. self-collision (cloth_solver.h:291-366) over tables in shared memory
+                    uint32_t* tab = reinterpret_cast<uint32_t*>(smem + sC.self_hash_off);
+                    const uint32_t buckets = static_cast<uint32_t>(sC.self_buckets);
+                    const float d_min = sP.self_distance;
+                    const float inv_cell = 1.0f / d_min;
+                    // the tables must be a power-of-two hash after the positions, inside this
+                    // launch's shared memory: otherwise record the error and skip the stage
+                    uint32_t dyn;
+                    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+                    const bool tables_ok =
+                        buckets >= 16u && (buckets & (buckets - 1u)) == 0u && sC.self_hash_off >= 16 * n_local &&
+                        (sC.self_hash_off & 15) == 0 &&
+                        static_cast<uint64_t>(sC.self_hash_off) +
+                                4ull * PXB_SELF_WORDS(static_cast<uint64_t>(buckets), static_cast<uint64_t>(sC.n_real)) <=
+                            dyn;
+                    if (!tables_ok) {
+                        if (tid == 0) atomicOr(err, PXB_DEVERR_BAD_INDEX);
+                    } else {
+                        self_build_hash(pos, tab, sC.n_real, sC.columns, sC.Q, sC.S, buckets, inv_cell, tid, T);
+                        if (tid < 32)
+                            self_pair_pass(pos, tab, sC.n_real, sC.columns, sC.Q, sC.S, buckets, d_min, inv_cell, tid);
+                    }
+                    __syncthreads();
+                    if (sC.self_restage) {
+                        // the tables borrowed the rest lengths' bytes: stage them again
+                        fence_proxy_async();
+                        __syncthreads();
+                        if (tid == 0) {
+                            const uint32_t rest_bytes = 4u * static_cast<uint32_t>(sC.rank[0].n_rest_pad);
+                            mbar_arrive_expect_tx(&bar, rest_bytes);
+                            if (rest_bytes) bulk_g2s(rest, sC.rest + sC.rank[0].rest_off, rest_bytes, &bar);
+                        }
+                        stage_phase ^= 1u;
+                        if (!mbar_wait_bounded(&bar, stage_phase) && tid == 0) atomicOr(err, PXB_DEVERR_TMA_TIMEOUT);
+                        __syncthreads();
+                    }
+                }
+            }
             for (int l = tid; l < n_local; l += T) {
                 const int gl = base + l;
                 float4 p4 = pos[l];
@@ -766,7 +825,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 float dsum = 0.0f;
                 if (p4.w != 0.0f) {
                     // 5. tether (cloth_solver.h:276-289); its anchor is a pinned particle
-                    const int2 teth = __ldg(&sC.tether[gl]);
+                    const int2 teth = self ? make_int2(-1, 0) : __ldg(&sC.tether[gl]);
                     if (teth.x >= 0) {
                         f3 anchor;
                         if (CL == 1) {
@@ -796,9 +855,9 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                         f3 n = mk(0.0f, 0.0f, 0.0f);
                         float depth = 0.0f;
                         // a mesh's swept test starts from the substep's start (cloth_solver.h:398-403)
-                        const bool mesh = kGeo && __ldg(&c->type) == PXB_SHAPE_TRIANGLE_MESH;
+                        const bool mesh = kExt && __ldg(&c->type) == PXB_SHAPE_TRIANGLE_MESH;
                         const f3 start = mesh ? xyz(gprv[gl]) : p;
-                        if (!project_particle<kGeo>(c, thickness, p, n, depth, start, mesh)) continue;
+                        if (!project_particle<kExt>(c, thickness, p, n, depth, start, mesh)) continue;
                         moved = true;
                         nsum = add(nsum, n);
                         dsum += depth;
@@ -999,7 +1058,7 @@ __device__ __forceinline__ void grid_sync(PxbGridSync* gs, unsigned int& epoch, 
     __syncthreads();
 }
 
-template <int kThreads, bool kGeo>
+template <int kThreads, bool kExt>
 __global__ void __launch_bounds__(kThreads, 1)
 cloth_grid_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders, const pxb_gravity_source* __restrict__ sources,
@@ -1197,9 +1256,9 @@ cloth_grid_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                         }
                         f3 nn = mk(0.0f, 0.0f, 0.0f);
                         float depth = 0.0f;
-                        const bool mesh = kGeo && __ldg(&c->type) == PXB_SHAPE_TRIANGLE_MESH;
+                        const bool mesh = kExt && __ldg(&c->type) == PXB_SHAPE_TRIANGLE_MESH;
                         const f3 start = mesh ? xyz(gprv[gl]) : p;
-                        if (!project_particle<kGeo>(c, thickness, p, nn, depth, start, mesh)) continue;
+                        if (!project_particle<kExt>(c, thickness, p, nn, depth, start, mesh)) continue;
                         moved = true;
                         nsum = add(nsum, nn);
                         dsum += depth;
@@ -1275,20 +1334,20 @@ cloth_grid_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
 }
 
-template <bool kGeo>
+template <bool kExt>
 static cudaError_t launch_grid_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
                                        const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                        const int32_t* order, PxbFrameResult* results, uint32_t* err,
                                        PxbGridSync* gs, int slot, int n_sms, cudaStream_t stream) {
     constexpr int kThreads = 1024;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cloth_grid_kernel<kThreads, kGeo>, kThreads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cloth_grid_kernel<kThreads, kExt>, kThreads, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     unsigned int blocks = static_cast<unsigned int>(n_sms);  // one CTA per SM: every one co-resident
     void* args[] = {(void*)&cloths, (void*)&steps, (void*)&colliders, (void*)&sources, (void*)&order,
                     (void*)&results, (void*)&err, (void*)&gs, (void*)&slot};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(cloth_grid_kernel<kThreads, kGeo>), dim3(blocks),
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(cloth_grid_kernel<kThreads, kExt>), dim3(blocks),
                                        dim3(kThreads), args, 0, stream);
 }
 
@@ -1299,7 +1358,7 @@ cudaError_t launch_cloth_grid(const PxbClothDev* cloths, const PxbClothStep* ste
                : launch_grid_variant<false>(cloths, steps, colliders, sources, order, results, err, gs, slot, n_sms, stream);
 }
 
-template <int kMaxThreads, int CL, bool kWarm, bool kGeo>
+template <int kMaxThreads, int CL, bool kWarm, bool kExt>
 static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
                                   const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                   const int32_t* order, PxbFrameResult* results, uint32_t* err,
@@ -1311,10 +1370,10 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     if (e != cudaSuccess) return e;
     if (dev < 64 && !(configured >> dev & 1ull)) {
         cudaFuncAttributes fa;
-        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm, kGeo>);
+        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt>);
         if (e != cudaSuccess) return e;
         if (fa.sharedSizeBytes > static_cast<size_t>(kClothStaticSmem)) return cudaErrorInvalidConfiguration;
-        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm, kGeo>,
+        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm, kExt>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
         if (e != cudaSuccess) return e;
         configured |= 1ull << dev;
@@ -1331,7 +1390,7 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm, kGeo>, cloths, steps, colliders,
+    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt>, cloths, steps, colliders,
                               sources, order, results, err, wsteps, mlp, wres);
 }
 
@@ -1352,22 +1411,22 @@ int cloth_variant_registers(int variant) {
     return regs[v];
 }
 
-template <int kMaxThreads, bool kWarm, bool kGeo>
+template <int kMaxThreads, bool kWarm, bool kExt>
 static cudaError_t launch_cl(int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
                              int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
                              const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres) {
     switch (cluster) {
-        case 1: return launch_variant<kMaxThreads, 1, kWarm, kGeo>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 2: return launch_variant<kMaxThreads, 2, kWarm, kGeo>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 4: return launch_variant<kMaxThreads, 4, kWarm, kGeo>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 8: return launch_variant<kMaxThreads, 8, kWarm, kGeo>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 1: return launch_variant<kMaxThreads, 1, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 2: return launch_variant<kMaxThreads, 2, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 4: return launch_variant<kMaxThreads, 4, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 8: return launch_variant<kMaxThreads, 8, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
         default: return cudaErrorInvalidValue;
     }
 }
 
-// Launches carrying a mesh or hull collider: the same dispatch over the kGeo instantiations.
+// Launches carrying a mesh or hull collider: the same dispatch over the kExt instantiations.
 static cudaError_t launch_geo(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,

@@ -87,7 +87,19 @@ struct PxbClothDev {
     const float* edge_rest;     // [6][n_layout] rest length to the grid neighbour (+x, -x, +y,
                                 // -y, +x+y, -x-y), 0 where no stretch constraint joins them
     float4* disp;               // [n_layout] warm-start displacement scratch
+    // Self-collision (one-CTA cloths): the spatial hash's bucket count (hash_bucket_count of the
+    // particle count) and where in dynamic shared memory its tables live: PXB_SELF_WORDS words
+    // from self_hash_off, in the rest-length region when they fit there (self_restage: the rest
+    // lengths are staged again afterwards), else after the lambda region.
+    int32_t self_buckets;
+    int32_t self_hash_off;
+    int32_t self_restage;
+    int32_t pad1;
 };
+
+// Words of the self-collision tables: bucket ends (buckets + 1), the sorted particle indices (n),
+// a block-scan scratch (32) and the 27-cell candidate table of the pair loop (64).
+#define PXB_SELF_WORDS(buckets, n) ((buckets) + 1 + (n) + 32 + 64)
 
 // Warm-start controls of one cloth for one step (pxb_cloths_step_warm / pxb_cloths_record).
 struct PxbWarmStep {
@@ -189,6 +201,8 @@ struct PxbClothStep {
     int32_t steps, iters, aero;
     int32_t col_begin, col_count, src_begin, src_count;
     int32_t write_lambdas;
+    float self_distance;     // ClothParams::self_distance when self-collision runs, else 0
+    int32_t self_collision;  // self_collision && self_distance > k_epsilon (cloth_solver.h:170)
 };
 
 // One registered strand set on the device. Particles are strand-major, 32 slots per strand
@@ -239,7 +253,7 @@ struct PxbFrameResult {
 };
 
 static_assert(sizeof(PxbSeg) == 32 && alignof(PxbSeg) == 16, "segment descriptor layout");
-static_assert(sizeof(PxbClothStep) == 184, "per-step record size is part of the staging contract");
+static_assert(sizeof(PxbClothStep) == 192, "per-step record size is part of the staging contract");
 static_assert(sizeof(PxbDevCollider) == 312, "collider snapshot size is part of the staging contract");
 static_assert(sizeof(PxbMeshNode) == 32 && sizeof(PxbMeshTri) == 64, "mesh record layout");
 

@@ -214,6 +214,13 @@ int slot_of_particle(int i, int cols, int Q, int S) {
 bool recognise_grid(const pxb_cloth_desc* d, int Q, int S, std::vector<ColourSpec>& out,
                     std::vector<int32_t>& rest_ref, std::vector<int32_t>& colour_batch) {
     const int cols = static_cast<int>(d->columns), rows = static_cast<int>(d->rows);
+    if (d->n_stretch == 0 && d->n_bend == 0 && d->n_stretch_batches == 0 && d->n_bend_batches == 0) {
+        // a grid of free particles (every constraint list cleared): no colour to solve
+        out.clear();
+        rest_ref.clear();
+        colour_batch.clear();
+        return true;
+    }
     for (int shear = 1; shear >= 0; --shear) {
         std::vector<ColourSpec> cs;
         grid_colours(cols, rows, shear != 0, Q, S, cs);
@@ -275,6 +282,11 @@ bool grid_triangles(const pxb_cloth_desc* d) {
 }
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+// Whether solve_cloth runs its self-collision stage for this cloth (cloth_solver.h:170).
+bool self_on(const ClothEntry& e) {
+    return e.params.self_collision && e.params.self_distance > PXB_EPSILON;
+}
 
 // Compliance of colour `c` of entry `e` (per-batch override, else the params value).
 float colour_compliance(const ClothEntry& e, int c) {
@@ -434,6 +446,29 @@ static void layout_ranks(ClothEntry& e) {
     e.n_lam = lam_total;
     e.dev.smem_bytes = smem_max;
     e.warm_smem = warm_max;
+    // Self-collision tables (one-CTA cloths): in the rest-length region when they fit there (the
+    // rest lengths are staged again after the stage), else after the lambda region.
+    e.self_ok = false;
+    e.self_smem = 0;
+    e.dev.self_buckets = 0;
+    e.dev.self_hash_off = 0;
+    e.dev.self_restage = 0;
+    if (e.ranks.size() == 1) {
+        uint32_t buckets = 16;  // detail::hash_bucket_count (cloth_solver.h:111-115)
+        while (buckets < e.n_particles * 2u && buckets < (1u << 22)) buckets <<= 1;
+        const int bytes = (4 * static_cast<int>(PXB_SELF_WORDS(buckets, e.n_particles)) + 15) & ~15;
+        const ClothEntry::Rank& rk = e.ranks[0];
+        e.dev.self_buckets = static_cast<int32_t>(buckets);
+        if (bytes <= 4 * rk.n_rest_pad) {
+            e.dev.self_hash_off = 16 * rk.n_rows * e.S;
+            e.dev.self_restage = 1;
+            e.self_smem = smem_max;
+        } else {
+            e.dev.self_hash_off = smem_max;
+            e.self_smem = smem_max + bytes;
+        }
+        e.self_ok = e.self_smem <= kMaxDynamicSmem;
+    }
 }
 
 void pxb_context::refresh_layout(ClothEntry& e) {
@@ -499,8 +534,6 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
     if (!d) return fail(PXB_ERR_INVALID_ARGUMENT, "null argument");
     if (d->n_particles == 0 || !d->particles)
         return fail(PXB_ERR_INVALID_ARGUMENT, "an empty cloth is refused (PhysicsWorld::add_cloth does the same)");
-    if (d->params.self_collision && d->params.self_distance > PXB_EPSILON)
-        return fail(PXB_ERR_UNSUPPORTED, "self-collision is not implemented on the device path");
     const uint32_t n = d->n_particles;
     auto chk_list = [&](const pxb_constraint* l, uint32_t cnt, const char* name) -> bool {
         if (cnt && !l) return false;
@@ -660,6 +693,9 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     std::memset(&e.dev, 0, sizeof(e.dev));
     std::memcpy(e.dev.rank, keep_ranks.rank, sizeof(e.dev.rank));
     e.dev.smem_bytes = keep_ranks.smem_bytes;
+    e.dev.self_buckets = keep_ranks.self_buckets;
+    e.dev.self_hash_off = keep_ranks.self_hash_off;
+    e.dev.self_restage = keep_ranks.self_restage;
     e.dev.pos = reinterpret_cast<float4*>(base + o_pos);
     e.dev.vel = reinterpret_cast<float4*>(base + o_vel);
     e.dev.prv = reinterpret_cast<float4*>(base + o_prv);
@@ -836,8 +872,10 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     for (uint32_t k = 0; k < n; ++k) {
         ents[k] = lookup(sd->cloths[k]);
         if (!ents[k]) return fail(PXB_ERR_INVALID_HANDLE, "cloth id %llu is not live", (unsigned long long)sd->cloths[k]);
-        if (ents[k]->params.self_collision && ents[k]->params.self_distance > PXB_EPSILON)
-            return fail(PXB_ERR_UNSUPPORTED, "self-collision is not implemented on the device path");
+        if (self_on(*ents[k]) && (!ents[k]->self_ok || ents[k]->grid))
+            return fail(PXB_ERR_UNSUPPORTED,
+                        "cloth %llu: self-collision runs on cloths solved by one CTA (sides up to 64) whose hash "
+                        "tables fit in shared memory", (unsigned long long)sd->cloths[k]);
         if (sd->collider_offsets) {
             if (sd->collider_offsets[k + 1] < sd->collider_offsets[k])
                 return fail(PXB_ERR_INVALID_ARGUMENT, "collider offsets decrease");
@@ -896,17 +934,22 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     const int cap = cloth_variant_threads(cloth_variant);
     const int regs = cloth_variant_registers(cloth_variant);
     std::vector<int> fit(n);
-    auto launch_smem = [&](const ClothEntry& e) { return warm ? e.warm_smem : e.dev.smem_bytes; };
+    auto launch_smem = [&](const ClothEntry& e) {
+        const int base = warm ? e.warm_smem : e.dev.smem_bytes;
+        return self_on(e) ? std::max(base, e.self_smem) : base;
+    };
     auto launch_threads = [&](const ClothEntry& e) {
         // the warm-start kernel runs whole warpgroups (the network's tiles are 128 rows)
         return warm ? std::min(cap, std::max(128, (e.threads + 127) & ~127)) : std::min(e.threads, cap);
     };
     for (uint32_t k = 0; k < n; ++k) fit[k] = ctas_per_sm(launch_smem(*ents[k]), launch_threads(*ents[k]), regs);
-    // cloths with a mesh or hull collider launch the kernel with those branches compiled in
+    // cloths with a mesh or hull collider, or with self-collision, launch the kernel with those
+    // stages compiled in
     std::vector<uint8_t> has_geo(n, 0);
-    if (sd->collider_offsets)
-        for (uint32_t k = 0; k < n; ++k)
-            has_geo[k] = cstage.any_geometry(sd->collider_offsets[k], sd->collider_offsets[k + 1] - sd->collider_offsets[k]);
+    for (uint32_t k = 0; k < n; ++k)
+        has_geo[k] = self_on(*ents[k]) ||
+                     (sd->collider_offsets &&
+                      cstage.any_geometry(sd->collider_offsets[k], sd->collider_offsets[k + 1] - sd->collider_offsets[k]));
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
@@ -961,6 +1004,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         s.src_begin = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k]) : 0;
         s.src_count = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k + 1] - sd->source_offsets[k]) : 0;
         s.write_lambdas = 1;
+        s.self_collision = self_on(e) ? 1 : 0;
+        s.self_distance = self_on(e) ? P.self_distance : 0.0f;
         hs_order[slot] = static_cast<int32_t>(ents[k] - cloths.data());
         if (warm) {
             PxbWarmStep& w = hs_warm[slot];
@@ -1256,6 +1301,8 @@ pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out
     out->n_segments = static_cast<int32_t>(e.segs.size());
     out->layout_slots = e.n_layout;
     out->constraint_slots = e.n_rest_total;
+    out->self_collision = e.self_ok && !e.grid ? 1 : 0;
+    out->self_smem_bytes = e.self_ok && !e.grid ? e.self_smem : 0;
     return PXB_OK;
 }
 
@@ -1280,8 +1327,6 @@ pxb_status pxb_cloth_set_params(pxb_context* ctx, uint64_t id, const pxb_cloth_p
     if (!ctx || !params) return PXB_ERR_INVALID_ARGUMENT;
     ClothEntry* e = ctx->lookup(id);
     if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
-    if (params->self_collision && params->self_distance > PXB_EPSILON)
-        return ctx->fail(PXB_ERR_UNSUPPORTED, "self-collision is not implemented on the device path");
     const pxb_cloth_params old = e->params;
     e->params = *params;
     ctx->refresh_layout(*e);

@@ -45,6 +45,8 @@ struct ClothEntry {
     int n_lam = 0;                         // lambda slots over all ranks
     int threads = 64;
     int warm_smem = 0;  // dynamic shared memory of the warm-start kernel (max over ranks)
+    bool self_ok = false;  // self-collision can run (one CTA, hash tables fit in shared memory)
+    int self_smem = 0;     // dynamic shared memory with self-collision on
     int aero_grid = 0;
     uint32_t n_triangle_indices = 0;
     uint32_t n_stretch = 0, n_bend = 0, n_stretch_batches = 0, n_bend_batches = 0;

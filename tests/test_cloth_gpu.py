@@ -308,10 +308,12 @@ def test_refusals_and_handles(ctx):
     p = A.ClothParams.defaults()
     p.self_collision = 1
     p.self_distance = 0.1
-    c = R.HostCloth(5, 5, 1.0, 1.0, params=p).arrays()
+    big = R.HostCloth(100, 100, 5.0, 5.0, params=p).arrays()  # a cluster: no self-collision there
+    bid = ctx.add_cloth(big)
     with pytest.raises(R.PxbError) as e:
-        ctx.add_cloth(c)
+        ctx.step([bid])
     assert e.value.status == 2  # UNSUPPORTED: no CPU fallback
+    ctx.remove_cloth(bid)
     ok = R.HostCloth(5, 5, 1.0, 1.0).arrays()
     cid = ctx.add_cloth(ok)
     mesh = np.zeros(1, A.COLLIDER)

@@ -73,12 +73,31 @@ def test_refusals_match_add_cloth():
     with pytest.raises(R.PxbError) as e:
         R.plan_cloth(empty)
     assert e.value.status == 1
+
+
+
+def test_self_collision_plans_on_one_cta_only():
+    """Self-collision (cloth_solver.h:291-366) runs on cloths one CTA holds: its hash tables go in
+    the rest-length region when they fit there, else after the lambdas. Clusters and the
+    whole-GPU path report that a step with it enabled would be refused."""
     p = A.ClothParams.defaults()
     p.self_collision = 1
     p.self_distance = 0.1
-    with pytest.raises(R.PxbError) as e:
-        R.plan_cloth(sheet(9, 9, params=p))
-    assert e.value.status == 2
+    for side in (9, 25, 64):
+        plan = R.plan_cloth(sheet(side, side, params=p))
+        assert plan["n_ranks"] == 1 and plan["self_collision"] == 1
+        assert plan["self_smem_bytes"] >= plan["smem_bytes"]
+        assert plan["self_smem_bytes"] <= 232448 - 4608
+    for side in (100, 512):
+        plan = R.plan_cloth(sheet(side, side, params=p))
+        assert plan["self_collision"] == 0
+    # every constraint list cleared (the reference's own self-collision tests do this): no colour
+    free = sheet(9, 9, params=p)
+    for f in ("stretch", "bend", "stretch_batches", "bend_batches"):
+        setattr(free, f, getattr(free, f)[:0].copy())
+    plan = R.plan_cloth(free)
+    assert plan["n_colours"] == 0 and plan["self_collision"] == 1
+    assert plan["self_smem_bytes"] > plan["smem_bytes"]  # no rest lengths to borrow
 
 
 def test_swapped_pair_is_caught_by_item_verification():

@@ -4,6 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
                     [--workload uniform_batch|single_drape|uneven_batch|warm_start|hair_groom|
                                 large_cloth_hair|mesh_floor] [--cloths C] [--floor mesh|box|none]
+                    [--self-collision]
 
 One step = one PhysicsWorld cloth frame for every cloth of the workload: a single batched
 launch of the device solver (pxb_cloths_step) advancing each cloth by solve_cloth(h = 1/60,
@@ -66,6 +67,8 @@ def parse():
                     choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom",
                              "large_cloth_hair", "mesh_floor"])
     ap.add_argument("--cloths", type=int, default=None)
+    ap.add_argument("--self-collision", action="store_true",
+                    help="turn ClothParams::self_collision on for every cloth of the workload")
     ap.add_argument("--floor", choices=["mesh", "box", "none"], default="mesh",
                     help="mesh_floor workload: the floor collider (box / none measure the mesh query's share)")
     ap.add_argument("--side", type=int, default=64, help="sheet side of the uniform batch")
@@ -79,6 +82,16 @@ def parse():
 
 
 def build_scene(args, rank):
+    sc = _build_scene(args, rank)
+    if getattr(args, "self_collision", False):
+        # ClothParams::self_collision on every cloth, at the builder's self_distance (0.6 x spacing)
+        for c in sc.cloths:
+            c.params.self_collision = 1
+        sc.name += " (self-collision)"
+    return sc
+
+
+def _build_scene(args, rank):
     from physxcoopa_b200 import scenes
     if args.workload == "single_drape":
         return scenes.single_drape(seed=rank)

@@ -97,9 +97,9 @@ struct PxbClothDev {
     int32_t pad1;
 };
 
-// Words of the self-collision tables: bucket ends (buckets + 1), the sorted particle indices (n),
-// a block-scan scratch (32) and the 27-cell candidate table of the pair loop (64).
-#define PXB_SELF_WORDS(buckets, n) ((buckets) + 1 + (n) + 32 + 64)
+// Words of the self-collision tables: bucket ends (buckets + 1), the sorted particle indices (n)
+// and a block-scan scratch (32).
+#define PXB_SELF_WORDS(buckets, n) ((buckets) + 1 + (n) + 32)
 
 // Warm-start controls of one cloth for one step (pxb_cloths_step_warm / pxb_cloths_record).
 struct PxbWarmStep {

@@ -9,14 +9,13 @@
 //     within a bucket) is built by the whole CTA: atomic bucket counts, a block-wide exclusive
 //     scan, and a stable scatter by one warp in index order (lanes of a chunk that share a bucket
 //     take consecutive places in lane order);
-//   * one warp then walks the particles in index order. For particle i the 27 cells are hashed by
-//     27 lanes at once and their candidates numbered in the reference's scan order (dz, dy, dx,
-//     then bucket position); 32 candidates are tested at a time against i's current position,
-//     the first one that pushes is applied, and only the candidates after it are tested again
-//     with the moved positions. The pushes, and the positions every test sees, are the
-//     reference's, in its order.
+//   * one warp then walks the particles in index order. For particle i, 27 lanes each own one of
+//     the 27 cells (in the reference's scan order) and scan their bucket for the first candidate
+//     that pushes; the first such candidate in the reference's order is applied and the cells
+//     after it are scanned again against the moved particle. The pushes, and the positions every
+//     test sees, are the reference's, in its order.
 // Tables (PXB_SELF_WORDS words of dynamic shared memory at `tab`): bucket ends [buckets + 1],
-// sorted particle indices [n], scan scratch [32], candidate table [64].
+// sorted particle indices [n], block-scan scratch [32].
 #ifndef PXB_SELF_COLLISION_CUH
 #define PXB_SELF_COLLISION_CUH
 
@@ -108,99 +107,95 @@ __device__ void self_build_hash(const float4* pos, uint32_t* tab, int n, int col
     __syncthreads();
 }
 
-// The pair pass of cloth_solver.h:325-365, by warp 0 (the caller's other warps wait at the
-// barrier after it). `pos` holds xyz + inverse mass in layout order.
-// The candidate table is rewritten for every particle, so `tab` is a plain pointer: no const or
-// restrict promise that would let the compiler keep an earlier particle's table.
-__device__ void self_pair_pass(float4* pos, uint32_t* tab, int n, int cols, int Q, int S, uint32_t buckets,
-                               float d_min, float inv_cell, int lane) {
+// One particle of the pair pass (cloth_solver.h:325-365), exactly, by the whole warp. Lane k < 27
+// owns cell k of the reference's scan order (dx, dy, dz) = (k % 3, k / 3 % 3, k / 9) - 1, dz
+// outermost, and a cursor into that cell's bucket. Each round every lane scans from its cursor to
+// its first candidate that pushes against the current positions; the lowest such lane holds the
+// first pushing candidate in the reference's order, applies it and moves its cursor past it. The
+// lanes before it have tested all their candidates and are done; the lanes after it scan again
+// from where they were, against the moved particle. Returns whether any push ran.
+__device__ bool self_exact_particle(float4* pos, const uint32_t* tab, int i, int n, int cols, uint32_t col_magic,
+                                   int Q, int S, uint32_t buckets, float d_min, float d2_min, float inv_cell,
+                                   int lane) {
     const uint32_t* ends = tab;
     const uint32_t* sorted = tab + buckets + 1;
-    uint32_t* cell_first = tab + buckets + 1 + n + 32;
-    uint32_t* cell_excl = cell_first + 32;
-    const float d2_min = d_min * d_min;
-    for (int i = 0; i < n; ++i) {
-        const int yi = i / cols, xi = i - yi * cols;
-        const int li = yi * S + (xi & 3) * Q + (xi >> 2);
-        float4 pi = pos[li];
-        if (pi.w == 0.0f) continue;
-        const int32_t cx = static_cast<int32_t>(floorf(pi.x * inv_cell));
-        const int32_t cy = static_cast<int32_t>(floorf(pi.y * inv_cell));
-        const int32_t cz = static_cast<int32_t>(floorf(pi.z * inv_cell));
-        // lane k < 27 is cell (dx, dy, dz) = (k % 3, k / 3 % 3, k / 9) - 1: the reference's loop
-        // order, dz outermost
-        uint32_t first = 0u, cnt = 0u;
-        if (lane < 27) {
-            const uint32_t b = self_hash(cx + lane % 3 - 1, cy + lane / 3 % 3 - 1, cz + lane / 9 - 1, buckets);
-            first = b ? ends[b - 1] : 0u;
-            cnt = ends[b] - first;
-        }
-        uint32_t inc = cnt;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-        if (total == 0u) continue;
-        cell_first[lane] = first;
-        cell_excl[lane] = inc - cnt;
-        __syncwarp();
-        for (uint32_t c0 = 0; c0 < total; c0 += 32u) {
-            const uint32_t c = c0 + static_cast<uint32_t>(lane);
-            int j = -1, lj = 0;
-            if (c < total) {
-                // the last cell whose first candidate number is <= c holds candidate c
-                int lo = 0, hi = 26;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (cell_excl[mid] <= c) lo = mid;
-                    else hi = mid - 1;
-                }
-                j = static_cast<int>(sorted[cell_first[lo] + (c - cell_excl[lo])]);
-                const int yj = j / cols, xj = j - yj * cols;
-                // each pair once; the 1-ring (Chebyshev distance 1 on the grid) is exempt
-                if (j <= i || (abs(xi - xj) <= 1 && abs(yi - yj) <= 1)) j = -1;
-                else lj = yj * S + (xj & 3) * Q + (xj >> 2);
-            }
-            uint32_t done = 0u;  // lanes at or before the last push of this chunk
-            for (;;) {
-                bool push = false;
-                float4 pj = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                float dx = 0.0f, dy = 0.0f, dz = 0.0f, len2 = 0.0f, w = 0.0f;
-                if (j >= 0 && !((done >> lane) & 1u)) {
-                    pj = pos[lj];
-                    w = pi.w + pj.w;
-                    if (w > 0.0f) {
-                        dx = pi.x - pj.x;
-                        dy = pi.y - pj.y;
-                        dz = pi.z - pj.z;
-                        len2 = dx * dx + dy * dy + dz * dz;
-                        push = !(len2 >= d2_min || len2 < PXB_EPSILON);
-                    }
-                }
-                const uint32_t m = __ballot_sync(0xffffffffu, push);
-                if (!m) break;
-                const int k0 = __ffs(m) - 1;
-                if (lane == k0) {
-                    const float len = sqrtf(len2);
-                    const float s = (d_min - len) / w;
-                    const float px = (dx / len) * s, py = (dy / len) * s, pz = (dz / len) * s;
-                    pi.x = pi.x + px * pi.w;
-                    pi.y = pi.y + py * pi.w;
-                    pi.z = pi.z + pz * pi.w;
-                    pj.x = pj.x - px * pj.w;
-                    pj.y = pj.y - py * pj.w;
-                    pj.z = pj.z - pz * pj.w;
-                    pos[lj] = pj;
-                    pos[li] = pi;
-                }
-                __syncwarp();
-                pi = pos[li];
-                done = k0 == 31 ? 0xffffffffu : ((2u << k0) - 1u);
-            }
-        }
-        __syncwarp();
+    const int yi = static_cast<int>(__umulhi(static_cast<uint32_t>(i), col_magic)), xi = i - yi * cols;
+    const int li = yi * S + (xi & 3) * Q + (xi >> 2);
+    float4 pi = pos[li];
+    if (pi.w == 0.0f) return false;
+    const int32_t cx = static_cast<int32_t>(floorf(pi.x * inv_cell));
+    const int32_t cy = static_cast<int32_t>(floorf(pi.y * inv_cell));
+    const int32_t cz = static_cast<int32_t>(floorf(pi.z * inv_cell));
+    uint32_t cur = 0u, last = 0u;
+    if (lane < 27) {
+        const uint32_t b = self_hash(cx + lane % 3 - 1, cy + lane / 3 % 3 - 1, cz + lane / 9 - 1, buckets);
+        cur = b ? ends[b - 1] : 0u;
+        last = ends[b];
     }
+    bool any = false;
+    for (;;) {
+        bool hit = false;
+        uint32_t hs = 0u;
+        int lj = 0;
+        float4 pj = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float dx = 0.0f, dy = 0.0f, dz = 0.0f, len2 = 0.0f, w = 0.0f;
+        for (uint32_t s = cur; s < last; ++s) {
+            const int j = static_cast<int>(sorted[s]);
+            if (j <= i) continue;  // each pair once
+            const int yj = static_cast<int>(__umulhi(static_cast<uint32_t>(j), col_magic)), xj = j - yj * cols;
+            if (abs(xi - xj) <= 1 && abs(yi - yj) <= 1) continue;  // the 1-ring is exempt
+            const int l = yj * S + (xj & 3) * Q + (xj >> 2);
+            const float4 q = pos[l];
+            const float ww = pi.w + q.w;
+            if (ww <= 0.0f) continue;
+            const float ex = pi.x - q.x, ey = pi.y - q.y, ez = pi.z - q.z;
+            const float e2 = ex * ex + ey * ey + ez * ez;
+            if (e2 >= d2_min || e2 < PXB_EPSILON) continue;
+            hit = true;
+            hs = s;
+            lj = l;
+            pj = q;
+            dx = ex; dy = ey; dz = ez; len2 = e2; w = ww;
+            break;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (!m) break;
+        any = true;
+        const int k0 = __ffs(m) - 1;
+        if (lane == k0) {
+            const float len = sqrtf(len2);
+            const float sc = (d_min - len) / w;
+            const float px = (dx / len) * sc, py = (dy / len) * sc, pz = (dz / len) * sc;
+            pi.x = pi.x + px * pi.w;
+            pi.y = pi.y + py * pi.w;
+            pi.z = pi.z + pz * pi.w;
+            pj.x = pj.x - px * pj.w;
+            pj.y = pj.y - py * pj.w;
+            pj.z = pj.z - pz * pj.w;
+            pos[lj] = pj;
+            pos[li] = pi;
+            cur = hs + 1u;
+        } else if (lane < k0) {
+            cur = last;
+        }
+        __syncwarp();
+        pi = pos[li];
+    }
+    return any;
+}
+
+// The pair pass of cloth_solver.h:325-365, by warp 0 (the caller's other warps wait at the
+// barrier after it): every particle in index order, each exactly. `pos` holds xyz + inverse mass
+// in layout order; it is written as the pass goes, so it carries no restrict promise.
+__device__ void self_pair_pass(float4* pos, const uint32_t* tab, int n, int cols, int Q, int S, uint32_t buckets,
+                               float d_min, float inv_cell, int lane) {
+    const float d2_min = d_min * d_min;
+    // row of index j = umulhi(j, ceil(2^32 / cols)), checked exact on the host for every j < n
+    const uint32_t col_magic = static_cast<uint32_t>((0x100000000ull + static_cast<uint32_t>(cols) - 1u) /
+                                                     static_cast<uint32_t>(cols));
+    for (int i = 0; i < n; ++i)
+        self_exact_particle(pos, tab, i, n, cols, col_magic, Q, S, buckets, d_min, d2_min, inv_cell, lane);
+    __syncwarp();
 }
 
 }  // namespace

@@ -467,7 +467,12 @@ static void layout_ranks(ClothEntry& e) {
             e.dev.self_hash_off = smem_max;
             e.self_smem = smem_max + bytes;
         }
-        e.self_ok = e.self_smem <= kMaxDynamicSmem;
+        // the pair pass finds a particle's row as umulhi(j, ceil(2^32 / columns)): exact for every j?
+        const uint64_t magic = ((1ull << 32) + static_cast<uint64_t>(e.cols) - 1) / static_cast<uint64_t>(e.cols);
+        bool rows_exact = true;
+        for (uint64_t j = 0; j < e.n_particles && rows_exact; ++j)
+            rows_exact = ((j * magic) >> 32) == j / static_cast<uint64_t>(e.cols);
+        e.self_ok = rows_exact && e.self_smem <= kMaxDynamicSmem;
     }
 }
 

@@ -356,6 +356,55 @@ pxb_status pxb_cloths_step_graph(pxb_context* ctx, const pxb_cloth_step_desc* st
 /* Copies the last step's per-cloth results to host memory (synchronizes the stream). */
 pxb_status pxb_cloths_read_results(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
                                    pxb_cloth_frame_result* out);
+/* ------------------------------------------------------------------------------------------ */
+/* A whole cloth frame: PhysicsWorld::step_cloths_ (physxcoopa/world.h:1749-1847)                */
+/* ------------------------------------------------------------------------------------------ */
+
+/* A rigid body's pose as the caller's world holds it (dynamics::Body::position / orientation,
+ * quaternion x, y, z, w), indexed by pxb_anchor::body_index. An anchor resolves against it only
+ * when `alive` is set and `generation` equals the anchor's body_generation (what
+ * PhysicsWorld::get_body checks); otherwise it keeps its last target. 36 bytes. */
+typedef struct pxb_body_pose {
+    float position[3];
+    float orientation[4];
+    uint32_t generation;
+    uint32_t alive;
+} pxb_body_pose;
+
+typedef struct pxb_cloth_frame_desc {
+    const uint64_t* cloths;                 /* live, enabled cloths to advance this frame */
+    uint32_t n_cloths;
+    const pxb_body_pose* bodies;            /* may be NULL when no cloth has anchors */
+    uint32_t n_bodies;
+    const pxb_collider* colliders;          /* each cloth's gathered colliders, flat */
+    const uint32_t* collider_offsets;       /* n_cloths + 1 offsets; NULL = no colliders */
+    const uint8_t* collider_moving;         /* per cloth: a non-static collider of its list moves
+                                               (world.h:1808-1812); NULL = none does */
+    float gravity[3];
+    const pxb_gravity_source* sources;
+    const uint32_t* source_offsets;
+    float fixed_dt;                         /* PhysicsConfig::fixed_dt */
+    uint32_t cloth_substeps;                /* PhysicsConfig::cloth_substeps */
+    uint32_t cloth_iterations;              /* PhysicsConfig::cloth_iterations */
+    float dt;                               /* this frame's dt */
+} pxb_cloth_frame_desc;
+
+/* One cloth frame as PhysicsWorld::step_cloths_ runs it, for every listed cloth: the frame's
+ * substep count (world.h:1753-1756); each anchor's target from its body's pose,
+ * position + orientation * local_position (world.h:1765-1772); the sleep gate (a moved anchor or
+ * a moving collider wakes the cloth; a sleeping cloth only carries its anchors' targets into their
+ * previous targets, world.h:1815-1825); one batched solve of the awake cloths; then the sleep
+ * bookkeeping on each solved cloth's max particle speed (below params.sleep_threshold for
+ * params.sleep_time seconds: asleep, velocities zeroed, world.h:1831-1845). The collider gather
+ * (broadphase) stays the caller's. Synchronous: it reads the solved cloths' results back.
+ * dt must be positive (PhysicsWorld steps with its fixed dt).
+ * awake_out (n_cloths entries, may be NULL) receives each cloth's awake flag after the frame. */
+pxb_status pxb_cloths_step_frame(pxb_context* ctx, const pxb_cloth_frame_desc* frame, uint8_t* awake_out);
+
+/* Cloth::awake and Cloth::sleep_timer of the listed cloths (a new cloth is awake, timer 0). */
+pxb_status pxb_cloths_read_sleep_state(pxb_context* ctx, const uint64_t* cloths, uint32_t n, uint8_t* awake_out,
+                                       float* sleep_timer_out);
+
 /* Copies positions of the listed cloths (3 floats per particle, cloths in list order) into
  * host memory `out` of `capacity` floats (synchronizes the stream). This is what a renderer or
  * a determinism hash reads back each frame. */
@@ -492,6 +541,12 @@ pxb_status pxb_host_cloth_destroy(pxb_host_cloth* cloth);
 /* cloth::pin_static (cloth_builder.h:271-292). Writes the number newly pinned to pinned_out. */
 pxb_status pxb_host_cloth_pin_static(pxb_host_cloth* cloth, const float world_point[3],
                                      float radius, uint32_t* pinned_out);
+/* cloth::pin_to_body (cloth_builder.h:235-258): pins every not-yet-pinned particle within
+ * `radius` of world_point to the body (index, generation) at the given pose, recording each
+ * anchor's position in the body's frame. Writes the number newly pinned to pinned_out. */
+pxb_status pxb_host_cloth_pin_to_body(pxb_host_cloth* cloth, uint32_t body_index, uint32_t body_generation,
+                                      const float body_position[3], const float body_orientation[4],
+                                      const float world_point[3], float radius, uint32_t* pinned_out);
 /* cloth::build_tethers (cloth_builder.h:308-358): geodesic Dijkstra over the stretch graph. */
 pxb_status pxb_host_cloth_build_tethers(pxb_host_cloth* cloth);
 /* A view of the cloth's arrays; pointers stay valid until the next builder call on it. */

@@ -244,6 +244,18 @@ uint32_t pxbref_cloth_pin_static(void* h, const float* point, float radius) {
     return px::cloth::pin_static(*static_cast<px::cloth::Cloth*>(h), v3(point), radius);
 }
 
+// cloth::pin_to_body (cloth_builder.h:235-258) against a body at the given pose.
+uint32_t pxbref_cloth_pin_to_body(void* h, uint32_t body_index, uint32_t body_generation, const float* body_position,
+                                  const float* body_orientation, const float* point, float radius) {
+    px::dynamics::BodyId id;
+    id.index = body_index;
+    id.generation = body_generation;
+    px::dynamics::Body body;
+    body.position = v3(body_position);
+    body.orientation = q4(body_orientation);
+    return px::cloth::pin_to_body(*static_cast<px::cloth::Cloth*>(h), id, body, v3(point), radius);
+}
+
 void pxbref_cloth_build_tethers(void* h) {
     px::cloth::build_tethers(*static_cast<px::cloth::Cloth*>(h));
 }

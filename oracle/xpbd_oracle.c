@@ -1281,3 +1281,50 @@ void orc_set_strand_roots(orc_strand_set* s, const float* positions, uint32_t n_
         if (i < n_orientations) memcpy(sd->root_orientation, &orientations[4 * i], sizeof(float) * 4);
     }
 }
+
+int orc_world_step_cloth(orc_cloth* c, const pxb_body_pose* bodies, uint32_t n_bodies, int collider_moving,
+                         const pxb_collider* colliders, uint32_t n_colliders, const float gravity[3],
+                         const pxb_gravity_source* sources, uint32_t n_sources, float fixed_dt,
+                         uint32_t cloth_substeps, uint32_t cloth_iterations, float dt, int* awake,
+                         float* sleep_timer) {
+    const uint32_t frame_substeps = orc_frame_substeps(dt, fixed_dt, cloth_substeps);
+    /* world.h:1765-1772: each anchor's target from its body's live pose */
+    int anchor_moved = 0;
+    for (uint32_t a = 0; a < c->n_anchors; ++a) {
+        pxb_anchor* an = &c->anchors[a];
+        const pxb_body_pose* b = NULL;
+        if (bodies && an->body_index < n_bodies && bodies[an->body_index].alive &&
+            bodies[an->body_index].generation == an->body_generation)
+            b = &bodies[an->body_index];
+        const v3 world = ld(an->world_position);
+        const v3 target = b ? add(ld(b->position), qrot(ldq(b->orientation), ld(an->local_position))) : world;
+        const v3 delta = sub(target, world);
+        if (dot(delta, delta) > K_EPSILON) anchor_moved = 1;
+        st(an->world_position, target);
+    }
+    /* world.h:1815-1825: the sleep gate */
+    if (anchor_moved || collider_moving) {
+        *awake = 1;
+        *sleep_timer = 0.0f;
+    }
+    if (!*awake) {
+        for (uint32_t a = 0; a < c->n_anchors; ++a)
+            memcpy(c->anchors[a].prev_world_position, c->anchors[a].world_position, sizeof(float) * 3);
+        return 0;
+    }
+    const int r = orc_step_cloth(c, colliders, n_colliders, gravity, sources, n_sources, frame_substeps,
+                                 cloth_iterations, dt);
+    if (r != 0) return r;
+    /* world.h:1831-1845: sleep bookkeeping */
+    if (orc_max_particle_speed(c->particles, c->n_particles) < c->params.sleep_threshold) {
+        *sleep_timer += dt;
+        if (*sleep_timer >= c->params.sleep_time) {
+            *awake = 0;
+            for (uint32_t i = 0; i < c->n_particles; ++i)
+                c->particles[i].velocity[0] = c->particles[i].velocity[1] = c->particles[i].velocity[2] = 0.0f;
+        }
+    } else {
+        *sleep_timer = 0.0f;
+    }
+    return 1;
+}

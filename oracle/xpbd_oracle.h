@@ -133,6 +133,16 @@ float orc_max_particle_speed(const pxb_particle* particles, uint32_t n);
 /* The substep count PhysicsWorld::step_cloths_ derives from a frame dt (world.h:1753-1757). */
 uint32_t orc_frame_substeps(float dt, float fixed_dt, uint32_t cloth_substeps);
 
+/* PhysicsWorld::step_cloths_'s per-cloth body (world.h:1762-1845) without the collider gather:
+ * anchors from the bodies' poses, the sleep gate, the solve (orc_step_cloth with the frame's
+ * substeps), the sleep bookkeeping. *awake / *sleep_timer are Cloth::awake / sleep_timer, read and
+ * written. Returns 1 when the cloth was solved, 0 when it slept, -1 as orc_solve_cloth. */
+int orc_world_step_cloth(orc_cloth* c, const pxb_body_pose* bodies, uint32_t n_bodies, int collider_moving,
+                         const pxb_collider* colliders, uint32_t n_colliders, const float gravity[3],
+                         const pxb_gravity_source* sources, uint32_t n_sources, float fixed_dt,
+                         uint32_t cloth_substeps, uint32_t cloth_iterations, float dt, int* awake,
+                         float* sleep_timer);
+
 #ifdef __cplusplus
 }
 #endif

@@ -30,6 +30,8 @@ COLLIDER = np.dtype([("type", "<i4"), ("enabled", "<i4"), ("position", "<f4", 3)
                      ("capsule_axis", "<i4"), ("sweep", "<f4", 3), ("end_orientation", "<f4", 4),
                      ("bounds_min", "<f4", 3), ("bounds_max", "<f4", 3),
                      ("geometry", "<u4"), ("geometry_scale", "<f4")])
+BODY_POSE = np.dtype([("position", "<f4", 3), ("orientation", "<f4", 4), ("generation", "<u4"),
+                      ("alive", "<u4")])
 GRAVITY_SOURCE = np.dtype([("centre", "<f4", 3), ("strength", "<f4"), ("radius", "<f4"),
                            ("range", "<f4")])
 FRAME_RESULT = np.dtype([("bounds_min", "<f4", 3), ("bounds_max", "<f4", 3),
@@ -37,6 +39,7 @@ FRAME_RESULT = np.dtype([("bounds_min", "<f4", 3), ("bounds_max", "<f4", 3),
 
 assert PARTICLE.itemsize == 40 and CONSTRAINT.itemsize == 16 and ANCHOR.itemsize == 48
 assert STRAND.itemsize == 64 and COLLIDER.itemsize == 152 and TETHER.itemsize == 12
+assert BODY_POSE.itemsize == 36
 
 SHAPE_SPHERE, SHAPE_BOX, SHAPE_CAPSULE, SHAPE_TRIANGLE_MESH, SHAPE_CONVEX_HULL = range(5)
 
@@ -212,6 +215,14 @@ class ClothStepDesc(C.Structure):
     _fields_ = [("cloths", P), ("n_cloths", u32), ("colliders", P), ("collider_offsets", P),
                 ("gravity", f32 * 3), ("sources", P), ("source_offsets", P),
                 ("substeps", u32), ("iterations", u32), ("h", f32)]
+
+
+class ClothFrameDesc(C.Structure):
+    """pxb_cloth_frame_desc: one PhysicsWorld::step_cloths_ frame."""
+    _fields_ = [("cloths", P), ("n_cloths", u32), ("bodies", P), ("n_bodies", u32), ("colliders", P),
+                ("collider_offsets", P), ("collider_moving", P), ("gravity", f32 * 3), ("sources", P),
+                ("source_offsets", P), ("fixed_dt", f32), ("cloth_substeps", u32), ("cloth_iterations", u32),
+                ("dt", f32)]
 
 
 class StrandStepDesc(C.Structure):

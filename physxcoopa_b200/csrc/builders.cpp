@@ -249,6 +249,41 @@ pxb_status pxb_host_cloth_pin_static(pxb_host_cloth* c, const float world_point[
     return PXB_OK;
 }
 
+// cloth::pin_to_body (cloth_builder.h:235-258): the anchor's local position is
+// inverse(orientation) * (p - body position), glm::inverse of a quaternion being its conjugate
+// over its squared length.
+pxb_status pxb_host_cloth_pin_to_body(pxb_host_cloth* c, uint32_t body_index, uint32_t body_generation,
+                                      const float body_position[3], const float body_orientation[4],
+                                      const float world_point[3], float radius, uint32_t* pinned_out) {
+    if (!c || !body_position || !body_orientation || !world_point) return PXB_ERR_INVALID_ARGUMENT;
+    const float r2 = radius * radius;
+    const pxb::hm::Q4 q = pxb::hm::ldq(body_orientation);
+    const float qq = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+    const pxb::hm::Q4 inv_rot{-q.x / qq, -q.y / qq, -q.z / qq, q.w / qq};
+    const V3 bp = pxb::hm::ld(body_position);
+    const V3 wp{world_point[0], world_point[1], world_point[2]};
+    uint32_t pinned = 0;
+    for (uint32_t i = 0; i < c->particles.size(); ++i) {
+        pxb_particle& p = c->particles[i];
+        if (p.inv_mass == 0.0f) continue;  // already pinned by an earlier anchor
+        const V3 d = pxb::hm::sub(pos_of(p), wp);
+        if (pxb::hm::dot(d, d) > r2) continue;
+        p.inv_mass = 0.0f;
+        p.velocity[0] = p.velocity[1] = p.velocity[2] = 0.0f;
+        pxb_anchor a{};
+        a.particle = i;
+        a.body_index = body_index;
+        a.body_generation = body_generation;
+        pxb::hm::st(a.local_position, pxb::hm::qrot(inv_rot, pxb::hm::sub(pos_of(p), bp)));
+        std::memcpy(a.world_position, p.position, sizeof(a.world_position));
+        std::memcpy(a.prev_world_position, p.position, sizeof(a.prev_world_position));
+        c->anchors.push_back(a);
+        ++pinned;
+    }
+    if (pinned_out) *pinned_out = pinned;
+    return PXB_OK;
+}
+
 pxb_status pxb_host_cloth_build_tethers(pxb_host_cloth* c) {
     if (!c) return PXB_ERR_INVALID_ARGUMENT;
     c->tethers.clear();

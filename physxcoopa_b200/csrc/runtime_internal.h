@@ -45,6 +45,8 @@ struct ClothEntry {
     int n_lam = 0;                         // lambda slots over all ranks
     int threads = 64;
     int warm_smem = 0;  // dynamic shared memory of the warm-start kernel (max over ranks)
+    bool awake = true;        // Cloth::awake (cloth.h:312), kept by pxb_cloths_step_frame
+    float sleep_timer = 0.0f; // Cloth::sleep_timer (cloth.h:313)
     bool self_ok = false;  // self-collision can run (one CTA, hash tables fit in shared memory)
     int self_smem = 0;     // dynamic shared memory with self-collision on
     int aero_grid = 0;
@@ -172,7 +174,7 @@ struct pxb_context {
             if (e.alive && e.dmem) cudaFree(e.dmem);
         for (GeometryEntry& g : geometries)
             if (g.alive && g.dmem) cudaFree(g.dmem);
-        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune, &d_mlp, &d_mlp_io, &d_wresults, &d_rec, &d_grid})
+        for (DevBuf* b : {&d_registry, &d_stage, &d_results, &d_gather, &d_gather_meta, &d_scratch, &d_tune, &d_mlp, &d_mlp_io, &d_wresults, &d_rec, &d_grid, &d_frame})
             if (b->p) cudaFree(b->p);
         if (pinned) cudaFreeHost(pinned);
         if (d_err) cudaFree(d_err);
@@ -216,6 +218,7 @@ struct pxb_context {
     int graph_kernels = 0;
     void drop_graph();
     DevBuf d_wresults, d_rec, d_grid;
+    DevBuf d_frame;  // pxb_cloths_step_frame: anchor records to scatter, cloths whose velocities to zero
     bool warm_fresh = false;
     bool last_step_warm = false;
     pxb_status fetch_warm_results();

@@ -59,6 +59,9 @@ SIGNATURES = {
     "pxb_solve_cloth_host": ([P, C.POINTER(A.ClothDesc), P, P, P, P, P, u32, f32p, u32, u32, f32,
                               f32p, f32p], C.c_int),
     "pxb_project_particles": ([P, P, f32, P, P, u32, P, P, P, P], C.c_int),
+    "pxb_cloths_step_frame": ([P, C.POINTER(A.ClothFrameDesc), P], C.c_int),
+    "pxb_cloths_read_sleep_state": ([P, P, u32, P, P], C.c_int),
+    "pxb_host_cloth_pin_to_body": ([P, u32, u32, f32p, f32p, f32p, f32, C.POINTER(u32)], C.c_int),
     "pxb_geometry_create_hull": ([P, C.POINTER(A.HullDesc), C.POINTER(u32)], C.c_int),
     "pxb_geometry_create_mesh": ([P, C.POINTER(A.MeshDesc), C.POINTER(u32)], C.c_int),
     "pxb_geometry_destroy": ([P, u32], C.c_int),
@@ -160,6 +163,15 @@ class HostCloth:
         if st:
             raise PxbError(st, "pin_static failed")
         return n.value
+
+    def pin_to_body(self, body_index, body_generation, body_position, body_orientation, point, radius):
+        """cloth::pin_to_body: anchors the particles within `radius` of `point` to the body."""
+        out = u32()
+        st = library().pxb_host_cloth_pin_to_body(self._h, body_index, body_generation, _vec(body_position),
+                                                   _vec(body_orientation, 4), _vec(point), radius, C.byref(out))
+        if st:
+            raise PxbError(st, "pin_to_body")
+        return int(out.value)
 
     def build_tethers(self):
         st = library().pxb_host_cloth_build_tethers(self._h)
@@ -489,6 +501,36 @@ class Context:
                                                    A.ptr(out), A.ptr(nrm), A.ptr(dep), A.ptr(hit)),
                     "project_particles")
         return hit, out, nrm, dep
+
+    # --- whole frames (PhysicsWorld::step_cloths_) ------------------------------------------
+    def step_frame(self, ids, bodies=None, colliders=None, collider_moving=None, gravity=(0, 0, -9.81),
+                   sources=None, fixed_dt=1.0 / 60.0, cloth_substeps=4, cloth_iterations=10, dt=1.0 / 60.0):
+        """pxb_cloths_step_frame: anchors from body poses, sleep gate, solve, sleep bookkeeping.
+        Returns each cloth's awake flag after the frame."""
+        ids = np.ascontiguousarray(ids, np.uint64)
+        n = len(ids)
+        cols, coff = _flatten(colliders, A.COLLIDER, n)
+        src, soff = _flatten(sources, A.GRAVITY_SOURCE, n)
+        bod = None if bodies is None else np.ascontiguousarray(bodies, A.BODY_POSE).reshape(-1)
+        mov = None if collider_moving is None else np.ascontiguousarray(collider_moving, np.uint8)
+        d = A.ClothFrameDesc()
+        d.cloths, d.n_cloths = A.ptr(ids), n
+        d.bodies, d.n_bodies = A.ptr(bod), 0 if bod is None else len(bod)
+        d.colliders, d.collider_offsets, d.collider_moving = A.ptr(cols), A.ptr(coff), A.ptr(mov)
+        d.gravity = _vec(gravity)
+        d.sources, d.source_offsets = A.ptr(src), A.ptr(soff)
+        d.fixed_dt, d.cloth_substeps, d.cloth_iterations, d.dt = fixed_dt, cloth_substeps, cloth_iterations, dt
+        awake = np.zeros(n, np.uint8)
+        self._check(self.lib.pxb_cloths_step_frame(self.h, C.byref(d), A.ptr(awake)), "step_frame")
+        return awake
+
+    def read_sleep_state(self, ids):
+        ids = np.ascontiguousarray(ids, np.uint64)
+        awake = np.zeros(len(ids), np.uint8)
+        timer = np.zeros(len(ids), np.float32)
+        self._check(self.lib.pxb_cloths_read_sleep_state(self.h, A.ptr(ids), len(ids), A.ptr(awake), A.ptr(timer)),
+                    "read_sleep_state")
+        return awake, timer
 
     # --- collider geometry ----------------------------------------------------------------
     def create_hull(self, hull) -> int:

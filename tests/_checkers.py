@@ -63,6 +63,8 @@ def oracle():
         lib.orc_step_strands.argtypes = [C.POINTER(OrcStrandSet), P, A.u32, f32p, P, A.u32,
                                          A.u32, A.u32, A.f32]
         lib.orc_set_strand_roots.argtypes = [C.POINTER(OrcStrandSet), P, A.u32, P, A.u32]
+        lib.orc_world_step_cloth.argtypes = [C.POINTER(OrcCloth), P, A.u32, C.c_int, P, A.u32, f32p, P, A.u32,
+                                             A.f32, A.u32, A.u32, A.f32, C.POINTER(C.c_int), C.POINTER(A.f32)]
         lib.orc_geometry_set_hull.argtypes = [A.u32, C.POINTER(A.HullDesc)]
         lib.orc_geometry_set_mesh.argtypes = [A.u32, C.POINTER(A.MeshDesc)]
         lib.orc_geometry_clear.argtypes = []
@@ -86,6 +88,8 @@ def ref():
         lib.pxbref_cloth_free.argtypes = [P]
         lib.pxbref_cloth_pin_static.argtypes = [P, f32p, A.f32]
         lib.pxbref_cloth_pin_static.restype = A.u32
+        lib.pxbref_cloth_pin_to_body.argtypes = [P, A.u32, A.u32, f32p, f32p, f32p, A.f32]
+        lib.pxbref_cloth_pin_to_body.restype = A.u32
         lib.pxbref_cloth_build_tethers.argtypes = [P]
         lib.pxbref_cloth_view.argtypes = [P, C.POINTER(A.ClothDesc)]
         lib.pxbref_cloth_bounds.argtypes = [P, f32p]
@@ -158,6 +162,29 @@ def oracle_step_cloth(c: ClothArrays, colliders=None, gravity=(0, 0, -9.81), sou
     c.time = o.time
     c.bounds = np.array(list(o.bounds_min) + list(o.bounds_max), np.float32)
     return c
+
+
+def oracle_world_step_cloth(c: ClothArrays, state, bodies=None, colliders=None, collider_moving=False,
+                            gravity=(0, 0, -9.81), sources=None, fixed_dt=1.0 / 60.0, cloth_substeps=4,
+                            cloth_iterations=10, dt=1.0 / 60.0):
+    """One PhysicsWorld::step_cloths_ frame of the oracle for one cloth (anchors from body poses,
+    sleep gate, solve, sleep bookkeeping). state: dict with "awake" and "sleep_timer", updated.
+    Returns 1 when the cloth was solved, 0 when it slept."""
+    o = _orc_cloth(c)
+    cols = colliders if colliders is not None else np.zeros(0, A.COLLIDER)
+    src = sources if sources is not None else np.zeros(0, A.GRAVITY_SOURCE)
+    bod = None if bodies is None else np.ascontiguousarray(bodies, A.BODY_POSE).reshape(-1)
+    awake = C.c_int(int(state["awake"]))
+    timer = A.f32(state["sleep_timer"])
+    r = oracle().orc_world_step_cloth(C.byref(o), A.ptr(bod), 0 if bod is None else len(bod), int(collider_moving),
+                                      A.ptr(cols), len(cols), vec(gravity), A.ptr(src), len(src), fixed_dt,
+                                      cloth_substeps, cloth_iterations, dt, C.byref(awake), C.byref(timer))
+    assert r >= 0, "oracle refused the input"
+    state["awake"], state["sleep_timer"] = int(awake.value), np.float32(timer.value)
+    if r == 1:
+        c.time = o.time
+        c.bounds = np.array(list(o.bounds_min) + list(o.bounds_max), np.float32)
+    return r
 
 
 def _orc_strands(s: StrandArrays):
@@ -256,6 +283,11 @@ class RefCloth:
 
     def pin_static(self, point, radius):
         return ref().pxbref_cloth_pin_static(self.h, vec(point), radius)
+
+    def pin_to_body(self, body_index, body_generation, body_position, body_orientation, point, radius):
+        return ref().pxbref_cloth_pin_to_body(self.h, body_index, body_generation, vec(body_position),
+                                              (C.c_float * 4)(*[float(x) for x in body_orientation]), vec(point),
+                                              radius)
 
     def build_tethers(self):
         ref().pxbref_cloth_build_tethers(self.h)

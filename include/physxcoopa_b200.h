@@ -401,6 +401,24 @@ typedef struct pxb_cloth_frame_desc {
  * awake_out (n_cloths entries, may be NULL) receives each cloth's awake flag after the frame. */
 pxb_status pxb_cloths_step_frame(pxb_context* ctx, const pxb_cloth_frame_desc* frame, uint8_t* awake_out);
 
+/* The cloth part of PhysicsWorld::world_state_hash (world.h:1334-1359): FNV-1a 64, continued
+ * from `seed` (1469598103934665603, the FNV offset basis, when no bodies were mixed before), over
+ * each listed cloth's particles in index order, position then velocity, the floats' bytes as they
+ * lie in memory. The device gathers those bytes for every cloth in one launch; the chain itself,
+ * serial by definition, runs on the host. Synchronous. */
+pxb_status pxb_cloths_state_hash(pxb_context* ctx, const uint64_t* cloths, uint32_t n, uint64_t seed,
+                                 uint64_t* hash_out);
+
+/* A renderer's vertex buffer over Cloth::triangles (physxcoopa/cloth/cloth.h:293-299, the index
+ * buffer a renderer draws): 6 floats per particle, cloths in list order, particles in index order
+ * -- position, then the unit vertex normal, the sum of cross(b - a, c - a) over the particle's
+ * triangles (make_grid_cloth's two per grid cell, cloth_builder.h:200-207) normalized, or zero
+ * where that sum is zero. The reference tree has no normal pass (its renderer is outside it), so
+ * this formula is the library's own. Refused for a cloth with no triangle list. `capacity` is in
+ * floats. Synchronous. */
+pxb_status pxb_cloths_read_render_buffer(pxb_context* ctx, const uint64_t* cloths, uint32_t n, float* out,
+                                         size_t capacity);
+
 /* Cloth::awake and Cloth::sleep_timer of the listed cloths (a new cloth is awake, timer 0). */
 pxb_status pxb_cloths_read_sleep_state(pxb_context* ctx, const uint64_t* cloths, uint32_t n, uint8_t* awake_out,
                                        float* sleep_timer_out);

@@ -1476,16 +1476,15 @@ pxb_status pxb_cloths_read_positions(pxb_context* ctx, const uint64_t* cloths, u
     if (static_cast<size_t>(total) > capacity) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "output too small");
     if (n == 0) return PXB_OK;
     if (pxb_status s = ctx->sync_registry()) return s;
-    if (pxb_status s = ctx->grow(ctx->d_gather_meta, 16 * static_cast<size_t>(n), "gather meta")) return s;
+    // the cloth order, then (256-byte aligned) the output offsets: sized before anything is copied
+    if (pxb_status s = ctx->grow(ctx->d_gather_meta, align256(4 * static_cast<size_t>(n)) + 8 * static_cast<size_t>(n),
+                                 "gather meta"))
+        return s;
     if (pxb_status s = ctx->grow(ctx->d_gather, 4 * static_cast<size_t>(total), "gather")) return s;
     char* meta = static_cast<char*>(ctx->d_gather_meta.p);
     pxb_status s = ctx->cuda(cudaMemcpyAsync(meta, order.data(), 4 * n, cudaMemcpyHostToDevice, ctx->stream), "gather order");
     if (!s) s = ctx->cuda(cudaMemcpyAsync(meta + align256(4 * n), offs.data(), 8 * n, cudaMemcpyHostToDevice, ctx->stream), "gather offsets");
     if (s) return s;
-    if (ctx->d_gather_meta.bytes < align256(4 * n) + 8 * n) {
-        if ((s = ctx->grow(ctx->d_gather_meta, align256(4 * n) + 8 * n, "gather meta"))) return s;
-        return pxb_cloths_read_positions(ctx, cloths, n, out, capacity);
-    }
     cudaError_t le = launch_gather_positions(static_cast<const PxbClothDev*>(ctx->d_registry.p),
                                              reinterpret_cast<const int32_t*>(meta),
                                              reinterpret_cast<const int64_t*>(meta + align256(4 * n)),

@@ -60,6 +60,8 @@ SIGNATURES = {
                               f32p, f32p], C.c_int),
     "pxb_project_particles": ([P, P, f32, P, P, u32, P, P, P, P], C.c_int),
     "pxb_cloths_step_frame": ([P, C.POINTER(A.ClothFrameDesc), P], C.c_int),
+    "pxb_cloths_state_hash": ([P, P, u32, u64, C.POINTER(u64)], C.c_int),
+    "pxb_cloths_read_render_buffer": ([P, P, u32, P, C.c_size_t], C.c_int),
     "pxb_cloths_read_sleep_state": ([P, P, u32, P, P], C.c_int),
     "pxb_host_cloth_pin_to_body": ([P, u32, u32, f32p, f32p, f32p, f32, C.POINTER(u32)], C.c_int),
     "pxb_geometry_create_hull": ([P, C.POINTER(A.HullDesc), C.POINTER(u32)], C.c_int),
@@ -523,6 +525,21 @@ class Context:
         awake = np.zeros(n, np.uint8)
         self._check(self.lib.pxb_cloths_step_frame(self.h, C.byref(d), A.ptr(awake)), "step_frame")
         return awake
+
+    def state_hash(self, ids, seed=1469598103934665603):
+        """pxb_cloths_state_hash: world_state_hash's cloth part, continued from `seed`."""
+        ids = np.ascontiguousarray(ids, np.uint64)
+        out = u64()
+        self._check(self.lib.pxb_cloths_state_hash(self.h, A.ptr(ids), len(ids), seed, C.byref(out)), "state_hash")
+        return int(out.value)
+
+    def read_render_buffer(self, ids, n_particles):
+        """pxb_cloths_read_render_buffer: (n, 6) float32, position and unit vertex normal."""
+        ids = np.ascontiguousarray(ids, np.uint64)
+        out = np.zeros((int(n_particles), 6), np.float32)
+        self._check(self.lib.pxb_cloths_read_render_buffer(self.h, A.ptr(ids), len(ids), A.ptr(out), out.size),
+                    "read_render_buffer")
+        return out
 
     def read_sleep_state(self, ids):
         ids = np.ascontiguousarray(ids, np.uint64)

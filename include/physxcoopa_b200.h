@@ -289,6 +289,10 @@ typedef struct pxb_cloth_plan {
                                  layout (one CTA, hash tables in shared memory); 0: a step with
                                  it enabled is refused with PXB_ERR_UNSUPPORTED */
     int32_t self_smem_bytes;  /* dynamic shared memory per CTA with self-collision on */
+    int32_t topology;         /* 0: make_grid_cloth's lists, solved as colour segments; 1: any
+                                 other lists (an imported mesh), one CTA, solved as runs of
+                                 particle-disjoint items in the reference's order (n_colours then
+                                 counts the runs) */
 } pxb_cloth_plan;
 
 /* Plans a cloth without a context or a GPU: validates it exactly as pxb_cloth_add does and
@@ -555,6 +559,26 @@ typedef struct pxb_grid_cloth_desc {
 } pxb_grid_cloth_desc;
 
 pxb_status pxb_host_cloth_make_grid(const pxb_grid_cloth_desc* desc, pxb_host_cloth** out);
+
+/* A cloth from an arbitrary triangle mesh (no reference builder; the reference's README names
+ * "a builder and a batch colouring pass" as what an imported-mesh cloth needs). One particle per
+ * vertex (mass total_mass / n_vertices, as make_grid_cloth spreads it); a stretch constraint per
+ * distinct edge in first-appearance order (triangle by triangle, edges (0,1), (1,2), (2,0)); with
+ * bend set, a bend constraint between the two opposite vertices of every edge exactly two
+ * triangles share (skipped when it repeats a stretch edge or an earlier bend pair). Each list is
+ * coloured greedily, first fit in list order, into particle-disjoint batches and stored batch by
+ * batch. Triangles are the mesh's; columns and rows are 0. A self_distance left at 0 becomes
+ * 0.6 x the mean edge length. */
+typedef struct pxb_mesh_cloth_desc {
+    const float* vertices;   /* xyz per vertex */
+    uint32_t n_vertices;
+    const uint32_t* indices; /* three per triangle */
+    uint32_t n_indices;
+    float total_mass;
+    int32_t bend;
+    pxb_cloth_params params;
+} pxb_mesh_cloth_desc;
+pxb_status pxb_host_cloth_make_mesh(const pxb_mesh_cloth_desc* desc, pxb_host_cloth** out);
 pxb_status pxb_host_cloth_destroy(pxb_host_cloth* cloth);
 /* cloth::pin_static (cloth_builder.h:271-292). Writes the number newly pinned to pinned_out. */
 pxb_status pxb_host_cloth_pin_static(pxb_host_cloth* cloth, const float world_point[3],

@@ -124,12 +124,18 @@ class StrandParams(C.Structure):
 P = C.c_void_p
 
 
+class MeshClothDesc(C.Structure):
+    """pxb_mesh_cloth_desc: a cloth built from an arbitrary triangle mesh."""
+    _fields_ = [("vertices", C.c_void_p), ("n_vertices", C.c_uint32), ("indices", C.c_void_p),
+                ("n_indices", C.c_uint32), ("total_mass", f32), ("bend", C.c_int32), ("params", ClothParams)]
+
+
 class ClothPlan(C.Structure):
     """pxb_cloth_plan: the device layout pxb_cloth_add would choose."""
     _fields_ = [("n_ranks", C.c_int32), ("rows_per_rank", C.c_int32), ("threads", C.c_int32),
                 ("smem_bytes", C.c_int32), ("n_colours", C.c_int32), ("n_segments", C.c_int32),
                 ("layout_slots", C.c_int32), ("constraint_slots", C.c_int32),
-                ("self_collision", C.c_int32), ("self_smem_bytes", C.c_int32)]
+                ("self_collision", C.c_int32), ("self_smem_bytes", C.c_int32), ("topology", C.c_int32)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

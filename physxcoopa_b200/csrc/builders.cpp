@@ -1,11 +1,12 @@
-// builders.cpp -- setup-time host builders of grid cloths (C-ABI pxb_host_cloth_*).
+// builders.cpp -- setup-time host builders of cloths (C-ABI pxb_host_cloth_*).
 //
 // Restates the reference's cloth construction so a cloth built here is the one the reference
 // would build, array for array and bit for bit:
 //   make_grid_cloth   physxcoopa/cloth/cloth_builder.h:81-219
 //   pin_static        physxcoopa/cloth/cloth_builder.h:271-292
 //   build_tethers     physxcoopa/cloth/cloth_builder.h:308-358
-// plus one documented extension, a seeded jitter applied before rest lengths are captured.
+// plus one documented extension, a seeded jitter applied before rest lengths are captured, and
+// pxb_host_cloth_make_mesh, a builder for arbitrary triangle meshes the reference does not have.
 // These run once at setup, on the host (they allocate freely), never per frame.
 #include <algorithm>
 #include <cmath>
@@ -14,6 +15,7 @@
 #include <limits>
 #include <new>
 #include <queue>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -213,6 +215,102 @@ pxb_status pxb_host_cloth_make_grid(const pxb_grid_cloth_desc* desc, pxb_host_cl
         for (size_t b = 0; b < c->stretch_batches.size(); ++b)
             c->stretch_batch_compliance[b] =
                 stretch_is_shear[b] ? c->params.shear_compliance : c->params.stretch_compliance;
+    }
+    *out = c;
+    return PXB_OK;
+}
+
+pxb_status pxb_host_cloth_make_mesh(const pxb_mesh_cloth_desc* desc, pxb_host_cloth** out) {
+    if (!desc || !out) return PXB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    const uint32_t n = desc->n_vertices;
+    if (n == 0 || !desc->vertices || desc->n_indices % 3 != 0 || (desc->n_indices && !desc->indices))
+        return PXB_ERR_INVALID_ARGUMENT;
+    for (uint32_t k = 0; k < desc->n_indices; ++k)
+        if (desc->indices[k] >= n) return PXB_ERR_INVALID_ARGUMENT;
+    auto* c = new (std::nothrow) pxb_host_cloth();
+    if (!c) return PXB_ERR_OUT_OF_MEMORY;
+    c->params = desc->params;
+    // --- particles: mass spread evenly (the rule of cloth_builder.h:95-98) ---
+    const float eps = 1e-6f;
+    const float particle_mass = (desc->total_mass > eps) ? desc->total_mass / static_cast<float>(n) : 0.0f;
+    const float inv_mass = (particle_mass > eps) ? 1.0f / particle_mass : 0.0f;
+    c->particles.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        pxb_particle& q = c->particles[i];
+        std::memcpy(q.position, desc->vertices + 3 * static_cast<size_t>(i), sizeof(q.position));
+        std::memcpy(q.prev_position, q.position, sizeof(q.position));
+        q.velocity[0] = q.velocity[1] = q.velocity[2] = 0.0f;
+        q.inv_mass = inv_mass;
+    }
+    auto key = [](uint32_t a, uint32_t b) {
+        return a < b ? (static_cast<uint64_t>(a) << 32 | b) : (static_cast<uint64_t>(b) << 32 | a);
+    };
+    auto make = [c](uint32_t a, uint32_t b) {
+        pxb_constraint k;
+        k.a = a;
+        k.b = b;
+        k.rest_length = pxb::hm::length(pxb::hm::sub(pos_of(c->particles[a]), pos_of(c->particles[b])));
+        k.lambda = 0.0f;
+        return k;
+    };
+    // --- distinct edges in first-appearance order, with the vertices opposite them ---
+    std::vector<pxb_constraint> stretch, bend;
+    std::vector<std::vector<uint32_t>> opposite;
+    std::unordered_map<uint64_t, uint32_t> edge_of;
+    const uint32_t nt = desc->n_indices / 3;
+    for (uint32_t t = 0; t < nt; ++t) {
+        const uint32_t* v = desc->indices + 3 * static_cast<size_t>(t);
+        for (int e = 0; e < 3; ++e) {
+            const uint32_t a = v[e], b = v[(e + 1) % 3], o = v[(e + 2) % 3];
+            if (a == b) continue;
+            auto it = edge_of.find(key(a, b));
+            if (it == edge_of.end()) {
+                it = edge_of.emplace(key(a, b), static_cast<uint32_t>(stretch.size())).first;
+                stretch.push_back(make(a, b));
+                opposite.emplace_back();
+            }
+            opposite[it->second].push_back(o);
+        }
+    }
+    if (desc->bend) {
+        std::unordered_map<uint64_t, uint32_t> bend_of;
+        for (size_t e = 0; e < stretch.size(); ++e) {
+            if (opposite[e].size() != 2) continue;
+            const uint32_t a = opposite[e][0], b = opposite[e][1];
+            if (a == b || edge_of.count(key(a, b)) || bend_of.count(key(a, b))) continue;
+            bend_of.emplace(key(a, b), static_cast<uint32_t>(bend.size()));
+            bend.push_back(make(a, b));
+        }
+    }
+    // --- greedy first-fit colouring, then the list stored batch by batch ---
+    auto colour = [n](const std::vector<pxb_constraint>& list, std::vector<pxb_constraint>& sorted,
+                      std::vector<pxb_batch>& batches) {
+        std::vector<std::vector<uint8_t>> used;  // used[b][particle]
+        std::vector<uint32_t> batch_of(list.size());
+        for (size_t k = 0; k < list.size(); ++k) {
+            size_t b = 0;
+            while (b < used.size() && (used[b][list[k].a] || used[b][list[k].b])) ++b;
+            if (b == used.size()) used.emplace_back(n, 0);
+            used[b][list[k].a] = used[b][list[k].b] = 1;
+            batch_of[k] = static_cast<uint32_t>(b);
+        }
+        sorted.clear();
+        batches.clear();
+        for (size_t b = 0; b < used.size(); ++b) {
+            const uint32_t begin = static_cast<uint32_t>(sorted.size());
+            for (size_t k = 0; k < list.size(); ++k)
+                if (batch_of[k] == b) sorted.push_back(list[k]);
+            batches.push_back(pxb_batch{begin, static_cast<uint32_t>(sorted.size())});
+        }
+    };
+    colour(stretch, c->stretch, c->stretch_batches);
+    colour(bend, c->bend, c->bend_batches);
+    c->triangles.assign(desc->indices, desc->indices + desc->n_indices);
+    if (c->params.self_distance <= 0.0f && !stretch.empty()) {
+        float sum = 0.0f;
+        for (const pxb_constraint& k : stretch) sum += k.rest_length;
+        c->params.self_distance = 0.6f * (sum / static_cast<float>(stretch.size()));
     }
     *out = c;
     return PXB_OK;

@@ -223,6 +223,44 @@ __device__ __forceinline__ void project_segment(float4* __restrict__ pos, float4
     }
 }
 
+// One run of a general-topology cloth (PxbRun): item i joins the slots packed in ends[i]
+// (a | b << 16), reads rest[i] and, when the batch is compliant, lamv[i]. The items of a run
+// share no particle, so they are projected like the items of a colour segment.
+template <bool kLam>
+__device__ __forceinline__ void load_run_item(PairItem& it, float4* pos, const float* rest, const uint32_t* ends,
+                                              const float* lamv, int i, int count) {
+    it.live = i < count;
+    const int ii = it.live ? i : 0;
+    const uint32_t w = ends[ii];
+    it.pa = &pos[w & 0xffffu];
+    it.pb = &pos[w >> 16];
+    it.a = *it.pa;
+    it.b = *it.pb;
+    it.rest = rest[ii];
+    it.lam = kLam ? lamv[ii] : 0.0f;
+}
+
+template <bool kLam, int kItems>
+__device__ __forceinline__ void project_run(float4* __restrict__ pos, const float* __restrict__ rest,
+                                            const uint32_t* __restrict__ ends, float* __restrict__ lamv, int count,
+                                            float alpha, int tid, int T) {
+    if constexpr (kItems == 2) {
+        for (int i = tid; i < count; i += 2 * T) {
+            PairItem x, y;
+            load_run_item<kLam>(x, pos, rest, ends, lamv, i, count);
+            load_run_item<kLam>(y, pos, rest, ends, lamv, i + T, count);
+            project_item<kLam>(x, lamv, i, alpha);
+            project_item<kLam>(y, lamv, i + T, alpha);
+        }
+    } else {
+        for (int i = tid; i < count; i += T) {
+            PairItem x;
+            load_run_item<kLam>(x, pos, rest, ends, lamv, i, count);
+            project_item<kLam>(x, lamv, i, alpha);
+        }
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
@@ -400,6 +438,29 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     const int4* seg4 = reinterpret_cast<const int4*>(s_seg);
     float4* pos_next = nxt_rank.pos;
     auto iterate = [&](int iters) {
+        if constexpr (kExt && CL == 1 && !kWarm) {
+            if (sC.topology != 0) {
+                // general topology: run after run, a block barrier after each; alpha evaluated
+                // as the reference does, compliance / (hs * hs)
+                const int n_runs = sC.n_runs;
+                const uint32_t* ends = reinterpret_cast<const uint32_t*>(rest + sC.list_items_pad);
+                const int4* runs = reinterpret_cast<const int4*>(sC.runs);
+                const float hs2 = sP.hs * sP.hs;
+                constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
+                for (int it = 0; it < iters; ++it) {
+                    for (int r = 0; r < n_runs; ++r) {
+                        const int4 run = __ldg(&runs[r]);
+                        const float alpha = __int_as_float(run.w) / hs2;
+                        if (run.z >= 0)
+                            project_run<true, kItems>(pos, rest + run.y, ends + run.y, U + run.z, run.x, alpha, tid, T);
+                        else
+                            project_run<false, kItems>(pos, rest + run.y, ends + run.y, U, run.x, alpha, tid, T);
+                        __syncthreads();
+                    }
+                }
+                return;
+            }
+        }
         const int n_colours = sC.n_colours;
         const uint32_t cross = sC.cross_mask;
         for (int it = 0; it < iters; ++it) {
@@ -477,7 +538,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     float4* __restrict__ gvel = sC.vel;
     float4* __restrict__ gprv = sC.prv;
     for (int step = 0; step < steps; ++step) {
-        const bool aero = sP.aero != 0 && sC.aero_grid != 0;
+        const bool list = kExt && CL == 1 && sC.topology != 0;
+        const bool aero = sP.aero != 0 && (sC.aero_grid != 0 || list);
         // --- 1. aerodynamics: gather the shares of the incident triangles -----------------
         // Velocities are parked in U (SoA) for the neighbour reads; each particle's summed
         // share is parked in its own prv slot until integrate consumes it.
@@ -492,6 +554,21 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             const int Q = sC.Q, S = sC.S, cols = sC.columns, rows = sC.rows;
             const f3 wind = mk(sP.wind[0], sP.wind[1], sP.wind[2]);
             const float drag = sP.air_drag, lift = sP.air_lift;
+            if (list) {
+                // general topology: a slot's triangles from the triangle index, ascending
+                for (int l = tid; l < n_local; l += T) {
+                    const int e0 = __ldg(&sC.tri_off[l]), e1 = __ldg(&sC.tri_off[l + 1]);
+                    f3 a = mk(0.0f, 0.0f, 0.0f);
+                    for (int k = e0; k < e1; ++k) {
+                        const int4 t = __ldg(&sC.tri_ent[k]);
+                        tri_share(xyz(pos[t.x]), xyz(pos[t.y]), xyz(pos[t.z]),
+                                  mk(U[t.x], U[n_local + t.x], U[2 * n_local + t.x]),
+                                  mk(U[t.y], U[n_local + t.y], U[2 * n_local + t.y]),
+                                  mk(U[t.z], U[n_local + t.z], U[2 * n_local + t.z]), wind, drag, lift, a);
+                    }
+                    gprv[l] = make_float4(a.x, a.y, a.z, 0.0f);
+                }
+            } else {
             // neighbour rows may belong to the previous / next rank
             auto P3 = [&](int g) -> f3 {
                 const int l = g - base;
@@ -540,6 +617,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     tri_share(p00, P3(lpp), P3(l0p), v00, V3(lpp), V3(l0p), wind, drag, lift, a);
                 }
                 gprv[gl] = make_float4(a.x, a.y, a.z, 0.0f);
+            }
             }
             cluster_or_block_sync<CL>();
         }

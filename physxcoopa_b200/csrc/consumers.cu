@@ -5,7 +5,8 @@
 //     cloth) and the host runs the chain;
 //   * a renderer's vertex buffer over Cloth::triangles (cloth.h:293-299): per particle its
 //     position and unit vertex normal, the normal being the sum of cross(b - a, c - a) over the
-//     particle's grid triangles (make_grid_cloth's two per cell), normalized.
+//     particle's triangles in ascending triangle order (a grid cloth's from make_grid_cloth's two
+//     per cell, any other cloth's from its triangle index), normalized.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -65,6 +66,20 @@ __global__ void render_buffer_kernel(const PxbClothDev* __restrict__ cloths, con
         const int y = i / cols, x = i - y * cols;
         const P3 p = ld(pos, x, y, Q, S);
         P3 nm{0.0f, 0.0f, 0.0f};
+        if (C->topology != 0) {
+            // general topology: the particle's triangles from the triangle index, ascending
+            const int l = slot(x, y, Q, S);
+            for (int k = C->tri_off[l]; k < C->tri_off[l + 1]; ++k) {
+                const int4 t = C->tri_ent[k];
+                const float4 a = pos[t.x], b = pos[t.y], c = pos[t.z];
+                face(P3{a.x, a.y, a.z}, P3{b.x, b.y, b.z}, P3{c.x, c.y, c.z}, nm);
+            }
+            const float l2 = nm.x * nm.x + nm.y * nm.y + nm.z * nm.z;
+            const float s = l2 > 0.0f ? 1.0f / sqrtf(l2) : 0.0f;
+            dst[6 * i] = p.x; dst[6 * i + 1] = p.y; dst[6 * i + 2] = p.z;
+            dst[6 * i + 3] = nm.x * s; dst[6 * i + 4] = nm.y * s; dst[6 * i + 5] = nm.z * s;
+            continue;
+        }
         const bool xm = x >= 1, xp = x + 1 < cols, ym = y >= 1, yp = y + 1 < rows;
         if (xm && ym) {  // cell (x-1, y-1): both faces
             const P3 a = ld(pos, x - 1, y - 1, Q, S), b = ld(pos, x, y - 1, Q, S), d = ld(pos, x - 1, y, Q, S);

@@ -94,7 +94,25 @@ struct PxbClothDev {
     int32_t self_buckets;
     int32_t self_hash_off;
     int32_t self_restage;
-    int32_t pad1;
+    // 0: grid layout (colour segments above). 1: general topology (any other mesh): one row of
+    // `columns` = n particles, constraints as runs of PxbRun, aerodynamics over the triangle
+    // index below; always one CTA.
+    int32_t topology;
+    const struct PxbRun* runs;  // [n_runs], solved in order, one block barrier after each
+    const int32_t* tri_off;     // [n_layout + 1] a slot's entries in tri_ent (ascending triangle)
+    const int4* tri_ent;        // one entry per triangle corner: the triangle's three corner slots
+    int32_t n_runs;
+    int32_t list_items_pad;     // items padded to 4: rest lengths are rest[0, pad), the packed
+                                // endpoint slots (a | b << 16) rest[pad, 2 * pad) as uint32 bits
+};
+
+// A run of a general-topology cloth: consecutive items of one reference batch, no two of which
+// share a particle, so its items are projected in parallel between two block barriers.
+struct alignas(16) PxbRun {
+    int32_t count;      // items (at least 1)
+    int32_t item_base;  // first item's rest / endpoint slot
+    int32_t lam_base;   // first item's lambda slot, or -1 when the batch has zero compliance
+    float compliance;   // the batch's compliance; alpha = compliance / (hs * hs)
 };
 
 // Words of the self-collision tables: bucket ends (buckets + 1), the sorted particle indices (n)

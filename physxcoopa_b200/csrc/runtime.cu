@@ -408,11 +408,150 @@ bool verify_ranks(const ClothEntry& e, const pxb_cloth_desc* d) {
         if (!v) return false;  // never solved
     return true;
 }
+
+// Compliance of batch `b` of the stretch (bend = false) or bend list: the per-batch override,
+// else the params value.
+float batch_compliance(const ClothEntry& e, bool bend, int b) {
+    if (bend) return e.bend_batch_comp.empty() ? e.params.bend_compliance : e.bend_batch_comp[b];
+    return e.stretch_batch_comp.empty() ? e.params.stretch_compliance : e.stretch_batch_comp[b];
+}
+
+// General topology: any constraint lists, solved as solve_cloth walks them (cloth_solver.h:
+// 256-271: every stretch batch, then every bend batch, each in list order; a constraint in no
+// batch is never solved). The walk is cut into runs of consecutive items that share no
+// particle: inside a run the serial order cannot change a result, so the device projects a
+// run's items in parallel and the outcome is the serial walk's. A run may continue into the
+// next batch of the same list when both batches have the same compliance. The particles form
+// one row of n (slot of particle i = (i % 4) * Q + i / 4), so every per-particle path of the
+// grid layout applies unchanged.
+bool build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
+    const uint32_t n = d->n_particles;
+    e.list = true;
+    e.cols = static_cast<int>(n);
+    e.rows = 1;
+    e.Q = (e.cols + 3) / 4;
+    e.S = 4 * e.Q;
+    e.n_layout = e.S;
+    e.n_particles = n;
+    if (e.n_layout > 65535) {
+        why = "a general-topology cloth holds at most 65532 particles";
+        return false;
+    }
+    e.runs.clear();
+    e.run_batch.clear();
+    e.item_ends.clear();
+    e.rest_ref.clear();
+    std::vector<uint32_t> stamp(n, 0);  // run id that last took the particle
+    std::vector<uint8_t> seen(static_cast<size_t>(d->n_stretch) + d->n_bend, 0);
+    uint32_t run_id = 0;
+    int max_run = 0;
+    char buf[256];
+    for (int bend = 0; bend < 2; ++bend) {
+        const uint32_t nb = bend ? d->n_bend_batches : d->n_stretch_batches;
+        const pxb_batch* bb = bend ? d->bend_batches : d->stretch_batches;
+        const pxb_constraint* list = bend ? d->bend : d->stretch;
+        const uint32_t n_list = bend ? d->n_bend : d->n_stretch;
+        const float* comp = bend ? d->bend_batch_compliance : d->stretch_batch_compliance;
+        bool open = false;
+        for (uint32_t b = 0; b < nb; ++b) {
+            if (bb[b].begin > bb[b].end || bb[b].end > n_list) {
+                snprintf(buf, sizeof(buf), "%s batch %u indexes past its list", bend ? "bend" : "stretch", b);
+                why = buf;
+                return false;
+            }
+            if (b > 0 && comp && std::memcmp(&comp[b], &comp[b - 1], 4) != 0) open = false;
+            for (uint32_t k = bb[b].begin; k < bb[b].end; ++k) {
+                const pxb_constraint& c = list[k];
+                const int32_t ref = bend ? static_cast<int32_t>(d->n_stretch + k) : static_cast<int32_t>(k);
+                if (seen[ref]++) {
+                    snprintf(buf, sizeof(buf), "%s constraint %u is in more than one batch", bend ? "bend" : "stretch", k);
+                    why = buf;
+                    return false;
+                }
+                if (!open || stamp[c.a] == run_id || stamp[c.b] == run_id) {
+                    ++run_id;
+                    e.runs.push_back(PxbRun{0, static_cast<int32_t>(e.item_ends.size()), -1, 0.0f});
+                    e.run_batch.push_back(make_int2(bend, static_cast<int>(b)));
+                    open = true;
+                }
+                stamp[c.a] = stamp[c.b] = run_id;
+                const uint32_t la = static_cast<uint32_t>(slot_of_particle(static_cast<int>(c.a), e.cols, e.Q, e.S));
+                const uint32_t lb = static_cast<uint32_t>(slot_of_particle(static_cast<int>(c.b), e.cols, e.Q, e.S));
+                e.item_ends.push_back(la | lb << 16);
+                e.rest_ref.push_back(ref);
+                max_run = std::max(max_run, ++e.runs.back().count);
+            }
+        }
+    }
+    const int items = static_cast<int>(e.item_ends.size());
+    e.list_items_pad = (items + 3) & ~3;
+    e.item_ends.resize(e.list_items_pad, 0u);
+    e.rest_ref.resize(e.list_items_pad, -1);
+    e.n_rest_total = 2 * e.list_items_pad;
+    e.n_colours = 0;
+    e.segs.clear();
+    e.colour_is_bend.clear();
+    e.colour_batch.clear();
+    e.cross_mask = 0;
+    e.ranks.assign(1, ClothEntry::Rank{});
+    ClothEntry::Rank& rk = e.ranks[0];
+    rk.n_rows = 1;
+    rk.colour_seg.assign(1, 0);
+    rk.n_rest_pad = e.n_rest_total;
+    // the triangle index: per slot, its triangles' corner slots in ascending triangle order
+    // (a triangle naming a particle twice is listed twice, as the reference adds its share twice)
+    const uint32_t nt = d->n_triangle_indices / 3;  // cloth_solver.h:204 reads whole triples
+    e.tri_off.assign(e.n_layout + 1, 0);
+    for (uint32_t t = 0; t < 3 * nt; ++t)
+        ++e.tri_off[slot_of_particle(static_cast<int>(d->triangles[t]), e.cols, e.Q, e.S) + 1];
+    for (int l = 0; l < e.n_layout; ++l) e.tri_off[l + 1] += e.tri_off[l];
+    e.tri_ent.assign(3 * nt, make_int4(0, 0, 0, 0));
+    {
+        std::vector<int32_t> fill(e.tri_off.begin(), e.tri_off.end() - 1);
+        for (uint32_t t = 0; t < nt; ++t) {
+            int s[3];
+            for (int q = 0; q < 3; ++q) s[q] = slot_of_particle(static_cast<int>(d->triangles[3 * t + q]), e.cols, e.Q, e.S);
+            for (int q = 0; q < 3; ++q) e.tri_ent[fill[s[q]]++] = make_int4(s[0], s[1], s[2], static_cast<int>(t));
+        }
+    }
+    e.threads = std::min(kClothMaxThreads, std::max(64, ((std::max((max_run + 1) / 2, e.n_layout / 4) + 31) & ~31)));
+    return true;
+}
 }  // namespace
 
 // Re-derives everything that depends on params: lambda slots, union regions, shared memory.
 static void layout_ranks(ClothEntry& e) {
     const bool aero = (e.params.air_drag > 0.0f || e.params.air_lift > 0.0f) && e.n_triangle_indices > 0;
+    if (e.list) {
+        // one CTA: positions | rest lengths + packed endpoints | lambdas or parked velocities
+        int lam = 0;
+        for (size_t r = 0; r < e.runs.size(); ++r) {
+            const float comp = batch_compliance(e, e.run_batch[r].x != 0, e.run_batch[r].y);
+            e.runs[r].compliance = comp;
+            e.runs[r].lam_base = comp != 0.0f ? lam : -1;
+            if (comp != 0.0f) lam += e.runs[r].count;
+        }
+        ClothEntry::Rank& rk = e.ranks[0];
+        rk.n_lam = lam;
+        rk.lam_off = 0;
+        const int u_floats = std::max(lam, aero ? 3 * e.n_layout : 0);
+        rk.smem = 16 * e.n_layout + 4 * rk.n_rest_pad + 4 * ((u_floats + 3) & ~3);
+        PxbRank& dr = e.dev.rank[0];
+        std::memset(&dr, 0, sizeof(dr));
+        dr.n_rows = 1;
+        dr.n_rest_pad = rk.n_rest_pad;
+        dr.n_lam = lam;
+        dr.smem_bytes = rk.smem;
+        e.n_lam = lam;
+        e.dev.smem_bytes = rk.smem;
+        e.warm_smem = rk.smem;
+        e.self_ok = false;  // the reference's self-collision skips grid neighbours: grid cloths only
+        e.self_smem = 0;
+        e.dev.self_buckets = 0;
+        e.dev.self_hash_off = 0;
+        e.dev.self_restage = 0;
+        return;
+    }
     int lam_total = 0, smem_max = 0, warm_max = 0;
     for (size_t r = 0; r < e.ranks.size(); ++r) {
         ClothEntry::Rank& rk = e.ranks[r];
@@ -483,6 +622,11 @@ void pxb_context::refresh_layout(ClothEntry& e) {
 }
 
 pxb_status pxb_context::upload_segments(ClothEntry& e) {
+    if (e.list)
+        return e.runs.empty() ? PXB_OK
+                              : cuda(cudaMemcpyAsync(const_cast<PxbRun*>(e.dev.runs), e.runs.data(),
+                                                     sizeof(PxbRun) * e.runs.size(), cudaMemcpyHostToDevice, stream),
+                                     "upload runs");
     return cuda(cudaMemcpyAsync(const_cast<PxbSeg*>(e.dev.segs), e.segs.data(),
                                 sizeof(PxbSeg) * e.segs.size(), cudaMemcpyHostToDevice, stream),
                 "upload segments");
@@ -560,28 +704,54 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
             return fail(PXB_ERR_INVALID_ARGUMENT, "tether %u indexes past the particles", k);
     for (uint32_t k = 0; k < d->n_triangle_indices; ++k)
         if (d->triangles[k] >= n) return fail(PXB_ERR_INVALID_ARGUMENT, "triangle index past the particles");
-    if (d->n_stretch_batches > PXB_MAX_COLOURS || d->n_bend_batches > PXB_MAX_COLOURS)
-        return fail(PXB_ERR_UNSUPPORTED, "more batches than the grid colouring has");
-
-    // --- grid recognition ---
-    if (d->columns < 2 || d->rows < 2 || d->columns * d->rows != n)
-        return fail(PXB_ERR_UNSUPPORTED, "only make_grid_cloth sheets run on the device path");
-    e.cols = static_cast<int>(d->columns);
-    e.rows = static_cast<int>(d->rows);
-    e.Q = (e.cols + 3) / 4;
-    e.S = 4 * e.Q;
-    e.n_layout = e.rows * e.S;
+    // --- what every layout keeps ---
     e.n_particles = n;
+    e.n_stretch = d->n_stretch;
+    e.n_bend = d->n_bend;
+    e.n_stretch_batches = d->n_stretch_batches;
+    e.n_bend_batches = d->n_bend_batches;
+    if (d->stretch_batch_compliance)
+        e.stretch_batch_comp.assign(d->stretch_batch_compliance, d->stretch_batch_compliance + d->n_stretch_batches);
+    if (d->bend_batch_compliance)
+        e.bend_batch_comp.assign(d->bend_batch_compliance, d->bend_batch_compliance + d->n_bend_batches);
+    e.params = d->params;
+    e.n_triangle_indices = d->n_triangle_indices;
+    e.time = d->time;
+    e.tethers.assign(d->tethers, d->tethers + d->n_tethers);
+    {
+        std::vector<int> per(n, 0);
+        for (const pxb_tether& t : e.tethers)
+            if (++per[t.particle] > 1)
+                return fail(PXB_ERR_UNSUPPORTED, "particle %u has more than one tether", t.particle);
+    }
+
+    // --- grid recognition: make_grid_cloth's lists and triangles, else the general layout ---
     std::vector<ColourSpec> cs;
     std::vector<int32_t> rest_ref, colour_batch;
-    if (!recognise_grid(d, e.Q, e.S, cs, rest_ref, colour_batch))
-        return fail(PXB_ERR_UNSUPPORTED,
-                    "constraint lists are not make_grid_cloth's for a %ux%u grid; only those run on the device path",
-                    d->columns, d->rows);
-    if (d->n_triangle_indices > 0 && !grid_triangles(d))
-        return fail(PXB_ERR_UNSUPPORTED, "triangle list is not make_grid_cloth's");
+    bool is_grid = d->n_stretch_batches <= PXB_MAX_COLOURS && d->n_bend_batches <= PXB_MAX_COLOURS &&
+                   d->columns >= 2 && d->rows >= 2 && static_cast<uint64_t>(d->columns) * d->rows == n;
+    if (is_grid) {
+        e.cols = static_cast<int>(d->columns);
+        e.rows = static_cast<int>(d->rows);
+        e.Q = (e.cols + 3) / 4;
+        e.S = 4 * e.Q;
+        e.n_layout = e.rows * e.S;
+        is_grid = recognise_grid(d, e.Q, e.S, cs, rest_ref, colour_batch) &&
+                  (d->n_triangle_indices == 0 || grid_triangles(d));
+    }
+    if (!is_grid) {
+        std::string why;
+        if (!build_list(d, e, why)) return fail(PXB_ERR_UNSUPPORTED, "%s", why.c_str());
+        e.aero_grid = 0;
+        layout_ranks(e);
+        if (e.dev.smem_bytes > kMaxDynamicSmem)
+            return fail(PXB_ERR_TOO_LARGE,
+                        "a general-topology cloth of %u particles and %d constraint items needs %d bytes of shared "
+                        "memory; one CTA holds %d",
+                        n, e.list_items_pad, e.dev.smem_bytes, kMaxDynamicSmem);
+        return PXB_OK;
+    }
     e.aero_grid = d->n_triangle_indices > 0 ? 1 : 0;
-    e.n_triangle_indices = d->n_triangle_indices;
 
     // --- colours -> per-rank device segments; the smallest cluster whose ranks fit ---
     e.n_colours = static_cast<int>(cs.size());
@@ -593,16 +763,6 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
         for (const HostSeg& h : cs[c].segs)
             if (h.a_base / e.S != (h.a_base + h.d) / e.S) e.cross_mask |= 1u << c;
     }
-    e.n_stretch = d->n_stretch;
-    e.n_bend = d->n_bend;
-    e.n_stretch_batches = d->n_stretch_batches;
-    e.n_bend_batches = d->n_bend_batches;
-    if (d->stretch_batch_compliance)
-        e.stretch_batch_comp.assign(d->stretch_batch_compliance, d->stretch_batch_compliance + d->n_stretch_batches);
-    if (d->bend_batch_compliance)
-        e.bend_batch_comp.assign(d->bend_batch_compliance, d->bend_batch_compliance + d->n_bend_batches);
-    e.params = d->params;
-    e.n_triangle_indices = d->n_triangle_indices;
     int max_colour = 0;
     bool placed = false;
     for (int cl = 1; cl <= PXB_MAX_RANKS && !placed; cl *= 2) {
@@ -623,16 +783,7 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
         e.grid = true;
     }
     if (!verify_ranks(e, d)) return fail(PXB_ERR_UNSUPPORTED, "colour segments do not reproduce the constraint lists");
-    e.time = d->time;
     e.threads = std::min(kClothMaxThreads, std::max(64, ((max_colour + 1) / 2 + 31) & ~31));
-    e.tethers.assign(d->tethers, d->tethers + d->n_tethers);
-    {
-        std::vector<int> per(n, 0);
-        for (const pxb_tether& t : e.tethers)
-            if (++per[t.particle] > 1)
-                return fail(PXB_ERR_UNSUPPORTED, "particle %u has more than one tether", t.particle);
-    }
-
     return PXB_OK;
 }
 
@@ -664,13 +815,15 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
         tether[slot_of_particle(static_cast<int>(t.particle), e.cols, e.Q, e.S)] =
             make_int2(slot_of_particle(static_cast<int>(t.anchor), e.cols, e.Q, e.S), ml);
     }
+    // rest lengths by rest slot; a general-topology cloth follows them with its packed endpoints
     std::vector<float> rest_h(e.n_rest_total, 0.0f);
-    for (int s = 0; s < e.n_rest_total; ++s) {
+    for (size_t s = 0; s < e.rest_ref.size(); ++s) {
         const int32_t r = e.rest_ref[s];
         if (r < 0) continue;  // row padding
         rest_h[s] = r < static_cast<int32_t>(e.n_stretch) ? d->stretch[r].rest_length
                                                           : d->bend[r - e.n_stretch].rest_length;
     }
+    if (e.list) std::memcpy(rest_h.data() + e.list_items_pad, e.item_ends.data(), 4 * e.item_ends.size());
     e.topology.resize(d->n_stretch + d->n_bend);
     for (uint32_t k = 0; k < d->n_stretch; ++k) e.topology[k] = {d->stretch[k].a, d->stretch[k].b, d->stretch[k].rest_length};
     for (uint32_t k = 0; k < d->n_bend; ++k) e.topology[d->n_stretch + k] = {d->bend[k].a, d->bend[k].b, d->bend[k].rest_length};
@@ -690,6 +843,8 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     const size_t o_recs = take(sizeof(PxbAnchorRec) * e.anchor_recs.size());
     const size_t o_segs = take(sizeof(PxbSeg) * e.segs.size());
     const size_t o_edge = take(4 * 6 * L), o_disp = take(16 * L);
+    const size_t o_runs = take(sizeof(PxbRun) * e.runs.size()), o_troff = take(4 * e.tri_off.size()),
+                 o_tent = take(sizeof(int4) * e.tri_ent.size());
     cudaError_t ce = cudaMalloc(&e.dmem, off);
     if (ce != cudaSuccess) return cuda(ce, "cudaMalloc(cloth)");
     e.dbytes = off;
@@ -727,6 +882,14 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
         if (!e.colour_is_bend[c]) e.dev.stretch_mask |= 1u << c;
     e.dev.edge_rest = reinterpret_cast<const float*>(base + o_edge);
     e.dev.disp = reinterpret_cast<float4*>(base + o_disp);
+    if (e.list) {
+        e.dev.topology = 1;
+        e.dev.runs = reinterpret_cast<const PxbRun*>(base + o_runs);
+        e.dev.tri_off = reinterpret_cast<const int32_t*>(base + o_troff);
+        e.dev.tri_ent = reinterpret_cast<const int4*>(base + o_tent);
+        e.dev.n_runs = static_cast<int32_t>(e.runs.size());
+        e.dev.list_items_pad = e.list_items_pad;
+    }
     // rest length from each slot to its six triangulation neighbours (+x, -x, +y, -y, +x+y,
     // -x-y), from the stretch list; 0 where no stretch constraint joins the pair
     std::vector<float> edge_rest(6 * L, 0.0f);
@@ -758,6 +921,8 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     up(base + o_anc, anchor_of.data(), 4 * L, "upload anchor_of");
     up(base + o_teth, tether.data(), 8 * L, "upload tethers");
     up(base + o_edge, edge_rest.data(), 4 * 6 * L, "upload edge rest lengths");
+    up(base + o_troff, e.tri_off.data(), 4 * e.tri_off.size(), "upload triangle index");
+    up(base + o_tent, e.tri_ent.data(), sizeof(int4) * e.tri_ent.size(), "upload triangle entries");
     if (!st) st = cuda(cudaMemsetAsync(base + o_disp, 0, 16 * L, stream), "zero displacement scratch");
     if (!st) st = upload_segments(e);
     if (!st) st = cuda(cudaMemsetAsync(base + o_lam, 0, 4 * static_cast<size_t>(e.n_rest_total), stream), "zero lambdas");
@@ -899,9 +1064,9 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
 
     if (warm) {
         for (uint32_t k = 0; k < n; ++k)
-            if (ents[k]->grid)
-                return fail(PXB_ERR_UNSUPPORTED, "cloth %llu runs on the whole-GPU path, which has no warm start",
-                            (unsigned long long)sd->cloths[k]);
+            if (ents[k]->grid || ents[k]->list)
+                return fail(PXB_ERR_UNSUPPORTED, "cloth %llu runs on the %s path, which has no warm start",
+                            (unsigned long long)sd->cloths[k], ents[k]->grid ? "whole-GPU" : "general-topology");
         for (uint32_t k = 0; k < n; ++k)
             if (ents[k]->warm_smem > kMaxDynamicSmem)
                 return fail(PXB_ERR_TOO_LARGE, "cloth %llu: the warm-start kernel needs %d bytes of shared memory",
@@ -948,11 +1113,11 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         return warm ? std::min(cap, std::max(128, (e.threads + 127) & ~127)) : std::min(e.threads, cap);
     };
     for (uint32_t k = 0; k < n; ++k) fit[k] = ctas_per_sm(launch_smem(*ents[k]), launch_threads(*ents[k]), regs);
-    // cloths with a mesh or hull collider, or with self-collision, launch the kernel with those
-    // stages compiled in
+    // cloths with a mesh or hull collider, with self-collision or of general topology launch the
+    // kernel with those stages compiled in
     std::vector<uint8_t> has_geo(n, 0);
     for (uint32_t k = 0; k < n; ++k)
-        has_geo[k] = self_on(*ents[k]) ||
+        has_geo[k] = self_on(*ents[k]) || ents[k]->list ||
                      (sd->collider_offsets &&
                       cstage.any_geometry(sd->collider_offsets[k], sd->collider_offsets[k + 1] - sd->collider_offsets[k]));
     std::vector<uint32_t> perm(n);
@@ -1308,6 +1473,8 @@ pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out
     out->constraint_slots = e.n_rest_total;
     out->self_collision = e.self_ok && !e.grid ? 1 : 0;
     out->self_smem_bytes = e.self_ok && !e.grid ? e.self_smem : 0;
+    out->topology = e.list ? 1 : 0;
+    if (e.list) out->n_colours = static_cast<int32_t>(e.runs.size());
     return PXB_OK;
 }
 
@@ -1391,6 +1558,18 @@ pxb_status pxb_cloth_read_lambdas(pxb_context* ctx, uint64_t id, float* stretch_
     if (s) return s;
     if (stretch_out) std::fill(stretch_out, stretch_out + n_stretch, 0.0f);
     if (bend_out) std::fill(bend_out, bend_out + n_bend, 0.0f);
+    if (e->list) {
+        for (const PxbRun& run : e->runs) {
+            if (run.lam_base < 0) continue;
+            for (int i = 0; i < run.count; ++i) {
+                const int32_t r = e->rest_ref[run.item_base + i];
+                const float v = lam[run.lam_base + i];
+                if (r < static_cast<int32_t>(e->n_stretch)) { if (stretch_out) stretch_out[r] = v; }
+                else if (bend_out) bend_out[r - e->n_stretch] = v;
+            }
+        }
+        return PXB_OK;
+    }
     for (const ClothEntry::Rank& rk : e->ranks) {
         for (int sg = rk.seg_begin; sg < rk.seg_begin + rk.colour_seg[e->n_colours]; ++sg) {
             const PxbSeg& g = e->segs[sg];

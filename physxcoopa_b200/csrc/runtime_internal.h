@@ -50,6 +50,16 @@ struct ClothEntry {
     bool self_ok = false;  // self-collision can run (one CTA, hash tables fit in shared memory)
     int self_smem = 0;     // dynamic shared memory with self-collision on
     int aero_grid = 0;
+    // General topology (PxbClothDev::topology 1): runs in solve order, each run's batch (bend
+    // flag, batch index) for its compliance, the packed endpoints of every item, and the
+    // per-slot triangle index.
+    bool list = false;
+    std::vector<PxbRun> runs;
+    std::vector<int2> run_batch;
+    std::vector<uint32_t> item_ends;
+    int list_items_pad = 0;
+    std::vector<int32_t> tri_off;
+    std::vector<int4> tri_ent;
     uint32_t n_triangle_indices = 0;
     uint32_t n_stretch = 0, n_bend = 0, n_stretch_batches = 0, n_bend_batches = 0;
     std::vector<float> stretch_batch_comp, bend_batch_comp;

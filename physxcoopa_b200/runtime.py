@@ -68,6 +68,7 @@ SIGNATURES = {
     "pxb_geometry_create_mesh": ([P, C.POINTER(A.MeshDesc), C.POINTER(u32)], C.c_int),
     "pxb_geometry_destroy": ([P, u32], C.c_int),
     "pxb_host_cloth_make_grid": ([C.POINTER(A.GridClothDesc), C.POINTER(P)], C.c_int),
+    "pxb_host_cloth_make_mesh": ([C.POINTER(A.MeshClothDesc), C.POINTER(P)], C.c_int),
     "pxb_host_cloth_destroy": ([P], C.c_int),
     "pxb_host_cloth_pin_static": ([P, f32p, f32, C.POINTER(u32)], C.c_int),
     "pxb_host_cloth_build_tethers": ([P], C.c_int),
@@ -153,6 +154,29 @@ class HostCloth:
         st = library().pxb_host_cloth_make_grid(C.byref(d), C.byref(self._h))
         if st:
             raise PxbError(st, "make_grid failed")
+
+    @classmethod
+    def from_mesh(cls, vertices, indices, total_mass=1.0, bend=True, params=None):
+        """A cloth over an arbitrary triangle mesh (pxb_host_cloth_make_mesh): one particle per
+        vertex, stretch along the distinct edges, bend across shared edges, both lists coloured
+        into particle-disjoint batches."""
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        ix = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        d = A.MeshClothDesc()
+        d.vertices = v.ctypes.data
+        d.n_vertices = len(v)
+        d.indices = ix.ctypes.data if len(ix) else None
+        d.n_indices = len(ix)
+        d.total_mass = total_mass
+        d.bend = 1 if bend else 0
+        d.params = params if params is not None else A.ClothParams.defaults()
+        self = cls.__new__(cls)
+        self._h = P()
+        st = library().pxb_host_cloth_make_mesh(C.byref(d), C.byref(self._h))
+        if st:
+            self._h = None
+            raise PxbError(st, "make_mesh failed")
+        return self
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:

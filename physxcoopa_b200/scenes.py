@@ -343,6 +343,84 @@ def mesh_floor_batch(n=4096, side=25, seed=12):
                       geometries=[floor])
 
 
+def disc_mesh(radius=0.5, rings=12, center=(0.0, 0.0, 1.0), jitter=0.0, seed=0):
+    """A triangulated disc with no grid structure: a centre vertex and `rings` rings of 6k
+    vertices (1 + 3 rings (rings + 1) in all), each ring stitched to the one inside it by an
+    angle-ordered walk, so vertex valences vary from 5 to 7 and edges run in every direction.
+    Vertices get a seeded in-plane jitter of `jitter` x the ring spacing. Faces wind
+    counter-clockwise seen from +z. Returns (vertices [n, 3] float32, indices [3 t] uint32)."""
+    rng = np.random.default_rng(seed)
+    pts = [(0.0, 0.0)]
+    start = [0, 1]
+    for k in range(1, rings + 1):
+        m = 6 * k
+        r = radius * k / rings
+        for j in range(m):
+            a = 2.0 * np.pi * j / m
+            pts.append((r * np.cos(a), r * np.sin(a)))
+        start.append(len(pts))
+    tris = [(0, 1 + j, 1 + (j + 1) % 6) for j in range(6)]
+    for k in range(2, rings + 1):
+        ni, no = 6 * (k - 1), 6 * k
+        si, so = start[k - 1], start[k]
+        i = o = 0
+        while i < ni or o < no:
+            # advance on the ring whose next vertex comes first in angle (exact integer compare)
+            if o < no and (i >= ni or (o + 1) * ni <= (i + 1) * no):
+                tris.append((si + i % ni, so + o, so + (o + 1) % no))
+                o += 1
+            else:
+                tris.append((si + i, so + o % no, si + (i + 1) % ni))
+                i += 1
+    v = np.zeros((len(pts), 3), np.float32)
+    v[:, :2] = np.array(pts, np.float64)
+    if jitter > 0.0:
+        v[1:, :2] += rng.uniform(-1.0, 1.0, (len(pts) - 1, 2)) * (jitter * radius / rings)
+    v += np.asarray(center, np.float32)
+    return v.astype(np.float32), np.array(tris, np.uint32).reshape(-1)
+
+
+def mesh_cloth(rings=12, radius=0.5, center=(0.0, 0.0, 1.0), seed=0, pins=(), params=None, tethers=True,
+               bend=True):
+    """A disc-mesh cloth built by pxb_host_cloth_make_mesh, with static pins ((point, radius)
+    pairs) and, when pinned, tethers."""
+    v, ix = disc_mesh(radius, rings, center, jitter=0.25, seed=seed)
+    h = HostCloth.from_mesh(v, ix, total_mass=1.0, bend=bend, params=params or cloth_params())
+    for point, r in pins:
+        h.pin_static(point, r)
+    if tethers and pins:
+        h.build_tethers()
+    return h.arrays()
+
+
+def mesh_drape(rings=12, seed=0):
+    """One disc-mesh cloth (1 + 3 rings (rings + 1) particles) pinned at two rim points, falling
+    onto a sphere."""
+    center = (0.0, 0.0, 1.0)
+    radius = 0.5
+    pins = [((center[0] - radius, center[1], center[2]), 0.3 * radius / rings),
+            ((center[0] + radius, center[1], center[2]), 0.3 * radius / rings)]
+    c = mesh_cloth(rings, radius, center, seed, pins)
+    col = collider_array([sphere(0.2, (0.0, 0.1, 0.6))])
+    return ClothScene(f"mesh_drape disc r{rings}", [c], [col], meta={"rings": rings})
+
+
+def mesh_cloth_batch(n=1024, rings=20, seed=13):
+    """N disc-mesh cloths (default 1024 x 1261 particles, 3660 stretch and 3540 bend
+    constraints each), every one pinned at two rim points and draped over its own sphere: the
+    general-topology path at batch scale."""
+    rng = np.random.default_rng(seed)
+    radius = 0.5
+    cloths, cols = [], []
+    for k in range(n):
+        center = (float(rng.uniform(-4, 4)), float(rng.uniform(-4, 4)), 1.0)
+        pins = [((center[0] - radius, center[1], center[2]), 0.3 * radius / rings),
+                ((center[0] + radius, center[1], center[2]), 0.3 * radius / rings)]
+        cloths.append(mesh_cloth(rings, radius, center, seed * 100003 + k, pins))
+        cols.append(collider_array([sphere(0.2, (center[0], center[1] + 0.1, 0.6))]))
+    return ClothScene(f"mesh_cloth_batch {n}x disc r{rings}", cloths, cols, meta={"rings": rings, "n": n})
+
+
 def register_geometries(ctx, scene):
     """Registers scene.geometries with a runtime.Context and rewrites the colliders' geometry ids
     from the scene's numbering (geometry k is id k + 1) to the ids the context returned. Returns

@@ -327,10 +327,11 @@ def test_refusals_and_handles(ctx):
     with pytest.raises(R.PxbError) as e:
         ctx.step([cid])
     assert e.value.status == 5  # stale handle
-    odd = ok.copy()
-    odd.stretch = odd.stretch[::-1].copy()  # not make_grid_cloth's order any more
+    past = ok.copy()
+    past.bend_batches = past.bend_batches.copy()
+    past.bend_batches[0]["end"] = len(past.bend) + 1  # a batch past its list
     with pytest.raises(R.PxbError) as e:
-        ctx.add_cloth(odd)
+        ctx.add_cloth(past)
     assert e.value.status == 2
     empty = ok.copy()
     empty.particles = empty.particles[:0]

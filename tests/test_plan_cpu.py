@@ -65,8 +65,12 @@ def test_refusals_match_add_cloth():
     ok = sheet(9, 9)
     odd = ok.copy()
     odd.stretch = odd.stretch[::-1].copy()
+    assert R.plan_cloth(odd)["topology"] == 1  # not make_grid_cloth's lists: the general layout
+    past = ok.copy()
+    past.stretch_batches = past.stretch_batches.copy()
+    past.stretch_batches[-1]["end"] = len(past.stretch) + 1
     with pytest.raises(R.PxbError) as e:
-        R.plan_cloth(odd)
+        R.plan_cloth(past)
     assert e.value.status == 2
     empty = ok.copy()
     empty.particles = empty.particles[:0]
@@ -101,12 +105,12 @@ def test_self_collision_plans_on_one_cta_only():
 
 
 def test_swapped_pair_is_caught_by_item_verification():
-    """Reversing one bend constraint's endpoints keeps the lists' shape but not the device's
-    (a, b) order: the planner must refuse rather than solve a different pair order."""
+    """Reversing one bend constraint's endpoints keeps the lists' shape but not the grid
+    segments' (a, b) order: the grid layout must not take it (it would solve a different pair
+    order); the general layout, which keeps every pair as listed, does."""
     c = sheet(20, 20)
+    assert R.plan_cloth(c)["topology"] == 0
     k = len(c.bend) // 2
     a, b = int(c.bend[k]["a"]), int(c.bend[k]["b"])
     c.bend[k]["a"], c.bend[k]["b"] = b, a
-    with pytest.raises(R.PxbError) as e:
-        R.plan_cloth(c)
-    assert e.value.status == 2
+    assert R.plan_cloth(c)["topology"] == 1

@@ -3,7 +3,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
                     [--workload uniform_batch|single_drape|uneven_batch|warm_start|hair_groom|
-                                large_cloth_hair|mesh_floor] [--cloths C] [--floor mesh|box|none]
+                                large_cloth_hair|mesh_floor|mesh_cloth] [--cloths C]
+                    [--floor mesh|box|none]
                     [--self-collision]
 
 One step = one PhysicsWorld cloth frame for every cloth of the workload: a single batched
@@ -36,6 +37,10 @@ cloth by cloth. The restart fallback (back to the prediction, 20 plain iteration
 beside it. `value` is the warm-start
 throughput, `plain` the plain one.
 
+--workload mesh_cloth is the general-topology path: 1024 cloths built from a triangulated disc
+(1261 particles each, no grid structure; pxb_host_cloth_make_mesh), each pinned at two rim points
+and draped over a sphere.
+
 --impl reference runs only that CPU implementation (rank 0; other ranks exit 0).
 """
 import argparse
@@ -65,7 +70,7 @@ def parse():
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--workload", default="uniform_batch",
                     choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom",
-                             "large_cloth_hair", "mesh_floor"])
+                             "large_cloth_hair", "mesh_floor", "mesh_cloth"])
     ap.add_argument("--cloths", type=int, default=None)
     ap.add_argument("--self-collision", action="store_true",
                     help="turn ClothParams::self_collision on for every cloth of the workload")
@@ -107,6 +112,8 @@ def _build_scene(args, rank):
             sc.geometries = []
             sc.name += f" ({args.floor} floor)"
         return sc
+    if args.workload == "mesh_cloth":
+        return scenes.mesh_cloth_batch(n=args.cloths or 1024, rings=20, seed=13 + rank)
     return scenes.uneven_batch(n=args.cloths or 4096, seed=2 + rank)
 
 

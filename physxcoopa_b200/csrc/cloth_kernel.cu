@@ -1,7 +1,7 @@
 // cloth_kernel.cu -- the XPBD cloth substep on sm_100a: one CTA per cloth, the cloth resident
 // in shared memory for the whole step.
 //
-// Replaces cloth::solve_cloth (physxcoopa/cloth/cloth_solver.h:158-460) for grid cloths. One
+// Replaces cloth::solve_cloth (physxcoopa/cloth/cloth_solver.h:158-460). One
 // launch advances a batch of cloths by one call each (the loop of PhysicsWorld::step_cloths_,
 // world.h:1759-1847). Per CTA:
 //
@@ -13,7 +13,8 @@
 //   substeps   1 aero (per-particle gather of its incident triangles, ascending triangle order)
 //              2+3 integrate + anchor lerp (owner thread)
 //              4 iterations x colours of project_distance over affine colour segments,
-//                one __syncthreads per colour (colours are particle-disjoint)
+//                one __syncthreads per colour (colours are particle-disjoint); a cloth of
+//                general topology walks its runs instead (PxbRun, kExt instantiations only)
 //              5+7+8 tethers, collider projection, velocity + friction + clamp (owner thread)
 //   epilogue   positions back to HBM with cp.async.bulk, lambdas stored, bounds and max speed
 //              reduced with warp shuffles.

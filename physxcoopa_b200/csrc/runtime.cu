@@ -2,13 +2,15 @@
 // registry, the per-step host prologue, launches and read-backs.
 //
 // The registry mirrors PhysicsWorld's cloth slots (add_cloth / remove_cloth, world.h:552-596):
-// generational ids, state resident on the device between steps. A cloth is accepted on the
-// device path when its constraint lists are exactly make_grid_cloth's (cloth_builder.h:81-219);
-// its colours are then expressed as affine segments over the class-permuted layout described in
-// pxb_internal.h, and every segment pair is checked against the reference lists before upload.
+// generational ids, state resident on the device between steps. A cloth whose constraint lists
+// are exactly make_grid_cloth's (cloth_builder.h:81-219) has its colours expressed as affine
+// segments over the class-permuted layout described in pxb_internal.h, every segment pair checked
+// against the reference lists before upload; any other cloth takes the general layout
+// (build_list: the reference's batch walk cut into runs of particle-disjoint items).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <unordered_map>
 #include <cmath>
 #include <cstdarg>
@@ -483,6 +485,80 @@ bool build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
             }
         }
     }
+    // Inside a run the items may be listed in any order (they share no particle). A warp's float4
+    // access to shared memory is served 8 lanes at a time, without bank conflict when those 8
+    // slots differ mod 8: order each run so that every aligned group of 8 items has distinct `a`
+    // residues and distinct `b` residues where the run allows it. Items are bucketed by (a mod 8,
+    // b mod 8); each group is a maximum matching of a residues to b residues over the non-empty
+    // buckets (augmenting paths, fullest buckets first), topped up from the fullest buckets.
+    for (const PxbRun& run : e.runs) {
+        std::vector<std::vector<int>> bucket(64);
+        for (int i = run.count - 1; i >= 0; --i) {
+            const uint32_t w = e.item_ends[run.item_base + i];
+            bucket[(w & 7u) * 8 + ((w >> 16) & 7u)].push_back(i);  // popped from the back: list order
+        }
+        auto fuller = [&](int x, int y) { return bucket[x].size() > bucket[y].size(); };
+        int match_b[8];
+        std::function<bool(int, uint32_t&)> augment = [&](int ra, uint32_t& seen) -> bool {
+            int cand[8], nc = 0;
+            for (int rb = 0; rb < 8; ++rb)
+                if (!bucket[ra * 8 + rb].empty()) cand[nc++] = ra * 8 + rb;
+            std::stable_sort(cand, cand + nc, fuller);
+            for (int q = 0; q < nc; ++q) {
+                const int rb = cand[q] & 7;
+                if (seen >> rb & 1u) continue;
+                seen |= 1u << rb;
+                if (match_b[rb] < 0 || augment(match_b[rb], seen)) {
+                    match_b[rb] = ra;
+                    return true;
+                }
+            }
+            return false;
+        };
+        std::vector<int> order;
+        order.reserve(run.count);
+        int left = run.count;
+        while (left > 0) {
+            std::fill(match_b, match_b + 8, -1);
+            int ras[8], options[8];
+            for (int ra = 0; ra < 8; ++ra) {
+                ras[ra] = ra;
+                options[ra] = 0;
+                for (int rb = 0; rb < 8; ++rb) options[ra] += bucket[ra * 8 + rb].empty() ? 0 : 1;
+            }
+            std::stable_sort(ras, ras + 8, [&](int x, int y) { return options[x] < options[y]; });
+            for (int q = 0; q < 8; ++q) {
+                uint32_t seen = 0;
+                augment(ras[q], seen);
+            }
+            int taken = 0;
+            for (int rb = 0; rb < 8; ++rb)
+                if (match_b[rb] >= 0) {
+                    std::vector<int>& bk = bucket[match_b[rb] * 8 + rb];
+                    order.push_back(bk.back());
+                    bk.pop_back();
+                    ++taken;
+                }
+            int by_size[64];
+            for (int k = 0; k < 64; ++k) by_size[k] = k;
+            std::stable_sort(by_size, by_size + 64, fuller);
+            for (int q = 0; q < 64 && taken < 8; ++q)
+                while (taken < 8 && !bucket[by_size[q]].empty()) {
+                    order.push_back(bucket[by_size[q]].back());
+                    bucket[by_size[q]].pop_back();
+                    ++taken;
+                }
+            left -= taken;
+        }
+        std::vector<uint32_t> ends(run.count);
+        std::vector<int32_t> refs(run.count);
+        for (int i = 0; i < run.count; ++i) {
+            ends[i] = e.item_ends[run.item_base + order[i]];
+            refs[i] = e.rest_ref[run.item_base + order[i]];
+        }
+        std::copy(ends.begin(), ends.end(), e.item_ends.begin() + run.item_base);
+        std::copy(refs.begin(), refs.end(), e.rest_ref.begin() + run.item_base);
+    }
     const int items = static_cast<int>(e.item_ends.size());
     e.list_items_pad = (items + 3) & ~3;
     e.item_ends.resize(e.list_items_pad, 0u);
@@ -514,7 +590,7 @@ bool build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
             for (int q = 0; q < 3; ++q) e.tri_ent[fill[s[q]]++] = make_int4(s[0], s[1], s[2], static_cast<int>(t));
         }
     }
-    e.threads = std::min(kClothMaxThreads, std::max(64, ((std::max((max_run + 1) / 2, e.n_layout / 4) + 31) & ~31)));
+    e.threads = std::max(64, (max_run + 31) & ~31);  // one item per thread; fitted to the SM in plan_cloth
     return true;
 }
 }  // namespace
@@ -749,6 +825,10 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
                         "a general-topology cloth of %u particles and %d constraint items needs %d bytes of shared "
                         "memory; one CTA holds %d",
                         n, e.list_items_pad, e.dev.smem_bytes, kMaxDynamicSmem);
+        // the CTAs shared memory lets an SM hold share the 1024 threads the 64-register kernel
+        // variant fits in the register file; within that, one thread per item of the longest run
+        const int per_sm = std::max(1, 233472 / (e.dev.smem_bytes + kClothStaticSmem + 1024));
+        e.threads = std::min(e.threads, std::max(64, (kClothMaxThreads / per_sm) & ~31));
         return PXB_OK;
     }
     e.aero_grid = d->n_triangle_indices > 0 ? 1 : 0;

@@ -591,6 +591,20 @@ pxb_status pxb_host_cloth_pin_to_body(pxb_host_cloth* cloth, uint32_t body_index
                                       const float world_point[3], float radius, uint32_t* pinned_out);
 /* cloth::build_tethers (cloth_builder.h:308-358): geodesic Dijkstra over the stretch graph. */
 pxb_status pxb_host_cloth_build_tethers(pxb_host_cloth* cloth);
+/* cloth::build_tethers on the device: the same tethers, bit for bit. Dijkstra's float distances
+ * are the unique fixpoint of dist[v] = min over neighbours u of dist[u] + |p_v - p_u| as long as
+ * no edge vanishes in that sum (dist[u] + |p_v - p_u| == dist[u] for two distinct particles); the
+ * device relaxes to that fixpoint in parallel and gives each particle the anchor of the neighbour
+ * the reference's priority queue settles first among those reaching its distance (smallest
+ * (dist, index)). When some edge does vanish the queue's order is no longer that, and the call
+ * returns PXB_ERR_UNSUPPORTED with the tethers unchanged (use pxb_host_cloth_build_tethers).
+ * Writes n_out tethers (at most n_particles) in particle order. */
+pxb_status pxb_build_tethers_device(pxb_context* ctx, const pxb_particle* particles, uint32_t n_particles,
+                                    const pxb_constraint* stretch, uint32_t n_stretch,
+                                    const pxb_anchor* anchors, uint32_t n_anchors, float tether_scale,
+                                    pxb_tether* out, uint32_t capacity, uint32_t* n_out);
+/* The same on a host cloth's arrays, replacing its tethers. */
+pxb_status pxb_host_cloth_build_tethers_device(pxb_context* ctx, pxb_host_cloth* cloth);
 /* A view of the cloth's arrays; pointers stay valid until the next builder call on it. */
 pxb_status pxb_host_cloth_view(pxb_host_cloth* cloth, pxb_cloth_desc* view_out);
 /* Mutable pointers into the same arrays, for host edits before upload. */

@@ -426,6 +426,20 @@ pxb_status pxb_host_cloth_build_tethers(pxb_host_cloth* c) {
     return PXB_OK;
 }
 
+pxb_status pxb_host_cloth_build_tethers_device(pxb_context* ctx, pxb_host_cloth* c) {
+    if (!ctx || !c) return PXB_ERR_INVALID_ARGUMENT;
+    std::vector<pxb_tether> t(c->particles.size());
+    uint32_t k = 0;
+    const pxb_status s = pxb_build_tethers_device(
+        ctx, c->particles.data(), static_cast<uint32_t>(c->particles.size()), c->stretch.data(),
+        static_cast<uint32_t>(c->stretch.size()), c->anchors.data(), static_cast<uint32_t>(c->anchors.size()),
+        c->params.tether_scale, t.data(), static_cast<uint32_t>(t.size()), &k);
+    if (s) return s;  // the cloth keeps its tethers
+    t.resize(k);
+    c->tethers.swap(t);
+    return PXB_OK;
+}
+
 pxb_status pxb_host_cloth_view(pxb_host_cloth* c, pxb_cloth_desc* v) {
     if (!c || !v) return PXB_ERR_INVALID_ARGUMENT;
     std::memset(v, 0, sizeof(*v));

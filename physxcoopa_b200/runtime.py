@@ -72,6 +72,8 @@ SIGNATURES = {
     "pxb_host_cloth_destroy": ([P], C.c_int),
     "pxb_host_cloth_pin_static": ([P, f32p, f32, C.POINTER(u32)], C.c_int),
     "pxb_host_cloth_build_tethers": ([P], C.c_int),
+    "pxb_host_cloth_build_tethers_device": ([P, P], C.c_int),
+    "pxb_build_tethers_device": ([P, P, u32, P, u32, P, u32, f32, P, u32, C.POINTER(u32)], C.c_int),
     "pxb_host_cloth_view": ([P, C.POINTER(A.ClothDesc)], C.c_int),
     "pxb_host_cloth_mutable": ([P, C.POINTER(P), C.POINTER(P), C.POINTER(P)], C.c_int),
     "pxb_measure_smem_bandwidth": ([P, C.POINTER(C.c_double)], C.c_int),
@@ -203,6 +205,22 @@ class HostCloth:
         st = library().pxb_host_cloth_build_tethers(self._h)
         if st:
             raise PxbError(st, "build_tethers failed")
+
+    def mutable_particles(self):
+        """The builder's particle array as a writable numpy view (pxb_host_cloth_mutable); valid
+        until the next builder call."""
+        pp, pa, pr = P(), P(), P()
+        st = library().pxb_host_cloth_mutable(self._h, C.byref(pp), C.byref(pa), C.byref(pr))
+        if st:
+            raise PxbError(st, "host_cloth_mutable")
+        v = A.ClothDesc()
+        library().pxb_host_cloth_view(self._h, C.byref(v))
+        buf = (C.c_char * (v.n_particles * A.PARTICLE.itemsize)).from_address(pp.value)
+        return np.frombuffer(buf, A.PARTICLE)
+
+    def build_tethers_device(self, ctx):
+        """cloth::build_tethers on the device (pxb_host_cloth_build_tethers_device)."""
+        ctx._check(library().pxb_host_cloth_build_tethers_device(ctx.h, self._h), "build_tethers_device")
 
     def arrays(self) -> ClothArrays:
         v = A.ClothDesc()

@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--floor", choices=["mesh", "box", "none"], default="mesh",
                     help="mesh_floor workload: the floor collider (box / none measure the mesh query's share)")
     ap.add_argument("--side", type=int, default=64, help="sheet side of the uniform batch")
+    ap.add_argument("--rings", type=int, default=20,
+                    help="mesh_cloth workload: rings of the disc mesh (1 + 3 rings (rings + 1) particles)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--graph", action="store_true",
@@ -113,7 +115,7 @@ def _build_scene(args, rank):
             sc.name += f" ({args.floor} floor)"
         return sc
     if args.workload == "mesh_cloth":
-        return scenes.mesh_cloth_batch(n=args.cloths or 1024, rings=20, seed=13 + rank)
+        return scenes.mesh_cloth_batch(n=args.cloths or 1024, rings=args.rings, seed=13 + rank)
     return scenes.uneven_batch(n=args.cloths or 4096, seed=2 + rank)
 
 

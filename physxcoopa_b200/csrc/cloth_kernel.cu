@@ -298,7 +298,7 @@ __device__ __forceinline__ void cluster_or_block_sync() {
     else __syncthreads();
 }
 
-template <int kMaxThreads, int CL, bool kWarm, bool kExt>
+template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders,
@@ -345,13 +345,20 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
     __syncthreads();
 
+    // a general-topology cloth whose state stays in HBM runs only in the kGmem instantiation,
+    // and that instantiation runs nothing else
+    constexpr bool kG = kGmem && kExt && CL == 1 && !kWarm;
+    if ((sC.topology == 2) != kG) {
+        if (tid == 0) atomicOr(err, PXB_DEVERR_BAD_INDEX);
+        return;
+    }
     const int n_ranks = CL > 1 ? sC.n_ranks : 1;
     const RankView me = rank_view<1>(sC, smem, rank);  // local view, plain shared addresses
-    float4* pos = me.pos;
-    float* U = me.U;
+    float4* pos = kG ? sC.pos : me.pos;
+    float* U = kG ? sC.list_scratch : me.U;
     const int n_local = me.n_local;
     const int base = me.base;
-    float* rest = reinterpret_cast<float*>(smem + 16 * static_cast<size_t>(n_local));
+    float* rest = kG ? const_cast<float*>(sC.rest) : reinterpret_cast<float*>(smem + 16 * static_cast<size_t>(n_local));
     RankView prv_rank{}, nxt_rank{};
     if constexpr (CL > 1) {
         if (rank > 0) prv_rank = rank_view<CL>(sC, smem, rank - 1);
@@ -359,7 +366,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
 
     // --- prologue: stage positions and rest lengths with TMA bulk copies -------------------
-    if (tid == 0) {
+    if (tid == 0 && !kG) {
         const uint32_t pos_bytes = 16u * static_cast<uint32_t>(n_local);
         const uint32_t rest_bytes = 4u * static_cast<uint32_t>(sC.rank[rank].n_rest_pad);
         mbar_arrive_expect_tx(&bar, pos_bytes + rest_bytes);
@@ -373,7 +380,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
     // A staging wait that runs out records the error and carries on: leaving early would strand
     // the other ranks of the cluster at their barriers.
-    const bool staged = mbar_wait_bounded(&bar, 0);
+    const bool staged = kG || mbar_wait_bounded(&bar, 0);
     if (!staged && tid == 0) atomicOr(err, PXB_DEVERR_TMA_TIMEOUT);
     __syncthreads();
 
@@ -974,7 +981,9 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     // One CTA: a bulk copy back to HBM (its own threads wrote every slot, then fenced). A
     // cluster rank's slots were also written by its neighbour through distributed shared
     // memory, so it stores with plain coalesced writes instead of the async proxy.
-    if constexpr (CL == 1) {
+    if constexpr (kG) {
+        // the positions never left HBM
+    } else if constexpr (CL == 1) {
         fence_proxy_async();
         __syncthreads();
         if (tid == 0) {
@@ -1437,7 +1446,7 @@ cudaError_t launch_cloth_grid(const PxbClothDev* cloths, const PxbClothStep* ste
                : launch_grid_variant<false>(cloths, steps, colliders, sources, order, results, err, gs, slot, n_sms, stream);
 }
 
-template <int kMaxThreads, int CL, bool kWarm, bool kExt>
+template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false>
 static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
                                   const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                   const int32_t* order, PxbFrameResult* results, uint32_t* err,
@@ -1449,10 +1458,10 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     if (e != cudaSuccess) return e;
     if (dev < 64 && !(configured >> dev & 1ull)) {
         cudaFuncAttributes fa;
-        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt>);
+        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem>);
         if (e != cudaSuccess) return e;
         if (fa.sharedSizeBytes > static_cast<size_t>(kClothStaticSmem)) return cudaErrorInvalidConfiguration;
-        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm, kExt>,
+        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
         if (e != cudaSuccess) return e;
         configured |= 1ull << dev;
@@ -1469,7 +1478,7 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt>, cloths, steps, colliders,
+    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem>, cloths, steps, colliders,
                               sources, order, results, err, wsteps, mlp, wres);
 }
 
@@ -1533,9 +1542,19 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
                               const pxb_gravity_source* sources, const int32_t* order,
                               PxbFrameResult* results, uint32_t* err, int n_cloths, int threads,
                               int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres, bool geo) {
+                              const unsigned char* mlp, PxbWarmResult* wres, int ext) {
     if (n_cloths <= 0) return cudaSuccess;
-    if (geo) return launch_geo(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths,
+    if (ext == 2) {
+        // general-topology cloths with their state in HBM: one CTA each, no warm start
+        if (cluster != 1 || wsteps) return cudaErrorInvalidValue;
+        if (threads > cloth_variant_threads(variant)) threads = cloth_variant_threads(variant);
+        switch (variant) {
+            case 0: return launch_variant<512, 1, false, true, true>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+            case 1: return launch_variant<768, 1, false, true, true>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+            default: return launch_variant<1024, 1, false, true, true>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        }
+    }
+    if (ext) return launch_geo(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths,
                                threads, smem_bytes, stream, wsteps, mlp, wres);
     if (wsteps) {
         // warm-start kernels: the 512-thread variant (registers for the network epilogue) or

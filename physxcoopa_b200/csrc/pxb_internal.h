@@ -96,7 +96,9 @@ struct PxbClothDev {
     int32_t self_restage;
     // 0: grid layout (colour segments above). 1: general topology (any other mesh): one row of
     // `columns` = n particles, constraints as runs of PxbRun, aerodynamics over the triangle
-    // index below; always one CTA.
+    // index below; always one CTA. 2: the same with the state left in HBM (positions, rest
+    // lengths and endpoints read in place, lambdas in list_scratch) for cloths whose state
+    // exceeds one CTA's shared memory.
     int32_t topology;
     const struct PxbRun* runs;  // [n_runs], solved in order, one block barrier after each
     const int32_t* tri_off;     // [n_layout + 1] a slot's entries in tri_ent (ascending triangle)
@@ -104,6 +106,7 @@ struct PxbClothDev {
     int32_t n_runs;
     int32_t list_items_pad;     // items padded to 4: rest lengths are rest[0, pad), the packed
                                 // endpoint slots (a | b << 16) rest[pad, 2 * pad) as uint32 bits
+    float* list_scratch;        // topology 2: lambdas / parked velocities in HBM, max(pad, 3 n_layout)
 };
 
 // A run of a general-topology cloth: consecutive items of one reference batch, no two of which

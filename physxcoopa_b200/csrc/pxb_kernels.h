@@ -25,13 +25,14 @@ int cloth_variant_threads(int variant);
 // Registers per thread of a variant's one-CTA kernel (read from the compiled kernel once).
 int cloth_variant_registers(int variant);
 // wsteps non-null selects the warm-start kernel (mlp may then be null: plain solve with the
-// residual measured, or recording only).
+// residual measured, or recording only). ext: 0 the plain kernel, 1 with the mesh / hull,
+// self-collision and general-topology stages, 2 general topology with the state in HBM.
 cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,
                               int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
                               const PxbWarmStep* wsteps = nullptr, const unsigned char* mlp = nullptr,
-                              PxbWarmResult* wres = nullptr, bool geo = false);
+                              PxbWarmResult* wres = nullptr, int ext = 0);
 
 // Warm-start kernel: network warpgroups per CTA and the shared memory they borrow from the
 // lambda region (weights blob, then per warpgroup an input and an activation tile).

@@ -426,7 +426,7 @@ float batch_compliance(const ClothEntry& e, bool bend, int b) {
 // next batch of the same list when both batches have the same compliance. The particles form
 // one row of n (slot of particle i = (i % 4) * Q + i / 4), so every per-particle path of the
 // grid layout applies unchanged.
-bool build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
+pxb_status build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
     const uint32_t n = d->n_particles;
     e.list = true;
     e.cols = static_cast<int>(n);
@@ -437,7 +437,7 @@ bool build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
     e.n_particles = n;
     if (e.n_layout > 65535) {
         why = "a general-topology cloth holds at most 65532 particles";
-        return false;
+        return PXB_ERR_TOO_LARGE;
     }
     e.runs.clear();
     e.run_batch.clear();
@@ -459,7 +459,7 @@ bool build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
             if (bb[b].begin > bb[b].end || bb[b].end > n_list) {
                 snprintf(buf, sizeof(buf), "%s batch %u indexes past its list", bend ? "bend" : "stretch", b);
                 why = buf;
-                return false;
+                return PXB_ERR_UNSUPPORTED;
             }
             if (b > 0 && comp && std::memcmp(&comp[b], &comp[b - 1], 4) != 0) open = false;
             for (uint32_t k = bb[b].begin; k < bb[b].end; ++k) {
@@ -468,7 +468,7 @@ bool build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
                 if (seen[ref]++) {
                     snprintf(buf, sizeof(buf), "%s constraint %u is in more than one batch", bend ? "bend" : "stretch", k);
                     why = buf;
-                    return false;
+                    return PXB_ERR_UNSUPPORTED;
                 }
                 if (!open || stamp[c.a] == run_id || stamp[c.b] == run_id) {
                     ++run_id;
@@ -591,7 +591,7 @@ bool build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
         }
     }
     e.threads = std::max(64, (max_run + 31) & ~31);  // one item per thread; fitted to the SM in plan_cloth
-    return true;
+    return PXB_OK;
 }
 }  // namespace
 
@@ -611,7 +611,7 @@ static void layout_ranks(ClothEntry& e) {
         rk.n_lam = lam;
         rk.lam_off = 0;
         const int u_floats = std::max(lam, aero ? 3 * e.n_layout : 0);
-        rk.smem = 16 * e.n_layout + 4 * rk.n_rest_pad + 4 * ((u_floats + 3) & ~3);
+        rk.smem = e.list_gmem ? 0 : 16 * e.n_layout + 4 * rk.n_rest_pad + 4 * ((u_floats + 3) & ~3);
         PxbRank& dr = e.dev.rank[0];
         std::memset(&dr, 0, sizeof(dr));
         dr.n_rows = 1;
@@ -817,14 +817,17 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
     }
     if (!is_grid) {
         std::string why;
-        if (!build_list(d, e, why)) return fail(PXB_ERR_UNSUPPORTED, "%s", why.c_str());
+        if (pxb_status st = build_list(d, e, why)) return fail(st, "%s", why.c_str());
         e.aero_grid = 0;
         layout_ranks(e);
-        if (e.dev.smem_bytes > kMaxDynamicSmem)
-            return fail(PXB_ERR_TOO_LARGE,
-                        "a general-topology cloth of %u particles and %d constraint items needs %d bytes of shared "
-                        "memory; one CTA holds %d",
-                        n, e.list_items_pad, e.dev.smem_bytes, kMaxDynamicSmem);
+        if (e.dev.smem_bytes > kMaxDynamicSmem) {
+            // beyond one CTA's shared memory: the same walk with the state left in HBM (L2-resident
+            // while its CTA runs), one thread per item of the longest run
+            e.list_gmem = true;
+            layout_ranks(e);
+            e.threads = std::min(e.threads, kClothMaxThreads);
+            return PXB_OK;
+        }
         // the CTAs shared memory lets an SM hold share the 1024 threads the 64-register kernel
         // variant fits in the register file; within that, one thread per item of the longest run
         const int per_sm = std::max(1, 233472 / (e.dev.smem_bytes + kClothStaticSmem + 1024));
@@ -925,6 +928,8 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     const size_t o_edge = take(4 * 6 * L), o_disp = take(16 * L);
     const size_t o_runs = take(sizeof(PxbRun) * e.runs.size()), o_troff = take(4 * e.tri_off.size()),
                  o_tent = take(sizeof(int4) * e.tri_ent.size());
+    // topology 2: lambdas (at most one per item) or parked velocities, whichever params ask for
+    const size_t o_scr = take(e.list_gmem ? 4 * std::max<size_t>(e.list_items_pad, 3 * L) : 0);
     cudaError_t ce = cudaMalloc(&e.dmem, off);
     if (ce != cudaSuccess) return cuda(ce, "cudaMalloc(cloth)");
     e.dbytes = off;
@@ -963,7 +968,8 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.edge_rest = reinterpret_cast<const float*>(base + o_edge);
     e.dev.disp = reinterpret_cast<float4*>(base + o_disp);
     if (e.list) {
-        e.dev.topology = 1;
+        e.dev.topology = e.list_gmem ? 2 : 1;
+        e.dev.list_scratch = e.list_gmem ? reinterpret_cast<float*>(base + o_scr) : nullptr;
         e.dev.runs = reinterpret_cast<const PxbRun*>(base + o_runs);
         e.dev.tri_off = reinterpret_cast<const int32_t*>(base + o_troff);
         e.dev.tri_ent = reinterpret_cast<const int4*>(base + o_tent);
@@ -1194,12 +1200,16 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     };
     for (uint32_t k = 0; k < n; ++k) fit[k] = ctas_per_sm(launch_smem(*ents[k]), launch_threads(*ents[k]), regs);
     // cloths with a mesh or hull collider, with self-collision or of general topology launch the
-    // kernel with those stages compiled in
+    // kernel with those stages compiled in (1); general-topology cloths with their state in HBM
+    // launch its HBM instantiation (2)
     std::vector<uint8_t> has_geo(n, 0);
     for (uint32_t k = 0; k < n; ++k)
-        has_geo[k] = self_on(*ents[k]) || ents[k]->list ||
-                     (sd->collider_offsets &&
-                      cstage.any_geometry(sd->collider_offsets[k], sd->collider_offsets[k + 1] - sd->collider_offsets[k]));
+        has_geo[k] = ents[k]->list_gmem
+                         ? 2
+                         : (self_on(*ents[k]) || ents[k]->list ||
+                            (sd->collider_offsets &&
+                             cstage.any_geometry(sd->collider_offsets[k],
+                                                 sd->collider_offsets[k + 1] - sd->collider_offsets[k])));
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
@@ -1312,15 +1322,15 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
             ++enqueued;
         }
     }
-    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; bool geo; };
+    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; int ext; };
     std::vector<Group> groups;
     for (uint32_t g0 = 0; g0 < n_plain;) {
         const int cluster = static_cast<int>(ents[perm[g0]]->ranks.size());
         const int group_fit = fit[perm[g0]];
-        const bool geo = has_geo[perm[g0]] != 0;
-        Group G{g0, g0, cluster, 64, 0, 0.0, geo};
+        const int ext = has_geo[perm[g0]];
+        Group G{g0, g0, cluster, 64, 0, 0.0, ext};
         while (G.g1 < n_plain && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster &&
-               fit[perm[G.g1]] == group_fit && (has_geo[perm[G.g1]] != 0) == geo) {
+               fit[perm[G.g1]] == group_fit && has_geo[perm[G.g1]] == ext) {
             const ClothEntry& e = *ents[perm[G.g1]];
             G.threads = std::max(G.threads, launch_threads(e));
             G.smem = std::max(G.smem, launch_smem(e));
@@ -1349,7 +1359,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                                            static_cast<int>(G.g1 - G.g0), G.threads, G.smem, st,
                                            warm ? reinterpret_cast<const PxbWarmStep*>(db + o_warm) + G.g0 : nullptr,
                                            warm && warm->warm_iters > 0 ? static_cast<const unsigned char*>(d_mlp.p) : nullptr,
-                                           warm ? static_cast<PxbWarmResult*>(d_wresults.p) + G.g0 : nullptr, G.geo);
+                                           warm ? static_cast<PxbWarmResult*>(d_wresults.p) + G.g0 : nullptr, G.ext);
         if (le != cudaSuccess) return cuda(le, "launch cloth_step");
         ++enqueued;
     }
@@ -1374,9 +1384,9 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                            uint64_t(reinterpret_cast<uintptr_t>(d_registry.p)), uint64_t(reinterpret_cast<uintptr_t>(pinned)),
                            uint64_t(reinterpret_cast<uintptr_t>(d_grid.p)), registry_epoch})
             key.push_back(v);
-        for (uint32_t k = 0; k < n; k += 64) {  // which cloths launch the mesh / hull kernels
+        for (uint32_t k = 0; k < n; k += 32) {  // which kernel instantiation each cloth launches
             uint64_t bits = 0;
-            for (uint32_t j = k; j < std::min(n, k + 64); ++j) bits |= uint64_t(has_geo[j]) << (j - k);
+            for (uint32_t j = k; j < std::min(n, k + 32); ++j) bits |= uint64_t(has_geo[j]) << (2 * (j - k));
             key.push_back(bits);
         }
         if (graph_exec && key == graph_key) {
@@ -1553,7 +1563,7 @@ pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out
     out->constraint_slots = e.n_rest_total;
     out->self_collision = e.self_ok && !e.grid ? 1 : 0;
     out->self_smem_bytes = e.self_ok && !e.grid ? e.self_smem : 0;
-    out->topology = e.list ? 1 : 0;
+    out->topology = e.list_gmem ? 2 : (e.list ? 1 : 0);
     if (e.list) out->n_colours = static_cast<int32_t>(e.runs.size());
     return PXB_OK;
 }

@@ -54,6 +54,7 @@ struct ClothEntry {
     // flag, batch index) for its compliance, the packed endpoints of every item, and the
     // per-slot triangle index.
     bool list = false;
+    bool list_gmem = false;  // its state exceeds one CTA's shared memory: solved in HBM (topology 2)
     std::vector<PxbRun> runs;
     std::vector<int2> run_batch;
     std::vector<uint32_t> item_ends;

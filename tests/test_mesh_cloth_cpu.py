@@ -161,9 +161,13 @@ def test_plan_general_topology_refusals():
     with pytest.raises(R.PxbError) as e:
         R.plan_cloth(past)
     assert e.value.status == A.PXB_ERR_UNSUPPORTED
-    big = S.mesh_cloth(34, tethers=False)  # 3571 particles, ~20k items: past one CTA's shared memory
+    # 3571 particles, ~20k items: past one CTA's shared memory, so its state stays in HBM
+    big = R.plan_cloth(S.mesh_cloth(34, tethers=False))
+    assert big["topology"] == 2 and big["smem_bytes"] == 0 and big["n_ranks"] == 1 and big["threads"] <= 1024
+    # past the 16-bit slot of the packed endpoints
+    v, ix = S.disc_mesh(0.5, 149)  # 67,051 particles
     with pytest.raises(R.PxbError) as e:
-        R.plan_cloth(big)
+        R.plan_cloth(R.HostCloth.from_mesh(v, ix, bend=False).arrays())
     assert e.value.status == A.PXB_ERR_TOO_LARGE
 
 

@@ -215,6 +215,15 @@ def test_general_topology_refusals(ctx):
         assert e.value.status == A.PXB_ERR_UNSUPPORTED
     finally:
         ctx.remove_cloth(cid)
-    with pytest.raises(R.PxbError) as e:
-        ctx.add_cloth(S.mesh_cloth(34, tethers=False))
-    assert e.value.status == A.PXB_ERR_TOO_LARGE
+
+
+def test_cloths_beyond_shared_memory_solve_in_hbm(ctx):
+    """Mesh cloths whose state exceeds one CTA's shared memory (topology 2: positions, rest
+    lengths and lambdas read in place in HBM) beside one that fits, equal to the oracle."""
+    big = S.mesh_drape(rings=34, seed=5)
+    huge = S.mesh_cloth(44, 0.6, (3.0, 0.0, 1.0), seed=6, pins=[((2.4, 0.0, 1.0), 0.3 * 0.6 / 44)])
+    small = S.mesh_drape(rings=8, seed=7)
+    assert R.plan_cloth(big.cloths[0])["topology"] == 2 and R.plan_cloth(huge)["topology"] == 2
+    cloths = [big.cloths[0], huge, small.cloths[0]]
+    cols = [big.colliders[0], collider_array([sphere(0.2, (3.0, 0.1, 0.6))]), small.colliders[0]]
+    run_against_oracle(ctx, cloths, cols, steps=12, check_every=4, what="hbm")

@@ -884,7 +884,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     } else {
                         self_build_hash(pos, tab, sC.n_real, sC.columns, sC.Q, sC.S, buckets, inv_cell, tid, T);
                         if (tid < 32)
-                            self_pair_pass(pos, tab, sC.n_real, sC.columns, sC.Q, sC.S, buckets, d_min, inv_cell, tid);
+                            self_pair_pass(pos, tab, sC.n_real, sC.columns, sC.ref_columns, sC.Q, sC.S, buckets, d_min,
+                                           inv_cell, tid);
                     }
                     __syncthreads();
                     if (sC.self_restage) {

@@ -107,6 +107,8 @@ struct PxbClothDev {
     int32_t list_items_pad;     // items padded to 4: rest lengths are rest[0, pad), the packed
                                 // endpoint slots (a | b << 16) rest[pad, 2 * pad) as uint32 bits
     float* list_scratch;        // topology 2: lambdas / parked velocities in HBM, max(pad, 3 n_layout)
+    int32_t ref_columns;        // Cloth::columns as given: self-collision's 1-ring exemption reads it
+    int32_t pad2;
 };
 
 // A run of a general-topology cloth: consecutive items of one reference batch, no two of which

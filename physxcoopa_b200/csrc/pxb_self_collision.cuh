@@ -114,13 +114,19 @@ __device__ void self_build_hash(const float4* pos, uint32_t* tab, int n, int col
 // first pushing candidate in the reference's order, applies it and moves its cursor past it. The
 // lanes before it have tested all their candidates and are done; the lanes after it scan again
 // from where they were, against the moved particle. Returns whether any push ran.
+// The 1-ring exemption (cloth_solver.h:346-352) reads the cloth's own `columns` (ex_cols, 0: no
+// exemption, row by multiply-high with ex_magic); the layout's columns (cols) only place particles.
+// On a grid cloth the two are the same.
 __device__ bool self_exact_particle(float4* pos, const uint32_t* tab, int i, int n, int cols, uint32_t col_magic,
-                                   int Q, int S, uint32_t buckets, float d_min, float d2_min, float inv_cell,
-                                   int lane) {
+                                   int ex_cols, uint32_t ex_magic, int Q, int S, uint32_t buckets, float d_min,
+                                   float d2_min, float inv_cell, int lane) {
     const uint32_t* ends = tab;
     const uint32_t* sorted = tab + buckets + 1;
     const int yi = static_cast<int>(__umulhi(static_cast<uint32_t>(i), col_magic)), xi = i - yi * cols;
     const int li = yi * S + (xi & 3) * Q + (xi >> 2);
+    const bool ex_same = ex_cols == cols;
+    const int eyi = ex_same ? yi : (ex_cols ? static_cast<int>(__umulhi(static_cast<uint32_t>(i), ex_magic)) : 0);
+    const int exi = ex_same ? xi : i - eyi * ex_cols;
     float4 pi = pos[li];
     if (pi.w == 0.0f) return false;
     const int32_t cx = static_cast<int32_t>(floorf(pi.x * inv_cell));
@@ -143,7 +149,14 @@ __device__ bool self_exact_particle(float4* pos, const uint32_t* tab, int i, int
             const int j = static_cast<int>(sorted[s]);
             if (j <= i) continue;  // each pair once
             const int yj = static_cast<int>(__umulhi(static_cast<uint32_t>(j), col_magic)), xj = j - yj * cols;
-            if (abs(xi - xj) <= 1 && abs(yi - yj) <= 1) continue;  // the 1-ring is exempt
+            if (ex_cols) {  // the 1-ring is exempt
+                int exj = xj, eyj = yj;
+                if (!ex_same) {
+                    eyj = static_cast<int>(__umulhi(static_cast<uint32_t>(j), ex_magic));
+                    exj = j - eyj * ex_cols;
+                }
+                if (abs(exi - exj) <= 1 && abs(eyi - eyj) <= 1) continue;
+            }
             const int l = yj * S + (xj & 3) * Q + (xj >> 2);
             const float4 q = pos[l];
             const float ww = pi.w + q.w;
@@ -187,14 +200,19 @@ __device__ bool self_exact_particle(float4* pos, const uint32_t* tab, int i, int
 // The pair pass of cloth_solver.h:325-365, by warp 0 (the caller's other warps wait at the
 // barrier after it): every particle in index order, each exactly. `pos` holds xyz + inverse mass
 // in layout order; it is written as the pass goes, so it carries no restrict promise.
-__device__ void self_pair_pass(float4* pos, const uint32_t* tab, int n, int cols, int Q, int S, uint32_t buckets,
-                               float d_min, float inv_cell, int lane) {
+__device__ void self_pair_pass(float4* pos, const uint32_t* tab, int n, int cols, int ex_cols, int Q, int S,
+                               uint32_t buckets, float d_min, float inv_cell, int lane) {
     const float d2_min = d_min * d_min;
-    // row of index j = umulhi(j, ceil(2^32 / cols)), checked exact on the host for every j < n
+    // row of index j = umulhi(j, ceil(2^32 / cols)), checked exact on the host for every j < n,
+    // and the same for ex_cols
     const uint32_t col_magic = static_cast<uint32_t>((0x100000000ull + static_cast<uint32_t>(cols) - 1u) /
                                                      static_cast<uint32_t>(cols));
+    const uint32_t ex_magic = ex_cols > 0 ? static_cast<uint32_t>((0x100000000ull + static_cast<uint32_t>(ex_cols) - 1u) /
+                                                                  static_cast<uint32_t>(ex_cols))
+                                          : 0u;
     for (int i = 0; i < n; ++i)
-        self_exact_particle(pos, tab, i, n, cols, col_magic, Q, S, buckets, d_min, d2_min, inv_cell, lane);
+        self_exact_particle(pos, tab, i, n, cols, col_magic, ex_cols, ex_magic, Q, S, buckets, d_min, d2_min, inv_cell,
+                            lane);
     __syncwarp();
 }
 

@@ -595,6 +595,36 @@ pxb_status build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) 
 }
 }  // namespace
 
+// Whether umulhi(j, ceil(2^32 / cols)) == j / cols for every j < n (the device's row of index j).
+static bool rows_by_multiply_high(uint32_t cols, uint32_t n) {
+    if (cols == 0) return true;
+    const uint64_t magic = ((1ull << 32) + cols - 1) / cols;
+    for (uint64_t j = 0; j < n; ++j)
+        if (((j * magic) >> 32) != j / cols) return false;
+    return true;
+}
+
+// Self-collision tables of a one-CTA cloth (the spatial hash's bucket ends, sorted indices and
+// scan scratch): in the rest-length region when they fit there (restaged after the stage), else
+// after the `smem` bytes the step already uses.
+static void place_self_tables(ClothEntry& e, int smem, int pos_bytes, int rest_bytes) {
+    uint32_t buckets = 16;  // detail::hash_bucket_count (cloth_solver.h:111-115)
+    while (buckets < e.n_particles * 2u && buckets < (1u << 22)) buckets <<= 1;
+    const int bytes = (4 * static_cast<int>(PXB_SELF_WORDS(buckets, e.n_particles)) + 15) & ~15;
+    e.dev.self_buckets = static_cast<int32_t>(buckets);
+    if (bytes <= rest_bytes) {
+        e.dev.self_hash_off = pos_bytes;
+        e.dev.self_restage = 1;
+        e.self_smem = smem;
+    } else {
+        e.dev.self_hash_off = smem;
+        e.self_smem = smem + bytes;
+    }
+    e.self_ok = rows_by_multiply_high(static_cast<uint32_t>(e.cols), e.n_particles) &&
+                rows_by_multiply_high(static_cast<uint32_t>(e.ref_columns), e.n_particles) &&
+                e.self_smem <= kMaxDynamicSmem;
+}
+
 // Re-derives everything that depends on params: lambda slots, union regions, shared memory.
 static void layout_ranks(ClothEntry& e) {
     const bool aero = (e.params.air_drag > 0.0f || e.params.air_lift > 0.0f) && e.n_triangle_indices > 0;
@@ -621,11 +651,12 @@ static void layout_ranks(ClothEntry& e) {
         e.n_lam = lam;
         e.dev.smem_bytes = rk.smem;
         e.warm_smem = rk.smem;
-        e.self_ok = false;  // the reference's self-collision skips grid neighbours: grid cloths only
+        e.self_ok = false;
         e.self_smem = 0;
         e.dev.self_buckets = 0;
         e.dev.self_hash_off = 0;
         e.dev.self_restage = 0;
+        if (!e.list_gmem) place_self_tables(e, rk.smem, 16 * e.n_layout, 4 * rk.n_rest_pad);
         return;
     }
     int lam_total = 0, smem_max = 0, warm_max = 0;
@@ -669,25 +700,8 @@ static void layout_ranks(ClothEntry& e) {
     e.dev.self_hash_off = 0;
     e.dev.self_restage = 0;
     if (e.ranks.size() == 1) {
-        uint32_t buckets = 16;  // detail::hash_bucket_count (cloth_solver.h:111-115)
-        while (buckets < e.n_particles * 2u && buckets < (1u << 22)) buckets <<= 1;
-        const int bytes = (4 * static_cast<int>(PXB_SELF_WORDS(buckets, e.n_particles)) + 15) & ~15;
         const ClothEntry::Rank& rk = e.ranks[0];
-        e.dev.self_buckets = static_cast<int32_t>(buckets);
-        if (bytes <= 4 * rk.n_rest_pad) {
-            e.dev.self_hash_off = 16 * rk.n_rows * e.S;
-            e.dev.self_restage = 1;
-            e.self_smem = smem_max;
-        } else {
-            e.dev.self_hash_off = smem_max;
-            e.self_smem = smem_max + bytes;
-        }
-        // the pair pass finds a particle's row as umulhi(j, ceil(2^32 / columns)): exact for every j?
-        const uint64_t magic = ((1ull << 32) + static_cast<uint64_t>(e.cols) - 1) / static_cast<uint64_t>(e.cols);
-        bool rows_exact = true;
-        for (uint64_t j = 0; j < e.n_particles && rows_exact; ++j)
-            rows_exact = ((j * magic) >> 32) == j / static_cast<uint64_t>(e.cols);
-        e.self_ok = rows_exact && e.self_smem <= kMaxDynamicSmem;
+        place_self_tables(e, smem_max, 16 * rk.n_rows * e.S, 4 * rk.n_rest_pad);
     }
 }
 
@@ -792,6 +806,8 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
         e.bend_batch_comp.assign(d->bend_batch_compliance, d->bend_batch_compliance + d->n_bend_batches);
     e.params = d->params;
     e.n_triangle_indices = d->n_triangle_indices;
+    // i % columns and i / columns for i < n are the same for every columns >= n
+    e.ref_columns = static_cast<int>(std::min<uint32_t>(d->columns, n));
     e.time = d->time;
     e.tethers.assign(d->tethers, d->tethers + d->n_tethers);
     {
@@ -941,6 +957,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.self_buckets = keep_ranks.self_buckets;
     e.dev.self_hash_off = keep_ranks.self_hash_off;
     e.dev.self_restage = keep_ranks.self_restage;
+    e.dev.ref_columns = e.ref_columns;
     e.dev.pos = reinterpret_cast<float4*>(base + o_pos);
     e.dev.vel = reinterpret_cast<float4*>(base + o_vel);
     e.dev.prv = reinterpret_cast<float4*>(base + o_prv);
@@ -1130,8 +1147,9 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         if (!ents[k]) return fail(PXB_ERR_INVALID_HANDLE, "cloth id %llu is not live", (unsigned long long)sd->cloths[k]);
         if (self_on(*ents[k]) && (!ents[k]->self_ok || ents[k]->grid))
             return fail(PXB_ERR_UNSUPPORTED,
-                        "cloth %llu: self-collision runs on cloths solved by one CTA (sides up to 64) whose hash "
-                        "tables fit in shared memory", (unsigned long long)sd->cloths[k]);
+                        "cloth %llu: self-collision runs on cloths one CTA holds in shared memory (grid sides up to "
+                        "64, general topology up to ~2800 particles) whose hash tables fit there",
+                        (unsigned long long)sd->cloths[k]);
         if (sd->collider_offsets) {
             if (sd->collider_offsets[k + 1] < sd->collider_offsets[k])
                 return fail(PXB_ERR_INVALID_ARGUMENT, "collider offsets decrease");

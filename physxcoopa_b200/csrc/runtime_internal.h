@@ -55,6 +55,7 @@ struct ClothEntry {
     // per-slot triangle index.
     bool list = false;
     bool list_gmem = false;  // its state exceeds one CTA's shared memory: solved in HBM (topology 2)
+    int ref_columns = 0;     // Cloth::columns as given (self-collision's 1-ring exemption)
     std::vector<PxbRun> runs;
     std::vector<int2> run_batch;
     std::vector<uint32_t> item_ends;

@@ -136,7 +136,7 @@ def unbatched(c):
 def test_plan_general_topology():
     m = S.mesh_cloth(12)
     p = R.plan_cloth(m)
-    assert p["topology"] == 1 and p["n_ranks"] == 1 and p["n_segments"] == 0 and p["self_collision"] == 0
+    assert p["topology"] == 1 and p["n_ranks"] == 1 and p["n_segments"] == 0 and p["self_collision"] == 1
     assert p["n_colours"] == len(m.stretch_batches) + len(m.bend_batches)  # one run per coloured batch
     g = S.single_drape().cloths[0]
     assert R.plan_cloth(g)["topology"] == 0
@@ -164,6 +164,7 @@ def test_plan_general_topology_refusals():
     # 3571 particles, ~20k items: past one CTA's shared memory, so its state stays in HBM
     big = R.plan_cloth(S.mesh_cloth(34, tethers=False))
     assert big["topology"] == 2 and big["smem_bytes"] == 0 and big["n_ranks"] == 1 and big["threads"] <= 1024
+    assert big["self_collision"] == 0  # its hash tables would need the shared memory it does not get
     # past the 16-bit slot of the packed endpoints
     v, ix = S.disc_mesh(0.5, 149)  # 67,051 particles
     with pytest.raises(R.PxbError) as e:
@@ -198,3 +199,31 @@ def test_oracle_equals_reference_on_serial_grid_lists():
     c = unbatched(sc.cloths[0])
     c.params.has_shear_compliance = 0
     oracle_vs_reference(c, sc.colliders[0], steps=15)
+
+
+def self_colliding_mesh(rings=10, seed=3):
+    """A disc mesh pinned at one rim point with self_distance 2.2 x its mean edge: non-adjacent
+    particles push on every substep (columns 0: no 1-ring exemption, as the reference reads it)."""
+    p = S.cloth_params(self_collision=1, has_shear_compliance=0)
+    c = S.mesh_cloth(rings, 0.5, (0.0, 0.0, 1.0), seed=seed, params=p, pins=[((0.5, 0.0, 1.0), 0.3 * 0.5 / rings)])
+    c.params.self_distance = 2.2 * float(np.mean(c.stretch["rest_length"]))
+    return c, collider_array([sphere(0.15, (0.1, 0.05, 0.7))])
+
+
+def self_colliding_regrid():
+    """The single drape's grid with its lists in one serial batch each and self_distance 2.2 x the
+    spacing: general topology, the 1-ring exemption through the cloth's own columns (32)."""
+    sc = S.single_drape(seed=9)
+    c = unbatched(sc.cloths[0])
+    c.params.has_shear_compliance = 0
+    c.params.self_collision = 1
+    c.params.self_distance = 2.2 * S.SPACING
+    return c, sc.colliders[0]
+
+
+@pytest.mark.skipif(not K.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("scene", [self_colliding_mesh, self_colliding_regrid])
+def test_oracle_equals_reference_with_self_collision_on_general_topology(scene):
+    c, col = scene()
+    assert R.plan_cloth(c)["topology"] == 1 and R.plan_cloth(c)["self_collision"] == 1
+    oracle_vs_reference(c, col, steps=8)

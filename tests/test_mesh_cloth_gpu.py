@@ -14,7 +14,7 @@ import _checkers as K
 from test_cloth_gpu import assert_equal_particles
 from test_consumers_gpu import fnv1a, state_bytes, FNV_BASIS
 from test_frame_oracle_ref import FIXED_DT, body_poses
-from test_mesh_cloth_cpu import unbatched
+from test_mesh_cloth_cpu import self_colliding_mesh, self_colliding_regrid, unbatched
 
 pytestmark = pytest.mark.gpu
 
@@ -197,8 +197,21 @@ def test_mesh_render_buffer_and_state_hash(ctx):
         ctx.remove_cloth(cid)
 
 
+@pytest.mark.parametrize("scene", [self_colliding_mesh, self_colliding_regrid])
+def test_self_collision_on_general_topology_equals_oracle(ctx, scene):
+    """Self-collision (cloth_solver.h:291-366) on general-topology cloths in shared memory, pushes
+    on every substep: the 1-ring exemption reads the cloth's own columns (0 for a mesh)."""
+    c, col = scene()
+    orc = run_against_oracle(ctx, [c], [col], steps=20, check_every=5, what=scene.__name__)
+    off = c.copy()
+    off.params.self_collision = 0
+    for _ in range(20):
+        K.oracle_step_cloth(off, col)
+    assert not np.array_equal(off.particles["position"], orc[0].particles["position"])  # the stage acted
+
+
 def test_general_topology_refusals(ctx):
-    c = S.mesh_cloth(6)
+    c = S.mesh_cloth(34, tethers=False)  # state in HBM: no shared memory for the hash tables
     c.params.self_collision = 1
     cid = ctx.add_cloth(c)
     try:

@@ -619,7 +619,9 @@ pxb_status pxb_host_cloth_mutable(pxb_host_cloth* cloth, pxb_particle** particle
 /* Uploads a strand set built by make_strands (strand_builder.h:58-127): strands contiguous,
  * stretch constraints in the builder's even / odd batches. Refuses an empty set with
  * PXB_ERR_INVALID_ARGUMENT (add_strands does the same), another layout with
- * PXB_ERR_UNSUPPORTED, and a strand of more than 32 particles with PXB_ERR_TOO_LARGE. */
+ * PXB_ERR_UNSUPPORTED, and a strand of more than 8192 particles with PXB_ERR_TOO_LARGE. Sets whose
+ * strands all have at most 32 particles run one lane per particle; a set with a longer strand
+ * runs the long-strand kernel (lanes stride over the particles, positions in shared memory). */
 pxb_status pxb_strands_add(pxb_context* ctx, const pxb_strand_set_desc* desc, uint64_t* id_out);
 pxb_status pxb_strands_remove(pxb_context* ctx, uint64_t id);
 pxb_status pxb_strands_set_params(pxb_context* ctx, uint64_t id, const pxb_strand_params* params);

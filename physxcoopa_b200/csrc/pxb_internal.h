@@ -229,8 +229,9 @@ struct PxbClothStep {
 };
 
 // One registered strand set on the device. Particles are strand-major, 32 slots per strand
-// (slot = strand * 32 + k, k < count[strand] <= 32); slot k's rest length is the one of the
-// stretch constraint (k, k + 1).
+// (slot = strand * 32 + k, k < count[strand] <= 32), or, when some strand is longer, each strand
+// padded to a multiple of 32 slots from base[strand]; slot k's rest length and lambda are the
+// stretch constraint (k, k + 1)'s.
 struct PxbStrandDev {
     float4* pos;               // xyz + inv_mass
     float4* vel;
@@ -246,7 +247,13 @@ struct PxbStrandDev {
     float* bounds_prev;        // last decoded bounds: min xyz, max xyz, max speed^2
     float* bounds_out;         // where this step's decoded bounds go (same buffer, stream-ordered)
     int32_t n_strands;
-    int32_t pad_;
+    // 0: every strand has at most 32 particles, slot = strand * 32 + k (strand_step_kernel).
+    // 1: some strand is longer: slot = base[strand] + k, strands padded to multiples of 32, solved
+    //    by strand_long_kernel, `warps` strands per block, each with pad_count slots of shared memory.
+    int32_t long_mode;
+    const int32_t* base;
+    int32_t pad_count;
+    int32_t warps;
 };
 
 // Per set, per step: the prologue of solve_strands (strand_solver.h:127-155) on the host.

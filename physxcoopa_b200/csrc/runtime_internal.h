@@ -86,6 +86,8 @@ struct StrandEntry {
     uint32_t generation = 0;
     uint32_t n_particles = 0, n_strands = 0, n_stretch = 0;
     std::vector<uint32_t> first, count;
+    std::vector<int32_t> base;             // first device slot of each strand (PxbStrandDev)
+    size_t n_slots = 0;                    // device slots over all strands
     std::vector<pxb_strand> records;       // root targets, host mirror
     std::vector<int32_t> stretch_slot;     // stretch list index -> device slot
     std::vector<TopologyEdge> topology;

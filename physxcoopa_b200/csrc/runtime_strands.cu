@@ -53,14 +53,14 @@ pxb_status pxb_context::upload_strand_records(StrandEntry& e) {
 // The per-particle global-shape falloff pow(1 - k / (count - 1), falloff) (strand_solver.h:
 // 227-229), evaluated on the host with the same single-precision operations as the reference.
 pxb_status pxb_context::upload_strand_shape(StrandEntry& e) {
-    std::vector<float> w(32 * static_cast<size_t>(e.n_strands), 0.0f);
+    std::vector<float> w(e.n_slots, 0.0f);
     for (uint32_t s = 0; s < e.n_strands; ++s) {
         const uint32_t n = e.count[s];
         if (n < 2) continue;
         const float inv_last = 1.0f / static_cast<float>(n - 1);
         for (uint32_t k = 1; k < n; ++k) {
             const float along = static_cast<float>(k) * inv_last;
-            w[32 * static_cast<size_t>(s) + k] = std::pow(1.0f - along, e.params.global_shape_falloff);
+            w[e.base[s] + k] = std::pow(1.0f - along, e.params.global_shape_falloff);
         }
     }
     pxb_status st = cuda(cudaMemcpyAsync(const_cast<float*>(e.dev.wshape), w.data(), 4 * w.size(),
@@ -69,14 +69,18 @@ pxb_status pxb_context::upload_strand_shape(StrandEntry& e) {
     return cuda(cudaStreamSynchronize(stream), "upload shape weights");
 }
 
+// Longest strand the device path takes: its positions and lambdas (20 B per particle) sit in one
+// warp's share of shared memory.
+constexpr uint32_t kMaxStrandParticles = 8192;
+
 static pxb_status strands_upload_particles(pxb_context* ctx, StrandEntry& e, const pxb_particle* particles) {
-    const size_t S = 32 * static_cast<size_t>(e.n_strands);
+    const size_t S = e.n_slots;
     std::vector<float4> pos(S, make_float4(0, 0, 0, 0)), vel(S, make_float4(0, 0, 0, 0)),
         prv(S, make_float4(0, 0, 0, 0));
     for (uint32_t s = 0; s < e.n_strands; ++s)
         for (uint32_t k = 0; k < e.count[s]; ++k) {
             const pxb_particle& p = particles[e.first[s] + k];
-            const size_t l = 32 * static_cast<size_t>(s) + k;
+            const size_t l = e.base[s] + k;
             pos[l] = make_float4(p.position[0], p.position[1], p.position[2], p.inv_mass);
             vel[l] = make_float4(p.velocity[0], p.velocity[1], p.velocity[2], 0.0f);
             prv[l] = make_float4(p.prev_position[0], p.prev_position[1], p.prev_position[2], 0.0f);
@@ -103,10 +107,21 @@ static pxb_status strands_add(pxb_context* ctx, const pxb_strand_set_desc* d, ui
     for (uint32_t s = 0; s < d->n_strands; ++s) {
         const pxb_strand& q = d->strands[s];
         if (q.first != next) return ctx->fail(PXB_ERR_UNSUPPORTED, "strands are not contiguous (make_strands layout)");
-        if (q.count > 32) return ctx->fail(PXB_ERR_TOO_LARGE, "strand %u has %u particles; the device path holds 32", s, q.count);
+        if (q.count > kMaxStrandParticles)
+            return ctx->fail(PXB_ERR_TOO_LARGE, "strand %u has %u particles; the device path holds %u", s, q.count,
+                             kMaxStrandParticles);
         e.first.push_back(q.first);
         e.count.push_back(q.count);
         next += q.count;
+    }
+    // slots: 32 per strand while every strand fits a warp's lanes; else each strand padded to a
+    // multiple of 32 (the long-strand kernel's layout)
+    uint32_t longest = 0;
+    for (uint32_t c : e.count) longest = std::max(longest, c);
+    const bool long_mode = longest > 32;
+    for (uint32_t s = 0; s < d->n_strands; ++s) {
+        e.base.push_back(static_cast<int32_t>(e.n_slots));
+        e.n_slots += long_mode ? std::max<size_t>(32, (e.count[s] + 31) & ~31u) : 32;
     }
     if (next != d->n_particles) return ctx->fail(PXB_ERR_UNSUPPORTED, "particles outside the strands");
     // make_strands' stretch lists: even (k-1 even) constraints of every strand, then odd ones.
@@ -117,7 +132,7 @@ static pxb_status strands_add(pxb_context* ctx, const pxb_strand_set_desc* d, ui
             for (uint32_t k = 1; k < e.count[s]; ++k)
                 if (static_cast<int>((k - 1) % 2) == parity) {
                     want.push_back({e.first[s] + k - 1, e.first[s] + k});
-                    slot.push_back(static_cast<int32_t>(32 * s + k - 1));
+                    slot.push_back(e.base[s] + static_cast<int32_t>(k) - 1);
                 }
     if (want.size() != d->n_stretch) return ctx->fail(PXB_ERR_UNSUPPORTED, "stretch list is not make_strands'");
     size_t n_even = 0;
@@ -140,12 +155,13 @@ static pxb_status strands_add(pxb_context* ctx, const pxb_strand_set_desc* d, ui
     e.time = d->time;
 
     // --- device buffers ---
-    const size_t S = 32 * static_cast<size_t>(e.n_strands);
+    const size_t S = e.n_slots;
     size_t off = 0;
     auto take = [&](size_t b) { const size_t o = off; off += al256(std::max<size_t>(b, 16)); return o; };
     const size_t o_pos = take(16 * S), o_vel = take(16 * S), o_prv = take(16 * S), o_rl = take(16 * S),
                  o_ro = take(16 * S), o_rest = take(4 * S), o_w = take(4 * S), o_lam = take(4 * S),
-                 o_cnt = take(4 * static_cast<size_t>(e.n_strands)), o_roots = take(64 * static_cast<size_t>(e.n_strands)),
+                 o_cnt = take(4 * static_cast<size_t>(e.n_strands)), o_base = take(4 * static_cast<size_t>(e.n_strands)),
+                 o_roots = take(64 * static_cast<size_t>(e.n_strands)),
                  o_keys = take(32), o_bounds = take(32);
     cudaError_t ce = cudaMalloc(&e.dmem, off);
     if (ce != cudaSuccess) return ctx->cuda(ce, "cudaMalloc(strands)");
@@ -164,12 +180,17 @@ static pxb_status strands_add(pxb_context* ctx, const pxb_strand_set_desc* d, ui
     e.dev.bounds_prev = reinterpret_cast<float*>(base + o_bounds);
     e.dev.bounds_out = e.dev.bounds_prev;
     e.dev.n_strands = static_cast<int32_t>(e.n_strands);
+    e.dev.base = reinterpret_cast<const int32_t*>(base + o_base);
+    e.dev.long_mode = long_mode ? 1 : 0;
+    e.dev.pad_count = static_cast<int32_t>((longest + 31) & ~31u);
+    // strands per block: as many as fit 96 KB of shared memory (20 B per slot), 1 to 8
+    e.dev.warps = static_cast<int32_t>(std::min<uint32_t>(8, std::max<uint32_t>(1, 98304 / (20 * std::max(32u, (longest + 31) & ~31u)))));
     std::vector<float4> rl(S, make_float4(0, 0, 0, 0)), ro(S, make_float4(0, 0, 0, 0));
     std::vector<float> rest(S, 0.0f);
     std::vector<int32_t> cnt(e.count.begin(), e.count.end());
     for (uint32_t s = 0; s < e.n_strands; ++s)
         for (uint32_t k = 0; k < e.count[s]; ++k) {
-            const size_t i = e.first[s] + k, l = 32 * static_cast<size_t>(s) + k;
+            const size_t i = e.first[s] + k, l = e.base[s] + k;
             rl[l] = make_float4(d->rest_local[3 * i], d->rest_local[3 * i + 1], d->rest_local[3 * i + 2], 0.0f);
             ro[l] = make_float4(d->rest_offset[3 * i], d->rest_offset[3 * i + 1], d->rest_offset[3 * i + 2], 0.0f);
         }
@@ -191,6 +212,7 @@ static pxb_status strands_add(pxb_context* ctx, const pxb_strand_set_desc* d, ui
     up(o_ro, ro.data(), 16 * S);
     up(o_rest, rest.data(), 4 * S);
     up(o_cnt, cnt.data(), 4 * cnt.size());
+    up(o_base, e.base.data(), 4 * e.base.size());
     up(o_bounds, b, 32);
     if (!st) st = ctx->cuda(cudaMemsetAsync(base + o_lam, 0, 4 * S, ctx->stream), "zero lambdas");
     if (!st) st = ctx->upload_strand_records(e);
@@ -291,7 +313,7 @@ pxb_status pxb_strands_read_particles(pxb_context* ctx, uint64_t id, pxb_particl
     StrandEntry* e = ctx->lookup_strands(id);
     if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "strand set id is not live");
     if (n != e->n_particles) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "particle count mismatch");
-    const size_t S = 32 * static_cast<size_t>(e->n_strands);
+    const size_t S = e->n_slots;
     std::vector<float4> pos(S), vel(S), prv(S);
     pxb_status st = ctx->cuda(cudaMemcpyAsync(pos.data(), e->dev.pos, 16 * S, cudaMemcpyDeviceToHost, ctx->stream), "read strand pos");
     if (!st) st = ctx->cuda(cudaMemcpyAsync(vel.data(), e->dev.vel, 16 * S, cudaMemcpyDeviceToHost, ctx->stream), "read strand vel");
@@ -300,7 +322,7 @@ pxb_status pxb_strands_read_particles(pxb_context* ctx, uint64_t id, pxb_particl
     if (st) return st;
     for (uint32_t s = 0; s < e->n_strands; ++s)
         for (uint32_t k = 0; k < e->count[s]; ++k) {
-            const size_t l = 32 * static_cast<size_t>(s) + k;
+            const size_t l = e->base[s] + k;
             pxb_particle& p = out[e->first[s] + k];
             p.position[0] = pos[l].x; p.position[1] = pos[l].y; p.position[2] = pos[l].z;
             p.inv_mass = pos[l].w;
@@ -315,7 +337,7 @@ pxb_status pxb_strands_read_lambdas(pxb_context* ctx, uint64_t id, float* out, u
     StrandEntry* e = ctx->lookup_strands(id);
     if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "strand set id is not live");
     if (n != e->n_stretch) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "lambda count mismatch");
-    std::vector<float> lam(32 * static_cast<size_t>(e->n_strands));
+    std::vector<float> lam(e->n_slots);
     pxb_status st = ctx->cuda(cudaMemcpyAsync(lam.data(), e->dev.lam, 4 * lam.size(), cudaMemcpyDeviceToHost, ctx->stream), "read lambdas");
     if (!st) st = ctx->check_device_error();
     if (st) return st;

@@ -2,7 +2,8 @@
 
 Stages without a transcendental call run in the reference's operation order in IEEE single
 precision, and scenes that only use those (no local shape, no turning root, no wind) are asserted
-EQUAL to the oracle. The local-shape rotation (acos / sin / cos) and the slerp of a turning root
+EQUAL to the oracle, for strands of up to 32 particles (one lane per particle) and longer ones
+(the long-strand kernel, lanes striding over the particles). The local-shape rotation (acos / sin / cos) and the slerp of a turning root
 use CUDA's libm, which may differ from the host's by an ulp; those scenes are held to the bars:
 within 1e-5 m after one step and 1e-3 m after many.
 """
@@ -63,6 +64,13 @@ EXACT = {
                                   box((0.2, 0.2, 0.05), (0.1, 0.0, 0.1))]),
     "compliant": dict(lines=[straight((0, 0, 0), 16)], p=params(stretch_compliance=1e-5, local_shape=0.0), iters=7),
     "short_and_single": dict(lines=[straight((0, 0, 0), 2), straight((0, 0.2, 0), 3)], p=params(local_shape=0.0)),
+    # strands longer than a warp (the long-strand kernel), alone and beside short ones
+    "long_hanging": dict(lines=[straight((0, 0, 0), 100, 0.01)], p=params(global_shape=0.0, local_shape=0.0)),
+    "long_mixed_drape": dict(lines=[straight((0, 0, 0.6), 40, 0.02), straight((0.05, 0, 0.6), 7, 0.02),
+                                    straight((0.1, 0, 0.6), 65, 0.02), straight((0.15, 0.02, 0.6), 33, 0.02)],
+                             p=params(local_shape=0.0, global_shape=0.3, thickness=0.02), cols=[sphere(0.3)]),
+    "long_compliant": dict(lines=[straight((0, 0, 0), 257, 0.004)], p=params(stretch_compliance=1e-5, local_shape=0.0),
+                           iters=7),
 }
 
 
@@ -86,6 +94,9 @@ TOLERANT = {
                             p=params(wind=(1.0, 0.5, 0.0), wind_turbulence=0.7)),
     "many_with_collider": dict(lines=[straight((0.01 * i, 0.01 * (i % 7), 0.35), 32) for i in range(64)],
                                p=params(), cols=[sphere(0.3)]),
+    # long strands hanging from their roots (combed straight down), local and global shape on
+    "long_hanging_defaults": dict(lines=[np.array([[0.01 * i, 0.0, 0.35 - 0.01 * k] for k in range(48 + 17 * i)],
+                                                  np.float32) for i in range(12)], p=params()),
 }
 
 
@@ -100,6 +111,18 @@ def test_transcendental_scenes_within_bars(ctx, name):
     assert np.array_equal(gpu["position"][roots], orc.particles["position"][roots])
     gpu, orc, _, _, _ = run_pair(ctx, s, 300, cols)
     assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-3
+    assert np.array_equal(gpu["position"][roots], orc.particles["position"][roots])
+
+
+def test_long_strands_falling_onto_a_collider_one_step_bar(ctx):
+    """Long strands (48 to 235 particles) falling from horizontal onto a sphere in a gusting wind:
+    a chaotic multi-pendulum, in which an ulp of CUDA's libm against glibc's (local-shape
+    rotation, gust) grows over the steps, so it is held to the one-step bar."""
+    s = R.make_strands([straight((0.01 * i, 0.0, 0.35), 48 + 17 * i, 0.01) for i in range(12)],
+                       params(wind=(0.5, 0.2, 0.0)))
+    gpu, orc, _, _, _ = run_pair(ctx, s, 1, collider_array([sphere(0.3)]))
+    assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-5
+    roots = orc.particles["inv_mass"] == 0
     assert np.array_equal(gpu["position"][roots], orc.particles["position"][roots])
 
 
@@ -136,9 +159,9 @@ def test_drop_in_solve_strands_on_host_arrays(ctx):
 
 
 def test_refusals(ctx):
-    long = R.make_strands([straight((0, 0, 0), 40)])
+    too_long = R.make_strands([straight((0, 0, 0), 8193, 0.001)])  # past one warp's shared memory
     with pytest.raises(R.PxbError) as e:
-        ctx.add_strands(long)
+        ctx.add_strands(too_long)
     assert e.value.status == 7
     ok = R.make_strands([straight((0, 0, 0))])
     odd = ok.copy()

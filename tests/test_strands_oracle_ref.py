@@ -69,6 +69,8 @@ SCENES = {
                             p=params(wind=(1.0, 0.5, 0.0), wind_turbulence=0.7), frames=40),
     "compliant_iters": dict(lines=lambda: [straight((0, 0, 0), 16)], p=params(stretch_compliance=1e-5),
                             frames=40, iters=7),
+    "long_strands_curl_collider": dict(lines=lambda: [straight((0.01 * i, 0, 0.35), 40 + 29 * i, 0.01) for i in range(4)],
+                                       p=params(wind=(0.5, 0.2, 0.0)), cols=lambda: [sphere(0.3)], frames=40),
 }
 
 

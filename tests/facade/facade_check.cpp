@@ -76,6 +76,20 @@ int main() {
         pxb::b200::solve_strands(dev, hmine, cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 4, 1.0f / 60.0f, h2);
     }
     bad += compare("strands 16x12, 90 frames", href.particles, hmine.particles);
+    // strands longer than a warp's 32 lanes, beside short ones (the long-strand kernel)
+    std::vector<px::hair::StrandDesc> ldescs;
+    for (int s = 0; s < 6; ++s) {
+        px::hair::StrandDesc d;
+        for (int k = 0; k < 20 + 23 * s; ++k) d.points.push_back(glm::vec3(0.02f * k, 0.01f * s, 0.6f));
+        ldescs.push_back(d);
+    }
+    px::hair::StrandSet lhref = px::hair::make_strands(ldescs, hp);
+    px::hair::StrandSet lhmine = lhref;
+    for (int i = 0; i < 60; ++i) {
+        px::hair::solve_strands(lhref, cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 4, 1.0f / 60.0f, h1);
+        pxb::b200::solve_strands(dev, lhmine, cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 4, 1.0f / 60.0f, h2);
+    }
+    bad += compare("strands of 20 to 135 particles, 60 frames", lhref.particles, lhmine.particles);
 
     // --- cloth onto a triangle-mesh floor with a convex-hull rock, both the reference's own
     //     objects (TriangleMesh::from_triangles, build_convex_hull) ---
@@ -114,6 +128,39 @@ int main() {
         pxb::b200::solve_cloth(dev, gmine, geo_cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 10, 1.0f / 60.0f, s2);
     }
     bad += compare("cloth 16x16 on a mesh floor and a hull, 150 frames", gref.particles, gmine.particles);
+
+    // --- a cloth of no grid structure: the 24x24 sheet's lists shuffled and each walked as one
+    //     serial batch, its triangles wound the other way, columns cleared (no 1-ring exemption),
+    //     self-collision on: the reference's solve_cloth walks any such cloth ---
+    px::cloth::GridClothDesc g3;
+    g3.columns = 24;
+    g3.rows = 24;
+    g3.width = 1.15f;
+    g3.height = 1.15f;
+    g3.center = glm::vec3(0.0f, 0.0f, 1.0f);
+    px::cloth::Cloth lref = px::cloth::make_grid_cloth(g3);
+    px::cloth::pin_static(lref, glm::vec3(-0.575f, 0.575f, 1.0f), 0.01f);
+    px::cloth::pin_static(lref, glm::vec3(0.575f, 0.575f, 1.0f), 0.01f);
+    px::cloth::build_tethers(lref);
+    uint64_t lcg = 12345u;
+    for (std::size_t k = lref.stretch.size(); k > 1; --k) {  // seeded Fisher-Yates
+        lcg = lcg * 6364136223846793005ull + 1442695040888963407ull;
+        std::swap(lref.stretch[k - 1], lref.stretch[(lcg >> 33) % k]);
+    }
+    lref.stretch_batches = {px::cloth::ConstraintBatch{0, static_cast<uint32_t>(lref.stretch.size())}};
+    lref.bend_batches = {px::cloth::ConstraintBatch{0, static_cast<uint32_t>(lref.bend.size())}};
+    for (std::size_t t = 0; t + 2 < lref.triangles.size(); t += 3) std::swap(lref.triangles[t + 1], lref.triangles[t + 2]);
+    lref.columns = 0;
+    lref.rows = 0;
+    lref.params.self_collision = true;
+    lref.params.self_distance = 0.12f;
+    px::cloth::Cloth lmine = lref;
+    for (int i = 0; i < 40; ++i) {
+        px::cloth::solve_cloth(lref, cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 10, 1.0f / 60.0f, s1);
+        pxb::b200::solve_cloth(dev, lmine, cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 10, 1.0f / 60.0f, s2);
+    }
+    bad += compare("general-topology cloth (shuffled serial lists, self-collision), 40 frames", lref.particles,
+                   lmine.particles);
     std::printf(bad ? "facade MISMATCH\n" : "facade ok\n");
     return bad ? 1 : 0;
 }

@@ -293,6 +293,9 @@ typedef struct pxb_cloth_plan {
                                  other lists (an imported mesh), one CTA, solved as runs of
                                  particle-disjoint items in the reference's order (n_colours then
                                  counts the runs) */
+    int32_t lean;             /* 1: only the positions in shared memory, rest lengths and lambdas
+                                 read in place in HBM (one CTA or two where a full-shared-memory
+                                 layout would need a larger cluster) */
 } pxb_cloth_plan;
 
 /* Plans a cloth without a context or a GPU: validates it exactly as pxb_cloth_add does and

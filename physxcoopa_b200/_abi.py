@@ -135,7 +135,8 @@ class ClothPlan(C.Structure):
     _fields_ = [("n_ranks", C.c_int32), ("rows_per_rank", C.c_int32), ("threads", C.c_int32),
                 ("smem_bytes", C.c_int32), ("n_colours", C.c_int32), ("n_segments", C.c_int32),
                 ("layout_slots", C.c_int32), ("constraint_slots", C.c_int32),
-                ("self_collision", C.c_int32), ("self_smem_bytes", C.c_int32), ("topology", C.c_int32)]
+                ("self_collision", C.c_int32), ("self_smem_bytes", C.c_int32), ("topology", C.c_int32),
+                ("lean", C.c_int32)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

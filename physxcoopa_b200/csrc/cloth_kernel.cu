@@ -298,7 +298,7 @@ __device__ __forceinline__ void cluster_or_block_sync() {
     else __syncthreads();
 }
 
-template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false>
+template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false, bool kLean = false>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders,
@@ -348,17 +348,22 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     // a general-topology cloth whose state stays in HBM runs only in the kGmem instantiation,
     // and that instantiation runs nothing else
     constexpr bool kG = kGmem && kExt && CL == 1 && !kWarm;
-    if ((sC.topology == 2) != kG) {
+    // a lean cloth (only positions in shared memory; rest lengths and lambdas read in place in
+    // HBM, velocities for the aerodynamic gather too) runs only in the kLean instantiations
+    constexpr bool kL = kLean && CL <= 2 && !kG;
+    if ((sC.topology == 2) != kG || (sC.lean != 0) != kL) {  // every rank of a cluster agrees
         if (tid == 0) atomicOr(err, PXB_DEVERR_BAD_INDEX);
         return;
     }
     const int n_ranks = CL > 1 ? sC.n_ranks : 1;
     const RankView me = rank_view<1>(sC, smem, rank);  // local view, plain shared addresses
     float4* pos = kG ? sC.pos : me.pos;
-    float* U = kG ? sC.list_scratch : me.U;
+    float* U = kG ? sC.list_scratch : (kL ? sC.lam_out + sC.rank[rank].lam_off : me.U);
     const int n_local = me.n_local;
     const int base = me.base;
     float* rest = kG ? const_cast<float*>(sC.rest) : reinterpret_cast<float*>(smem + 16 * static_cast<size_t>(n_local));
+    // where the colour loop reads rest lengths: shared memory, or in place in HBM (lean)
+    float* RG = kL ? const_cast<float*>(sC.rest) + sC.rank[rank].rest_off : rest;
     RankView prv_rank{}, nxt_rank{};
     if constexpr (CL > 1) {
         if (rank > 0) prv_rank = rank_view<CL>(sC, smem, rank - 1);
@@ -368,7 +373,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     // --- prologue: stage positions and rest lengths with TMA bulk copies -------------------
     if (tid == 0 && !kG) {
         const uint32_t pos_bytes = 16u * static_cast<uint32_t>(n_local);
-        const uint32_t rest_bytes = 4u * static_cast<uint32_t>(sC.rank[rank].n_rest_pad);
+        const uint32_t rest_bytes = kL ? 0u : 4u * static_cast<uint32_t>(sC.rank[rank].n_rest_pad);
         mbar_arrive_expect_tx(&bar, pos_bytes + rest_bytes);
         bulk_g2s(pos, sC.pos + base, pos_bytes, &bar);
         if (rest_bytes) bulk_g2s(rest, sC.rest + sC.rank[rank].rest_off, rest_bytes, &bar);
@@ -479,9 +484,9 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
                     constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
                     if (h1.w >= 0)
-                        project_segment<CL, true, kItems>(pos, pos_next, rest + h1.z, U + h1.w, n_local, h0, h1, alpha, tid, T);
+                        project_segment<CL, true, kItems>(pos, pos_next, RG + h1.z, U + h1.w, n_local, h0, h1, alpha, tid, T);
                     else
-                        project_segment<CL, false, kItems>(pos, pos_next, rest + h1.z, U, n_local, h0, h1, alpha, tid, T);
+                        project_segment<CL, false, kItems>(pos, pos_next, RG + h1.z, U, n_local, h0, h1, alpha, tid, T);
                 }
                 // Colours that join rows need every rank to see the others' writes; a pair
                 // of row-local colours only needs this CTA's. The last colour always syncs
@@ -506,7 +511,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 const int count = h0.x, per_row = h0.z, a_base = h0.w;
                 const uint32_t magic = static_cast<uint32_t>(h0.y);
                 const int row_stride = h1.x, d = h1.y;
-                const float* rr = rest + h1.z;
+                const float* rr = RG + h1.z;
                 for (int i = tid; i < count; i += T) {
                     const int row = seg_row(i, magic);
                     const int la = a_base + row * row_stride + (i - row * per_row), lb = la + d;
@@ -552,11 +557,13 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         // Velocities are parked in U (SoA) for the neighbour reads; each particle's summed
         // share is parked in its own prv slot until integrate consumes it.
         if (aero) {
-            for (int l = tid; l < n_local; l += T) {
-                const float4 vv = gvel[base + l];
-                U[l] = vv.x;
-                U[n_local + l] = vv.y;
-                U[2 * n_local + l] = vv.z;
+            if constexpr (!kL) {  // a lean cloth reads the velocities in place
+                for (int l = tid; l < n_local; l += T) {
+                    const float4 vv = gvel[base + l];
+                    U[l] = vv.x;
+                    U[n_local + l] = vv.y;
+                    U[2 * n_local + l] = vv.z;
+                }
             }
             cluster_or_block_sync<CL>();
             const int Q = sC.Q, S = sC.S, cols = sC.columns, rows = sC.rows;
@@ -585,6 +592,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 return xyz(nxt_rank.pos[l - n_local]);
             };
             auto V3 = [&](int g) -> f3 {
+                if constexpr (kL) return xyz(gvel[g]);
                 const int l = g - base;
                 if (CL == 1 || (l >= 0 && l < n_local)) return mk(U[l], U[n_local + l], U[2 * n_local + l]);
                 if (l < 0) {
@@ -602,7 +610,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 const int x = 4 * (j - cls * Q) + cls;
                 if (x >= cols || y >= rows) continue;  // ghost slot
                 const bool xm = x >= 1, xp = x + 1 < cols, ym = y >= 1, yp = y + 1 < rows;
-                const f3 p00 = xyz(pos[l]), v00 = mk(U[l], U[n_local + l], U[2 * n_local + l]);
+                const f3 p00 = xyz(pos[l]);
+                const f3 v00 = kL ? xyz(gvel[gl]) : mk(U[l], U[n_local + l], U[2 * n_local + l]);
                 f3 a = mk(0.0f, 0.0f, 0.0f);
                 if (xm && ym) {  // cell (x-1, y-1): T0 then T1
                     const int lmm = lay(x - 1, y - 1, Q, S), l0m = lay(x, y - 1, Q, S),
@@ -689,9 +698,10 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 // rest lengths are staged again below); recording alone uses the lambda region.
                 uint32_t dyn;
                 asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-                unsigned char* ub = net ? reinterpret_cast<unsigned char*>(rest) : reinterpret_cast<unsigned char*>(U);
-                const int u_cap = net ? static_cast<int>(dyn) - 16 * n_local
-                                      : static_cast<int>(dyn) - (16 * n_local + 4 * sC.rank[rank].n_rest_pad);
+                // a lean cloth has nothing after its positions in shared memory: all of it is scratch
+                unsigned char* ub = (net || kL) ? reinterpret_cast<unsigned char*>(rest) : reinterpret_cast<unsigned char*>(U);
+                const int u_cap = (net || kL) ? static_cast<int>(dyn) - 16 * n_local
+                                              : static_cast<int>(dyn) - (16 * n_local + 4 * sC.rank[rank].n_rest_pad);
                 int n_wg = (u_cap - kWarmTileOff) / kWarmTileBytes;
                 n_wg = n_wg < T / 128 ? n_wg : T / 128;
                 n_wg = n_wg < kWarmGroups ? n_wg : kWarmGroups;
@@ -774,7 +784,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     tc::fence_after_sync();
                     if (net && tid < 32) tc::tmem_dealloc(s_tmem, n_wg > 2 ? 256u : (n_wg > 1 ? 128u : 64u));
                 }
-                if (net) {
+                if (net && !kL) {
                     // the rest lengths come back: TMA bulk copy, next phase of the staging barrier
                     fence_proxy_async();
                     __syncthreads();
@@ -1447,7 +1457,7 @@ cudaError_t launch_cloth_grid(const PxbClothDev* cloths, const PxbClothStep* ste
                : launch_grid_variant<false>(cloths, steps, colliders, sources, order, results, err, gs, slot, n_sms, stream);
 }
 
-template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false>
+template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false, bool kLean = false>
 static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
                                   const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                   const int32_t* order, PxbFrameResult* results, uint32_t* err,
@@ -1459,10 +1469,10 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     if (e != cudaSuccess) return e;
     if (dev < 64 && !(configured >> dev & 1ull)) {
         cudaFuncAttributes fa;
-        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem>);
+        e = cudaFuncGetAttributes(&fa, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem, kLean>);
         if (e != cudaSuccess) return e;
         if (fa.sharedSizeBytes > static_cast<size_t>(kClothStaticSmem)) return cudaErrorInvalidConfiguration;
-        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem>,
+        e = cudaFuncSetAttribute(cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem, kLean>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
         if (e != cudaSuccess) return e;
         configured |= 1ull << dev;
@@ -1479,7 +1489,7 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem>, cloths, steps, colliders,
+    return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem, kLean>, cloths, steps, colliders,
                               sources, order, results, err, wsteps, mlp, wres);
 }
 
@@ -1516,6 +1526,43 @@ static cudaError_t launch_cl(int cluster, const PxbClothDev* cloths, const PxbCl
 }
 
 // Launches carrying a mesh or hull collider: the same dispatch over the kExt instantiations.
+// Lean cloths: one CTA or a 2-CTA cluster, plain / extended, plain / warm-start kernels.
+template <int kMaxThreads, bool kWarm, bool kExt>
+static cudaError_t launch_lean_cl(int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
+                                  const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                                  const int32_t* order, PxbFrameResult* results, uint32_t* err,
+                                  int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
+                                  const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres) {
+    switch (cluster) {
+        case 1: return launch_variant<kMaxThreads, 1, kWarm, kExt, false, true>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 2: return launch_variant<kMaxThreads, 2, kWarm, kExt, false, true>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <bool kExt>
+static cudaError_t launch_lean(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
+                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
+                               int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
+                               const unsigned char* mlp, PxbWarmResult* wres) {
+    if (wsteps) {
+        if (variant == 0) {
+            if (threads > 512) threads = 512;
+            return launch_lean_cl<512, true, kExt>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        }
+        if (threads > 1024) threads = 1024;
+        if (threads < 128) threads = 128;
+        return launch_lean_cl<1024, true, kExt>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+    }
+    if (threads > cloth_variant_threads(variant)) threads = cloth_variant_threads(variant);
+    switch (variant) {
+        case 0: return launch_lean_cl<512, false, kExt>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        case 1: return launch_lean_cl<768, false, kExt>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+        default: return launch_lean_cl<1024, false, kExt>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, nullptr, nullptr, nullptr);
+    }
+}
+
 static cudaError_t launch_geo(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
@@ -1545,6 +1592,11 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
                               int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
                               const unsigned char* mlp, PxbWarmResult* wres, int ext) {
     if (n_cloths <= 0) return cudaSuccess;
+    if (ext == 3 || ext == 4)
+        return ext == 4 ? launch_lean<true>(variant, cluster, cloths, steps, colliders, sources, order, results, err,
+                                            n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres)
+                        : launch_lean<false>(variant, cluster, cloths, steps, colliders, sources, order, results, err,
+                                             n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
     if (ext == 2) {
         // general-topology cloths with their state in HBM: one CTA each, no warm start
         if (cluster != 1 || wsteps) return cudaErrorInvalidValue;

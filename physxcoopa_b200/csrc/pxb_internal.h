@@ -108,7 +108,9 @@ struct PxbClothDev {
                                 // endpoint slots (a | b << 16) rest[pad, 2 * pad) as uint32 bits
     float* list_scratch;        // topology 2: lambdas / parked velocities in HBM, max(pad, 3 n_layout)
     int32_t ref_columns;        // Cloth::columns as given: self-collision's 1-ring exemption reads it
-    int32_t pad2;
+    // 1: a lean grid cloth: only positions in shared memory, its rest lengths and lambdas read in
+    // place in HBM (rest + rank.rest_off, lam_out + rank.lam_off), velocities too; one or two CTAs
+    int32_t lean;
 };
 
 // A run of a general-topology cloth: consecutive items of one reference batch, no two of which

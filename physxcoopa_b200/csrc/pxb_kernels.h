@@ -26,7 +26,8 @@ int cloth_variant_threads(int variant);
 int cloth_variant_registers(int variant);
 // wsteps non-null selects the warm-start kernel (mlp may then be null: plain solve with the
 // residual measured, or recording only). ext: 0 the plain kernel, 1 with the mesh / hull,
-// self-collision and general-topology stages, 2 general topology with the state in HBM.
+// self-collision and general-topology stages, 2 general topology with the state in HBM, 3 and 4
+// the lean instantiations of 0 and 1 (rest lengths and lambdas in HBM; one CTA or two).
 cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,

@@ -675,9 +675,15 @@ static void layout_ranks(ClothEntry& e) {
         lam_total += lam;
         const int n_local = rk.n_rows * e.S;
         const int u_floats = std::max(lam, (aero && e.aero_grid) ? 3 * n_local : 0);
-        rk.smem = 16 * n_local + 4 * rk.n_rest_pad + 4 * ((u_floats + 3) & ~3);
+        if (e.lean) {
+            // positions only; the warm start's network tiles go right after them
+            rk.smem = 16 * n_local;
+            warm_max = std::max(warm_max, 16 * n_local + kWarmUMin);
+        } else {
+            rk.smem = 16 * n_local + 4 * rk.n_rest_pad + 4 * ((u_floats + 3) & ~3);
+            warm_max = std::max(warm_max, 16 * n_local + 4 * rk.n_rest_pad + std::max(4 * ((u_floats + 3) & ~3), kWarmUMin));
+        }
         smem_max = std::max(smem_max, rk.smem);
-        warm_max = std::max(warm_max, 16 * n_local + 4 * rk.n_rest_pad + std::max(4 * ((u_floats + 3) & ~3), kWarmUMin));
         PxbRank& dr = e.dev.rank[r];
         dr.row0 = rk.row0;
         dr.n_rows = rk.n_rows;
@@ -701,7 +707,7 @@ static void layout_ranks(ClothEntry& e) {
     e.dev.self_restage = 0;
     if (e.ranks.size() == 1) {
         const ClothEntry::Rank& rk = e.ranks[0];
-        place_self_tables(e, smem_max, 16 * rk.n_rows * e.S, 4 * rk.n_rest_pad);
+        place_self_tables(e, smem_max, 16 * rk.n_rows * e.S, e.lean ? 0 : 4 * rk.n_rest_pad);
     }
 }
 
@@ -864,13 +870,20 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
     }
     int max_colour = 0;
     bool placed = false;
-    for (int cl = 1; cl <= PXB_MAX_RANKS && !placed; cl *= 2) {
+    // One CTA with everything in shared memory; else lean (positions only in shared memory, rest
+    // lengths and lambdas read in place in HBM) on one CTA or two, as long as the warm start's
+    // tiles still fit beside the positions; else a cluster of 2, 4 or 8 CTAs.
+    const struct { int cl; bool lean; } tries[] = {{1, false}, {1, true}, {2, true}, {2, false}, {4, false}, {8, false}};
+    for (const auto& t : tries) {
+        if (placed) break;
         std::vector<int32_t> padded;
-        if (!build_ranks(e, cs, rest_ref, cl, padded, max_colour)) continue;
+        if (!build_ranks(e, cs, rest_ref, t.cl, padded, max_colour)) continue;
+        e.lean = t.lean;
         e.rest_ref.swap(padded);
         layout_ranks(e);
-        if (e.dev.smem_bytes <= kMaxDynamicSmem) placed = true;
+        if (e.dev.smem_bytes <= kMaxDynamicSmem && (!t.lean || e.warm_smem <= kMaxDynamicSmem)) placed = true;
     }
+    if (!placed) e.lean = false;
     if (!placed) {
         // Beyond a cluster: the whole-GPU path (every SM on this cloth, state in global memory).
         std::vector<int32_t> padded;
@@ -958,6 +971,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.self_hash_off = keep_ranks.self_hash_off;
     e.dev.self_restage = keep_ranks.self_restage;
     e.dev.ref_columns = e.ref_columns;
+    e.dev.lean = e.lean ? 1 : 0;
     e.dev.pos = reinterpret_cast<float4*>(base + o_pos);
     e.dev.vel = reinterpret_cast<float4*>(base + o_vel);
     e.dev.prv = reinterpret_cast<float4*>(base + o_prv);
@@ -1228,6 +1242,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                             (sd->collider_offsets &&
                              cstage.any_geometry(sd->collider_offsets[k],
                                                  sd->collider_offsets[k + 1] - sd->collider_offsets[k])));
+    for (uint32_t k = 0; k < n; ++k)
+        if (ents[k]->lean) has_geo[k] = static_cast<uint8_t>(3 + has_geo[k]);  // lean instantiations
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
@@ -1402,9 +1418,9 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                            uint64_t(reinterpret_cast<uintptr_t>(d_registry.p)), uint64_t(reinterpret_cast<uintptr_t>(pinned)),
                            uint64_t(reinterpret_cast<uintptr_t>(d_grid.p)), registry_epoch})
             key.push_back(v);
-        for (uint32_t k = 0; k < n; k += 32) {  // which kernel instantiation each cloth launches
+        for (uint32_t k = 0; k < n; k += 21) {  // which kernel instantiation each cloth launches
             uint64_t bits = 0;
-            for (uint32_t j = k; j < std::min(n, k + 32); ++j) bits |= uint64_t(has_geo[j]) << (2 * (j - k));
+            for (uint32_t j = k; j < std::min(n, k + 21); ++j) bits |= uint64_t(has_geo[j]) << (3 * (j - k));
             key.push_back(bits);
         }
         if (graph_exec && key == graph_key) {
@@ -1582,6 +1598,7 @@ pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out
     out->self_collision = e.self_ok && !e.grid ? 1 : 0;
     out->self_smem_bytes = e.self_ok && !e.grid ? e.self_smem : 0;
     out->topology = e.list_gmem ? 2 : (e.list ? 1 : 0);
+    out->lean = e.lean ? 1 : 0;
     if (e.list) out->n_colours = static_cast<int32_t>(e.runs.size());
     return PXB_OK;
 }

@@ -25,6 +25,7 @@ struct TopologyEdge {
 struct ClothEntry {
     bool alive = false;
     bool grid = false;  // beyond a cluster: solved by every SM from global memory
+    bool lean = false;  // only positions in shared memory (PxbClothDev::lean), one CTA or two
     uint32_t generation = 0;
     uint32_t n_particles = 0;
     int cols = 0, rows = 0, Q = 0, S = 0, n_layout = 0;

@@ -392,27 +392,30 @@ def clustered_sheet(cols, rows, seed, pins="corners", params=None):
 
 
 CLUSTERED = {
-    # (columns, rows); the planner gives these 2, 4, 8, 2 and 2 CTAs
-    "c2_65": dict(shape=(65, 65), cols=[sphere(0.5, (0.1, 0, 0.4))]),
-    "c4_100_sources": dict(shape=(100, 100), cols=[capsule(0.2, 0.5, (0, 0, 0.5), axis=0)],
-                          sources=[((0.5, -0.3, -2.0), 9.81, 1.0, 10.0)]),
-    "c8_128_edge": dict(shape=(128, 128), pins="edge",
-                        cols=[box((0.6, 0.5, 0.4), (0.2, 0.1, 0.3), (0.0, 0.3826834, 0.0, 0.9238795))]),
-    "c2_tall_40x180": dict(shape=(40, 180), cols=[sphere(0.6, (0, 0.5, 0.2))]),
-    "c2_wind_97x61": dict(shape=(97, 61), params=dict(wind=(0.5, 0.2, 0.0), wind_turbulence=0.5)),
+    # (columns, rows) and the layout the planner gives: (CTAs, lean). Lean: only the positions in
+    # shared memory, rest lengths and lambdas read in place in HBM.
+    "lean1_65": dict(shape=(65, 65), layout=(1, 1), cols=[sphere(0.5, (0.1, 0, 0.4))]),
+    "lean1_100_sources": dict(shape=(100, 100), layout=(1, 1), cols=[capsule(0.2, 0.5, (0, 0, 0.5), axis=0)],
+                              sources=[((0.5, -0.3, -2.0), 9.81, 1.0, 10.0)]),
+    "lean2_128_edge": dict(shape=(128, 128), layout=(2, 1), pins="edge",
+                           cols=[box((0.6, 0.5, 0.4), (0.2, 0.1, 0.3), (0.0, 0.3826834, 0.0, 0.9238795))]),
+    "lean1_tall_40x180": dict(shape=(40, 180), layout=(1, 1), cols=[sphere(0.6, (0, 0.5, 0.2))]),
+    "lean2_wind_150x97": dict(shape=(150, 97), layout=(2, 1), params=dict(wind=(0.5, 0.2, 0.0), wind_turbulence=0.5)),
+    "c8_160": dict(shape=(160, 160), layout=(8, 0), cols=[sphere(0.8, (0, 0, 0.2))]),
 }
 
 
 @pytest.mark.parametrize("name", sorted(CLUSTERED))
 def test_clustered_cloth_equals_oracle(ctx, name):
-    """Cloths too large for one CTA's shared memory run on a cluster of CTAs (rows split, the
-    neighbour rows read through distributed shared memory); results equal the oracle's."""
+    """Cloths too large for one CTA's shared memory run lean (positions only in shared memory) on
+    one CTA or two, or on a cluster of CTAs (rows split, the neighbour rows read through
+    distributed shared memory); results equal the oracle's."""
     sc = CLUSTERED[name]
     params = scenes.cloth_params(**{k: (A.C.c_float * 3)(*v) if isinstance(v, tuple) else v
                                     for k, v in sc.get("params", {}).items()})
     cloth = clustered_sheet(*sc["shape"], seed=11, pins=sc.get("pins", "corners"), params=params)
     plan = R.plan_cloth(cloth)
-    assert plan["n_ranks"] > 1, plan
+    assert (plan["n_ranks"], plan["lean"]) == sc["layout"], plan
     cols = collider_array(sc["cols"]) if sc.get("cols") else None
     src = gravity_sources(sc["sources"]) if sc.get("sources") else None
     gpu, orc, res_, lam, t = run_pair(ctx, cloth, cols, sources=src, steps=1)
@@ -443,12 +446,13 @@ def compliant_mask(batches, compliance, n):
 
 
 def test_batch_of_every_cluster_size(ctx):
-    """One step call over cloths of every cluster size: at least one launch per size, all equal
-    to the oracle, positions gathered in the caller's order."""
-    shapes = [(20, 20), (128, 128), (64, 64), (65, 65), (100, 100), (16, 16), (72, 72)]
+    """One step call over cloths of every layout (one CTA, lean on one CTA or two, a cluster of
+    eight): at least one launch per layout, all equal to the oracle, positions gathered in the
+    caller's order."""
+    shapes = [(20, 20), (128, 128), (64, 64), (65, 65), (100, 100), (16, 16), (160, 160)]
     cloths = [clustered_sheet(c, r, seed=k) for k, (c, r) in enumerate(shapes)]
-    sizes = {R.plan_cloth(c)["n_ranks"] for c in cloths}
-    assert sizes == {1, 2, 4, 8}
+    sizes = {(R.plan_cloth(c)["n_ranks"], R.plan_cloth(c)["lean"]) for c in cloths}
+    assert sizes == {(1, 0), (1, 1), (2, 1), (8, 0)}
     cols = [collider_array([sphere(0.3 + 0.05 * k, (0.05 * k, 0, 0.4))]) for k in range(len(cloths))]
     orcs = [c.copy() for c in cloths]
     ids = [ctx.add_cloth(c) for c in cloths]

@@ -159,15 +159,17 @@ def test_terrain_drape_equals_oracle_1_and_300_steps(ctx):
             ctx.destroy_geometry(g)
 
 
-@pytest.mark.parametrize("side", [100, 200])
+@pytest.mark.parametrize("side", [100, 128, 160, 200])
 def test_cluster_and_whole_gpu_paths_with_mesh_and_hull(ctx, side):
-    """100 x 100 runs as a thread-block cluster, 200 x 200 on the whole-GPU kernel."""
+    """100 x 100 runs lean on one CTA, 128 x 128 lean on two, 160 x 160 on a cluster of eight,
+    200 x 200 on the whole-GPU kernel."""
     sc = S.terrain_drape(side=side, seed=5)
     plan = R.plan_cloth(sc.cloths[0])
-    assert (plan["n_ranks"] > 1) if side == 100 else (plan["n_ranks"] == 0)
+    want = {100: (1, 1), 128: (2, 1), 160: (8, 0), 200: (0, 0)}[side]
+    assert (plan["n_ranks"], plan["lean"]) == want, plan
     gids = _scene_with_oracle(ctx, sc)
     try:
-        gpu, orc = run_scene(ctx, sc, 12 if side == 100 else 3)
+        gpu, orc = run_scene(ctx, sc, 3 if side == 200 else 12)
         assert_equal_particles(gpu[0], orc[0].particles, f"{side}^2")
     finally:
         for g in gids:

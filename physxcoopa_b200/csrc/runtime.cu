@@ -676,9 +676,11 @@ static void layout_ranks(ClothEntry& e) {
         const int n_local = rk.n_rows * e.S;
         const int u_floats = std::max(lam, (aero && e.aero_grid) ? 3 * n_local : 0);
         if (e.lean) {
-            // positions only; the warm start's network tiles go right after them
+            // positions only; the warm start's network tiles go right after them, as many of its
+            // warpgroups' tiles as fit (at least one)
             rk.smem = 16 * n_local;
-            warm_max = std::max(warm_max, 16 * n_local + kWarmUMin);
+            const int tiles = std::min(kMaxDynamicSmem, 16 * n_local + kWarmTileOff + kWarmGroups * kWarmTileBytes);
+            warm_max = std::max(warm_max, std::max(16 * n_local + kWarmUMin, tiles));
         } else {
             rk.smem = 16 * n_local + 4 * rk.n_rest_pad + 4 * ((u_floats + 3) & ~3);
             warm_max = std::max(warm_max, 16 * n_local + 4 * rk.n_rest_pad + std::max(4 * ((u_floats + 3) & ~3), kWarmUMin));

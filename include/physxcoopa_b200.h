@@ -435,6 +435,23 @@ pxb_status pxb_cloths_read_sleep_state(pxb_context* ctx, const uint64_t* cloths,
  * a determinism hash reads back each frame. */
 pxb_status pxb_cloths_read_positions(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
                                      float* out, size_t capacity);
+/* Pipelined form for a renderer that draws frame k while frame k + 1 is simulated: snapshots
+ * the same positions on the device (after every step enqueued so far) and copies them into
+ * host `out` on a copy stream, returning at once, so the copy overlaps the next step. `out`
+ * must stay valid until pxb_cloths_wait_positions returns, and should be pinned host memory
+ * (cudaHostAlloc) for the copy to run asynchronously. Two snapshots may be in flight; a third
+ * call first waits for the older one. */
+pxb_status pxb_cloths_read_positions_async(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
+                                           float* out, size_t capacity);
+/* The same for the last step's per-cloth results (what pxb_cloths_read_results returns), copied
+ * into host `out` (n records, pinned for an asynchronous copy) without waiting for the step, so
+ * the caller can enqueue the next step at once; every listed cloth must have been in the last
+ * (plain) step. Two copies may be in flight. */
+pxb_status pxb_cloths_read_results_async(pxb_context* ctx, const uint64_t* cloths, uint32_t n,
+                                         pxb_cloth_frame_result* out);
+/* Blocks until every copy started by pxb_cloths_read_positions_async or
+ * pxb_cloths_read_results_async has landed, then checks the device error word. */
+pxb_status pxb_cloths_wait_positions(pxb_context* ctx);
 /* The same gather into DEVICE memory `out_device` (capacity floats), allocating nothing. No
  * counterpart in the reference. For callers that may not allocate device memory while they run
  * (a per-frame reader inside a fixed memory budget, or code where cudaMalloc / cudaFree would

@@ -1163,8 +1163,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         if (!ents[k]) return fail(PXB_ERR_INVALID_HANDLE, "cloth id %llu is not live", (unsigned long long)sd->cloths[k]);
         if (self_on(*ents[k]) && (!ents[k]->self_ok || ents[k]->grid))
             return fail(PXB_ERR_UNSUPPORTED,
-                        "cloth %llu: self-collision runs on cloths one CTA holds in shared memory (grid sides up to "
-                        "64, general topology up to ~2800 particles) whose hash tables fit there",
+                        "cloth %llu: self-collision runs on cloths one CTA holds in shared memory with its hash "
+                        "tables (grid sides up to ~84, general topology up to ~2800 particles)",
                         (unsigned long long)sd->cloths[k]);
         if (sd->collider_offsets) {
             if (sd->collider_offsets[k + 1] < sd->collider_offsets[k])
@@ -1457,7 +1457,10 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         }
     }
     last_step.resize(n);
-    for (uint32_t slot = 0; slot < n; ++slot) last_step[slot] = sd->cloths[perm[slot]];
+    for (uint32_t slot = 0; slot < n; ++slot) {
+        last_step[slot] = sd->cloths[perm[slot]];
+        ents[perm[slot]]->last_slot = static_cast<int32_t>(slot);
+    }
     last_step_warm = warm != nullptr;
     warm_fresh = false;
     results_fresh = false;

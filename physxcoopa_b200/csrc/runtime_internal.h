@@ -77,6 +77,7 @@ struct ClothEntry {
     size_t dbytes = 0;
     PxbFrameResult result{};
     bool has_result = false;
+    int32_t last_slot = -1;  // launch slot in the last step (pxb_context::last_step)
     PxbWarmResult warm_result{};
     bool has_warm_result = false;
 };
@@ -179,8 +180,27 @@ struct pxb_context {
     }
     int cloth_variant = 0;  // kernel block-size cap, see pxb_kernels.h (autotuned or set)
     DevBuf d_tune;          // cloth state saved across an autotune
+    // Pipelined position read-back (pxb_cloths_read_positions_async): two device snapshots,
+    // each gathered on `stream` and copied to the host on `copy_stream`, which waits for it.
+    cudaStream_t copy_stream = nullptr;
+    DevBuf d_snap[2], d_snap_meta[2];
+    cudaEvent_t snap_ready[2] = {}, snap_copied[2] = {};
+    bool snap_busy[2] = {false, false};
+    int snap_next = 0;
+    DevBuf d_res_snap[2];  // pxb_cloths_read_results_async: slots, times, gathered records
+    cudaEvent_t res_ready[2] = {}, res_copied[2] = {};
+    bool res_busy[2] = {false, false};
+    int res_next = 0;
 
     ~pxb_context() {
+        if (copy_stream) cudaStreamSynchronize(copy_stream);
+        for (int k = 0; k < 2; ++k) {
+            for (DevBuf* b : {&d_snap[k], &d_snap_meta[k], &d_res_snap[k]})
+                if (b->p) cudaFree(b->p);
+            for (cudaEvent_t ev : {snap_ready[k], snap_copied[k], res_ready[k], res_copied[k]})
+                if (ev) cudaEventDestroy(ev);
+        }
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
         for (ClothEntry& e : cloths)

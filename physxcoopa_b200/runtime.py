@@ -56,6 +56,9 @@ SIGNATURES = {
     "pxb_cloths_step_graph": ([P, C.POINTER(A.ClothStepDesc)], C.c_int),
     "pxb_cloths_read_results": ([P, P, u32, P], C.c_int),
     "pxb_cloths_read_positions": ([P, P, u32, P, C.c_size_t], C.c_int),
+    "pxb_cloths_read_positions_async": ([P, P, u32, P, C.c_size_t], C.c_int),
+    "pxb_cloths_wait_positions": ([P], C.c_int),
+    "pxb_cloths_read_results_async": ([P, P, u32, P], C.c_int),
     "pxb_solve_cloth_host": ([P, C.POINTER(A.ClothDesc), P, P, P, P, P, u32, f32p, u32, u32, f32,
                               f32p, f32p], C.c_int),
     "pxb_project_particles": ([P, P, f32, P, P, u32, P, P, P, P], C.c_int),
@@ -515,6 +518,23 @@ class Context:
         self._check(self.lib.pxb_cloths_read_results(self.h, A.ptr(ids), len(ids), A.ptr(out)),
                     "read_results")
         return out
+
+    def read_positions_async(self, ids, out):
+        """pxb_cloths_read_positions_async into `out` (float32, ideally pinned); completes at
+        wait_positions()."""
+        ids = np.ascontiguousarray(ids, np.uint64)
+        self._check(self.lib.pxb_cloths_read_positions_async(self.h, A.ptr(ids), len(ids), out.ctypes.data, out.size),
+                    "read_positions_async")
+
+    def read_results_async(self, ids, out):
+        """pxb_cloths_read_results_async into `out` (A.FRAME_RESULT records, ideally pinned);
+        completes at wait_positions()."""
+        ids = np.ascontiguousarray(ids, np.uint64)
+        self._check(self.lib.pxb_cloths_read_results_async(self.h, A.ptr(ids), len(ids), out.ctypes.data),
+                    "read_results_async")
+
+    def wait_positions(self):
+        self._check(self.lib.pxb_cloths_wait_positions(self.h), "wait_positions")
 
     def read_positions(self, ids, out=None):
         ids = np.ascontiguousarray(ids, np.uint64)

@@ -138,3 +138,55 @@ def test_render_buffer_refusals(ctx):
         assert e.value.status == A.PXB_ERR_INVALID_ARGUMENT
     finally:
         ctx.remove_cloth(cid)
+
+
+def test_pipelined_position_reads(ctx):
+    """pxb_cloths_read_positions_async: each call snapshots the state after the steps before it
+    and lands it in its own buffer while the next step runs; a third call in flight reuses the
+    first snapshot buffer once its copy has landed."""
+    sc = S.single_drape(seed=4)
+    c = sc.cloths[0]
+    n = len(c.particles)
+    cid = ctx.add_cloth(c)
+    orc = c.copy()
+    try:
+        bufs = [np.zeros(3 * n, np.float32) for _ in range(3)]
+        want = []
+        for k in range(3):
+            ctx.step([cid], sc.colliders)
+            K.oracle_step_cloth(orc, sc.colliders[0])
+            want.append(orc.particles["position"].copy())
+            ctx.read_positions_async([cid], bufs[k])
+        ctx.wait_positions()
+        for k in range(3):
+            assert np.array_equal(bufs[k].reshape(-1, 3), want[k]), k
+        with pytest.raises(R.PxbError) as e:
+            ctx.read_positions_async([cid], np.zeros(3 * n - 1, np.float32))
+        assert e.value.status == A.PXB_ERR_INVALID_ARGUMENT
+    finally:
+        ctx.remove_cloth(cid)
+
+
+def test_pipelined_results_reads(ctx):
+    """pxb_cloths_read_results_async: the last step's per-cloth results in the caller's order,
+    equal to the blocking read, landing while the next step runs."""
+    cloths = [S.single_drape(seed=s).cloths[0] for s in (5, 6, 7)]
+    cols = [S.single_drape(seed=s).colliders[0] for s in (5, 6, 7)]
+    ids = [ctx.add_cloth(c) for c in cloths]
+    try:
+        got = [np.zeros(3, A.FRAME_RESULT) for _ in range(2)]
+        want = []
+        for k in range(2):
+            ctx.step(ids, cols)
+            want.append(ctx.read_results(ids[::-1]).copy())
+            ctx.read_results_async(ids[::-1], got[k])
+        ctx.wait_positions()
+        for k in range(2):
+            assert np.array_equal(got[k].view(np.uint8), want[k].view(np.uint8)), k
+        with pytest.raises(R.PxbError) as e:
+            ctx.step(ids[:1], cols[:1])
+            ctx.read_results_async(ids[1:], got[0][:2])  # not in the last step
+        assert e.value.status == A.PXB_ERR_INVALID_ARGUMENT
+    finally:
+        for i in ids:
+            ctx.remove_cloth(i)

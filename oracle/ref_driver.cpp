@@ -334,6 +334,15 @@ int pxbref_geometry_set_mesh(uint32_t id, const pxb_mesh_desc* d) {
     return 0;
 }
 
+// Registers TriangleMesh::from_height_grid over the reference's own HeightGrid (height_grid.h).
+int pxbref_geometry_set_height_grid(uint32_t id, int nx, int ny, float cell_x, float cell_y, const float* heights,
+                                    uint32_t n_heights) {
+    auto grid = std::make_shared<const px::geometry::HeightGrid>(
+        nx, ny, glm::vec2(cell_x, cell_y), std::vector<float>(heights, heights + n_heights));
+    g_meshes[id] = std::make_unique<px::geometry::TriangleMesh>(px::geometry::TriangleMesh::from_height_grid(grid));
+    return 0;
+}
+
 void pxbref_geometry_clear() {
     g_hulls.clear();
     g_meshes.clear();

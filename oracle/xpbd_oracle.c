@@ -8,6 +8,7 @@
  */
 #include "xpbd_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -114,6 +115,14 @@ typedef struct {
     orc_bvh_node* nodes;
     uint32_t n_nodes;
     uint32_t* order;
+    /* geometry::HeightGrid (height_grid.h) behind TriangleMesh::from_height_grid */
+    int grid;
+    int nx, ny;
+    float cell_x, cell_y;
+    float* h;                     /* nx * ny heights, row j at j * nx */
+    float* fine;                  /* (lo, hi) per 8 x 8-cell block */
+    float* coarse;                /* (lo, hi) per 64 x 64-cell block */
+    int fine_w, fine_h, coarse_w, coarse_h;
 } orc_geometry;
 
 #define ORC_MAX_GEOMETRY 1024
@@ -122,6 +131,7 @@ static orc_geometry g_geo[ORC_MAX_GEOMETRY];
 static void free_geometry(orc_geometry* g) {
     free(g->verts); free(g->planes); free(g->starts); free(g->fverts);
     free(g->mverts); free(g->idx); free(g->normals); free(g->nodes); free(g->order);
+    free(g->h); free(g->fine); free(g->coarse);
     memset(g, 0, sizeof(*g));
 }
 
@@ -173,6 +183,49 @@ int orc_geometry_set_mesh(uint32_t id, const pxb_mesh_desc* d) {
     g->nodes = (orc_bvh_node*)malloc(sizeof(orc_bvh_node) * (2 * T + 1));
     g->order = (uint32_t*)malloc(sizeof(uint32_t) * (T ? T : 1));
     g->n_nodes = T ? orc_bvh_build(g->mverts, g->idx, T, g->nodes, g->order) : 0;
+    return 0;
+}
+
+/* HeightGrid's constructor and build_pyramid_ (height_grid.h): at least 2 x 2 samples, heights
+ * padded with zeros; per 8- and 64-cell block the lowest and highest sample of its cells. */
+int orc_geometry_set_height_grid(uint32_t id, int nx, int ny, float cell_x, float cell_y, const float* heights,
+                                 uint32_t n_heights) {
+    if (id == 0 || id >= ORC_MAX_GEOMETRY) return -1;
+    orc_geometry* g = &g_geo[id];
+    free_geometry(g);
+    g->type = PXB_SHAPE_TRIANGLE_MESH;
+    g->grid = 1;
+    g->nx = nx < 2 ? 2 : nx;
+    g->ny = ny < 2 ? 2 : ny;
+    g->cell_x = cell_x;
+    g->cell_y = cell_y;
+    const size_t n = (size_t)g->nx * g->ny;
+    g->h = (float*)calloc(n, sizeof(float));
+    memcpy(g->h, heights, sizeof(float) * (n_heights < n ? n_heights : n));
+    const int cx = g->nx - 1, cy = g->ny - 1;
+    g->fine_w = (cx + 7) / 8;
+    g->fine_h = (cy + 7) / 8;
+    g->coarse_w = (cx + 63) / 64;
+    g->coarse_h = (cy + 63) / 64;
+    g->fine = (float*)malloc(sizeof(float) * 2 * g->fine_w * g->fine_h);
+    g->coarse = (float*)malloc(sizeof(float) * 2 * g->coarse_w * g->coarse_h);
+    for (int k = 0; k < g->fine_w * g->fine_h; ++k) { g->fine[2 * k] = FLT_MAX; g->fine[2 * k + 1] = -FLT_MAX; }
+    for (int k = 0; k < g->coarse_w * g->coarse_h; ++k) { g->coarse[2 * k] = FLT_MAX; g->coarse[2 * k + 1] = -FLT_MAX; }
+    for (int j = 0; j < g->ny; ++j)
+        for (int i = 0; i < g->nx; ++i) {
+            const float hv = g->h[(size_t)j * g->nx + i];
+            for (int dj = -1; dj <= 0; ++dj)
+                for (int di = -1; di <= 0; ++di) {
+                    const int ci = i + di, cj = j + dj;
+                    if (ci < 0 || cj < 0 || ci >= cx || cj >= cy) continue;
+                    float* f = &g->fine[2 * ((cj / 8) * g->fine_w + ci / 8)];
+                    float* c = &g->coarse[2 * ((cj / 64) * g->coarse_w + ci / 64)];
+                    if (hv < f[0]) f[0] = hv; /* std::min(lo, h) */
+                    if (f[1] < hv) f[1] = hv; /* std::max(hi, h) */
+                    if (hv < c[0]) c[0] = hv;
+                    if (c[1] < hv) c[1] = hv;
+                }
+        }
     return 0;
 }
 
@@ -356,6 +409,83 @@ static void mesh_tri(const orc_geometry* g, uint32_t t, v3* v0, v3* v1, v3* v2) 
     *v2 = ld(&g->mverts[3 * g->idx[3 * t + 2]]);
 }
 
+/* HeightGrid::vertex / triangle_vertices (height_grid.h): cell (i, j)'s triangles are
+ * (i,j)-(i+1,j)-(i+1,j+1) and (i,j)-(i+1,j+1)-(i,j+1), numbered (j (nx - 1) + i) * 2 + half */
+static v3 grid_vertex(const orc_geometry* g, int i, int j) {
+    return mk((float)i * g->cell_x, (float)j * g->cell_y, g->h[(size_t)j * g->nx + i]);
+}
+static void grid_tri(const orc_geometry* g, uint32_t tri, v3* v0, v3* v1, v3* v2) {
+    const int half = (int)(tri & 1u);
+    const int cell = (int)(tri >> 1);
+    const int i = cell % (g->nx - 1), j = cell / (g->nx - 1);
+    *v0 = grid_vertex(g, i, j);
+    if (half == 0) {
+        *v1 = grid_vertex(g, i + 1, j);
+        *v2 = grid_vertex(g, i + 1, j + 1);
+    } else {
+        *v1 = grid_vertex(g, i + 1, j + 1);
+        *v2 = grid_vertex(g, i, j + 1);
+    }
+}
+
+/* TriangleMesh::triangle_vertices / triangle_normal (triangle_mesh.h:224, 280-290); a grid's
+ * normal is HeightGrid::triangle_normal, normalize(cross(v1 - v0, v2 - v0)), +z when degenerate */
+static void tri_verts(const orc_geometry* g, uint32_t tri, v3* v0, v3* v1, v3* v2) {
+    if (g->grid) grid_tri(g, tri, v0, v1, v2);
+    else mesh_tri(g, tri, v0, v1, v2);
+}
+static v3 tri_normal(const orc_geometry* g, uint32_t tri) {
+    if (!g->grid) return ld(&g->normals[3 * tri]);
+    v3 v0, v1, v2;
+    grid_tri(g, tri, &v0, &v1, &v2);
+    const v3 n = cross(sub(v1, v0), sub(v2, v0));
+    const float l = len(n);
+    return l > 0.0f ? divs(n, l) : mk(0.0f, 0.0f, 1.0f);
+}
+
+typedef int (*box_pred)(const void* ctx, const float* mn, const float* mx);
+typedef void (*tri_fn)(void* ctx, uint32_t tri);
+
+/* HeightGrid::visit_ (height_grid.h): 64-cell blocks, their 8-cell blocks, their cells, each in
+ * row-major order, a block or cell skipped when its box (cells x, y; lowest to highest sample)
+ * fails the test; a cell's two triangles in order */
+static void grid_visit(const orc_geometry* g, box_pred pred, const void* pctx, tri_fn fn, void* fctx) {
+    const int cx = g->nx - 1, cy = g->ny - 1;
+#define GH(i, j) g->h[(size_t)(j) * g->nx + (i)]
+    for (int gj = 0; gj < g->coarse_h; ++gj)
+        for (int gi = 0; gi < g->coarse_w; ++gi) {
+            const int c0i = gi * 64, c0j = gj * 64;
+            const int c1i = c0i + 64 < cx ? c0i + 64 : cx, c1j = c0j + 64 < cy ? c0j + 64 : cy;
+            const float* cr = &g->coarse[2 * (gj * g->coarse_w + gi)];
+            float mn[3] = {(float)c0i * g->cell_x, (float)c0j * g->cell_y, cr[0]};
+            float mx[3] = {(float)c1i * g->cell_x, (float)c1j * g->cell_y, cr[1]};
+            if (!pred(pctx, mn, mx)) continue;
+            for (int fj = c0j / 8; fj * 8 < c1j; ++fj)
+                for (int fi = c0i / 8; fi * 8 < c1i; ++fi) {
+                    const int f0i = fi * 8, f0j = fj * 8;
+                    const int f1i = f0i + 8 < cx ? f0i + 8 : cx, f1j = f0j + 8 < cy ? f0j + 8 : cy;
+                    const float* fr = &g->fine[2 * (fj * g->fine_w + fi)];
+                    float fmn[3] = {(float)f0i * g->cell_x, (float)f0j * g->cell_y, fr[0]};
+                    float fmx[3] = {(float)f1i * g->cell_x, (float)f1j * g->cell_y, fr[1]};
+                    if (!pred(pctx, fmn, fmx)) continue;
+                    for (int j = f0j; j < f1j; ++j)
+                        for (int i = f0i; i < f1i; ++i) {
+                            /* std::min / std::max of the cell's four samples, as written */
+                            const float a = GH(i, j), b = GH(i + 1, j), c = GH(i, j + 1), d = GH(i + 1, j + 1);
+                            const float lo1 = b < a ? b : a, lo2 = d < c ? d : c;
+                            const float hi1 = a < b ? b : a, hi2 = c < d ? d : c;
+                            float cmn[3] = {(float)i * g->cell_x, (float)j * g->cell_y, lo2 < lo1 ? lo2 : lo1};
+                            float cmx[3] = {(float)(i + 1) * g->cell_x, (float)(j + 1) * g->cell_y,
+                                            hi1 < hi2 ? hi2 : hi1};
+                            if (!pred(pctx, cmn, cmx)) continue;
+                            fn(fctx, (uint32_t)((j * cx + i) * 2));
+                            fn(fctx, (uint32_t)((j * cx + i) * 2 + 1));
+                        }
+                }
+        }
+#undef GH
+}
+
 typedef struct {
     const orc_geometry* g;
     ray3 ray;
@@ -364,26 +494,33 @@ typedef struct {
     int crossed;
 } raycast_state;
 
-/* MeshBVH::raycast_recursive_ with the swept crossing callback (cloth_collision.h:243-257) */
+/* the swept crossing callback (cloth_collision.h:243-257) on one triangle */
+static void raycast_tri(void* ctx, uint32_t tri) {
+    raycast_state* s = (raycast_state*)ctx;
+    v3 v0, v1, v2;
+    tri_verts(s->g, tri, &v0, &v1, &v2);
+    float t = 0.0f;
+    if ((ray_triangle(&s->ray, v0, v1, v2, &t) || ray_triangle(&s->ray, v0, v2, v1, &t)) && t < s->best_t) {
+        s->best_t = t;
+        s->crossed_tri = tri;
+        s->crossed = 1;
+    }
+}
+
+/* MeshBVH::raycast_recursive_ */
 static void raycast_node(raycast_state* s, int32_t idx) {
     const orc_bvh_node* node = &s->g->nodes[idx];
     if (!ray_box(&s->ray, node->mn, node->mx)) return;
     if (node->left < 0) {
-        for (uint32_t i = 0; i < node->tri_count; ++i) {
-            const uint32_t tri = s->g->order[node->tri_start + i];
-            v3 v0, v1, v2;
-            mesh_tri(s->g, tri, &v0, &v1, &v2);
-            float t = 0.0f;
-            if ((ray_triangle(&s->ray, v0, v1, v2, &t) || ray_triangle(&s->ray, v0, v2, v1, &t)) && t < s->best_t) {
-                s->best_t = t;
-                s->crossed_tri = tri;
-                s->crossed = 1;
-            }
-        }
+        for (uint32_t i = 0; i < node->tri_count; ++i) raycast_tri(s, s->g->order[node->tri_start + i]);
     } else {
         raycast_node(s, node->left);
         raycast_node(s, node->right);
     }
+}
+
+static int ray_pred(const void* ctx, const float* mn, const float* mx) {
+    return ray_box(&((const raycast_state*)ctx)->ray, mn, mx);
 }
 
 typedef struct {
@@ -396,30 +533,37 @@ typedef struct {
     int hit, any_front;
 } query_state;
 
-/* MeshBVH::query_recursive_ with the proximity callback (cloth_collision.h:291-310) */
+/* the proximity callback (cloth_collision.h:291-310) on one triangle */
+static void query_tri(void* ctx, uint32_t tri) {
+    query_state* s = (query_state*)ctx;
+    v3 v0, v1, v2;
+    tri_verts(s->g, tri, &v0, &v1, &v2);
+    const v3 closest = closest_on_triangle(s->local_p, v0, v1, v2);
+    const v3 delta = sub(s->local_p, closest);
+    const float d2 = dot(delta, delta);
+    if (d2 > s->lt2) return;
+    if (dot(delta, tri_normal(s->g, tri)) >= 0.0f) s->any_front = 1;
+    if (d2 > s->best_d2) return;
+    s->best_d2 = d2;
+    s->best_point = closest;
+    s->best_delta = delta;
+    s->best_tri = tri;
+    s->hit = 1;
+}
+
+/* AABB::overlaps (aabb.h:35-39) of a box with the query box */
+static int overlap_pred(const void* ctx, const float* mn, const float* mx) {
+    const query_state* s = (const query_state*)ctx;
+    return mn[0] <= s->qmax.x && mx[0] >= s->qmin.x && mn[1] <= s->qmax.y && mx[1] >= s->qmin.y &&
+           mn[2] <= s->qmax.z && mx[2] >= s->qmin.z;
+}
+
+/* MeshBVH::query_recursive_ */
 static void query_node(query_state* s, int32_t idx) {
     const orc_bvh_node* node = &s->g->nodes[idx];
-    /* AABB::overlaps (aabb.h:35-39) */
-    if (!(node->mn[0] <= s->qmax.x && node->mx[0] >= s->qmin.x && node->mn[1] <= s->qmax.y &&
-          node->mx[1] >= s->qmin.y && node->mn[2] <= s->qmax.z && node->mx[2] >= s->qmin.z))
-        return;
+    if (!overlap_pred(s, node->mn, node->mx)) return;
     if (node->left < 0) {
-        for (uint32_t i = 0; i < node->tri_count; ++i) {
-            const uint32_t tri = s->g->order[node->tri_start + i];
-            v3 v0, v1, v2;
-            mesh_tri(s->g, tri, &v0, &v1, &v2);
-            const v3 closest = closest_on_triangle(s->local_p, v0, v1, v2);
-            const v3 delta = sub(s->local_p, closest);
-            const float d2 = dot(delta, delta);
-            if (d2 > s->lt2) continue;
-            if (dot(delta, ld(&s->g->normals[3 * tri])) >= 0.0f) s->any_front = 1;
-            if (d2 > s->best_d2) continue;
-            s->best_d2 = d2;
-            s->best_point = closest;
-            s->best_delta = delta;
-            s->best_tri = tri;
-            s->hit = 1;
-        }
+        for (uint32_t i = 0; i < node->tri_count; ++i) query_tri(s, s->g->order[node->tri_start + i]);
     } else {
         query_node(s, node->left);
         query_node(s, node->right);
@@ -430,7 +574,7 @@ static void query_node(query_state* s, int32_t idx) {
 static int project_mesh(const pxb_collider* s, v3 pose_pos, q4 pose_rot, float thickness, v3* p,
                         v3* normal_out, float* depth_out, const v3* motion_start) {
     const orc_geometry* g = geometry_of(s, PXB_SHAPE_TRIANGLE_MESH);
-    if (!g || g->n_nodes == 0) return 0;
+    if (!g || (!g->grid && g->n_nodes == 0)) return 0; /* TriangleMesh::empty() */
     const q4 rot = qmul(pose_rot, ldq(s->local_rotation));
     const q4 inv_rot = qinverse(rot);
     const v3 mesh_origin = add(pose_pos, qrot(pose_rot, ld(s->local_center)));
@@ -451,10 +595,11 @@ static int project_mesh(const pxb_collider* s, v3 pose_pos, q4 pose_rot, float t
             rs.best_t = seg_len;
             rs.crossed_tri = 0;
             rs.crossed = 0;
-            raycast_node(&rs, 0);
+            if (g->grid) grid_visit(g, ray_pred, &rs, raycast_tri, &rs);
+            else raycast_node(&rs, 0);
             if (rs.crossed) {
                 const v3 local_hit = add(rs.ray.origin, mul(rs.ray.direction, rs.best_t));
-                v3 face = safe_normalize(ld(&g->normals[3 * rs.crossed_tri]));
+                v3 face = safe_normalize(tri_normal(g, rs.crossed_tri));
                 if (dot(sub(local_start, local_hit), face) < 0.0f) face = neg(face);
                 const v3 local_fixed = add(local_hit, mul(face, local_thickness));
                 *depth_out = len(sub(local_p, local_fixed)) * scale;
@@ -473,15 +618,16 @@ static int project_mesh(const pxb_collider* s, v3 pose_pos, q4 pose_rot, float t
     qs.qmax = add(local_p, mk(local_thickness, local_thickness, local_thickness));
     qs.lt2 = local_thickness * local_thickness;
     qs.best_d2 = local_thickness * local_thickness;
-    query_node(&qs, 0);
+    if (g->grid) grid_visit(g, overlap_pred, &qs, query_tri, &qs);
+    else query_node(&qs, 0);
     if (!qs.hit) return 0;
     v3 best_normal;
     if (!qs.any_front) {
-        best_normal = safe_normalize(ld(&g->normals[3 * qs.best_tri]));
+        best_normal = safe_normalize(tri_normal(g, qs.best_tri));
     } else if (qs.best_d2 > K_EPSILON * K_EPSILON) {
         best_normal = divs(qs.best_delta, sqrtf(qs.best_d2));
     } else {
-        const v3 face = safe_normalize(ld(&g->normals[3 * qs.best_tri]));
+        const v3 face = safe_normalize(tri_normal(g, qs.best_tri));
         best_normal = (dot(qs.best_delta, face) < 0.0f) ? neg(face) : face;
     }
     const v3 local_fixed = add(qs.best_point, mul(best_normal, local_thickness));

@@ -60,6 +60,10 @@ int orc_solve_cloth(orc_cloth* c, const pxb_collider* colliders, uint32_t n_coll
  * MeshBVH built by orc_bvh_build. */
 int orc_geometry_set_hull(uint32_t id, const pxb_hull_desc* desc);
 int orc_geometry_set_mesh(uint32_t id, const pxb_mesh_desc* desc);
+/* A TriangleMesh::from_height_grid over geometry::HeightGrid(nx, ny, (cell_x, cell_y), heights)
+ * (height_grid.h), queried through the grid's block pyramid as the reference does. */
+int orc_geometry_set_height_grid(uint32_t id, int nx, int ny, float cell_x, float cell_y, const float* heights,
+                                 uint32_t n_heights);
 void orc_geometry_clear(void);
 
 /* One MeshBVH node (mesh_bvh.h): bounds, children (left < 0 for a leaf) and the leaf's range of

@@ -130,6 +130,12 @@ class MeshClothDesc(C.Structure):
                 ("n_indices", C.c_uint32), ("total_mass", f32), ("bend", C.c_int32), ("params", ClothParams)]
 
 
+class HeightGridDesc(C.Structure):
+    """pxb_height_grid_desc: geometry::HeightGrid's samples."""
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("cell_x", f32), ("cell_y", f32),
+                ("heights", C.c_void_p), ("n_heights", C.c_uint32)]
+
+
 class ClothPlan(C.Structure):
     """pxb_cloth_plan: the device layout pxb_cloth_add would choose."""
     _fields_ = [("n_ranks", C.c_int32), ("rows_per_rank", C.c_int32), ("threads", C.c_int32),

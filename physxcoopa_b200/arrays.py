@@ -287,6 +287,35 @@ class Mesh:
         return self.vertices.min(axis=0), self.vertices.max(axis=0)
 
 
+class HeightGrid:
+    """geometry::HeightGrid's samples (physxcoopa/geometry/height_grid.h): nx x ny heights, row j
+    at j * nx, sample (i, j) at (i * cell_x, j * cell_y, height); used as a TriangleMesh through
+    TriangleMesh::from_height_grid (triangle_mesh.h:210-215), two triangles per cell."""
+
+    def __init__(self, nx, ny, cell, heights):
+        self.nx, self.ny = int(nx), int(ny)
+        self.cell = (float(cell[0]), float(cell[1]))
+        self.heights = np.ascontiguousarray(heights, np.float32).reshape(-1)
+
+    def desc(self):
+        d = A.HeightGridDesc()
+        d.nx, d.ny = self.nx, self.ny
+        d.cell_x, d.cell_y = self.cell
+        d.heights = A.ptr(self.heights)
+        d.n_heights = len(self.heights)
+        return d
+
+    def local_bounds(self):
+        """HeightGrid::bounds(): the box of every sample (heights padded with zeros)."""
+        nx, ny = max(2, self.nx), max(2, self.ny)
+        h = np.zeros(nx * ny, np.float32)
+        h[:min(len(self.heights), nx * ny)] = self.heights[:nx * ny]
+        lo = np.array([0.0, 0.0, h.min()], np.float32)
+        hi = np.array([np.float32(nx - 1) * np.float32(self.cell[0]), np.float32(ny - 1) * np.float32(self.cell[1]),
+                       h.max()], np.float32)
+        return lo, hi
+
+
 def make_collider(shape_type, position=(0, 0, 0), orientation=IDENTITY, *, radius=0.5,
                   half_extents=(0.5, 0.5, 0.5), capsule_radius=0.5, capsule_half_height=0.5,
                   capsule_axis=2, local_center=(0, 0, 0), local_rotation=IDENTITY,

@@ -27,7 +27,7 @@ from typing import List, Optional
 import numpy as np
 
 from . import _abi as A
-from .arrays import (ClothArrays, Hull, Mesh, box, capsule, collider_array, gravity_sources, hull_collider,
+from .arrays import (ClothArrays, HeightGrid, Hull, Mesh, box, capsule, collider_array, gravity_sources, hull_collider,
                      mesh_collider, sphere)
 from .runtime import HostCloth
 
@@ -303,6 +303,24 @@ def terrain_mesh(n=32, size=3.0, amp=0.15, seed=0):
             b, c, d = a + 1, a + n + 2, a + n + 1
             idx += [a, b, c, a, c, d]
     return Mesh(verts, np.array(idx, np.uint32))
+
+
+def height_grid_terrain(nx=40, ny=40, cell=0.08, amp=0.12, seed=0):
+    """A seeded height grid (geometry::HeightGrid): two sine ridges plus uniform noise of
+    amplitude amp / 4, centred on the origin by the collider's local centre."""
+    rng = np.random.default_rng(seed)
+    i, j = np.meshgrid(np.arange(nx), np.arange(ny))
+    h = amp * (np.sin(0.35 * i + 0.2) * np.cos(0.27 * j)) + rng.uniform(-0.25, 0.25, (ny, nx)) * amp
+    return HeightGrid(nx, ny, (cell, cell), h.astype(np.float32).reshape(-1))
+
+
+def height_grid_drape(side=20, seed=14, params=None):
+    """One sheet dropped onto a height-grid terrain (geometry id 1) beside a sphere."""
+    grid = height_grid_terrain(40, 36, 0.06, 0.1, seed)
+    centre = (-0.5 * 39 * 0.06, -0.5 * 35 * 0.06, 0.0)
+    c = _sheet(side, (0.0, 0.0, 0.3), seed, [], params=params, tethers=False)
+    cols = collider_array([mesh_collider(1, grid, local_center=centre), sphere(0.12, (0.3, -0.2, 0.15))])
+    return ClothScene(f"height_grid_drape {side}x{side}", [c], [cols], meta={"side": side}, geometries=[grid])
 
 
 def terrain_drape(side=32, seed=11, params=None):

@@ -380,7 +380,14 @@ def ref_project(collider, thickness, p, motion_start=None):
 def register_geometry(gid, geometry):
     """Registers a Hull or Mesh (physxcoopa_b200.arrays) under `gid` with the oracle and, when
     it is built, the reference driver, so colliders naming `gid` mean the same shape to both."""
-    from physxcoopa_b200.arrays import Hull
+    from physxcoopa_b200.arrays import HeightGrid, Hull
+    if isinstance(geometry, HeightGrid):
+        args = (gid, geometry.nx, geometry.ny, C.c_float(geometry.cell[0]), C.c_float(geometry.cell[1]),
+                A.ptr(geometry.heights), len(geometry.heights))
+        assert oracle().orc_geometry_set_height_grid(*args) == 0
+        if ref_available():
+            assert ref().pxbref_geometry_set_height_grid(*args) == 0
+        return
     d = geometry.desc()
     if isinstance(geometry, Hull):
         assert oracle().orc_geometry_set_hull(gid, C.byref(d)) == 0

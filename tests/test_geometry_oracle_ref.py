@@ -8,7 +8,7 @@ import pytest
 
 from physxcoopa_b200 import _abi as A
 from physxcoopa_b200 import scenes as S
-from physxcoopa_b200.arrays import collider_array, hull_collider, mesh_collider, sphere
+from physxcoopa_b200.arrays import HeightGrid, collider_array, hull_collider, mesh_collider, sphere
 
 import _checkers as K
 
@@ -252,3 +252,51 @@ def test_strands_over_a_mesh_and_hull_match_reference_bitwise():
     got = ref.arrays(p)
     for f in ("position", "velocity", "prev_position"):
         assert same(orc.particles[f], got.particles[f]), f
+
+
+def grids():
+    """Height grids of one coarse block, of several (the 64-cell blocks and the ragged 8-cell
+    blocks at their edges), and flat with a spike (equal distances to many triangles)."""
+    flat = np.zeros(24 * 20, np.float32)
+    flat[10 * 24 + 11] = 0.3
+    return {"small": S.height_grid_terrain(20, 17, 0.1, 0.15, seed=2),
+            "multi_block": S.height_grid_terrain(140, 75, 0.02, 0.05, seed=3),
+            "flat_spike": HeightGrid(24, 20, (0.05, 0.07), flat)}
+
+
+@pytest.mark.parametrize("name", ["small", "multi_block", "flat_spike"])
+def test_height_grid_projection_matches_reference(name):
+    """TriangleMesh::from_height_grid (triangle_mesh.h:210-215): queries walk the grid's block
+    pyramid (height_grid.h), not a MeshBVH; the oracle restates it and equals the reference."""
+    grid = grids()[name]
+    K.register_geometry(9, grid)
+    rng = np.random.default_rng(13)
+    lo, hi = grid.local_bounds()
+    total = 0
+    for q in QUATS[:2]:
+        for scale in (1.0, 0.8):
+            col = mesh_collider(9, grid, (0.1, -0.3, 0.05), unit(q), scale=scale, local_center=(-0.4, -0.3, 0.0))
+            local = rng.uniform(lo - 0.04, hi + 0.04, (300, 3)).astype(np.float32)
+            world = np.array([K_pose(col, p) for p in local], np.float32)
+            total += compare(col, 0.04, world)
+            d = rng.normal(size=(300, 3)).astype(np.float32)
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            total += compare(col, 0.04, world, (world + 0.25 * d).astype(np.float32))
+    assert total > 100
+
+
+def test_cloth_on_height_grid_matches_reference_bitwise():
+    sc = S.height_grid_drape(side=16, params=A.ClothParams.defaults())
+    _register(sc)
+    ref = K.RefCloth.from_arrays(sc.cloths[0])
+    orc = sc.cloths[0].copy()
+    cols = sc.colliders[0]
+    for step in range(60):
+        ref.solve(cols, substeps=4, iterations=6)
+        K.oracle_step_cloth(orc, cols, substeps=4, iterations=6)
+        if step % 20 == 19:
+            got = ref.arrays()
+            for f in ("position", "prev_position", "velocity"):
+                assert same(orc.particles[f], got.particles[f]), (step, f)
+    # it came to rest on the terrain
+    assert ref.arrays().particles["position"][:, 2].min() > -0.2

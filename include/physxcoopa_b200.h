@@ -550,6 +550,18 @@ pxb_status pxb_geometry_create_mesh(pxb_context* ctx, const pxb_mesh_desc* desc,
 
 /* Waits for the context's stream, then frees the geometry. A later step naming its id is refused
  * with PXB_ERR_INVALID_HANDLE. */
+/* A height-grid mesh (TriangleMesh::from_height_grid over geometry::HeightGrid, height_grid.h,
+ * triangle_mesh.h:210-215): nx x ny samples (at least 2 x 2; heights padded with zeros), sample
+ * (i, j) at (i * cell_x, j * cell_y, heights[j * nx + i]), two triangles per cell. Mesh colliders
+ * naming it are queried through the grid's block pyramid in the reference's order. At most 2^24
+ * samples. */
+typedef struct pxb_height_grid_desc {
+    uint32_t nx, ny;
+    float cell_x, cell_y;
+    const float* heights;
+    uint32_t n_heights;
+} pxb_height_grid_desc;
+pxb_status pxb_geometry_create_height_grid(pxb_context* ctx, const pxb_height_grid_desc* desc, uint32_t* id_out);
 pxb_status pxb_geometry_destroy(pxb_context* ctx, uint32_t id);
 
 /* ------------------------------------------------------------------------------------------ */

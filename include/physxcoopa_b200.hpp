@@ -70,13 +70,26 @@ public:
         geometry_[h] = id;
         return id;
     }
-    // The device copy of a Shape's triangle mesh (Shape::mesh, shape.h:85). Height-grid meshes
-    // (TriangleMesh::from_height_grid) have no vertex arrays and are refused.
+    // The device copy of a Shape's triangle mesh (Shape::mesh, shape.h:85). A height-grid mesh
+    // (TriangleMesh::from_height_grid, triangle_mesh.h:210) registers its grid's samples.
     uint32_t geometry_id(const coopa::physx::geometry::TriangleMesh* m) {
         if (!m) return 0;
         auto it = geometry_.find(m);
         if (it != geometry_.end()) return it->second;
-        if (m->height_grid()) throw std::runtime_error("height-grid meshes are not supported by the device path");
+        if (const coopa::physx::geometry::HeightGrid* g = m->height_grid()) {
+            pxb_height_grid_desc hd;
+            std::memset(&hd, 0, sizeof(hd));
+            hd.nx = static_cast<uint32_t>(g->nx());
+            hd.ny = static_cast<uint32_t>(g->ny());
+            hd.cell_x = g->cell().x;
+            hd.cell_y = g->cell().y;
+            hd.heights = g->heights().data();
+            hd.n_heights = static_cast<uint32_t>(g->heights().size());
+            uint32_t id = 0;
+            check(pxb_geometry_create_height_grid(ctx_, &hd, &id), "register height grid");
+            geometry_[m] = id;
+            return id;
+        }
         pxb_mesh_desc d;
         std::memset(&d, 0, sizeof(d));
         d.vertices = reinterpret_cast<const float*>(m->vertices().data());

@@ -212,6 +212,13 @@ void ColliderStage::fill(const pxb_context* ctx, const pxb_collider* c, uint32_t
         o.qi[0] = inv.x; o.qi[1] = inv.y; o.qi[2] = inv.z; o.qi[3] = inv.w;
         st(o.origin, origin);
         o.scale = c[k].geometry_scale > 1e-6f ? c[k].geometry_scale : 1.0f;
+        if (g->grid) {  // a height grid: its record, walked through its block pyramid
+            o.geo_count = 1;
+            o.geo_aux = -1;
+            o.geo = g->d_tris;
+            o.nodes = nullptr;
+            continue;
+        }
         o.geo_count = g->n_nodes;
         o.geo_aux = g->depth;
         o.geo = g->d_tris;
@@ -307,6 +314,66 @@ pxb_status pxb_geometry_create_mesh(pxb_context* ctx, const pxb_mesh_desc* d, ui
         g.n_nodes = static_cast<int>(bvh.nodes.size());
         g.depth = bvh.depth;
     }
+    *id_out = add_geometry(ctx, std::move(g));
+    return PXB_OK;
+}
+
+pxb_status pxb_geometry_create_height_grid(pxb_context* ctx, const pxb_height_grid_desc* d, uint32_t* id_out) {
+    if (!ctx || !d || !id_out) return PXB_ERR_INVALID_ARGUMENT;
+    if (d->n_heights && !d->heights) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "null heights");
+    // HeightGrid's constructor (height_grid.h): at least 2 x 2 samples, heights padded with zeros
+    const int nx = std::max<int>(2, static_cast<int>(std::min<uint32_t>(d->nx, 1u << 15)));
+    const int ny = std::max<int>(2, static_cast<int>(std::min<uint32_t>(d->ny, 1u << 15)));
+    if (d->nx > (1u << 15) || d->ny > (1u << 15) || static_cast<uint64_t>(nx) * ny > (1ull << 24))
+        return ctx->fail(PXB_ERR_TOO_LARGE, "height grid of %u x %u samples (at most 2^24 samples, sides up to 32768)",
+                         d->nx, d->ny);
+    const size_t n = static_cast<size_t>(nx) * ny;
+    std::vector<float> h(n, 0.0f);
+    std::memcpy(h.data(), d->heights, sizeof(float) * std::min<size_t>(n, d->n_heights));
+    // build_pyramid_: each 8- and 64-cell block's lowest and highest sample over its cells
+    const int cx = nx - 1, cy = ny - 1;
+    const int fw = (cx + 7) / 8, fh = (cy + 7) / 8, cw = (cx + 63) / 64, ch = (cy + 63) / 64;
+    std::vector<float> fine(2 * static_cast<size_t>(fw) * fh), coarse(2 * static_cast<size_t>(cw) * ch);
+    for (size_t k = 0; k < fine.size(); k += 2) { fine[k] = std::numeric_limits<float>::max(); fine[k + 1] = std::numeric_limits<float>::lowest(); }
+    for (size_t k = 0; k < coarse.size(); k += 2) { coarse[k] = std::numeric_limits<float>::max(); coarse[k + 1] = std::numeric_limits<float>::lowest(); }
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const float hv = h[static_cast<size_t>(j) * nx + i];
+            for (int dj = -1; dj <= 0; ++dj)
+                for (int di = -1; di <= 0; ++di) {
+                    const int ci = i + di, cj = j + dj;
+                    if (ci < 0 || cj < 0 || ci >= cx || cj >= cy) continue;
+                    float* f = &fine[2 * (static_cast<size_t>(cj / 8) * fw + ci / 8)];
+                    float* c = &coarse[2 * (static_cast<size_t>(cj / 64) * cw + ci / 64)];
+                    f[0] = std::min(f[0], hv);
+                    f[1] = std::max(f[1], hv);
+                    c[0] = std::min(c[0], hv);
+                    c[1] = std::max(c[1], hv);
+                }
+        }
+    // the device record: two header float4s, heights, 8-cell ranges, 64-cell ranges
+    std::vector<float> rec(8 + n + fine.size() + coarse.size());
+    const int32_t head[8] = {nx, ny, 0, 0, fw, fh, cw, ch};
+    std::memcpy(rec.data(), head, sizeof(head));
+    std::memcpy(&rec[2], &d->cell_x, 4);
+    std::memcpy(&rec[3], &d->cell_y, 4);
+    std::memcpy(&rec[8], h.data(), 4 * n);
+    std::memcpy(&rec[8 + n], fine.data(), 4 * fine.size());
+    std::memcpy(&rec[8 + n + fine.size()], coarse.data(), 4 * coarse.size());
+    void* mem = nullptr;
+    if (pxb_status s = ctx->cuda(cudaMalloc(&mem, 4 * rec.size()), "height grid")) return s;
+    if (pxb_status s = ctx->cuda(cudaMemcpy(mem, rec.data(), 4 * rec.size(), cudaMemcpyHostToDevice), "upload height grid")) {
+        cudaFree(mem);
+        return s;
+    }
+    GeometryEntry g;
+    g.alive = true;
+    g.type = PXB_SHAPE_TRIANGLE_MESH;
+    g.grid = true;
+    g.dmem = mem;
+    g.d_tris = static_cast<const float4*>(mem);
+    g.n_nodes = 1;
+    g.depth = -1;
     *id_out = add_geometry(ctx, std::move(g));
     return PXB_OK;
 }

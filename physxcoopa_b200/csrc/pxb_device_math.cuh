@@ -280,17 +280,138 @@ __device__ __forceinline__ bool ray_box(f3 o, f3 inv, float max_d, float4 na, fl
 // length), then the proximity query (MeshBVH::query over the thickness box). Both walk the
 // hierarchy depth first, left child before right, which is MeshBVH's recursion order, so every
 // tie between equally near triangles resolves as in the reference.
-__device__ __noinline__ bool project_mesh(const PxbDevCollider* __restrict__ c, float thickness, f3& p,
-                                          f3& normal_out, float& depth_out, f3 start, bool has_start) {
-    const int n_nodes = __ldg(&c->geo_count);
-    if (n_nodes == 0) return false;  // TriangleMesh::empty()
-    const float4* __restrict__ nodes = c->nodes;
-    const float4* __restrict__ tris = c->geo;
+// A stored mesh's triangles: the hierarchy in PxbMeshNode records, the triangles in its order
+// with their normals (PxbMeshTri). Walks are depth-first, left before right (MeshBVH).
+struct BvhTris {
+    const float4* __restrict__ nodes;
+    const float4* __restrict__ tris;
+    __device__ __forceinline__ void tri(int j, f3& v0, f3& v1, f3& v2) const {
+        v0 = ldx(&tris[4 * j]);
+        v1 = ldx(&tris[4 * j + 1]);
+        v2 = ldx(&tris[4 * j + 2]);
+    }
+    __device__ __forceinline__ f3 normal(int j) const { return ldx(&tris[4 * j + 3]); }
+    // every triangle of every node whose box passes `box(mn, mx)` (float4: xyz used)
+    template <class Box, class Fn>
+    __device__ __forceinline__ void visit(Box box, Fn fn) const {
+        int stack[PXB_MESH_MAX_DEPTH + 4];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const int idx = stack[--sp];
+            const float4 na = __ldg(&nodes[2 * idx]), nb = __ldg(&nodes[2 * idx + 1]);
+            if (!box(na, nb)) continue;
+            const int left = __float_as_int(na.w), right = __float_as_int(nb.w);
+            if (left >= 0) {
+                stack[sp++] = right;
+                stack[sp++] = left;
+                continue;
+            }
+            const int t0 = -1 - left;
+            for (int j = t0; j < t0 + right; ++j) fn(j);
+        }
+    }
+};
+
+// A height grid's triangles (geometry::HeightGrid, height_grid.h), from the geometry record:
+// float4 (nx, ny as int bits, cell x, y), float4 (8-cell block columns, rows, 64-cell block
+// columns, rows as int bits), then nx * ny heights (row j at j * nx), the 8-cell blocks' and the
+// 64-cell blocks' (lowest, highest) sample. Cell (i, j)'s triangles are (i,j)-(i+1,j)-(i+1,j+1)
+// and (i,j)-(i+1,j+1)-(i,j+1), numbered (j (nx - 1) + i) * 2 + half.
+struct GridTris {
+    const float* __restrict__ h;
+    const float* __restrict__ fine;
+    const float* __restrict__ coarse;
+    int nx, ny, fw, fh, cw, ch;
+    float cx, cy;
+    __device__ __forceinline__ explicit GridTris(const float4* g) {
+        const float4 a = __ldg(&g[0]), b = __ldg(&g[1]);
+        nx = __float_as_int(a.x);
+        ny = __float_as_int(a.y);
+        cx = a.z;
+        cy = a.w;
+        fw = __float_as_int(b.x);
+        fh = __float_as_int(b.y);
+        cw = __float_as_int(b.z);
+        ch = __float_as_int(b.w);
+        h = reinterpret_cast<const float*>(g + 2);
+        fine = h + static_cast<size_t>(nx) * ny;
+        coarse = fine + 2 * static_cast<size_t>(fw) * fh;
+    }
+    __device__ __forceinline__ float at(int i, int j) const { return __ldg(&h[static_cast<size_t>(j) * nx + i]); }
+    __device__ __forceinline__ f3 vertex(int i, int j) const {
+        return mk(static_cast<float>(i) * cx, static_cast<float>(j) * cy, at(i, j));
+    }
+    __device__ __forceinline__ void tri(int t, f3& v0, f3& v1, f3& v2) const {
+        const int half = t & 1, cell = t >> 1;
+        const int j = cell / (nx - 1), i = cell - j * (nx - 1);
+        v0 = vertex(i, j);
+        if (half == 0) {
+            v1 = vertex(i + 1, j);
+            v2 = vertex(i + 1, j + 1);
+        } else {
+            v1 = vertex(i + 1, j + 1);
+            v2 = vertex(i, j + 1);
+        }
+    }
+    // HeightGrid::triangle_normal: normalize(cross(v1 - v0, v2 - v0)), +z when degenerate
+    __device__ __forceinline__ f3 normal(int t) const {
+        f3 v0, v1, v2;
+        tri(t, v0, v1, v2);
+        const f3 n = cross(sub(v1, v0), sub(v2, v0));
+        const float l = len(n);
+        return l > 0.0f ? divs(n, l) : mk(0.0f, 0.0f, 1.0f);
+    }
+    // HeightGrid::visit_: 64-cell blocks, their 8-cell blocks, their cells, each row-major, a
+    // block or cell skipped when its box fails `box`; a cell's two triangles in order
+    template <class Box, class Fn>
+    __device__ __forceinline__ void visit(Box box, Fn fn) const {
+        const int cxn = nx - 1, cyn = ny - 1;
+        for (int gj = 0; gj < ch; ++gj)
+            for (int gi = 0; gi < cw; ++gi) {
+                const int c0i = gi * 64, c0j = gj * 64;
+                const int c1i = min(c0i + 64, cxn), c1j = min(c0j + 64, cyn);
+                const float* r = coarse + 2 * (static_cast<size_t>(gj) * cw + gi);
+                if (!box(make_float4(static_cast<float>(c0i) * cx, static_cast<float>(c0j) * cy, __ldg(&r[0]), 0.0f),
+                         make_float4(static_cast<float>(c1i) * cx, static_cast<float>(c1j) * cy, __ldg(&r[1]), 0.0f)))
+                    continue;
+                for (int fj = c0j / 8; fj * 8 < c1j; ++fj)
+                    for (int fi = c0i / 8; fi * 8 < c1i; ++fi) {
+                        const int f0i = fi * 8, f0j = fj * 8;
+                        const int f1i = min(f0i + 8, cxn), f1j = min(f0j + 8, cyn);
+                        const float* q = fine + 2 * (static_cast<size_t>(fj) * fw + fi);
+                        if (!box(make_float4(static_cast<float>(f0i) * cx, static_cast<float>(f0j) * cy, __ldg(&q[0]), 0.0f),
+                                 make_float4(static_cast<float>(f1i) * cx, static_cast<float>(f1j) * cy, __ldg(&q[1]), 0.0f)))
+                            continue;
+                        for (int j = f0j; j < f1j; ++j)
+                            for (int i = f0i; i < f1i; ++i) {
+                                // std::min / std::max of the cell's four samples, as the reference writes them
+                                const float a = at(i, j), b = at(i + 1, j), c = at(i, j + 1), d = at(i + 1, j + 1);
+                                const float lo1 = b < a ? b : a, lo2 = d < c ? d : c;
+                                const float hi1 = a < b ? b : a, hi2 = c < d ? d : c;
+                                if (!box(make_float4(static_cast<float>(i) * cx, static_cast<float>(j) * cy,
+                                                     lo2 < lo1 ? lo2 : lo1, 0.0f),
+                                         make_float4(static_cast<float>(i + 1) * cx, static_cast<float>(j + 1) * cy,
+                                                     hi1 < hi2 ? hi2 : hi1, 0.0f)))
+                                    continue;
+                                fn((j * cxn + i) * 2);
+                                fn((j * cxn + i) * 2 + 1);
+                            }
+                    }
+            }
+    }
+};
+
+// project_at_pose_'s TriangleMesh branch (cloth_collision.h:205-340) over either source: the
+// swept crossing raycast (first hit along the substep's motion), else the proximity query (the
+// last of equally near triangles kept).
+template <class Tris>
+__device__ __forceinline__ bool project_tris(const PxbDevCollider* __restrict__ c, const Tris& T, float thickness,
+                                             f3& p, f3& normal_out, float& depth_out, f3 start, bool has_start) {
     const f3 origin = ld3(c->origin);
     const float scale = __ldg(&c->scale);
     const f3 local_p = divs(qrot4(c->qi, sub(p, origin)), scale);
     const float lt = thickness / scale;
-    int stack[PXB_MESH_MAX_DEPTH + 4];
 
     if (has_start) {
         const f3 local_start = divs(qrot4(c->qi, sub(start, origin)), scale);
@@ -301,32 +422,20 @@ __device__ __noinline__ bool project_mesh(const PxbDevCollider* __restrict__ c, 
             const f3 inv = mk(1.0f / (dir.x + 1e-9f), 1.0f / (dir.y + 1e-9f), 1.0f / (dir.z + 1e-9f));
             float best_t = seg_len;
             int crossed = -1;
-            int sp = 0;
-            stack[sp++] = 0;
-            while (sp > 0) {
-                const int idx = stack[--sp];
-                const float4 na = __ldg(&nodes[2 * idx]), nb = __ldg(&nodes[2 * idx + 1]);
-                if (!ray_box(local_start, inv, seg_len, na, nb)) continue;
-                const int left = __float_as_int(na.w), right = __float_as_int(nb.w);
-                if (left >= 0) {
-                    stack[sp++] = right;
-                    stack[sp++] = left;
-                    continue;
-                }
-                const int t0 = -1 - left;
-                for (int j = t0; j < t0 + right; ++j) {
-                    const f3 v0 = ldx(&tris[4 * j]), v1 = ldx(&tris[4 * j + 1]), v2 = ldx(&tris[4 * j + 2]);
-                    float t = 0.0f;
-                    if ((ray_triangle(local_start, dir, seg_len, v0, v1, v2, t) ||
-                         ray_triangle(local_start, dir, seg_len, v0, v2, v1, t)) && t < best_t) {
-                        best_t = t;
-                        crossed = j;
-                    }
-                }
-            }
+            T.visit([&](float4 na, float4 nb) { return ray_box(local_start, inv, seg_len, na, nb); },
+                    [&](int j) {
+                        f3 v0, v1, v2;
+                        T.tri(j, v0, v1, v2);
+                        float t = 0.0f;
+                        if ((ray_triangle(local_start, dir, seg_len, v0, v1, v2, t) ||
+                             ray_triangle(local_start, dir, seg_len, v0, v2, v1, t)) && t < best_t) {
+                            best_t = t;
+                            crossed = j;
+                        }
+                    });
             if (crossed >= 0) {
                 const f3 local_hit = add(local_start, mul(dir, best_t));
-                f3 face = safe_normalize(ldx(&tris[4 * crossed + 3]));
+                f3 face = safe_normalize(T.normal(crossed));
                 if (dot(sub(local_start, local_hit), face) < 0.0f) face = neg(face);
                 const f3 local_fixed = add(local_hit, mul(face, lt));
                 depth_out = len(sub(local_p, local_fixed)) * scale;
@@ -344,44 +453,33 @@ __device__ __noinline__ bool project_mesh(const PxbDevCollider* __restrict__ c, 
     f3 best_point = mk(0.0f, 0.0f, 0.0f), best_delta = mk(0.0f, 0.0f, 0.0f);
     int best_tri = -1;
     bool any_front = false;
-    int sp = 0;
-    stack[sp++] = 0;
-    while (sp > 0) {
-        const int idx = stack[--sp];
-        const float4 na = __ldg(&nodes[2 * idx]), nb = __ldg(&nodes[2 * idx + 1]);
-        // AABB::overlaps (aabb.h:35-39)
-        if (!(na.x <= qmx.x && nb.x >= qmn.x && na.y <= qmx.y && nb.y >= qmn.y && na.z <= qmx.z &&
-              nb.z >= qmn.z))
-            continue;
-        const int left = __float_as_int(na.w), right = __float_as_int(nb.w);
-        if (left >= 0) {
-            stack[sp++] = right;
-            stack[sp++] = left;
-            continue;
-        }
-        const int t0 = -1 - left;
-        for (int j = t0; j < t0 + right; ++j) {
-            const f3 v0 = ldx(&tris[4 * j]), v1 = ldx(&tris[4 * j + 1]), v2 = ldx(&tris[4 * j + 2]);
-            const f3 closest = closest_on_triangle(local_p, v0, v1, v2);
-            const f3 delta = sub(local_p, closest);
-            const float d2 = dot(delta, delta);
-            if (d2 > lt2) continue;
-            if (dot(delta, ldx(&tris[4 * j + 3])) >= 0.0f) any_front = true;
-            if (d2 > best_d2) continue;
-            best_d2 = d2;
-            best_point = closest;
-            best_delta = delta;
-            best_tri = j;
-        }
-    }
+    // AABB::overlaps (aabb.h:35-39)
+    T.visit([&](float4 na, float4 nb) {
+                return na.x <= qmx.x && nb.x >= qmn.x && na.y <= qmx.y && nb.y >= qmn.y && na.z <= qmx.z &&
+                       nb.z >= qmn.z;
+            },
+            [&](int j) {
+                f3 v0, v1, v2;
+                T.tri(j, v0, v1, v2);
+                const f3 closest = closest_on_triangle(local_p, v0, v1, v2);
+                const f3 delta = sub(local_p, closest);
+                const float d2 = dot(delta, delta);
+                if (d2 > lt2) return;
+                if (dot(delta, T.normal(j)) >= 0.0f) any_front = true;
+                if (d2 > best_d2) return;
+                best_d2 = d2;
+                best_point = closest;
+                best_delta = delta;
+                best_tri = j;
+            });
     if (best_tri < 0) return false;
     f3 bn;
     if (!any_front) {
-        bn = safe_normalize(ldx(&tris[4 * best_tri + 3]));
+        bn = safe_normalize(T.normal(best_tri));
     } else if (best_d2 > PXB_EPSILON * PXB_EPSILON) {
         bn = divs(best_delta, sqrtf(best_d2));
     } else {
-        const f3 face = safe_normalize(ldx(&tris[4 * best_tri + 3]));
+        const f3 face = safe_normalize(T.normal(best_tri));
         bn = dot(best_delta, face) < 0.0f ? neg(face) : face;
     }
     const f3 local_fixed = add(best_point, mul(bn, lt));
@@ -389,6 +487,16 @@ __device__ __noinline__ bool project_mesh(const PxbDevCollider* __restrict__ c, 
     p = add(origin, qrot4(c->q, mul(local_fixed, scale)));
     normal_out = qrot4(c->q, bn);
     return true;
+}
+
+// A mesh collider: a stored mesh (geo_count hierarchy nodes, 0 when empty) or a height grid
+// (geo_aux -1, geo its record).
+__device__ __noinline__ bool project_mesh(const PxbDevCollider* __restrict__ c, float thickness, f3& p,
+                                          f3& normal_out, float& depth_out, f3 start, bool has_start) {
+    if (__ldg(&c->geo_aux) < 0)
+        return project_tris(c, GridTris(c->geo), thickness, p, normal_out, depth_out, start, has_start);
+    if (__ldg(&c->geo_count) == 0) return false;  // TriangleMesh::empty()
+    return project_tris(c, BvhTris{c->nodes, c->geo}, thickness, p, normal_out, depth_out, start, has_start);
 }
 
 // cloth::project_particle (cloth_collision.h:386-420). `start` is the particle's position at

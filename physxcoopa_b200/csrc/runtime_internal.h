@@ -113,8 +113,9 @@ struct GeometryEntry {
     // mesh: device copy of the hierarchy (PxbMeshNode) and triangles in its order (PxbMeshTri)
     void* dmem = nullptr;
     const float4* d_nodes = nullptr;
-    const float4* d_tris = nullptr;
+    const float4* d_tris = nullptr;  // a height grid: its record (see GridTris in pxb_device_math.cuh)
     int n_nodes = 0, depth = 0;
+    bool grid = false;               // TriangleMesh::from_height_grid
 };
 
 // The colliders of one step as the device reads them: the records plus the hulls posed for this

@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 from . import _abi as A
-from .arrays import ClothArrays, StrandArrays
+from .arrays import ClothArrays, HeightGrid, Hull, StrandArrays
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libphysxcoopa_b200.so")
 
@@ -69,6 +69,7 @@ SIGNATURES = {
     "pxb_host_cloth_pin_to_body": ([P, u32, u32, f32p, f32p, f32p, f32, C.POINTER(u32)], C.c_int),
     "pxb_geometry_create_hull": ([P, C.POINTER(A.HullDesc), C.POINTER(u32)], C.c_int),
     "pxb_geometry_create_mesh": ([P, C.POINTER(A.MeshDesc), C.POINTER(u32)], C.c_int),
+    "pxb_geometry_create_height_grid": ([P, C.POINTER(A.HeightGridDesc), C.POINTER(u32)], C.c_int),
     "pxb_geometry_destroy": ([P, u32], C.c_int),
     "pxb_host_cloth_make_grid": ([C.POINTER(A.GridClothDesc), C.POINTER(P)], C.c_int),
     "pxb_host_cloth_make_mesh": ([C.POINTER(A.MeshClothDesc), C.POINTER(P)], C.c_int),
@@ -625,6 +626,23 @@ class Context:
         out = u32()
         self._check(self.lib.pxb_geometry_create_mesh(self.h, C.byref(d), C.byref(out)), "create_mesh")
         return int(out.value)
+
+    def create_height_grid(self, grid) -> int:
+        """pxb_geometry_create_height_grid: returns the id a TriangleMesh collider over
+        TriangleMesh::from_height_grid(grid) names."""
+        d = grid.desc()
+        out = u32()
+        self._check(self.lib.pxb_geometry_create_height_grid(self.h, C.byref(d), C.byref(out)),
+                    "create_height_grid")
+        return int(out.value)
+
+    def create_geometry(self, g) -> int:
+        """Registers a Hull, a Mesh or a HeightGrid."""
+        if isinstance(g, Hull):
+            return self.create_hull(g)
+        if isinstance(g, HeightGrid):
+            return self.create_height_grid(g)
+        return self.create_mesh(g)
 
     def destroy_geometry(self, gid):
         self._check(self.lib.pxb_geometry_destroy(self.h, gid), "destroy_geometry")

@@ -443,7 +443,7 @@ def register_geometries(ctx, scene):
     """Registers scene.geometries with a runtime.Context and rewrites the colliders' geometry ids
     from the scene's numbering (geometry k is id k + 1) to the ids the context returned. Returns
     those ids."""
-    ids = [ctx.create_hull(g) if isinstance(g, Hull) else ctx.create_mesh(g) for g in scene.geometries]
+    ids = [ctx.create_geometry(g) for g in scene.geometries]
     remap = {k + 1: gid for k, gid in enumerate(ids)}
     for cols in scene.colliders:
         if cols is None:

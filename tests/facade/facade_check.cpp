@@ -4,6 +4,7 @@
 // device on another; every particle must come out equal. Exit status 0 on success.
 #include <cmath>
 #include <cstdio>
+#include <memory>
 #include <vector>
 
 #include <physxcoopa/cloth/cloth_builder.h>
@@ -128,6 +129,28 @@ int main() {
         pxb::b200::solve_cloth(dev, gmine, geo_cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 10, 1.0f / 60.0f, s2);
     }
     bad += compare("cloth 16x16 on a mesh floor and a hull, 150 frames", gref.particles, gmine.particles);
+
+    // --- the same sheet onto a heightfield terrain (TriangleMesh::from_height_grid) ---
+    std::vector<float> hts(30 * 26);
+    for (int j = 0; j < 26; ++j)
+        for (int i = 0; i < 30; ++i)
+            hts[j * 30 + i] = 0.08f * std::sin(0.4f * static_cast<float>(i)) * std::cos(0.3f * static_cast<float>(j));
+    const px::geometry::TriangleMesh terrain = px::geometry::TriangleMesh::from_height_grid(
+        std::make_shared<const px::geometry::HeightGrid>(30, 26, glm::vec2(0.07f, 0.07f), hts));
+    px::collision::Shape terrain_shape = px::collision::Shape::make_mesh(&terrain);
+    terrain_shape.enabled = true;
+    px::cloth::ClothCollider tc;
+    tc.shape = &terrain_shape;
+    tc.position = glm::vec3(-1.0f, -0.9f, 0.0f);
+    tc.bounds = px::collision::world_bounds(terrain_shape, tc.position, tc.orientation);
+    const std::vector<px::cloth::ClothCollider> terrain_cols = {tc};
+    px::cloth::Cloth tref = px::cloth::make_grid_cloth(g2);
+    px::cloth::Cloth tmine = tref;
+    for (int i = 0; i < 150; ++i) {
+        px::cloth::solve_cloth(tref, terrain_cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 10, 1.0f / 60.0f, s1);
+        pxb::b200::solve_cloth(dev, tmine, terrain_cols, glm::vec3(0.0f, 0.0f, -9.81f), 4, 10, 1.0f / 60.0f, s2);
+    }
+    bad += compare("cloth 16x16 on a height-grid terrain, 150 frames", tref.particles, tmine.particles);
 
     // --- a cloth of no grid structure: the 24x24 sheet's lists shuffled and each walked as one
     //     serial batch, its triangles wound the other way, columns cleared (no 1-ring exemption),

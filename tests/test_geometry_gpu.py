@@ -31,7 +31,7 @@ def ctx():
 
 
 def register(ctx, geometry):
-    gid = ctx.create_hull(geometry) if isinstance(geometry, Hull) else ctx.create_mesh(geometry)
+    gid = ctx.create_geometry(geometry)
     K.register_geometry(gid, geometry)
     return gid
 
@@ -65,6 +65,9 @@ GEOMETRIES = {
     "corner": S.corner_mesh,
     "terrain": lambda: S.terrain_mesh(20, 2.0, 0.2, seed=3),
     "terrain_computed_normals": lambda: S.terrain_mesh(9, 2.0, 0.3, seed=4),
+    # TriangleMesh::from_height_grid: one 64-cell block; several, with ragged 8-cell blocks
+    "height_grid": lambda: S.height_grid_terrain(20, 17, 0.1, 0.15, seed=2),
+    "height_grid_blocks": lambda: S.height_grid_terrain(140, 75, 0.02, 0.05, seed=3),
 }
 
 
@@ -268,3 +271,20 @@ def test_geometry_refusals_and_lifetime(ctx):
     assert e.value.status == A.PXB_ERR_INVALID_ARGUMENT
     empty = ctx.create_mesh(Mesh(np.zeros((0, 3)), np.zeros(0)))  # accepted; never collides
     ctx.destroy_geometry(empty)
+
+
+def test_height_grid_drape_equals_oracle_1_and_300_steps(ctx):
+    """A cloth settling on TriangleMesh::from_height_grid: the device walks the grid's block
+    pyramid in the reference's order (height_grid.h), so every step equals the oracle."""
+    sc = S.height_grid_drape(side=24)
+    gids = _scene_with_oracle(ctx, sc)
+    try:
+        gpu, orc = run_scene(ctx, sc, 1)
+        assert_equal_particles(gpu[0], orc[0].particles, "step 1")
+        gpu, orc = run_scene(ctx, sc, 300)
+        assert maxdiff(gpu[0]["position"], orc[0].particles["position"]) <= 1e-3
+        assert_equal_particles(gpu[0], orc[0].particles, "step 300")
+        assert gpu[0]["position"][:, 2].min() > -0.2
+    finally:
+        for g in gids:
+            ctx.destroy_geometry(g)

@@ -489,14 +489,24 @@ __device__ __forceinline__ bool project_tris(const PxbDevCollider* __restrict__ 
     return true;
 }
 
+// The two walks are separate calls so that each is register-allocated on its own.
+__device__ __noinline__ bool project_grid_mesh(const PxbDevCollider* __restrict__ c, float thickness, f3& p,
+                                               f3& normal_out, float& depth_out, f3 start, bool has_start) {
+    return project_tris(c, GridTris(c->geo), thickness, p, normal_out, depth_out, start, has_start);
+}
+
+__device__ __noinline__ bool project_bvh_mesh(const PxbDevCollider* __restrict__ c, float thickness, f3& p,
+                                              f3& normal_out, float& depth_out, f3 start, bool has_start) {
+    return project_tris(c, BvhTris{c->nodes, c->geo}, thickness, p, normal_out, depth_out, start, has_start);
+}
+
 // A mesh collider: a stored mesh (geo_count hierarchy nodes, 0 when empty) or a height grid
 // (geo_aux -1, geo its record).
-__device__ __noinline__ bool project_mesh(const PxbDevCollider* __restrict__ c, float thickness, f3& p,
-                                          f3& normal_out, float& depth_out, f3 start, bool has_start) {
-    if (__ldg(&c->geo_aux) < 0)
-        return project_tris(c, GridTris(c->geo), thickness, p, normal_out, depth_out, start, has_start);
+__device__ __forceinline__ bool project_mesh(const PxbDevCollider* __restrict__ c, float thickness, f3& p,
+                                             f3& normal_out, float& depth_out, f3 start, bool has_start) {
+    if (__ldg(&c->geo_aux) < 0) return project_grid_mesh(c, thickness, p, normal_out, depth_out, start, has_start);
     if (__ldg(&c->geo_count) == 0) return false;  // TriangleMesh::empty()
-    return project_tris(c, BvhTris{c->nodes, c->geo}, thickness, p, normal_out, depth_out, start, has_start);
+    return project_bvh_mesh(c, thickness, p, normal_out, depth_out, start, has_start);
 }
 
 // cloth::project_particle (cloth_collision.h:386-420). `start` is the particle's position at

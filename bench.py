@@ -4,7 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
                     [--workload uniform_batch|single_drape|uneven_batch|warm_start|hair_groom|
                                 large_cloth_hair|mesh_floor|mesh_cloth] [--cloths C]
-                    [--floor mesh|box|none]
+                    [--floor mesh|height_grid|box|none]
                     [--self-collision]
 
 One step = one PhysicsWorld cloth frame for every cloth of the workload: a single batched
@@ -74,8 +74,9 @@ def parse():
     ap.add_argument("--cloths", type=int, default=None)
     ap.add_argument("--self-collision", action="store_true",
                     help="turn ClothParams::self_collision on for every cloth of the workload")
-    ap.add_argument("--floor", choices=["mesh", "box", "none"], default="mesh",
-                    help="mesh_floor workload: the floor collider (box / none measure the mesh query's share)")
+    ap.add_argument("--floor", choices=["mesh", "height_grid", "box", "none"], default="mesh",
+                    help="mesh_floor workload: the floor collider (height_grid: the same samples as "
+                         "TriangleMesh::from_height_grid; box / none measure the mesh query's share)")
     ap.add_argument("--side", type=int, default=64, help="sheet side of the uniform batch")
     ap.add_argument("--rings", type=int, default=20,
                     help="mesh_cloth workload: rings of the disc mesh (1 + 3 rings (rings + 1) particles)")
@@ -106,7 +107,15 @@ def _build_scene(args, rank):
         return scenes.uniform_batch(n=args.cloths or 1024, side=args.side, seed=1 + rank)
     if args.workload == "mesh_floor":
         sc = scenes.mesh_floor_batch(n=args.cloths or 4096, side=25, seed=12 + rank)
-        if args.floor != "mesh":  # the same sheets on an analytic box floor, or on nothing
+        if args.floor == "height_grid":  # the floor's 33 x 33 samples as a height grid
+            from physxcoopa_b200.arrays import HeightGrid, collider_array, mesh_collider
+            mesh = sc.geometries[0]
+            grid = HeightGrid(33, 33, (0.125, 0.125), np.ascontiguousarray(mesh.vertices[:, 2], np.float32))
+            floor = collider_array([mesh_collider(1, grid, local_center=(-2.0, -2.0, 0.0))])
+            sc.colliders = [floor.copy() for _ in sc.cloths]
+            sc.geometries = [grid]
+            sc.name += " (height-grid floor)"
+        elif args.floor != "mesh":  # the same sheets on an analytic box floor, or on nothing
             from physxcoopa_b200.arrays import box, collider_array
             floor = collider_array([box((2.0, 2.0, 0.02), (0.0, 0.0, -0.02))]) if args.floor == "box" \
                 else collider_array([])

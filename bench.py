@@ -106,16 +106,9 @@ def _build_scene(args, rank):
     if args.workload == "uniform_batch":
         return scenes.uniform_batch(n=args.cloths or 1024, side=args.side, seed=1 + rank)
     if args.workload == "mesh_floor":
-        sc = scenes.mesh_floor_batch(n=args.cloths or 4096, side=25, seed=12 + rank)
-        if args.floor == "height_grid":  # the floor's 33 x 33 samples as a height grid
-            from physxcoopa_b200.arrays import HeightGrid, collider_array, mesh_collider
-            mesh = sc.geometries[0]
-            grid = HeightGrid(33, 33, (0.125, 0.125), np.ascontiguousarray(mesh.vertices[:, 2], np.float32))
-            floor = collider_array([mesh_collider(1, grid, local_center=(-2.0, -2.0, 0.0))])
-            sc.colliders = [floor.copy() for _ in sc.cloths]
-            sc.geometries = [grid]
-            sc.name += " (height-grid floor)"
-        elif args.floor != "mesh":  # the same sheets on an analytic box floor, or on nothing
+        sc = scenes.mesh_floor_batch(n=args.cloths or 4096, side=25, seed=12 + rank,
+                                     height_grid=args.floor == "height_grid")
+        if args.floor in ("box", "none"):  # the same sheets on an analytic box floor, or on nothing
             from physxcoopa_b200.arrays import box, collider_array
             floor = collider_array([box((2.0, 2.0, 0.02), (0.0, 0.0, -0.02))]) if args.floor == "box" \
                 else collider_array([])

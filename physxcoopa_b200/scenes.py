@@ -342,22 +342,28 @@ def terrain_drape(side=32, seed=11, params=None):
                       geometries=[terrain, rock])
 
 
-def mesh_floor_batch(n=4096, side=25, seed=12):
+def mesh_floor_batch(n=4096, side=25, seed=12, height_grid=False, params=None):
     """N sheets of side x side (default 4096 x 25^2) resting on one 2048-triangle mesh floor: the
     reference's own costing case for mesh colliders (a 25x25 sheet on a 2048-triangle floor,
     cloth/README.md:98-102), batched. The floor is a 4 x 4 m height field of 32 x 32 cells with
     3 cm seeded bumps; each sheet is placed 6 cm above it at a seeded position, unpinned, with the
-    floor as its one collider (geometry id 1)."""
+    floor as its one collider (geometry id 1). height_grid: the floor's 33 x 33 samples as a
+    HeightGrid instead (TriangleMesh::from_height_grid), the same surface samples."""
     rng = np.random.default_rng(seed)
     floor = terrain_mesh(32, 4.0, 0.03, seed)
-    col = collider_array([mesh_collider(1, floor)])
+    if height_grid:
+        floor = HeightGrid(33, 33, (0.125, 0.125), np.ascontiguousarray(floor.vertices[:, 2], np.float32))
+        col = collider_array([mesh_collider(1, floor, local_center=(-2.0, -2.0, 0.0))])
+    else:
+        col = collider_array([mesh_collider(1, floor)])
     half = (side - 1) * SPACING * 0.5
     cloths, cols = [], []
     for k in range(n):
         cx, cy = (float(v) for v in rng.uniform(-2.0 + half, 2.0 - half, 2))
-        cloths.append(_sheet(side, (cx, cy, 0.06), seed * 100003 + k, [], tethers=False))
+        cloths.append(_sheet(side, (cx, cy, 0.06), seed * 100003 + k, [], params=params, tethers=False))
         cols.append(col.copy())
-    return ClothScene(f"mesh_floor_batch {n}x{side}^2", cloths, cols, meta={"side": side, "n": n},
+    name = f"mesh_floor_batch {n}x{side}^2" + (" (height-grid floor)" if height_grid else "")
+    return ClothScene(name, cloths, cols, meta={"side": side, "n": n},
                       geometries=[floor])
 
 

@@ -300,3 +300,21 @@ def test_cloth_on_height_grid_matches_reference_bitwise():
                 assert same(orc.particles[f], got.particles[f]), (step, f)
     # it came to rest on the terrain
     assert ref.arrays().particles["position"][:, 2].min() > -0.2
+
+
+def test_height_grid_floor_batch_matches_reference_bitwise():
+    """The benchmark's height-grid floor (the 2048-triangle floor's 33 x 33 samples through
+    TriangleMesh::from_height_grid) with sheets resting on it, under the reference's default
+    parameters (no shear-compliance extension)."""
+    sc = S.mesh_floor_batch(n=2, side=25, height_grid=True, params=A.ClothParams.defaults())
+    _register(sc)
+    for cloth, cols in zip(sc.cloths, sc.colliders):
+        ref = K.RefCloth.from_arrays(cloth)
+        orc = cloth.copy()
+        for _ in range(20):
+            ref.solve(cols, substeps=4, iterations=10)
+            K.oracle_step_cloth(orc, cols, substeps=4, iterations=10)
+        got = ref.arrays()
+        for f in ("position", "prev_position", "velocity"):
+            assert same(orc.particles[f], got.particles[f]), f
+        assert got.particles["position"][:, 2].min() > -0.03

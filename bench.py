@@ -1,47 +1,50 @@
 #!/usr/bin/env python
-"""Cloth XPBD benchmark: cloth vertex-substeps/s on B200.
+"""Cloth XPBD benchmark: cloth vertex-substeps/s on B200, plain XPBD and the learned warm start.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
-                    [--workload uniform_batch|single_drape|uneven_batch|warm_start|hair_groom|
+                    [--workload uneven_batch|uniform_batch|single_drape|warm_start|hair_groom|
                                 large_cloth_hair|mesh_floor|mesh_cloth] [--cloths C]
-                    [--floor mesh|height_grid|box|none]
+                    [--no-warm] [--shear-compliance X] [--floor mesh|height_grid|box|none]
                     [--self-collision]
 
-One step = one PhysicsWorld cloth frame for every cloth of the workload: a single batched
-launch of the device solver (pxb_cloths_step) advancing each cloth by solve_cloth(h = 1/60,
-4 substeps, 10 iterations). Default workload: the uniform batch, 1024 sheets of 64x64, seeded
-synthetic scenes (physxcoopa_b200/scenes.py). Vertex-substeps = sum of particles x substeps x
-steps.
+Default workload: the uneven batch, 4096 sheets with sides drawn U{16..128}, 1-3 sphere / capsule /
+oriented-box colliders each, half of them under a point gravity source, 4 substeps x 10 iterations,
+seeded synthetic scenes (physxcoopa_b200/scenes.py; no dataset exists for this path). One step =
+one PhysicsWorld cloth frame for every cloth: solve_cloth(h = 1/60) on each, batched in one
+pxb_cloths_step call. Vertex-substeps = sum of particles x substeps x steps.
+
+Compliances: structural and shear constraints at the one stretch compliance the reference's
+ClothParams holds (0), bend 1e-4, in both arms; --shear-compliance X gives the shear constraints
+their own compliance through the library's per-batch extension (no reference counterpart).
 
   value    device-resident throughput: inputs in HBM, K steps timed with CUDA events on the
-           library's own stream, max over ranks (weak scaling: each rank runs the full batch).
-  e2e      the same steps through the public C-ABI as an engine frame uses it: per step the
-           step inputs (per-cloth step records, colliders) go host->device from pinned memory
-           and every cloth's particle positions plus per-cloth bounds/speed come back to
-           pinned host memory.
+           library's stream, max over ranks.
+  e2e      the same steps through the public C-ABI as an engine frame uses it: per step the step
+           inputs (per-cloth step records, colliders, sources) go host->device from pinned memory,
+           every particle position and the per-cloth bounds / speed come back to pinned host
+           memory (pipelined one frame, as a renderer consumes them).
+  warm_start  the learned warm start on the same batch: a network trained on rows recorded from
+           the plain 20-iteration solver on a separately seeded batch (the library's own kernels,
+           Adam lr 1e-3), then the batch stepped with 20 plain iterations and with the network plus
+           4 iterations; where a warm substep's residual (max |len / rest - 1| over the stretch
+           constraints) exceeds that cloth's largest residual under the plain solver over the same
+           steps, it keeps iterating (4 at a time, at most 20): equal residual, cloth by cloth.
   roofline shared-memory bound (the cloth lives in shared memory during a step): algorithmic
-           bytes per launch = sum over cloths of (iterations x constraints x 68 B + particles x
-           150 B) x substeps, over the measured per-launch duration, against the device's
+           bytes per step = sum over cloths of (iterations x constraints x 68 B + particles x
+           150 B) x substeps, over the measured per-step duration, against the device's
            shared-memory bandwidth measured on the spot by pxb_measure_smem_bandwidth.
   cpu_baseline  the reference's own solve_cloth (oracle/_ref, compiled from the reference's
-           headers) on a bounded sample of the workload on the host's cores, whole cloths per
-           thread as the reference's serial dispatch solves them.
+           headers, cloths built by the reference's own make_grid_cloth / pin_static /
+           build_tethers) on a bounded sample of the workload on this host: 1 thread and all
+           threads, at -O2 and at -O3 -march=native.
 
---workload warm_start is the learned warm start on the uneven batch: training rows recorded from
-the plain 20-iteration solver on a separately seeded batch, the network trained (Adam, lr 1e-3),
-then the same benchmark state stepped with 20 plain iterations and with the network plus 4
-iterations; where a substep's residual (max |len / rest - 1| over the stretch constraints) still
-exceeds that cloth's largest residual under the plain solver over the same steps, it keeps
-iterating (4 at a time, residual checked after each block, at most 20 in all): equal residual,
-cloth by cloth. The restart fallback (back to the prediction, 20 plain iterations) is reported
-beside it. `value` is the warm-start
-throughput, `plain` the plain one.
+--impl reference runs only that CPU implementation (rank 0; other ranks exit 0), on this arm's
+config, with all host threads; it maps no library of this package.
 
---workload mesh_cloth is the general-topology path: 1024 cloths built from a triangulated disc
-(1261 particles each, no grid structure; pxb_host_cloth_make_mesh), each pinned at two rim points
-and draped over a sphere.
-
---impl reference runs only that CPU implementation (rank 0; other ranks exit 0).
+Several GPUs (torchrun): the batch grows with the ranks (4096 sheets per GPU, weak scaling), is
+split over them by cost (physxcoopa_b200/shard.py, largest first onto the least-loaded rank), each
+rank steps its share with no collective, and the e2e frames gather every cloth's bounds and speed
+to every rank with one all-gather.
 """
 import argparse
 import json
@@ -60,6 +63,7 @@ sys.path.insert(0, ROOT)
 SPEC = "cloth vertex-substeps/s on 1 B200: plain XPBD vs NN warm-start at equal residual"
 METRIC = SPEC
 UNIT = "vertex-substeps/s"
+PLAN_WORKLOADS = ("uneven_batch", "uniform_batch", "single_drape")
 
 
 def parse():
@@ -68,10 +72,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
-    ap.add_argument("--workload", default="uniform_batch",
-                    choices=["uniform_batch", "single_drape", "uneven_batch", "warm_start", "hair_groom",
+    ap.add_argument("--workload", default="uneven_batch",
+                    choices=["uneven_batch", "uniform_batch", "single_drape", "warm_start", "hair_groom",
                              "large_cloth_hair", "mesh_floor", "mesh_cloth"])
     ap.add_argument("--cloths", type=int, default=None)
+    ap.add_argument("--no-warm", action="store_true",
+                    help="uneven batch: leave out the warm-start comparison")
+    ap.add_argument("--shear-compliance", type=float, default=None,
+                    help="give the shear constraints their own compliance (library extension; the "
+                         "reference arm cannot run it)")
     ap.add_argument("--self-collision", action="store_true",
                     help="turn ClothParams::self_collision on for every cloth of the workload")
     ap.add_argument("--floor", choices=["mesh", "height_grid", "box", "none"], default="mesh",
@@ -82,6 +91,8 @@ def parse():
                     help="mesh_cloth workload: rings of the disc mesh (1 + 3 rings (rings + 1) particles)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=3.0,
+                    help="wall seconds of reference CPU work per timed sample")
     ap.add_argument("--graph", action="store_true",
                     help="step through the captured CUDA graph (pxb_cloths_step_graph) instead of pxb_cloths_step")
     ap.add_argument("--variant", type=int, default=None,
@@ -89,22 +100,69 @@ def parse():
     return ap.parse_args()
 
 
-def build_scene(args, rank):
-    sc = _build_scene(args, rank)
-    if getattr(args, "self_collision", False):
-        # ClothParams::self_collision on every cloth, at the builder's self_distance (0.6 x spacing)
-        for c in sc.cloths:
-            c.params.self_collision = 1
-        sc.name += " (self-collision)"
-    return sc
+# ------------------------------------------------------------------------------------------
+# workloads
+# ------------------------------------------------------------------------------------------
 
-
-def _build_scene(args, rank):
+def sheet_params(args):
     from physxcoopa_b200 import scenes
-    if args.workload == "single_drape":
-        return scenes.single_drape(seed=rank)
+    p = (scenes.reference_params() if args.shear_compliance is None
+         else scenes.cloth_params(shear_compliance=args.shear_compliance))
+    if args.self_collision:  # at the builder's self_distance (0.6 x spacing)
+        p.self_collision = 1
+    return p
+
+
+def total_cloths(args, world):
+    """Sheets of the whole job: the configuration's batch per GPU (weak scaling)."""
+    default = {"uneven_batch": 4096, "uniform_batch": 1024, "single_drape": 1}[args.workload]
+    return (args.cloths or default) * world
+
+
+def plan(args, world):
+    """(name, specs) of a plan workload: every sheet's draws, before any builder runs."""
+    from physxcoopa_b200 import scenes
+    n = total_cloths(args, world)
+    if args.workload == "uneven_batch":
+        return scenes.uneven_name(n), scenes.uneven_plan(n, seed=2)
     if args.workload == "uniform_batch":
-        return scenes.uniform_batch(n=args.cloths or 1024, side=args.side, seed=1 + rank)
+        return scenes.uniform_name(n, args.side), scenes.uniform_plan(n, args.side, seed=1)
+    return scenes.single_drape_name(), scenes.single_drape_plan(seed=0)
+
+
+def workload_config(args, name, n_cloths, vertices, substeps=4, iterations=10, h=1.0 / 60.0, n_gpus=1):
+    """The `config` of the JSON line: identical in both arms for the same arguments."""
+    cfg = {"workload": name, "cloths": n_cloths, "vertices": vertices, "substeps": substeps,
+           "iterations": iterations, "h": h,
+           "compliance": ("structural and shear 0 (ClothParams::stretch_compliance, the reference's one "
+                          "stretch compliance), bend 1e-4" if args.shear_compliance is None else
+                          f"structural 0 / shear {args.shear_compliance:g} / bend 1e-4 (per-batch compliance)"),
+           "l2": "inputs larger than L2 (device state of the batch exceeds 126 MB)"
+           if vertices * 64 > 126e6 else "inputs fit in L2",
+           "parallelism": f"independent cloths, {n_gpus} GPU(s), cost-balanced shares"}
+    if args.workload == "uneven_batch":
+        cfg["colliders"] = ("1-3 per sheet from sphere r U(0.2,0.5) / capsule r U(0.1,0.3) half-length "
+                            "U(0.2,0.6) / box half-extents U(0.1,0.5), random orientations; half the "
+                            "sheets under one point source (9.81, 1 m, 10 m)")
+    if args.self_collision:
+        cfg["self_collision"] = "on, self_distance 0.6 x spacing"
+    return cfg
+
+
+def build_gpu_scene(args, rank, world):
+    """The scene this rank steps. Plan workloads: this rank's cost-balanced share of the job's
+    sheets (all of them on one GPU), built by the library's builders."""
+    from physxcoopa_b200 import scenes, shard
+    if args.workload in PLAN_WORKLOADS:
+        name, specs = plan(args, world)
+        costs = [shard.cloth_cost(s.side * s.side) for s in specs]
+        shares = shard.partition(costs, world)
+        mine = shares[rank]
+        params = sheet_params(args)
+        cloths = [scenes.build_sheet(specs[i], params) for i in mine]
+        sc = scenes.ClothScene(name, cloths, [specs[i].colliders for i in mine],
+                               sources=[specs[i].source for i in mine])
+        return sc, shares, sum(s.side * s.side for s in specs), len(specs)
     if args.workload == "mesh_floor":
         sc = scenes.mesh_floor_batch(n=args.cloths or 4096, side=25, seed=12 + rank,
                                      height_grid=args.floor == "height_grid")
@@ -115,18 +173,12 @@ def _build_scene(args, rank):
             sc.colliders = [floor.copy() for _ in sc.cloths]
             sc.geometries = []
             sc.name += f" ({args.floor} floor)"
-        return sc
-    if args.workload == "mesh_cloth":
-        return scenes.mesh_cloth_batch(n=args.cloths or 1024, rings=args.rings, seed=13 + rank)
-    return scenes.uneven_batch(n=args.cloths or 4096, seed=2 + rank)
-
-
-def workload_config(args, sc):
-    return {"workload": sc.name, "cloths": len(sc.cloths), "vertices": sc.vertices,
-            "substeps": sc.substeps, "iterations": sc.iterations, "h": sc.h,
-            "compliance": "structural 0 / shear 1e-6 / bend 1e-4",
-            "l2": "inputs larger than L2 (device state of the batch exceeds 126 MB)"
-            if sc.vertices * 64 > 126e6 else "inputs fit in L2"}
+    else:  # mesh_cloth
+        sc = scenes.mesh_cloth_batch(n=args.cloths or 1024, rings=args.rings, seed=13 + rank)
+    if args.self_collision:
+        for c in sc.cloths:
+            c.params.self_collision = 1
+    return sc, None, sc.vertices * world, len(sc.cloths) * world
 
 
 # ------------------------------------------------------------------------------------------
@@ -184,71 +236,195 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------
-# reference CPU implementation (oracle/_ref) on the host cores
+# the reference CPU implementation (oracle/_ref) on the host cores
 # ------------------------------------------------------------------------------------------
 
-def reference_cpu(sc, seconds_target=12.0, threads=None):
-    """Times the reference's solve_cloth on a bounded sample of the workload. Returns a dict."""
+CPU_BUILDS = {"O2": ("libpxbref.so", "-O2"), "native": ("libpxbref_native.so", "-O3 -march=native")}
+
+
+def _ref_handles(lib, specs, params):
+    """The sheets built by the reference's own builders: make_grid_cloth (with the seeded jitter),
+    pin_static at each pin, build_tethers when pinned."""
+    import ctypes as C
+    from physxcoopa_b200 import scenes
+    hs = []
+    for s in specs:
+        d = scenes.grid_desc(s.side, s.center, s.seed, params)
+        h = lib.pxbref_cloth_make_grid(C.byref(d))
+        for point, radius in s.pins:
+            lib.pxbref_cloth_pin_static(h, (C.c_float * 3)(*point), radius)
+        if s.pins:
+            lib.pxbref_cloth_build_tethers(h)
+        hs.append(h)
+    return hs
+
+
+def _ref_cpu_child(q, build, plan_args, params_blob, threads, steps, warmup, target_s):
+    """Runs in a spawned process (a reference build that does not run on this CPU, or any crash,
+    ends only this process). Builds a sample of the plan's sheets with the reference's builders,
+    sized so one step over it takes about target_s on `threads` threads, then steps it warmup +
+    steps times with pxbref_bench_cloths (the reference's solve_cloth per cloth, whole cloths per
+    thread). Puts (rates per timed step, sample size, threads) on q."""
     import ctypes as C
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import _checkers as K
     from physxcoopa_b200 import _abi as A
-    threads = threads or os.cpu_count() or 1
-    kind = "reference" if K.ref_available() else "port"
-    n_total = len(sc.cloths)
+    args = argparse.Namespace(**plan_args)
+    _, specs = plan(args, 1)
+    params = A.ClothParams.from_buffer_copy(params_blob)
+    lib = K.load_ref(os.path.join(ROOT, "oracle", "_ref", CPU_BUILDS[build][0]))
+    g = K.vec((0.0, 0.0, -9.81))
 
-    # collider geometry under the ids the scene's colliders name
-    gids = getattr(sc, "geometries_ids", None) or [k + 1 for k in range(len(sc.geometries))]
-    for gid, g in zip(gids, sc.geometries):
-        K.register_geometry(gid, g)
+    def run(handles, idx, n_steps, nthreads):
+        cols = [specs[i].colliders for i in idx]
+        flat = np.ascontiguousarray(np.concatenate(cols))
+        offs = np.zeros(len(idx) + 1, np.uint32)
+        offs[1:] = np.cumsum([len(c) for c in cols])
+        srcs = [specs[i].source if specs[i].source is not None else np.zeros(0, A.GRAVITY_SOURCE) for i in idx]
+        sflat = np.ascontiguousarray(np.concatenate(srcs)) if srcs else np.zeros(0, A.GRAVITY_SOURCE)
+        soffs = np.zeros(len(idx) + 1, np.uint32)
+        soffs[1:] = np.cumsum([len(x) for x in srcs])
+        hv = (C.c_void_p * len(handles))(*handles)
+        return lib.pxbref_bench_cloths(hv, len(handles), A.ptr(flat), A.ptr(offs), A.ptr(sflat), A.ptr(soffs),
+                                       g, 4, 10, 1.0 / 60.0, n_steps, nthreads)
 
-    def timed(sample, steps, nthreads):
-        if kind == "reference":
-            refs = [K.RefCloth.from_arrays(sc.cloths[i]) for i in sample]
-            cols = [sc.colliders[i] for i in sample]
-            flat = np.ascontiguousarray(np.concatenate(cols)) if cols else np.zeros(0, A.COLLIDER)
-            offs = np.zeros(len(sample) + 1, np.uint32)
-            offs[1:] = np.cumsum([len(c) for c in cols])
-            srcs = [sc.sources[i] if sc.sources and sc.sources[i] is not None
-                    else np.zeros(0, A.GRAVITY_SOURCE) for i in sample]
-            sflat = np.ascontiguousarray(np.concatenate(srcs)) if srcs else np.zeros(0, A.GRAVITY_SOURCE)
-            soffs = np.zeros(len(sample) + 1, np.uint32)
-            soffs[1:] = np.cumsum([len(x) for x in srcs])
-            handles = (C.c_void_p * len(refs))(*[r.h for r in refs])
-            return K.ref().pxbref_bench_cloths(handles, len(refs), A.ptr(flat), A.ptr(offs),
-                                               A.ptr(sflat), A.ptr(soffs), K.vec(sc.gravity),
-                                               sc.substeps, sc.iterations, sc.h, steps, nthreads)
-        # the C restatement, single-threaded
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            for i in sample:
-                c = sc.cloths[i].copy()
-                K.oracle_step_cloth(c, sc.colliders[i], sources=sc.sources[i] if sc.sources else None,
-                                    substeps=sc.substeps, iterations=sc.iterations, h=sc.h)
-        return time.perf_counter() - t0
+    # calibrate on the plan's first sheets, one thread
+    probe_idx = list(range(min(8, len(specs))))
+    probe = _ref_handles(lib, [specs[i] for i in probe_idx], params)
+    wall = run(probe, probe_idx, 1, 1)
+    per_vertex = wall / max(1, sum(specs[i].side ** 2 for i in probe_idx))
+    for h in probe:
+        lib.pxbref_cloth_free(h)
+    budget = target_s * threads / max(per_vertex, 1e-12)
+    n, acc = 0, 0
+    while n < len(specs) and (acc < budget or n < threads):
+        acc += specs[n].side ** 2
+        n += 1
+    idx = list(range(n))
+    handles = _ref_handles(lib, [specs[i] for i in idx], params)
+    verts = sum(specs[i].side ** 2 for i in idx) * 4
+    for _ in range(warmup):
+        run(handles, idx, 1, threads)
+    rates = [verts / run(handles, idx, 1, threads) for _ in range(steps)]
+    for h in handles:
+        lib.pxbref_cloth_free(h)
+    q.put({"rates": rates, "n_sample": n, "threads": threads})
 
-    # calibrate on one cloth, one step, one thread
-    probe = timed([0], 1, 1)
-    per_cloth = max(probe, 1e-4)
-    nthreads = threads if kind == "reference" else 1
-    n_sample = int(min(n_total, max(nthreads, seconds_target * nthreads / per_cloth)))
-    n_sample = max(1, (n_sample // nthreads) * nthreads) if n_sample >= nthreads else n_sample
-    sample = list(range(n_sample))
-    wall = timed(sample, 1, nthreads)
-    steps = 1
-    if wall < 0.5 * seconds_target and n_sample == n_total:
-        steps = max(1, int(seconds_target / max(wall, 1e-3)))
-        wall = timed(sample, steps, nthreads)
-    verts = sum(len(sc.cloths[i].particles) for i in sample) * sc.substeps * steps
-    return {"value": verts / wall, "unit": UNIT, "cores": nthreads, "kind": kind,
-            "sample": f"{n_sample} of {n_total} cloths of the workload, {steps} step(s) each, "
-                      f"{nthreads} host threads, {wall:.1f} s (reference solve_cloth -O2; the "
-                      f"reference has one stretch compliance, so shear runs at the structural one)"
-            if kind == "reference" else f"{n_sample} cloths, oracle port, 1 thread, {wall:.1f} s"}
+
+def ref_cpu(args, build, threads, steps, warmup, target_s):
+    """One CPU mode of the reference (build x threads) in a spawned process. Returns the child's
+    dict, or {"unavailable": why}."""
+    import multiprocessing as mp
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", CPU_BUILDS[build][0])):
+        return {"unavailable": f"oracle/_ref/{CPU_BUILDS[build][0]} was not built"}
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    plan_args = {"workload": args.workload, "cloths": args.cloths, "side": args.side}
+    p = ctx.Process(target=_ref_cpu_child, args=(q, build, plan_args, bytes(sheet_params(args)), threads, steps,
+                                                 warmup, target_s))
+    p.start()
+    res = None
+    deadline = time.time() + 600
+    while time.time() < deadline:
+        try:
+            res = q.get(timeout=1.0)
+            break
+        except Exception:  # queue.Empty
+            if not p.is_alive():
+                break
+    p.join(timeout=30)
+    if res is None:
+        return {"unavailable": f"the {CPU_BUILDS[build][1]} build did not run here (exit code {p.exitcode})"}
+    return res
+
+
+def cpu_modes(args, steps=1, warmup=0, target_s=None):
+    """The reference on this host: 1 thread and all threads, each at -O2 and -O3 -march=native."""
+    target_s = target_s or args.cpu_seconds
+    n_all = os.cpu_count() or 1
+    modes = {}
+    for build in ("O2", "native"):
+        for threads in (1, n_all):
+            r = ref_cpu(args, build, threads, steps, warmup, target_s)
+            key = f"{build}_{threads}thread" if threads == 1 else f"{build}_{threads}threads"
+            if "unavailable" in r:
+                modes[key] = r
+            else:
+                modes[key] = {"value": statistics.median(r["rates"]), "flags": CPU_BUILDS[build][1],
+                              "threads": threads, "sample_cloths": r["n_sample"], "timed_steps": len(r["rates"])}
+    return modes
+
+
+def cpu_baseline_from_modes(modes, n_total):
+    """The all-threads mode of the faster build is the baseline; every mode is listed."""
+    best = None
+    for k, m in modes.items():
+        if "value" in m and m["threads"] > 1 and (best is None or m["value"] > modes[best]["value"]):
+            best = k
+    if best is None:
+        return None
+    m = modes[best]
+    return {"value": m["value"], "unit": UNIT, "cores": m["threads"], "kind": "reference",
+            "sample": f"first {m['sample_cloths']} of {n_total} sheets of the workload, built by the reference's "
+                      f"make_grid_cloth / pin_static / build_tethers, stepped by its solve_cloth (serial per cloth, "
+                      f"whole cloths over {m['threads']} host threads), {m['flags']}; median of {m['timed_steps']} "
+                      f"step(s)",
+            "modes": modes}
+
+
+def reference_arm(args):
+    """--impl reference: the reference's solve_cloth on the host cores, on this arm's config."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.workload not in PLAN_WORKLOADS:
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference arm runs the sheet workloads "
+                                                              f"{', '.join(PLAN_WORKLOADS)}"}))
+        return 0
+    if args.shear_compliance is not None:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's ClothParams has one stretch "
+                                                              "compliance; a separate shear compliance is a "
+                                                              "library extension"}))
+        return 0
+    name, specs = plan(args, world)
+    n_all = os.cpu_count() or 1
+    W = max(args.warmup, 0)
+    target = min(args.cpu_seconds, 180.0 / max(1, args.steps + W))
+    per_build = {}
+    for build in ("O2", "native"):
+        per_build[build] = ref_cpu(args, build, n_all, args.steps, W, target)
+    ok = {b: r for b, r in per_build.items() if "rates" in r}
+    if not ok:
+        print(json.dumps({"impl": "reference", "unavailable": "; ".join(r["unavailable"] for r in per_build.values())}))
+        return 0
+    best = max(ok, key=lambda b: statistics.median(ok[b]["rates"]))
+    value = statistics.median(ok[best]["rates"])
+    modes = {}
+    for b, r in per_build.items():
+        modes[f"{b}_{n_all}threads"] = ({"value": statistics.median(r["rates"]), "flags": CPU_BUILDS[b][1],
+                                         "threads": n_all, "sample_cloths": r["n_sample"],
+                                         "timed_steps": len(r["rates"])} if "rates" in r else r)
+    for b in ("O2", "native"):  # one-thread figures beside them (two samples each)
+        r = ref_cpu(args, b, 1, 2, 0, 2.0)
+        modes[f"{b}_1thread"] = ({"value": statistics.median(r["rates"]), "flags": CPU_BUILDS[b][1], "threads": 1,
+                                  "sample_cloths": r["n_sample"], "timed_steps": len(r["rates"])}
+                                 if "rates" in r else r)
+    cb = {"value": value, "unit": UNIT, "cores": n_all, "kind": "reference",
+          "sample": f"first {ok[best]['n_sample']} of {len(specs)} sheets per step, built by the reference's "
+                    f"make_grid_cloth / pin_static / build_tethers and stepped by its solve_cloth (serial per cloth, "
+                    f"whole cloths over {n_all} host threads), {CPU_BUILDS[best][1]} (the faster build)",
+          "modes": modes}
+    vertices = sum(s.side * s.side for s in specs)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": W, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scenes)",
+            "config": workload_config(args, name, len(specs), vertices, n_gpus=world),
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
 
 
 # ------------------------------------------------------------------------------------------
-# main
+# other workloads
 # ------------------------------------------------------------------------------------------
 
 def bench_hair(args, ctx_factory):
@@ -283,13 +459,12 @@ def bench_hair(args, ctx_factory):
     value = units * args.steps / (ms * 1e-3)
     # end to end: per frame the roots go up, the step runs, positions come back
     n = len(sc.sets[0].particles)
-    out = np.zeros(n, __import__("physxcoopa_b200._abi", fromlist=["A"]).PARTICLE)
     e0 = time.perf_counter()
     for f in range(max(3, args.steps // 2)):
         pos, rot = sc.root_path(f + 1)
         ctx.set_strand_roots(sid, pos, rot)
         ctx.step_strands([sid], [sc.meta["colliders_at"](f + 1)], iterations=sc.iterations)
-        out = ctx.read_strand_particles(sid, n)
+        ctx.read_strand_particles(sid, n)
     e2e_s = (time.perf_counter() - e0) / max(3, args.steps // 2)
     line = {"metric": "hair particle-substeps/s", "value": value, "unit": "particle-substeps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
@@ -325,7 +500,6 @@ def bench_large(args, local_rank):
     whole-GPU path) stepped together with the 65,536 x 32 groom (20 iterations, roots on a moving
     sphere). One step = one frame of both. Units: (cloth vertices + hair particles) x substeps."""
     import torch
-    from physxcoopa_b200 import _abi as A
     from physxcoopa_b200 import runtime as R
     from physxcoopa_b200 import scenes
     from physxcoopa_b200.arrays import capsule, collider_array
@@ -358,7 +532,6 @@ def bench_large(args, local_rank):
     clocks.start()
     time.sleep(0.3)
     l0 = ctx.launch_count
-    cloth_ms = 0.0
     with torch.cuda.stream(stream):
         t0.record(stream)
         for _ in range(args.steps):
@@ -403,20 +576,20 @@ def bench_large(args, local_rank):
     return line
 
 
-def bench_warm(args, local_rank):
-    """Learned warm start vs the plain 20-iteration solver at equal residual (see the module
-    docstring). Returns the JSON line."""
+# ------------------------------------------------------------------------------------------
+# the learned warm start (config 4) on a cloth batch
+# ------------------------------------------------------------------------------------------
+
+def warm_start_comparison(args, ctx, sc, local_rank, steps):
+    """Plain 20 iterations against the network + 4 iterations at equal per-cloth residual, on a
+    fresh copy of `sc` each run (see the module docstring). Returns a dict for the JSON line."""
     import torch
-    from physxcoopa_b200 import _abi as A
-    from physxcoopa_b200 import runtime as R
     from physxcoopa_b200 import scenes
-    n = args.cloths or 4096
     plain_iters, warm_iters = 20, 4
-    ctx = R.Context(local_rank)
     ctx.set_cloth_variant(0 if args.variant is None else args.variant)
     # --- training rows from the plain solver on a separately seeded batch -------------------
     t0 = time.perf_counter()
-    tr = scenes.uneven_batch(n=min(512, n), seed=102)
+    tr = scenes.uneven_batch(n=512, seed=102, params=sheet_params(args))
     ids = [ctx.add_cloth(c) for c in tr.cloths]
     xs, ys = [], []
     rec_steps, want = 40, 2_000_000
@@ -433,14 +606,12 @@ def bench_warm(args, local_rank):
     loss = ctx.mlp_train(X, Y, epochs=40, batch=8192, learning_rate=1e-3, seed=0)
     t_train = time.perf_counter() - t0
 
-    sc = scenes.uneven_batch(n=n, seed=2)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local_rank))
     W = max(args.warmup, 3)
 
-    def run(kind, taus=None, collect=False, e2e=False):
-        """Steps a fresh copy of the benchmark batch: W plain warm-up steps, then args.steps of
-        `kind`. Timed with CUDA events unless `collect`, which reads the per-step warm results
-        (a host round trip per step) instead."""
+    def run(kind, taus=None, collect=False):
+        """Steps a fresh copy of the batch: W plain warm-up steps, then `steps` of `kind`. Timed
+        with CUDA events unless `collect`, which reads the per-step warm results instead."""
         ids = [ctx.add_cloth(c) for c in sc.cloths]
         d, keep = ctx.make_step(ids, sc.colliders, sc.gravity, sc.sources, sc.substeps, plain_iters, sc.h)
         for _ in range(W):
@@ -449,12 +620,10 @@ def bench_warm(args, local_rank):
         res = []
         t_a, t_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = ctx.launch_count
-        ids_np = np.ascontiguousarray(ids, np.uint64)
-        out = torch.empty(3 * sc.vertices, dtype=torch.float32, pin_memory=True).numpy() if e2e else None
         torch.cuda.synchronize()
         with torch.cuda.stream(stream):
             t_a.record(stream)
-            for _ in range(args.steps):
+            for _ in range(steps):
                 if kind == "plain":
                     ctx.step_desc(d)
                 elif kind == "plain_residual":
@@ -463,13 +632,11 @@ def bench_warm(args, local_rank):
                     ctx.step_warm_desc(d, warm_iterations=warm_iters, thresholds=taus)
                 else:
                     ctx.step_warm_desc(d, warm_iterations=warm_iters, thresholds=taus, continue_iterations=True)
-                if e2e:
-                    ctx.read_positions(ids_np, out)
                 if collect:
                     res.append(ctx.read_warm_results(ids))
             t_b.record(stream)
         torch.cuda.synchronize()
-        ms = t_a.elapsed_time(t_b) / args.steps
+        ms = t_a.elapsed_time(t_b) / steps
         launches = ctx.launch_count - l0
         for i in ids:
             ctx.remove_cloth(i)
@@ -482,60 +649,56 @@ def bench_warm(args, local_rank):
     taus = rp.max(0).astype(np.float32)
     _, res_w, _ = run("warm", taus, collect=True)
     rw = np.stack([r["residual"] for r in res_w])
-    fb = float(sum(r["fallbacks"].sum() for r in res_w) / sum(r["substeps"].sum() for r in res_w))
-    extra = float(sum(r["extra_iterations"].sum() for r in res_w) / sum(r["substeps"].sum() for r in res_w))
+    subs = sum(r["substeps"].sum() for r in res_w)
+    fb = float(sum(r["fallbacks"].sum() for r in res_w) / subs)
+    extra = float(sum(r["extra_iterations"].sum() for r in res_w) / subs)
     ms_restart, _, _ = run("warm_restart", taus)
+    ms_warm, _, launches = run("warm", taus)
+    verts = sc.vertices * sc.substeps
+    return {"workload": "the same batch: 20 plain iterations vs the network + 4 iterations, equal residual "
+                        "cloth by cloth",
+            "plain": {"iterations": plain_iters, "value": verts / (ms_plain * 1e-3), "ms_per_step": ms_plain,
+                      "residual_median": float(np.median(rp)), "residual_max": float(rp.max())},
+            "warm": {"iterations": warm_iters, "value": verts / (ms_warm * 1e-3), "ms_per_step": ms_warm,
+                     "residual_median": float(np.median(rw)), "residual_max": float(rw.max()),
+                     "gpu_launches": launches},
+            "speedup_vs_plain": ms_plain / ms_warm,
+            "fallback_rate": fb, "extra_iterations_per_substep": extra,
+            "fallback": "continue iterating from the warm state, 4 at a time, to the threshold or 20 iterations",
+            "restart_fallback": {"ms_per_step": ms_restart, "speedup_vs_plain": ms_plain / ms_restart,
+                                 "note": "restart from the prediction with 20 plain iterations"},
+            "residual": "max |len/rest - 1| over the stretch constraints, per cloth and substep",
+            "equal_residual": "a warm substep keeps iterating while its residual exceeds the plain solver's largest "
+                              "residual for that cloth over the same steps",
+            "dtype": "f32 solve; network bf16 weights and activations, fp32 accumulation (tcgen05, TMEM)",
+            "timed_steps": steps,
+            "training": {"rows": int(len(X)), "final_loss": loss, "record_s": t_rec, "train_s": t_train,
+                         "scenes": f"uneven batch seed 102 (512 sheets), plain 20 iterations, {rec_steps} steps"}}
+
+
+def bench_warm(args, local_rank):
+    """--workload warm_start: the comparison alone on the uneven batch, as its own JSON line."""
+    from physxcoopa_b200 import runtime as R
+    from physxcoopa_b200 import scenes
+    ctx = R.Context(local_rank)
+    sc = scenes.uneven_batch(n=args.cloths or 4096, seed=2, params=sheet_params(args))
     clocks = ClockSampler(local_rank)
     clocks.start()
-    time.sleep(0.3)
-    ms_w_total, _, launches = run("warm", taus)
+    w = warm_start_comparison(args, ctx, sc, local_rank, args.steps)
     clk = clocks.stop()
-    ms_e2e, _, _ = run("warm", taus, e2e=True)
-    verts = sc.vertices * sc.substeps
-    value = verts / (ms_w_total * 1e-3)
-    plain_value = verts / (ms_plain * 1e-3)
-    al = lambda x: (x + 255) & ~255
-    n_col = sum(len(c) for c in sc.colliders)
-    n_src = sum(0 if s is None else len(s) for s in (sc.sources or []))
-    h2d = al(192 * n) + al(312 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * n) + al(48 * n)
-    d2h = 12 * sc.vertices + 16 * n
-    cons = sum(len(c.stretch) + len(c.bend) for c in sc.cloths)
-    iters_done = warm_iters + extra
-    algo_bytes = sc.substeps * (iters_done * cons * 68 + sc.vertices * 150)
-    smem_bw = ctx.measure_smem_bandwidth()
-    achieved = algo_bytes / (ms_w_total * 1e-3) / 1e9
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": W,
-        "ms_per_step": ms_w_total, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 solve, bf16 network (fp32 accumulation)", "data": "synthetic (seeded scenes)",
-        "config": dict(workload_config(args, sc), workload=f"warm_start on {sc.name}", iterations=plain_iters,
-                       warm_iterations=warm_iters, residual="max |len/rest - 1| over stretch constraints",
-                       equal_residual="per cloth: fall back where the residual exceeds the plain solver's "
-                                      "max residual for that cloth over the same steps"),
-        "plain": {"value": plain_value, "ms_per_step": ms_plain, "residual_median": float(np.median(rp)),
-                  "residual_max": float(rp.max())},
-        "warm_start": {"speedup_vs_plain": value / plain_value, "fallback_rate": fb,
-                       "fallback": "continue iterating from the warm state, 4 at a time, to the threshold "
-                                   "or 20 iterations", "extra_iterations_per_substep": extra,
-                       "restart_fallback": {"ms_per_step": ms_restart, "speedup_vs_plain": ms_plain / ms_restart,
-                                            "note": "restart from the prediction with 20 plain iterations"},
-                       "residual_median": float(np.median(rw)), "residual_max": float(rw.max()),
-                       "training": {"rows": int(len(X)), "final_loss": loss, "record_s": t_rec, "train_s": t_train,
-                                    "scenes": "uneven batch seed 102 (512 cloths), plain 20 iterations, "
-                                              f"{rec_steps} steps"}},
-        "e2e": {"value": verts / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_bw / 1e9, "unit": "GB/s",
-                     "frac": achieved * 1e9 / smem_bw, "traffic": None,
-                     "peak_source": "measured on this GPU by pxb_measure_smem_bandwidth",
-                     "kernel": "cloth_step_kernel (warm start)", "algorithmic_bytes_per_launch": algo_bytes},
-        "cpu_baseline": None,
-        "gpu_launches": launches,
-        "clocks": clk,
-    }
     ctx.close()
-    return line
+    return {"metric": METRIC, "value": w["warm"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": w["warm"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 solve, bf16 network (fp32 accumulation)",
+            "data": "synthetic (seeded scenes)",
+            "config": dict(workload=f"warm_start on {sc.name}", cloths=len(sc.cloths), vertices=sc.vertices),
+            "warm_start": w, "roofline": None, "cpu_baseline": None, "gpu_launches": w["warm"]["gpu_launches"],
+            "clocks": clk}
 
+
+# ------------------------------------------------------------------------------------------
+# main: a cloth batch
+# ------------------------------------------------------------------------------------------
 
 def main():
     args = parse()
@@ -546,22 +709,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        sc = build_scene(args, 0)
-        res = []
-        for _ in range(max(args.warmup, 0)):
-            pass  # the reference has no warm-up state; each sample builds fresh cloths
-        for _ in range(args.steps):
-            res.append(reference_cpu(sc, seconds_target=8.0))
-        value = statistics.median(r["value"] for r in res)
-        cb = dict(res[0])
-        cb["value"] = value
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes)",
-                "config": workload_config(args, sc), "impl": "reference", "cpu_baseline": cb,
-                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
-        return 0
+        return reference_arm(args)
 
     if args.workload == "hair_groom":
         from physxcoopa_b200 import runtime as R
@@ -583,8 +731,9 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     from physxcoopa_b200 import runtime as R
+    from physxcoopa_b200 import shard
 
-    sc = build_scene(args, rank)
+    sc, shares, job_vertices, job_cloths = build_gpu_scene(args, rank, world)
     ctx = R.Context(local_rank)
     if sc.geometries:
         from physxcoopa_b200 import scenes
@@ -594,7 +743,6 @@ def main():
                             sc.iterations, sc.h)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local_rank))
 
-    tune = None
     if args.variant is None:
         best, ms = ctx.autotune(d, trials=2)
         tune = {"chosen_variant": best, "ms_per_step_by_variant": ms,
@@ -603,7 +751,8 @@ def main():
         ctx.set_cloth_variant(args.variant)
         tune = {"chosen_variant": args.variant, "fixed": True}
     step = ctx.step_graph_desc if args.graph else ctx.step_desc
-    for _ in range(max(args.warmup, 3)):
+    W = max(args.warmup, 3)
+    for _ in range(W):
         step(d)
     ctx.synchronize()
     smem_bw = ctx.measure_smem_bandwidth()
@@ -641,10 +790,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms, per_launch_ms = float(t[0]), float(t[1])
 
-    verts_per_step = sc.vertices * sc.substeps
-    value = world * verts_per_step * args.steps / (elapsed_ms * 1e-3)
+    value = job_vertices * sc.substeps * args.steps / (elapsed_ms * 1e-3)
 
-    # --- roofline of the dominant kernel (shared memory) ----------------------------------
+    # --- roofline of the dominant kernel (shared memory), this rank's share ------------------
     cons = sum(len(c.stretch) + len(c.bend) for c in sc.cloths)
     algo_bytes = sc.substeps * (sc.iterations * cons * 68 + sc.vertices * 150)
     achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
@@ -653,22 +801,17 @@ def main():
     prof = os.path.join(ROOT, "profiles", f"cloth_step_{args.workload}.json")
     if os.path.exists(prof):
         try:
-            pj = json.load(open(prof))
-            traffic = pj.get("dram_bytes_per_launch_full_workload")
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch_full_workload")
         except (OSError, ValueError):
             traffic = None
 
     # --- end to end through the public API with host buffers -----------------------------
-    import ctypes as C
     e2e_steps = args.e2e_steps or max(3, args.steps // 2)
-    out = torch.empty(3 * sc.vertices, dtype=torch.float32, pin_memory=True)
-    out_np = out.numpy()
-    # pinned host buffers the pipelined read alternates between (frame k lands while k + 1 runs)
-    outs_np = [out_np, torch.empty(3 * sc.vertices, dtype=torch.float32, pin_memory=True).numpy()]
-    ids_np = np.ascontiguousarray(ids, np.uint64)
     from physxcoopa_b200 import _abi as A
+    outs_np = [torch.empty(3 * sc.vertices, dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
+    ids_np = np.ascontiguousarray(ids, np.uint64)
     res_out = np.zeros(len(ids), A.FRAME_RESULT)
-    # and for the per-cloth results (bounds, largest speed, time: 32 B per cloth)
+    # per-cloth results (bounds, largest speed, time: 32 B per cloth), pinned
     res_pinned = [torch.empty(8 * len(ids), dtype=torch.float32, pin_memory=True).numpy().view(A.FRAME_RESULT)
                   for _ in range(2)]
     # pxb_cloths_step uploads one staging block per step: per-cloth step records (192 B),
@@ -694,14 +837,14 @@ def main():
            + al(hull_bytes))
     d2h = 12 * sc.vertices + 32 * len(ids) + 4
     ctx.synchronize()
-    if dist:
-        dist.barrier()
+
     def timed_e2e(pipelined):
         """Per step: the step call (its inputs uploaded from pinned memory), every particle
         position and the per-cloth results read back to pinned host memory. Pipelined:
         pxb_cloths_read_positions_async / pxb_cloths_read_results_async, step k's read-back
         copied while step k + 1 is prepared and runs, every copy landed before the closing
-        event; else the blocking pxb_cloths_read_positions / pxb_cloths_read_results."""
+        event; else the blocking pxb_cloths_read_positions / pxb_cloths_read_results. With
+        several ranks each frame's results are gathered to every rank (one all-gather)."""
         ctx.synchronize()
         if dist:
             dist.barrier()
@@ -714,9 +857,14 @@ def main():
                 if pipelined:
                     ctx.read_positions_async(ids_np, outs_np[k % 2])
                     ctx.read_results_async(ids_np, res_pinned[k % 2])
+                    if dist:  # the broadphase of every rank needs this frame's results
+                        ctx.wait_positions()
+                        shard.gather_results(res_pinned[k % 2], shares, job_cloths)
                 else:
-                    ctx.read_positions(ids_np, out_np)
+                    ctx.read_positions(ids_np, outs_np[0])
                     ctx.lib.pxb_cloths_read_results(ctx.h, A.ptr(ids_np), len(ids_np), A.ptr(res_out))
+                    if dist:
+                        shard.gather_results(res_out, shares, job_cloths)
             if pipelined:
                 ctx.wait_positions()
             e1.record(stream)
@@ -726,40 +874,47 @@ def main():
             t = torch.tensor([ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t[0])
-        return world * verts_per_step * e2e_steps / (ms * 1e-3)
+        return job_vertices * sc.substeps * e2e_steps / (ms * 1e-3)
 
     e2e_blocking = timed_e2e(False)
     e2e_value = timed_e2e(True)
 
+    # --- the learned warm start on the same batch (rank 0, one GPU) -------------------------
+    warm = None
+    if args.workload == "uneven_batch" and not args.no_warm and rank == 0 and world == 1:
+        warm = warm_start_comparison(args, ctx, sc, local_rank, args.steps)
+
     line = None
     if rank == 0:
         cpu = None
-        if world == 1 and not args.no_cpu_baseline:
-            cpu = reference_cpu(sc)
+        if world == 1 and not args.no_cpu_baseline and args.workload in PLAN_WORKLOADS:
+            cpu = cpu_baseline_from_modes(cpu_modes(args), job_cloths)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps,
+            "warmup": W, "ms_per_step": elapsed_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scenes)",
-            "config": dict(workload_config(args, sc), parallelism=f"independent cloth batches x{world}",
-                           autotune=tune, launch="pxb_cloths_step_graph (captured CUDA graph)" if args.graph
-                           else "pxb_cloths_step"),
+            "config": workload_config(args, sc.name, job_cloths, job_vertices, sc.substeps, sc.iterations, sc.h,
+                                      n_gpus=world),
+            "launch": {"entry": "pxb_cloths_step_graph (captured CUDA graph)" if args.graph else "pxb_cloths_step",
+                       "autotune": tune},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                     "read_back": "pipelined: pxb_cloths_read_positions_async + pxb_cloths_read_results_async, "
                                  "each step's positions and results copied to pinned host memory while the "
                                  "next step is prepared and runs",
                     "blocking_value": e2e_blocking},
+            "warm_start": warm,
             "roofline": {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "measured on this GPU by pxb_measure_smem_bandwidth",
                          "kernel": "cloth_step_kernel", "per_launch_ms": per_launch_ms,
+                         "per_launch": "one pxb_cloths_step (all of the step's grouped launches)",
                          "algorithmic_bytes_per_launch": algo_bytes,
                          "hbm": hbm_roofline(traffic, per_launch_ms)},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk,
-            "spec_metric": SPEC,
         }
         print(json.dumps(line))
     del keep

@@ -29,7 +29,6 @@ import numpy as np
 from . import _abi as A
 from .arrays import (ClothArrays, HeightGrid, Hull, Mesh, box, capsule, collider_array, gravity_sources, hull_collider,
                      mesh_collider, sphere)
-from .runtime import HostCloth
 
 SPACING = 0.05
 STRUCTURAL, SHEAR, BEND = 0.0, 1e-6, 1e-4
@@ -66,7 +65,31 @@ def cloth_params(**kw):
     return p
 
 
+def reference_params():
+    """The configurations' compliances as the reference's ClothParams can hold them: one stretch
+    compliance for the structural and the shear constraints (0), bend 1e-4. The per-batch shear
+    compliance of cloth_params() has no counterpart in the reference solver."""
+    return cloth_params(has_shear_compliance=0, shear_compliance=0.0)
+
+
+def grid_desc(side, center, seed, params=None):
+    """The pxb_grid_cloth_desc of a benchmark sheet: side x side particles at SPACING, +-1 mm
+    jitter from `seed`, 1 kg, shear on."""
+    width = (side - 1) * SPACING
+    d = A.GridClothDesc()
+    d.columns, d.rows, d.width, d.height = side, side, width, width
+    d.center = (A.C.c_float * 3)(*[float(v) for v in center])
+    d.orientation = (A.C.c_float * 4)(0.0, 0.0, 0.0, 1.0)
+    d.total_mass = 1.0
+    d.shear = 1
+    d.params = params if params is not None else cloth_params()
+    d.jitter = 1e-3
+    d.jitter_seed = seed
+    return d
+
+
 def _sheet(side, center, seed, pins, params=None, tethers=True):
+    from .runtime import HostCloth
     width = (side - 1) * SPACING
     h = HostCloth(side, side, width, width, center=center, params=params or cloth_params(),
                   jitter=1e-3, seed=seed)
@@ -89,25 +112,61 @@ def _corner_pins(side, center, pattern):
     return [((cx - half + k * SPACING, cy + half, cz), r) for k in range(side)]
 
 
-def single_drape(seed=0):
+@dataclass
+class SheetSpec:
+    """One sheet of a batch as drawn from the batch's seed, before any builder runs."""
+    side: int
+    center: tuple
+    seed: int
+    pins: list
+    colliders: np.ndarray
+    source: Optional[np.ndarray]
+
+
+def build_sheet(spec, params=None):
+    """A planned sheet built by the library's builders (jitter, pins, tethers when pinned)."""
+    return _sheet(spec.side, spec.center, spec.seed, spec.pins, params)
+
+
+def single_drape_name():
+    return "single_drape 32x32"
+
+
+def single_drape_plan(seed=0):
+    """The one sheet of the single drape: 32 x 32, two top corners pinned, a sphere of r 0.3 m
+    0.5 m below its centre."""
     center = (0.0, 0.0, 1.0)
-    c = _sheet(32, center, seed, _corner_pins(32, center, 0))
-    col = collider_array([sphere(0.3, (0.0, 0.0, 0.5))])
-    return ClothScene("single_drape 32x32", [c], [col], meta={"side": 32})
+    return [SheetSpec(32, center, seed, _corner_pins(32, center, 0),
+                      collider_array([sphere(0.3, (0.0, 0.0, 0.5))]), None)]
 
 
-def uniform_batch(n=1024, side=64, seed=1):
+def single_drape(seed=0, params=None):
+    s = single_drape_plan(seed)[0]
+    return ClothScene(single_drape_name(), [build_sheet(s, params)], [s.colliders], meta={"side": 32})
+
+
+def uniform_name(n, side):
+    return f"uniform_batch {n}x{side}^2"
+
+
+def uniform_plan(n=1024, side=64, seed=1):
+    """The draws of the uniform batch, sheet by sheet: pin pattern, then one sphere."""
     rng = np.random.default_rng(seed)
     center = (0.0, 0.0, 1.0)
-    cloths, cols = [], []
+    specs = []
     for k in range(n):
         pattern = int(rng.integers(0, 3))
-        cloths.append(_sheet(side, center, seed * 100003 + k, _corner_pins(side, center, pattern)))
         r = float(rng.uniform(0.2, 0.5))
         off = rng.uniform(-0.3, 0.3, 3)
-        cols.append(collider_array([sphere(r, (center[0] + off[0], center[1] + off[1],
-                                               center[2] - 0.5 + off[2]))]))
-    return ClothScene(f"uniform_batch {n}x{side}^2", cloths, cols, meta={"side": side, "n": n})
+        col = collider_array([sphere(r, (center[0] + off[0], center[1] + off[1], center[2] - 0.5 + off[2]))])
+        specs.append(SheetSpec(side, center, seed * 100003 + k, _corner_pins(side, center, pattern), col, None))
+    return specs
+
+
+def uniform_batch(n=1024, side=64, seed=1, params=None):
+    specs = uniform_plan(n, side, seed)
+    return ClothScene(uniform_name(n, side), [build_sheet(s, params) for s in specs], [s.colliders for s in specs],
+                      meta={"side": side, "n": n})
 
 
 def _random_quat(rng):
@@ -116,16 +175,18 @@ def _random_quat(rng):
     return tuple(float(v) for v in q.astype(np.float32))
 
 
-def uneven_batch(n=4096, lo=16, hi=128, seed=2, max_side=None):
+def uneven_plan(n=4096, lo=16, hi=128, seed=2, max_side=None):
+    """The draws of the uneven batch, sheet by sheet (side, pins, colliders, gravity source), in
+    the order uneven_batch consumes them: the first k specs of a batch of n are the batch of k."""
     rng = np.random.default_rng(seed)
-    cloths, cols, srcs = [], [], []
+    specs = []
     for k in range(n):
         side = int(rng.integers(lo, hi + 1))
         if max_side is not None:
             side = min(side, max_side)
         center = (0.0, 0.0, 1.0)
         pattern = int(rng.integers(0, 3))
-        cloths.append(_sheet(side, center, seed * 100003 + k, _corner_pins(side, center, pattern)))
+        pins = _corner_pins(side, center, pattern)
         recs = []
         for _ in range(int(rng.integers(1, 4))):
             kind = int(rng.integers(0, 3))
@@ -139,14 +200,27 @@ def uneven_batch(n=4096, lo=16, hi=128, seed=2, max_side=None):
             else:
                 recs.append(box(tuple(float(v) for v in rng.uniform(0.1, 0.5, 3)), pos,
                                 _random_quat(rng)))
-        cols.append(collider_array(recs))
+        src = None
         if k % 2 == 0:
-            srcs.append(gravity_sources([((float(rng.uniform(-2, 2)), float(rng.uniform(-2, 2)),
-                                           -3.0), 9.81, 1.0, 10.0)]))
-        else:
-            srcs.append(None)
-    return ClothScene(f"uneven_batch {n} sides U{{{lo}..{hi}}}", cloths, cols, sources=srcs,
-                      meta={"n": n, "lo": lo, "hi": hi})
+            src = gravity_sources([((float(rng.uniform(-2, 2)), float(rng.uniform(-2, 2)), -3.0),
+                                    9.81, 1.0, 10.0)])
+        specs.append(SheetSpec(side, center, seed * 100003 + k, pins, collider_array(recs), src))
+    return specs
+
+
+def uneven_name(n, lo=16, hi=128):
+    return f"uneven_batch {n} sides U{{{lo}..{hi}}}"
+
+
+def uneven_batch(n=4096, lo=16, hi=128, seed=2, max_side=None, params=None, first=None):
+    """The uneven batch built by the library's builders. `first` builds only the first sheets of
+    the batch (a sample with the batch's own draws); `params` replaces cloth_params()."""
+    specs = uneven_plan(n, lo, hi, seed, max_side)
+    if first is not None:
+        specs = specs[:first]
+    cloths = [build_sheet(s, params) for s in specs]
+    return ClothScene(uneven_name(n, lo, hi), cloths, [s.colliders for s in specs],
+                      sources=[s.source for s in specs], meta={"n": n, "lo": lo, "hi": hi})
 
 
 @dataclass
@@ -409,6 +483,7 @@ def mesh_cloth(rings=12, radius=0.5, center=(0.0, 0.0, 1.0), seed=0, pins=(), pa
     """A disc-mesh cloth built by pxb_host_cloth_make_mesh, with static pins ((point, radius)
     pairs) and, when pinned, tethers."""
     v, ix = disc_mesh(radius, rings, center, jitter=0.25, seed=seed)
+    from .runtime import HostCloth
     h = HostCloth.from_mesh(v, ix, total_mass=1.0, bend=bend, params=params or cloth_params())
     for point, r in pins:
         h.pin_static(point, r)

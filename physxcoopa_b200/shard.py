@@ -35,13 +35,24 @@ def partition(costs: Sequence[int], n_ranks: int) -> List[List[int]]:
 
 def gather_results(local: np.ndarray, shares: List[List[int]], n_total: int, group=None) -> np.ndarray:
     """Frame-end exchange: every rank contributes the per-cloth results (a structured array in
-    its share's order) and receives all of them in global cloth order. Uses the default process
-    group (NCCL between GPUs, gloo on CPU); the only collective of a sharded step."""
+    its share's order) and receives all of them in global cloth order. One tensor all-gather of
+    the records' bytes, each rank's block padded to the largest share (on the GPU under NCCL, in
+    host memory under gloo); the only collective of a sharded step."""
+    import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
-    parts = [None] * world
-    dist.all_gather_object(parts, np.ascontiguousarray(local), group=group)
+    rec = local.dtype.itemsize
+    width = max(len(s) for s in shares) * rec
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+    mine = torch.zeros(width, dtype=torch.uint8)
+    raw = np.ascontiguousarray(local).view(np.uint8).reshape(-1)
+    mine[:len(raw)] = torch.from_numpy(raw.copy())
+    mine = mine.to(dev)
+    parts = [torch.empty(width, dtype=torch.uint8, device=dev) for _ in range(world)]
+    dist.all_gather(parts, mine, group=group)
     out = np.zeros(n_total, local.dtype)
     for r in range(world):
-        out[np.asarray(shares[r], np.int64)] = parts[r]
+        block = parts[r].cpu().numpy()[:len(shares[r]) * rec].view(local.dtype)
+        out[np.asarray(shares[r], np.int64)] = block
     return out

@@ -16,6 +16,8 @@ from physxcoopa_b200.arrays import ClothArrays, StrandArrays
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libpxbref.so")
+# the same reference sources built -O3 -march=native (the CPU baseline's second build mode)
+REF_SO_NATIVE = os.path.join(ROOT, "oracle", "_ref", "libpxbref_native.so")
 
 f32p = C.POINTER(C.c_float)
 P = C.c_void_p
@@ -80,39 +82,44 @@ def ref_available():
 def ref():
     global _ref
     if _ref is None:
-        lib = C.CDLL(REF_SO)
-        lib.pxbref_cloth_make_grid.argtypes = [C.POINTER(A.GridClothDesc)]
-        lib.pxbref_cloth_make_grid.restype = P
-        lib.pxbref_cloth_from_desc.argtypes = [C.POINTER(A.ClothDesc)]
-        lib.pxbref_cloth_from_desc.restype = P
-        lib.pxbref_cloth_free.argtypes = [P]
-        lib.pxbref_cloth_pin_static.argtypes = [P, f32p, A.f32]
-        lib.pxbref_cloth_pin_static.restype = A.u32
-        lib.pxbref_cloth_pin_to_body.argtypes = [P, A.u32, A.u32, f32p, f32p, f32p, A.f32]
-        lib.pxbref_cloth_pin_to_body.restype = A.u32
-        lib.pxbref_cloth_build_tethers.argtypes = [P]
-        lib.pxbref_cloth_view.argtypes = [P, C.POINTER(A.ClothDesc)]
-        lib.pxbref_cloth_bounds.argtypes = [P, f32p]
-        lib.pxbref_solve_cloth.argtypes = [P, P, A.u32, f32p, A.u32, A.u32, A.f32]
-        lib.pxbref_project_particle.argtypes = [P, A.f32, f32p, f32p, f32p, P]
-        lib.pxbref_geometry_set_hull.argtypes = [A.u32, C.POINTER(A.HullDesc)]
-        lib.pxbref_geometry_set_mesh.argtypes = [A.u32, C.POINTER(A.MeshDesc)]
-        lib.pxbref_geometry_clear.argtypes = []
-        lib.pxbref_geometry_clear.restype = None
-        lib.pxbref_build_convex_hull.argtypes = [P, A.u32, P, A.u32, C.POINTER(A.u32), P, A.u32, P, P, A.u32]
-        lib.pxbref_project_particle.restype = C.c_int
-        lib.pxbref_bench_cloths.argtypes = [C.POINTER(P), A.u32, P, P, P, P, f32p, A.u32, A.u32,
-                                            A.f32, A.u32, A.u32]
-        lib.pxbref_bench_cloths.restype = C.c_double
-        lib.pxbref_strands_make.argtypes = [A.u32, P, P, P, P, C.POINTER(A.StrandParams)]
-        lib.pxbref_strands_make.restype = P
-        lib.pxbref_strands_free.argtypes = [P]
-        lib.pxbref_strands_view.argtypes = [P, C.POINTER(A.StrandSetDesc)]
-        lib.pxbref_strands_bounds.argtypes = [P, f32p]
-        lib.pxbref_strands_set_roots.argtypes = [P, P, A.u32, P, A.u32]
-        lib.pxbref_solve_strands.argtypes = [P, P, A.u32, f32p, A.u32, A.u32, A.f32]
-        _ref = lib
+        _ref = load_ref(REF_SO)
     return _ref
+
+
+def load_ref(path):
+    """Loads one build of the reference driver and declares its entry points."""
+    lib = C.CDLL(path)
+    lib.pxbref_cloth_make_grid.argtypes = [C.POINTER(A.GridClothDesc)]
+    lib.pxbref_cloth_make_grid.restype = P
+    lib.pxbref_cloth_from_desc.argtypes = [C.POINTER(A.ClothDesc)]
+    lib.pxbref_cloth_from_desc.restype = P
+    lib.pxbref_cloth_free.argtypes = [P]
+    lib.pxbref_cloth_pin_static.argtypes = [P, f32p, A.f32]
+    lib.pxbref_cloth_pin_static.restype = A.u32
+    lib.pxbref_cloth_pin_to_body.argtypes = [P, A.u32, A.u32, f32p, f32p, f32p, A.f32]
+    lib.pxbref_cloth_pin_to_body.restype = A.u32
+    lib.pxbref_cloth_build_tethers.argtypes = [P]
+    lib.pxbref_cloth_view.argtypes = [P, C.POINTER(A.ClothDesc)]
+    lib.pxbref_cloth_bounds.argtypes = [P, f32p]
+    lib.pxbref_solve_cloth.argtypes = [P, P, A.u32, f32p, A.u32, A.u32, A.f32]
+    lib.pxbref_project_particle.argtypes = [P, A.f32, f32p, f32p, f32p, P]
+    lib.pxbref_geometry_set_hull.argtypes = [A.u32, C.POINTER(A.HullDesc)]
+    lib.pxbref_geometry_set_mesh.argtypes = [A.u32, C.POINTER(A.MeshDesc)]
+    lib.pxbref_geometry_clear.argtypes = []
+    lib.pxbref_geometry_clear.restype = None
+    lib.pxbref_build_convex_hull.argtypes = [P, A.u32, P, A.u32, C.POINTER(A.u32), P, A.u32, P, P, A.u32]
+    lib.pxbref_project_particle.restype = C.c_int
+    lib.pxbref_bench_cloths.argtypes = [C.POINTER(P), A.u32, P, P, P, P, f32p, A.u32, A.u32,
+                                        A.f32, A.u32, A.u32]
+    lib.pxbref_bench_cloths.restype = C.c_double
+    lib.pxbref_strands_make.argtypes = [A.u32, P, P, P, P, C.POINTER(A.StrandParams)]
+    lib.pxbref_strands_make.restype = P
+    lib.pxbref_strands_free.argtypes = [P]
+    lib.pxbref_strands_view.argtypes = [P, C.POINTER(A.StrandSetDesc)]
+    lib.pxbref_strands_bounds.argtypes = [P, f32p]
+    lib.pxbref_strands_set_roots.argtypes = [P, P, A.u32, P, A.u32]
+    lib.pxbref_solve_strands.argtypes = [P, P, A.u32, f32p, A.u32, A.u32, A.f32]
+    return lib
 
 
 def vec(x):

@@ -459,7 +459,8 @@ pxb_status pxb_cloths_wait_positions(pxb_context* ctx);
  * on demand, this never does. At most 4096 cloths per call (PXB_ERR_TOO_LARGE beyond); the
  * per-call cloth list lives in a 48 KB array compiled into the library, held on every GPU that
  * loads it until exit. The first call on a device looks up that array's address (set-up):
- * make it before any stream capture. The registry must be current (a step since the last
+ * make it before any stream capture. The call list is assembled in a static host buffer under a
+ * mutex (no allocation, no large stack frame), so concurrent host calls take turns. The registry must be current (a step since the last
  * add / remove / parameter change), else PXB_ERR_INVALID_ARGUMENT. Enqueued on the context
  * stream, returns before completion; calls that overlap on the GPU (other contexts or streams
  * of the same device) share the array and race -- serialise them. */
@@ -553,8 +554,9 @@ pxb_status pxb_geometry_create_mesh(pxb_context* ctx, const pxb_mesh_desc* desc,
 /* A height-grid mesh (TriangleMesh::from_height_grid over geometry::HeightGrid, height_grid.h,
  * triangle_mesh.h:210-215): nx x ny samples (at least 2 x 2; heights padded with zeros), sample
  * (i, j) at (i * cell_x, j * cell_y, heights[j * nx + i]), two triangles per cell. Mesh colliders
- * naming it are queried through the grid's block pyramid in the reference's order. At most 2^24
- * samples. */
+ * naming it are queried through the grid's block pyramid in the reference's order. Sides of at
+ * most 32768 samples and at most 2^24 samples in all, else PXB_ERR_TOO_LARGE (the reference's
+ * HeightGrid has no such limit). */
 typedef struct pxb_height_grid_desc {
     uint32_t nx, ny;
     float cell_x, cell_y;

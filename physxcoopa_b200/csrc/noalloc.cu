@@ -37,6 +37,14 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char* g_scratch_ptr[kMaxDevices] = {};
 
+// The per-call cloth list is assembled in host memory that is also static (no allocation and no
+// 48 KB on the caller's stack, which render and worker threads may not have): one buffer for the
+// process, filled and uploaded under this mutex. Its upload is a pageable copy, so the buffer is
+// free again when cudaMemcpyAsync returns.
+std::mutex g_list_mutex;
+int32_t g_order[kMaxCloths];
+int64_t g_offs[kMaxCloths];
+
 // The device address of g_gather_scratch on `device` (which must be current), looked up once.
 cudaError_t scratch_on(int device, unsigned char** out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -64,17 +72,6 @@ pxb_status pxb_cloths_gather_positions_device(pxb_context* ctx, const uint64_t* 
         return ctx->fail(PXB_ERR_INVALID_ARGUMENT,
                          "cloths were added, removed or changed since the last step: step them (or call "
                          "pxb_cloths_read_positions) once before gathering without allocation");
-    int32_t order[kMaxCloths];
-    int64_t offs[kMaxCloths];
-    int64_t total = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-        ClothEntry* e = ctx->lookup(cloths[k]);
-        if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
-        order[k] = static_cast<int32_t>(e - ctx->cloths.data());
-        offs[k] = total;
-        total += 3 * static_cast<int64_t>(e->n_particles);
-    }
-    if (static_cast<size_t>(total) > capacity) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "output too small");
     int device = -1;
     if (pxb_status s = ctx->cuda(cudaGetDevice(&device), "current device")) return s;
     if (device != ctx->device || device < 0 || device >= kMaxDevices)
@@ -82,14 +79,26 @@ pxb_status pxb_cloths_gather_positions_device(pxb_context* ctx, const uint64_t* 
                          ctx->device, device);
     unsigned char* scratch = nullptr;
     if (pxb_status s = ctx->cuda(scratch_on(device, &scratch), "look up the gather scratch")) return s;
-    // Pageable host sources: each copy has left the host arrays when cudaMemcpyAsync returns,
-    // and runs in stream order before the kernel.
-    if (pxb_status s = ctx->cuda(cudaMemcpyAsync(scratch, order, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice,
-                                                 ctx->stream), "upload gather order"))
-        return s;
-    if (pxb_status s = ctx->cuda(cudaMemcpyAsync(scratch + kOrderBytes, offs, 8 * static_cast<size_t>(n),
-                                                 cudaMemcpyHostToDevice, ctx->stream), "upload gather offsets"))
-        return s;
+    {
+        std::lock_guard<std::mutex> lock(g_list_mutex);
+        int64_t total = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            ClothEntry* e = ctx->lookup(cloths[k]);
+            if (!e) return ctx->fail(PXB_ERR_INVALID_HANDLE, "cloth id is not live");
+            g_order[k] = static_cast<int32_t>(e - ctx->cloths.data());
+            g_offs[k] = total;
+            total += 3 * static_cast<int64_t>(e->n_particles);
+        }
+        if (static_cast<size_t>(total) > capacity) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "output too small");
+        // Pageable host sources: each copy has left the host buffers when cudaMemcpyAsync
+        // returns, and runs in stream order before the kernel.
+        if (pxb_status s = ctx->cuda(cudaMemcpyAsync(scratch, g_order, 4 * static_cast<size_t>(n),
+                                                     cudaMemcpyHostToDevice, ctx->stream), "upload gather order"))
+            return s;
+        if (pxb_status s = ctx->cuda(cudaMemcpyAsync(scratch + kOrderBytes, g_offs, 8 * static_cast<size_t>(n),
+                                                     cudaMemcpyHostToDevice, ctx->stream), "upload gather offsets"))
+            return s;
+    }
     cudaError_t le = launch_gather_positions(static_cast<const PxbClothDev*>(ctx->d_registry.p),
                                              reinterpret_cast<const int32_t*>(scratch),
                                              reinterpret_cast<const int64_t*>(scratch + kOrderBytes),

@@ -62,6 +62,33 @@ def test_device_gather_equals_host_read_on_consecutive_calls():
         ctx.close()
 
 
+def test_device_gather_allocates_nothing():
+    """On a fresh context, after one step and with nothing read back yet (so no buffer of the
+    host read path exists), the gather leaves the device's free memory unchanged; its output is
+    compared with pxb_cloths_read_positions only afterwards."""
+    import torch
+    ctx = R.Context(0)
+    try:
+        cloths, cols = sheets()
+        ids = [ctx.add_cloth(c) for c in cloths]
+        total = 3 * sum(len(c.particles) for c in cloths)
+        out = torch.zeros(total, dtype=torch.float32, device="cuda")
+        ctx.step(ids, cols)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        for _ in range(2):
+            ctx.gather_positions_device(ids, out.data_ptr(), total)
+        ctx.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0, f"device memory changed by {free0 - free1} bytes across the gathers"
+        host = np.zeros(total, np.float32)
+        ctx.read_positions(ids, host)
+        assert np.array_equal(out.cpu().numpy(), host)
+    finally:
+        ctx.close()
+
+
 def test_device_gather_refusals():
     import torch
     ctx = R.Context(0)

@@ -568,7 +568,7 @@ def bench_large(args, local_rank):
                        "cloth_ms_last_step": cloth_last_ms,
                        "l2": "cloth state (~18 MB) fits in L2; hair state 2.1 M particles x 48 B exceeds it"},
             "e2e": {"value": units / e2e_s, "unit": "vertex-substeps/s",
-                    "h2d_bytes_per_step": 192 + 312 + 64 * len(hair.sets[0].strands) + 312,
+                    "h2d_bytes_per_step": 200 + 312 + 64 * len(hair.sets[0].strands) + 312,
                     "d2h_bytes_per_step": 12 * n_cloth + 40 * n_hair},
             "roofline": None, "cpu_baseline": None, "gpu_launches": launches, "clocks": clk}
     del keep_c, keep_s
@@ -814,7 +814,7 @@ def main():
     # per-cloth results (bounds, largest speed, time: 32 B per cloth), pinned
     res_pinned = [torch.empty(8 * len(ids), dtype=torch.float32, pin_memory=True).numpy().view(A.FRAME_RESULT)
                   for _ in range(2)]
-    # pxb_cloths_step uploads one staging block per step: per-cloth step records (192 B),
+    # pxb_cloths_step uploads one staging block per step: per-cloth step records (200 B),
     # collider snapshots (312 B), gravity sources (24 B), the launch order (4 B) and the posed
     # convex hulls (16 B x (2 faces + 2 face-vertex entries) per distinct hull and pose), each
     # section padded to 256 B.
@@ -833,7 +833,7 @@ def main():
                     seen.add(key)
                     g = sc.geometries[gids.index(int(c["geometry"]))]
                     hull_bytes += 16 * (2 * len(g.face_planes) + 2 * len(g.face_vertices))
-    h2d = (al(192 * len(ids)) + al(312 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * len(ids))
+    h2d = (al(200 * len(ids)) + al(312 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * len(ids))
            + al(hull_bytes))
     d2h = 12 * sc.vertices + 32 * len(ids) + 4
     ctx.synchronize()

@@ -484,6 +484,15 @@ pxb_status pxb_solve_cloth_host(pxb_context* ctx, const pxb_cloth_desc* desc,
  * threads, 1 = 768, 2 = 1024; a larger block has more warps to hide latency but fewer
  * registers per thread). Results are identical across variants; only speed differs. */
 pxb_status pxb_context_set_cloth_variant(pxb_context* ctx, int32_t variant);
+/* Failure-path testing (no counterpart in the reference). Cloths beyond an 8-CTA cluster step on
+ * every SM with a grid barrier between colours; each barrier wait is bounded (grid_wait_polls
+ * polls of about 64 ns, default 2^22) and, when it runs out, records an error word, stops all
+ * later barrier waits of the launch so it ends at once, and makes the next synchronising call
+ * return PXB_ERR_DEVICE_STATUS (which clears the word). With `unreachable` set, no grid barrier
+ * can complete, so that path runs on purpose; the cloth's state after such a step is
+ * meaningless -- rewrite it (pxb_cloth_write_particles) or re-add the cloth. The context stays
+ * usable: restore the defaults with (1 << 22, 0). */
+pxb_status pxb_context_set_wait_test(pxb_context* ctx, uint32_t grid_wait_polls, uint32_t unreachable);
 /* Autotuner: times every kernel variant on `step` (the caller's real batch, `trials` launches
  * each after one warm-up) and keeps the fastest on the context. The listed cloths' device state
  * and host mirrors are saved first and restored after, so tuning does not advance them.
@@ -694,6 +703,36 @@ pxb_status pxb_strands_step(pxb_context* ctx, const pxb_strand_step_desc* step);
 pxb_status pxb_strands_read_results(pxb_context* ctx, const uint64_t* sets, uint32_t n,
                                     pxb_cloth_frame_result* out);
 
+typedef struct pxb_strand_frame_desc {
+    const uint64_t* sets;                   /* live strand sets to advance this frame */
+    uint32_t n_sets;
+    const pxb_collider* colliders;          /* each set's gathered colliders, flat */
+    const uint32_t* collider_offsets;       /* n_sets + 1 offsets; NULL = no colliders */
+    const uint8_t* collider_moving;         /* per set: a non-static collider of its list moves
+                                               (world.h:1905-1911); NULL = none does */
+    float gravity[3];
+    const pxb_gravity_source* sources;
+    const uint32_t* source_offsets;
+    float fixed_dt;                         /* PhysicsConfig::fixed_dt */
+    uint32_t cloth_substeps;                /* PhysicsConfig::cloth_substeps */
+    uint32_t cloth_iterations;              /* PhysicsConfig::cloth_iterations */
+    float dt;                               /* this frame's dt */
+} pxb_strand_frame_desc;
+
+/* One strand frame as PhysicsWorld::step_strands_ runs it (world.h:1861-1957), for every listed
+ * set: the frame's substep count; a root whose target moved since the last one (|root -
+ * prev_root|^2 > 1e-6, set by pxb_strands_set_roots) or a moving collider wakes the set; a
+ * sleeping set only carries its roots' targets into their previous targets; one batched solve
+ * of the awake sets (gravity at each set's bounds centre when it has sources); then the sleep
+ * bookkeeping on each solved set's max particle speed (below params.sleep_threshold for
+ * params.sleep_time seconds: asleep, velocities zeroed). The collider gather (broadphase or the
+ * set's allowlist) stays the caller's. Synchronous. dt must be positive. awake_out (n_sets
+ * entries, may be NULL) receives each set's awake flag after the frame. */
+pxb_status pxb_strands_step_frame(pxb_context* ctx, const pxb_strand_frame_desc* frame, uint8_t* awake_out);
+/* StrandSet::awake and StrandSet::sleep_timer of the listed sets (a new set is awake, timer 0). */
+pxb_status pxb_strands_read_sleep_state(pxb_context* ctx, const uint64_t* sets, uint32_t n, uint8_t* awake_out,
+                                        float* sleep_timer_out);
+
 /* Drop-in hair::solve_strands on HOST memory: the set described by `desc` is advanced and its
  * particles, stretch lambdas and time written back (bounds_out, 6 floats, may be NULL). */
 pxb_status pxb_solve_strands_host(pxb_context* ctx, const pxb_strand_set_desc* desc,
@@ -812,6 +851,25 @@ pxb_status pxb_cloths_record(pxb_context* ctx, const pxb_cloth_step_desc* step, 
  * per second, one 1024-thread CTA per SM copying float4s between two shared buffers). The
  * cloth kernel is bound by this figure; benchmarks use it as the roofline denominator. */
 pxb_status pxb_measure_smem_bandwidth(pxb_context* ctx, double* bytes_per_second);
+/* Self-check of the solver's division on this device (no counterpart in the reference): the
+ * constraint direction d / |d| is computed as three correctly rounded quotients from one
+ * reciprocal (Markstein's method). mismatches[0] counts divisor significands (every one of the
+ * 2^23, at three exponents) whose refined reciprocal is not the correctly rounded one;
+ * mismatches[1] counts, over `samples` seeded random constraints (3 quotients each), quotients
+ * that differ from IEEE division. Both must be 0. */
+pxb_status pxb_check_quotients(pxb_context* ctx, uint64_t samples, uint64_t seed, uint64_t mismatches[2]);
+/* The same division over whole significands: for divisor significands [b_first, b_first +
+ * b_count) (of the 2^23) and every numerator significand, the number of quotients that differ
+ * from IEEE division (the full sweep, b_first 0 and b_count 2^23, is every case the method's
+ * rounding depends on; it takes a few minutes). */
+pxb_status pxb_check_quotient_significands(pxb_context* ctx, uint32_t b_first, uint32_t b_count, uint64_t* mismatches);
+/* Self-check of one whole constraint projection: the solver's form (packed two-lane FP32
+ * arithmetic, shared reciprocal) against the reference's scalar IEEE operations on `samples`
+ * seeded random endpoint pairs (ordinary, near-zero and subnormal coordinates, signed zeros,
+ * pinned endpoints, compliances and lambdas). *mismatches counts projections differing in any
+ * output bit; the first such input (8 floats: a xyzw, b xyzw) goes to first_bad when not NULL. */
+pxb_status pxb_check_projections(pxb_context* ctx, uint64_t samples, uint64_t seed, uint64_t* mismatches,
+                                 float* first_bad);
 
 #ifdef __cplusplus
 }  /* extern "C" */

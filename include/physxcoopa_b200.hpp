@@ -8,7 +8,11 @@
 //   hair::solve_strands(StrandSet&, colliders, gravity, substeps, iterations, h, scratch)
 //        (physxcoopa/hair/strand_solver.h:121-123)
 //
-// in namespace pxb::b200, backed by the device solver. The Cloth / StrandSet is advanced in
+// in namespace pxb::b200, backed by the device solver: a call site changes only its namespace
+// (px::cloth::solve_cloth(c, cols, g, 4, 10, h, scratch) becomes pxb::b200::solve_cloth(c, cols,
+// g, 4, 10, h, scratch)). Those overloads run on the calling thread's own context
+// (thread_device(): CUDA device 0 unless set_thread_device chose another); the overloads that
+// take a Device& first use the caller's. The Cloth / StrandSet is advanced in
 // place exactly as the reference advances it; the scratch and dispatcher arguments are accepted
 // for signature compatibility and not used (the device needs neither). Vectors are handed to
 // the library as they are: pxb_particle, pxb_constraint, pxb_anchor... are the reference's own
@@ -19,9 +23,11 @@
 #define PHYSXCOOPA_B200_HPP
 
 #include <cstring>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
+#include <utility>
 #include <vector>
 
 #include "physxcoopa_b200.h"
@@ -39,9 +45,10 @@ static_assert(sizeof(coopa::physx::hair::Strand) == sizeof(pxb_strand), "strand 
 // One context per thread that steps cloths (the C-ABI is single-threaded per context).
 class Device {
 public:
-    explicit Device(int device = 0) {
+    explicit Device(int device = 0) : index_(device) {
         if (pxb_context_create(device, &ctx_) != PXB_OK) throw std::runtime_error("pxb_context_create failed");
     }
+    int index() const { return index_; }
     ~Device() { pxb_context_destroy(ctx_); }
     Device(const Device&) = delete;
     Device& operator=(const Device&) = delete;
@@ -110,6 +117,7 @@ public:
     }
 
 private:
+    int index_ = 0;
     pxb_context* ctx_ = nullptr;
     std::unordered_map<const void*, uint32_t> geometry_;
 };
@@ -275,6 +283,61 @@ void solve_strands(Device& dev, coopa::physx::hair::StrandSet& set,
               "solve_strands");
     set.bounds.min = glm::vec3(bounds[0], bounds[1], bounds[2]);
     set.bounds.max = glm::vec3(bounds[3], bounds[4], bounds[5]);
+}
+
+// ------------------------------------------------------------------------------------------
+// The reference's exact signatures, on the calling thread's context
+// ------------------------------------------------------------------------------------------
+
+namespace detail {
+inline int& thread_device_index() {
+    thread_local int device = 0;
+    return device;
+}
+inline std::unique_ptr<Device>& thread_device_slot() {
+    thread_local std::unique_ptr<Device> dev;
+    return dev;
+}
+}  // namespace detail
+
+// The CUDA device the calling thread's reference-signature calls run on (default 0). Takes
+// effect at the thread's next call; the thread's previous context (and the cloths it held) is
+// released then.
+inline void set_thread_device(int device) { detail::thread_device_index() = device; }
+
+// The calling thread's context, created on its first use (one per host thread, as the C-ABI
+// requires).
+inline Device& thread_device() {
+    auto& slot = detail::thread_device_slot();
+    const int want = detail::thread_device_index();
+    if (!slot || slot->index() != want) slot.reset(new Device(want));
+    return *slot;
+}
+
+// cloth::solve_cloth(Cloth&, colliders, gravity, substeps, iterations, h, scratch, dispatch)
+// (cloth_solver.h:158-161): the dispatcher is accepted and unused.
+template <typename Dispatch>
+void solve_cloth(coopa::physx::cloth::Cloth& c, const std::vector<coopa::physx::cloth::ClothCollider>& colliders,
+                 const glm::vec3& gravity, uint32_t substeps, uint32_t iterations, float h,
+                 coopa::physx::cloth::ClothSolverScratch& scratch, Dispatch&& dispatch) {
+    solve_cloth(thread_device(), c, colliders, gravity, substeps, iterations, h, scratch,
+                std::forward<Dispatch>(dispatch));
+}
+
+// The serial overload (cloth_solver.h:463-467).
+inline void solve_cloth(coopa::physx::cloth::Cloth& c, const std::vector<coopa::physx::cloth::ClothCollider>& colliders,
+                        const glm::vec3& gravity, uint32_t substeps, uint32_t iterations, float h,
+                        coopa::physx::cloth::ClothSolverScratch& scratch) {
+    solve_cloth(thread_device(), c, colliders, gravity, substeps, iterations, h, scratch);
+}
+
+// hair::solve_strands(StrandSet&, colliders, gravity, substeps, iterations, h, scratch)
+// (strand_solver.h:121-123).
+inline void solve_strands(coopa::physx::hair::StrandSet& set,
+                          const std::vector<coopa::physx::cloth::ClothCollider>& colliders,
+                          const glm::vec3& gravity, uint32_t substeps, uint32_t iterations, float h,
+                          coopa::physx::hair::StrandSolverScratch& scratch) {
+    solve_strands(thread_device(), set, colliders, gravity, substeps, iterations, h, scratch);
 }
 
 }  // namespace b200

@@ -1474,3 +1474,44 @@ int orc_world_step_cloth(orc_cloth* c, const pxb_body_pose* bodies, uint32_t n_b
     }
     return 1;
 }
+
+int orc_world_step_strands(orc_strand_set* s, int collider_moving, const pxb_collider* colliders,
+                           uint32_t n_colliders, const float gravity[3], const pxb_gravity_source* sources,
+                           uint32_t n_sources, float fixed_dt, uint32_t cloth_substeps,
+                           uint32_t cloth_iterations, float dt, int* awake, float* sleep_timer) {
+    const uint32_t frame_substeps = orc_frame_substeps(dt, fixed_dt, cloth_substeps);
+    /* world.h:1872-1878: a root that moved is motion the groom has to answer */
+    int root_moved = 0;
+    for (uint32_t i = 0; i < s->n_strands && !root_moved; ++i) {
+        const v3 delta = sub(ld(s->strands[i].root_position), ld(s->strands[i].prev_root_position));
+        if (dot(delta, delta) > K_EPSILON) root_moved = 1;
+    }
+    /* world.h:1926-1937: the sleep gate */
+    if (root_moved || collider_moving) {
+        *awake = 1;
+        *sleep_timer = 0.0f;
+    }
+    if (!*awake) {
+        for (uint32_t i = 0; i < s->n_strands; ++i) {
+            memcpy(s->strands[i].prev_root_position, s->strands[i].root_position, sizeof(float) * 3);
+            memcpy(s->strands[i].prev_root_orientation, s->strands[i].root_orientation, sizeof(float) * 4);
+        }
+        return 0;
+    }
+    /* world.h:1941-1945 */
+    const int r = orc_step_strands(s, colliders, n_colliders, gravity, sources, n_sources, frame_substeps,
+                                   cloth_iterations, dt);
+    if (r != 0) return r;
+    /* world.h:1947-1955: sleep bookkeeping */
+    if (orc_max_particle_speed(s->particles, s->n_particles) < s->params.sleep_threshold) {
+        *sleep_timer += dt;
+        if (*sleep_timer >= s->params.sleep_time) {
+            *awake = 0;
+            for (uint32_t i = 0; i < s->n_particles; ++i)
+                s->particles[i].velocity[0] = s->particles[i].velocity[1] = s->particles[i].velocity[2] = 0.0f;
+        }
+    } else {
+        *sleep_timer = 0.0f;
+    }
+    return 1;
+}

@@ -147,6 +147,18 @@ int orc_world_step_cloth(orc_cloth* c, const pxb_body_pose* bodies, uint32_t n_b
                          uint32_t cloth_substeps, uint32_t cloth_iterations, float dt, int* awake,
                          float* sleep_timer);
 
+/* PhysicsWorld::step_strands_'s per-set body (world.h:1861-1957) without the collider gather: a
+ * root that moved since the last target (|root - prev_root|^2 > k_epsilon) or a moving collider
+ * wakes the set; a sleeping set only carries its roots' targets into their previous targets; an
+ * awake set is solved (orc_step_strands with the frame's substeps, gravity at the bounds centre
+ * when there are sources), then the sleep bookkeeping on its max particle speed. *awake /
+ * *sleep_timer are StrandSet::awake / sleep_timer, read and written. Returns 1 when the set was
+ * solved, 0 when it slept, -1 as orc_solve_strands. */
+int orc_world_step_strands(orc_strand_set* s, int collider_moving, const pxb_collider* colliders,
+                           uint32_t n_colliders, const float gravity[3], const pxb_gravity_source* sources,
+                           uint32_t n_sources, float fixed_dt, uint32_t cloth_substeps,
+                           uint32_t cloth_iterations, float dt, int* awake, float* sleep_timer);
+
 #ifdef __cplusplus
 }
 #endif

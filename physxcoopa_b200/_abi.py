@@ -238,6 +238,13 @@ class ClothFrameDesc(C.Structure):
                 ("dt", f32)]
 
 
+class StrandFrameDesc(C.Structure):
+    """pxb_strand_frame_desc: one PhysicsWorld::step_strands_ frame."""
+    _fields_ = [("sets", P), ("n_sets", u32), ("colliders", P), ("collider_offsets", P), ("collider_moving", P),
+                ("gravity", f32 * 3), ("sources", P), ("source_offsets", P), ("fixed_dt", f32),
+                ("cloth_substeps", u32), ("cloth_iterations", u32), ("dt", f32)]
+
+
 class StrandStepDesc(C.Structure):
     """pxb_strand_step_desc."""
     _fields_ = [("sets", P), ("n_sets", u32), ("colliders", P), ("collider_offsets", P),

@@ -1,6 +1,6 @@
 """Builds the C-ABI shared library in-tree: physxcoopa_b200/_lib/libphysxcoopa_b200.so.
 
-nvcc compiles every source in csrc/ for sm_100a only, with IEEE single-precision arithmetic
+nvcc compiles every source in csrc/ for sm_100a only (in parallel, one object each, then one link), with IEEE single-precision arithmetic
 and no contraction (-fmad=false on the device, -ffp-contract=off on the host) so the solver's
 rounding is the reference's. Run `python -m physxcoopa_b200.build` or call build().
 """
@@ -43,20 +43,38 @@ def up_to_date():
 
 
 def build(force=False, verbose=False):
-    """Compiles the library unless it is newer than every input. Returns the library path."""
+    """Compiles the library unless it is newer than every input. Returns the library path.
+    Each source compiles to its own object in parallel (physxcoopa_b200/_build), then one link."""
     if not force and up_to_date():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(objdir, os.path.basename(f) + ".o") for f in srcs]
+
+    def compile_one(pair):
+        src, obj = pair
+        cmd = ["nvcc", *NVCC_FLAGS, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd))
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, zip(srcs, objs)))
+    for r in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc failed building libphysxcoopa_b200.so")
+        if verbose and (r.stdout or r.stderr):
+            sys.stderr.write(r.stdout + r.stderr)
     tmp = LIB + ".tmp"
-    cmd = ["nvcc", *NVCC_FLAGS, "-shared", "-o", tmp, *sources()]
-    if verbose:
-        print(" ".join(cmd))
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    r = subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs],
+                       capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libphysxcoopa_b200.so")
-    if verbose and (r.stdout or r.stderr):
-        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed linking libphysxcoopa_b200.so")
     os.replace(tmp, LIB)
     return LIB
 

@@ -11,6 +11,7 @@
 
 #include "../../include/physxcoopa_b200.h"
 #include "pxb_internal.h"
+#include "pxb_quotient.cuh"
 
 namespace pxb {
 namespace {
@@ -541,25 +542,49 @@ __device__ __forceinline__ bool project_particle(const PxbDevCollider* __restric
 // One XPBD distance projection (cloth_solver.h:119-138)
 // ------------------------------------------------------------------------------------------
 
-// Computes the new endpoint positions of one constraint. Returns false when the reference
-// returns early (both pinned, or coincident endpoints) -- nothing is written then.
+// The new endpoint positions and dlambda of one constraint, computed unconditionally; returns
+// false where the reference returns early (both endpoints pinned, or coincident endpoints), and
+// the caller then writes nothing. Every operation is the reference's, in its order and with its
+// rounding: the pairs (x, y) of d, of d*d and of the corrections go through the two-lane FP32
+// instructions (each lane rounded as the scalar one), (dz, w) = (a.z - b.z, a.w + b.w) through
+// one of them (b times (-1, 1) is exact, the sum rounded once). kLam false means the colour's
+// compliance is exactly +0, so -c - alpha * lambda is -c. pxb_check_projections compares this
+// form with the scalar one, every output bit.
+template <bool kLam = true>
+__device__ __forceinline__ bool distance_core(float4& pa, float4& pb, float rest, float lam, float alpha,
+                                              float& dlambda) {
+    const float2 dxy = fma2_rn(make_float2(pb.x, pb.y), make_float2(-1.0f, -1.0f), make_float2(pa.x, pa.y));
+    const float2 dzw = fma2_rn(make_float2(pb.z, pb.w), make_float2(-1.0f, 1.0f), make_float2(pa.z, pa.w));
+    const float dz = dzw.x, w = dzw.y;
+    const float2 sq = mul2_rn(dxy, dxy);
+    const float l = sqrtf((sq.x + sq.y) + dz * dz);
+    const bool ok = !(w <= 0.0f) && !(l < PXB_EPSILON);
+    float nx, ny, nz;
+    unit3(dxy.x, dxy.y, dz, l, nx, ny, nz);
+    const float c = l - rest;
+    const float num = kLam ? -c - alpha * lam : -c;
+    dlambda = num / (w + alpha);
+    const float2 cxy = mul2_rn(make_float2(dlambda, dlambda), make_float2(nx, ny));
+    const float cz = dlambda * nz;
+    // The endpoint updates stay scalar: built from an endpoint's own inverse mass (one register
+    // of a loaded pair repeated in both lanes), the packed form measured wrong in the y lane.
+    pa.x = pa.x + pa.w * cxy.x;
+    pa.y = pa.y + pa.w * cxy.y;
+    pa.z = pa.z + pa.w * cz;
+    pb.x = pb.x - pb.w * cxy.x;
+    pb.y = pb.y - pb.w * cxy.y;
+    pb.z = pb.z - pb.w * cz;
+    return ok;
+}
+
+// One XPBD distance projection: returns false (and leaves pa, pb alone) where the reference
+// returns early.
 __device__ __forceinline__ bool solve_pair(float4& pa, float4& pb, float rest, float lam,
                                            float alpha, float& dlambda) {
-    const float w = pa.w + pb.w;
-    if (w <= 0.0f) return false;
-    const float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
-    const float l = sqrtf(dx * dx + dy * dy + dz * dz);
-    if (l < PXB_EPSILON) return false;
-    const float nx = dx / l, ny = dy / l, nz = dz / l;
-    const float c = l - rest;
-    dlambda = (-c - alpha * lam) / (w + alpha);
-    const float cx = dlambda * nx, cy = dlambda * ny, cz = dlambda * nz;
-    pa.x = pa.x + pa.w * cx;
-    pa.y = pa.y + pa.w * cy;
-    pa.z = pa.z + pa.w * cz;
-    pb.x = pb.x - pb.w * cx;
-    pb.y = pb.y - pb.w * cy;
-    pb.z = pb.z - pb.w * cz;
+    float4 a = pa, b = pb;
+    if (!distance_core(a, b, rest, lam, alpha, dlambda)) return false;
+    pa = a;
+    pb = b;
     return true;
 }
 

@@ -228,6 +228,8 @@ struct PxbClothStep {
     int32_t write_lambdas;
     float self_distance;     // ClothParams::self_distance when self-collision runs, else 0
     int32_t self_collision;  // self_collision && self_distance > k_epsilon (cloth_solver.h:170)
+    uint32_t grid_wait_polls;   // whole-GPU path: polls of a grid-barrier wait before it gives up
+    uint32_t grid_extra_arrivals;  // 0; a test sets it so no grid barrier can complete
 };
 
 // One registered strand set on the device. Particles are strand-major, 32 slots per strand
@@ -285,7 +287,7 @@ struct PxbFrameResult {
 };
 
 static_assert(sizeof(PxbSeg) == 32 && alignof(PxbSeg) == 16, "segment descriptor layout");
-static_assert(sizeof(PxbClothStep) == 192, "per-step record size is part of the staging contract");
+static_assert(sizeof(PxbClothStep) == 200, "per-step record size is part of the staging contract");
 static_assert(sizeof(PxbDevCollider) == 312, "collider snapshot size is part of the staging contract");
 static_assert(sizeof(PxbMeshNode) == 32 && sizeof(PxbMeshTri) == 64, "mesh record layout");
 

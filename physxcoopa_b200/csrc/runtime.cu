@@ -634,8 +634,9 @@ static void layout_ranks(ClothEntry& e) {
         for (size_t r = 0; r < e.runs.size(); ++r) {
             const float comp = batch_compliance(e, e.run_batch[r].x != 0, e.run_batch[r].y);
             e.runs[r].compliance = comp;
-            e.runs[r].lam_base = comp != 0.0f ? lam : -1;
-            if (comp != 0.0f) lam += e.runs[r].count;
+            const bool has_lam = comp != 0.0f || std::signbit(comp);  // exactly +0: no lambdas
+            e.runs[r].lam_base = has_lam ? lam : -1;
+            if (has_lam) lam += e.runs[r].count;
         }
         ClothEntry::Rank& rk = e.ranks[0];
         rk.n_lam = lam;
@@ -664,7 +665,9 @@ static void layout_ranks(ClothEntry& e) {
         ClothEntry::Rank& rk = e.ranks[r];
         int lam = 0;
         for (int c = 0; c < e.n_colours; ++c) {
-            const bool has_lam = colour_compliance(e, c) != 0.0f;
+            // a colour without lambdas must have a compliance of exactly +0 (the kernel then
+            // takes -c - alpha * lambda as -c); -0 keeps its lambdas like any other value
+            const bool has_lam = colour_compliance(e, c) != 0.0f || std::signbit(colour_compliance(e, c));
             for (int sg = rk.seg_begin + rk.colour_seg[c]; sg < rk.seg_begin + rk.colour_seg[c + 1]; ++sg) {
                 e.segs[sg].lam_base = has_lam ? lam : -1;
                 if (has_lam) lam += e.segs[sg].count;
@@ -1300,6 +1303,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         s.src_begin = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k]) : 0;
         s.src_count = sd->source_offsets ? static_cast<int32_t>(sd->source_offsets[k + 1] - sd->source_offsets[k]) : 0;
         s.write_lambdas = 1;
+        s.grid_wait_polls = grid_wait_polls;
+        s.grid_extra_arrivals = grid_extra_arrivals;
         s.self_collision = self_on(e) ? 1 : 0;
         s.self_distance = self_on(e) ? P.self_distance : 0.0f;
         hs_order[slot] = static_cast<int32_t>(ents[k] - cloths.data());
@@ -1930,6 +1935,14 @@ pxb_status pxb_solve_cloth_host(pxb_context* ctx, const pxb_cloth_desc* desc, px
     return PXB_OK;
 }
 
+
+pxb_status pxb_context_set_wait_test(pxb_context* ctx, uint32_t grid_wait_polls, uint32_t unreachable) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    if (grid_wait_polls == 0) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "a wait needs at least one poll");
+    ctx->grid_wait_polls = grid_wait_polls;
+    ctx->grid_extra_arrivals = unreachable ? 1u : 0u;
+    return PXB_OK;
+}
 
 pxb_status pxb_context_set_cloth_variant(pxb_context* ctx, int32_t variant) {
     if (!ctx) return PXB_ERR_INVALID_ARGUMENT;

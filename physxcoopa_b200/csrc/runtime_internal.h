@@ -99,6 +99,8 @@ struct StrandEntry {
     PxbStrandDev dev{};
     float bounds[7] = {0, 0, 0, 0, 0, 0, 0};
     bool has_result = false;
+    bool awake = true;         // StrandSet::awake (pxb_strands_step_frame)
+    float sleep_timer = 0.0f;  // StrandSet::sleep_timer
 };
 
 // One registered collider geometry (pxb_geometry_create_hull / _mesh); id = index + 1.
@@ -157,6 +159,10 @@ struct pxb_context {
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[kSideStreams] = {};
     uint32_t* d_err = nullptr;
+    // whole-GPU path: polls of a grid-barrier wait before it expires, and the test setting that
+    // makes every grid barrier unreachable (pxb_context_set_wait_test)
+    uint32_t grid_wait_polls = 1u << 22;
+    uint32_t grid_extra_arrivals = 0;
     std::string error;
     uint64_t launches = 0;
     std::vector<ClothEntry> cloths;

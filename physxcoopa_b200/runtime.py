@@ -66,6 +66,8 @@ SIGNATURES = {
     "pxb_cloths_state_hash": ([P, P, u32, u64, C.POINTER(u64)], C.c_int),
     "pxb_cloths_read_render_buffer": ([P, P, u32, P, C.c_size_t], C.c_int),
     "pxb_cloths_read_sleep_state": ([P, P, u32, P, P], C.c_int),
+    "pxb_strands_step_frame": ([P, C.POINTER(A.StrandFrameDesc), P], C.c_int),
+    "pxb_strands_read_sleep_state": ([P, P, u32, P, P], C.c_int),
     "pxb_host_cloth_pin_to_body": ([P, u32, u32, f32p, f32p, f32p, f32, C.POINTER(u32)], C.c_int),
     "pxb_geometry_create_hull": ([P, C.POINTER(A.HullDesc), C.POINTER(u32)], C.c_int),
     "pxb_geometry_create_mesh": ([P, C.POINTER(A.MeshDesc), C.POINTER(u32)], C.c_int),
@@ -81,7 +83,11 @@ SIGNATURES = {
     "pxb_host_cloth_view": ([P, C.POINTER(A.ClothDesc)], C.c_int),
     "pxb_host_cloth_mutable": ([P, C.POINTER(P), C.POINTER(P), C.POINTER(P)], C.c_int),
     "pxb_measure_smem_bandwidth": ([P, C.POINTER(C.c_double)], C.c_int),
+    "pxb_check_quotients": ([P, u64, u64, C.POINTER(u64)], C.c_int),
+    "pxb_check_quotient_significands": ([P, u32, u32, C.POINTER(u64)], C.c_int),
+    "pxb_check_projections": ([P, u64, u64, C.POINTER(u64), C.POINTER(f32)], C.c_int),
     "pxb_context_set_cloth_variant": ([P, C.c_int32], C.c_int),
+    "pxb_context_set_wait_test": ([P, u32, u32], C.c_int),
     "pxb_strands_add": ([P, C.POINTER(A.StrandSetDesc), C.POINTER(u64)], C.c_int),
     "pxb_strands_remove": ([P, u64], C.c_int),
     "pxb_strands_set_params": ([P, u64, C.POINTER(A.StrandParams)], C.c_int),
@@ -342,6 +348,27 @@ class Context:
         self._check(self.lib.pxb_measure_smem_bandwidth(self.h, C.byref(v)), "measure_smem_bandwidth")
         return v.value
 
+    def check_quotients(self, samples, seed=0):
+        """pxb_check_quotients: (reciprocal mismatches, quotient mismatches); both should be 0."""
+        out = (u64 * 2)()
+        self._check(self.lib.pxb_check_quotients(self.h, samples, seed, out), "check_quotients")
+        return int(out[0]), int(out[1])
+
+    def check_projections(self, samples, seed=0):
+        """pxb_check_projections: (mismatching projections, first mismatching input or None)."""
+        out = u64()
+        fb = (f32 * 8)()
+        self._check(self.lib.pxb_check_projections(self.h, samples, seed, C.byref(out), fb), "check_projections")
+        return int(out.value), (list(fb) if out.value else None)
+
+    def check_quotient_significands(self, b_first=0, b_count=1 << 23):
+        """pxb_check_quotient_significands: quotients differing from IEEE division over divisor
+        significands [b_first, b_first + b_count) and every numerator significand."""
+        out = u64()
+        self._check(self.lib.pxb_check_quotient_significands(self.h, b_first, b_count, C.byref(out)),
+                    "check_quotient_significands")
+        return int(out.value)
+
     @property
     def launch_count(self):
         return int(self.lib.pxb_context_launch_count(self.h))
@@ -502,6 +529,12 @@ class Context:
         self.step_desc(d)
         del keep
 
+    def set_wait_test(self, grid_wait_polls=1 << 22, unreachable=False):
+        """pxb_context_set_wait_test: bound of a grid-barrier wait, and whether no grid barrier
+        can complete (to drive the expiry path in a test)."""
+        self._check(self.lib.pxb_context_set_wait_test(self.h, grid_wait_polls, 1 if unreachable else 0),
+                    "set_wait_test")
+
     def set_cloth_variant(self, variant):
         self._check(self.lib.pxb_context_set_cloth_variant(self.h, variant), "set_cloth_variant")
 
@@ -588,6 +621,33 @@ class Context:
         awake = np.zeros(n, np.uint8)
         self._check(self.lib.pxb_cloths_step_frame(self.h, C.byref(d), A.ptr(awake)), "step_frame")
         return awake
+
+    def step_strands_frame(self, ids, colliders=None, collider_moving=None, gravity=(0, 0, -9.81), sources=None,
+                           fixed_dt=1.0 / 60.0, cloth_substeps=4, cloth_iterations=10, dt=1.0 / 60.0):
+        """pxb_strands_step_frame: root-moved wake, sleep gate, solve, sleep bookkeeping. Returns
+        each set's awake flag after the frame."""
+        ids = np.ascontiguousarray(ids, np.uint64)
+        n = len(ids)
+        cols, coff = _flatten(colliders, A.COLLIDER, n)
+        src, soff = _flatten(sources, A.GRAVITY_SOURCE, n)
+        mov = None if collider_moving is None else np.ascontiguousarray(collider_moving, np.uint8)
+        d = A.StrandFrameDesc()
+        d.sets, d.n_sets = A.ptr(ids), n
+        d.colliders, d.collider_offsets, d.collider_moving = A.ptr(cols), A.ptr(coff), A.ptr(mov)
+        d.gravity = _vec(gravity)
+        d.sources, d.source_offsets = A.ptr(src), A.ptr(soff)
+        d.fixed_dt, d.cloth_substeps, d.cloth_iterations, d.dt = fixed_dt, cloth_substeps, cloth_iterations, dt
+        awake = np.zeros(n, np.uint8)
+        self._check(self.lib.pxb_strands_step_frame(self.h, C.byref(d), A.ptr(awake)), "strands_step_frame")
+        return awake
+
+    def read_strand_sleep_state(self, ids):
+        ids = np.ascontiguousarray(ids, np.uint64)
+        awake = np.zeros(len(ids), np.uint8)
+        timer = np.zeros(len(ids), np.float32)
+        self._check(self.lib.pxb_strands_read_sleep_state(self.h, A.ptr(ids), len(ids), A.ptr(awake), A.ptr(timer)),
+                    "strands_read_sleep_state")
+        return awake, timer
 
     def state_hash(self, ids, seed=1469598103934665603):
         """pxb_cloths_state_hash: world_state_hash's cloth part, continued from `seed`."""

@@ -67,6 +67,8 @@ def oracle():
         lib.orc_set_strand_roots.argtypes = [C.POINTER(OrcStrandSet), P, A.u32, P, A.u32]
         lib.orc_world_step_cloth.argtypes = [C.POINTER(OrcCloth), P, A.u32, C.c_int, P, A.u32, f32p, P, A.u32,
                                              A.f32, A.u32, A.u32, A.f32, C.POINTER(C.c_int), C.POINTER(A.f32)]
+        lib.orc_world_step_strands.argtypes = [C.POINTER(OrcStrandSet), C.c_int, P, A.u32, f32p, P, A.u32,
+                                               A.f32, A.u32, A.u32, A.f32, C.POINTER(C.c_int), C.POINTER(A.f32)]
         lib.orc_geometry_set_hull.argtypes = [A.u32, C.POINTER(A.HullDesc)]
         lib.orc_geometry_set_mesh.argtypes = [A.u32, C.POINTER(A.MeshDesc)]
         lib.orc_geometry_clear.argtypes = []
@@ -228,6 +230,28 @@ def oracle_step_strands(s: StrandArrays, colliders=None, gravity=(0, 0, -9.81), 
     s.time = o.time
     s.bounds = np.array(list(o.bounds_min) + list(o.bounds_max), np.float32)
     return s
+
+
+def oracle_world_step_strands(s: StrandArrays, state, colliders=None, collider_moving=False, gravity=(0, 0, -9.81),
+                              sources=None, fixed_dt=1.0 / 60.0, cloth_substeps=4, cloth_iterations=10,
+                              dt=1.0 / 60.0):
+    """One PhysicsWorld::step_strands_ frame of the oracle for one set (root-moved wake, sleep
+    gate, solve, sleep bookkeeping). state: dict with "awake" and "sleep_timer", updated. Returns 1
+    when the set was solved, 0 when it slept."""
+    o = _orc_strands(s)
+    cols = colliders if colliders is not None else np.zeros(0, A.COLLIDER)
+    src = sources if sources is not None else np.zeros(0, A.GRAVITY_SOURCE)
+    awake = C.c_int(int(state["awake"]))
+    timer = A.f32(state["sleep_timer"])
+    r = oracle().orc_world_step_strands(C.byref(o), int(collider_moving), A.ptr(cols), len(cols), vec(gravity),
+                                        A.ptr(src), len(src), fixed_dt, cloth_substeps, cloth_iterations, dt,
+                                        C.byref(awake), C.byref(timer))
+    assert r >= 0, "oracle refused the input"
+    state["awake"], state["sleep_timer"] = int(awake.value), np.float32(timer.value)
+    if r == 1:
+        s.time = o.time
+        s.bounds = np.array(list(o.bounds_min) + list(o.bounds_max), np.float32)
+    return r
 
 
 def oracle_set_strand_roots(s: StrandArrays, positions, orientations=None):

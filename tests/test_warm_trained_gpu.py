@@ -1,0 +1,105 @@
+"""The learned warm start with a network trained by the library's own kernels, against the plain
+20-iteration solver it replaces.
+
+The network is trained (pxb_mlp_train: Adam, lr 1e-3) on rows recorded from the plain solver on
+one seeded batch of sheets, then evaluated on another. At each of several steps along the plain
+solver's trajectory, three copies of every sheet start from the same state and take one step:
+
+* plain: 20 iterations (the residual it ends each substep with sets the cloth's threshold);
+* warm: the trained network's displacement, 4 iterations, then 4 more at a time while the
+  residual (max |len / rest - 1| over the stretch constraints) exceeds the threshold, at most 20;
+* without the network: the same iteration rule from the plain prediction (a network of zeros).
+
+Bars: the warm positions stay within 1e-3 m of the plain ones; each warm substep ends at or below
+its cloth's threshold unless it used all 20 iterations; and the trained network needs fewer
+iterations than the same rule without it -- what the network gains.
+"""
+import numpy as np
+import pytest
+
+from physxcoopa_b200 import _abi as A
+from physxcoopa_b200 import runtime as R
+from physxcoopa_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+PLAIN, WARM = 20, 4
+
+
+def zero_net():
+    z = {"w1": np.zeros((64, 24)), "b1": np.zeros(64), "w2": np.zeros((64, 64)), "b2": np.zeros(64),
+         "w3": np.zeros((3, 64)), "b3": np.zeros(3), "in_mean": np.zeros(24), "in_scale": np.ones(24),
+         "out_scale": np.ones(3)}
+    return A.MlpWeights.from_numpy(**z)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    ctx = R.Context(0)
+    tr = scenes.uneven_batch(n=64, lo=16, hi=64, seed=102, params=scenes.reference_params())
+    ids = [ctx.add_cloth(c) for c in tr.cloths]
+    xs, ys = [], []
+    for step in range(16):
+        x, y = ctx.record(ids, tr.colliders, sources=tr.sources, iterations=PLAIN, substep=step % 4)
+        xs.append(x)
+        ys.append(y)
+    for i in ids:
+        ctx.remove_cloth(i)
+    loss = ctx.mlp_train(np.concatenate(xs), np.concatenate(ys), epochs=30, batch=8192, learning_rate=1e-3, seed=0)
+    yield ctx, ctx.get_mlp(), loss
+    ctx.close()
+
+
+def test_trained_network_within_bar_at_the_residual_and_saves_iterations(trained):
+    ctx, net, loss = trained
+    assert np.isfinite(loss)
+    ev = scenes.uneven_batch(n=24, lo=16, hi=64, seed=7, params=scenes.reference_params())
+    n = len(ev.cloths)
+    plain_ids = [ctx.add_cloth(c) for c in ev.cloths]
+    warm_ids = [ctx.add_cloth(c) for c in ev.cloths]
+    zero_ids = [ctx.add_cloth(c) for c in ev.cloths]
+    dp, dw, dz = (ctx.make_step(ids, ev.colliders, ev.gravity, ev.sources, 4, PLAIN, ev.h)
+                  for ids in (plain_ids, warm_ids, zero_ids))
+    worst, iters_net, iters_zero, capped = 0.0, 0, 0, 0
+    try:
+        for step in range(12):
+            # the warm copies start where the plain one is
+            for p, w, z, c in zip(plain_ids, warm_ids, zero_ids, ev.cloths):
+                state = ctx.read_particles(p, len(c.particles))
+                ctx.write_particles(w, state)
+                ctx.write_particles(z, state)
+            ctx.step_warm_desc(dp[0], warm_iterations=0)  # plain 20, residual measured
+            tau = ctx.read_warm_results(plain_ids)["residual"].astype(np.float32)
+            ctx.set_mlp(net)
+            ctx.step_warm_desc(dw[0], warm_iterations=WARM, thresholds=tau, continue_iterations=True)
+            rw = ctx.read_warm_results(warm_ids)
+            ctx.set_mlp(zero_net())
+            ctx.step_warm_desc(dz[0], warm_iterations=WARM, thresholds=tau, continue_iterations=True)
+            rz = ctx.read_warm_results(zero_ids)
+            for k in range(n):
+                m = len(ev.cloths[k].particles)
+                a = ctx.read_particles(plain_ids[k], m)["position"].astype(np.float64)
+                b = ctx.read_particles(warm_ids[k], m)["position"].astype(np.float64)
+                worst = max(worst, float(np.abs(a - b).max()))
+            used_w = WARM * rw["substeps"] + rw["extra_iterations"]
+            used_z = WARM * rz["substeps"] + rz["extra_iterations"]
+            iters_net += int(used_w.sum())
+            iters_zero += int(used_z.sum())
+            # a warm cloth ends its step at or below its threshold, unless one of its substeps
+            # kept iterating to the plain count (the reported residual is the substeps' largest)
+            may_cap = rw["extra_iterations"] >= PLAIN - WARM
+            ok = (rw["residual"] <= tau) | may_cap
+            capped += int((~(rw["residual"] <= tau)).sum())
+            assert np.all(ok), (step, rw, tau)
+        substeps = 12 * 4 * n
+        print(f"\nwarm start on {n} sheets x 12 steps: max |warm - plain| {worst:.3g} m; iterations per substep "
+              f"with the trained network {iters_net / substeps:.2f}, without it {iters_zero / substeps:.2f}, "
+              f"plain {PLAIN}; warm steps ending above the threshold after all {PLAIN} iterations: {capped}; "
+              f"training loss {loss:.4g}")
+        assert worst <= 1e-3
+        assert iters_net < iters_zero
+        assert iters_net < PLAIN * substeps
+    finally:
+        for ids in (plain_ids, warm_ids, zero_ids):
+            for i in ids:
+                ctx.remove_cloth(i)

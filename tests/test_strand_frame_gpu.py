@@ -25,7 +25,7 @@ def roots_of(lines, offset):
 
 def test_strand_frames_wake_sleep_and_equal_the_oracle():
     ctx = R.Context(0)
-    sleepy = dict(local_shape=0.0, global_shape=0.5, damping=6.0, sleep_threshold=0.05, sleep_time=0.25)
+    sleepy = dict(local_shape=0.0, global_shape=0.5, damping=6.0, sleep_threshold=0.1, sleep_time=0.25)
     lines_a = [straight((0.03 * i, 0.0, 1.0), 14, 0.02) for i in range(6)]      # roots driven along x
     lines_b = [straight((0.0, 0.5 + 0.03 * i, 1.0), 10, 0.02) for i in range(4)]  # still roots; a collider
     lines_c = [straight((1.0, 0.0, 1.0), 40, 0.01)]                              # long strand, gravity source
@@ -37,15 +37,15 @@ def test_strand_frames_wake_sleep_and_equal_the_oracle():
     src_c = gravity_sources([((1.0, 0.0, -2.0), 9.81, 1.0, 10.0)])
     slept, woke = set(), set()
     try:
-        for f in range(150):
-            # set A: its roots slide for the first 20 frames and again from frame 110
-            if f < 20 or f >= 110:
-                x = 0.004 * min(f, 20) + (0.01 * (f - 109) if f >= 110 else 0.0)
-                pos = roots_of(lines_a, (x, 0.0, 0.0))
-                ctx.set_strand_roots(ids[0], pos)
-                K.oracle_set_strand_roots(orcs[0], pos)
+        for f in range(180):
+            # set A: the engine sets its roots every frame (set_strand_roots, from the scalp's
+            # transform); they slide for the first 10 frames and again from frame 150
+            x = 0.004 * min(f, 10) + (0.01 * (f - 149) if f >= 150 else 0.0)
+            pos = roots_of(lines_a, (x, 0.0, 0.0))
+            ctx.set_strand_roots(ids[0], pos)
+            K.oracle_set_strand_roots(orcs[0], pos)
             cols = [None, collider_array([sphere(0.05, (0.02, 0.55, 0.85))]), None]
-            moving = [0, 1 if f in (90, 91) else 0, 0]
+            moving = [0, 1 if f in (120, 121) else 0, 0]
             awake = ctx.step_strands_frame(ids, colliders=cols, collider_moving=moving,
                                            sources=[None, None, src_c], fixed_dt=FIXED_DT, cloth_substeps=4,
                                            cloth_iterations=6, dt=FIXED_DT)

@@ -97,6 +97,8 @@ def parse():
                     help="step through the captured CUDA graph (pxb_cloths_step_graph) instead of pxb_cloths_step")
     ap.add_argument("--variant", type=int, default=None,
                     help="fix the kernel variant (0/1/2) instead of autotuning")
+    ap.add_argument("--launch", choices=["queue", "cta"], default="queue",
+                    help="with --variant: persistent work-queue kernels (queue) or one CTA per cloth (cta)")
     return ap.parse_args()
 
 
@@ -745,11 +747,16 @@ def main():
 
     if args.variant is None:
         best, ms = ctx.autotune(d, trials=2)
-        tune = {"chosen_variant": best, "ms_per_step_by_variant": ms,
-                "variants": "block-size cap 512 / 768 / 1024 threads"}
+        tune = {"chosen": {"block_cap": [512, 768, 1024][best % 3],
+                           "launch": "persistent work queue" if best >= 3 else "one CTA per cloth"},
+                "ms_per_step": {"one CTA per cloth": ms[:3], "persistent work queue": ms[3:]},
+                "variants": "block-size cap 512 / 768 / 1024 threads x launch form"}
     else:
         ctx.set_cloth_variant(args.variant)
-        tune = {"chosen_variant": args.variant, "fixed": True}
+        ctx.set_launch_mode(1 if args.launch == "queue" else 0)
+        tune = {"chosen": {"block_cap": [512, 768, 1024][args.variant],
+                           "launch": "persistent work queue" if args.launch == "queue" else "one CTA per cloth"},
+                "fixed": True}
     step = ctx.step_graph_desc if args.graph else ctx.step_desc
     W = max(args.warmup, 3)
     for _ in range(W):
@@ -815,7 +822,8 @@ def main():
     res_pinned = [torch.empty(8 * len(ids), dtype=torch.float32, pin_memory=True).numpy().view(A.FRAME_RESULT)
                   for _ in range(2)]
     # pxb_cloths_step uploads one staging block per step: per-cloth step records (200 B),
-    # collider snapshots (312 B), gravity sources (24 B), the launch order (4 B) and the posed
+    # collider snapshots (312 B), gravity sources (24 B), the launch order (4 B), the launch
+    # groups' work-queue counters (4 B per cloth at most) and the posed
     # convex hulls (16 B x (2 faces + 2 face-vertex entries) per distinct hull and pose), each
     # section padded to 256 B.
     al = lambda x: (x + 255) & ~255
@@ -834,7 +842,7 @@ def main():
                     g = sc.geometries[gids.index(int(c["geometry"]))]
                     hull_bytes += 16 * (2 * len(g.face_planes) + 2 * len(g.face_vertices))
     h2d = (al(200 * len(ids)) + al(312 * max(n_col, 1)) + al(24 * max(n_src, 1)) + al(4 * len(ids))
-           + al(hull_bytes))
+           + al(4 * len(ids)) + al(hull_bytes))
     d2h = 12 * sc.vertices + 32 * len(ids) + 4
     ctx.synchronize()
 

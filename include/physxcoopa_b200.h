@@ -493,10 +493,21 @@ pxb_status pxb_context_set_cloth_variant(pxb_context* ctx, int32_t variant);
  * meaningless -- rewrite it (pxb_cloth_write_particles) or re-add the cloth. The context stays
  * usable: restore the defaults with (1 << 22, 0). */
 pxb_status pxb_context_set_wait_test(pxb_context* ctx, uint32_t grid_wait_polls, uint32_t unreachable);
-/* Autotuner: times every kernel variant on `step` (the caller's real batch, `trials` launches
- * each after one warm-up) and keeps the fastest on the context. The listed cloths' device state
- * and host mirrors are saved first and restored after, so tuning does not advance them.
- * variant_out and ms_out (one entry per variant, milliseconds per step) may be NULL. */
+/* Launch form of pxb_cloths_step (no counterpart in the reference, whose step_cloths_ walks its
+ * cloths one after another). Cloths are grouped by layout and launched largest first. Mode 1
+ * (default): each group runs as a persistent kernel, as many CTAs (clusters) as the SMs hold,
+ * each popping the group's next cloth from a device work queue (one atomic per cloth) until the
+ * queue is empty. Mode 0: one CTA (cluster) per cloth, the hardware scheduler handing them out.
+ * Results are identical; only speed differs. */
+pxb_status pxb_context_set_launch_mode(pxb_context* ctx, int32_t mode);
+/* Autotuner: times every kernel variant in both launch forms on `step` (the caller's real batch,
+ * `trials` launches each after one warm-up) and keeps the fastest pair on the context. The
+ * listed cloths' device state and host mirrors are saved first and restored after, so tuning
+ * does not advance them. variant_out (may be NULL) receives variant + 3 * mode of the pair kept;
+ * ms_out (may be NULL) six entries, milliseconds per step: variants 0-2 one CTA per cloth, then
+ * variants 0-2 persistent. The threads a constraint colour runs with follow the block size;
+ * iterations are never fused between barriers (the reference's Gauss-Seidel order needs one
+ * after every colour). */
 pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step, uint32_t trials,
                                int32_t* variant_out, float* ms_out);
 

@@ -409,13 +409,13 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
                               const pxb_gravity_source* sources, const int32_t* order,
                               PxbFrameResult* results, uint32_t* err, int n_cloths, int threads,
                               int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres, int ext) {
+                              const unsigned char* mlp, PxbWarmResult* wres, int ext, int* queue, int persistent_units) {
     if (n_cloths <= 0) return cudaSuccess;
-    if (ext == 3 || ext == 4) return launch_cloth_lean(ext == 4, variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-    if (ext == 2) return launch_cloth_gmem(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-    if (ext) return launch_cloth_geo(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-    if (wsteps) return launch_cloth_warm(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-    return launch_cloth_plain(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+    if (ext == 3 || ext == 4) return launch_cloth_lean(ext == 4, variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+    if (ext == 2) return launch_cloth_gmem(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+    if (ext) return launch_cloth_geo(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+    if (wsteps) return launch_cloth_warm(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+    return launch_cloth_plain(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
 }
 
 cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness, const float* pts,

@@ -300,7 +300,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                   const pxb_gravity_source* __restrict__ sources,
                   const int32_t* __restrict__ order, PxbFrameResult* __restrict__ results,
                   uint32_t* __restrict__ err, const PxbWarmStep* __restrict__ wsteps,
-                  const unsigned char* __restrict__ mlp_blob, PxbWarmResult* __restrict__ wres) {
+                  const unsigned char* __restrict__ mlp_blob, PxbWarmResult* __restrict__ wres,
+                  int* __restrict__ queue, int n_items) {
     extern __shared__ __align__(16) unsigned char smem[];
     // warm-start state: per-rank residuals, the network warpgroups' MMA barriers, TMEM base
     __shared__ float s_resid[PXB_MAX_RANKS];
@@ -318,11 +319,44 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     __shared__ float s_base[3];
     __shared__ float s_run[3];
 
+    __shared__ int s_slot;
+
     const int tid = threadIdx.x;
     const int T = blockDim.x;
     int rank = 0;
     if constexpr (CL > 1) rank = static_cast<int>(cg::this_cluster().block_rank());
-    const int slot = blockIdx.x / CL;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        if constexpr (kWarm)
+            for (int g = 0; g < kWarmGroups; ++g) tc::mbar_init(&s_wbar[g], 1);
+        fence_proxy_async();
+    }
+    // barrier parities live as long as the CTA: a persistent CTA stages cloth after cloth
+    uint32_t wphase = 0;       // parity of this thread's network-warpgroup MMA barrier
+    uint32_t stage_phase = 1;  // parity of the staging barrier's last completed phase
+
+    // One cloth per CTA (cluster), or, with a work queue, cloth after cloth: the queue holds
+    // the launch group's cloths in decreasing size (the runtime's order), rank 0 pops the next
+    // with one atomic and hands it to the cluster; every pop returns, so the loop is bounded
+    // by n_items.
+    for (int item = 0;; ++item) {
+    int slot;
+    if (queue == nullptr) {
+        if (item > 0) break;
+        slot = blockIdx.x / CL;
+    } else {
+        if (rank == 0 && tid == 0) {
+            const int v = atomicAdd(queue, 1);
+            if constexpr (CL > 1) {
+                for (int q = 0; q < CL; ++q) *cg::this_cluster().map_shared_rank(&s_slot, q) = v;
+            } else {
+                s_slot = v;
+            }
+        }
+        cluster_or_block_sync<CL>();
+        slot = s_slot;
+        if (slot >= n_items) break;
+    }
     {
         const int ci = __ldg(&order[slot]);
         const int* srcC = reinterpret_cast<const int*>(&cloths[ci]);
@@ -331,12 +365,6 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         const int* srcP = reinterpret_cast<const int*>(&stepp[slot]);
         int* dstP = reinterpret_cast<int*>(&sP);
         for (int i = tid; i < static_cast<int>(sizeof(PxbClothStep) / 4); i += T) dstP[i] = srcP[i];
-    }
-    if (tid == 0) {
-        mbar_init(&bar, 1);
-        if constexpr (kWarm)
-            for (int g = 0; g < kWarmGroups; ++g) tc::mbar_init(&s_wbar[g], 1);
-        fence_proxy_async();
     }
     __syncthreads();
 
@@ -380,7 +408,11 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
     // A staging wait that runs out records the error and carries on: leaving early would strand
     // the other ranks of the cluster at their barriers.
-    const bool staged = kG || mbar_wait_bounded(&bar, 0);
+    bool staged = true;
+    if (!kG) {
+        stage_phase ^= 1u;
+        staged = mbar_wait_bounded(&bar, stage_phase);
+    }
     if (!staged && tid == 0) atomicOr(err, PXB_DEVERR_TMA_TIMEOUT);
     __syncthreads();
 
@@ -536,8 +568,6 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         cluster_or_block_sync<CL>();  // s_red / s_resid free again
         return m;
     };
-    uint32_t wphase = 0;   // parity of this thread's network-warpgroup MMA barrier
-    uint32_t stage_phase = 0;  // parity of the staging barrier's last completed phase
     float w_resid = 0.0f;  // max residual over the step's substeps
     int w_fallbacks = 0;
     int w_extra = 0;       // iterations run after the warm ones
@@ -1058,7 +1088,10 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         out->max_speed = sqrtf(r[6]);
         out->time = 0.0f;
     }
-    if constexpr (CL > 1) cg::this_cluster().sync();  // no rank leaves while its memory is read
+    // no rank leaves (or takes the next cloth) while its memory is read; no thread overwrites
+    // the cloth's shared state before every thread is done with it
+    cluster_or_block_sync<CL>();
+    }  // cloth loop
 }
 
 template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false, bool kLean = false>
@@ -1066,7 +1099,8 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
                                   const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                   const int32_t* order, PxbFrameResult* results, uint32_t* err,
                                   int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
-                                  const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres) {
+                                  const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres,
+                                  int* queue, int persistent_units) {
     static uint64_t configured = 0;  // one bit per device the attributes have been set on
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -1081,8 +1115,11 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
         if (e != cudaSuccess) return e;
         configured |= 1ull << dev;
     }
+    // one CTA (cluster) per cloth, or persistent_units of them popping cloths from `queue`
+    const bool persistent = queue != nullptr && persistent_units > 0 && persistent_units < n_cloths;
+    const int units = persistent ? persistent_units : n_cloths;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(static_cast<unsigned>(n_cloths * CL));
+    cfg.gridDim = dim3(static_cast<unsigned>(units * CL));
     cfg.blockDim = dim3(static_cast<unsigned>(threads));
     cfg.dynamicSmemBytes = static_cast<size_t>(smem_bytes);
     cfg.stream = stream;
@@ -1094,7 +1131,7 @@ static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep*
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, cloth_step_kernel<kMaxThreads, CL, kWarm, kExt, kGmem, kLean>, cloths, steps, colliders,
-                              sources, order, results, err, wsteps, mlp, wres);
+                              sources, order, results, err, wsteps, mlp, wres, persistent ? queue : nullptr, n_cloths);
 }
 
 template <int kMaxThreads, bool kWarm, bool kExt>
@@ -1102,12 +1139,12 @@ static cudaError_t launch_cl(int cluster, const PxbClothDev* cloths, const PxbCl
                              const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                              const int32_t* order, PxbFrameResult* results, uint32_t* err,
                              int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
-                             const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres) {
+                             const PxbWarmStep* wsteps, const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units) {
     switch (cluster) {
-        case 1: return launch_variant<kMaxThreads, 1, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 2: return launch_variant<kMaxThreads, 2, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 4: return launch_variant<kMaxThreads, 4, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 8: return launch_variant<kMaxThreads, 8, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 1: return launch_variant<kMaxThreads, 1, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+        case 2: return launch_variant<kMaxThreads, 2, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+        case 4: return launch_variant<kMaxThreads, 4, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+        case 8: return launch_variant<kMaxThreads, 8, kWarm, kExt>(cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1117,27 +1154,27 @@ cudaError_t launch_cloth_plain(int variant, int cluster, const PxbClothDev* clot
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
                               int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres);
+                              const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units);
 cudaError_t launch_cloth_warm(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
                               int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres);
+                              const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units);
 cudaError_t launch_cloth_geo(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
                               int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres);
+                              const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units);
 cudaError_t launch_cloth_lean(bool ext, int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
                               int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres);
+                              const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units);
 cudaError_t launch_cloth_gmem(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
                               int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres);
+                              const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units);
 
 }  // namespace pxb
 

@@ -8,12 +8,12 @@ cudaError_t launch_cloth_plain(int variant, int cluster, const PxbClothDev* clot
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
                               int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
-                              const unsigned char* mlp, PxbWarmResult* wres) {
+                              const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units) {
     if (threads > cloth_variant_threads(variant)) threads = cloth_variant_threads(variant);
     switch (variant) {
-        case 0: return launch_cl<512, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        case 1: return launch_cl<768, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
-        default: return launch_cl<1024, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres);
+        case 0: return launch_cl<512, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+        case 1: return launch_cl<768, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
+        default: return launch_cl<1024, false, false>(cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
     }
 }
 

@@ -28,12 +28,16 @@ int cloth_variant_registers(int variant);
 // residual measured, or recording only). ext: 0 the plain kernel, 1 with the mesh / hull,
 // self-collision and general-topology stages, 2 general topology with the state in HBM, 3 and 4
 // the lean instantiations of 0 and 1 (rest lengths and lambdas in HBM; one CTA or two).
+// queue / persistent_units: with a zeroed counter and a unit count below n_cloths, that many
+// CTAs (clusters) stay resident and pop the group's cloths from the counter, largest first;
+// else one CTA (cluster) per cloth.
 cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err,
                               int n_cloths, int threads, int smem_bytes, cudaStream_t stream,
                               const PxbWarmStep* wsteps = nullptr, const unsigned char* mlp = nullptr,
-                              PxbWarmResult* wres = nullptr, int ext = 0);
+                              PxbWarmResult* wres = nullptr, int ext = 0, int* queue = nullptr,
+                              int persistent_units = 0);
 
 // Warm-start kernel: network warpgroups per CTA and the shared memory they borrow from the
 // lambda region (weights blob, then per warpgroup an input and an activation tile).

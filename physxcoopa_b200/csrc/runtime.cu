@@ -1204,9 +1204,11 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     const size_t b_src = sizeof(pxb_gravity_source) * std::max<uint32_t>(n_src, 1);
     const size_t b_order = sizeof(int32_t) * n;
     const size_t b_warm = warm ? sizeof(PxbWarmStep) * n : 0;
+    const size_t b_queue = sizeof(int32_t) * n;  // one work-queue counter per launch group (at most n)
     const size_t o_cols = align256(b_steps), o_src = o_cols + align256(b_cols),
-                 o_order = o_src + align256(b_src), o_warm = o_order + align256(b_order),
-                 o_geo = o_warm + align256(b_warm), total = o_geo + align256(cstage.bytes());
+                 o_order = o_src + align256(b_src), o_queue = o_order + align256(b_order),
+                 o_warm = o_queue + align256(b_queue), o_geo = o_warm + align256(b_warm),
+                 total = o_geo + align256(cstage.bytes());
     if (pxb_status s = grow_pinned(total)) return s;
     if (pxb_status s = grow(d_stage, total, "step staging")) return s;
     if (pxb_status s = grow(d_results, sizeof(PxbFrameResult) * n, "results")) return s;
@@ -1217,6 +1219,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     auto* hs_src = reinterpret_cast<pxb_gravity_source*>(hb + o_src);
     auto* hs_order = reinterpret_cast<int32_t*>(hb + o_order);
     auto* hs_warm = reinterpret_cast<PxbWarmStep*>(hb + o_warm);
+    std::memset(hb + o_queue, 0, b_queue);  // every group's queue starts at its first cloth
     cstage.fill(this, sd->colliders, n_col, hs_cols, reinterpret_cast<float4*>(hb + o_geo),
                 reinterpret_cast<const float4*>(static_cast<char*>(d_stage.p) + o_geo));
     if (n_src) std::memcpy(hs_src, sd->sources, sizeof(pxb_gravity_source) * n_src);
@@ -1363,13 +1366,13 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
             ++enqueued;
         }
     }
-    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; int ext; };
+    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; int ext; int fit; };
     std::vector<Group> groups;
     for (uint32_t g0 = 0; g0 < n_plain;) {
         const int cluster = static_cast<int>(ents[perm[g0]]->ranks.size());
         const int group_fit = fit[perm[g0]];
         const int ext = has_geo[perm[g0]];
-        Group G{g0, g0, cluster, 64, 0, 0.0, ext};
+        Group G{g0, g0, cluster, 64, 0, 0.0, ext, group_fit};
         while (G.g1 < n_plain && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster &&
                fit[perm[G.g1]] == group_fit && has_geo[perm[G.g1]] == ext) {
             const ClothEntry& e = *ents[perm[G.g1]];
@@ -1383,6 +1386,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     }
     std::stable_sort(groups.begin(), groups.end(), [](const Group& a, const Group& b) { return a.work > b.work; });
     const bool fan_out = groups.size() > 1;
+    // the persistent form (launch_mode 1): a group's CTAs stay resident and pop its cloths
+    const bool persistent = launch_mode == 1;
     if (fan_out) {
         if (pxb_status s = cuda(cudaEventRecord(fork, stream), "fork")) return s;
         for (int k = 0; k < std::min<int>(kSideStreams, static_cast<int>(groups.size())); ++k)
@@ -1400,7 +1405,9 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                                            static_cast<int>(G.g1 - G.g0), G.threads, G.smem, st,
                                            warm ? reinterpret_cast<const PxbWarmStep*>(db + o_warm) + G.g0 : nullptr,
                                            warm && warm->warm_iters > 0 ? static_cast<const unsigned char*>(d_mlp.p) : nullptr,
-                                           warm ? static_cast<PxbWarmResult*>(d_wresults.p) + G.g0 : nullptr, G.ext);
+                                           warm ? static_cast<PxbWarmResult*>(d_wresults.p) + G.g0 : nullptr, G.ext,
+                                           persistent ? reinterpret_cast<int*>(db + o_queue) + gi : nullptr,
+                                           persistent ? std::max(1, n_sms * std::max(G.fit, 1) / G.cluster) : 0);
         if (le != cudaSuccess) return cuda(le, "launch cloth_step");
         ++enqueued;
     }
@@ -1944,6 +1951,13 @@ pxb_status pxb_context_set_wait_test(pxb_context* ctx, uint32_t grid_wait_polls,
     return PXB_OK;
 }
 
+pxb_status pxb_context_set_launch_mode(pxb_context* ctx, int32_t mode) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    if (mode != 0 && mode != 1) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "launch mode must be 0 or 1");
+    ctx->launch_mode = mode;
+    return PXB_OK;
+}
+
 pxb_status pxb_context_set_cloth_variant(pxb_context* ctx, int32_t variant) {
     if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
     if (variant < 0 || variant >= kClothVariants)
@@ -2001,12 +2015,13 @@ pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
-    const int before = ctx->cloth_variant;
-    int best = before;
+    const int before = ctx->cloth_variant, before_mode = ctx->launch_mode;
+    int best = before + kClothVariants * before_mode;
     float best_ms = 0.0f;
     pxb_status st = PXB_OK;
-    for (int v = 0; v < kClothVariants && !st; ++v) {
-        ctx->cloth_variant = v;
+    for (int v = 0; v < 2 * kClothVariants && !st; ++v) {
+        ctx->cloth_variant = v % kClothVariants;
+        ctx->launch_mode = v / kClothVariants;
         st = ctx->step_cloths(step);  // warm-up (and attribute set-up) of this variant
         if (st) break;
         cudaEventRecord(t0, ctx->stream);
@@ -2028,7 +2043,8 @@ pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step
     if (!rs) rs = ctx->check_device_error();
     ctx->results_fresh = false;
     ctx->last_step.clear();
-    ctx->cloth_variant = st ? before : best;
+    ctx->cloth_variant = st ? before : best % kClothVariants;
+    ctx->launch_mode = st ? before_mode : best / kClothVariants;
     if (st) return st;
     if (rs) return rs;
     if (variant_out) *variant_out = best;

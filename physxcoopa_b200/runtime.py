@@ -87,6 +87,7 @@ SIGNATURES = {
     "pxb_check_quotient_significands": ([P, u32, u32, C.POINTER(u64)], C.c_int),
     "pxb_check_projections": ([P, u64, u64, C.POINTER(u64), C.POINTER(f32)], C.c_int),
     "pxb_context_set_cloth_variant": ([P, C.c_int32], C.c_int),
+    "pxb_context_set_launch_mode": ([P, C.c_int32], C.c_int),
     "pxb_context_set_wait_test": ([P, u32, u32], C.c_int),
     "pxb_strands_add": ([P, C.POINTER(A.StrandSetDesc), C.POINTER(u64)], C.c_int),
     "pxb_strands_remove": ([P, u64], C.c_int),
@@ -535,13 +536,18 @@ class Context:
         self._check(self.lib.pxb_context_set_wait_test(self.h, grid_wait_polls, 1 if unreachable else 0),
                     "set_wait_test")
 
+    def set_launch_mode(self, mode):
+        """pxb_context_set_launch_mode: 1 persistent work-queue kernels, 0 one CTA per cloth."""
+        self._check(self.lib.pxb_context_set_launch_mode(self.h, mode), "set_launch_mode")
+
     def set_cloth_variant(self, variant):
         self._check(self.lib.pxb_context_set_cloth_variant(self.h, variant), "set_cloth_variant")
 
     def autotune(self, d, trials=3):
-        """Times the kernel variants on step desc `d` (state restored); returns (best, ms list)."""
+        """Times the kernel variants in both launch forms on step desc `d` (state restored);
+        returns (best = variant + 3 * launch mode, ms list of six)."""
         best = C.c_int32()
-        ms = (C.c_float * 3)()
+        ms = (C.c_float * 6)()
         self._check(self.lib.pxb_cloths_autotune(self.h, C.byref(d), trials, C.byref(best), ms),
                     "autotune")
         return best.value, list(ms)

@@ -188,21 +188,26 @@ def test_gravity_sources_equal_oracle(ctx):
 
 
 def test_kernel_variants_agree_and_autotune_restores_state(ctx):
+    """Every block-size variant in both launch forms (one CTA per cloth; persistent CTAs popping
+    a work queue) gives the same bits; the autotuner leaves the cloths where they were."""
     sc = scenes.uniform_batch(n=6, side=40, seed=4)
     outs = []
-    for variant in range(3):
-        ids = [ctx.add_cloth(c) for c in sc.cloths]
-        ctx.set_cloth_variant(variant)
-        for _ in range(5):
-            ctx.step(ids, sc.colliders)
-        outs.append([ctx.read_particles(i, len(c.particles)).tobytes() for i, c in zip(ids, sc.cloths)])
-        for i in ids:
-            ctx.remove_cloth(i)
-    assert outs[0] == outs[1] == outs[2]
+    for mode in (0, 1):
+        for variant in range(3):
+            ids = [ctx.add_cloth(c) for c in sc.cloths]
+            ctx.set_cloth_variant(variant)
+            ctx.set_launch_mode(mode)
+            for _ in range(5):
+                ctx.step(ids, sc.colliders)
+            outs.append([ctx.read_particles(i, len(c.particles)).tobytes() for i, c in zip(ids, sc.cloths)])
+            for i in ids:
+                ctx.remove_cloth(i)
+    assert all(o == outs[0] for o in outs)
+    ctx.set_launch_mode(1)
     ids = [ctx.add_cloth(c) for c in sc.cloths]
     d, keep = ctx.make_step(ids, sc.colliders)
     best, ms = ctx.autotune(d, trials=2)
-    assert best in (0, 1, 2) and all(m > 0 for m in ms)
+    assert best in range(6) and len(ms) == 6 and all(m > 0 for m in ms)
     for i, c in zip(ids, sc.cloths):  # tuning did not advance the cloths
         assert np.array_equal(ctx.read_particles(i, len(c.particles))["position"], c.particles["position"])
         assert ctx.read_time(i) == np.float32(c.time)

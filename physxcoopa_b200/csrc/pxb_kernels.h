@@ -61,11 +61,18 @@ int mlp_infer_smem_bytes();
 cudaError_t launch_mlp_infer(const float* X, int n, const unsigned char* blob, float* Y, uint32_t* err,
                              int n_sms, cudaStream_t stream);
 void mlp_pack_blob(const pxb_mlp_weights& m, unsigned char* out);
-// Training (mlp_train.cu): gradients of a batch given as row indices, and an Adam update.
-cudaError_t launch_mlp_grad(const float* X, const float* T, const uint32_t* idx, int rows, const pxb_mlp_weights* W,
-                            pxb_mlp_weights* G, float* loss, cudaStream_t stream);
-cudaError_t launch_mlp_adam(pxb_mlp_weights* W, const pxb_mlp_weights* G, pxb_mlp_weights* M, pxb_mlp_weights* V,
-                            float lr, float b1t, float b2t, cudaStream_t stream);
+// Training (mlp_train.cu), on the tensor cores: gradients of `rows` rows given as indices (part of
+// an optimiser batch of batch_rows rows) as per-CTA partials in `part` (mlp_partial_floats(n_sms)
+// floats); returns the number of CTAs launched (the partials to sum), *status the launch error.
+// Adam (or a plain reduce into G) then sums the partials in CTA order.
+size_t mlp_partial_floats(int n_sms);
+int launch_mlp_grad(const float* X, const float* T, const uint32_t* idx, int rows, int batch_rows,
+                    const pxb_mlp_weights* W, float* part, uint32_t* err, int n_sms, cudaStream_t stream,
+                    cudaError_t* status);
+cudaError_t launch_mlp_adam(const float* part, int n_parts, int n_sms, pxb_mlp_weights* W, pxb_mlp_weights* M,
+                            pxb_mlp_weights* V, float lr, float b1t, float b2t, float* loss, cudaStream_t stream);
+cudaError_t launch_mlp_reduce(const float* part, int n_parts, int n_sms, pxb_mlp_weights* G, float* loss,
+                              cudaStream_t stream);
 
 cudaError_t launch_project_points(const PxbDevCollider* collider, float thickness,
                                   const float* pts, const float* starts, int n, float* out,

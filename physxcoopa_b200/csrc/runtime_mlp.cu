@@ -128,11 +128,11 @@ pxb_status pxb_mlp_train(pxb_context* ctx, const float* features, const float* t
             w.w3[o][i] = static_cast<float>(0.1 * normal01(seed) / std::sqrt(double(kMlpHidden)));
     fit_normalisation(features, targets, n, w);
 
-    // device: X | Y | row order | W | G | M | V | loss
+    // device: X | Y | row order | W | M | V | loss | gradient partials (one block per CTA)
     const size_t bx = sizeof(float) * kMlpIn * n, by = sizeof(float) * 3 * n, bi = sizeof(uint32_t) * n;
-    const size_t bw = sizeof(pxb_mlp_weights);
-    const size_t oy = al256(bx), oi = oy + al256(by), ow = oi + al256(bi), og = ow + al256(bw), om = og + al256(bw),
-                 ov = om + al256(bw), ol = ov + al256(bw), total = ol + 256;
+    const size_t bw = sizeof(pxb_mlp_weights), bp = sizeof(float) * mlp_partial_floats(ctx->n_sms);
+    const size_t oy = al256(bx), oi = oy + al256(by), ow = oi + al256(bi), om = ow + al256(bw), ov = om + al256(bw),
+                 ol = ov + al256(bw), op = ol + 256, total = op + al256(bp);
     DevBuf buf;
     if (pxb_status s = ctx->grow(buf, total, "training buffers")) return s;
     char* b = static_cast<char*>(buf.p);
@@ -140,10 +140,10 @@ pxb_status pxb_mlp_train(pxb_context* ctx, const float* features, const float* t
     auto* Y = reinterpret_cast<float*>(b + oy);
     auto* I = reinterpret_cast<uint32_t*>(b + oi);
     auto* W = reinterpret_cast<pxb_mlp_weights*>(b + ow);
-    auto* G = reinterpret_cast<pxb_mlp_weights*>(b + og);
     auto* M = reinterpret_cast<pxb_mlp_weights*>(b + om);
     auto* V = reinterpret_cast<pxb_mlp_weights*>(b + ov);
     auto* L = reinterpret_cast<float*>(b + ol);
+    auto* part = reinterpret_cast<float*>(b + op);
     cudaStream_t st = ctx->stream;
     pxb_status s = PXB_OK;
     auto chk = [&](cudaError_t e, const char* what) {
@@ -167,9 +167,11 @@ pxb_status pxb_mlp_train(pxb_context* ctx, const float* features, const float* t
         for (uint64_t r0 = 0; r0 < n && !s; r0 += batch) {
             const int rows = static_cast<int>(std::min<uint64_t>(batch, n - r0));
             ++t;
-            chk(cudaMemsetAsync(G, 0, bw, st), "zero gradients");
-            chk(launch_mlp_grad(X, Y, I + r0, rows, W, G, L, st), "launch gradients");
-            chk(launch_mlp_adam(W, G, M, V, lr, std::pow(0.9f, float(t)), std::pow(0.999f, float(t)), st),
+            cudaError_t ge = cudaSuccess;
+            const int parts = launch_mlp_grad(X, Y, I + r0, rows, rows, W, part, ctx->d_err, ctx->n_sms, st, &ge);
+            chk(ge, "launch gradients");
+            chk(launch_mlp_adam(part, parts, ctx->n_sms, W, M, V, lr, std::pow(0.9f, float(t)),
+                                std::pow(0.999f, float(t)), L, st),
                 "launch adam");
             ctx->launches += 2;
         }
@@ -198,9 +200,9 @@ pxb_status pxb_mlp_loss_gradients(pxb_context* ctx, const float* features, const
     if (!ctx->has_mlp) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "no network installed");
     if (n > 0x7FFFFFFFull) return ctx->fail(PXB_ERR_TOO_LARGE, "too many rows");
     const size_t bx = sizeof(float) * kMlpIn * n, by = sizeof(float) * 3 * n, bi = sizeof(uint32_t) * n;
-    const size_t bw = sizeof(pxb_mlp_weights);
+    const size_t bw = sizeof(pxb_mlp_weights), bp = sizeof(float) * mlp_partial_floats(ctx->n_sms);
     const size_t oy = al256(bx), oi = oy + al256(by), ow = oi + al256(bi), og = ow + al256(bw), ol = og + al256(bw),
-                 total = ol + 256;
+                 op = ol + 256, total = op + al256(bp);
     DevBuf buf;
     if (pxb_status s = ctx->grow(buf, total, "gradient buffers")) return s;
     char* b = static_cast<char*>(buf.p);
@@ -217,12 +219,16 @@ pxb_status pxb_mlp_loss_gradients(pxb_context* ctx, const float* features, const
     chk(cudaMemcpyAsync(b + ow, &ctx->mlp, bw, cudaMemcpyHostToDevice, st), "upload weights");
     chk(cudaMemsetAsync(b + og, 0, bw, st), "zero gradients");
     chk(cudaMemsetAsync(b + ol, 0, sizeof(float), st), "zero loss");
-    chk(launch_mlp_grad(reinterpret_cast<float*>(b), reinterpret_cast<float*>(b + oy),
-                        reinterpret_cast<uint32_t*>(b + oi), static_cast<int>(n),
-                        reinterpret_cast<pxb_mlp_weights*>(b + ow), reinterpret_cast<pxb_mlp_weights*>(b + og),
-                        reinterpret_cast<float*>(b + ol), st),
-        "launch gradients");
-    ++ctx->launches;
+    cudaError_t ge = cudaSuccess;
+    auto* part = reinterpret_cast<float*>(b + op);
+    const int parts = launch_mlp_grad(reinterpret_cast<float*>(b), reinterpret_cast<float*>(b + oy),
+                                      reinterpret_cast<uint32_t*>(b + oi), static_cast<int>(n), static_cast<int>(n),
+                                      reinterpret_cast<pxb_mlp_weights*>(b + ow), part, ctx->d_err, ctx->n_sms, st, &ge);
+    chk(ge, "launch gradients");
+    chk(launch_mlp_reduce(part, parts, ctx->n_sms, reinterpret_cast<pxb_mlp_weights*>(b + og),
+                          reinterpret_cast<float*>(b + ol), st),
+        "launch gradient sum");
+    ctx->launches += 2;
     float lsum = 0.0f;
     chk(cudaMemcpyAsync(grads, b + og, bw, cudaMemcpyDeviceToHost, st), "read gradients");
     chk(cudaMemcpyAsync(&lsum, b + ol, sizeof(float), cudaMemcpyDeviceToHost, st), "read loss");

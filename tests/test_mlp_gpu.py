@@ -13,6 +13,7 @@ import pytest
 
 from physxcoopa_b200 import _abi as A
 from physxcoopa_b200 import runtime as R
+from oracle import mlp_oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -91,41 +92,40 @@ def test_deterministic(ctx):
     assert np.array_equal(ctx.mlp_infer(x), ctx.mlp_infer(x))
 
 
-def loss_and_grads_f64(W, x, t):
-    """Float64 restatement of the training loss and its gradients (no bf16 rounding)."""
-    f = {k: np.asarray(v, np.float64) for k, v in W.items()}
-    xn = (x - f["in_mean"]) * f["in_scale"]
-    z1 = xn @ f["w1"].T + f["b1"]
-    s1 = 1 / (1 + np.exp(-z1))
-    h1 = z1 * s1
-    z2 = h1 @ f["w2"].T + f["b2"]
-    s2 = 1 / (1 + np.exp(-z2))
-    h2 = z2 * s2
-    y = h2 @ f["w3"].T + f["b3"]
-    e = y - t / f["out_scale"]
-    n = len(x)
-    loss = (e * e).sum() / (3 * n)
-    dy = 2 * e / (3 * n)
-    g = {"w3": dy.T @ h2, "b3": dy.sum(0)}
-    dz2 = (dy @ f["w3"]) * (s2 * (1 + z2 * (1 - s2)))
-    g["w2"], g["b2"] = dz2.T @ h1, dz2.sum(0)
-    dz1 = (dz2 @ f["w2"]) * (s1 * (1 + z1 * (1 - s1)))
-    g["w1"], g["b1"] = dz1.T @ xn, dz1.sum(0)
-    return loss, g
-
-
-def test_training_gradients_match_float64(ctx):
-    rng = np.random.default_rng(11)
+@pytest.mark.parametrize("n", [1, 300, 40000])
+def test_training_gradients_match_the_oracle(ctx, n):
+    """Loss and gradients from the tensor-core training kernel (BF16 operands, FP32 accumulation
+    in TMEM; 40000 rows = 313 tiles, so CTAs accumulate several tiles) against the oracle's float64
+    restatement with the device's bf16 roundings (bar: 2e-3 of each field's largest gradient
+    worst case, 2e-4 on average), and against the unrounded float64 gradients (5e-2)."""
+    rng = np.random.default_rng(11 + n)
     W = random_weights(rng)
     ctx.set_mlp(A.MlpWeights.from_numpy(**W))
-    x = rng.normal(0, 1, (300, 24)).astype(np.float32)
-    t = (rng.normal(0, 1, (300, 3)) * W["out_scale"]).astype(np.float32)
+    x = rng.normal(0, 1, (n, 24)).astype(np.float32)
+    t = (rng.normal(0, 1, (n, 3)) * W["out_scale"]).astype(np.float32)
     loss, g = ctx.mlp_loss_gradients(x, t)
-    ref_loss, ref = loss_and_grads_f64(W, x.astype(np.float64), t.astype(np.float64))
-    assert abs(loss - ref_loss) <= 1e-5 * max(1.0, ref_loss)
+    ref_loss, ref = mlp_oracle.loss_and_gradients(W, x, t)
+    exact_loss, exact = mlp_oracle.loss_and_gradients(W, x, t, round_bf16=False)
+    assert abs(loss - ref_loss) <= 1e-3 * ref_loss, (loss, ref_loss)
+    assert abs(loss - exact_loss) <= 2e-2 * exact_loss, (loss, exact_loss)
     for k, v in ref.items():
         scale = np.abs(v).max()
-        assert np.abs(g[k] - v).max() <= 1e-4 * scale + 1e-9, k
+        d = np.abs(np.asarray(g[k], np.float64) - v)
+        assert d.max() <= 2e-3 * scale, (k, d.max() / scale)
+        assert d.mean() <= 2e-4 * scale, (k, d.mean() / scale)
+        assert np.abs(np.asarray(g[k], np.float64) - exact[k]).max() <= 5e-2 * np.abs(exact[k]).max(), k
+
+
+def test_training_gradients_are_deterministic(ctx):
+    rng = np.random.default_rng(5)
+    ctx.set_mlp(A.MlpWeights.from_numpy(**random_weights(rng)))
+    x = rng.normal(0, 1, (20000, 24)).astype(np.float32)
+    t = rng.normal(0, 1e-3, (20000, 3)).astype(np.float32)
+    l1, g1 = ctx.mlp_loss_gradients(x, t)
+    l2, g2 = ctx.mlp_loss_gradients(x, t)
+    assert l1 == l2
+    for k in g1:
+        assert np.array_equal(g1[k], g2[k]), k
 
 
 def test_training_fits_a_smooth_map(ctx):

@@ -295,7 +295,9 @@ typedef struct pxb_cloth_plan {
                                  counts the runs) */
     int32_t lean;             /* 1: only the positions in shared memory, rest lengths and lambdas
                                  read in place in HBM (one CTA or two where a full-shared-memory
-                                 layout would need a larger cluster) */
+                                 layout would need a larger cluster); 2: the same on one CTA
+                                 with the positions as float arrays and an index into the
+                                 cloth's distinct inverse masses (pxb_context_set_lean_arrays) */
 } pxb_cloth_plan;
 
 /* Plans a cloth without a context or a GPU: validates it exactly as pxb_cloth_add does and
@@ -500,6 +502,12 @@ pxb_status pxb_context_set_wait_test(pxb_context* ctx, uint32_t grid_wait_polls,
  * queue is empty. Mode 0: one CTA (cluster) per cloth, the hardware scheduler handing them out.
  * Results are identical; only speed differs. */
 pxb_status pxb_context_set_launch_mode(pxb_context* ctx, int32_t mode);
+/* Layout choice for cloths added from now on (no counterpart in the reference). With `enable`
+ * (default), a grid cloth too large for one CTA's shared memory as float4 positions but small
+ * enough as float arrays (12 bytes per particle plus a one-byte index into a table of its
+ * distinct inverse masses; sheets up to 128 x 128) runs on one CTA in that form; with 0 it runs
+ * on a cluster of two CTAs as before. Results are identical; only speed differs. */
+pxb_status pxb_context_set_lean_arrays(pxb_context* ctx, int32_t enable);
 /* Autotuner: times every kernel variant in both launch forms on `step` (the caller's real batch,
  * `trials` launches each after one warm-up) and keeps the fastest pair on the context. The
  * listed cloths' device state and host mirrors are saved first and restored after, so tuning

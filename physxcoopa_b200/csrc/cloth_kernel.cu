@@ -411,6 +411,7 @@ cudaError_t launch_cloth_step(int variant, int cluster, const PxbClothDev* cloth
                               int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
                               const unsigned char* mlp, PxbWarmResult* wres, int ext, int* queue, int persistent_units) {
     if (n_cloths <= 0) return cudaSuccess;
+    if (ext == 5 || ext == 6) return launch_cloth_soa(ext == 6, variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
     if (ext == 3 || ext == 4) return launch_cloth_lean(ext == 4, variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
     if (ext == 2) return launch_cloth_gmem(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);
     if (ext) return launch_cloth_geo(variant, cluster, cloths, steps, colliders, sources, order, results, err, n_cloths, threads, smem_bytes, stream, wsteps, mlp, wres, queue, persistent_units);

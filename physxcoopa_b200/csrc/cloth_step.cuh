@@ -257,6 +257,135 @@ __device__ __forceinline__ void project_run(float4* __restrict__ pos, const floa
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// Positions of a lean one-CTA cloth as three float arrays (PxbClothDev::lean == 2)
+// ------------------------------------------------------------------------------------------
+
+// x, y, z of slot l at x[l], x[n + l], x[2n + l]; its inverse mass is wt[wi[l]] (the cloth's
+// table of distinct values, in shared memory), or, with w_hbm, pos[l].w read in place in HBM.
+// Indexing yields a reference that reads and writes a float4 (x, y, z, inverse mass), so the
+// stages outside the projection read like those of the float4 layout; a write keeps the inverse
+// mass, which no stage changes.
+struct SoaPos {
+    float* x;
+    const uint8_t* wi;
+    const float* wt;
+    const float4* g;
+    int n;
+    bool w_hbm;
+    __device__ __forceinline__ float w(int l) const { return w_hbm ? __ldg(&g[l].w) : wt[wi[l]]; }
+    __device__ __forceinline__ float4 get(int l) const { return make_float4(x[l], x[n + l], x[2 * n + l], w(l)); }
+    __device__ __forceinline__ void set(int l, float4 v) const {
+        x[l] = v.x;
+        x[n + l] = v.y;
+        x[2 * n + l] = v.z;
+    }
+    struct Ref;
+    __device__ __forceinline__ Ref operator[](int l) const;
+};
+
+struct SoaPos::Ref {
+    SoaPos s;
+    int l;
+    __device__ __forceinline__ operator float4() const { return s.get(l); }
+    __device__ __forceinline__ Ref& operator=(float4 v) {
+        s.set(l, v);
+        return *this;
+    }
+    __device__ __forceinline__ Ref& operator=(const Ref& o) {
+        s.set(l, o.s.get(o.l));
+        return *this;
+    }
+};
+
+__device__ __forceinline__ SoaPos::Ref SoaPos::operator[](int l) const { return Ref{*this, l}; }
+
+// Positions from HBM (layout order, float4) into the arrays; each slot's inverse mass becomes
+// its index in the table (binary search over the bit patterns, ascending). A value missing from
+// the table records PXB_DEVERR_BAD_INDEX and takes index 0. Plain loads: the warm start stages
+// from positions this kernel wrote. Called by every thread; the caller synchronises afterwards.
+__device__ __forceinline__ void soa_stage(const SoaPos& P, float* wt_smem, const float4* src,
+                                          const float* __restrict__ wtab, int n_wtab, uint32_t* err, int tid,
+                                          int T) {
+    for (int i = tid; i < n_wtab; i += T) wt_smem[i] = __ldg(&wtab[i]);
+    __syncthreads();
+    uint8_t* wi = const_cast<uint8_t*>(P.wi);
+    for (int l = tid; l < P.n; l += T) {
+        const float4 v = src[l];
+        P.x[l] = v.x;
+        P.x[P.n + l] = v.y;
+        P.x[2 * P.n + l] = v.z;
+        if (!P.w_hbm) {
+            const uint32_t key = __float_as_uint(v.w);
+            int lo = 0, hi = n_wtab - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (__float_as_uint(wt_smem[mid]) < key) lo = mid + 1;
+                else hi = mid;
+            }
+            if (n_wtab == 0 || __float_as_uint(wt_smem[lo]) != key) {
+                atomicOr(err, PXB_DEVERR_BAD_INDEX);
+                lo = 0;
+            }
+            wi[l] = static_cast<uint8_t>(lo);
+        }
+    }
+}
+
+// One colour segment of a lean one-CTA cloth held as arrays: the same items, addresses and
+// arithmetic as project_segment; the inverse masses from the table (kWH false) or from HBM.
+template <bool kWH, bool kLam, int kItems>
+__device__ __forceinline__ void project_segment_soa(const SoaPos& P, const float* __restrict__ rest,
+                                                    float* __restrict__ lamv, int4 h0, int4 h1, float alpha, int tid,
+                                                    int T) {
+    const int count = h0.x, per_row = h0.z, a_base = h0.w;
+    const uint32_t magic = static_cast<uint32_t>(h0.y);
+    const int row_stride = h1.x, d = h1.y;
+    const int n = P.n;
+    float* __restrict__ X = P.x;
+    auto wof = [&](int l) -> float { return kWH ? __ldg(&P.g[l].w) : P.wt[P.wi[l]]; };
+    auto one = [&](int i, int& la, int& lb, float4& a, float4& b, float& r, float& lam, bool& live) {
+        live = i < count;
+        const int ii = live ? i : 0;
+        const int row = seg_row(ii, magic);
+        la = a_base + row * row_stride + (ii - row * per_row);
+        lb = la + d;
+        a = make_float4(X[la], X[n + la], X[2 * n + la], wof(la));
+        b = make_float4(X[lb], X[n + lb], X[2 * n + lb], wof(lb));
+        r = rest[ii];
+        lam = kLam ? lamv[ii] : 0.0f;
+    };
+    auto put = [&](int i, int la, int lb, float4 a, float4 b, float r, float lam, bool live) {
+        float dlambda;
+        if (distance_core<kLam>(a, b, r, lam, alpha, dlambda) && live) {
+            X[la] = a.x; X[n + la] = a.y; X[2 * n + la] = a.z;
+            X[lb] = b.x; X[n + lb] = b.y; X[2 * n + lb] = b.z;
+            if (kLam) lamv[i] = lam + dlambda;
+        }
+    };
+    if constexpr (kItems == 2) {
+        for (int i = tid; i < count; i += 2 * T) {
+            int la0, lb0, la1, lb1;
+            float4 a0, b0, a1, b1;
+            float r0, r1, m0, m1;
+            bool v0, v1;
+            one(i, la0, lb0, a0, b0, r0, m0, v0);
+            one(i + T, la1, lb1, a1, b1, r1, m1, v1);
+            put(i, la0, lb0, a0, b0, r0, m0, v0);
+            put(i + T, la1, lb1, a1, b1, r1, m1, v1);
+        }
+    } else {
+        for (int i = tid; i < count; i += T) {
+            int la, lb;
+            float4 a, b;
+            float r, m;
+            bool v;
+            one(i, la, lb, a, b, r, m, v);
+            put(i, la, lb, a, b, r, m, v);
+        }
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
@@ -293,7 +422,7 @@ __device__ __forceinline__ void cluster_or_block_sync() {
     else __syncthreads();
 }
 
-template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false, bool kLean = false>
+template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false, int kLean = 0>
 __global__ void __launch_bounds__(kMaxThreads, 1)
 cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __restrict__ stepp,
                   const PxbDevCollider* __restrict__ colliders,
@@ -373,14 +502,27 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     constexpr bool kG = kGmem && kExt && CL == 1 && !kWarm;
     // a lean cloth (only positions in shared memory; rest lengths and lambdas read in place in
     // HBM, velocities for the aerodynamic gather too) runs only in the kLean instantiations
-    constexpr bool kL = kLean && CL <= 2 && !kG;
-    if ((sC.topology == 2) != kG || (sC.lean != 0) != kL) {  // every rank of a cluster agrees
+    constexpr bool kL = kLean != 0 && CL <= 2 && !kG;
+    // a lean one-CTA cloth whose positions are three float arrays runs only in the kLean == 2
+    // instantiations
+    constexpr bool kS = kLean == 2 && CL == 1 && !kG;
+    constexpr int kWantLean = kS ? 2 : (kL ? 1 : 0);
+    if ((sC.topology == 2) != kG || sC.lean != kWantLean) {  // every rank of a cluster agrees
         if (tid == 0) atomicOr(err, PXB_DEVERR_BAD_INDEX);
         return;
     }
     const int n_ranks = CL > 1 ? sC.n_ranks : 1;
     const RankView me = rank_view<1>(sC, smem, rank);  // local view, plain shared addresses
-    float4* pos = kG ? sC.pos : me.pos;
+    auto pos = [&]() {
+        if constexpr (kS) {
+            const int n = me.n_local;
+            return SoaPos{reinterpret_cast<float*>(smem), smem + 12 * static_cast<size_t>(n),
+                          reinterpret_cast<const float*>(smem + 12 * static_cast<size_t>(n) + ((n + 15) & ~15)),
+                          sC.pos + me.base, n, sC.n_wtab == 0};
+        } else {
+            return kG ? sC.pos : me.pos;
+        }
+    }();
     float* U = kG ? sC.list_scratch : (kL ? sC.lam_out + sC.rank[rank].lam_off : me.U);
     const int n_local = me.n_local;
     const int base = me.base;
@@ -394,12 +536,14 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }
 
     // --- prologue: stage positions and rest lengths with TMA bulk copies -------------------
-    if (tid == 0 && !kG) {
-        const uint32_t pos_bytes = 16u * static_cast<uint32_t>(n_local);
-        const uint32_t rest_bytes = kL ? 0u : 4u * static_cast<uint32_t>(sC.rank[rank].n_rest_pad);
-        mbar_arrive_expect_tx(&bar, pos_bytes + rest_bytes);
-        bulk_g2s(pos, sC.pos + base, pos_bytes, &bar);
-        if (rest_bytes) bulk_g2s(rest, sC.rest + sC.rank[rank].rest_off, rest_bytes, &bar);
+    if constexpr (!kS) {  // a cloth held as arrays is staged by its threads below
+        if (tid == 0 && !kG) {
+            const uint32_t pos_bytes = 16u * static_cast<uint32_t>(n_local);
+            const uint32_t rest_bytes = kL ? 0u : 4u * static_cast<uint32_t>(sC.rank[rank].n_rest_pad);
+            mbar_arrive_expect_tx(&bar, pos_bytes + rest_bytes);
+            bulk_g2s(pos, sC.pos + base, pos_bytes, &bar);
+            if (rest_bytes) bulk_g2s(rest, sC.rest + sC.rank[rank].rest_off, rest_bytes, &bar);
+        }
     }
     {
         const int sb = sC.rank[rank].seg_begin;
@@ -409,7 +553,9 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     // A staging wait that runs out records the error and carries on: leaving early would strand
     // the other ranks of the cluster at their barriers.
     bool staged = true;
-    if (!kG) {
+    if constexpr (kS) {
+        soa_stage(pos, const_cast<float*>(pos.wt), sC.pos + base, sC.wtab, sC.n_wtab, err, tid, T);
+    } else if (!kG) {
         stage_phase ^= 1u;
         staged = mbar_wait_bounded(&bar, stage_phase);
     }
@@ -478,7 +624,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     const int4* seg4 = reinterpret_cast<const int4*>(s_seg);
     float4* pos_next = nxt_rank.pos;
     auto iterate = [&](int iters) {
-        if constexpr (kExt && CL == 1 && !kWarm) {
+        if constexpr (kExt && CL == 1 && !kWarm && !kS) {
             if (sC.topology != 0) {
                 // general topology: run after run, a block barrier after each; alpha evaluated
                 // as the reference does, compliance / (hs * hs)
@@ -510,10 +656,19 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
                     const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
                     constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
-                    if (h1.w >= 0)
+                    if constexpr (kS) {
+                        if (pos.w_hbm) {
+                            if (h1.w >= 0) project_segment_soa<true, true, kItems>(pos, RG + h1.z, U + h1.w, h0, h1, alpha, tid, T);
+                            else project_segment_soa<true, false, kItems>(pos, RG + h1.z, U, h0, h1, alpha, tid, T);
+                        } else {
+                            if (h1.w >= 0) project_segment_soa<false, true, kItems>(pos, RG + h1.z, U + h1.w, h0, h1, alpha, tid, T);
+                            else project_segment_soa<false, false, kItems>(pos, RG + h1.z, U, h0, h1, alpha, tid, T);
+                        }
+                    } else if (h1.w >= 0) {
                         project_segment<CL, true, kItems>(pos, pos_next, RG + h1.z, U + h1.w, n_local, h0, h1, alpha, tid, T);
-                    else
+                    } else {
                         project_segment<CL, false, kItems>(pos, pos_next, RG + h1.z, U, n_local, h0, h1, alpha, tid, T);
+                    }
                 }
                 // Colours that join rows need every rank to see the others' writes; a pair
                 // of row-local colours only needs this CTA's. The last colour always syncs
@@ -718,15 +873,23 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             float4* __restrict__ gpos = sC.pos;
             // the prediction goes to HBM: the fallback restarts from it, targets are measured from it
             for (int l = tid; l < n_local; l += T) gpos[base + l] = pos[l];
+            // a cloth held as arrays reads its features from HBM and lends the network its
+            // shared memory: every slot is in HBM before either happens
+            if constexpr (kS) __syncthreads();
             if (net || rec) {
                 // With the network, its scratch is the rest lengths plus the lambda region (the
                 // rest lengths are staged again below); recording alone uses the lambda region.
                 uint32_t dyn;
                 asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-                // a lean cloth has nothing after its positions in shared memory: all of it is scratch
-                unsigned char* ub = (net || kL) ? reinterpret_cast<unsigned char*>(rest) : reinterpret_cast<unsigned char*>(U);
-                const int u_cap = (net || kL) ? static_cast<int>(dyn) - 16 * n_local
-                                              : static_cast<int>(dyn) - (16 * n_local + 4 * sC.rank[rank].n_rest_pad);
+                // a lean cloth has nothing after its positions in shared memory: all of it is
+                // scratch; a cloth held as arrays lends the network all of shared memory (its
+                // positions are in HBM, just written, and are staged again afterwards)
+                unsigned char* ub = kS ? smem
+                                       : (net || kL) ? reinterpret_cast<unsigned char*>(rest)
+                                                     : reinterpret_cast<unsigned char*>(U);
+                const int u_cap = kS ? static_cast<int>(dyn)
+                                     : (net || kL) ? static_cast<int>(dyn) - 16 * n_local
+                                                   : static_cast<int>(dyn) - (16 * n_local + 4 * sC.rank[rank].n_rest_pad);
                 int n_wg = (u_cap - kWarmTileOff) / kWarmTileBytes;
                 n_wg = n_wg < T / 128 ? n_wg : T / 128;
                 n_wg = n_wg < kWarmGroups ? n_wg : kWarmGroups;
@@ -764,7 +927,9 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                                 const int cls = j / Q;
                                 const int xx = 4 * (j - cls * Q) + cls;
                                 if (xx < cols && y < rows) {
-                                    const float4 p = pos[l];
+                                    // positions from HBM for a cloth held as arrays: the network's
+                                    // tiles overwrite them in shared memory
+                                    const float4 p = kS ? gpos[gl] : float4(pos[l]);
                                     const float4 q0 = gprv[gl], v = gvel[gl];
                                     x[0] = p.x - q0.x; x[1] = p.y - q0.y; x[2] = p.z - q0.z;
                                     x[3] = v.x; x[4] = v.y; x[5] = v.z;
@@ -777,7 +942,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                                         const int ng = lay(nx, ny, Q, S_);
                                         const int nloc = ng - base;
                                         float4 q;
-                                        if (CL == 1 || (nloc >= 0 && nloc < n_local)) q = pos[nloc];
+                                        if (kS) q = gpos[ng];
+                                        else if (CL == 1 || (nloc >= 0 && nloc < n_local)) q = pos[nloc];
                                         else if (nloc < 0) q = prv_rank.pos[nloc + prv_rank.n_local];
                                         else q = nxt_rank.pos[nloc - n_local];
                                         const float ex = q.x - p.x, ey = q.y - p.y, ez = q.z - p.z;
@@ -823,6 +989,12 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 }
                 // every rank's features are read before any rank moves a particle
                 cluster_or_block_sync<CL>();
+                if constexpr (kS) {
+                    if (net) {  // the prediction back from HBM
+                        soa_stage(pos, const_cast<float*>(pos.wt), gpos + base, sC.wtab, sC.n_wtab, err, tid, T);
+                        __syncthreads();
+                    }
+                }
                 if (net) {
                     for (int l = tid; l < n_local; l += T) {
                         const int gl = base + l;
@@ -880,7 +1052,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             const int col_begin = sP.col_begin, col_count = sP.col_count;
             const float thickness = sP.thickness, inv_hs = sP.inv_hs;
             bool self = false;
-            if constexpr (kExt && CL == 1) {
+            if constexpr (kExt && CL == 1 && !kS) {
                 self = sP.self_collision != 0;
                 if (self) {
                     // 5. tethers on their own: 6. self-collision reads every particle after them
@@ -1019,6 +1191,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     // memory, so it stores with plain coalesced writes instead of the async proxy.
     if constexpr (kG) {
         // the positions never left HBM
+    } else if constexpr (kS) {
+        for (int l = tid; l < n_local; l += T) sC.pos[base + l] = pos[l];
     } else if constexpr (CL == 1) {
         fence_proxy_async();
         __syncthreads();
@@ -1094,7 +1268,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     }  // cloth loop
 }
 
-template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false, bool kLean = false>
+template <int kMaxThreads, int CL, bool kWarm, bool kExt, bool kGmem = false, int kLean = 0>
 static cudaError_t launch_variant(const PxbClothDev* cloths, const PxbClothStep* steps,
                                   const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                                   const int32_t* order, PxbFrameResult* results, uint32_t* err,
@@ -1170,6 +1344,11 @@ cudaError_t launch_cloth_lean(bool ext, int variant, int cluster, const PxbCloth
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
                               int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
                               const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units);
+cudaError_t launch_cloth_soa(bool ext, int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
+                             const PxbDevCollider* colliders, const pxb_gravity_source* sources,
+                             const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,
+                             int threads, int smem_bytes, cudaStream_t stream, const PxbWarmStep* wsteps,
+                             const unsigned char* mlp, PxbWarmResult* wres, int* queue, int persistent_units);
 cudaError_t launch_cloth_gmem(int variant, int cluster, const PxbClothDev* cloths, const PxbClothStep* steps,
                               const PxbDevCollider* colliders, const pxb_gravity_source* sources,
                               const int32_t* order, PxbFrameResult* results, uint32_t* err, int n_cloths,

@@ -109,9 +109,17 @@ struct PxbClothDev {
     float* list_scratch;        // topology 2: lambdas / parked velocities in HBM, max(pad, 3 n_layout)
     int32_t ref_columns;        // Cloth::columns as given: self-collision's 1-ring exemption reads it
     // 1: a lean grid cloth: only positions in shared memory, its rest lengths and lambdas read in
-    // place in HBM (rest + rank.rest_off, lam_out + rank.lam_off), velocities too; one or two CTAs
+    // place in HBM (rest + rank.rest_off, lam_out + rank.lam_off), velocities too; one or two CTAs.
+    // 2: the same on one CTA with the positions held as three float arrays (x, y, z) and one byte
+    // per slot indexing wtab, the cloth's distinct inverse masses in ascending bit order
+    // (n_wtab <= PXB_MAX_WTAB of them); n_wtab == 0 reads the inverse masses in place from
+    // pos[].w in HBM instead (a cloth with more distinct values than the table holds).
     int32_t lean;
+    int32_t n_wtab;
+    const float* wtab;
 };
+
+#define PXB_MAX_WTAB 256
 
 // A run of a general-topology cloth: consecutive items of one reference batch, no two of which
 // share a particle, so its items are projected in parallel between two block barriers.

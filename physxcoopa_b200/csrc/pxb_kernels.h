@@ -15,6 +15,11 @@ namespace pxb {
 // sm_100 per-block limit of 227 KB.
 constexpr int kClothStaticSmem = 4608;
 constexpr int kMaxDynamicSmem = 232448 - kClothStaticSmem;
+// Dynamic shared memory of a lean one-CTA cloth held as float arrays (PxbClothDev::lean 2):
+// x, y, z (12 bytes per slot), one inverse-mass index byte per slot padded to 16, the table.
+__host__ __device__ constexpr int soa_smem_bytes(int n_local) {
+    return 12 * n_local + ((n_local + 15) & ~15) + 4 * PXB_MAX_WTAB;
+}
 constexpr int kClothOwned = 4;      // particles per thread in the cloth kernel
 constexpr int kClothMaxThreads = 1024;
 

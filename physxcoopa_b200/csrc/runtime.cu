@@ -678,7 +678,12 @@ static void layout_ranks(ClothEntry& e) {
         lam_total += lam;
         const int n_local = rk.n_rows * e.S;
         const int u_floats = std::max(lam, (aero && e.aero_grid) ? 3 * n_local : 0);
-        if (e.lean) {
+        if (e.lean && e.soa) {
+            // positions as arrays plus the inverse-mass index and table; the warm start's network
+            // borrows all of shared memory while the positions wait in HBM
+            rk.smem = (pxb::soa_smem_bytes(n_local) + 15) & ~15;
+            warm_max = std::max(warm_max, std::max(rk.smem, std::min(kMaxDynamicSmem, kWarmTileOff + kWarmGroups * kWarmTileBytes)));
+        } else if (e.lean) {
             // positions only; the warm start's network tiles go right after them, as many of its
             // warpgroups' tiles as fit (at least one)
             rk.smem = 16 * n_local;
@@ -710,7 +715,7 @@ static void layout_ranks(ClothEntry& e) {
     e.dev.self_buckets = 0;
     e.dev.self_hash_off = 0;
     e.dev.self_restage = 0;
-    if (e.ranks.size() == 1) {
+    if (e.ranks.size() == 1 && !e.soa) {  // a cloth held as arrays has no room for the tables
         const ClothEntry::Rank& rk = e.ranks[0];
         place_self_tables(e, smem_max, 16 * rk.n_rows * e.S, e.lean ? 0 : 4 * rk.n_rest_pad);
     }
@@ -751,6 +756,31 @@ pxb_status pxb_context::upload_particles(ClothEntry& e, const pxb_particle* part
             return fail(PXB_ERR_UNSUPPORTED, "tether %u anchors to an unpinned particle %u", t.particle,
                         t.anchor);
     }
+    if (e.soa) {
+        // the table of distinct inverse masses (ascending bit patterns) the kernel indexes; with
+        // more than the table holds, the kernel reads them in place from the positions in HBM
+        std::vector<uint32_t> bits;
+        bits.reserve(static_cast<size_t>(n) + 1);
+        for (int l = 0; l < e.n_layout; ++l) {
+            uint32_t b;
+            std::memcpy(&b, &pos[l].w, 4);
+            bits.push_back(b);
+        }
+        std::sort(bits.begin(), bits.end());
+        bits.erase(std::unique(bits.begin(), bits.end()), bits.end());
+        const int n_wtab = bits.size() <= static_cast<size_t>(PXB_MAX_WTAB) ? static_cast<int>(bits.size()) : 0;
+        if (n_wtab) {
+            pxb_status s = cuda(cudaMemcpyAsync(const_cast<float*>(e.dev.wtab), bits.data(), 4 * bits.size(),
+                                                cudaMemcpyHostToDevice, stream),
+                                "upload inverse-mass table");
+            if (s) return s;
+        }
+        if (n_wtab != e.dev.n_wtab) {
+            e.dev.n_wtab = n_wtab;
+            registry_dirty = true;
+            ++registry_epoch;
+        }
+    }
     const size_t bytes = 16 * static_cast<size_t>(e.n_layout);
     pxb_status s = cuda(cudaMemcpyAsync(e.dev.pos, pos.data(), bytes, cudaMemcpyHostToDevice, stream), "upload pos");
     if (s) return s;
@@ -774,7 +804,8 @@ pxb_status pxb_context::upload_anchor_records(ClothEntry& e) {
 // Everything add_cloth decides before touching the device: validation, grid recognition, the
 // cluster size, per-rank colour segments (verified item by item against the constraint lists)
 // and the shared-memory layout. Needs no context, so the layout can be planned on any host.
-static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string& err) {
+// soa_layouts: the float-array lean layout may be chosen (pxb_context_set_lean_arrays).
+static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string& err, bool soa_layouts = true) {
     char buf[512];
     auto fail = [&](pxb_status st, const char* fmt, auto... args) {
         snprintf(buf, sizeof(buf), fmt, args...);
@@ -876,19 +907,25 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
     int max_colour = 0;
     bool placed = false;
     // One CTA with everything in shared memory; else lean (positions only in shared memory, rest
-    // lengths and lambdas read in place in HBM) on one CTA or two, as long as the warm start's
-    // tiles still fit beside the positions; else a cluster of 2, 4 or 8 CTAs.
-    const struct { int cl; bool lean; } tries[] = {{1, false}, {1, true}, {2, true}, {2, false}, {4, false}, {8, false}};
+    // lengths and lambdas read in place in HBM) on one CTA as float4, as long as the warm start's
+    // tiles still fit beside the positions; else lean on one CTA with the positions as float
+    // arrays (12 bytes and an inverse-mass index per slot); else lean on two CTAs; else a
+    // cluster of 2, 4 or 8 CTAs.
+    const struct { int cl; bool lean, soa; } tries[] = {{1, false, false}, {1, true, false}, {1, true, true},
+                                                        {2, true, false}, {2, false, false}, {4, false, false},
+                                                        {8, false, false}};
     for (const auto& t : tries) {
         if (placed) break;
+        if (t.soa && !soa_layouts) continue;
         std::vector<int32_t> padded;
         if (!build_ranks(e, cs, rest_ref, t.cl, padded, max_colour)) continue;
         e.lean = t.lean;
+        e.soa = t.soa;
         e.rest_ref.swap(padded);
         layout_ranks(e);
         if (e.dev.smem_bytes <= kMaxDynamicSmem && (!t.lean || e.warm_smem <= kMaxDynamicSmem)) placed = true;
     }
-    if (!placed) e.lean = false;
+    if (!placed) e.lean = e.soa = false;
     if (!placed) {
         // Beyond a cluster: the whole-GPU path (every SM on this cloth, state in global memory).
         std::vector<int32_t> padded;
@@ -908,7 +945,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     if (!d || !id_out) return fail(PXB_ERR_INVALID_ARGUMENT, "null argument");
     ClothEntry e;
     std::string msg;
-    if (pxb_status st = plan_cloth(d, e, msg)) return fail(st, "%s", msg.c_str());
+    if (pxb_status st = plan_cloth(d, e, msg, soa_layouts)) return fail(st, "%s", msg.c_str());
     const uint32_t n = d->n_particles;
 
     // --- anchors: one device record per anchor; a particle follows its LAST anchor ---
@@ -964,6 +1001,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
                  o_tent = take(sizeof(int4) * e.tri_ent.size());
     // topology 2: lambdas (at most one per item) or parked velocities, whichever params ask for
     const size_t o_scr = take(e.list_gmem ? 4 * std::max<size_t>(e.list_items_pad, 3 * L) : 0);
+    const size_t o_wtab = take(e.soa ? 4 * PXB_MAX_WTAB : 0);
     cudaError_t ce = cudaMalloc(&e.dmem, off);
     if (ce != cudaSuccess) return cuda(ce, "cudaMalloc(cloth)");
     e.dbytes = off;
@@ -976,7 +1014,9 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.self_hash_off = keep_ranks.self_hash_off;
     e.dev.self_restage = keep_ranks.self_restage;
     e.dev.ref_columns = e.ref_columns;
-    e.dev.lean = e.lean ? 1 : 0;
+    e.dev.lean = e.lean ? (e.soa ? 2 : 1) : 0;
+    e.dev.wtab = e.soa ? reinterpret_cast<const float*>(base + o_wtab) : nullptr;
+    e.dev.n_wtab = 0;  // upload_particles fills the table
     e.dev.pos = reinterpret_cast<float4*>(base + o_pos);
     e.dev.vel = reinterpret_cast<float4*>(base + o_vel);
     e.dev.prv = reinterpret_cast<float4*>(base + o_prv);
@@ -1251,7 +1291,8 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
                              cstage.any_geometry(sd->collider_offsets[k],
                                                  sd->collider_offsets[k + 1] - sd->collider_offsets[k])));
     for (uint32_t k = 0; k < n; ++k)
-        if (ents[k]->lean) has_geo[k] = static_cast<uint8_t>(3 + has_geo[k]);  // lean instantiations
+        if (ents[k]->lean)  // lean instantiations: float4 (3, 4), float arrays (5, 6)
+            has_geo[k] = static_cast<uint8_t>((ents[k]->soa ? 5 : 3) + has_geo[k]);
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
@@ -1615,7 +1656,7 @@ pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out
     out->self_collision = e.self_ok && !e.grid ? 1 : 0;
     out->self_smem_bytes = e.self_ok && !e.grid ? e.self_smem : 0;
     out->topology = e.list_gmem ? 2 : (e.list ? 1 : 0);
-    out->lean = e.lean ? 1 : 0;
+    out->lean = e.lean ? (e.soa ? 2 : 1) : 0;
     if (e.list) out->n_colours = static_cast<int32_t>(e.runs.size());
     return PXB_OK;
 }
@@ -1955,6 +1996,12 @@ pxb_status pxb_context_set_launch_mode(pxb_context* ctx, int32_t mode) {
     if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
     if (mode != 0 && mode != 1) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "launch mode must be 0 or 1");
     ctx->launch_mode = mode;
+    return PXB_OK;
+}
+
+pxb_status pxb_context_set_lean_arrays(pxb_context* ctx, int32_t enable) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    ctx->soa_layouts = enable != 0;
     return PXB_OK;
 }
 

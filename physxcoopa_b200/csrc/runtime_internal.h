@@ -26,6 +26,7 @@ struct ClothEntry {
     bool alive = false;
     bool grid = false;  // beyond a cluster: solved by every SM from global memory
     bool lean = false;  // only positions in shared memory (PxbClothDev::lean), one CTA or two
+    bool soa = false;   // lean on one CTA with the positions as float arrays (PxbClothDev::lean 2)
     uint32_t generation = 0;
     uint32_t n_particles = 0;
     int cols = 0, rows = 0, Q = 0, S = 0, n_layout = 0;
@@ -187,6 +188,7 @@ struct pxb_context {
     }
     int cloth_variant = 0;  // kernel block-size cap, see pxb_kernels.h (autotuned or set)
     int launch_mode = 1;    // 1: persistent CTAs popping a work queue per launch group; 0: one CTA per cloth
+    bool soa_layouts = true;  // cloths added from now on may take the float-array lean layout
     DevBuf d_tune;          // cloth state saved across an autotune
     // Pipelined position read-back (pxb_cloths_read_positions_async): two device snapshots,
     // each gathered on `stream` and copied to the host on `copy_stream`, which waits for it.

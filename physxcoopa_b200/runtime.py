@@ -88,6 +88,7 @@ SIGNATURES = {
     "pxb_check_projections": ([P, u64, u64, C.POINTER(u64), C.POINTER(f32)], C.c_int),
     "pxb_context_set_cloth_variant": ([P, C.c_int32], C.c_int),
     "pxb_context_set_launch_mode": ([P, C.c_int32], C.c_int),
+    "pxb_context_set_lean_arrays": ([P, C.c_int32], C.c_int),
     "pxb_context_set_wait_test": ([P, u32, u32], C.c_int),
     "pxb_strands_add": ([P, C.POINTER(A.StrandSetDesc), C.POINTER(u64)], C.c_int),
     "pxb_strands_remove": ([P, u64], C.c_int),
@@ -535,6 +536,11 @@ class Context:
         can complete (to drive the expiry path in a test)."""
         self._check(self.lib.pxb_context_set_wait_test(self.h, grid_wait_polls, 1 if unreachable else 0),
                     "set_wait_test")
+
+    def set_lean_arrays(self, enable):
+        """pxb_context_set_lean_arrays: cloths added afterwards may (1) or may not (0) take the
+        one-CTA float-array layout."""
+        self._check(self.lib.pxb_context_set_lean_arrays(self.h, 1 if enable else 0), "set_lean_arrays")
 
     def set_launch_mode(self, mode):
         """pxb_context_set_launch_mode: 1 persistent work-queue kernels, 0 one CTA per cloth."""

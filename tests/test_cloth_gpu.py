@@ -398,14 +398,15 @@ def clustered_sheet(cols, rows, seed, pins="corners", params=None):
 
 CLUSTERED = {
     # (columns, rows) and the layout the planner gives: (CTAs, lean). Lean: only the positions in
-    # shared memory, rest lengths and lambdas read in place in HBM.
+    # shared memory, rest lengths and lambdas read in place in HBM; lean 2: as float arrays.
     "lean1_65": dict(shape=(65, 65), layout=(1, 1), cols=[sphere(0.5, (0.1, 0, 0.4))]),
     "lean1_100_sources": dict(shape=(100, 100), layout=(1, 1), cols=[capsule(0.2, 0.5, (0, 0, 0.5), axis=0)],
                               sources=[((0.5, -0.3, -2.0), 9.81, 1.0, 10.0)]),
-    "lean2_128_edge": dict(shape=(128, 128), layout=(2, 1), pins="edge",
+    "arrays_128_edge": dict(shape=(128, 128), layout=(1, 2), pins="edge",
                            cols=[box((0.6, 0.5, 0.4), (0.2, 0.1, 0.3), (0.0, 0.3826834, 0.0, 0.9238795))]),
     "lean1_tall_40x180": dict(shape=(40, 180), layout=(1, 1), cols=[sphere(0.6, (0, 0.5, 0.2))]),
-    "lean2_wind_150x97": dict(shape=(150, 97), layout=(2, 1), params=dict(wind=(0.5, 0.2, 0.0), wind_turbulence=0.5)),
+    "arrays_wind_150x97": dict(shape=(150, 97), layout=(1, 2), params=dict(wind=(0.5, 0.2, 0.0), wind_turbulence=0.5)),
+    "lean2_wind_150x130": dict(shape=(150, 130), layout=(2, 1), params=dict(wind=(0.5, 0.2, 0.0), wind_turbulence=0.5)),
     "c8_160": dict(shape=(160, 160), layout=(8, 0), cols=[sphere(0.8, (0, 0, 0.2))]),
 }
 
@@ -451,13 +452,13 @@ def compliant_mask(batches, compliance, n):
 
 
 def test_batch_of_every_cluster_size(ctx):
-    """One step call over cloths of every layout (one CTA, lean on one CTA or two, a cluster of
-    eight): at least one launch per layout, all equal to the oracle, positions gathered in the
-    caller's order."""
-    shapes = [(20, 20), (128, 128), (64, 64), (65, 65), (100, 100), (16, 16), (160, 160)]
+    """One step call over cloths of every layout (one CTA, lean on one CTA as float4 or as float
+    arrays or on two CTAs, a cluster of eight): at least one launch per layout, all equal to the
+    oracle, positions gathered in the caller's order."""
+    shapes = [(20, 20), (128, 128), (64, 64), (65, 65), (100, 100), (16, 16), (150, 130), (160, 160)]
     cloths = [clustered_sheet(c, r, seed=k) for k, (c, r) in enumerate(shapes)]
     sizes = {(R.plan_cloth(c)["n_ranks"], R.plan_cloth(c)["lean"]) for c in cloths}
-    assert sizes == {(1, 0), (1, 1), (2, 1), (8, 0)}
+    assert sizes == {(1, 0), (1, 1), (1, 2), (2, 1), (8, 0)}
     cols = [collider_array([sphere(0.3 + 0.05 * k, (0.05 * k, 0, 0.4))]) for k in range(len(cloths))]
     orcs = [c.copy() for c in cloths]
     ids = [ctx.add_cloth(c) for c in cloths]

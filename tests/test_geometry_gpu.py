@@ -162,13 +162,13 @@ def test_terrain_drape_equals_oracle_1_and_300_steps(ctx):
             ctx.destroy_geometry(g)
 
 
-@pytest.mark.parametrize("side", [100, 128, 160, 200])
+@pytest.mark.parametrize("side", [100, 128, 140, 160, 200])
 def test_cluster_and_whole_gpu_paths_with_mesh_and_hull(ctx, side):
-    """100 x 100 runs lean on one CTA, 128 x 128 lean on two, 160 x 160 on a cluster of eight,
-    200 x 200 on the whole-GPU kernel."""
+    """100 x 100 runs lean on one CTA, 128 x 128 lean on one CTA as float arrays, 140 x 140 lean
+    on two CTAs, 160 x 160 on a cluster of eight, 200 x 200 on the whole-GPU kernel."""
     sc = S.terrain_drape(side=side, seed=5)
     plan = R.plan_cloth(sc.cloths[0])
-    want = {100: (1, 1), 128: (2, 1), 160: (8, 0), 200: (0, 0)}[side]
+    want = {100: (1, 1), 128: (1, 2), 140: (2, 1), 160: (8, 0), 200: (0, 0)}[side]
     assert (plan["n_ranks"], plan["lean"]) == want, plan
     gids = _scene_with_oracle(ctx, sc)
     try:

@@ -99,6 +99,8 @@ def parse():
                     help="fix the kernel variant (0/1/2) instead of autotuning")
     ap.add_argument("--launch", choices=["queue", "cta"], default="queue",
                     help="with --variant: persistent work-queue kernels (queue) or one CTA per cloth (cta)")
+    ap.add_argument("--no-lean-arrays", action="store_true",
+                    help="lay sheets of sides 110-128 out on 2-CTA clusters instead of one CTA with float arrays")
     return ap.parse_args()
 
 
@@ -737,6 +739,8 @@ def main():
 
     sc, shares, job_vertices, job_cloths = build_gpu_scene(args, rank, world)
     ctx = R.Context(local_rank)
+    if args.no_lean_arrays:
+        ctx.set_lean_arrays(False)
     if sc.geometries:
         from physxcoopa_b200 import scenes
         scenes.register_geometries(ctx, sc)
@@ -905,7 +909,8 @@ def main():
             "config": workload_config(args, sc.name, job_cloths, job_vertices, sc.substeps, sc.iterations, sc.h,
                                       n_gpus=world),
             "launch": {"entry": "pxb_cloths_step_graph (captured CUDA graph)" if args.graph else "pxb_cloths_step",
-                       "autotune": tune},
+                       "autotune": tune,
+                       "sides_110_128": "two-CTA clusters" if args.no_lean_arrays else "one CTA, positions as float arrays"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                     "read_back": "pipelined: pxb_cloths_read_positions_async + pxb_cloths_read_results_async, "

@@ -258,27 +258,31 @@ __device__ __forceinline__ void project_run(float4* __restrict__ pos, const floa
 }
 
 // ------------------------------------------------------------------------------------------
-// Positions of a lean one-CTA cloth as three float arrays (PxbClothDev::lean == 2)
+// Positions of a lean one-CTA cloth as float arrays (PxbClothDev::lean == 2)
 // ------------------------------------------------------------------------------------------
 
-// x, y, z of slot l at x[l], x[n + l], x[2n + l]; its inverse mass is wt[wi[l]] (the cloth's
-// table of distinct values, in shared memory), or, with w_hbm, pos[l].w read in place in HBM.
+// x, y of slot l at xy[l] (one 8-byte access), z at z[l]; its inverse mass is wt[wi[l]] (the
+// cloth's table of distinct values, in shared memory), or, with w_hbm, pos[l].w read in place in
+// HBM.
 // Indexing yields a reference that reads and writes a float4 (x, y, z, inverse mass), so the
 // stages outside the projection read like those of the float4 layout; a write keeps the inverse
 // mass, which no stage changes.
 struct SoaPos {
-    float* x;
+    float2* xy;
+    float* z;
     const uint8_t* wi;
     const float* wt;
     const float4* g;
     int n;
     bool w_hbm;
     __device__ __forceinline__ float w(int l) const { return w_hbm ? __ldg(&g[l].w) : wt[wi[l]]; }
-    __device__ __forceinline__ float4 get(int l) const { return make_float4(x[l], x[n + l], x[2 * n + l], w(l)); }
+    __device__ __forceinline__ float4 get(int l) const {
+        const float2 p = xy[l];
+        return make_float4(p.x, p.y, z[l], w(l));
+    }
     __device__ __forceinline__ void set(int l, float4 v) const {
-        x[l] = v.x;
-        x[n + l] = v.y;
-        x[2 * n + l] = v.z;
+        xy[l] = make_float2(v.x, v.y);
+        z[l] = v.z;
     }
     struct Ref;
     __device__ __forceinline__ Ref operator[](int l) const;
@@ -312,9 +316,8 @@ __device__ __forceinline__ void soa_stage(const SoaPos& P, float* wt_smem, const
     uint8_t* wi = const_cast<uint8_t*>(P.wi);
     for (int l = tid; l < P.n; l += T) {
         const float4 v = src[l];
-        P.x[l] = v.x;
-        P.x[P.n + l] = v.y;
-        P.x[2 * P.n + l] = v.z;
+        P.xy[l] = make_float2(v.x, v.y);
+        P.z[l] = v.z;
         if (!P.w_hbm) {
             const uint32_t key = __float_as_uint(v.w);
             int lo = 0, hi = n_wtab - 1;
@@ -341,8 +344,8 @@ __device__ __forceinline__ void project_segment_soa(const SoaPos& P, const float
     const int count = h0.x, per_row = h0.z, a_base = h0.w;
     const uint32_t magic = static_cast<uint32_t>(h0.y);
     const int row_stride = h1.x, d = h1.y;
-    const int n = P.n;
-    float* __restrict__ X = P.x;
+    float2* __restrict__ XY = P.xy;
+    float* __restrict__ Z = P.z;
     auto wof = [&](int l) -> float { return kWH ? __ldg(&P.g[l].w) : P.wt[P.wi[l]]; };
     auto one = [&](int i, int& la, int& lb, float4& a, float4& b, float& r, float& lam, bool& live) {
         live = i < count;
@@ -350,16 +353,19 @@ __device__ __forceinline__ void project_segment_soa(const SoaPos& P, const float
         const int row = seg_row(ii, magic);
         la = a_base + row * row_stride + (ii - row * per_row);
         lb = la + d;
-        a = make_float4(X[la], X[n + la], X[2 * n + la], wof(la));
-        b = make_float4(X[lb], X[n + lb], X[2 * n + lb], wof(lb));
+        const float2 pa = XY[la], pb = XY[lb];
+        a = make_float4(pa.x, pa.y, Z[la], wof(la));
+        b = make_float4(pb.x, pb.y, Z[lb], wof(lb));
         r = rest[ii];
         lam = kLam ? lamv[ii] : 0.0f;
     };
     auto put = [&](int i, int la, int lb, float4 a, float4 b, float r, float lam, bool live) {
         float dlambda;
         if (distance_core<kLam>(a, b, r, lam, alpha, dlambda) && live) {
-            X[la] = a.x; X[n + la] = a.y; X[2 * n + la] = a.z;
-            X[lb] = b.x; X[n + lb] = b.y; X[2 * n + lb] = b.z;
+            XY[la] = make_float2(a.x, a.y);
+            Z[la] = a.z;
+            XY[lb] = make_float2(b.x, b.y);
+            Z[lb] = b.z;
             if (kLam) lamv[i] = lam + dlambda;
         }
     };
@@ -503,7 +509,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     // a lean cloth (only positions in shared memory; rest lengths and lambdas read in place in
     // HBM, velocities for the aerodynamic gather too) runs only in the kLean instantiations
     constexpr bool kL = kLean != 0 && CL <= 2 && !kG;
-    // a lean one-CTA cloth whose positions are three float arrays runs only in the kLean == 2
+    // a lean one-CTA cloth whose positions are float arrays runs only in the kLean == 2
     // instantiations
     constexpr bool kS = kLean == 2 && CL == 1 && !kG;
     constexpr int kWantLean = kS ? 2 : (kL ? 1 : 0);
@@ -516,7 +522,8 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
     auto pos = [&]() {
         if constexpr (kS) {
             const int n = me.n_local;
-            return SoaPos{reinterpret_cast<float*>(smem), smem + 12 * static_cast<size_t>(n),
+            return SoaPos{reinterpret_cast<float2*>(smem), reinterpret_cast<float*>(smem + 8 * static_cast<size_t>(n)),
+                          smem + 12 * static_cast<size_t>(n),
                           reinterpret_cast<const float*>(smem + 12 * static_cast<size_t>(n) + ((n + 15) & ~15)),
                           sC.pos + me.base, n, sC.n_wtab == 0};
         } else {

@@ -110,7 +110,7 @@ struct PxbClothDev {
     int32_t ref_columns;        // Cloth::columns as given: self-collision's 1-ring exemption reads it
     // 1: a lean grid cloth: only positions in shared memory, its rest lengths and lambdas read in
     // place in HBM (rest + rank.rest_off, lam_out + rank.lam_off), velocities too; one or two CTAs.
-    // 2: the same on one CTA with the positions held as three float arrays (x, y, z) and one byte
+    // 2: the same on one CTA with the positions held as float arrays (x and y as float2, z) and one byte
     // per slot indexing wtab, the cloth's distinct inverse masses in ascending bit order
     // (n_wtab <= PXB_MAX_WTAB of them); n_wtab == 0 reads the inverse masses in place from
     // pos[].w in HBM instead (a cloth with more distinct values than the table holds).

@@ -584,13 +584,26 @@ def bench_large(args, local_rank):
 # the learned warm start (config 4) on a cloth batch
 # ------------------------------------------------------------------------------------------
 
-def warm_start_comparison(args, ctx, sc, local_rank, steps):
+def warm_start_comparison(args, ctx, sc, local_rank, steps, tuned=False):
     """Plain 20 iterations against the network + 4 iterations at equal per-cloth residual, on a
-    fresh copy of `sc` each run (see the module docstring). Returns a dict for the JSON line."""
+    fresh copy of `sc` each run (see the module docstring). Each arm runs at its best kernel
+    configuration: the plain arm at the context's autotuned block size and launch form (tuned
+    here unless `tuned` or --variant), the warm arm at the faster of its two block sizes (512 and
+    1024 threads). Returns a dict for the JSON line."""
     import torch
     from physxcoopa_b200 import scenes
     plain_iters, warm_iters = 20, 4
-    ctx.set_cloth_variant(0 if args.variant is None else args.variant)
+    if args.variant is not None:
+        ctx.set_cloth_variant(args.variant)
+        ctx.set_launch_mode(1 if args.launch == "queue" else 0)
+    elif not tuned:
+        ids = [ctx.add_cloth(c) for c in sc.cloths]
+        d, keep = ctx.make_step(ids, sc.colliders, sc.gravity, sc.sources, sc.substeps, plain_iters, sc.h)
+        ctx.autotune(d, trials=2)
+        for i in ids:
+            ctx.remove_cloth(i)
+        del keep
+    plain_variant = ctx.cloth_variant
     # --- training rows from the plain solver on a separately seeded batch -------------------
     t0 = time.perf_counter()
     tr = scenes.uneven_batch(n=512, seed=102, params=sheet_params(args))
@@ -656,8 +669,16 @@ def warm_start_comparison(args, ctx, sc, local_rank, steps):
     subs = sum(r["substeps"].sum() for r in res_w)
     fb = float(sum(r["fallbacks"].sum() for r in res_w) / subs)
     extra = float(sum(r["extra_iterations"].sum() for r in res_w) / subs)
+    # the warm kernel comes in two block sizes (variants 0 and 1-2 run 512 and 1024 threads)
+    warm_ms = {}
+    for v in ((args.variant,) if args.variant is not None else (0, 2)):
+        ctx.set_cloth_variant(v)
+        warm_ms[v] = run("warm", taus)
+    best_v = min(warm_ms, key=lambda v: warm_ms[v][0])
+    ms_warm, _, launches = warm_ms[best_v]
+    ctx.set_cloth_variant(best_v)
     ms_restart, _, _ = run("warm_restart", taus)
-    ms_warm, _, launches = run("warm", taus)
+    ctx.set_cloth_variant(plain_variant)
     verts = sc.vertices * sc.substeps
     return {"workload": "the same batch: 20 plain iterations vs the network + 4 iterations, equal residual "
                         "cloth by cloth",
@@ -667,6 +688,9 @@ def warm_start_comparison(args, ctx, sc, local_rank, steps):
                      "residual_median": float(np.median(rw)), "residual_max": float(rw.max()),
                      "gpu_launches": launches},
             "speedup_vs_plain": ms_plain / ms_warm,
+            "kernels": {"plain_block_cap": [512, 768, 1024][plain_variant],
+                        "warm_block_threads": {[512, 1024, 1024][v]: warm_ms[v][0] for v in warm_ms},
+                        "launch": "persistent work queue" if ctx.launch_mode == 1 else "one CTA per cloth"},
             "fallback_rate": fb, "extra_iterations_per_substep": extra,
             "fallback": "continue iterating from the warm state, 4 at a time, to the threshold or 20 iterations",
             "restart_fallback": {"ms_per_step": ms_restart, "speedup_vs_plain": ms_plain / ms_restart,
@@ -894,7 +918,7 @@ def main():
     # --- the learned warm start on the same batch (rank 0, one GPU) -------------------------
     warm = None
     if args.workload == "uneven_batch" and not args.no_warm and rank == 0 and world == 1:
-        warm = warm_start_comparison(args, ctx, sc, local_rank, args.steps)
+        warm = warm_start_comparison(args, ctx, sc, local_rank, args.steps, tuned=True)
 
     line = None
     if rank == 0:

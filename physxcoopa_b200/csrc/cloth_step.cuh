@@ -880,23 +880,17 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             float4* __restrict__ gpos = sC.pos;
             // the prediction goes to HBM: the fallback restarts from it, targets are measured from it
             for (int l = tid; l < n_local; l += T) gpos[base + l] = pos[l];
-            // a cloth held as arrays reads its features from HBM and lends the network its
-            // shared memory: every slot is in HBM before either happens
-            if constexpr (kS) __syncthreads();
+            // The features are read from HBM and the network borrows all of shared memory
+            // (positions, rest lengths and the lambda region, staged again after it; the lambdas
+            // are reset after it anyway), so every warpgroup the block has can run tiles, not
+            // only those whose tiles fit beside the positions. Every rank's prediction is in HBM
+            // before any feature is read or any scratch written.
+            if (net || rec) cluster_or_block_sync<CL>();
             if (net || rec) {
-                // With the network, its scratch is the rest lengths plus the lambda region (the
-                // rest lengths are staged again below); recording alone uses the lambda region.
                 uint32_t dyn;
                 asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-                // a lean cloth has nothing after its positions in shared memory: all of it is
-                // scratch; a cloth held as arrays lends the network all of shared memory (its
-                // positions are in HBM, just written, and are staged again afterwards)
-                unsigned char* ub = kS ? smem
-                                       : (net || kL) ? reinterpret_cast<unsigned char*>(rest)
-                                                     : reinterpret_cast<unsigned char*>(U);
-                const int u_cap = kS ? static_cast<int>(dyn)
-                                     : (net || kL) ? static_cast<int>(dyn) - 16 * n_local
-                                                   : static_cast<int>(dyn) - (16 * n_local + 4 * sC.rank[rank].n_rest_pad);
+                unsigned char* ub = smem;
+                const int u_cap = static_cast<int>(dyn);
                 int n_wg = (u_cap - kWarmTileOff) / kWarmTileBytes;
                 n_wg = n_wg < T / 128 ? n_wg : T / 128;
                 n_wg = n_wg < kWarmGroups ? n_wg : kWarmGroups;
@@ -934,9 +928,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                                 const int cls = j / Q;
                                 const int xx = 4 * (j - cls * Q) + cls;
                                 if (xx < cols && y < rows) {
-                                    // positions from HBM for a cloth held as arrays: the network's
-                                    // tiles overwrite them in shared memory
-                                    const float4 p = kS ? gpos[gl] : float4(pos[l]);
+                                    const float4 p = gpos[gl];
                                     const float4 q0 = gprv[gl], v = gvel[gl];
                                     x[0] = p.x - q0.x; x[1] = p.y - q0.y; x[2] = p.z - q0.z;
                                     x[3] = v.x; x[4] = v.y; x[5] = v.z;
@@ -946,13 +938,7 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                                         const int nx = xx + dxs[e], ny = y + dys[e];
                                         const float r = __ldg(&sC.edge_rest[e * nl + gl]);
                                         if (nx < 0 || ny < 0 || nx >= cols || ny >= rows || !(r > 0.0f)) continue;
-                                        const int ng = lay(nx, ny, Q, S_);
-                                        const int nloc = ng - base;
-                                        float4 q;
-                                        if (kS) q = gpos[ng];
-                                        else if (CL == 1 || (nloc >= 0 && nloc < n_local)) q = pos[nloc];
-                                        else if (nloc < 0) q = prv_rank.pos[nloc + prv_rank.n_local];
-                                        else q = nxt_rank.pos[nloc - n_local];
+                                        const float4 q = gpos[lay(nx, ny, Q, S_)];
                                         const float ex = q.x - p.x, ey = q.y - p.y, ez = q.z - p.z;
                                         const float len = sqrtf(ex * ex + ey * ey + ez * ez);
                                         if (len > PXB_EPSILON) {
@@ -982,6 +968,15 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     tc::fence_after_sync();
                     if (net && tid < 32) tc::tmem_dealloc(s_tmem, n_wg > 2 ? 256u : (n_wg > 1 ? 128u : 64u));
                 }
+                if (net) {
+                    // the prediction back from HBM (plain loads: this kernel wrote it)
+                    __syncthreads();
+                    if constexpr (kS) {
+                        soa_stage(pos, const_cast<float*>(pos.wt), gpos + base, sC.wtab, sC.n_wtab, err, tid, T);
+                    } else {
+                        for (int l = tid; l < n_local; l += T) pos[l] = gpos[base + l];
+                    }
+                }
                 if (net && !kL) {
                     // the rest lengths come back: TMA bulk copy, next phase of the staging barrier
                     fence_proxy_async();
@@ -994,14 +989,9 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     stage_phase ^= 1u;
                     if (!mbar_wait_bounded(&bar, stage_phase) && tid == 0) atomicOr(err, PXB_DEVERR_TMA_TIMEOUT);
                 }
-                // every rank's features are read before any rank moves a particle
+                // every rank's positions are back before any rank moves a particle (or reads a
+                // neighbour's through distributed shared memory)
                 cluster_or_block_sync<CL>();
-                if constexpr (kS) {
-                    if (net) {  // the prediction back from HBM
-                        soa_stage(pos, const_cast<float*>(pos.wt), gpos + base, sC.wtab, sC.n_wtab, err, tid, T);
-                        __syncthreads();
-                    }
-                }
                 if (net) {
                     for (int l = tid; l < n_local; l += T) {
                         const int gl = base + l;

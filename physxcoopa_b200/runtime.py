@@ -319,6 +319,8 @@ class Context:
             raise PxbError(st, "pxb_context_create failed (is a CUDA device visible?)")
         self._keep = []
         self._slots = {}
+        self.cloth_variant = 0  # the context's kernel variant and launch form, as last set
+        self.launch_mode = 1
 
     def close(self):
         if self.h:
@@ -545,9 +547,11 @@ class Context:
     def set_launch_mode(self, mode):
         """pxb_context_set_launch_mode: 1 persistent work-queue kernels, 0 one CTA per cloth."""
         self._check(self.lib.pxb_context_set_launch_mode(self.h, mode), "set_launch_mode")
+        self.launch_mode = mode
 
     def set_cloth_variant(self, variant):
         self._check(self.lib.pxb_context_set_cloth_variant(self.h, variant), "set_cloth_variant")
+        self.cloth_variant = variant
 
     def autotune(self, d, trials=3):
         """Times the kernel variants in both launch forms on step desc `d` (state restored);
@@ -556,6 +560,7 @@ class Context:
         ms = (C.c_float * 6)()
         self._check(self.lib.pxb_cloths_autotune(self.h, C.byref(d), trials, C.byref(best), ms),
                     "autotune")
+        self.cloth_variant, self.launch_mode = best.value % 3, best.value // 3
         return best.value, list(ms)
 
     def read_results(self, ids):

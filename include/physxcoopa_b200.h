@@ -460,8 +460,8 @@ pxb_status pxb_cloths_wait_positions(pxb_context* ctx);
  * synchronise the device or is not permitted): pxb_cloths_read_positions grows internal buffers
  * on demand, this never does. At most 4096 cloths per call (PXB_ERR_TOO_LARGE beyond); the
  * per-call cloth list lives in a 48 KB array compiled into the library, held on every GPU that
- * loads it until exit. The first call on a device looks up that array's address (set-up):
- * make it before any stream capture. The call list is assembled in a static host buffer under a
+ * loads it until exit. A context's first call looks up that array's address (set-up) and
+ * keeps it on the context: make it before any stream capture. The call list is assembled in a static host buffer under a
  * mutex (no allocation, no large stack frame), so concurrent host calls take turns. The registry must be current (a step since the last
  * add / remove / parameter change), else PXB_ERR_INVALID_ARGUMENT. Enqueued on the context
  * stream, returns before completion; calls that overlap on the GPU (other contexts or streams

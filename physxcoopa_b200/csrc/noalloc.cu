@@ -10,8 +10,9 @@
 // Its only scratch, the per-call cloth list (registry slot and output offset of each cloth),
 // lives in a fixed-size array compiled into the library: kMaxCloths entries, 48 KB, present on
 // every GPU that loads the library until the process exits. Host code gets the array's device
-// address with cudaGetSymbolAddress, once per device, on the first call made on that device
-// (the set-up). Every call overwrites the entries it uses before its kernel reads them, so
+// address with cudaGetSymbolAddress once per context, on the context's first call (the set-up),
+// and keeps it on the context: a context made after a device reset, or in another CUDA context
+// of the device, looks the address up again. Every call overwrites the entries it uses before its kernel reads them, so
 // nothing has to start at zero; but all calls share the one array, so calls that can run at the
 // same time on the GPU (from different contexts or streams of one device) race, and must be
 // serialised by the caller. Calls on one context are ordered on its stream.
@@ -34,8 +35,6 @@ constexpr size_t kOffsetBytes = 8 * kMaxCloths;  // int64 first output float per
 static __device__ __align__(256) unsigned char g_gather_scratch[kOrderBytes + kOffsetBytes];
 
 constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-unsigned char* g_scratch_ptr[kMaxDevices] = {};
 
 // The per-call cloth list is assembled in host memory that is also static (no allocation and no
 // 48 KB on the caller's stack, which render and worker threads may not have): one buffer for the
@@ -45,16 +44,16 @@ std::mutex g_list_mutex;
 int32_t g_order[kMaxCloths];
 int64_t g_offs[kMaxCloths];
 
-// The device address of g_gather_scratch on `device` (which must be current), looked up once.
-cudaError_t scratch_on(int device, unsigned char** out) {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[device]) {
+// The device address of g_gather_scratch in the context's device (which must be current),
+// looked up at the context's first call.
+cudaError_t scratch_of(pxb_context* ctx, unsigned char** out) {
+    if (!ctx->gather_scratch) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_gather_scratch);
         if (e != cudaSuccess) return e;
-        g_scratch_ptr[device] = static_cast<unsigned char*>(p);
+        ctx->gather_scratch = static_cast<unsigned char*>(p);
     }
-    *out = g_scratch_ptr[device];
+    *out = ctx->gather_scratch;
     return cudaSuccess;
 }
 
@@ -78,7 +77,7 @@ pxb_status pxb_cloths_gather_positions_device(pxb_context* ctx, const uint64_t* 
         return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "the context's device (%d) is not the current device (%d)",
                          ctx->device, device);
     unsigned char* scratch = nullptr;
-    if (pxb_status s = ctx->cuda(scratch_on(device, &scratch), "look up the gather scratch")) return s;
+    if (pxb_status s = ctx->cuda(scratch_of(ctx, &scratch), "look up the gather scratch")) return s;
     {
         std::lock_guard<std::mutex> lock(g_list_mutex);
         int64_t total = 0;

@@ -189,6 +189,7 @@ struct pxb_context {
     int cloth_variant = 0;  // kernel block-size cap, see pxb_kernels.h (autotuned or set)
     int launch_mode = 1;    // 1: persistent CTAs popping a work queue per launch group; 0: one CTA per cloth
     bool soa_layouts = true;  // cloths added from now on may take the float-array lean layout
+    unsigned char* gather_scratch = nullptr;  // pxb_cloths_gather_positions_device's static scratch
     DevBuf d_tune;          // cloth state saved across an autotune
     // Pipelined position read-back (pxb_cloths_read_positions_async): two device snapshots,
     // each gathered on `stream` and copied to the host on `copy_stream`, which waits for it.

@@ -99,6 +99,11 @@ def parse():
                     help="fix the kernel variant (0/1/2) instead of autotuning")
     ap.add_argument("--launch", choices=["queue", "cta"], default="queue",
                     help="with --variant: persistent work-queue kernels (queue) or one CTA per cloth (cta)")
+    ap.add_argument("--iterations", type=int, default=None,
+                    help="constraint iterations per substep of the cloth workloads (default: the workload's, 10)")
+    ap.add_argument("--thread-fit", type=int, choices=[0, 1], default=None,
+                    help="threads per CTA of one-CTA grid sheets: 1 splits an SM between the CTAs its shared "
+                         "memory holds, 0 gives each sheet its own count")
     ap.add_argument("--no-lean-arrays", action="store_true",
                     help="lay sheets of sides 110-128 out on 2-CTA clusters instead of one CTA with float arrays")
     return ap.parse_args()
@@ -762,9 +767,13 @@ def main():
     from physxcoopa_b200 import shard
 
     sc, shares, job_vertices, job_cloths = build_gpu_scene(args, rank, world)
+    if args.iterations:
+        sc.iterations = args.iterations
     ctx = R.Context(local_rank)
     if args.no_lean_arrays:
         ctx.set_lean_arrays(False)
+    if args.thread_fit is not None:
+        ctx.set_thread_fit(args.thread_fit)
     if sc.geometries:
         from physxcoopa_b200 import scenes
         scenes.register_geometries(ctx, sc)
@@ -778,7 +787,9 @@ def main():
         tune = {"chosen": {"block_cap": [512, 768, 1024][best % 3],
                            "launch": "persistent work queue" if best >= 3 else "one CTA per cloth"},
                 "ms_per_step": {"one CTA per cloth": ms[:3], "persistent work queue": ms[3:]},
-                "variants": "block-size cap 512 / 768 / 1024 threads x launch form"}
+                "variants": "block-size cap 512 / 768 / 1024 threads x launch form, then per layout class",
+                "thread_fit": ctx.tuning()["thread_fit"],
+                "classes": ctx.tuning()["classes"]}
     else:
         ctx.set_cloth_variant(args.variant)
         ctx.set_launch_mode(1 if args.launch == "queue" else 0)

@@ -484,7 +484,8 @@ pxb_status pxb_solve_cloth_host(pxb_context* ctx, const pxb_cloth_desc* desc,
 
 /* Kernel variant used by pxb_cloths_step: the block-size cap of the cloth kernel (0 = 512
  * threads, 1 = 768, 2 = 1024; a larger block has more warps to hide latency but fewer
- * registers per thread). Results are identical across variants; only speed differs. */
+ * registers per thread), for every layout class (clears the autotuner's per-class choices).
+ * Results are identical across variants; only speed differs. */
 pxb_status pxb_context_set_cloth_variant(pxb_context* ctx, int32_t variant);
 /* Failure-path testing (no counterpart in the reference). Cloths beyond an 8-CTA cluster step on
  * every SM with a grid barrier between colours; each barrier wait is bounded (grid_wait_polls
@@ -502,6 +503,12 @@ pxb_status pxb_context_set_wait_test(pxb_context* ctx, uint32_t grid_wait_polls,
  * queue is empty. Mode 0: one CTA (cluster) per cloth, the hardware scheduler handing them out.
  * Results are identical; only speed differs. */
 pxb_status pxb_context_set_launch_mode(pxb_context* ctx, int32_t mode);
+/* Threads per CTA of one-CTA grid cloths (no counterpart in the reference). Mode 0: a cloth runs
+ * with half the items of its largest colour in threads, up to the kernel variant's cap. Mode 1
+ * (default): where shared memory lets an SM hold k CTAs of the cloth, it runs with at most 1/k of
+ * the threads the variant's registers allow, so k CTAs share each SM (one projects while another
+ * waits at a colour barrier). Results are identical; only speed differs. */
+pxb_status pxb_context_set_thread_fit(pxb_context* ctx, int32_t mode);
 /* Layout choice for cloths added from now on (no counterpart in the reference). With `enable`
  * (default), a grid cloth too large for one CTA's shared memory as float4 positions but small
  * enough as float arrays (12 bytes per particle plus a one-byte index into a table of its
@@ -509,15 +516,28 @@ pxb_status pxb_context_set_launch_mode(pxb_context* ctx, int32_t mode);
  * on a cluster of two CTAs as before. Results are identical; only speed differs. */
 pxb_status pxb_context_set_lean_arrays(pxb_context* ctx, int32_t enable);
 /* Autotuner: times every kernel variant in both launch forms on `step` (the caller's real batch,
- * `trials` launches each after one warm-up) and keeps the fastest pair on the context. The
- * listed cloths' device state and host mirrors are saved first and restored after, so tuning
- * does not advance them. variant_out (may be NULL) receives variant + 3 * mode of the pair kept;
- * ms_out (may be NULL) six entries, milliseconds per step: variants 0-2 one CTA per cloth, then
- * variants 0-2 persistent. The threads a constraint colour runs with follow the block size;
- * iterations are never fused between barriers (the reference's Gauss-Seidel order needs one
- * after every colour). */
+ * `trials` launches each after one warm-up) and keeps the fastest pair on the context. Then, one
+ * layout class at a time (largest share of the batch first), it times the class's cloths at the
+ * other two variants with the rest unchanged and keeps a variant that is faster. The listed
+ * cloths' device state and host mirrors are saved first and restored after, so tuning does not
+ * advance them. variant_out (may be NULL) receives variant + 3 * mode of the pair kept; ms_out
+ * (may be NULL) six entries, milliseconds per step: variants 0-2 one CTA per cloth, then variants
+ * 0-2 persistent. The threads a constraint colour runs with follow the block size (and the
+ * thread fit, pxb_context_set_thread_fit); iterations are never fused between barriers (the
+ * reference's Gauss-Seidel order needs one after every colour). */
 pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step, uint32_t trials,
                                int32_t* variant_out, float* ms_out);
+/* Layout classes of the per-class block-size choice: class = 3 * kind + residency, kind 0 a sheet
+ * held whole in shared memory, 1 the same with mesh / hull colliders, self-collision or general
+ * topology, 2 general topology with its state in HBM, 3 / 4 lean float4 positions (plain /
+ * extended), 5 / 6 lean float arrays (plain / extended); residency 0, 1, 2 for one, two, three
+ * or more of the cloth's CTAs per SM by shared memory. */
+#define PXB_TUNE_CLASSES 21
+/* The kernel configuration in use: block-size variant (0-2: caps of 512 / 768 / 1024 threads),
+ * launch mode, thread fit, and per layout class the variant it runs (PXB_TUNE_CLASSES entries;
+ * may be NULL) with the layout slots the last plain step launched in it (may be NULL). */
+pxb_status pxb_context_get_tuning(pxb_context* ctx, int32_t* variant, int32_t* launch_mode, int32_t* thread_fit,
+                                  int32_t* class_variants, double* class_slots);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Collision primitive: cloth::project_particle (physxcoopa/cloth/cloth_collision.h:386-420)    */

@@ -259,10 +259,11 @@ cloth_grid_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     const int se = sC.rank[0].colour_seg[c + 1];
                     for (int sg = sC.rank[0].colour_seg[c]; sg < se; ++sg) {
                         const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
+                        int i0 = gt;
                         if (h1.w >= 0)
-                            project_segment<1, true, 1>(pos, nullptr, rest + h1.z, lam + h1.w, n, h0, h1, alpha, gt, GT);
+                            project_segment<1, true, 1>(pos, nullptr, rest + h1.z, lam + h1.w, n, h0, h1, alpha, i0, GT);
                         else
-                            project_segment<1, false, 1>(pos, nullptr, rest + h1.z, lam, n, h0, h1, alpha, gt, GT);
+                            project_segment<1, false, 1>(pos, nullptr, rest + h1.z, lam, n, h0, h1, alpha, i0, GT);
                     }
                     grid_sync(gs, epoch, err, sP.grid_wait_polls, sP.grid_extra_arrivals);
                 }

@@ -195,7 +195,8 @@ __device__ __forceinline__ void project_item(PairItem& it, float* lamv, int i, f
 template <int CL, bool kLam, int kItems>
 __device__ __forceinline__ void project_segment(float4* __restrict__ pos, float4* __restrict__ pos_next,
                                                 const float* __restrict__ rest, float* __restrict__ lamv,
-                                                int n_local, int4 h0, int4 h1, float alpha, int tid, int T) {
+                                                int n_local, int4 h0, int4 h1, float alpha, int& i0, int T) {
+    const int tid = i0;
     const int count = h0.x, per_row = h0.z, a_base = h0.w;
     const uint32_t magic = static_cast<uint32_t>(h0.y);
     const int row_stride = h1.x, d = h1.y;
@@ -210,12 +211,14 @@ __device__ __forceinline__ void project_segment(float4* __restrict__ pos, float4
             project_item<kLam>(y, lamv, i + T, alpha);
         }
     } else {
-        for (int i = tid; i < count; i += T) {
+        int i = i0;
+        for (; i < count; i += T) {
             PairItem x;
             load_item<CL, kLam>(x, pos, pos_next, rest, lamv, n_local, i, count, magic, per_row, a_base,
                                 row_stride, d);
             project_item<kLam>(x, lamv, i, alpha);
         }
+        i0 = i - count;  // the thread's first item of the colour's next segment
     }
 }
 
@@ -339,8 +342,9 @@ __device__ __forceinline__ void soa_stage(const SoaPos& P, float* wt_smem, const
 // arithmetic as project_segment; the inverse masses from the table (kWH false) or from HBM.
 template <bool kWH, bool kLam, int kItems>
 __device__ __forceinline__ void project_segment_soa(const SoaPos& P, const float* __restrict__ rest,
-                                                    float* __restrict__ lamv, int4 h0, int4 h1, float alpha, int tid,
+                                                    float* __restrict__ lamv, int4 h0, int4 h1, float alpha, int& i0,
                                                     int T) {
+    const int tid = i0;
     const int count = h0.x, per_row = h0.z, a_base = h0.w;
     const uint32_t magic = static_cast<uint32_t>(h0.y);
     const int row_stride = h1.x, d = h1.y;
@@ -381,13 +385,48 @@ __device__ __forceinline__ void project_segment_soa(const SoaPos& P, const float
             put(i + T, la1, lb1, a1, b1, r1, m1, v1);
         }
     } else {
-        for (int i = tid; i < count; i += T) {
+        int i = i0;
+        for (; i < count; i += T) {
             int la, lb;
             float4 a, b;
             float r, m;
             bool v;
             one(i, la, lb, a, b, r, m, v);
             put(i, la, lb, a, b, r, m, v);
+        }
+        i0 = i - count;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// The constraint iterations of a one-CTA grid cloth, out of line
+// ------------------------------------------------------------------------------------------
+
+// `iters` sweeps of every colour, a CTA barrier after each. Called, not inlined, from the step
+// kernel: the projection loop is then register-allocated on its own instead of sharing the
+// kernel's register budget (64 per thread at 1024 threads) with every value the kernel keeps
+// live across the iterations; the call's register saves happen once per substep.
+// The thread's items continue from segment to segment (items t, t + T, ... of the colour's
+// segments end to end), so every thread of a colour gets the floor or the ceiling of its share,
+// however the items split into segments.
+template <int kItems>
+__device__ __noinline__ void grid_iterations(int iters, int n_colours, const int4* __restrict__ seg4,
+                                             const int* __restrict__ colour_seg, const float* __restrict__ alpha_of,
+                                             float4* __restrict__ pos, const float* __restrict__ RG,
+                                             float* __restrict__ U, int n_local, int tid, int T) {
+    for (int it = 0; it < iters; ++it) {
+        for (int c = 0; c < n_colours; ++c) {
+            const float alpha = alpha_of[c];
+            const int se = colour_seg[c + 1];
+            int i0 = tid;
+            for (int sg = colour_seg[c]; sg < se; ++sg) {
+                const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
+                if (h1.w >= 0)
+                    project_segment<1, true, kItems>(pos, nullptr, RG + h1.z, U + h1.w, n_local, h0, h1, alpha, i0, T);
+                else
+                    project_segment<1, false, kItems>(pos, nullptr, RG + h1.z, U, n_local, h0, h1, alpha, i0, T);
+            }
+            __syncthreads();
         }
     }
 }
@@ -654,27 +693,38 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 return;
             }
         }
+        // Float4 positions on one CTA: the colour loop out of line (float arrays measured slower
+        // that way and stay inline).
+        if constexpr (CL == 1 && !kG && !kS) {
+            constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
+            grid_iterations<kItems>(iters, sC.n_colours, seg4, sC.rank[0].colour_seg, sP.alpha, pos, RG, U, n_local, tid, T);
+            return;
+        }
         const int n_colours = sC.n_colours;
         const uint32_t cross = sC.cross_mask;
         for (int it = 0; it < iters; ++it) {
             for (int c = 0; c < n_colours; ++c) {
                 const float alpha = sP.alpha[c];
                 const int se = sC.rank[rank].colour_seg[c + 1];
+                // The thread's items continue from segment to segment (items t, t + T, ... of
+                // the colour's segments end to end), so every thread of the colour gets the
+                // floor or the ceiling of its share, however the items split into segments.
+                int i0 = tid;
                 for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
                     const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
                     constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
                     if constexpr (kS) {
                         if (pos.w_hbm) {
-                            if (h1.w >= 0) project_segment_soa<true, true, kItems>(pos, RG + h1.z, U + h1.w, h0, h1, alpha, tid, T);
-                            else project_segment_soa<true, false, kItems>(pos, RG + h1.z, U, h0, h1, alpha, tid, T);
+                            if (h1.w >= 0) project_segment_soa<true, true, kItems>(pos, RG + h1.z, U + h1.w, h0, h1, alpha, i0, T);
+                            else project_segment_soa<true, false, kItems>(pos, RG + h1.z, U, h0, h1, alpha, i0, T);
                         } else {
-                            if (h1.w >= 0) project_segment_soa<false, true, kItems>(pos, RG + h1.z, U + h1.w, h0, h1, alpha, tid, T);
-                            else project_segment_soa<false, false, kItems>(pos, RG + h1.z, U, h0, h1, alpha, tid, T);
+                            if (h1.w >= 0) project_segment_soa<false, true, kItems>(pos, RG + h1.z, U + h1.w, h0, h1, alpha, i0, T);
+                            else project_segment_soa<false, false, kItems>(pos, RG + h1.z, U, h0, h1, alpha, i0, T);
                         }
                     } else if (h1.w >= 0) {
-                        project_segment<CL, true, kItems>(pos, pos_next, RG + h1.z, U + h1.w, n_local, h0, h1, alpha, tid, T);
+                        project_segment<CL, true, kItems>(pos, pos_next, RG + h1.z, U + h1.w, n_local, h0, h1, alpha, i0, T);
                     } else {
-                        project_segment<CL, false, kItems>(pos, pos_next, RG + h1.z, U, n_local, h0, h1, alpha, tid, T);
+                        project_segment<CL, false, kItems>(pos, pos_next, RG + h1.z, U, n_local, h0, h1, alpha, i0, T);
                     }
                 }
                 // Colours that join rows need every rank to see the others' writes; a pair

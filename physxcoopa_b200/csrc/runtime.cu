@@ -1267,18 +1267,10 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     // (shared memory, threads, registers): one launch per group, so a small cloth is not
     // launched with a large one's shared memory and thread count. Larger cloths first within a
     // group, so the block scheduler's tail holds the small ones.
-    const int cap = cloth_variant_threads(cloth_variant);
-    const int regs = cloth_variant_registers(cloth_variant);
-    std::vector<int> fit(n);
     auto launch_smem = [&](const ClothEntry& e) {
         const int base = warm ? e.warm_smem : e.dev.smem_bytes;
         return self_on(e) ? std::max(base, e.self_smem) : base;
     };
-    auto launch_threads = [&](const ClothEntry& e) {
-        // the warm-start kernel runs whole warpgroups (the network's tiles are 128 rows)
-        return warm ? std::min(cap, std::max(128, (e.threads + 127) & ~127)) : std::min(e.threads, cap);
-    };
-    for (uint32_t k = 0; k < n; ++k) fit[k] = ctas_per_sm(launch_smem(*ents[k]), launch_threads(*ents[k]), regs);
     // cloths with a mesh or hull collider, with self-collision or of general topology launch the
     // kernel with those stages compiled in (1); general-topology cloths with their state in HBM
     // launch its HBM instantiation (2)
@@ -1293,6 +1285,37 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     for (uint32_t k = 0; k < n; ++k)
         if (ents[k]->lean)  // lean instantiations: float4 (3, 4), float arrays (5, 6)
             has_geo[k] = static_cast<uint8_t>((ents[k]->soa ? 5 : 3) + has_geo[k]);
+    // Block-size variant of each cloth: its layout class's (autotuned), else the context's. A
+    // warm-start step runs the context's.
+    auto smem_ctas = [&](const ClothEntry& e) {
+        return std::max(1, 233472 / (launch_smem(e) + kClothStaticSmem + 1024));
+    };
+    std::vector<int> tclass(n), var(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        tclass[k] = 3 * has_geo[k] + std::min(smem_ctas(*ents[k]), 3) - 1;
+        var[k] = (!warm && class_variant[tclass[k]] > 0) ? class_variant[tclass[k]] - 1 : cloth_variant;
+    }
+    if (!warm) {
+        for (double& w : class_work) w = 0.0;
+        for (uint32_t k = 0; k < n; ++k)
+            if (!ents[k]->grid) class_work[tclass[k]] += static_cast<double>(ents[k]->n_layout);
+    }
+    auto launch_threads = [&](const ClothEntry& e, int v) {
+        const int cap = cloth_variant_threads(v);
+        // the warm-start kernel runs whole warpgroups (the network's tiles are 128 rows)
+        if (warm) return std::min(cap, std::max(128, (e.threads + 127) & ~127));
+        int t = std::min(e.threads, cap);
+        if (thread_fit && e.ranks.size() == 1 && !e.grid && !e.list) {
+            // the CTAs shared memory lets an SM hold split the threads the variant's registers allow
+            const int regs = cloth_variant_registers(v);
+            const int share = (65536 / (((regs + 7) & ~7) * smem_ctas(e))) & ~31;
+            t = std::min(t, std::max(64, share));
+        }
+        return t;
+    };
+    std::vector<int> fit(n);
+    for (uint32_t k = 0; k < n; ++k)
+        fit[k] = ctas_per_sm(launch_smem(*ents[k]), launch_threads(*ents[k], var[k]), cloth_variant_registers(var[k]));
     std::vector<uint32_t> perm(n);
     for (uint32_t k = 0; k < n; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
@@ -1301,6 +1324,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         if (rx != ry) return rx < ry;
         if (fit[x] != fit[y]) return fit[x] < fit[y];
         if (has_geo[x] != has_geo[y]) return has_geo[x] < has_geo[y];
+        if (var[x] != var[y]) return var[x] < var[y];
         return ents[x]->n_layout > ents[y]->n_layout;
     });
     const pxb::hm::V3 g = pxb::hm::ld(sd->gravity);
@@ -1407,17 +1431,18 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
             ++enqueued;
         }
     }
-    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; int ext; int fit; };
+    struct Group { uint32_t g0, g1; int cluster, threads, smem; double work; int ext; int fit; int variant; };
     std::vector<Group> groups;
     for (uint32_t g0 = 0; g0 < n_plain;) {
         const int cluster = static_cast<int>(ents[perm[g0]]->ranks.size());
         const int group_fit = fit[perm[g0]];
         const int ext = has_geo[perm[g0]];
-        Group G{g0, g0, cluster, 64, 0, 0.0, ext, group_fit};
+        const int gv = var[perm[g0]];
+        Group G{g0, g0, cluster, 64, 0, 0.0, ext, group_fit, gv};
         while (G.g1 < n_plain && static_cast<int>(ents[perm[G.g1]]->ranks.size()) == cluster &&
-               fit[perm[G.g1]] == group_fit && has_geo[perm[G.g1]] == ext) {
+               fit[perm[G.g1]] == group_fit && has_geo[perm[G.g1]] == ext && var[perm[G.g1]] == gv) {
             const ClothEntry& e = *ents[perm[G.g1]];
-            G.threads = std::max(G.threads, launch_threads(e));
+            G.threads = std::max(G.threads, launch_threads(e, gv));
             G.smem = std::max(G.smem, launch_smem(e));
             G.work += static_cast<double>(e.n_layout);
             ++G.g1;
@@ -1437,7 +1462,7 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const Group& G = groups[gi];
         cudaStream_t st = fan_out ? side[gi % kSideStreams] : stream;
-        cudaError_t le = launch_cloth_step(cloth_variant, G.cluster, static_cast<const PxbClothDev*>(d_registry.p),
+        cudaError_t le = launch_cloth_step(G.variant, G.cluster, static_cast<const PxbClothDev*>(d_registry.p),
                                            reinterpret_cast<const PxbClothStep*>(db) + G.g0,
                                            reinterpret_cast<const PxbDevCollider*>(db + o_cols),
                                            reinterpret_cast<const pxb_gravity_source*>(db + o_src),
@@ -1476,6 +1501,11 @@ pxb_status pxb_context::step_cloths(const pxb_cloth_step_desc* sd, const WarmCfg
         for (uint32_t k = 0; k < n; k += 21) {  // which kernel instantiation each cloth launches
             uint64_t bits = 0;
             for (uint32_t j = k; j < std::min(n, k + 21); ++j) bits |= uint64_t(has_geo[j]) << (3 * (j - k));
+            key.push_back(bits);
+        }
+        for (uint32_t k = 0; k < n; k += 32) {  // and with which block-size variant
+            uint64_t bits = 0;
+            for (uint32_t j = k; j < std::min(n, k + 32); ++j) bits |= uint64_t(var[j]) << (2 * (j - k));
             key.push_back(bits);
         }
         if (graph_exec && key == graph_key) {
@@ -1999,6 +2029,26 @@ pxb_status pxb_context_set_launch_mode(pxb_context* ctx, int32_t mode) {
     return PXB_OK;
 }
 
+pxb_status pxb_context_get_tuning(pxb_context* ctx, int32_t* variant, int32_t* launch_mode, int32_t* thread_fit,
+                                  int32_t* class_variants, double* class_slots) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    if (variant) *variant = ctx->cloth_variant;
+    if (launch_mode) *launch_mode = ctx->launch_mode;
+    if (thread_fit) *thread_fit = ctx->thread_fit;
+    for (int c = 0; c < PXB_TUNE_CLASSES; ++c) {
+        if (class_variants) class_variants[c] = ctx->class_variant[c] > 0 ? ctx->class_variant[c] - 1 : ctx->cloth_variant;
+        if (class_slots) class_slots[c] = ctx->class_work[c];
+    }
+    return PXB_OK;
+}
+
+pxb_status pxb_context_set_thread_fit(pxb_context* ctx, int32_t mode) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    if (mode != 0 && mode != 1) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "thread fit must be 0 or 1");
+    ctx->thread_fit = mode;
+    return PXB_OK;
+}
+
 pxb_status pxb_context_set_lean_arrays(pxb_context* ctx, int32_t enable) {
     if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
     ctx->soa_layouts = enable != 0;
@@ -2010,6 +2060,7 @@ pxb_status pxb_context_set_cloth_variant(pxb_context* ctx, int32_t variant) {
     if (variant < 0 || variant >= kClothVariants)
         return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "variant must be in [0, %d)", kClothVariants);
     ctx->cloth_variant = variant;
+    std::memset(ctx->class_variant, 0, sizeof(ctx->class_variant));  // every class at this variant
     return PXB_OK;
 }
 
@@ -2063,25 +2114,63 @@ pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     const int before = ctx->cloth_variant, before_mode = ctx->launch_mode;
+    int before_class[PXB_TUNE_CLASSES];
+    std::memcpy(before_class, ctx->class_variant, sizeof(before_class));
+    std::memset(ctx->class_variant, 0, sizeof(ctx->class_variant));
     int best = before + kClothVariants * before_mode;
     float best_ms = 0.0f;
     pxb_status st = PXB_OK;
+    // one warm-up step (attribute set-up), then `trials` timed steps
+    auto time_steps = [&](float& ms) -> pxb_status {
+        if (pxb_status s = ctx->step_cloths(step)) return s;
+        cudaEventRecord(t0, ctx->stream);
+        for (uint32_t r = 0; r < trials; ++r)
+            if (pxb_status s = ctx->step_cloths(step)) return s;
+        cudaEventRecord(t1, ctx->stream);
+        if (cudaEventSynchronize(t1) != cudaSuccess) return ctx->fail(PXB_ERR_CUDA, "autotune timing");
+        ms = 0.0f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        ms /= static_cast<float>(trials);
+        return PXB_OK;
+    };
     for (int v = 0; v < 2 * kClothVariants && !st; ++v) {
         ctx->cloth_variant = v % kClothVariants;
         ctx->launch_mode = v / kClothVariants;
-        st = ctx->step_cloths(step);  // warm-up (and attribute set-up) of this variant
-        if (st) break;
-        cudaEventRecord(t0, ctx->stream);
-        for (uint32_t r = 0; r < trials && !st; ++r) st = ctx->step_cloths(step);
-        cudaEventRecord(t1, ctx->stream);
-        if (cudaEventSynchronize(t1) != cudaSuccess) st = ctx->fail(PXB_ERR_CUDA, "autotune timing");
         float ms = 0.0f;
-        cudaEventElapsedTime(&ms, t0, t1);
-        ms /= static_cast<float>(trials);
+        st = time_steps(ms);
+        if (st) break;
         if (ms_out) ms_out[v] = ms;
         if (v == 0 || ms < best_ms) {
             best_ms = ms;
             best = v;
+        }
+    }
+    // Per layout class, largest share first: the other variants for its cloths alone, kept when
+    // faster by more than the timing's noise (0.3 %).
+    if (!st) {
+        ctx->cloth_variant = best % kClothVariants;
+        ctx->launch_mode = best / kClothVariants;
+        float cur = 0.0f;
+        st = time_steps(cur);  // also records each class's share under the chosen pair
+        std::vector<int> classes;
+        for (int c = 0; c < PXB_TUNE_CLASSES; ++c)
+            if (ctx->class_work[c] > 0.0) classes.push_back(c);
+        std::stable_sort(classes.begin(), classes.end(),
+                         [&](int a, int b) { return ctx->class_work[a] > ctx->class_work[b]; });
+        for (size_t ci = 0; ci < classes.size() && classes.size() > 1 && !st; ++ci) {
+            const int c = classes[ci];
+            int keep = 0;
+            for (int v = 0; v < kClothVariants && !st; ++v) {
+                if (v == ctx->cloth_variant) continue;
+                ctx->class_variant[c] = v + 1;
+                float ms = 0.0f;
+                st = time_steps(ms);
+                if (!st && ms < cur * 0.997f) {
+                    cur = ms;
+                    keep = v + 1;
+                }
+            }
+            ctx->class_variant[c] = keep;
         }
     }
     cudaEventDestroy(t0);
@@ -2092,6 +2181,7 @@ pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step
     ctx->last_step.clear();
     ctx->cloth_variant = st ? before : best % kClothVariants;
     ctx->launch_mode = st ? before_mode : best / kClothVariants;
+    if (st) std::memcpy(ctx->class_variant, before_class, sizeof(before_class));
     if (st) return st;
     if (rs) return rs;
     if (variant_out) *variant_out = best;

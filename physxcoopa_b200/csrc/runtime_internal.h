@@ -188,6 +188,15 @@ struct pxb_context {
     }
     int cloth_variant = 0;  // kernel block-size cap, see pxb_kernels.h (autotuned or set)
     int launch_mode = 1;    // 1: persistent CTAs popping a work queue per launch group; 0: one CTA per cloth
+    // 1: a one-CTA grid cloth whose shared memory lets an SM hold k of its CTAs launches with
+    // 1/k of the threads the kernel's register file allows, so k CTAs are resident at once;
+    // 0: it launches with its own thread count (half its largest colour, up to the cap)
+    int thread_fit = 1;
+    // Block-size variant per layout class (PXB_TUNE_CLASSES: kernel instantiation x how many of
+    // the cloth's CTAs shared memory lets an SM hold), stored + 1 (0: cloth_variant); set by the
+    // autotuner. The last plain step records the layout slots each class launched.
+    int class_variant[PXB_TUNE_CLASSES] = {};
+    double class_work[PXB_TUNE_CLASSES] = {};
     bool soa_layouts = true;  // cloths added from now on may take the float-array lean layout
     unsigned char* gather_scratch = nullptr;  // pxb_cloths_gather_positions_device's static scratch
     DevBuf d_tune;          // cloth state saved across an autotune

@@ -89,6 +89,9 @@ SIGNATURES = {
     "pxb_context_set_cloth_variant": ([P, C.c_int32], C.c_int),
     "pxb_context_set_launch_mode": ([P, C.c_int32], C.c_int),
     "pxb_context_set_lean_arrays": ([P, C.c_int32], C.c_int),
+    "pxb_context_set_thread_fit": ([P, C.c_int32], C.c_int),
+    "pxb_context_get_tuning": ([P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                C.POINTER(C.c_int32), C.POINTER(C.c_double)], C.c_int),
     "pxb_context_set_wait_test": ([P, u32, u32], C.c_int),
     "pxb_strands_add": ([P, C.POINTER(A.StrandSetDesc), C.POINTER(u64)], C.c_int),
     "pxb_strands_remove": ([P, u64], C.c_int),
@@ -543,6 +546,27 @@ class Context:
         """pxb_context_set_lean_arrays: cloths added afterwards may (1) or may not (0) take the
         one-CTA float-array layout."""
         self._check(self.lib.pxb_context_set_lean_arrays(self.h, 1 if enable else 0), "set_lean_arrays")
+
+    def set_thread_fit(self, mode):
+        """pxb_context_set_thread_fit: 1 splits an SM's threads between the CTAs of one-CTA grid
+        cloths that shared memory lets it hold, 0 gives each its own thread count."""
+        self._check(self.lib.pxb_context_set_thread_fit(self.h, mode), "set_thread_fit")
+
+    TUNE_CLASS_KINDS = ("whole in shared memory", "whole in shared memory, extended stages",
+                        "general topology in HBM", "lean float4", "lean float4, extended stages",
+                        "lean float arrays", "lean float arrays, extended stages")
+
+    def tuning(self):
+        """pxb_context_get_tuning: the block-size variant, launch mode, thread fit, and per layout
+        class that the last plain step launched, its variant and its layout slots."""
+        v, m, f = C.c_int32(), C.c_int32(), C.c_int32()
+        cv = (C.c_int32 * 21)()
+        cw = (C.c_double * 21)()
+        self._check(self.lib.pxb_context_get_tuning(self.h, C.byref(v), C.byref(m), C.byref(f), cv, cw), "tuning")
+        classes = [{"kind": self.TUNE_CLASS_KINDS[c // 3], "ctas_per_sm_by_smem": ("1", "2", "3+")[c % 3],
+                    "block_cap": (512, 768, 1024)[cv[c]], "slots": int(cw[c])}
+                   for c in range(21) if cw[c] > 0]
+        return {"variant": v.value, "launch_mode": m.value, "thread_fit": f.value, "classes": classes}
 
     def set_launch_mode(self, mode):
         """pxb_context_set_launch_mode: 1 persistent work-queue kernels, 0 one CTA per cloth."""

@@ -104,6 +104,8 @@ def parse():
     ap.add_argument("--thread-fit", type=int, choices=[0, 1], default=None,
                     help="threads per CTA of one-CTA grid sheets: 1 splits an SM between the CTAs its shared "
                          "memory holds, 0 gives each sheet its own count")
+    ap.add_argument("--lean-mid", type=int, choices=[0, 1], default=None,
+                    help="sheets an SM holds one of when held whole: 1 lean where that holds two or more, 0 whole")
     ap.add_argument("--no-lean-arrays", action="store_true",
                     help="lay sheets of sides 110-128 out on 2-CTA clusters instead of one CTA with float arrays")
     return ap.parse_args()
@@ -774,6 +776,8 @@ def main():
         ctx.set_lean_arrays(False)
     if args.thread_fit is not None:
         ctx.set_thread_fit(args.thread_fit)
+    if args.lean_mid is not None:
+        ctx.set_lean_mid(args.lean_mid)
     if sc.geometries:
         from physxcoopa_b200 import scenes
         scenes.register_geometries(ctx, sc)

@@ -510,6 +510,12 @@ pxb_status pxb_context_set_launch_mode(pxb_context* ctx, int32_t mode);
  * waits at a colour barrier). Results are identical; only speed differs. */
 pxb_status pxb_context_set_thread_fit(pxb_context* ctx, int32_t mode);
 /* Layout choice for cloths added from now on (no counterpart in the reference). With `enable`
+ * (default), a sheet small enough to be held whole in one CTA's shared memory, but so large that
+ * an SM then holds only one of its CTAs, takes the lean layout (positions alone in shared memory,
+ * rest lengths and lambdas read in place in HBM) where that lets an SM hold two or more; with 0 it
+ * is held whole. Results are identical; only speed differs. */
+pxb_status pxb_context_set_lean_mid(pxb_context* ctx, int32_t enable);
+/* Layout choice for cloths added from now on (no counterpart in the reference). With `enable`
  * (default), a grid cloth too large for one CTA's shared memory as float4 positions but small
  * enough as float arrays (12 bytes per particle plus a one-byte index into a table of its
  * distinct inverse masses; sheets up to 128 x 128) runs on one CTA in that form; with 0 it runs

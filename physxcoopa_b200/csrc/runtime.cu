@@ -805,7 +805,10 @@ pxb_status pxb_context::upload_anchor_records(ClothEntry& e) {
 // cluster size, per-rank colour segments (verified item by item against the constraint lists)
 // and the shared-memory layout. Needs no context, so the layout can be planned on any host.
 // soa_layouts: the float-array lean layout may be chosen (pxb_context_set_lean_arrays).
-static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string& err, bool soa_layouts = true) {
+// lean_mid: a sheet held whole whose shared memory lets an SM hold only one of its CTAs takes the
+// lean layout instead where that lets an SM hold two or more (pxb_context_set_lean_mid).
+static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string& err, bool soa_layouts = true,
+                             bool lean_mid = true) {
     char buf[512];
     auto fail = [&](pxb_status st, const char* fmt, auto... args) {
         snprintf(buf, sizeof(buf), fmt, args...);
@@ -914,9 +917,12 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
     const struct { int cl; bool lean, soa; } tries[] = {{1, false, false}, {1, true, false}, {1, true, true},
                                                         {2, true, false}, {2, false, false}, {4, false, false},
                                                         {8, false, false}};
+    auto smem_ctas = [](int bytes) { return 233472 / (bytes + kClothStaticSmem + 1024); };
+    bool whole_fits = false;  // held whole, one CTA per SM: kept unless the lean layout does better
     for (const auto& t : tries) {
         if (placed) break;
         if (t.soa && !soa_layouts) continue;
+        if (whole_fits && !(t.cl == 1 && t.lean && !t.soa)) break;
         std::vector<int32_t> padded;
         if (!build_ranks(e, cs, rest_ref, t.cl, padded, max_colour)) continue;
         e.lean = t.lean;
@@ -924,6 +930,19 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
         e.rest_ref.swap(padded);
         layout_ranks(e);
         if (e.dev.smem_bytes <= kMaxDynamicSmem && (!t.lean || e.warm_smem <= kMaxDynamicSmem)) placed = true;
+        if (placed && whole_fits && smem_ctas(e.dev.smem_bytes) < 2) placed = false;
+        if (placed && lean_mid && t.cl == 1 && !t.lean && smem_ctas(e.dev.smem_bytes) < 2) {
+            whole_fits = true;
+            placed = false;
+        }
+    }
+    if (!placed && whole_fits) {  // back to the sheet held whole
+        std::vector<int32_t> padded;
+        build_ranks(e, cs, rest_ref, 1, padded, max_colour);
+        e.lean = e.soa = false;
+        e.rest_ref.swap(padded);
+        layout_ranks(e);
+        placed = true;
     }
     if (!placed) e.lean = e.soa = false;
     if (!placed) {
@@ -945,7 +964,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     if (!d || !id_out) return fail(PXB_ERR_INVALID_ARGUMENT, "null argument");
     ClothEntry e;
     std::string msg;
-    if (pxb_status st = plan_cloth(d, e, msg, soa_layouts)) return fail(st, "%s", msg.c_str());
+    if (pxb_status st = plan_cloth(d, e, msg, soa_layouts, lean_mid)) return fail(st, "%s", msg.c_str());
     const uint32_t n = d->n_particles;
 
     // --- anchors: one device record per anchor; a particle follows its LAST anchor ---
@@ -2046,6 +2065,12 @@ pxb_status pxb_context_set_thread_fit(pxb_context* ctx, int32_t mode) {
     if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
     if (mode != 0 && mode != 1) return ctx->fail(PXB_ERR_INVALID_ARGUMENT, "thread fit must be 0 or 1");
     ctx->thread_fit = mode;
+    return PXB_OK;
+}
+
+pxb_status pxb_context_set_lean_mid(pxb_context* ctx, int32_t enable) {
+    if (!ctx) return PXB_ERR_INVALID_ARGUMENT;
+    ctx->lean_mid = enable != 0;
     return PXB_OK;
 }
 

@@ -198,6 +198,7 @@ struct pxb_context {
     int class_variant[PXB_TUNE_CLASSES] = {};
     double class_work[PXB_TUNE_CLASSES] = {};
     bool soa_layouts = true;  // cloths added from now on may take the float-array lean layout
+    bool lean_mid = true;     // ... and the lean layout where it lets an SM hold more of their CTAs
     unsigned char* gather_scratch = nullptr;  // pxb_cloths_gather_positions_device's static scratch
     DevBuf d_tune;          // cloth state saved across an autotune
     // Pipelined position read-back (pxb_cloths_read_positions_async): two device snapshots,

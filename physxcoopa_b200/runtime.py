@@ -90,6 +90,7 @@ SIGNATURES = {
     "pxb_context_set_launch_mode": ([P, C.c_int32], C.c_int),
     "pxb_context_set_lean_arrays": ([P, C.c_int32], C.c_int),
     "pxb_context_set_thread_fit": ([P, C.c_int32], C.c_int),
+    "pxb_context_set_lean_mid": ([P, C.c_int32], C.c_int),
     "pxb_context_get_tuning": ([P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)], C.c_int),
     "pxb_context_set_wait_test": ([P, u32, u32], C.c_int),
@@ -546,6 +547,11 @@ class Context:
         """pxb_context_set_lean_arrays: cloths added afterwards may (1) or may not (0) take the
         one-CTA float-array layout."""
         self._check(self.lib.pxb_context_set_lean_arrays(self.h, 1 if enable else 0), "set_lean_arrays")
+
+    def set_lean_mid(self, enable):
+        """pxb_context_set_lean_mid: sheets added afterwards that an SM would hold one of when held
+        whole take the lean layout where it holds two or more (1), or stay whole (0)."""
+        self._check(self.lib.pxb_context_set_lean_mid(self.h, 1 if enable else 0), "set_lean_mid")
 
     def set_thread_fit(self, mode):
         """pxb_context_set_thread_fit: 1 splits an SM's threads between the CTAs of one-CTA grid

@@ -64,12 +64,12 @@ def run_pair(ctx, cloth, cols, steps, iterations=10):
 
 @pytest.mark.parametrize("side", [9, 24, 48, 64, 80])
 def test_folding_sheet_equals_oracle(ctx, side):
-    """Up to 64 the sheet is all in shared memory; at 80 it is lean (positions only in shared
-    memory, rest lengths and lambdas in HBM) and the hash tables take the room after the
-    positions."""
+    """Up to 44 the sheet is all in shared memory; from 48 (where an SM would hold only one CTA of
+    the whole sheet) it is lean (positions only in shared memory, rest lengths and lambdas in HBM)
+    and the hash tables take the room after the positions."""
     cloth, cols = folding_sheet(side)
     plan = R.plan_cloth(cloth)
-    assert plan["n_ranks"] == 1 and plan["self_collision"] == 1 and plan["lean"] == (side > 64)
+    assert plan["n_ranks"] == 1 and plan["self_collision"] == 1 and plan["lean"] == (side > 44)
     gpu, orc = run_pair(ctx, cloth, cols, 1)
     assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-5
     assert_equal_particles(gpu, orc.particles, "step 1")

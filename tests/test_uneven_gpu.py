@@ -36,7 +36,7 @@ def pick(per_layout):
     want = {"small": per_layout, "lean1": per_layout, "lean2": per_layout}
     out = []
     for i, s in enumerate(PLAN):
-        key = "small" if s.side <= 64 else ("lean1" if s.side <= 109 else "lean2")
+        key = "small" if s.side <= 44 else ("lean1" if s.side <= 109 else "lean2")
         if want[key] > 0:
             want[key] -= 1
             out.append(i)

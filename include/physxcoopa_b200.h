@@ -298,6 +298,8 @@ typedef struct pxb_cloth_plan {
                                  layout would need a larger cluster); 2: the same on one CTA
                                  with the positions as float arrays and an index into the
                                  cloth's distinct inverse masses (pxb_context_set_lean_arrays) */
+    int32_t phases;           /* barrier-separated phases per iteration: colours in a row that
+                                 touch disjoint particles share one (one CTA only; else n_colours) */
 } pxb_cloth_plan;
 
 /* Plans a cloth without a context or a GPU: validates it exactly as pxb_cloth_add does and

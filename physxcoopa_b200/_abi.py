@@ -142,7 +142,7 @@ class ClothPlan(C.Structure):
                 ("smem_bytes", C.c_int32), ("n_colours", C.c_int32), ("n_segments", C.c_int32),
                 ("layout_slots", C.c_int32), ("constraint_slots", C.c_int32),
                 ("self_collision", C.c_int32), ("self_smem_bytes", C.c_int32), ("topology", C.c_int32),
-                ("lean", C.c_int32)]
+                ("lean", C.c_int32), ("phases", C.c_int32)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

@@ -409,16 +409,18 @@ __device__ __forceinline__ void project_segment_soa(const SoaPos& P, const float
 // The thread's items continue from segment to segment (items t, t + T, ... of the colour's
 // segments end to end), so every thread of a colour gets the floor or the ceiling of its share,
 // however the items split into segments.
+// Bit c of sync_mask clear: colours c and c + 1 touch disjoint particles and run as one phase
+// (no barrier between them; the thread's items continue from one into the other).
 template <int kItems>
 __device__ __noinline__ void grid_iterations(int iters, int n_colours, const int4* __restrict__ seg4,
                                              const int* __restrict__ colour_seg, const float* __restrict__ alpha_of,
                                              float4* __restrict__ pos, const float* __restrict__ RG,
-                                             float* __restrict__ U, int n_local, int tid, int T) {
+                                             float* __restrict__ U, int n_local, int tid, int T, uint32_t sync_mask) {
+    int i0 = tid;
     for (int it = 0; it < iters; ++it) {
         for (int c = 0; c < n_colours; ++c) {
             const float alpha = alpha_of[c];
             const int se = colour_seg[c + 1];
-            int i0 = tid;
             for (int sg = colour_seg[c]; sg < se; ++sg) {
                 const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
                 if (h1.w >= 0)
@@ -426,7 +428,10 @@ __device__ __noinline__ void grid_iterations(int iters, int n_colours, const int
                 else
                     project_segment<1, false, kItems>(pos, nullptr, RG + h1.z, U, n_local, h0, h1, alpha, i0, T);
             }
-            __syncthreads();
+            if ((sync_mask >> c) & 1u) {
+                __syncthreads();
+                i0 = tid;
+            }
         }
     }
 }
@@ -697,19 +702,22 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
         // that way and stay inline).
         if constexpr (CL == 1 && !kG && !kS) {
             constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
-            grid_iterations<kItems>(iters, sC.n_colours, seg4, sC.rank[0].colour_seg, sP.alpha, pos, RG, U, n_local, tid, T);
+            grid_iterations<kItems>(iters, sC.n_colours, seg4, sC.rank[0].colour_seg, sP.alpha, pos, RG, U, n_local, tid, T,
+                                    sC.sync_mask);
             return;
         }
         const int n_colours = sC.n_colours;
         const uint32_t cross = sC.cross_mask;
+        // one CTA: a clear bit joins colour c and c + 1 into one phase (disjoint particles)
+        const uint32_t sync_mask = CL == 1 ? sC.sync_mask : 0xffffffffu;
+        // The thread's items continue from segment to segment (items t, t + T, ... of the
+        // phase's segments end to end), so every thread gets the floor or the ceiling of its
+        // share, however the items split into segments.
+        int i0 = tid;
         for (int it = 0; it < iters; ++it) {
             for (int c = 0; c < n_colours; ++c) {
                 const float alpha = sP.alpha[c];
                 const int se = sC.rank[rank].colour_seg[c + 1];
-                // The thread's items continue from segment to segment (items t, t + T, ... of
-                // the colour's segments end to end), so every thread of the colour gets the
-                // floor or the ceiling of its share, however the items split into segments.
-                int i0 = tid;
                 for (int sg = sC.rank[rank].colour_seg[c]; sg < se; ++sg) {
                     const int4 h0 = seg4[2 * sg], h1 = seg4[2 * sg + 1];
                     constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
@@ -732,8 +740,13 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                 // the cluster: the tether stage reads anchors anywhere in the cloth.
                 const int cn = (c + 1 < n_colours) ? c + 1 : 0;
                 const bool last = it + 1 == iters && c + 1 == n_colours;
-                if (CL > 1 && (((cross >> c) | (cross >> cn)) & 1u || last)) cluster_or_block_sync<CL>();
-                else __syncthreads();
+                if (CL > 1 && (((cross >> c) | (cross >> cn)) & 1u || last)) {
+                    cluster_or_block_sync<CL>();
+                    i0 = tid;
+                } else if ((sync_mask >> c) & 1u) {
+                    __syncthreads();
+                    i0 = tid;
+                }
             }
         }
     };

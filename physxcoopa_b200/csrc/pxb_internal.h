@@ -83,7 +83,8 @@ struct PxbClothDev {
     int32_t threads;            // block size this cloth runs with
     int32_t aero_grid;          // triangles are exactly make_grid_cloth's (cloth_builder.h:200-207)
     uint32_t stretch_mask;      // bit c: colour c comes from the stretch list
-    int32_t pad0;
+    uint32_t sync_mask;         // one CTA: bit c set = a CTA barrier after colour c (clear: colours
+                                // c and c + 1 touch disjoint particles and run as one phase)
     const float* edge_rest;     // [6][n_layout] rest length to the grid neighbour (+x, -x, +y,
                                 // -y, +x+y, -x-y), 0 where no stretch constraint joins them
     float4* disp;               // [n_layout] warm-start displacement scratch

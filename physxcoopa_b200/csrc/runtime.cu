@@ -805,6 +805,49 @@ pxb_status pxb_context::upload_anchor_records(ClothEntry& e) {
 // cluster size, per-rank colour segments (verified item by item against the constraint lists)
 // and the shared-memory layout. Needs no context, so the layout can be planned on any host.
 // soa_layouts: the float-array lean layout may be chosen (pxb_context_set_lean_arrays).
+// Barriers of a one-CTA grid cloth's colour loop: the reference projects colour after colour, so
+// each colour waits for the one before. Where two consecutive colours touch disjoint particles
+// (the bend colours of phases 0 and 1, or 2 and 3, along a row or a column), projecting them
+// together gives the same result as one after the other: they form one phase, with no barrier
+// between them. A phase grows while its next colour is disjoint from every colour in it. Bit c of
+// the mask: a barrier after colour c. Clusters and the whole-GPU path keep every barrier.
+static uint32_t colour_sync_mask(const ClothEntry& e) {
+    uint32_t mask = 0xffffffffu;
+    if (e.ranks.size() != 1 || e.grid || e.list || e.n_colours < 2) return mask;
+    const ClothEntry::Rank& rk = e.ranks[0];
+    const int n_slots = rk.n_rows * e.S;
+    std::vector<uint8_t> phase(static_cast<size_t>(n_slots), 0);  // slot -> phase id + 1 (mod 255)
+    int pid = 1;
+    auto touch = [&](int c, bool mark, bool& clash) {
+        for (int sg = rk.seg_begin + rk.colour_seg[c]; sg < rk.seg_begin + rk.colour_seg[c + 1]; ++sg) {
+            const PxbSeg& g = e.segs[sg];
+            for (int i = 0; i < g.count; ++i) {
+                const int row = i / g.per_row;
+                const int la = g.a_base + row * g.row_stride + (i - row * g.per_row), lb = la + g.d;
+                for (int l : {la, lb}) {
+                    if (l < 0 || l >= n_slots) { clash = true; continue; }
+                    if (mark) phase[l] = static_cast<uint8_t>(pid);
+                    else if (phase[l] == pid) clash = true;
+                }
+            }
+        }
+    };
+    bool dummy = false;
+    touch(0, true, dummy);
+    for (int c = 1; c < e.n_colours; ++c) {
+        bool clash = false;
+        touch(c, false, clash);
+        if (clash) {
+            pid = pid % 255 + 1;  // a new phase: stale marks of an old id are ignored below
+            if (pid == 1) std::fill(phase.begin(), phase.end(), 0);
+        } else {
+            mask &= ~(1u << (c - 1));  // colour c joins colour c - 1's phase
+        }
+        touch(c, true, dummy);
+    }
+    return mask;
+}
+
 // lean_mid: a sheet held whole whose shared memory lets an SM hold only one of its CTAs takes the
 // lean layout instead where that lets an SM hold two or more (pxb_context_set_lean_mid).
 static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string& err, bool soa_layouts = true,
@@ -1049,6 +1092,7 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
     e.dev.rows_per_rank = e.ranks[0].n_rows;
     e.dev.n_colours = e.n_colours;
     e.dev.cross_mask = e.cross_mask;
+    e.dev.sync_mask = colour_sync_mask(e);
     e.dev.n_layout = e.n_layout;
     e.dev.n_real = static_cast<int32_t>(n);
     e.dev.columns = e.cols;
@@ -1707,6 +1751,11 @@ pxb_status pxb_cloth_plan_layout(const pxb_cloth_desc* desc, pxb_cloth_plan* out
     out->topology = e.list_gmem ? 2 : (e.list ? 1 : 0);
     out->lean = e.lean ? (e.soa ? 2 : 1) : 0;
     if (e.list) out->n_colours = static_cast<int32_t>(e.runs.size());
+    {
+        const uint32_t m = colour_sync_mask(e);
+        out->phases = e.list ? out->n_colours
+                             : __builtin_popcount(m & (e.n_colours >= 32 ? 0xffffffffu : ((1u << e.n_colours) - 1u)));
+    }
     return PXB_OK;
 }
 

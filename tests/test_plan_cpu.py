@@ -114,3 +114,20 @@ def test_swapped_pair_is_caught_by_item_verification():
     a, b = int(c.bend[k]["a"]), int(c.bend[k]["b"])
     c.bend[k]["a"], c.bend[k]["b"] = b, a
     assert R.plan_cloth(c)["topology"] == 1
+
+
+@pytest.mark.parametrize("shape,shear", [((16, 16), True), ((64, 64), True), ((96, 96), True), ((128, 128), True),
+                                         ((33, 20), False), ((150, 130), True)])
+def test_disjoint_bend_colours_share_a_phase(shape, shear):
+    """On one CTA, consecutive colours that touch disjoint particles run as one phase with no
+    barrier between them: the row bends of phases 0 and 1 (columns x = 0, 2 mod 4 against 1, 3),
+    of 2 and 3, and the same for the column bends. Every other pair of consecutive colours shares
+    particles, so a sheet's 16 colours (12 without shear) take 12 phases (8). Clusters keep a
+    barrier after every colour."""
+    plan = R.plan_cloth(sheet(*shape, shear=shear))
+    n_colours = 16 if shear else 12
+    assert plan["n_colours"] == n_colours
+    if plan["n_ranks"] == 1:
+        assert plan["phases"] == n_colours - 4
+    else:
+        assert plan["phases"] == n_colours

@@ -526,7 +526,8 @@ pxb_status pxb_context_set_lean_arrays(pxb_context* ctx, int32_t enable);
 /* Autotuner: times every kernel variant in both launch forms on `step` (the caller's real batch,
  * `trials` launches each after one warm-up) and keeps the fastest pair on the context. Then, one
  * layout class at a time (largest share of the batch first), it times the class's cloths at the
- * other two variants with the rest unchanged and keeps a variant that is faster. The listed
+ * other two variants with the rest unchanged, alternating with the current choice, and keeps a
+ * variant that is faster by more than 1 %. The listed
  * cloths' device state and host mirrors are saved first and restored after, so tuning does not
  * advance them. variant_out (may be NULL) receives variant + 3 * mode of the pair kept; ms_out
  * (may be NULL) six entries, milliseconds per step: variants 0-2 one CTA per cloth, then variants

@@ -2219,8 +2219,9 @@ pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step
             best = v;
         }
     }
-    // Per layout class, largest share first: the other variants for its cloths alone, kept when
-    // faster by more than the timing's noise (0.3 %).
+    // Per layout class, largest share first: each other variant for its cloths alone, timed in
+    // turn with the current choice (current, other, current, other, so that a drift of the clock
+    // over the comparison falls on both) and kept when faster by more than 1 %.
     if (!st) {
         ctx->cloth_variant = best % kClothVariants;
         ctx->launch_mode = best / kClothVariants;
@@ -2235,14 +2236,19 @@ pxb_status pxb_cloths_autotune(pxb_context* ctx, const pxb_cloth_step_desc* step
             const int c = classes[ci];
             int keep = 0;
             for (int v = 0; v < kClothVariants && !st; ++v) {
-                if (v == ctx->cloth_variant) continue;
-                ctx->class_variant[c] = v + 1;
-                float ms = 0.0f;
-                st = time_steps(ms);
-                if (!st && ms < cur * 0.997f) {
-                    cur = ms;
-                    keep = v + 1;
+                if (v == ctx->cloth_variant || v + 1 == keep) continue;
+                float base = 0.0f, alt = 0.0f;
+                for (int rep = 0; rep < 2 && !st; ++rep) {
+                    float ms = 0.0f;
+                    ctx->class_variant[c] = keep;
+                    st = time_steps(ms);
+                    base += ms;
+                    if (st) break;
+                    ctx->class_variant[c] = v + 1;
+                    st = time_steps(ms);
+                    alt += ms;
                 }
+                if (!st && alt < base * 0.99f) keep = v + 1;
             }
             ctx->class_variant[c] = keep;
         }

@@ -267,8 +267,10 @@ void pxb_cloth_params_default(pxb_cloth_params* out);
 /* ------------------------------------------------------------------------------------------ */
 
 /* Uploads a cloth. Refuses an empty cloth (n_particles == 0) like add_cloth does, and a cloth
- * the device path does not implement (self_collision on) with PXB_ERR_UNSUPPORTED. The returned
- * id is generational: it goes stale after pxb_cloth_remove. */
+ * the device path does not implement (self_collision on) with PXB_ERR_UNSUPPORTED. A cloth of
+ * general topology (constraint lists not make_grid_cloth's) may have up to 2^24 layout slots
+ * (4 * ceil(n_particles / 4)); beyond, PXB_ERR_TOO_LARGE. The returned id is generational: it
+ * goes stale after pxb_cloth_remove. */
 pxb_status pxb_cloth_add(pxb_context* ctx, const pxb_cloth_desc* desc, uint64_t* id_out);
 pxb_status pxb_cloth_remove(pxb_context* ctx, uint64_t id);
 

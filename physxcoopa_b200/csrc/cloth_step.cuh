@@ -227,34 +227,42 @@ __device__ __forceinline__ void project_segment(float4* __restrict__ pos, float4
 // share no particle, so they are projected like the items of a colour segment.
 template <bool kLam>
 __device__ __forceinline__ void load_run_item(PairItem& it, float4* pos, const float* rest, const uint32_t* ends,
-                                              const float* lamv, int i, int count) {
+                                              const float* lamv, int i, int count, bool wide = false) {
     it.live = i < count;
     const int ii = it.live ? i : 0;
-    const uint32_t w = ends[ii];
-    it.pa = &pos[w & 0xffffu];
-    it.pb = &pos[w >> 16];
+    if (wide) {  // two words per item: (a, b)
+        const uint2 w = reinterpret_cast<const uint2*>(ends)[ii];
+        it.pa = &pos[w.x];
+        it.pb = &pos[w.y];
+    } else {
+        const uint32_t w = ends[ii];
+        it.pa = &pos[w & 0xffffu];
+        it.pb = &pos[w >> 16];
+    }
     it.a = *it.pa;
     it.b = *it.pb;
     it.rest = rest[ii];
     it.lam = kLam ? lamv[ii] : 0.0f;
 }
 
-template <bool kLam, int kItems>
+// wide: ends holds (a, b) word pairs (a cloth of more than kListNarrowSlots slots, in HBM); the
+// runs' item offsets index items either way.
+template <bool kLam, int kItems, bool kWide = false>
 __device__ __forceinline__ void project_run(float4* __restrict__ pos, const float* __restrict__ rest,
                                             const uint32_t* __restrict__ ends, float* __restrict__ lamv, int count,
                                             float alpha, int tid, int T) {
     if constexpr (kItems == 2) {
         for (int i = tid; i < count; i += 2 * T) {
             PairItem x, y;
-            load_run_item<kLam>(x, pos, rest, ends, lamv, i, count);
-            load_run_item<kLam>(y, pos, rest, ends, lamv, i + T, count);
+            load_run_item<kLam>(x, pos, rest, ends, lamv, i, count, kWide);
+            load_run_item<kLam>(y, pos, rest, ends, lamv, i + T, count, kWide);
             project_item<kLam>(x, lamv, i, alpha);
             project_item<kLam>(y, lamv, i + T, alpha);
         }
     } else {
         for (int i = tid; i < count; i += T) {
             PairItem x;
-            load_run_item<kLam>(x, pos, rest, ends, lamv, i, count);
+            load_run_item<kLam>(x, pos, rest, ends, lamv, i, count, kWide);
             project_item<kLam>(x, lamv, i, alpha);
         }
     }
@@ -688,10 +696,22 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
                     for (int r = 0; r < n_runs; ++r) {
                         const int4 run = __ldg(&runs[r]);
                         const float alpha = __int_as_float(run.w) / hs2;
-                        if (run.z >= 0)
-                            project_run<true, kItems>(pos, rest + run.y, ends + run.y, U + run.z, run.x, alpha, tid, T);
-                        else
-                            project_run<false, kItems>(pos, rest + run.y, ends + run.y, U, run.x, alpha, tid, T);
+                        bool done = false;
+                        if constexpr (kG) {
+                            if (sC.n_layout > kListNarrowSlots) {  // endpoints as (a, b) word pairs
+                                if (run.z >= 0)
+                                    project_run<true, kItems, true>(pos, rest + run.y, ends + 2 * run.y, U + run.z, run.x, alpha, tid, T);
+                                else
+                                    project_run<false, kItems, true>(pos, rest + run.y, ends + 2 * run.y, U, run.x, alpha, tid, T);
+                                done = true;
+                            }
+                        }
+                        if (!done) {
+                            if (run.z >= 0)
+                                project_run<true, kItems>(pos, rest + run.y, ends + run.y, U + run.z, run.x, alpha, tid, T);
+                            else
+                                project_run<false, kItems>(pos, rest + run.y, ends + run.y, U, run.x, alpha, tid, T);
+                        }
                         __syncthreads();
                     }
                 }

@@ -106,7 +106,9 @@ struct PxbClothDev {
     const int4* tri_ent;        // one entry per triangle corner: the triangle's three corner slots
     int32_t n_runs;
     int32_t list_items_pad;     // items padded to 4: rest lengths are rest[0, pad), the packed
-                                // endpoint slots (a | b << 16) rest[pad, 2 * pad) as uint32 bits
+                                // endpoint slots (a | b << 16) rest[pad, 2 * pad) as uint32 bits,
+                                // or with more than kListNarrowSlots slots (a, b) pairs in
+                                // rest[pad, 3 * pad)
     float* list_scratch;        // topology 2: lambdas / parked velocities in HBM, max(pad, 3 n_layout)
     int32_t ref_columns;        // Cloth::columns as given: self-collision's 1-ring exemption reads it
     // 1: a lean grid cloth: only positions in shared memory, its rest lengths and lambdas read in
@@ -121,6 +123,11 @@ struct PxbClothDev {
 };
 
 #define PXB_MAX_WTAB 256
+
+// General-topology cloths: endpoint slots packed as a | b << 16 in one word while the layout has at
+// most 65535 slots; beyond, as two words (a, b) (only in HBM: such a cloth never fits shared memory).
+constexpr int kListNarrowSlots = 65535;
+constexpr int kListMaxSlots = 1 << 24;
 
 // A run of a general-topology cloth: consecutive items of one reference batch, no two of which
 // share a particle, so its items are projected in parallel between two block barriers.

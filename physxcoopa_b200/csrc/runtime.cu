@@ -427,6 +427,7 @@ float batch_compliance(const ClothEntry& e, bool bend, int b) {
 // one row of n (slot of particle i = (i % 4) * Q + i / 4), so every per-particle path of the
 // grid layout applies unchanged.
 pxb_status build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) {
+    static_assert(kListMaxSlots % 4 == 0, "slots are whole groups of four");
     const uint32_t n = d->n_particles;
     e.list = true;
     e.cols = static_cast<int>(n);
@@ -435,8 +436,8 @@ pxb_status build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) 
     e.S = 4 * e.Q;
     e.n_layout = e.S;
     e.n_particles = n;
-    if (e.n_layout > 65535) {
-        why = "a general-topology cloth holds at most 65532 particles";
+    if (e.n_layout > kListMaxSlots) {
+        why = "a general-topology cloth holds at most 16777212 particles";
         return PXB_ERR_TOO_LARGE;
     }
     e.runs.clear();
@@ -479,7 +480,7 @@ pxb_status build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) 
                 stamp[c.a] = stamp[c.b] = run_id;
                 const uint32_t la = static_cast<uint32_t>(slot_of_particle(static_cast<int>(c.a), e.cols, e.Q, e.S));
                 const uint32_t lb = static_cast<uint32_t>(slot_of_particle(static_cast<int>(c.b), e.cols, e.Q, e.S));
-                e.item_ends.push_back(la | lb << 16);
+                e.item_ends.push_back(la | static_cast<uint64_t>(lb) << 32);
                 e.rest_ref.push_back(ref);
                 max_run = std::max(max_run, ++e.runs.back().count);
             }
@@ -494,8 +495,8 @@ pxb_status build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) 
     for (const PxbRun& run : e.runs) {
         std::vector<std::vector<int>> bucket(64);
         for (int i = run.count - 1; i >= 0; --i) {
-            const uint32_t w = e.item_ends[run.item_base + i];
-            bucket[(w & 7u) * 8 + ((w >> 16) & 7u)].push_back(i);  // popped from the back: list order
+            const uint64_t w = e.item_ends[run.item_base + i];
+            bucket[(w & 7u) * 8 + ((w >> 32) & 7u)].push_back(i);  // popped from the back: list order
         }
         auto fuller = [&](int x, int y) { return bucket[x].size() > bucket[y].size(); };
         int match_b[8];
@@ -550,7 +551,7 @@ pxb_status build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) 
                 }
             left -= taken;
         }
-        std::vector<uint32_t> ends(run.count);
+        std::vector<uint64_t> ends(run.count);
         std::vector<int32_t> refs(run.count);
         for (int i = 0; i < run.count; ++i) {
             ends[i] = e.item_ends[run.item_base + order[i]];
@@ -563,7 +564,9 @@ pxb_status build_list(const pxb_cloth_desc* d, ClothEntry& e, std::string& why) 
     e.list_items_pad = (items + 3) & ~3;
     e.item_ends.resize(e.list_items_pad, 0u);
     e.rest_ref.resize(e.list_items_pad, -1);
-    e.n_rest_total = 2 * e.list_items_pad;
+    // endpoints after the rest lengths: one word per item (a | b << 16), or two (a, b) for a cloth
+    // of more than 65535 slots
+    e.n_rest_total = (list_wide(e) ? 3 : 2) * e.list_items_pad;
     e.n_colours = 0;
     e.segs.clear();
     e.colour_is_bend.clear();
@@ -1039,7 +1042,19 @@ pxb_status pxb_context::add_cloth(const pxb_cloth_desc* d, uint64_t* id_out) {
         rest_h[s] = r < static_cast<int32_t>(e.n_stretch) ? d->stretch[r].rest_length
                                                           : d->bend[r - e.n_stretch].rest_length;
     }
-    if (e.list) std::memcpy(rest_h.data() + e.list_items_pad, e.item_ends.data(), 4 * e.item_ends.size());
+    if (e.list) {
+        uint32_t* w = reinterpret_cast<uint32_t*>(rest_h.data() + e.list_items_pad);
+        for (size_t i = 0; i < e.item_ends.size(); ++i) {
+            const uint64_t v = e.item_ends[i];
+            const uint32_t la = static_cast<uint32_t>(v), lb = static_cast<uint32_t>(v >> 32);
+            if (list_wide(e)) {
+                w[2 * i] = la;
+                w[2 * i + 1] = lb;
+            } else {
+                w[i] = la | lb << 16;
+            }
+        }
+    }
     e.topology.resize(d->n_stretch + d->n_bend);
     for (uint32_t k = 0; k < d->n_stretch; ++k) e.topology[k] = {d->stretch[k].a, d->stretch[k].b, d->stretch[k].rest_length};
     for (uint32_t k = 0; k < d->n_bend; ++k) e.topology[d->n_stretch + k] = {d->bend[k].a, d->bend[k].b, d->bend[k].rest_length};

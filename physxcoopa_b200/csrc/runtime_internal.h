@@ -60,7 +60,7 @@ struct ClothEntry {
     int ref_columns = 0;     // Cloth::columns as given (self-collision's 1-ring exemption)
     std::vector<PxbRun> runs;
     std::vector<int2> run_batch;
-    std::vector<uint32_t> item_ends;
+    std::vector<uint64_t> item_ends;  // per item: a slot | b slot << 32
     int list_items_pad = 0;
     std::vector<int32_t> tri_off;
     std::vector<int4> tri_ent;
@@ -82,6 +82,9 @@ struct ClothEntry {
     PxbWarmResult warm_result{};
     bool has_warm_result = false;
 };
+
+// General-topology endpoints stored as two words per item (more than 65535 layout slots).
+inline bool list_wide(const ClothEntry& e) { return e.list && e.n_layout > kListNarrowSlots; }
 
 // One registered strand set (hair::StrandSet mirrors + device buffers).
 struct StrandEntry {

@@ -165,11 +165,14 @@ def test_plan_general_topology_refusals():
     big = R.plan_cloth(S.mesh_cloth(34, tethers=False))
     assert big["topology"] == 2 and big["smem_bytes"] == 0 and big["n_ranks"] == 1 and big["threads"] <= 1024
     assert big["self_collision"] == 0  # its hash tables would need the shared memory it does not get
-    # past the 16-bit slot of the packed endpoints
+    # past the 16-bit slot of one packed endpoint word: two words per item, three times the
+    # padded item count of rest-length and endpoint slots
     v, ix = S.disc_mesh(0.5, 149)  # 67,051 particles
-    with pytest.raises(R.PxbError) as e:
-        R.plan_cloth(R.HostCloth.from_mesh(v, ix, bend=False).arrays())
-    assert e.value.status == A.PXB_ERR_TOO_LARGE
+    wide = R.plan_cloth(R.HostCloth.from_mesh(v, ix, bend=False).arrays())
+    assert wide["topology"] == 2 and wide["layout_slots"] > 65535
+    assert wide["constraint_slots"] % 3 == 0 and wide["constraint_slots"] // 3 % 4 == 0
+    narrow = R.plan_cloth(S.mesh_cloth(34, tethers=False))
+    assert narrow["constraint_slots"] % 2 == 0
 
 
 def oracle_vs_reference(c, colliders, steps, iterations=10):

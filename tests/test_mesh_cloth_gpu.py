@@ -240,3 +240,15 @@ def test_cloths_beyond_shared_memory_solve_in_hbm(ctx):
     cloths = [big.cloths[0], huge, small.cloths[0]]
     cols = [big.colliders[0], collider_array([sphere(0.2, (3.0, 0.1, 0.6))]), small.colliders[0]]
     run_against_oracle(ctx, cloths, cols, steps=12, check_every=4, what="hbm")
+
+
+def test_mesh_cloth_beyond_16_bit_slots_equals_oracle(ctx):
+    """A mesh cloth of more than 65535 layout slots (a disc of 150 rings: 67,951 particles) keeps
+    its constraint endpoints as two 32-bit words per item instead of one packed word; solved in
+    HBM, equal to the oracle."""
+    sc = S.mesh_drape(rings=150, seed=9)
+    cloth = sc.cloths[0]
+    assert len(cloth.particles) > 65535
+    plan = R.plan_cloth(cloth)
+    assert plan["topology"] == 2 and plan["layout_slots"] > 65535
+    run_against_oracle(ctx, [cloth], [sc.colliders[0]], steps=3, check_every=3, what="wide")

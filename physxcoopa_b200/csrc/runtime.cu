@@ -963,7 +963,13 @@ static pxb_status plan_cloth(const pxb_cloth_desc* d, ClothEntry& e, std::string
     const struct { int cl; bool lean, soa; } tries[] = {{1, false, false}, {1, true, false}, {1, true, true},
                                                         {2, true, false}, {2, false, false}, {4, false, false},
                                                         {8, false, false}};
-    auto smem_ctas = [](int bytes) { return 233472 / (bytes + kClothStaticSmem + 1024); };
+    // CTAs per SM by shared memory, with the self-collision tables when the cloth comes with
+    // self-collision on (they may take more room beside a lean sheet's positions)
+    const bool self_at_add = self_on(e);
+    auto smem_ctas = [&](int bytes) {
+        const int b = self_at_add && e.self_ok ? std::max(bytes, e.self_smem) : bytes;
+        return 233472 / (b + kClothStaticSmem + 1024);
+    };
     bool whole_fits = false;  // held whole, one CTA per SM: kept unless the lean layout does better
     for (const auto& t : tries) {
         if (placed) break;

@@ -64,12 +64,14 @@ def run_pair(ctx, cloth, cols, steps, iterations=10):
 
 @pytest.mark.parametrize("side", [9, 24, 48, 64, 80])
 def test_folding_sheet_equals_oracle(ctx, side):
-    """Up to 44 the sheet is all in shared memory; from 48 (where an SM would hold only one CTA of
-    the whole sheet) it is lean (positions only in shared memory, rest lengths and lambdas in HBM)
-    and the hash tables take the room after the positions."""
+    """Up to 44 the sheet is all in shared memory. At 48 an SM would hold one CTA of the whole
+    sheet but two of the lean one with its hash tables, so it is lean (positions only in shared
+    memory, rest lengths and lambdas in HBM, the hash tables after the positions). At 64 the lean
+    sheet with its tables leaves one CTA per SM too, so it stays whole. At 80 only the lean layout
+    fits."""
     cloth, cols = folding_sheet(side)
     plan = R.plan_cloth(cloth)
-    assert plan["n_ranks"] == 1 and plan["self_collision"] == 1 and plan["lean"] == (side > 44)
+    assert plan["n_ranks"] == 1 and plan["self_collision"] == 1 and plan["lean"] == (side in (48, 80))
     gpu, orc = run_pair(ctx, cloth, cols, 1)
     assert maxdiff(gpu["position"], orc.particles["position"]) <= 1e-5
     assert_equal_particles(gpu, orc.particles, "step 1")

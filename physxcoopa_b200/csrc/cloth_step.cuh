@@ -218,7 +218,7 @@ __device__ __forceinline__ void project_segment(float4* __restrict__ pos, float4
                                 row_stride, d);
             project_item<kLam>(x, lamv, i, alpha);
         }
-        i0 = i - count;  // the thread's first item of the colour's next segment
+        i0 = i - count;  // the thread's first item in the next segment of the phase
     }
 }
 
@@ -410,7 +410,7 @@ __device__ __forceinline__ void project_segment_soa(const SoaPos& P, const float
 // The constraint iterations of a one-CTA grid cloth, out of line
 // ------------------------------------------------------------------------------------------
 
-// `iters` sweeps of every colour, a CTA barrier after each. Called, not inlined, from the step
+// `iters` sweeps of every colour, a CTA barrier after each phase. Called, not inlined, from the step
 // kernel: the projection loop is then register-allocated on its own instead of sharing the
 // kernel's register budget (64 per thread at 1024 threads) with every value the kernel keeps
 // live across the iterations; the call's register saves happen once per substep.

@@ -407,6 +407,44 @@ __device__ __forceinline__ void project_segment_soa(const SoaPos& P, const float
 }
 
 // ------------------------------------------------------------------------------------------
+// The constraint iterations of a general-topology cloth (one CTA), out of line
+// ------------------------------------------------------------------------------------------
+
+// `iters` walks of the runs in order, a CTA barrier after each run; alpha of a run evaluated as
+// the reference does, compliance / (hs * hs). Out of line for the same reason as the grid loop
+// below. kWideOk compiles the two-word endpoint form in (the instantiation whose state is in HBM,
+// the only one a cloth of more than kListNarrowSlots slots runs in); `wide` selects it.
+template <int kItems, bool kWideOk>
+__device__ __noinline__ void list_iterations(int iters, int n_runs, const int4* __restrict__ runs, float hs2,
+                                             float4* __restrict__ pos, const float* __restrict__ rest,
+                                             const uint32_t* __restrict__ ends, float* __restrict__ U, bool wide,
+                                             int tid, int T) {
+    for (int it = 0; it < iters; ++it) {
+        for (int r = 0; r < n_runs; ++r) {
+            const int4 run = __ldg(&runs[r]);
+            const float alpha = __int_as_float(run.w) / hs2;
+            bool done = false;
+            if constexpr (kWideOk) {
+                if (wide) {
+                    if (run.z >= 0)
+                        project_run<true, kItems, true>(pos, rest + run.y, ends + 2 * run.y, U + run.z, run.x, alpha, tid, T);
+                    else
+                        project_run<false, kItems, true>(pos, rest + run.y, ends + 2 * run.y, U, run.x, alpha, tid, T);
+                    done = true;
+                }
+            }
+            if (!done) {
+                if (run.z >= 0)
+                    project_run<true, kItems>(pos, rest + run.y, ends + run.y, U + run.z, run.x, alpha, tid, T);
+                else
+                    project_run<false, kItems>(pos, rest + run.y, ends + run.y, U, run.x, alpha, tid, T);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // The constraint iterations of a one-CTA grid cloth, out of line
 // ------------------------------------------------------------------------------------------
 
@@ -687,34 +725,11 @@ cloth_step_kernel(const PxbClothDev* __restrict__ cloths, const PxbClothStep* __
             if (sC.topology != 0) {
                 // general topology: run after run, a block barrier after each; alpha evaluated
                 // as the reference does, compliance / (hs * hs)
-                const int n_runs = sC.n_runs;
                 const uint32_t* ends = reinterpret_cast<const uint32_t*>(rest + sC.list_items_pad);
-                const int4* runs = reinterpret_cast<const int4*>(sC.runs);
-                const float hs2 = sP.hs * sP.hs;
                 constexpr int kItems = kMaxThreads <= 512 ? 2 : 1;
-                for (int it = 0; it < iters; ++it) {
-                    for (int r = 0; r < n_runs; ++r) {
-                        const int4 run = __ldg(&runs[r]);
-                        const float alpha = __int_as_float(run.w) / hs2;
-                        bool done = false;
-                        if constexpr (kG) {
-                            if (sC.n_layout > kListNarrowSlots) {  // endpoints as (a, b) word pairs
-                                if (run.z >= 0)
-                                    project_run<true, kItems, true>(pos, rest + run.y, ends + 2 * run.y, U + run.z, run.x, alpha, tid, T);
-                                else
-                                    project_run<false, kItems, true>(pos, rest + run.y, ends + 2 * run.y, U, run.x, alpha, tid, T);
-                                done = true;
-                            }
-                        }
-                        if (!done) {
-                            if (run.z >= 0)
-                                project_run<true, kItems>(pos, rest + run.y, ends + run.y, U + run.z, run.x, alpha, tid, T);
-                            else
-                                project_run<false, kItems>(pos, rest + run.y, ends + run.y, U, run.x, alpha, tid, T);
-                        }
-                        __syncthreads();
-                    }
-                }
+                const bool wide = kG && sC.n_layout > kListNarrowSlots;  // endpoints as (a, b) word pairs
+                list_iterations<kItems, kG>(iters, sC.n_runs, reinterpret_cast<const int4*>(sC.runs), sP.hs * sP.hs,
+                                            pos, rest, ends, U, wide, tid, T);
                 return;
             }
         }

@@ -131,3 +131,35 @@ def test_disjoint_bend_colours_share_a_phase(shape, shear):
         assert plan["phases"] == n_colours - 4
     else:
         assert plan["phases"] == n_colours
+
+
+def expected_phases(c):
+    """Phases per iteration restated from the cloth's own batches: the non-empty batches in the
+    reference's order (stretch, then bend), a phase growing while the next batch shares no
+    particle with any batch already in it."""
+    sets = []
+    for cons, batches in ((c.stretch, c.stretch_batches), (c.bend, c.bend_batches)):
+        for b in batches:
+            part = cons[int(b["begin"]):int(b["end"])]
+            if len(part):
+                sets.append(set(part["a"].tolist()) | set(part["b"].tolist()))
+    phases, cur = 0, None
+    for s in sets:
+        if cur is not None and not (cur & s):
+            cur |= s
+        else:
+            phases += 1
+            cur = set(s)
+    return phases
+
+
+@pytest.mark.parametrize("shape", [(2, 2), (3, 3), (2, 7), (5, 3), (4, 9), (7, 7), (9, 4), (17, 5), (30, 31), (44, 44)])
+@pytest.mark.parametrize("shear", [True, False])
+def test_phases_match_a_restatement_from_the_batches(shape, shear):
+    """The host's phase split (colour_sync_mask) against the same rule applied to the reference's
+    own batches, on sheets small enough that some colours are empty and others lose their
+    neighbours."""
+    c = sheet(*shape, shear=shear)
+    plan = R.plan_cloth(c)
+    assert plan["n_ranks"] == 1 and plan["topology"] == 0
+    assert plan["phases"] == expected_phases(c)

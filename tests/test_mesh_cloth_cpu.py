@@ -197,6 +197,17 @@ def test_oracle_equals_reference_on_a_mesh_cloth():
 
 
 @pytest.mark.skipif(not K.ref_available(), reason="oracle/_ref not built")
+def test_oracle_equals_reference_on_a_mesh_cloth_past_16_bit_slots():
+    """The 67,951-particle disc the device solves with two-word endpoints: oracle and compiled
+    reference agree on it too."""
+    sc = S.mesh_drape(rings=150, seed=9)
+    c = sc.cloths[0]
+    assert len(c.particles) > 65535
+    c.params.has_shear_compliance = 0
+    oracle_vs_reference(c, sc.colliders[0], steps=2)
+
+
+@pytest.mark.skipif(not K.ref_available(), reason="oracle/_ref not built")
 def test_oracle_equals_reference_on_serial_grid_lists():
     sc = S.single_drape(seed=6)
     c = unbatched(sc.cloths[0])
